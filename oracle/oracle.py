@@ -1,0 +1,233 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings of the FP64 CPU oracle.
+
+The oracle restates the reference (ESPResSo) CPU P3M + short-range path in
+FP64 and adds an independent direct Ewald sum.  Only the test suite, the
+smoke check and the CPU-baseline leg of bench.py import this module; the
+product path never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_REF = os.path.join(_HERE, "_ref", "libref_math.so")
+
+
+class P3MParams(ctypes.Structure):
+    _fields_ = [("box", ctypes.c_double * 3), ("mesh", ctypes.c_int * 3),
+                ("cao", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("r_cut", ctypes.c_double), ("prefactor", ctypes.c_double),
+                ("epsilon", ctypes.c_double), ("mesh_off", ctypes.c_double * 3),
+                ("skin", ctypes.c_double)]
+
+
+class PairParams(ctypes.Structure):
+    _fields_ = [("lj_eps", ctypes.c_double), ("lj_sig", ctypes.c_double),
+                ("lj_cut", ctypes.c_double), ("lj_shift", ctypes.c_double),
+                ("lj_offset", ctypes.c_double), ("lj_min", ctypes.c_double),
+                ("wca_eps", ctypes.c_double), ("wca_sig", ctypes.c_double)]
+
+
+def build():
+    """Compile liboracle.so (and the reference-math shim when the reference
+    tree is present) with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _load():
+    if not os.path.exists(_LIB):
+        build()
+    lib = ctypes.CDLL(_LIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    lp = ctypes.POINTER(ctypes.c_long)
+    pp = ctypes.POINTER(P3MParams)
+    lib.oracle_p3m_kspace.argtypes = [pp, ctypes.c_long, dp, dp, dp, dp, dp, dp]
+    lib.oracle_influence_function.argtypes = [pp, dp]
+    lib.oracle_short_range.argtypes = [pp, ctypes.c_long, dp, dp, ip, ctypes.c_int,
+                                       ctypes.POINTER(PairParams), dp, dp, dp]
+    lib.oracle_cell_grid.argtypes = [dp, ctypes.c_double, ip, dp]
+    lib.oracle_cell_index.argtypes = [dp, ctypes.c_double, ctypes.c_long, dp, ip]
+    lib.oracle_verlet_pairs.argtypes = [dp, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_long, dp, dp, ip, ctypes.c_int,
+                                        dp, ctypes.c_long, lp]
+    lib.oracle_verlet_pairs.restype = ctypes.c_long
+    lib.oracle_rs_error.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_double, dp]
+    lib.oracle_rs_error.restype = ctypes.c_double
+    lib.oracle_ks_error.argtypes = [ctypes.c_double, ip, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, ctypes.c_double, dp]
+    lib.oracle_ks_error.restype = ctypes.c_double
+    lib.oracle_ewald.argtypes = [dp, ctypes.c_long, dp, dp, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double, dp, dp]
+    for name in ("oracle_bspline", "oracle_as_erfc_part", "oracle_sinc",
+                 "oracle_cotangent_sum"):
+        getattr(lib, name).restype = ctypes.c_double
+    lib.oracle_bspline.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    lib.oracle_as_erfc_part.argtypes = [ctypes.c_double]
+    lib.oracle_sinc.argtypes = [ctypes.c_double]
+    lib.oracle_cotangent_sum.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    return lib
+
+
+lib = _load()
+
+
+def ref_math():
+    """The reference's own math headers behind a C ABI, or None when the
+    shim was not built (reference tree absent)."""
+    if not os.path.exists(_REF):
+        return None
+    r = ctypes.CDLL(_REF)
+    for name in ("ref_bspline", "ref_as_erfc_part", "ref_sinc", "ref_cotangent_sum"):
+        getattr(r, name).restype = ctypes.c_double
+    r.ref_bspline.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    r.ref_as_erfc_part.argtypes = [ctypes.c_double]
+    r.ref_sinc.argtypes = [ctypes.c_double]
+    r.ref_cotangent_sum.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    return r
+
+
+def _d(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def make_params(box, mesh, cao, alpha, r_cut, prefactor, epsilon=0.0,
+                mesh_off=(0.5, 0.5, 0.5), skin=0.4):
+    p = P3MParams()
+    box = np.broadcast_to(np.asarray(box, dtype=float), (3,))
+    mesh = np.broadcast_to(np.asarray(mesh, dtype=int), (3,))
+    for d in range(3):
+        p.box[d] = float(box[d])
+        p.mesh[d] = int(mesh[d])
+        p.mesh_off[d] = float(mesh_off[d])
+    p.cao, p.alpha, p.r_cut = int(cao), float(alpha), float(r_cut)
+    p.prefactor, p.epsilon, p.skin = float(prefactor), float(epsilon), float(skin)
+    return p
+
+
+def p3m_kspace(params, pos, q, want_mesh=False):
+    """k-space forces (N,3), energy and the k-space virial tensor (3,3)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    n = len(q)
+    f = np.zeros((n, 3))
+    e = np.zeros(1)
+    v = np.zeros(9)
+    rho = np.zeros(tuple(params.mesh)) if want_mesh else None
+    rc = lib.oracle_p3m_kspace(ctypes.byref(params), n, _d(pos), _d(q), _d(f),
+                               _d(e), _d(v), _d(rho) if want_mesh else None)
+    if rc:
+        raise RuntimeError(f"oracle_p3m_kspace failed ({rc})")
+    out = (f, e[0], v.reshape(3, 3))
+    return out + (rho,) if want_mesh else out
+
+
+def influence_function(params):
+    g = np.zeros(tuple(params.mesh))
+    lib.oracle_influence_function(ctypes.byref(params), _d(g))
+    return g
+
+
+def pair_table(ntypes, entries):
+    """entries: dict {(ti, tj): dict(lj_eps=..., ...)} filled symmetrically."""
+    tab = (PairParams * (ntypes * ntypes))()
+    for (a, b), kw in entries.items():
+        for (x, y) in ((a, b), (b, a)):
+            e = tab[x * ntypes + y]
+            for k, v in kw.items():
+                setattr(e, k, float(v))
+    return tab
+
+
+def short_range(params, pos, q, types=None, ntypes=1, tab=None):
+    """Real-space Coulomb + LJ/WCA forces, energies {coulomb, non_bonded}
+    and virials (two 3x3)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    n = len(q)
+    f = np.zeros((n, 3))
+    e = np.zeros(2)
+    v = np.zeros(18)
+    t = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
+    rc = lib.oracle_short_range(ctypes.byref(params), n, _d(pos), _d(q),
+                                _i(t) if t is not None else None, ntypes, tab,
+                                _d(f), _d(e), _d(v))
+    if rc:
+        raise RuntimeError(f"oracle_short_range failed ({rc})")
+    return f, e, v[:9].reshape(3, 3), v[9:].reshape(3, 3)
+
+
+def cell_grid(box, range_):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    cg = np.zeros(3, dtype=np.int32)
+    cs = np.zeros(3)
+    rc = lib.oracle_cell_grid(_d(box), float(range_), _i(cg), _d(cs))
+    if rc:
+        raise RuntimeError(f"oracle_cell_grid failed ({rc})")
+    return cg, cs
+
+
+def cell_index(box, range_, pos):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    out = np.zeros(len(pos), dtype=np.int32)
+    rc = lib.oracle_cell_index(_d(box), float(range_), len(pos), _d(pos), _i(out))
+    if rc:
+        raise RuntimeError(f"oracle_cell_index failed ({rc})")
+    return out
+
+
+def verlet_pairs(box, skin, coulomb_cut, pos, q, types=None, ia_cut=None):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    n = len(q)
+    if ia_cut is None:
+        ia_cut = np.full((1, 1), -1.0)
+    ia_cut = np.ascontiguousarray(ia_cut, dtype=np.float64)
+    nt = ia_cut.shape[0]
+    t = None if types is None else np.ascontiguousarray(types, dtype=np.int32)
+    cap = max(16, 64 * n)
+    while True:
+        out = np.zeros(2 * cap, dtype=np.int64)
+        cnt = lib.oracle_verlet_pairs(_d(box), float(skin), float(coulomb_cut), n,
+                                      _d(pos), _d(q), _i(t) if t is not None else None,
+                                      nt, _d(ia_cut), cap,
+                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
+        if cnt == -1:
+            cap *= 4
+            continue
+        if cnt < 0:
+            raise RuntimeError("oracle_verlet_pairs failed")
+        return out[:2 * cnt].reshape(-1, 2)
+
+
+def rs_error(pref, r_cut_iL, n_c_part, sum_q2, alpha_L, box):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    return lib.oracle_rs_error(pref, r_cut_iL, n_c_part, sum_q2, alpha_L, _d(box))
+
+
+def ks_error(pref, mesh, cao, n_c_part, sum_q2, alpha_L, box):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    m = np.ascontiguousarray(np.broadcast_to(mesh, (3,)), dtype=np.int32)
+    return lib.oracle_ks_error(pref, _i(m), cao, n_c_part, sum_q2, alpha_L, _d(box))
+
+
+def ewald(box, pos, q, prefactor, alpha, r_cut, kmax, epsilon=0.0):
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    f = np.zeros((len(q), 3))
+    e = np.zeros(1)
+    lib.oracle_ewald(_d(box), len(q), _d(pos), _d(q), prefactor, alpha, r_cut,
+                     int(kmax), epsilon, _d(f), _d(e))
+    return f, e[0]

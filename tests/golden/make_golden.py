@@ -1,0 +1,113 @@
+"""Generate the golden fixtures under tests/golden/ from the reference tree.
+
+Run once in a container that has the ESPResSo source tree (default
+/root/reference, override with $P3MX_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+Sources (paths relative to the ESPResSo tree):
+  * testsuite/python/data/coulomb_cloud_wall_system.data  (id pos q f)
+    with the parameters and energy of testsuite/python/coulomb_cloud_wall.py:40-47
+  * testsuite/python/data/coulomb_tuning_system.npz (coulomb_tuning.py:37-47)
+  * testsuite/python/data/lj_system.dat (lj.py:28-47)
+  * known answers written in testsuite/python/electrostatic_interactions.py:81-124
+    and testsuite/python/p3m_madelung.py:202-313 (parameters and constants)
+  * values of the reference's own math headers (bspline.hpp, AS_erfc_part.hpp,
+    p3m/math.hpp) evaluated through oracle/_ref/libref_math.so, which
+    oracle/Makefile compiles from the reference tree in place.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("P3MX_REFERENCE", "/root/reference")
+DATA = os.path.join(REF, "testsuite", "python", "data")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+
+def main():
+    d = np.genfromtxt(os.path.join(DATA, "coulomb_cloud_wall_system.data"))
+    np.savez_compressed(
+        os.path.join(HERE, "coulomb_cloud_wall.npz"),
+        pos=d[:, 1:4], q=d[:, 4], forces=d[:, 5:8],
+        box=np.array([10., 10., 10.]), mesh=np.array([64, 64, 64]), cao=7,
+        alpha=2.70746, r_cut=1.001, accuracy=1e-3, energy=148.94229549,
+        force_atol=2e-3, energy_atol=1e-3)
+
+    t = np.load(os.path.join(DATA, "coulomb_tuning_system.npz"))
+    np.savez_compressed(os.path.join(HERE, "coulomb_tuning.npz"),
+                        pos=t["pos"], q=t["charges"], forces=t["forces"],
+                        box=np.array([10., 10., 10.]), accuracy=5e-4,
+                        force_atol=2e-3)
+
+    lj = np.loadtxt(os.path.join(DATA, "lj_system.dat"))
+    np.savez_compressed(os.path.join(HERE, "lj_system.npz"),
+                        pos=lj[:, 1:4], forces=lj[:, 4:7], box=10.7437,
+                        eps=1.0, sig=1.0, cut=1.12246, skin=0.4,
+                        shift=0.2499999999700293)
+
+    known = {
+        "two_charges": {
+            "source": "testsuite/python/electrostatic_interactions.py:81-124",
+            "box": 20.0, "pos": [[9.0, 2.0, 2.0], [11.0, 2.0, 2.0]],
+            "q": [1.0, -1.0], "prefactor": 1.1, "mesh": 22, "cao": 7,
+            "r_cut": 8.90625, "alpha": 0.387611049779351, "accuracy": 1e-7,
+            "energy_per_prefactor": -0.501062398379,
+            "force_x_per_prefactor": 0.248921612, "tol": 1e-5,
+            "dipole_tol": 1e-10},
+        "madelung_wire": {
+            "source": "testsuite/python/p3m_madelung.py:202-234",
+            "n_pairs": 64, "mesh": 32, "cao": 7, "r_cut": 14.0,
+            "alpha": 0.27362958, "accuracy": 1e-8,
+            "madelung": float(-2.0 * np.log(2.0)), "base": [0, 0, 1],
+            "energy_rtol": 5e-7, "pressure_rtol": 1e-6},
+        "madelung_sheet": {
+            "source": "testsuite/python/p3m_madelung.py:236-277",
+            "n_pairs": 24, "mesh": 48, "cao": 7, "r_cut": 22.0,
+            "alpha": 0.179719, "accuracy": 1e-8,
+            "madelung": -1.6155426267128247, "base": [1, 1, 0],
+            "energy_rtol": 1e-7, "pressure_rtol": 5e-7},
+        "madelung_cube": {
+            "source": "testsuite/python/p3m_madelung.py:279-313",
+            "n_pairs": 6, "mesh": 72, "cao": 7, "r_cut": 5.6,
+            "alpha": 0.8163977, "accuracy": 1e-9,
+            "madelung": -1.74756459463318219, "base": [1, 1, 1],
+            "energy_rtol": 1e-6, "pressure_rtol": 5e-6,
+            "gpu_params": {"mesh": 42, "cao": 7, "r_cut": 5.5,
+                           "alpha": 0.709017, "accuracy": 3e-7}},
+    }
+    with open(os.path.join(HERE, "known_answers.json"), "w") as fh:
+        json.dump(known, fh, indent=1)
+
+    from oracle import oracle as O
+    O.build()
+    r = O.ref_math()
+    if r is None:
+        raise SystemExit("oracle/_ref/libref_math.so missing: reference tree absent")
+    xs = np.linspace(-0.5, 0.5, 41)
+    bs = np.zeros((8, 7, len(xs)))
+    for order in range(1, 8):
+        for i in range(order):
+            for k, x in enumerate(xs):
+                bs[order, i, k] = r.ref_bspline(order, i, float(x))
+    ds = np.linspace(0.0, 6.0, 121)
+    ase = np.array([r.ref_as_erfc_part(float(x)) for x in ds])
+    ss = np.linspace(-1.0, 1.0, 201)
+    sinc = np.array([r.ref_sinc(float(x)) for x in ss])
+    meshes = np.array([16, 22, 32, 42, 64])
+    cot = np.zeros((8, len(meshes), 64))
+    for cao in range(1, 8):
+        for mi, m in enumerate(meshes):
+            for n in range(-m // 2, m // 2):
+                cot[cao, mi, n + 32] = r.ref_cotangent_sum(cao, n, 1.0 / m)
+    np.savez_compressed(os.path.join(HERE, "ref_math.npz"), bspline_x=xs,
+                        bspline=bs, as_erfc_d=ds, as_erfc=ase, sinc_x=ss,
+                        sinc=sinc, cot_meshes=meshes, cot=cot)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
