@@ -1,0 +1,901 @@
+// C ABI of the drop-in boundary (include/p3mx.h): actor life cycle,
+// parameter validation with the reference's messages, the P3M tuner, and
+// host<->device staging.  No exception crosses the ABI.
+#include "../../include/p3mx.h"
+#include "engine.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace p3mx;
+
+namespace {
+
+constexpr double kMeshOff = 0.5;            // P3M_MESHOFF, config.hpp:45-46
+constexpr double kTuneCaoTooLarge = 1.0;    // TuningAlgorithm.cpp:47-51
+constexpr double kTuneAccTooLarge = 3.0;
+constexpr double kRcutPrec = 1e-3;          // P3M_RCUT_PREC
+constexpr double kTimeGranularity = 2.0;    // TuningAlgorithm.hpp:82
+constexpr int kMaxConsecutiveTrials = 20;   // TuningAlgorithm.hpp:86
+
+// pinned host staging for host-pointer calls
+struct Pinned {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~Pinned() {
+    if (p)
+      cudaFreeHost(p);
+  }
+  void ensure(size_t n) {
+    if (n <= bytes && p)
+      return;
+    if (p)
+      cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMallocHost(&p, n ? n : 16) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(P3MX_ENOMEM, "pinned host allocation failed");
+    }
+    bytes = n ? n : 16;
+  }
+  template <typename T> T *as() { return static_cast<T *>(p); }
+};
+
+bool mesh_fft_ok(int m) {
+  if (m < 2 || (m % 2))
+    return false;
+  int x = m;
+  for (int p = 2; p <= 31; ++p)
+    while (x % p == 0)
+      x /= p;
+  return x == 1;
+}
+
+} // namespace
+
+struct p3mx_handle {
+  p3mx_params prm{};
+  p3mx_system sys{};
+  bool sys_set = false;
+  // current P3M parameters (given or tuned)
+  int mesh[3] = {-1, -1, -1};
+  int cao = -1;
+  double r_cut = -1, alpha = -1, accuracy = 0, mesh_off[3] = {kMeshOff, kMeshOff, kMeshOff};
+  double r_cut_iL = 0, alpha_L = 0;
+  bool is_tuned = false, activated = false;
+  double rs_err = 0, ks_err = 0;
+  std::unique_ptr<Engine> eng;
+  size_t n = 0;
+  int ntypes = 1;
+  std::vector<PairIA> table{PairIA{0, 0, 0, 0, 0, 0, 0, 0, 0, -1.0}};
+  std::string err;
+  Pinned h_in, h_out;
+  // charge census
+  int n_charged = 0;
+  double sum_q2 = 0, sum_q = 0;
+};
+
+namespace {
+
+int fail(p3mx_handle *h, Error const &e) {
+  if (h)
+    h->err = e.what();
+  return e.code;
+}
+
+template <typename F> int guarded(p3mx_handle *h, F &&fn) {
+  if (!h)
+    return P3MX_EHANDLE;
+  try {
+    fn();
+    h->err.clear();
+    return P3MX_OK;
+  } catch (Error const &e) {
+    return fail(h, e);
+  } catch (std::exception const &e) {
+    h->err = e.what();
+    return P3MX_ERUNTIME;
+  }
+}
+
+// P3MParameters constructor checks (p3m/common.hpp:95-150) and the
+// prefactor check of Actor::set_prefactor (actor.hpp:49-54).
+void validate(p3mx_params const &p) {
+  bool const tuning = p.tune != 0;
+  if (p.prefactor <= 0.)
+    throw Error(P3MX_EDOMAIN, "Parameter 'prefactor' must be > 0");
+  if (p.epsilon < 0.)
+    throw Error(P3MX_EDOMAIN, "Parameter 'epsilon' must be >= 0");
+  if (p.accuracy <= 0.)
+    throw Error(P3MX_EDOMAIN, "Parameter 'accuracy' must be > 0");
+  if (p.r_cut <= 0. && !(tuning && p.r_cut == -1.))
+    throw Error(P3MX_EDOMAIN, "Parameter 'r_cut' must be > 0");
+  if (p.alpha <= 0. && !(tuning && p.alpha == -1.))
+    throw Error(P3MX_EDOMAIN, "Parameter 'alpha' must be > 0");
+  bool const all_pos = p.mesh[0] >= 1 && p.mesh[1] >= 1 && p.mesh[2] >= 1;
+  bool const first_only = p.mesh[0] >= 1 && p.mesh[1] == -1 && p.mesh[2] == -1;
+  bool const all_tune = tuning && p.mesh[0] == -1 && p.mesh[1] == -1 && p.mesh[2] == -1;
+  if (!(all_pos || first_only || all_tune))
+    throw Error(P3MX_EDOMAIN, "Parameter 'mesh' must be > 0");
+  for (int d = 0; d < 3; ++d)
+    if (p.mesh[d] != -1 && p.mesh[d] % 2)
+      throw Error(P3MX_EDOMAIN, "P3M requires an even number of mesh points in all directions");
+  bool const off_ok = p.mesh_off[0] >= 0. && p.mesh_off[0] <= 1. && p.mesh_off[1] >= 0. &&
+                      p.mesh_off[1] <= 1. && p.mesh_off[2] >= 0. && p.mesh_off[2] <= 1.;
+  bool const off_default = p.mesh_off[0] == -1. && p.mesh_off[1] == -1. && p.mesh_off[2] == -1.;
+  if (!off_ok && !off_default)
+    throw Error(P3MX_EDOMAIN, "Parameter 'mesh_off' must be >= 0 and <= 1");
+  if ((p.cao < 1 || p.cao > 7) && (!tuning || p.cao != -1))
+    throw Error(P3MX_EDOMAIN, "Parameter 'cao' must be >= 1 and <= 7");
+  if (!tuning && (p.cao > p.mesh[0] || p.cao > p.mesh[1] || p.cao > p.mesh[2]))
+    throw Error(P3MX_EDOMAIN, "Parameter 'cao' cannot be larger than 'mesh'");
+  if (p.charge_neutrality_tolerance < 0. && p.charge_neutrality_tolerance != -1.)
+    throw Error(P3MX_EDOMAIN, "Parameter 'charge_neutrality_tolerance' must be >= 0");
+}
+
+std::string actor_name(p3mx_handle const *h) {
+  return h->prm.single_precision ? "CoulombP3MGPU" : "CoulombP3M";
+}
+
+// Engine configuration for the handle's current parameters.
+void configure_engine(p3mx_handle *h) {
+  if (!h->eng || h->eng->fp32() != (h->prm.single_precision != 0))
+    h->eng = std::make_unique<Engine>(h->prm.single_precision != 0);
+  ReplicaConf c;
+  for (int d = 0; d < 3; ++d) {
+    c.box[d] = h->sys.box[d];
+    c.mesh[d] = h->mesh[d];
+    c.mesh_off[d] = h->mesh_off[d];
+  }
+  c.prefactor = h->prm.prefactor;
+  c.epsilon = h->prm.epsilon;
+  c.cao = h->cao;
+  c.alpha = h->alpha;
+  c.r_cut = h->r_cut;
+  c.skin = h->sys.skin;
+  c.p0 = 0;
+  c.np = static_cast<long long>(h->n);
+  h->eng->set_pair_table(h->ntypes, h->table);
+  h->eng->configure({c}, static_cast<long long>(h->n));
+}
+
+// sanity_checks_boxl (p3m.cpp:793-818) and the non-metallic cubic-box rule.
+void sanity_checks(p3mx_handle *h) {
+  for (int i = 0; i < 3; ++i) {
+    double const cao_cut = (static_cast<double>(h->cao) / 2.0) * (h->sys.box[i] / h->mesh[i]);
+    if (cao_cut >= 0.5 * h->sys.box[i]) {
+      std::ostringstream m;
+      m << "P3M_init: k-space cutoff " << cao_cut << " is larger than half of box dimension "
+        << h->sys.box[i];
+      throw Error(P3MX_ERUNTIME, m.str());
+    }
+  }
+  if (h->prm.epsilon != 0.0) {
+    if (h->sys.box[0] != h->sys.box[1] || h->sys.box[1] != h->sys.box[2] ||
+        h->mesh[0] != h->mesh[1] || h->mesh[1] != h->mesh[2])
+      throw Error(P3MX_ERUNTIME, actor_name(h) + ": non-metallic epsilon requires cubic box");
+  }
+  for (int d = 0; d < 3; ++d)
+    if (!mesh_fft_ok(h->mesh[d]))
+      throw Error(P3MX_EDOMAIN, "mesh " + std::to_string(h->mesh[d]) +
+                                    " is not supported by the FFT (even sizes with prime factors <= 31)");
+}
+
+double rs_error(double pref, double r_cut_iL, int n_c, double sum_q2, double alpha_L,
+                const double *box) {
+  double const V = box[0] * box[1] * box[2];
+  return (2. * pref * sum_q2 * std::exp(-(r_cut_iL * alpha_L) * (r_cut_iL * alpha_L))) /
+         std::sqrt(static_cast<double>(n_c) * r_cut_iL * box[0] * V);
+}
+
+// ---------------------------------------------------------------------
+// Tuner: restatement of TuningAlgorithm / CoulombTuningAlgorithm
+// (p3m/TuningAlgorithm.cpp:57-328, electrostatics/p3m.cpp:595-791) with the
+// k-space error summed on the device and trials timed with CUDA events on
+// full force evaluations (long + short range).
+struct Tuner {
+  p3mx_handle *h;
+  const double *pos;
+  const double *q;
+  const int *type;
+  bool dev;
+  double r_cut_iL_min = 0, r_cut_iL_max = 0;
+  int cao_min = 1, cao_max = 7, cao_best = 7;
+  double dens_min = 0, dens_max = 0;
+  bool tune_mesh = false;
+  size_t n_trials = 0;
+  Engine *err_eng = nullptr;
+
+  void log(const char *fmt, double a = 0, double b = 0) {
+    (void)fmt;
+    (void)a;
+    (void)b;
+  }
+
+  std::tuple<double, double, double, double> accuracy(const int *mesh, int cao, double r_cut_iL) {
+    double const *box = h->sys.box;
+    double const pref = h->prm.prefactor;
+    double rs = rs_error(pref, r_cut_iL, h->n_charged, h->sum_q2, 0., box);
+    double alpha_L;
+    if (std::sqrt(2.0) * rs > h->prm.accuracy)
+      alpha_L = std::sqrt(std::log(std::sqrt(2.0) * rs / h->prm.accuracy)) / r_cut_iL;
+    else
+      alpha_L = 0.1;
+    rs = rs_error(pref, r_cut_iL, h->n_charged, h->sum_q2, alpha_L, box);
+    double const ks = err_eng->ks_error(mesh, cao, h->n_charged, h->sum_q2, alpha_L, box, pref);
+    return {std::hypot(rs, ks), rs, ks, alpha_L};
+  }
+
+  double benchmark() {
+    configure_engine(h);
+    Engine &e = *h->eng;
+    e.upload(pos, q, type, dev, e.stream());
+    e.census(e.stream());
+    cudaEvent_t t0, t1;
+    P3MX_CUDA(cudaEventCreate(&t0));
+    P3MX_CUDA(cudaEventCreate(&t1));
+    int const timings = std::max(1, h->prm.timings);
+    e.long_range(e.d_force(), true, false, false, e.stream(), nullptr, nullptr);
+    e.short_range(e.d_force(), false, false, e.stream(), nullptr, nullptr);
+    P3MX_CUDA(cudaEventRecord(t0, e.stream()));
+    for (int k = 0; k < timings; ++k) {
+      e.long_range(e.d_force(), true, false, false, e.stream(), nullptr, nullptr);
+      e.short_range(e.d_force(), false, false, e.stream(), nullptr, nullptr);
+    }
+    P3MX_CUDA(cudaEventRecord(t1, e.stream()));
+    P3MX_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    P3MX_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return static_cast<double>(ms) / timings;
+  }
+
+  void commit(const int *mesh, int cao, double r_cut_iL, double alpha_L) {
+    double const L0 = h->sys.box[0];
+    h->r_cut = r_cut_iL * L0;
+    h->r_cut_iL = r_cut_iL;
+    h->cao = cao;
+    h->alpha_L = alpha_L;
+    h->alpha = alpha_L / L0;
+    for (int d = 0; d < 3; ++d)
+      h->mesh[d] = mesh[d];
+  }
+
+  double get_mc_time(const int *mesh, int cao, double &t_rc, double &t_al, double &t_acc) {
+    double const *box = h->sys.box;
+    double const skin = h->sys.skin;
+    double k_cut = std::numeric_limits<double>::max();
+    int min_mesh = std::min({mesh[0], mesh[1], mesh[2]});
+    for (int d = 0; d < 3; ++d)
+      k_cut = std::min(k_cut, (static_cast<double>(cao) / 2.) * box[d] / mesh[d]);
+    double const min_box = std::min({box[0], box[1], box[2]});
+    double const k_cut_max = min_box - skin;
+    if (cao >= min_mesh || k_cut >= k_cut_max)
+      return -kTuneCaoTooLarge;
+    for (int d = 0; d < 3; ++d)
+      if (!mesh_fft_ok(mesh[d]))
+        return -kTuneCaoTooLarge;
+    double rs, ks;
+    std::tie(t_acc, rs, ks, t_al) = accuracy(mesh, cao, r_cut_iL_max);
+    if (t_acc > h->prm.accuracy)
+      return -kTuneAccTooLarge;
+    double lo = r_cut_iL_min, hi = r_cut_iL_max, rc;
+    for (;;) {
+      rc = 0.5 * (lo + hi);
+      if (hi - lo < kRcutPrec)
+        break;
+      double acc;
+      std::tie(acc, rs, ks, t_al) = accuracy(mesh, cao, rc);
+      if (acc > h->prm.accuracy)
+        lo = rc;
+      else
+        hi = rc;
+    }
+    t_rc = rc = hi;
+    // the real-space cutoff plus skin must fit the cell system
+    if (t_rc * box[0] + skin > 0.5 * min_box)
+      return -kTuneAccTooLarge;
+    commit(mesh, cao, rc, t_al);
+    double const t = benchmark();
+    std::tie(t_acc, rs, ks, t_al) = accuracy(mesh, cao, rc);
+    if (h->prm.verbose)
+      std::printf("%-4d %-3d %.5e %.5e %.3e %.3e %.3e %-8.4f\n", mesh[0], cao, rc, t_al, t_acc, rs,
+                  ks, t);
+    ++n_trials;
+    return t;
+  }
+
+  double get_m_time(const int *mesh, int &t_cao, double &t_rc, double &t_al, double &t_acc) {
+    double best = -1., rc = 0., al = 0., acc = 0.;
+    int final_dir = 0;
+    int cao = t_cao;
+    double tmp;
+    do {
+      tmp = get_mc_time(mesh, cao, rc, al, acc);
+      if (tmp == -kTuneCaoTooLarge)
+        return tmp;
+      if (tmp >= 0.) {
+        best = tmp;
+        t_rc = rc;
+        t_al = al;
+        t_acc = acc;
+        t_cao = cao;
+        break;
+      }
+      cao++;
+      final_dir = 1;
+    } while (cao <= cao_max);
+    if (cao > cao_max)
+      return -kTuneCaoTooLarge;
+    if (cao == cao_min)
+      final_dir = 1;
+    else if (cao == cao_max)
+      final_dir = -1;
+    if (final_dir == 0) {
+      double dir_times[3] = {0, 0, 0};
+      for (final_dir = -1; final_dir <= 1; final_dir += 2) {
+        dir_times[final_dir + 1] = tmp = get_mc_time(mesh, cao + final_dir, rc, al, acc);
+        if (tmp < 0.)
+          continue;
+        if (tmp < best) {
+          best = tmp;
+          t_rc = rc;
+          t_al = al;
+          t_acc = acc;
+          t_cao = cao + final_dir;
+        }
+      }
+      if (dir_times[0] == best) {
+        final_dir = -1;
+      } else if (dir_times[2] == best) {
+        final_dir = 1;
+      } else {
+        if ((dir_times[0] >= 0 && dir_times[0] < best + kTimeGranularity) &&
+            (dir_times[2] < 0 || dir_times[2] > dir_times[0]))
+          final_dir = -1;
+        else if ((dir_times[2] >= 0 && dir_times[2] < best + kTimeGranularity) &&
+                 (dir_times[0] < 0 || dir_times[0] > dir_times[2]))
+          final_dir = 1;
+        else
+          return best;
+      }
+      cao += 2 * final_dir;
+    } else {
+      cao += final_dir;
+    }
+    for (; cao >= cao_min && cao <= cao_max; cao += final_dir) {
+      tmp = get_mc_time(mesh, cao, rc, al, acc);
+      if (tmp < 0.)
+        break;
+      if (tmp < best) {
+        best = tmp;
+        t_rc = rc;
+        t_al = al;
+        t_acc = acc;
+        t_cao = cao;
+      } else if (tmp > best + kTimeGranularity) {
+        break;
+      }
+    }
+    return best;
+  }
+
+  void run() {
+    double const *box = h->sys.box;
+    double const L0 = box[0];
+    // determine_r_cut_limits (TuningAlgorithm.cpp:57-74)
+    if (h->r_cut_iL == 0.) {
+      double const min_box = std::min({box[0], box[1], box[2]});
+      r_cut_iL_min = 0.;
+      r_cut_iL_max = (std::min(min_box, min_box / 2.) - h->sys.skin) / L0;
+    } else {
+      r_cut_iL_min = r_cut_iL_max = h->r_cut_iL;
+    }
+    // determine_cao_limits(7)
+    if (h->cao == -1) {
+      cao_min = 1;
+      cao_max = 7;
+      cao_best = 7;
+    } else {
+      cao_min = cao_max = cao_best = h->cao;
+    }
+    // determine_mesh_limits (p3m.cpp:676-707)
+    int fixed_mesh[3] = {h->mesh[0], h->mesh[1], h->mesh[2]};
+    if (h->mesh[0] == -1 && h->mesh[1] == -1 && h->mesh[2] == -1) {
+      double const norm = std::cbrt(box[0] * box[1] * box[2]);
+      double const maxn = 512., minn = std::min(maxn, std::cbrt(static_cast<double>(h->n_charged)));
+      dens_min = minn / norm;
+      dens_max = maxn / norm;
+      tune_mesh = true;
+    } else {
+      double const dens = static_cast<double>(h->mesh[0]) / box[0];
+      dens_min = dens_max = dens;
+      if (h->mesh[1] == -1 && h->mesh[2] == -1) {
+        for (int i : {1, 2}) {
+          fixed_mesh[i] = static_cast<int>(std::round(dens * box[i]));
+          fixed_mesh[i] += fixed_mesh[i] % 2;
+        }
+      }
+    }
+    if (h->prm.verbose) {
+      std::printf("%s tune parameters: Accuracy goal = %.5e prefactor = %.5e\n",
+                  actor_name(h).c_str(), h->prm.accuracy, h->prm.prefactor);
+      std::printf("System: box_l = %.5e # charged part = %d Sum[q_i^2] = %.5e\n", box[0],
+                  h->n_charged, h->sum_q2);
+      std::printf("mesh cao r_cut_iL    alpha_L     err       rs_err    ks_err    time [ms]\n");
+    }
+    // get_time (p3m.cpp:709-754)
+    struct {
+      int mesh[3];
+      int cao = -1;
+      double alpha_L = -1, r_cut_iL = -1, accuracy = -1;
+      double time = std::numeric_limits<double>::max();
+    } best;
+    double dens = dens_min;
+    while (dens <= dens_max) {
+      int tm[3];
+      if (tune_mesh) {
+        for (int i = 0; i < 3; ++i) {
+          tm[i] = static_cast<int>(std::round(box[i] * dens));
+          tm[i] += tm[i] % 2;
+        }
+      } else {
+        for (int i = 0; i < 3; ++i)
+          tm[i] = fixed_mesh[i];
+      }
+      int tcao = cao_best;
+      double trc = 0, tal = 0, tacc = 0;
+      double const t = get_m_time(tm, tcao, trc, tal, tacc);
+      if (t >= 0.) {
+        r_cut_iL_max = trc;
+        if (t < best.time) {
+          n_trials = 0;
+          for (int i = 0; i < 3; ++i)
+            best.mesh[i] = tm[i];
+          best.cao = tcao;
+          best.r_cut_iL = trc;
+          best.alpha_L = tal;
+          best.accuracy = tacc;
+          best.time = t;
+        } else if (t > best.time + kTimeGranularity ||
+                   n_trials > static_cast<size_t>(kMaxConsecutiveTrials)) {
+          break;
+        }
+      }
+      if (!tune_mesh)
+        break;
+      dens += 0.1;
+    }
+    if (best.time == std::numeric_limits<double>::max())
+      throw Error(P3MX_ERUNTIME, actor_name(h) + ": failed to reach requested accuracy");
+    h->accuracy = best.accuracy;
+    commit(best.mesh, best.cao, best.r_cut_iL, best.alpha_L);
+    if (h->prm.verbose)
+      std::printf("\nresulting parameters: mesh: (%d, %d, %d), cao: %d, r_cut_iL: %.4e,\n"
+                  "                      alpha_L: %.4e, accuracy: %.4e, time: %.2f\n",
+                  best.mesh[0], best.mesh[1], best.mesh[2], best.cao, best.r_cut_iL, best.alpha_L,
+                  best.accuracy, best.time);
+  }
+};
+
+void host_census(p3mx_handle *h, size_t n, const double *q, bool dev) {
+  std::vector<double> qq(n);
+  if (n) {
+    if (dev)
+      P3MX_CUDA(cudaMemcpy(qq.data(), q, n * sizeof(double), cudaMemcpyDeviceToHost));
+    else
+      std::memcpy(qq.data(), q, n * sizeof(double));
+  }
+  h->n_charged = 0;
+  h->sum_q2 = h->sum_q = 0.;
+  // Kahan sum for the neutrality ratio (coulomb.cpp:269-285)
+  double ks = 0., kc = 0., qmin = std::numeric_limits<double>::infinity();
+  for (double v : qq) {
+    if (v != 0.) {
+      h->n_charged++;
+      h->sum_q2 += v * v;
+      h->sum_q += v;
+      double const y = v - kc;
+      double const t = ks + y;
+      kc = (t - ks) - y;
+      ks = t;
+      qmin = std::min(qmin, std::abs(v));
+    }
+  }
+  if (h->prm.check_neutrality && h->prm.charge_neutrality_tolerance != -1. && h->n_charged > 0) {
+    double const ratio = std::abs(ks) / qmin;
+    if (ratio >= h->prm.charge_neutrality_tolerance) {
+      std::ostringstream m;
+      m.setf(std::ios::scientific);
+      m.precision(4);
+      m << ratio;
+      throw Error(P3MX_ERUNTIME,
+                  "The system is not charge neutral. Please neutralize the system before adding a "
+                  "new actor by adding the corresponding counterions to the system. Alternatively "
+                  "you can turn off the electroneutrality check by supplying "
+                  "check_neutrality=False when creating the actor. In this case you may be "
+                  "simulating a non-neutral system which will affect physical observables like "
+                  "e.g. the pressure, the chemical potentials of charged species or potential "
+                  "energies of the system. Since simulations of non charge neutral systems are "
+                  "special please make sure you know what you are doing. The relative charge "
+                  "excess was " +
+                      m.str());
+    }
+  }
+}
+
+void ensure_ready(p3mx_handle *h, size_t n) {
+  if (!h->activated)
+    throw Error(P3MX_ERUNTIME, "actor not activated: call p3mx_activate first");
+  if (n != h->n || !h->eng) {
+    h->n = n;
+    configure_engine(h);
+  }
+}
+
+} // namespace
+
+extern "C" {
+
+const char *p3mx_version(void) { return "p3mx 0.1 sm_100a (FP64 + FP32-mixed P3M, LJ/WCA)"; }
+
+int p3mx_create(const p3mx_params *params, p3mx_handle **out) {
+  if (!params || !out)
+    return P3MX_EHANDLE;
+  *out = nullptr;
+  auto h = std::make_unique<p3mx_handle>();
+  h->prm = *params;
+  try {
+    validate(h->prm);
+  } catch (Error const &e) {
+    // no handle exists yet; report via a detached handle carrying the message
+    h->err = e.what();
+    *out = h.release();
+    return e.code;
+  }
+  for (int d = 0; d < 3; ++d) {
+    h->mesh[d] = params->mesh[d];
+    h->mesh_off[d] = (params->mesh_off[d] == -1.) ? kMeshOff : params->mesh_off[d];
+  }
+  h->cao = params->cao;
+  h->r_cut = params->r_cut == -1. ? 0. : params->r_cut;
+  h->alpha = params->alpha == -1. ? 0. : params->alpha;
+  h->accuracy = params->accuracy;
+  h->is_tuned = !params->tune;
+  *out = h.release();
+  return P3MX_OK;
+}
+
+void p3mx_destroy(p3mx_handle *h) { delete h; }
+
+const char *p3mx_last_error(const p3mx_handle *h) { return h ? h->err.c_str() : "NULL handle"; }
+
+int p3mx_set_system(p3mx_handle *h, const p3mx_system *sys) {
+  return guarded(h, [&] {
+    if (!sys)
+      throw Error(P3MX_EDOMAIN, "system descriptor is NULL");
+    for (int d = 0; d < 3; ++d)
+      if (!(sys->box[d] > 0.))
+        throw Error(P3MX_EDOMAIN, "box_l must be > 0");
+    if (sys->skin < 0.)
+      throw Error(P3MX_EDOMAIN, "Parameter 'skin' must be >= 0");
+    h->sys = *sys;
+    h->sys_set = true;
+    if (h->activated) {
+      // on_boxl_change -> scaleby_box_l: r_cut and alpha follow the box
+      h->r_cut = h->r_cut_iL * h->sys.box[0];
+      h->alpha = h->alpha_L / h->sys.box[0];
+      sanity_checks(h);
+      configure_engine(h);
+    }
+  });
+}
+
+int p3mx_activate(p3mx_handle *h, size_t n, const double *pos, const double *q, unsigned flags) {
+  return guarded(h, [&] {
+    if (!h->sys_set)
+      throw Error(P3MX_ERUNTIME, "box not set: call p3mx_set_system first");
+    if (!(h->sys.periodic[0] && h->sys.periodic[1] && h->sys.periodic[2]))
+      throw Error(P3MX_ERUNTIME, actor_name(h) + ": requires periodicity (True, True, True)");
+    bool const dev = (flags & P3MX_DEVICE_PTRS) != 0;
+    h->activated = false;
+    // scaled parameters, tune() p3m.cpp:758-765
+    double const L0 = h->sys.box[0];
+    if (h->alpha_L == 0. && h->alpha != 0.)
+      h->alpha_L = h->alpha * L0;
+    if (h->r_cut_iL == 0. && h->r_cut != 0.)
+      h->r_cut_iL = h->r_cut / L0;
+    host_census(h, n, q, dev);
+    h->n = n;
+    if (!h->is_tuned) {
+      if (h->n_charged == 0)
+        throw Error(P3MX_ERUNTIME, actor_name(h) + ": no charged particles in the system");
+      Engine err_eng(false);
+      Tuner t{h, pos, q, nullptr, dev};
+      t.err_eng = &err_eng;
+      t.run();
+      h->is_tuned = true;
+    } else {
+      h->r_cut_iL = h->r_cut / L0;
+      h->alpha_L = h->alpha * L0;
+    }
+    for (int d = 0; d < 3; ++d)
+      if (h->mesh[d] == -1)
+        throw Error(P3MX_EDOMAIN, "Parameter 'mesh' must be > 0");
+    sanity_checks(h);
+    configure_engine(h);
+    // final error estimate of the committed parameters
+    h->rs_err = rs_error(h->prm.prefactor, h->r_cut_iL, std::max(1, h->n_charged), h->sum_q2,
+                         h->alpha_L, h->sys.box);
+    h->ks_err = h->eng->ks_error(h->mesh, h->cao, std::max(1, h->n_charged), h->sum_q2,
+                                 h->alpha_L, h->sys.box, h->prm.prefactor);
+    h->activated = true;
+  });
+}
+
+int p3mx_get_tuned(const p3mx_handle *h, p3mx_tuned *out) {
+  if (!h || !out)
+    return P3MX_EHANDLE;
+  for (int d = 0; d < 3; ++d) {
+    out->mesh[d] = h->mesh[d];
+    out->mesh_off[d] = h->mesh_off[d];
+    out->a[d] = (h->sys_set && h->mesh[d] > 0) ? h->sys.box[d] / h->mesh[d] : 0.;
+  }
+  out->cao = h->cao;
+  out->r_cut = h->r_cut;
+  out->alpha = h->alpha;
+  out->r_cut_iL = h->r_cut_iL;
+  out->alpha_L = h->alpha_L;
+  out->accuracy = h->accuracy;
+  out->epsilon = h->prm.epsilon;
+  out->is_tuned = h->is_tuned ? 1 : 0;
+  out->single_precision = h->prm.single_precision;
+  out->rs_error = h->rs_err;
+  out->ks_error = h->ks_err;
+  return P3MX_OK;
+}
+
+int p3mx_set_pair_params(p3mx_handle *h, int ntypes, const p3mx_pair_params *table) {
+  return guarded(h, [&] {
+    if (ntypes < 1 || !table)
+      throw Error(P3MX_EDOMAIN, "pair table needs ntypes >= 1");
+    std::vector<PairIA> t(static_cast<size_t>(ntypes) * ntypes);
+    for (int k = 0; k < ntypes * ntypes; ++k) {
+      auto const &s = table[k];
+      if (s.lj_eps < 0.)
+        throw Error(P3MX_EDOMAIN, "LJ parameter 'epsilon' has to be >= 0");
+      if (s.lj_sig < 0.)
+        throw Error(P3MX_EDOMAIN, "LJ parameter 'sigma' has to be >= 0");
+      if (s.lj_cut < 0.)
+        throw Error(P3MX_EDOMAIN, "LJ parameter 'cutoff' has to be >= 0");
+      if (s.wca_eps < 0.)
+        throw Error(P3MX_EDOMAIN, "WCA parameter 'epsilon' has to be >= 0");
+      if (s.wca_sig < 0.)
+        throw Error(P3MX_EDOMAIN, "WCA parameter 'sigma' has to be >= 0");
+      PairIA &d = t[k];
+      d.lj_eps = s.lj_eps;
+      d.lj_sig = s.lj_sig;
+      d.lj_cut = s.lj_cut;
+      d.lj_shift = s.lj_shift;
+      d.lj_offset = s.lj_offset;
+      d.lj_min = std::max(s.lj_min, 0.);
+      d.wca_eps = s.wca_eps;
+      d.wca_sig = s.wca_sig;
+      d.wca_cut = (s.wca_sig != 0.) ? s.wca_sig * std::pow(2., 1. / 6.) : 0.;
+      // max_cutoff of the pair (nonbonded_interaction_data.cpp): inactive
+      // when no potential is switched on
+      double ic = -1.0;
+      if (s.lj_cut > 0. && s.lj_eps != 0.)
+        ic = std::max(ic, s.lj_cut + s.lj_offset);
+      if (d.wca_cut > 0. && s.wca_eps != 0.)
+        ic = std::max(ic, d.wca_cut);
+      d.ia_cut = ic;
+    }
+    h->ntypes = ntypes;
+    h->table = t;
+    if (h->eng) {
+      h->eng->set_pair_table(ntypes, t);
+    }
+  });
+}
+
+static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *q, const int *type,
+                     bool dev, cudaStream_t st) {
+  Engine &e = *h->eng;
+  if (dev || n == 0) {
+    e.upload(pos, q, type, true, st);
+    return;
+  }
+  size_t const bytes = n * (4 * sizeof(double) + sizeof(int));
+  h->h_in.ensure(bytes);
+  double *pp = h->h_in.as<double>();
+  std::memcpy(pp, pos, 3 * n * sizeof(double));
+  std::memcpy(pp + 3 * n, q, n * sizeof(double));
+  int *tt = reinterpret_cast<int *>(pp + 4 * n);
+  if (type)
+    std::memcpy(tt, type, n * sizeof(int));
+  else
+    std::memset(tt, 0, n * sizeof(int));
+  e.upload(pp, pp + 3 * n, tt, false, st);
+}
+
+static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwrite,
+                      cudaStream_t st) {
+  Engine &e = *h->eng;
+  if (!f || n == 0)
+    return;
+  if (dev) {
+    // device destination: forces were computed straight into f
+    return;
+  }
+  h->h_out.ensure(3 * n * sizeof(double));
+  double *o = h->h_out.as<double>();
+  P3MX_CUDA(cudaMemcpyAsync(o, e.d_force(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  if (overwrite)
+    std::memcpy(f, o, 3 * n * sizeof(double));
+  else
+    for (size_t k = 0; k < 3 * n; ++k)
+      f[k] += o[k];
+}
+
+int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q, double *f,
+                    double *energy, double *virial9, unsigned flags, void *stream) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
+    bool const dev = flags & P3MX_DEVICE_PTRS;
+    bool const ow = flags & P3MX_OVERWRITE;
+    stage_in(h, n, pos, q, nullptr, dev, st);
+    e.census(st);
+    double *fd = nullptr;
+    if ((flags & P3MX_FORCES) && f)
+      fd = dev ? f : e.d_force();
+    std::vector<double> en, vir;
+    e.long_range(fd, dev ? ow : true, energy && (flags & P3MX_ENERGY), virial9 && (flags & P3MX_VIRIAL),
+                 st, &en, &vir);
+    if (energy && (flags & P3MX_ENERGY))
+      *energy = en.empty() ? 0. : en[0];
+    if (virial9 && (flags & P3MX_VIRIAL))
+      for (int k = 0; k < 9; ++k)
+        virial9[k] = vir.empty() ? 0. : vir[k];
+    if (fd)
+      stage_out(h, n, f, dev, ow, st);
+    P3MX_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos, const double *q, const int *type,
+                     double *f, double *energy2, double *virial18, unsigned flags, void *stream) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
+    bool const dev = flags & P3MX_DEVICE_PTRS;
+    bool const ow = flags & P3MX_OVERWRITE;
+    stage_in(h, n, pos, q, type, dev, st);
+    double *fd = nullptr;
+    if ((flags & P3MX_FORCES) && f)
+      fd = dev ? f : e.d_force();
+    bool const want = (energy2 && (flags & P3MX_ENERGY)) || (virial18 && (flags & P3MX_VIRIAL));
+    std::vector<double> en, vir;
+    if (fd) {
+      e.short_range(fd, dev ? ow : true, want, st, &en, &vir);
+    } else {
+      // energies only: compute into the scratch force buffer
+      e.short_range(e.d_force(), true, want, st, &en, &vir);
+    }
+    if (energy2 && (flags & P3MX_ENERGY))
+      for (int k = 0; k < 2; ++k)
+        energy2[k] = en.empty() ? 0. : en[k];
+    if (virial18 && (flags & P3MX_VIRIAL))
+      for (int k = 0; k < 18; ++k)
+        virial18[k] = vir.empty() ? 0. : vir[k];
+    if (fd)
+      stage_out(h, n, f, dev, ow, st);
+    P3MX_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, const int *type,
+                double *f, double *energy3, double *virial27, unsigned flags, void *stream) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
+    bool const dev = flags & P3MX_DEVICE_PTRS;
+    bool const ow = flags & P3MX_OVERWRITE;
+    stage_in(h, n, pos, q, type, dev, st);
+    bool const want_e = energy3 && (flags & P3MX_ENERGY);
+    bool const want_v = virial27 && (flags & P3MX_VIRIAL);
+    if (want_e || h->prm.epsilon != 0.)
+      e.census(st);
+    double *fd = (dev && f) ? f : e.d_force();
+    std::vector<double> enk, virk, ens, virs;
+    e.long_range(fd, dev ? ow : true, want_e, want_v, st, &enk, &virk);
+    e.short_range(fd, false, want_e || want_v, st, &ens, &virs);
+    if (want_e) {
+      energy3[0] = ens[0];
+      energy3[1] = enk[0];
+      energy3[2] = ens[1];
+    }
+    if (want_v)
+      for (int k = 0; k < 9; ++k) {
+        virial27[k] = virs[k];
+        virial27[9 + k] = virk[k];
+        virial27[18 + k] = virs[9 + k];
+      }
+    if (f)
+      stage_out(h, n, f, dev, ow, st);
+    P3MX_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int p3mx_cell_grid(p3mx_handle *h, int *cell_grid, double *cell_size) {
+  return guarded(h, [&] {
+    if (!h->eng)
+      throw Error(P3MX_ERUNTIME, "actor not activated");
+    h->eng->cell_grid(0, cell_grid, cell_size);
+  });
+}
+
+int p3mx_cell_index(p3mx_handle *h, size_t n, const double *pos, int *cell) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    e.upload_positions(pos, false, e.stream());
+    auto v = e.cell_index_ghost(e.stream());
+    std::memcpy(cell, v.data(), n * sizeof(int));
+  });
+}
+
+int p3mx_verlet_pairs(p3mx_handle *h, size_t n, const double *pos, const double *q, const int *type,
+                      int *pairs, size_t cap, size_t *count) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    e.upload(pos, q, type, false, e.stream());
+    auto v = e.verlet_pairs(e.stream());
+    size_t const np = v.size() / 2;
+    if (count)
+      *count = np;
+    std::memcpy(pairs, v.data(), std::min(np, cap) * 2 * sizeof(int));
+  });
+}
+
+int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap) {
+  return guarded(h, [&] {
+    if (!h->eng)
+      throw Error(P3MX_ERUNTIME, "actor not activated");
+    auto v = h->eng->mesh_copy(0, h->eng->stream());
+    if (cap < v.size())
+      throw Error(P3MX_EDOMAIN, "output buffer too small for the mesh");
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+  });
+}
+
+int p3mx_error_estimate(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,
+                        double r_cut_iL, const double *box, double prefactor, double *rs_err,
+                        double *ks_err) {
+  try {
+    Engine e(false);
+    if (rs_err)
+      *rs_err = rs_error(prefactor, r_cut_iL, n_c_part, sum_q2, alpha_L, box);
+    if (ks_err)
+      *ks_err = e.ks_error(mesh, cao, n_c_part, sum_q2, alpha_L, box, prefactor);
+    return P3MX_OK;
+  } catch (Error const &e) {
+    return e.code;
+  }
+}
+
+} // extern "C"

@@ -1,0 +1,805 @@
+// Engine implementation: geometry, FFT plans, block tables and the two
+// force pipelines (see engine.cuh).
+#include "engine.cuh"
+#include "p3m_kernels.cuh"
+#include "sort.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+
+namespace p3mx {
+
+namespace {
+
+// Radix factorisation of an FFT length: 4s first, then 2, 3, 5, 7 and any
+// remaining prime (handled by the generic radix, up to 31).
+AxisPlan make_plan(int n, int tw_off) {
+  AxisPlan pl{};
+  pl.n = n;
+  pl.tw_off = tw_off;
+  int m = n;
+  std::vector<int> f;
+  while (m % 4 == 0) {
+    f.push_back(4);
+    m /= 4;
+  }
+  while (m % 2 == 0) {
+    f.push_back(2);
+    m /= 2;
+  }
+  for (int p = 3; m > 1; p += 2) {
+    while (m % p == 0) {
+      f.push_back(p);
+      m /= p;
+    }
+  }
+  if (f.empty())
+    f.push_back(1);
+  if (static_cast<int>(f.size()) > kMaxStages)
+    throw Error(1, "FFT length " + std::to_string(n) + " has too many factors");
+  for (int p : f)
+    if (p > 31)
+      throw Error(1, "mesh size " + std::to_string(n) +
+                         " has a prime factor > 31; choose a mesh with factors <= 31");
+  pl.nstages = (n == 1) ? 0 : static_cast<int>(f.size());
+  for (int s = 0; s < pl.nstages; ++s)
+    pl.radix[s] = f[s];
+  return pl;
+}
+
+int cell_grid_host(const double *box, double range, int *cg, double *cs) {
+  // RegularDecomposition::create_cell_grid on one rank
+  // (RegularDecomposition.cpp:289-385, max_num_cells 32768).
+  int const max_num_cells = 32768, min_num_cells = 8;
+  double cell_range[3] = {range, range, range};
+  if (range <= 0.0) {
+    for (int i = 0; i < 3; ++i)
+      cg[i] = 2;
+  } else {
+    double const volume = box[0] * box[1] * box[2];
+    double const scale = std::cbrt(max_num_cells / volume);
+    for (int i = 0; i < 3; ++i) {
+      cg[i] = static_cast<int>(std::ceil(box[i] * scale));
+      cell_range[i] = box[i] / static_cast<double>(cg[i]);
+      if (cell_range[i] < range) {
+        cg[i] = static_cast<int>(std::floor(box[i] / range));
+        if (cg[i] < 1)
+          return 2;
+        cell_range[i] = box[i] / static_cast<double>(cg[i]);
+      }
+    }
+    for (;;) {
+      long const nc = long(cg[0]) * cg[1] * cg[2];
+      if (nc <= max_num_cells)
+        break;
+      int mi = 0;
+      double ms = cell_range[0];
+      for (int i = 1; i < 3; ++i)
+        if (cg[i] > 1 && cell_range[i] < ms) {
+          mi = i;
+          ms = cell_range[i];
+        }
+      cg[mi]--;
+      cell_range[mi] = box[mi] / cg[mi];
+    }
+    if (long(cg[0]) * cg[1] * cg[2] < min_num_cells)
+      return 3;
+  }
+  for (int i = 0; i < 3; ++i)
+    cs[i] = box[i] / static_cast<double>(cg[i]);
+  return 0;
+}
+
+template <typename T> void upload_vec(DevBuf &b, std::vector<T> const &v, cudaStream_t st) {
+  b.ensure(std::max<size_t>(1, v.size()) * sizeof(T));
+  if (!v.empty())
+    P3MX_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+} // namespace
+
+Engine::Engine(bool fp32) : m_fp32(fp32) {
+  P3MX_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+  m_ia.assign(1, PairIA{0, 0, 0, 0, 0, 0, 0, 0, 0, -1.0});
+}
+
+Engine::~Engine() {
+  if (m_stream)
+    cudaStreamDestroy(m_stream);
+}
+
+void Engine::set_pair_table(int ntypes, std::vector<PairIA> const &tab) {
+  if (ntypes < 1 || static_cast<int>(tab.size()) != ntypes * ntypes)
+    throw Error(1, "pair table must hold ntypes^2 entries");
+  m_ntypes = ntypes;
+  m_ia = tab;
+  upload_vec(m_ia_d, m_ia, m_stream);
+  m_lists_valid = false;
+  if (!m_conf.empty())
+    configure(std::vector<ReplicaConf>(m_conf), m_n);
+}
+
+void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) {
+  m_conf = conf;
+  m_n = n_total;
+  int const R = static_cast<int>(conf.size());
+  m_geom.assign(R, RepGeom{});
+  // twiddle tables for every distinct axis length
+  std::map<int, int> tw_off;
+  std::vector<std::complex<double>> tw;
+  auto twoff = [&](int n) {
+    auto it = tw_off.find(n);
+    if (it != tw_off.end())
+      return it->second;
+    int const off = static_cast<int>(tw.size());
+    for (int k = 0; k < n; ++k)
+      tw.push_back(std::polar(1.0, -2.0 * kPi * k / n));
+    tw_off[n] = off;
+    return off;
+  };
+  double max_ia = -1.0;
+  for (auto const &e : m_ia)
+    max_ia = std::max(max_ia, e.ia_cut);
+  m_bins = m_cplx = m_cells = 0;
+  for (int r = 0; r < R; ++r) {
+    auto const &c = conf[r];
+    auto &G = m_geom[r];
+    G.cao = c.cao;
+    G.alpha = c.alpha;
+    G.r_cut = c.r_cut;
+    G.prefactor = c.prefactor;
+    G.epsilon = c.epsilon;
+    G.V = c.box[0] * c.box[1] * c.box[2];
+    G.p0 = c.p0;
+    G.np = c.np;
+    // pos_shift, interpolation.hpp:142
+    G.pos_shift = std::floor((c.cao - 1) / 2.0) - (c.cao % 2) / 2.0;
+    for (int d = 0; d < 3; ++d) {
+      if (c.mesh[d] < 2 || c.mesh[d] % 2)
+        throw Error(1, "P3M requires an even number of mesh points in all directions");
+      G.box[d] = c.box[d];
+      G.box_i[d] = 1.0 / c.box[d];
+      G.mesh[d] = c.mesh[d];
+      G.ai[d] = c.mesh[d] / c.box[d];
+      double const a = 1.0 / G.ai[d];
+      double const cao_cut = (static_cast<double>(c.cao) / 2.0) * a;
+      double const outer_ld_grid = (0.0 - (cao_cut + c.skin)) * G.ai[d] - c.mesh_off[d];
+      G.ld_ind[d] = static_cast<int>(std::ceil(outer_ld_grid));
+      G.ld_pos[d] = (G.ld_ind[d] + c.mesh_off[d]) * a;
+      G.plan[d] = make_plan(c.mesh[d], twoff(c.mesh[d]));
+    }
+    G.hp = ((c.mesh[2] / 2 + 1) + 3) / 4 * 4;
+    G.rm_off = m_bins;
+    G.km_off = m_cplx;
+    m_bins += static_cast<long long>(c.mesh[0]) * c.mesh[1] * c.mesh[2];
+    m_cplx += static_cast<long long>(c.mesh[0]) * c.mesh[1] * G.hp;
+    // short-range cell system
+    G.skin = c.skin;
+    G.coulomb_cut = (c.prefactor != 0.0) ? c.r_cut : 0.0;
+    G.max_cut = std::max(G.coulomb_cut, max_ia);
+    double cs[3];
+    if (cell_grid_host(c.box, G.max_cut + c.skin, G.cg, cs))
+      throw Error(2, "interaction range " + std::to_string(G.max_cut + c.skin) +
+                         " is larger than the box allows");
+    for (int d = 0; d < 3; ++d)
+      G.inv_cs[d] = 1.0 / cs[d];
+    G.cell_off = m_cells;
+    m_cells += static_cast<long long>(G.cg[0]) * G.cg[1] * G.cg[2];
+  }
+  if (m_bins >= (1LL << 31) || m_n >= (1LL << 31))
+    throw Error(1, "batch too large for 32-bit bin/particle indices");
+  cudaStream_t st = m_stream;
+  upload_vec(m_geom_d, m_geom, st);
+  {
+    std::vector<typename CplxOf<double>::type> t64(tw.size());
+    for (size_t k = 0; k < tw.size(); ++k)
+      t64[k] = double2{tw[k].real(), tw[k].imag()};
+    if (m_fp32) {
+      std::vector<float2> t32(tw.size());
+      for (size_t k = 0; k < tw.size(); ++k)
+        t32[k] = float2{static_cast<float>(tw[k].real()), static_cast<float>(tw[k].imag())};
+      upload_vec(m_tw, t32, st);
+    } else {
+      upload_vec(m_tw, t64, st);
+    }
+  }
+  // replica id of every particle
+  {
+    std::vector<int> rep_of(std::max<long long>(1, m_n), 0);
+    for (int r = 0; r < R; ++r)
+      for (long long i = conf[r].p0; i < conf[r].p0 + conf[r].np; ++i)
+        rep_of[i] = r;
+    upload_vec(m_rep_of, rep_of, st);
+  }
+  // block tables
+  size_t const csz = m_fp32 ? sizeof(float2) : sizeof(double2);
+  size_t const cap = m_fp32 ? 4096 : 2048; // complex elements per smem buffer
+  {
+    std::vector<int2> bm, bc, bcen, bp;
+    m_blk_census_start.assign(1, 0);
+    m_blk_pair_start.assign(1, 0);
+    for (int r = 0; r < R; ++r) {
+      long long const ms = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].mesh[2];
+      long long const cs2 = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].hp;
+      for (int b = 0; b < ceil_div(ms, 256); ++b)
+        bm.push_back(int2{r, b});
+      for (int b = 0; b < ceil_div(cs2, 256); ++b)
+        bc.push_back(int2{r, b});
+      for (int b = 0; b < std::max(1, ceil_div(conf[r].np, 2048)); ++b)
+        bcen.push_back(int2{r, b});
+      m_blk_census_start.push_back(static_cast<int>(bcen.size()));
+      for (int b = 0; b < std::max(1, ceil_div(conf[r].np, 256)); ++b)
+        bp.push_back(int2{r, b});
+      m_blk_pair_start.push_back(static_cast<int>(bp.size()));
+    }
+    m_n_blk_mesh = static_cast<int>(bm.size());
+    m_n_blk_cplx = static_cast<int>(bc.size());
+    m_n_blk_census = static_cast<int>(bcen.size());
+    m_n_blk_pair = static_cast<int>(bp.size());
+    upload_vec(m_blk_mesh, bm, st);
+    upload_vec(m_blk_cplx, bc, st);
+    upload_vec(m_blk_census, bcen, st);
+    upload_vec(m_blk_pair, bp, st);
+    upload_vec(m_blk_census_start_d, m_blk_census_start, st);
+    upload_vec(m_blk_pair_start_d, m_blk_pair_start, st);
+  }
+  {
+    std::vector<Blk> zf, y, x, zi;
+    m_blk_x_start.assign(1, 0);
+    int maxM0 = 1, maxM1 = 1, maxM2 = 1;
+    for (auto const &G : m_geom) {
+      maxM0 = std::max(maxM0, G.mesh[0]);
+      maxM1 = std::max(maxM1, G.mesh[1]);
+      maxM2 = std::max(maxM2, G.mesh[2]);
+    }
+    m_tile_y = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / maxM1)));
+    m_tile_x = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / (3 * maxM0))));
+    size_t smem_zf = 0, smem_zi = 0;
+    for (int r = 0; r < R; ++r) {
+      auto const &G = m_geom[r];
+      int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+      int const H = M2 / 2 + 1;
+      int const lines = M0 * M1;
+      int const lz = static_cast<int>(std::max<size_t>(1, cap / M2));
+      for (int l = 0; l < lines; l += lz)
+        zf.push_back(Blk{r, l, std::min(lz, lines - l), 0});
+      smem_zf = std::max(smem_zf, 2 * static_cast<size_t>(std::min(lz, lines)) * M2 * csz);
+      int const lzi = static_cast<int>(std::max<size_t>(1, cap / (3 * M2)));
+      for (int l = 0; l < lines; l += lzi)
+        zi.push_back(Blk{r, l, std::min(lzi, lines - l), 0});
+      smem_zi = std::max(smem_zi, 2 * 3 * static_cast<size_t>(std::min(lzi, lines)) * M2 * csz);
+      for (int xx = 0; xx < M0; ++xx)
+        for (int k0 = 0; k0 < H; k0 += m_tile_y)
+          y.push_back(Blk{r, xx, k0, 0});
+      for (int yy = 0; yy < M1; ++yy)
+        for (int k0 = 0; k0 < H; k0 += m_tile_x)
+          x.push_back(Blk{r, yy, k0, 0});
+      m_blk_x_start.push_back(static_cast<int>(x.size()));
+    }
+    m_smem_zf = smem_zf;
+    m_smem_zi = smem_zi;
+    m_smem_y = 2 * static_cast<size_t>(m_tile_y) * maxM1 * csz;
+    m_smem_x = 2 * 3 * static_cast<size_t>(m_tile_x) * maxM0 * csz;
+    m_n_blk_zf = static_cast<int>(zf.size());
+    m_n_blk_y = static_cast<int>(y.size());
+    m_n_blk_x = static_cast<int>(x.size());
+    m_n_blk_zi = static_cast<int>(zi.size());
+    upload_vec(m_blk_zf, zf, st);
+    upload_vec(m_blk_y, y, st);
+    upload_vec(m_blk_x, x, st);
+    upload_vec(m_blk_zi, zi, st);
+    upload_vec(m_blk_x_start_d, m_blk_x_start, st);
+    // opt-in dynamic shared memory; static arrays of the kernels (<= 2 KB)
+    // stay inside the 227 KB per-block limit
+    size_t const limit = 220 * 1024;
+    if (std::max({m_smem_zf, m_smem_zi, m_smem_y, m_smem_x}) > limit)
+      throw Error(1, "mesh too large for the shared-memory FFT tiles");
+    // one process-wide opt-in value, so engines of different sizes coexist
+    auto attr = [limit](auto kern, size_t) {
+      P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(limit)));
+    };
+    if (m_fp32) {
+      attr(k_fft_z_fwd<float>, m_smem_zf);
+      attr(k_fft_y<float>, m_smem_y);
+      attr(k_fft_x_kspace<float>, m_smem_x);
+      attr(k_fft_z_inv3<float>, m_smem_zi);
+    } else {
+      attr(k_fft_z_fwd<double>, m_smem_zf);
+      attr(k_fft_y<double>, m_smem_y);
+      attr(k_fft_x_kspace<double>, m_smem_x);
+      attr(k_fft_z_inv3<double>, m_smem_zi);
+    }
+  }
+  // buffers
+  size_t const rsz = m_fp32 ? sizeof(float) : sizeof(double);
+  long long const n = std::max<long long>(1, m_n);
+  m_pos.ensure(3 * n * sizeof(double));
+  m_q.ensure(n * sizeof(double));
+  m_type.ensure(n * sizeof(int));
+  m_force.ensure(3 * n * sizeof(double));
+  m_key.ensure(n * sizeof(int));
+  m_slot.ensure(n * sizeof(int));
+  m_perm.ensure(n * sizeof(int));
+  m_cnt.ensure((m_bins + 1) * sizeof(int));
+  m_start.ensure((m_bins + 1) * sizeof(int));
+  m_scan_tiles.ensure((ceil_div(std::max(m_bins, m_cells) + 1, kScanTile) + 1) * sizeof(int));
+  m_dist.ensure(3 * n * rsz);
+  m_W.ensure(3 * 7 * n * rsz);
+  m_scz.ensure(n * sizeof(int));
+  m_skey.ensure(n * sizeof(int));
+  m_rho.ensure(m_bins * rsz);
+  m_E.ensure(3 * m_bins * rsz);
+  m_ck.ensure(m_cplx * csz);
+  m_field.ensure(3 * m_cplx * csz);
+  m_ginf.ensure(m_cplx * rsz);
+  m_part_x.ensure(static_cast<size_t>(m_n_blk_x) * 8 * sizeof(double));
+  m_sums_x.ensure(static_cast<size_t>(R) * 8 * sizeof(double));
+  m_part_census.ensure(static_cast<size_t>(m_n_blk_census) * 6 * sizeof(double));
+  m_sums_census.ensure(static_cast<size_t>(R) * 6 * sizeof(double));
+  m_dipole.ensure(static_cast<size_t>(R) * 3 * sizeof(double));
+  m_ckey.ensure(n * sizeof(int));
+  m_cslot.ensure(n * sizeof(int));
+  m_ccnt.ensure((m_cells + 1) * sizeof(int));
+  m_cstart.ensure((m_cells + 1) * sizeof(int));
+  m_cperm.ensure(n * sizeof(int));
+  m_pq.ensure(n * sizeof(double4));
+  m_spq.ensure(n * sizeof(double4));
+  m_stype.ensure(n * sizeof(int));
+  m_scell.ensure(n * sizeof(int));
+  m_nb_cnt.ensure(n * sizeof(int));
+  m_overflow.ensure(sizeof(int));
+  m_flag.ensure(sizeof(int));
+  m_pos_ref.ensure(3 * n * sizeof(double));
+  m_part_pair.ensure(static_cast<size_t>(m_n_blk_pair) * 20 * sizeof(double));
+  m_sums_pair.ensure(static_cast<size_t>(R) * 20 * sizeof(double));
+  if (m_ia_d.p == nullptr)
+    upload_vec(m_ia_d, m_ia, st);
+  m_ginf_valid = false;
+  m_lists_valid = false;
+  P3MX_CUDA(cudaStreamSynchronize(st));
+}
+
+void Engine::upload(const double *pos, const double *q, const int *type, bool device_ptrs,
+                    cudaStream_t st) {
+  cudaMemcpyKind const k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (m_n == 0)
+    return;
+  P3MX_CUDA(cudaMemcpyAsync(m_pos.p, pos, 3 * m_n * sizeof(double), k, st));
+  P3MX_CUDA(cudaMemcpyAsync(m_q.p, q, m_n * sizeof(double), k, st));
+  if (type)
+    P3MX_CUDA(cudaMemcpyAsync(m_type.p, type, m_n * sizeof(int), k, st));
+  else
+    P3MX_CUDA(cudaMemsetAsync(m_type.p, 0, m_n * sizeof(int), st));
+}
+
+void Engine::upload_positions(const double *pos, bool device_ptrs, cudaStream_t st) {
+  if (m_n == 0)
+    return;
+  P3MX_CUDA(cudaMemcpyAsync(m_pos.p, pos, 3 * m_n * sizeof(double),
+                            device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+}
+
+void Engine::census(cudaStream_t st) {
+  int const R = n_rep();
+  k_census<<<m_n_blk_census, 256, 0, st>>>(m_blk_census.as<int2>(), m_geom_d.as<RepGeom>(),
+                                           d_pos(), d_q(), m_part_census.as<double>());
+  k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_census.as<double>(), 6,
+                                                      m_blk_census_start_d.as<int>(), R,
+                                                      m_sums_census.as<double>());
+  m_census_h.assign(static_cast<size_t>(R) * 6, 0.0);
+  P3MX_CUDA(cudaMemcpyAsync(m_census_h.data(), m_sums_census.p, R * 6 * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> dip(3 * R);
+  for (int r = 0; r < R; ++r) {
+    m_geom[r].sum_q = m_census_h[6 * r + 1];
+    m_geom[r].sum_q2 = m_census_h[6 * r + 2];
+    for (int d = 0; d < 3; ++d)
+      dip[3 * r + d] = m_census_h[6 * r + 3 + d];
+  }
+  upload_vec(m_geom_d, m_geom, st);
+  upload_vec(m_dipole, dip, st);
+}
+
+void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
+                       cudaStream_t st, const int *cond) {
+  exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
+  k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond);
+  k_fix_buckets<<<ceil_div(nkeys, 256), 256, 0, st>>>(start, perm, nkeys, cond);
+}
+
+#define P3MX_CAO_DISPATCH(cao, KERNEL_CALL)                                    \
+  switch (cao) {                                                               \
+  case 1: { constexpr int P = 1; KERNEL_CALL; } break;                         \
+  case 2: { constexpr int P = 2; KERNEL_CALL; } break;                         \
+  case 3: { constexpr int P = 3; KERNEL_CALL; } break;                         \
+  case 4: { constexpr int P = 4; KERNEL_CALL; } break;                         \
+  case 5: { constexpr int P = 5; KERNEL_CALL; } break;                         \
+  case 6: { constexpr int P = 6; KERNEL_CALL; } break;                         \
+  default: { constexpr int P = 7; KERNEL_CALL; } break;                        \
+  }
+
+template <typename Real>
+void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
+                          cudaStream_t st) {
+  using C = typename CplxOf<Real>::type;
+  int const R = n_rep();
+  // all replicas of one engine share cao (the batch tuner fixes cao per
+  // batch); meshes may differ
+  int const cao = m_geom[0].cao;
+  for (auto const &G : m_geom)
+    if (G.cao != cao)
+      throw Error(1, "replicas of one batch must share the charge-assignment order");
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
+  if (!m_ginf_valid) {
+    k_influence<Real><<<m_n_blk_cplx, 256, 0, st>>>(geom, m_blk_cplx.as<int2>(), m_ginf.as<Real>());
+    m_ginf_valid = true;
+  }
+  // 1. corner binning + deterministic counting sort
+  P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_bins + 1) * sizeof(int), st));
+  int const nb = ceil_div(m_n, 256);
+  if (m_n > 0) {
+    k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
+                                        m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>());
+    sort_keys(m_key.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
+              m_perm.as<int>(), m_bins, st);
+    P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P><<<nb, 256, 0, st>>>(
+                               geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
+                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_scz.as<int>(),
+                               m_skey.as<int>())));
+  } else {
+    P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_bins + 1) * sizeof(int), st));
+  }
+  // 2. gather-based charge assignment
+  P3MX_CAO_DISPATCH(cao, (k_p3m_assign<Real, P><<<m_n_blk_mesh, 256, 0, st>>>(
+                             geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
+                             m_scz.as<int>(), m_rho.as<Real>())));
+  // 3. forward FFT z (r2c) and y
+  C const *tw = m_tw.as<C>();
+  k_fft_z_fwd<Real><<<m_n_blk_zf, 256, m_smem_zf, st>>>(geom, m_blk_zf.as<Blk>(), m_rho.as<Real>(),
+                                                        m_ck.as<C>(), tw);
+  k_fft_y<Real><<<dim3(m_n_blk_y, 1), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_ck.as<C>(), 0,
+                                                          m_tile_y, false, tw);
+  // 4. x pass fused with the k-space operator (+ energy/virial partials)
+  bool const want_f = (f != nullptr);
+  bool const want_ev = want_e || want_v;
+  k_fft_x_kspace<Real><<<m_n_blk_x, 256, m_smem_x, st>>>(
+      geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx, m_tile_x,
+      want_f ? 1 : 0, want_ev ? 1 : 0, m_part_x.as<double>(), tw);
+  if (want_ev)
+    k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_x.as<double>(), 8,
+                                                        m_blk_x_start_d.as<int>(), R,
+                                                        m_sums_x.as<double>());
+  if (!want_f)
+    return;
+  // 5. backward FFT y (3 fields), z (c2r, 3 fields)
+  k_fft_y<Real><<<dim3(m_n_blk_y, 3), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_field.as<C>(),
+                                                          m_cplx, m_tile_y, true, tw);
+  k_fft_z_inv3<Real><<<m_n_blk_zi, 256, m_smem_zi, st>>>(geom, m_blk_zi.as<Blk>(), m_field.as<C>(),
+                                                         m_cplx, m_E.as<Real>(), m_bins, tw);
+  // 6. force back-interpolation
+  if (m_n > 0) {
+    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P><<<nb, 256, 0, st>>>(
+                               geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
+                               m_W.as<Real>(), m_E.as<Real>(), m_bins, d_q(), m_dipole.as<double>(),
+                               m_n, f, overwrite ? 1 : 0)));
+  }
+}
+
+void Engine::long_range(double *f, bool overwrite, bool want_energy, bool want_virial,
+                        cudaStream_t st, std::vector<double> *energies,
+                        std::vector<double> *virials) {
+  if (m_fp32)
+    long_range_t<float>(f, overwrite, want_energy, want_virial, st);
+  else
+    long_range_t<double>(f, overwrite, want_energy, want_virial, st);
+  P3MX_CUDA(cudaGetLastError());
+  if (want_energy || want_virial) {
+    int const R = n_rep();
+    std::vector<double> sums(static_cast<size_t>(R) * 8);
+    P3MX_CUDA(cudaMemcpyAsync(sums.data(), m_sums_x.p, sums.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    if (energies)
+      energies->assign(R, 0.0);
+    if (virials)
+      virials->assign(static_cast<size_t>(R) * 9, 0.0);
+    for (int r = 0; r < R; ++r) {
+      auto const &G = m_geom[r];
+      double const *s = &sums[8 * r];
+      if (energies) {
+        // p3m.cpp:551-589: mesh sum / 2V, self energy, net charge, dipole
+        double e = s[0] / (2.0 * G.V);
+        e -= G.sum_q2 * G.alpha / std::sqrt(kPi);
+        e -= G.sum_q * G.sum_q * kPi / (2.0 * G.V * G.alpha * G.alpha);
+        if (G.epsilon != 0.0) {
+          double const *m = &m_census_h[6 * r + 3];
+          e += 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0) * (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        }
+        (*energies)[r] = e * G.prefactor;
+      }
+      if (virials) {
+        // long_range_pressure, p3m.cpp:394-449
+        double t[9];
+        t[0] = s[1] + s[7];
+        t[1] = s[2];
+        t[2] = s[3];
+        t[4] = s[4] + s[7];
+        t[5] = s[5];
+        t[8] = s[6] + s[7];
+        t[3] = t[1];
+        t[6] = t[2];
+        t[7] = t[5];
+        for (int k = 0; k < 9; ++k)
+          (*virials)[9 * r + k] = t[k] * G.prefactor / (2.0 * G.V);
+      }
+    }
+  }
+}
+
+void Engine::build_lists(cudaStream_t st) {
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
+  int const nb = ceil_div(m_n, 256);
+  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
+  k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr);
+  sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
+            m_cperm.as<int>(), m_cells, st);
+  k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
+                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr);
+  if (m_max_nb == 0) {
+    // neighbour estimate from the densest replica plus margin
+    double est = 16.0;
+    for (auto const &G : m_geom) {
+      double const rc = G.max_cut + G.skin;
+      double const rho = G.np / G.V;
+      est = std::max(est, 1.5 * 4.18879 * rc * rc * rc * rho + 32.0);
+    }
+    m_max_nb = static_cast<int>(est);
+  }
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    m_nb.ensure(static_cast<size_t>(m_max_nb) * std::max<long long>(1, m_n) * sizeof(int));
+    P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, sizeof(int), st));
+    k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
+                                       m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
+                                       m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
+                                       m_overflow.as<int>(), nullptr);
+    int ov = 0;
+    P3MX_CUDA(cudaMemcpyAsync(&ov, m_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    if (ov == 0)
+      break;
+    m_max_nb = ov + ov / 4 + 16;
+    if (attempt == 3)
+      throw Error(2, "Verlet list overflow");
+  }
+  P3MX_CUDA(cudaMemcpyAsync(m_pos_ref.p, d_pos(), 3 * m_n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  m_lists_valid = true;
+}
+
+__global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                              const int *__restrict__ perm, const double *__restrict__ pos,
+                              const double *__restrict__ q, long long n, double4 *__restrict__ spq) {
+  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  int const i = perm[s];
+  RepGeom const &G = reps[rep_of[i]];
+  spq[s] = make_double4(fold_coord(pos[3 * i], G.box[0]), fold_coord(pos[3 * i + 1], G.box[1]),
+                        fold_coord(pos[3 * i + 2], G.box[2]), q[i]);
+}
+
+void Engine::refresh_sorted_positions(cudaStream_t st) {
+  k_refresh_spq<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(),
+                                                    m_cperm.as<int>(), d_pos(), d_q(), m_n,
+                                                    m_spq.as<double4>());
+}
+
+template <typename Real>
+void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
+  if (m_n == 0)
+    return;
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
+  int const nb = ceil_div(m_n, 256);
+  bool rebuild = !m_lists_valid;
+  if (!rebuild) {
+    P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
+    k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
+                                             m_n, m_flag.as<int>());
+    int flag = 0;
+    P3MX_CUDA(cudaMemcpyAsync(&flag, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    rebuild = (flag != 0);
+  }
+  if (rebuild)
+    build_lists(st);
+  else
+    refresh_sorted_positions(st);
+  size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
+  k_pair_forces<Real><<<m_n_blk_pair, 256, smem, st>>>(geom, m_blk_pair.as<int2>(), m_spq.as<double4>(),
+                                             m_stype.as<int>(), m_cperm.as<int>(), m_ia_d.as<PairIA>(),
+                                             m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+                                             overwrite ? 1 : 0, want_ev ? 1 : 0,
+                                             m_part_pair.as<double>());
+}
+
+void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,
+                         std::vector<double> *energies, std::vector<double> *virials) {
+  if (m_fp32)
+    short_range_t<float>(f, overwrite, want_ev, st);
+  else
+    short_range_t<double>(f, overwrite, want_ev, st);
+  P3MX_CUDA(cudaGetLastError());
+  if (want_ev && m_n > 0) {
+    int const R = n_rep();
+    k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_pair.as<double>(), 20,
+                                                        m_blk_pair_start_d.as<int>(), R,
+                                                        m_sums_pair.as<double>());
+    std::vector<double> sums(static_cast<size_t>(R) * 20);
+    P3MX_CUDA(cudaMemcpyAsync(sums.data(), m_sums_pair.p, sums.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    if (energies)
+      energies->assign(static_cast<size_t>(R) * 2, 0.0);
+    if (virials)
+      virials->assign(static_cast<size_t>(R) * 18, 0.0);
+    for (int r = 0; r < R; ++r) {
+      if (energies) {
+        (*energies)[2 * r] = sums[20 * r];
+        (*energies)[2 * r + 1] = sums[20 * r + 1];
+      }
+      if (virials)
+        for (int k = 0; k < 18; ++k)
+          (*virials)[18 * r + k] = sums[20 * r + 2 + k];
+    }
+  }
+}
+
+// Graph-capturable short-range step: the displacement check raises a device
+// flag, and the whole rebuild chain (cell binning, counting sort, gather,
+// Verlet build, reference positions) runs only when it is set, so no host
+// decision is needed between steps.
+void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
+  if (m_n == 0)
+    return;
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
+  int const nb = ceil_div(m_n, 256);
+  int *flag = m_flag.as<int>();
+  k_fill_int<<<1, 32, 0, st>>>(flag, 0, 1, nullptr);
+  k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
+                                           m_n, flag);
+  k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag);
+  k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag);
+  sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
+            m_cperm.as<int>(), m_cells, st, flag);
+  k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
+                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), flag);
+  k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
+                                     m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
+                                     m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
+                                     m_overflow.as<int>(), flag);
+  k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag);
+  refresh_sorted_positions(st);
+  size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
+  if (m_fp32)
+    k_pair_forces<float><<<m_n_blk_pair, 256, smem, st>>>(
+        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0, 0,
+        m_part_pair.as<double>());
+  else
+    k_pair_forces<double><<<m_n_blk_pair, 256, smem, st>>>(
+        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0, 0,
+        m_part_pair.as<double>());
+}
+
+int Engine::list_overflow(cudaStream_t st) {
+  int ov = 0;
+  P3MX_CUDA(cudaMemcpyAsync(&ov, m_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  return ov;
+}
+
+void Engine::ensure_lists(cudaStream_t st, double nb_margin) {
+  int want = m_max_nb;
+  if (nb_margin > 1.0) {
+    double est = 16.0;
+    for (auto const &G : m_geom) {
+      double const rc = G.max_cut + G.skin;
+      est = std::max(est, nb_margin * 4.18879 * rc * rc * rc * (G.np / G.V) + 48.0);
+    }
+    want = std::max(want, static_cast<int>(est));
+  }
+  if (want != m_max_nb) {
+    m_max_nb = want;
+    m_lists_valid = false;
+  }
+  if (!m_lists_valid)
+    build_lists(st);
+}
+
+std::vector<int> Engine::cell_index_ghost(cudaStream_t st) {
+  std::vector<int> out(m_n);
+  if (m_n == 0)
+    return out;
+  DevBuf gi;
+  gi.ensure(m_n * sizeof(int));
+  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
+  k_cell_bin<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(),
+                                                 d_q(), m_n, m_ckey.as<int>(), m_cslot.as<int>(),
+                                                 m_ccnt.as<int>(), m_pq.as<double4>(), gi.as<int>(),
+                                                 nullptr);
+  P3MX_CUDA(cudaMemcpyAsync(out.data(), gi.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  m_lists_valid = false;
+  return out;
+}
+
+std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
+  build_lists(st);
+  std::vector<int> cnt(m_n), perm(m_n);
+  std::vector<int> nbh(static_cast<size_t>(m_max_nb) * m_n);
+  P3MX_CUDA(cudaMemcpyAsync(cnt.data(), m_nb_cnt.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaMemcpyAsync(perm.data(), m_cperm.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaMemcpyAsync(nbh.data(), m_nb.p, nbh.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> pairs;
+  for (long long a = 0; a < m_n; ++a)
+    for (int k = 0; k < cnt[a]; ++k) {
+      int const b = nbh[static_cast<size_t>(k) * m_n + a];
+      int const i = perm[a], j = perm[b];
+      if (i < j) {
+        pairs.push_back(i);
+        pairs.push_back(j);
+      }
+    }
+  return pairs;
+}
+
+std::vector<double> Engine::mesh_copy(int r, cudaStream_t st) {
+  auto const &G = m_geom[r];
+  long long const ms = static_cast<long long>(G.mesh[0]) * G.mesh[1] * G.mesh[2];
+  std::vector<double> out(ms);
+  if (m_fp32) {
+    std::vector<float> t(ms);
+    P3MX_CUDA(cudaMemcpyAsync(t.data(), m_rho.as<float>() + G.rm_off, ms * sizeof(float),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    for (long long k = 0; k < ms; ++k)
+      out[k] = t[k];
+  } else {
+    P3MX_CUDA(cudaMemcpyAsync(out.data(), m_rho.as<double>() + G.rm_off, ms * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+  }
+  return out;
+}
+
+void Engine::cell_grid(int r, int *cg, double *cs) const {
+  for (int d = 0; d < 3; ++d) {
+    cg[d] = m_geom[r].cg[d];
+    cs[d] = 1.0 / m_geom[r].inv_cs[d];
+  }
+}
+
+double Engine::ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,
+                        const double *box, double prefactor) {
+  int const nblk = 296;
+  m_ks_part.ensure(nblk * sizeof(double));
+  k_ks_error<<<nblk, 256, 0, m_stream>>>(mesh[0], mesh[1], mesh[2], cao, alpha_L,
+                                         m_ks_part.as<double>());
+  std::vector<double> part(nblk);
+  P3MX_CUDA(cudaMemcpyAsync(part.data(), m_ks_part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost,
+                            m_stream));
+  P3MX_CUDA(cudaStreamSynchronize(m_stream));
+  double he_q = 0.0;
+  for (double v : part)
+    he_q += v;
+  return 2. * prefactor * sum_q2 * std::sqrt(he_q / static_cast<double>(n_c_part)) / (box[1] * box[2]);
+}
+
+} // namespace p3mx

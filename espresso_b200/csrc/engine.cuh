@@ -1,0 +1,165 @@
+// Host-side engine: owns device buffers, FFT plans and block tables for a
+// batch of one or more independent periodic systems (replicas), and runs
+// the long-range (P3M) and short-range (pair) pipelines on one stream.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "pair.cuh"
+
+#include <memory>
+#include <vector>
+
+namespace p3mx {
+
+// Raw device buffer with grow-only reallocation.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(DevBuf const &) = delete;
+  DevBuf &operator=(DevBuf const &) = delete;
+  ~DevBuf() {
+    if (p)
+      cudaFree(p);
+  }
+  void ensure(size_t nbytes) {
+    if (nbytes <= bytes && p)
+      return;
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t const want = nbytes ? nbytes : 16;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(4, "device allocation of " + std::to_string(want) + " bytes failed");
+    }
+    bytes = want;
+  }
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Host-side configuration of one replica.
+struct ReplicaConf {
+  double box[3] = {0, 0, 0};
+  double prefactor = 0.0;
+  double epsilon = 0.0;
+  double mesh_off[3] = {0.5, 0.5, 0.5};
+  int mesh[3] = {0, 0, 0};
+  int cao = 0;
+  double alpha = 0.0;
+  double r_cut = 0.0;
+  double skin = 0.4;
+  long long p0 = 0, np = 0;
+};
+
+struct Timing {
+  float ms_long = 0.f, ms_short = 0.f;
+};
+
+class Engine {
+public:
+  explicit Engine(bool fp32);
+  ~Engine();
+
+  bool fp32() const { return m_fp32; }
+  int n_rep() const { return static_cast<int>(m_conf.size()); }
+  long long n_part() const { return m_n; }
+  ReplicaConf const &conf(int r) const { return m_conf[r]; }
+  cudaStream_t stream() const { return m_stream; }
+
+  // (Re)builds geometry, plans, block tables; allocates the buffers.
+  void configure(std::vector<ReplicaConf> const &conf, long long n_total);
+  // LJ/WCA table (ntypes^2 entries, symmetric).
+  void set_pair_table(int ntypes, std::vector<PairIA> const &tab);
+
+  // Device-resident particle arrays in user order (AoS positions/forces).
+  double *d_pos() const { return m_pos.as<double>(); }
+  double *d_q() const { return m_q.as<double>(); }
+  int *d_type() const { return m_type.as<int>(); }
+  double *d_force() const { return m_force.as<double>(); }
+  void upload(const double *pos, const double *q, const int *type, bool device_ptrs,
+              cudaStream_t st);
+  void upload_positions(const double *pos, bool device_ptrs, cudaStream_t st);
+
+  // Charge census (n_charged, sum q, sum q^2, dipole) per replica -> host.
+  void census(cudaStream_t st);
+  std::vector<double> const &census_host() const { return m_census_h; }
+
+  // k-space pipeline for all replicas.  f: device force array (3N) or
+  // nullptr; energies[r], virial[r*9] written on the host if requested.
+  void long_range(double *f, bool overwrite, bool want_energy, bool want_virial,
+                  cudaStream_t st, std::vector<double> *energies,
+                  std::vector<double> *virials);
+  // Real-space + LJ/WCA over Verlet lists.  energies[r*2], virials[r*18].
+  void short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,
+                   std::vector<double> *energies, std::vector<double> *virials);
+  // Graph-capturable short-range evaluation (device-side rebuild decision).
+  void short_range_graph(double *f, bool overwrite, cudaStream_t st);
+  // Build lists now if invalid (capacity margin factor for graph use).
+  void ensure_lists(cudaStream_t st, double nb_margin = 1.5);
+  // Largest neighbour count that did not fit (0 if none) since last reset.
+  int list_overflow(cudaStream_t st);
+  // Force the next short_range call to rebuild cells and lists.
+  void invalidate_lists() { m_lists_valid = false; }
+
+  // Introspection for parity tests.
+  std::vector<int> cell_index_ghost(cudaStream_t st);
+  std::vector<int> verlet_pairs(cudaStream_t st);
+  std::vector<double> mesh_copy(int r, cudaStream_t st);
+  void cell_grid(int r, int *cg, double *cs) const;
+
+  // k-space error sum (device, FP64) for tuning.
+  double ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,
+                  const double *box, double prefactor);
+
+private:
+  template <typename Real> void long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
+                                             cudaStream_t st);
+  template <typename Real> void short_range_t(double *f, bool overwrite, bool want_ev,
+                                              cudaStream_t st);
+  void build_lists(cudaStream_t st);
+  void refresh_sorted_positions(cudaStream_t st);
+  void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
+                 cudaStream_t st, const int *cond = nullptr);
+
+  bool m_fp32;
+  cudaStream_t m_stream = nullptr;
+  std::vector<ReplicaConf> m_conf;
+  std::vector<RepGeom> m_geom;
+  long long m_n = 0;
+  long long m_bins = 0, m_cplx = 0, m_cells = 0;
+  int m_ntypes = 1;
+  std::vector<PairIA> m_ia;
+
+  // tables
+  DevBuf m_geom_d, m_rep_of, m_tw, m_ia_d;
+  DevBuf m_blk_mesh, m_blk_cplx, m_blk_census, m_blk_pair;
+  DevBuf m_blk_zf, m_blk_y, m_blk_x, m_blk_zi;
+  std::vector<int> m_blk_x_start, m_blk_census_start, m_blk_pair_start;
+  DevBuf m_blk_x_start_d, m_blk_census_start_d, m_blk_pair_start_d;
+  int m_n_blk_mesh = 0, m_n_blk_cplx = 0, m_n_blk_census = 0, m_n_blk_pair = 0;
+  int m_n_blk_zf = 0, m_n_blk_y = 0, m_n_blk_x = 0, m_n_blk_zi = 0;
+  int m_tile_y = 16, m_tile_x = 16;
+  size_t m_smem_zf = 0, m_smem_y = 0, m_smem_x = 0, m_smem_zi = 0;
+
+  // particles
+  DevBuf m_pos, m_q, m_type, m_force;
+  // p3m
+  DevBuf m_key, m_slot, m_cnt, m_start, m_perm, m_scan_tiles;
+  DevBuf m_dist, m_W, m_scz, m_skey;
+  DevBuf m_rho, m_ck, m_field, m_E, m_ginf;
+  DevBuf m_part_x, m_part_census, m_sums_x, m_sums_census, m_dipole;
+  bool m_ginf_valid = false;
+  std::vector<double> m_census_h;
+  // short range
+  DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_stype, m_scell;
+  DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_part_pair, m_sums_pair;
+  int m_max_nb = 0;
+  bool m_lists_valid = false;
+  // misc host staging
+  DevBuf m_ks_part;
+};
+
+} // namespace p3mx

@@ -1,0 +1,371 @@
+// Hand-written mixed-radix 3D FFT for the P3M mesh (sm_100a).
+//
+// Real mesh [M0][M1][M2] (z fastest) <-> complex half mesh [M0][M1][hp]
+// (kz < M2/2+1 used, hp = padded row length).  Forward = exp(-i k x),
+// backward = exp(+i k x), both unnormalised, as the reference's FFTW
+// plans (fft/fft.cpp:682-696).  Each pass stages a tile of lines in shared
+// memory and runs Stockham autosort stages of radix 4, 2 or a generic
+// prime radix (Govindaraju et al. 2008 formulation); twiddles come from an
+// FP64-computed table rounded to the working precision.
+//
+// The x pass is fused with the P3M k-space work that follows the forward
+// transform: optimal influence function, ik-differentiation (three field
+// components), k-space energy and pressure-tensor sums, and the three
+// backward x transforms -- one HBM round trip instead of five.
+#pragma once
+
+#include "common.cuh"
+
+namespace p3mx {
+
+// Block work item of an FFT pass: replica, first item, item count.
+struct Blk {
+  int rep;
+  int a;   // first line / x / y index
+  int b;   // second index (kz tile start) or unused
+  int pad;
+};
+
+template <typename C> __device__ inline C ld_tw(const C *__restrict__ tw, int k, bool inv) {
+  C w = tw[k];
+  if (inv)
+    w.y = -w.y;
+  return w;
+}
+
+template <typename C, int R>
+__device__ inline void dft_small(C *v, const C *__restrict__ tw, int n, bool inv) {
+  if constexpr (R == 2) {
+    C const a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    C const s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]);
+    C const s2 = cadd(v[1], v[3]), s3 = csub(v[1], v[3]);
+    // forward: multiply s3 by -i; backward: by +i
+    C const s3r = inv ? C{-s3.y, s3.x} : C{s3.y, -s3.x};
+    v[0] = cadd(s0, s2);
+    v[2] = csub(s0, s2);
+    v[1] = cadd(s1, s3r);
+    v[3] = csub(s1, s3r);
+  } else {
+    C out[R];
+    int const step = n / R;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      C acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        int const e = (r * m) % R;
+        acc = cadd(acc, cmul(v[r], ld_tw(tw, e * step, inv)));
+      }
+      out[m] = acc;
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m)
+      v[m] = out[m];
+  }
+}
+
+// Generic (runtime) radix for primes beyond the templated set.
+template <typename C>
+__device__ inline void dft_dyn(C *v, int R, const C *__restrict__ tw, int n, bool inv) {
+  C out[32];
+  int const step = n / R;
+  for (int m = 0; m < R; ++m) {
+    C acc = v[0];
+    for (int r = 1; r < R; ++r) {
+      int const e = (r * m) % R;
+      acc = cadd(acc, cmul(v[r], ld_tw(tw, e * step, inv)));
+    }
+    out[m] = acc;
+  }
+  for (int m = 0; m < R; ++m)
+    v[m] = out[m];
+}
+
+// One Stockham stage over `nlines` lines of length n held in shared memory.
+template <typename C, int R>
+__device__ inline void fft_stage_t(const C *src, C *dst, int n, int nlines, int Ns,
+                                   const C *__restrict__ tw, bool inv) {
+  int const nb = n / R;
+  int const total = nb * nlines;
+  int const tstride = n / (Ns * R);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int const line = t / nb;
+    int const j = t - line * nb;
+    C const *s = src + line * n;
+    C *d = dst + line * n;
+    int const jm = j % Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      v[r] = s[j + r * nb];
+      if (r > 0 && jm != 0)
+        v[r] = cmul(v[r], ld_tw(tw, (r * jm * tstride) % n, inv));
+    }
+    dft_small<C, R>(v, tw, n, inv);
+    int const base = (j / Ns) * Ns * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      d[base + r * Ns] = v[r];
+  }
+}
+
+template <typename C>
+__device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int nlines, int Ns,
+                                     int R, const C *__restrict__ tw, bool inv) {
+  int const nb = n / R;
+  int const total = nb * nlines;
+  int const tstride = n / (Ns * R);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int const line = t / nb;
+    int const j = t - line * nb;
+    C const *s = src + line * n;
+    C *d = dst + line * n;
+    int const jm = j % Ns;
+    C v[32];
+    for (int r = 0; r < R; ++r) {
+      v[r] = s[j + r * nb];
+      if (r > 0 && jm != 0)
+        v[r] = cmul(v[r], ld_tw(tw, (r * jm * tstride) % n, inv));
+    }
+    dft_dyn(v, R, tw, n, inv);
+    int const base = (j / Ns) * Ns * R + jm;
+    for (int r = 0; r < R; ++r)
+      d[base + r * Ns] = v[r];
+  }
+}
+
+// Full transform of nlines lines in `a` (scratch `b`); returns the buffer
+// holding the result.  All threads of the block must call it.
+template <typename C>
+__device__ C *fft_lines(C *a, C *b, int nlines, AxisPlan const &pl,
+                        const C *__restrict__ twtab, bool inv) {
+  int const n = pl.n;
+  const C *tw = twtab + pl.tw_off;
+  int Ns = 1;
+  C *src = a, *dst = b;
+  for (int s = 0; s < pl.nstages; ++s) {
+    int const R = pl.radix[s];
+    switch (R) {
+    case 2: fft_stage_t<C, 2>(src, dst, n, nlines, Ns, tw, inv); break;
+    case 3: fft_stage_t<C, 3>(src, dst, n, nlines, Ns, tw, inv); break;
+    case 4: fft_stage_t<C, 4>(src, dst, n, nlines, Ns, tw, inv); break;
+    case 5: fft_stage_t<C, 5>(src, dst, n, nlines, Ns, tw, inv); break;
+    case 7: fft_stage_t<C, 7>(src, dst, n, nlines, Ns, tw, inv); break;
+    default: fft_stage_dyn<C>(src, dst, n, nlines, Ns, R, tw, inv); break;
+    }
+    __syncthreads();
+    Ns *= R;
+    C *t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+// ---- pass z, forward: real lines -> complex half lines -----------------
+template <typename Real>
+__global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+                            const Real *__restrict__ rmesh,
+                            typename CplxOf<Real>::type *__restrict__ cmesh,
+                            const typename CplxOf<Real>::type *__restrict__ twtab) {
+  using C = typename CplxOf<Real>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Blk const bk = blks[blockIdx.x];
+  RepGeom const &G = reps[bk.rep];
+  int const n = G.mesh[2];
+  int const nl = bk.b; // lines in this block
+  C *a = reinterpret_cast<C *>(smem_raw);
+  C *b = a + nl * n;
+  long long const line0 = bk.a;
+  const Real *src = rmesh + G.rm_off + line0 * n;
+  for (int e = threadIdx.x; e < nl * n; e += blockDim.x)
+    a[e] = C{src[e], Real(0)};
+  __syncthreads();
+  C *res = fft_lines<C>(a, b, nl, G.plan[2], twtab, false);
+  int const H = n / 2 + 1;
+  for (int e = threadIdx.x; e < nl * G.hp; e += blockDim.x) {
+    int const l = e / G.hp, k = e - l * G.hp;
+    C v = (k < H) ? res[l * n + k] : C{Real(0), Real(0)};
+    cmesh[G.km_off + (line0 + l) * G.hp + k] = v;
+  }
+}
+
+// ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
+template <typename Real>
+__global__ void k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+                        typename CplxOf<Real>::type *__restrict__ c0,
+                        long long field_stride, int tile, bool inv,
+                        const typename CplxOf<Real>::type *__restrict__ twtab) {
+  using C = typename CplxOf<Real>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Blk const bk = blks[blockIdx.x];
+  RepGeom const &G = reps[bk.rep];
+  C *cm = c0 + field_stride * blockIdx.y;
+  int const M1 = G.mesh[1];
+  int const H = G.mesh[2] / 2 + 1;
+  int const x = bk.a, kz0 = bk.b;
+  int const T = min(tile, H - kz0);
+  C *a = reinterpret_cast<C *>(smem_raw);
+  C *b = a + T * M1;
+  long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp;
+  for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
+    int const y = e / T, t = e - y * T;
+    a[t * M1 + y] = cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t];
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(a, b, T, G.plan[1], twtab, inv);
+  for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
+    int const y = e / T, t = e - y * T;
+    cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t] = res[t * M1 + y];
+  }
+}
+
+// ---- pass x fused with the k-space operator -----------------------------
+// Per block: one ky, a tile of kz; partials[blk*8 + {E, Pxx, Pxy, Pxz, Pyy,
+// Pyz, Pzz, diag}] in FP64 (Hermitian weights 1 for kz = 0, M2/2, else 2).
+template <typename Real>
+__global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+                               const typename CplxOf<Real>::type *__restrict__ rho_hat,
+                               const Real *__restrict__ ginf,
+                               typename CplxOf<Real>::type *__restrict__ field0,
+                               long long field_stride, int tile, int want_fields,
+                               int want_ev, double *__restrict__ partials,
+                               const typename CplxOf<Real>::type *__restrict__ twtab) {
+  using C = typename CplxOf<Real>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Blk const bk = blks[blockIdx.x];
+  RepGeom const &G = reps[bk.rep];
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const H = M2 / 2 + 1;
+  int const y = bk.a, kz0 = bk.b;
+  int const T = min(tile, H - kz0);
+  int const L = T * M0;
+  C *a = reinterpret_cast<C *>(smem_raw);
+  C *b = a + 3 * L; // scratch of the same size (3 fields)
+  long long const stride_x = static_cast<long long>(M1) * G.hp;
+  long long const base = G.km_off + static_cast<long long>(y) * G.hp + kz0;
+  for (int e = threadIdx.x; e < L; e += blockDim.x) {
+    int const x = e / T, t = e - x * T;
+    a[t * M0 + x] = rho_hat[base + x * stride_x + t];
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(a, b, T, G.plan[0], twtab, false);
+  // k-space operator
+  double const wv[3] = {2.0 * kPi * G.box_i[0], 2.0 * kPi * G.box_i[1],
+                        2.0 * kPi * G.box_i[2]};
+  double const hai2 = (1.0 / 2.0 / G.alpha) * (1.0 / 2.0 / G.alpha);
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  C *fbuf = (res == a) ? b : a; // the three field lines go to the free buffer
+  // d_op (Nyquist zeroed) integer shift of index i in a mesh of size m
+  auto dop = [](int i, int m) { return (i == m / 2) ? 0 : (i < m / 2 ? i : i - m); };
+  int const kyd = dop(y, M1);
+  for (int e = threadIdx.x; e < L; e += blockDim.x) {
+    int const t = e / M0, x = e - t * M0;
+    int const kz = kz0 + t;
+    C const rh = res[t * M0 + x];
+    Real const g = ginf[base + x * stride_x + t];
+    int const kxd = dop(x, M0), kzd = dop(kz, M2);
+    if (want_ev) {
+      double const wgt = (kz == 0 || kz == M2 / 2) ? 1.0 : 2.0;
+      double const ek = wgt * static_cast<double>(g) *
+                        (static_cast<double>(rh.x) * rh.x + static_cast<double>(rh.y) * rh.y);
+      acc[0] += ek;
+      double const kx = kxd * wv[0], ky = kyd * wv[1], kzv = kzd * wv[2];
+      double const nsq = kx * kx + ky * ky + kzv * kzv;
+      if (nsq != 0.0) {
+        double const pr = ek * (-2.0 * (1.0 / nsq + hai2));
+        acc[1] += pr * kx * kx;
+        acc[2] += pr * kx * ky;
+        acc[3] += pr * kx * kzv;
+        acc[4] += pr * ky * ky;
+        acc[5] += pr * ky * kzv;
+        acc[6] += pr * kzv * kzv;
+        acc[7] += ek;
+      }
+    }
+    if (want_fields) {
+      C const phi{g * rh.x, g * rh.y};
+      Real const k0 = static_cast<Real>(kxd) * static_cast<Real>(wv[0]);
+      Real const k1 = static_cast<Real>(kyd) * static_cast<Real>(wv[1]);
+      Real const k2 = static_cast<Real>(kzd) * static_cast<Real>(wv[2]);
+      fbuf[0 * L + t * M0 + x] = C{-k0 * phi.y, k0 * phi.x};
+      fbuf[1 * L + t * M0 + x] = C{-k1 * phi.y, k1 * phi.x};
+      fbuf[2 * L + t * M0 + x] = C{-k2 * phi.y, k2 * phi.x};
+    }
+  }
+  if (want_ev) {
+    // block reduction of the 8 partial sums (fixed order -> deterministic)
+    __shared__ double red[8][32];
+    int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0)
+        red[k][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+      double s = 0.0;
+      int const nw = (blockDim.x + 31) >> 5;
+      for (int w = 0; w < nw; ++w)
+        s += red[threadIdx.x][w];
+      partials[static_cast<long long>(blockIdx.x) * 8 + threadIdx.x] = s;
+    }
+  }
+  if (!want_fields)
+    return;
+  __syncthreads();
+  C *scratch = (fbuf == a) ? b : a;
+  C *fres = fft_lines<C>(fbuf, scratch, 3 * T, G.plan[0], twtab, true);
+  for (int e = threadIdx.x; e < 3 * L; e += blockDim.x) {
+    int const d = e / L, r = e - d * L;
+    int const x = r / T, t = r - x * T;
+    field0[field_stride * d + base + x * stride_x + t] = fres[d * L + t * M0 + x];
+  }
+}
+
+// ---- pass z, backward for the 3 field components -> real fields --------
+template <typename Real>
+__global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+                             const typename CplxOf<Real>::type *__restrict__ field0,
+                             long long field_stride, Real *__restrict__ efield,
+                             long long efield_stride,
+                             const typename CplxOf<Real>::type *__restrict__ twtab) {
+  using C = typename CplxOf<Real>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Blk const bk = blks[blockIdx.x];
+  RepGeom const &G = reps[bk.rep];
+  int const n = G.mesh[2];
+  int const H = n / 2 + 1;
+  int const nl = bk.b;
+  long long const line0 = bk.a;
+  C *a = reinterpret_cast<C *>(smem_raw);
+  C *b = a + 3 * nl * n;
+  for (int e = threadIdx.x; e < 3 * nl * n; e += blockDim.x) {
+    int const dl = e / n, k = e - dl * n; // dl = d * nl + l
+    int const d = dl / nl, l = dl - d * nl;
+    const C *src = field0 + field_stride * d + G.km_off + (line0 + l) * G.hp;
+    C v;
+    if (k < H) {
+      v = src[k];
+    } else {
+      v = cconj(src[n - k]);
+    }
+    a[e] = v;
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(a, b, 3 * nl, G.plan[2], twtab, true);
+  for (int e = threadIdx.x; e < 3 * nl * n; e += blockDim.x) {
+    int const dl = e / n, z = e - dl * n;
+    int const d = dl / nl, l = dl - d * nl;
+    efield[efield_stride * d + G.rm_off + (line0 + l) * n + z] = res[e].x;
+  }
+}
+
+} // namespace p3mx

@@ -1,0 +1,433 @@
+// P3M particle <-> mesh kernels (sm_100a): corner binning, B-spline weights,
+// gather-based deterministic charge assignment, force back-interpolation,
+// influence function, charge census and the k-space error sum.
+#pragma once
+
+#include "common.cuh"
+
+namespace p3mx {
+
+// Fold into [0, L) like algorithm/periodic_fold.hpp:72-89 (repeated shifts);
+// far-away coordinates are first brought close by whole periods.
+__device__ inline double fold_coord(double x, double L) {
+  if (x < -2.0 * L || x >= 3.0 * L)
+    x -= floor(x / L) * L;
+  int guard = 0;
+  while (x < 0.0 && guard++ < 8)
+    x += L;
+  while (x >= L && guard++ < 16)
+    x -= L;
+  return x;
+}
+
+// Cardinal B-spline weights of order P at the P points around a particle
+// (x = distance to the nearest mesh point, [-0.5, 0.5]) by the Cox-de Boor
+// recursion; w[i] = M_P(x + 1/2 + P-1-i), the values tabulated in
+// utils/math/bspline.hpp:30-177.
+template <int P, typename Real>
+__device__ inline void bspline_weights(Real x, Real *w) {
+  Real c[P];
+  Real const u = x + Real(0.5);
+  c[0] = Real(1);
+#pragma unroll
+  for (int n = 1; n < P; ++n) {
+    Real const inv_n = Real(1) / Real(n);
+    c[n] = Real(0);
+#pragma unroll
+    for (int k = n; k >= 0; --k) {
+      Real const left = (k > 0) ? c[k - 1] : Real(0);
+      c[k] = ((u + Real(k)) * c[k] + (Real(n + 1) - u - Real(k)) * left) * inv_n;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < P; ++i)
+    w[i] = c[P - 1 - i];
+}
+
+// Per particle: nearest-mesh-point corner and the distance to it, following
+// p3m_calculate_interpolation_weights (p3m/interpolation.hpp:138-178) with
+// the single-rank CA-mesh origin of P3MLocalMesh (p3m/common.cpp:34-106).
+// key = corner bin (replica mesh offset + (cx*M1+cy)*M2+cz).
+template <typename Real>
+__global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                          const double *__restrict__ pos, long long n,
+                          int *__restrict__ key, int *__restrict__ slot,
+                          int *__restrict__ cnt, Real *__restrict__ dist) {
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  RepGeom const &G = reps[rep_of[i]];
+  int g[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double const xf = fold_coord(pos[3 * i + d], G.box[d]);
+    double const p = ((xf - G.ld_pos[d]) * G.ai[d]) - G.pos_shift;
+    int const nmp = static_cast<int>(p);
+    double const ds = (p - nmp) - 0.5;
+    int c = (G.ld_ind[d] + nmp) % G.mesh[d];
+    if (c < 0)
+      c += G.mesh[d];
+    g[d] = c;
+    dist[3 * i + d] = static_cast<Real>(ds);
+  }
+  int const k = static_cast<int>(G.rm_off) + (g[0] * G.mesh[1] + g[1]) * G.mesh[2] + g[2];
+  key[i] = k;
+  slot[i] = atomicAdd(&cnt[k], 1);
+}
+
+// Weights in corner-sorted order: W[s] = {q*wx[0..P), wy[0..P), wz[0..P)};
+// also the z corner and the corner key of every sorted particle.
+template <typename Real, int P>
+__global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
+                              const int *__restrict__ key, const Real *__restrict__ dist,
+                              const double *__restrict__ q, const int *__restrict__ rep_of,
+                              long long n, Real *__restrict__ W, int *__restrict__ s_cz,
+                              int *__restrict__ s_key) {
+  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  int const i = perm[s];
+  RepGeom const &G = reps[rep_of[i]];
+  Real w[3][P];
+  bspline_weights<P>(dist[3 * i + 0], w[0]);
+  bspline_weights<P>(dist[3 * i + 1], w[1]);
+  bspline_weights<P>(dist[3 * i + 2], w[2]);
+  Real const qi = static_cast<Real>(q[i]);
+  Real *o = W + s * (3 * P);
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    o[k] = qi * w[0][k];
+    o[P + k] = w[1][k];
+    o[2 * P + k] = w[2][k];
+  }
+  int const loc = key[i] - static_cast<int>(G.rm_off);
+  s_key[s] = loc;
+  s_cz[s] = loc % G.mesh[2];
+}
+
+// Two-sum (Knuth): exact error term of a + b, for compensated summation.
+template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v) {
+  Real const t = s + v;
+  Real const bp = t - s;
+  Real const err = (s - (t - bp)) + (v - bp);
+  s = t;
+  c += err;
+}
+
+// Gather-based charge assignment: one thread per mesh point g sums, in a
+// fixed order, the contributions q*wx*wy*wz of every particle whose stencil
+// covers g (corners in [g-P+1, g] per axis, periodic).  No atomics: the
+// result is bitwise reproducible.  For FP32 the column sums are combined
+// with compensated (two-sum) accumulation.
+template <typename Real, int P>
+__global__ void __launch_bounds__(256)
+k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+             const int *__restrict__ start, const Real *__restrict__ W,
+             const int *__restrict__ s_cz, Real *__restrict__ rho) {
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  long long const local = static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  long long const msize = static_cast<long long>(M0) * M1 * M2;
+  if (local >= msize)
+    return;
+  int const gz = static_cast<int>(local % M2);
+  int const gy = static_cast<int>((local / M2) % M1);
+  int const gx = static_cast<int>(local / (static_cast<long long>(M1) * M2));
+  const int *st = start + G.rm_off;
+  Real sum = Real(0), comp = Real(0);
+  int const z_lo = gz - (P - 1);
+#pragma unroll 1
+  for (int kx = 0; kx < P; ++kx) {
+    int cx = gx - kx;
+    if (cx < 0)
+      cx += M0;
+#pragma unroll 1
+    for (int ky = 0; ky < P; ++ky) {
+      int cy = gy - ky;
+      if (cy < 0)
+        cy += M1;
+      int const row = (cx * M1 + cy) * M2;
+      Real col = Real(0);
+      // corner z in [z_lo, gz], split at the periodic wrap
+      int r0a, r0b, r1a = 0, r1b = 0;
+      if (z_lo >= 0) {
+        r0a = st[row + z_lo];
+        r0b = st[row + gz + 1];
+      } else {
+        r1a = st[row + M2 + z_lo];
+        r1b = st[row + M2];
+        r0a = st[row];
+        r0b = st[row + gz + 1];
+      }
+      for (int s = r1a; s < r1b; ++s) {
+        int const kz = gz - (s_cz[s] - M2);
+        const Real *w = W + static_cast<long long>(s) * (3 * P);
+        col += w[kx] * w[P + ky] * w[2 * P + kz];
+      }
+      for (int s = r0a; s < r0b; ++s) {
+        int const kz = gz - s_cz[s];
+        const Real *w = W + static_cast<long long>(s) * (3 * P);
+        col += w[kx] * w[P + ky] * w[2 * P + kz];
+      }
+      if constexpr (sizeof(Real) == 4)
+        two_sum(sum, comp, col);
+      else
+        sum += col;
+    }
+  }
+  rho[G.rm_off + local] = sum + comp;
+}
+
+// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373):
+// per sorted particle F -= prefactor/V * sum_{stencil} (q wx wy wz) E, FP32
+// row sums accumulated in FP64; plus the dipole term for epsilon != 0
+// (p3m.cpp:540-547).  Writes (or adds) to f[3*i] of the original index.
+template <typename Real, int P>
+__global__ void __launch_bounds__(256)
+k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
+             const int *__restrict__ rep_of, const int *__restrict__ s_key,
+             const Real *__restrict__ W, const Real *__restrict__ E, long long estride,
+             const double *__restrict__ q, const double *__restrict__ dipole,
+             long long n, double *__restrict__ f, int overwrite) {
+  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  int const i = perm[s];
+  int const r = rep_of[i];
+  RepGeom const &G = reps[r];
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const loc = s_key[s];
+  int const cz = loc % M2;
+  int const cy = (loc / M2) % M1;
+  int const cx = loc / (M1 * M2);
+  Real wv[3 * P];
+  const Real *w = W + s * (3 * P);
+#pragma unroll
+  for (int k = 0; k < 3 * P; ++k)
+    wv[k] = w[k];
+  int zi[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    int z = cz + k;
+    zi[k] = (z >= M2) ? z - M2 : z;
+  }
+  const Real *E0 = E + G.rm_off;
+  const Real *E1 = E0 + estride;
+  const Real *E2 = E1 + estride;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll 1
+  for (int kx = 0; kx < P; ++kx) {
+    int gx = cx + kx;
+    if (gx >= M0)
+      gx -= M0;
+#pragma unroll
+    for (int ky = 0; ky < P; ++ky) {
+      int gy = cy + ky;
+      if (gy >= M1)
+        gy -= M1;
+      long long const row = (static_cast<long long>(gx) * M1 + gy) * M2;
+      Real const wxy = wv[kx] * wv[P + ky];
+      Real ax = Real(0), ay = Real(0), az = Real(0);
+#pragma unroll
+      for (int kz = 0; kz < P; ++kz) {
+        long long const idx = row + zi[kz];
+        Real const wt = wxy * wv[2 * P + kz];
+        ax += wt * E0[idx];
+        ay += wt * E1[idx];
+        az += wt * E2[idx];
+      }
+      fx += static_cast<double>(ax);
+      fy += static_cast<double>(ay);
+      fz += static_cast<double>(az);
+    }
+  }
+  double const pref = G.prefactor / G.V;
+  double ox = -pref * fx, oy = -pref * fy, oz = -pref * fz;
+  if (G.epsilon != 0.0) {
+    double const qi = q[i];
+    double const c = G.prefactor * 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0);
+    ox -= qi * c * dipole[3 * r + 0];
+    oy -= qi * c * dipole[3 * r + 1];
+    oz -= qi * c * dipole[3 * r + 2];
+  }
+  if (overwrite) {
+    f[3 * i + 0] = ox;
+    f[3 * i + 1] = oy;
+    f[3 * i + 2] = oz;
+  } else {
+    f[3 * i + 0] += ox;
+    f[3 * i + 1] += oy;
+    f[3 * i + 2] += oz;
+  }
+}
+
+// sinc with the Taylor branch of p3m/math.hpp:53-81.
+__device__ inline double sinc_d(double x) {
+  double const pix = kPi * x;
+  if (fabs(x) > 0.1)
+    return sin(pix) / pix;
+  double const p2 = pix * pix;
+  return 1.0 + p2 * (-1.0 / 6.0 + p2 * (1.0 / 120.0 + p2 * (-1.0 / 5040.0 + p2 * (1.0 / 362880.0))));
+}
+
+// Optimal influence function on the r2c half mesh for m = 0 aliasing
+// (G_opt<S,0>, p3m/influence_function.hpp:53-150): computed in FP64,
+// stored in the working precision.  With m = 0 the force (S=1) and energy
+// (S=0) functions are identical, so one array serves both.
+template <typename Real>
+__global__ void k_influence(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+                            Real *__restrict__ ginf) {
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  long long const local = static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  long long const csize = static_cast<long long>(M0) * M1 * G.hp;
+  if (local >= csize)
+    return;
+  int const kz = static_cast<int>(local % G.hp);
+  int const y = static_cast<int>((local / G.hp) % M1);
+  int const x = static_cast<int>(local / (static_cast<long long>(M1) * G.hp));
+  double val = 0.0;
+  if (kz <= M2 / 2) {
+    bool const all_half = (x % (M0 / 2) == 0) && (y % (M1 / 2) == 0) && (kz % (M2 / 2) == 0);
+    if (!all_half) {
+      auto shift = [](int i, int m) { return (i < m / 2) ? i : i - m; }; // M/2 -> -M/2
+      int const sh[3] = {shift(x, M0), shift(y, M1), shift(kz, M2)};
+      double k[3], fnm[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        k[d] = sh[d] * ((2.0 * kPi) * G.box_i[d]);
+        double const h = G.box[d] / G.mesh[d];
+        double const wvi = 1.0 / ((2.0 * kPi) / h);
+        fnm[d] = sinc_d(k[d] * wvi);
+      }
+      double const k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+      if (k2 != 0.0) {
+        double const U2 = pow(fnm[0] * fnm[1] * fnm[2], 2.0 * G.cao);
+        double const ex = (1.0 / (2.0 * G.alpha)) * (1.0 / (2.0 * G.alpha)) * k2;
+        double num = 0.0;
+        if (ex < 30.0)
+          num = U2 * (exp(-ex) * (4.0 * kPi / k2));
+        val = num / (U2 * U2);
+      }
+    }
+  }
+  ginf[G.km_off + local] = static_cast<Real>(val);
+}
+
+// Per-block FP64 partial sums over particles of one replica:
+// {n_charged, sum q, sum q^2, Mx, My, Mz} (p3m.cpp:98-115, 376-386).
+__global__ void k_census(const int2 *__restrict__ blk, const RepGeom *__restrict__ reps,
+                         const double *__restrict__ pos, const double *__restrict__ q,
+                         double *__restrict__ partials) {
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  long long const i0 = G.p0 + static_cast<long long>(bk.y) * 2048;
+  long long const i1 = min(G.p0 + G.np, i0 + 2048);
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    double const qi = q[i];
+    if (qi != 0.0) {
+      acc[0] += 1.0;
+      acc[1] += qi;
+      acc[2] += qi * qi;
+      acc[3] += qi * pos[3 * i + 0];
+      acc[4] += qi * pos[3 * i + 1];
+      acc[5] += qi * pos[3 * i + 2];
+    }
+  }
+  __shared__ double red[6][32];
+  int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0)
+      red[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w)
+      s += red[threadIdx.x][w];
+    partials[static_cast<long long>(blockIdx.x) * 6 + threadIdx.x] = s;
+  }
+}
+
+// Sum per-block partials of each replica in block order (deterministic).
+__global__ void k_reduce_partials(const double *__restrict__ partials, int width,
+                                  const int *__restrict__ blk_start, int n_rep,
+                                  double *__restrict__ out) {
+  int const r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rep)
+    return;
+  for (int k = 0; k < width; ++k) {
+    double s = 0.0;
+    for (int b = blk_start[r]; b < blk_start[r + 1]; ++b)
+      s += partials[static_cast<long long>(b) * width + k];
+    out[static_cast<long long>(r) * width + k] = s;
+  }
+}
+
+// Closed-form aliasing sum sum_m sinc^(2P)(n/M + m) (Hockney & Eastwood
+// eq. 7-66, p3m/math.hpp:92-149).
+__device__ inline double cot_sum(int cao, int n, double mesh_i) {
+  double const th = static_cast<double>(n) * mesh_i * kPi;
+  double const c = cos(th) * cos(th);
+  switch (cao) {
+  case 1: return 1.0;
+  case 2: return (1. + c * 2.) / 3.;
+  case 3: return (2. + c * (11. + c * 2.)) / 15.;
+  case 4: return (17. + c * (180. + c * (114. + c * 4.))) / 315.;
+  case 5: return (62. + c * (1072. + c * (1452. + c * (247. + c * 2.)))) / 2835.;
+  case 6:
+    return (1382. + c * (35396. + c * (83021. + c * (34096. + c * (2026. + c * 4.))))) / 155925.;
+  default:
+    return (21844. + c * (776661. + c * (2801040. + c * (2123860. + c * (349500. + c * (8166. + c * 4.)))))) /
+           6081075.;
+  }
+}
+
+// Hockney-Eastwood k-space error sum in FP64 (p3m_k_space_error with
+// p3m_tune_aliasing_sums, p3m.cpp:146-243; the GPU version of
+// p3m_gpu_error_cuda.cu:47-143), per-block partials, fixed-order reduce.
+__global__ void k_ks_error(int M0, int M1, int M2, int cao, double alpha_L,
+                           double *__restrict__ partials) {
+  long long const total = static_cast<long long>(M0) * M1 * M2;
+  double const mi0 = 1.0 / M0, mi1 = 1.0 / M1, mi2 = 1.0 / M2;
+  double const f1 = (kPi / alpha_L) * (kPi / alpha_L);
+  double acc = 0.0;
+  for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int const nz = static_cast<int>(t % M2) - M2 / 2;
+    int const ny = static_cast<int>((t / M2) % M1) - M1 / 2;
+    int const nx = static_cast<int>(t / (static_cast<long long>(M1) * M2)) - M0 / 2;
+    if (nx == 0 && ny == 0 && nz == 0)
+      continue;
+    double const n2 = double(nx) * nx + double(ny) * ny + double(nz) * nz;
+    double const cs = cot_sum(cao, nx, mi0) * cot_sum(cao, ny, mi1) * cot_sum(cao, nz, mi2);
+    double const ex = exp(-f1 * n2);
+    double const en = pow(sinc_d(nx * mi0) * sinc_d(ny * mi1) * sinc_d(nz * mi2), 2.0 * cao);
+    double const a1 = ex * ex / n2;
+    double const a2 = en * ex * n2 / n2;
+    double const d = a1 - (a2 / cs) * (a2 / cs) / n2;
+    if (d > 0.0 && fabs(d / a1) > 1e-14)
+      acc += d;
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1)
+    acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0)
+    red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w)
+      s += red[w];
+    partials[blockIdx.x] = s;
+  }
+}
+
+} // namespace p3mx

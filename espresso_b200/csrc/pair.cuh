@@ -1,0 +1,320 @@
+// Short-range path (sm_100a): regular-decomposition cell binning, Verlet
+// list build, and the real-space erfc-Coulomb + LJ/WCA pair kernel.
+#pragma once
+
+#include "common.cuh"
+#include "p3m_kernels.cuh"
+
+namespace p3mx {
+
+// LJ/WCA parameters of a type pair, device copy (lj.hpp, wca.hpp).
+struct PairIA {
+  double lj_eps, lj_sig, lj_cut, lj_shift, lj_offset, lj_min;
+  double wca_eps, wca_sig, wca_cut;
+  double ia_cut; // max of active cutoffs, -1 when inactive
+};
+
+// Cell of a folded position, position_to_cell_index
+// (RegularDecomposition.cpp:51-80) on a single rank: floor(x/cell)+1,
+// clamped to the grid for x < L.  Returns interior coordinates 0..cg-1.
+__device__ inline void cell_coords(RepGeom const &G, const double *xf, int *c) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int cp = static_cast<int>(floor(xf[d] * G.inv_cs[d])) + 1;
+    if (cp < 1)
+      cp = 1;
+    else if (cp > G.cg[d])
+      cp = G.cg[d];
+    c[d] = cp - 1;
+  }
+}
+
+// Cell key (column-major over the interior grid, x fastest, as the
+// reference orders cells) and counting-sort slot of every particle; also
+// the folded position (double4 with charge in w) for the pair kernels.
+__global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                           const double *__restrict__ pos, const double *__restrict__ q,
+                           long long n, int *__restrict__ key, int *__restrict__ slot,
+                           int *__restrict__ cnt, double4 *__restrict__ pq,
+                           int *__restrict__ ghost_index, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  RepGeom const &G = reps[rep_of[i]];
+  double xf[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    xf[d] = fold_coord(pos[3 * i + d], G.box[d]);
+  int c[3];
+  cell_coords(G, xf, c);
+  int const k = static_cast<int>(G.cell_off) + c[0] + G.cg[0] * (c[1] + G.cg[1] * c[2]);
+  key[i] = k;
+  slot[i] = atomicAdd(&cnt[k], 1);
+  pq[i] = make_double4(xf[0], xf[1], xf[2], q[i]);
+  if (ghost_index) {
+    int const g0 = G.cg[0] + 2, g1 = G.cg[1] + 2;
+    ghost_index[i] = (c[0] + 1) + g0 * ((c[1] + 1) + g1 * (c[2] + 1));
+  }
+}
+
+// Gather particle data into cell-sorted order.
+__global__ void k_cell_gather(const int *__restrict__ perm, const double4 *__restrict__ pq,
+                              const int *__restrict__ type, const int *__restrict__ key,
+                              long long n, double4 *__restrict__ spq, int *__restrict__ stype,
+                              int *__restrict__ scell, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  int const i = perm[s];
+  spq[s] = pq[i];
+  stype[s] = type ? type[i] : 0;
+  scell[s] = key[i];
+}
+
+__device__ inline double mi_d(double dx, double L, double Li) {
+  // get_mi_coord (BoxGeometry.hpp:47-60)
+  if (fabs(dx) > 0.5 * L)
+    return dx - rint(dx * Li) * L;
+  return dx;
+}
+
+// Verlet list (full, both directions) of every cell-sorted particle a:
+// partners b != a in the 27 (unique) neighbour cells with the
+// VerletCriterion (VerletCriterion.hpp:68-97): d^2 <= (max_cut+skin)^2 and
+// (both charged and d^2 <= (r_cut+skin)^2, or the type pair is active and
+// d^2 <= (ia_cut+skin)^2).  Neighbour k of a is stored at nb[k*n + a].
+__global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
+                               const double4 *__restrict__ spq, const int *__restrict__ stype,
+                               const int *__restrict__ scell, const int *__restrict__ cstart,
+                               const PairIA *__restrict__ ia, int ntypes, long long n,
+                               int max_nb, int *__restrict__ nb, int *__restrict__ nb_cnt,
+                               int *__restrict__ overflow, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (a >= n)
+    return;
+  RepGeom const &G = reps[rep_of_sorted[a]];
+  double4 const pa = spq[a];
+  int const ta = stype[a];
+  int const loc = scell[a] - static_cast<int>(G.cell_off);
+  int const c0 = loc % G.cg[0];
+  int const c1 = (loc / G.cg[0]) % G.cg[1];
+  int const c2 = loc / (G.cg[0] * G.cg[1]);
+  double const emax2 = (G.max_cut + G.skin) * (G.max_cut + G.skin);
+  double const ecoul2 = (G.coulomb_cut > 0.0) ? (G.coulomb_cut + G.skin) * (G.coulomb_cut + G.skin) : -1.0;
+  double const Li[3] = {G.box_i[0], G.box_i[1], G.box_i[2]};
+  int count = 0;
+  // offsets per axis without duplicates for grids of size 1 or 2
+  int lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = (G.cg[d] >= 3) ? -1 : 0;
+    hi[d] = (G.cg[d] >= 2) ? 1 : 0;
+  }
+  for (int dz = lo[2]; dz <= hi[2]; ++dz) {
+    int z = c2 + dz;
+    z = (z < 0) ? z + G.cg[2] : (z >= G.cg[2] ? z - G.cg[2] : z);
+    for (int dy = lo[1]; dy <= hi[1]; ++dy) {
+      int y = c1 + dy;
+      y = (y < 0) ? y + G.cg[1] : (y >= G.cg[1] ? y - G.cg[1] : y);
+      for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+        int x = c0 + dx;
+        x = (x < 0) ? x + G.cg[0] : (x >= G.cg[0] ? x - G.cg[0] : x);
+        int const cell = static_cast<int>(G.cell_off) + x + G.cg[0] * (y + G.cg[1] * z);
+        for (int b = cstart[cell]; b < cstart[cell + 1]; ++b) {
+          if (b == a)
+            continue;
+          double4 const pb = spq[b];
+          double const d0 = mi_d(pa.x - pb.x, G.box[0], Li[0]);
+          double const d1 = mi_d(pa.y - pb.y, G.box[1], Li[1]);
+          double const d2v = mi_d(pa.z - pb.z, G.box[2], Li[2]);
+          double const d2 = d0 * d0 + d1 * d1 + d2v * d2v;
+          if (d2 > emax2)
+            continue;
+          bool take = (ecoul2 >= 0.0 && d2 <= ecoul2 && pa.w != 0.0 && pb.w != 0.0);
+          if (!take) {
+            double const ic = ia[ta * ntypes + stype[b]].ia_cut;
+            take = (ic != -1.0) && d2 <= (ic + G.skin) * (ic + G.skin);
+          }
+          if (take) {
+            if (count < max_nb)
+              nb[static_cast<long long>(count) * n + a] = b;
+            ++count;
+          }
+        }
+      }
+    }
+  }
+  nb_cnt[a] = min(count, max_nb);
+  if (count > max_nb)
+    atomicMax(overflow, count);
+}
+
+// A&S 7.1.26 approximation of exp(d^2) erfc(d), as the reference's real-
+// space kernel uses it (utils/math/AS_erfc_part.hpp:29-40).
+template <typename Real> __device__ inline Real as_erfc_part(Real d) {
+  Real const a1 = Real(0.254829592), a2 = Real(-0.284496736), a3 = Real(1.421413741),
+             a4 = Real(-1.453152027), a5 = Real(1.061405429), p = Real(0.3275911);
+  Real const t = Real(1) / (Real(1) + p * d);
+  return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5))));
+}
+
+template <typename Real> __device__ inline Real exp_r(Real x);
+template <> __device__ inline float exp_r<float>(float x) { return expf(x); }
+template <> __device__ inline double exp_r<double>(double x) { return exp(x); }
+template <typename Real> __device__ inline Real sqrt_r(Real x);
+template <> __device__ inline float sqrt_r<float>(float x) { return sqrtf(x); }
+template <> __device__ inline double sqrt_r<double>(double x) { return sqrt(x); }
+
+// Pair kernel over the Verlet list: real-space Coulomb
+// (CoulombP3M::pair_force / pair_energy, p3m.hpp:146-180) plus LJ and WCA
+// (lj.hpp:41-60, wca.hpp:39-55), minimum-image distance in FP64, pair
+// arithmetic in Real, per-particle accumulation in Real (no atomics: each
+// particle owns its force).  Energies/virials: each pair is seen from both
+// ends, so per-particle sums are halved; per-block FP64 partials
+// {E_coul, E_nb, Vc[9], Vn[9]} (width 20).
+template <typename Real>
+__global__ void __launch_bounds__(256)
+k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+              const double4 *__restrict__ spq, const int *__restrict__ stype,
+              const int *__restrict__ perm, const PairIA *__restrict__ ia_g, int ntypes,
+              long long n, const int *__restrict__ nb, const int *__restrict__ nb_cnt,
+              double *__restrict__ f, int overwrite, int want_ev,
+              double *__restrict__ partials) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PairIA *ia = reinterpret_cast<PairIA *>(smem_raw);
+  for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
+    ia[k] = ia_g[k];
+  __syncthreads();
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  double ev[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k)
+    ev[k] = 0.0;
+  if (a < G.p0 + G.np) {
+    double4 const pa = spq[a];
+    int const ta = stype[a];
+    Real const alpha = static_cast<Real>(G.alpha);
+    Real const r_cut = static_cast<Real>(G.r_cut);
+    Real const two_a_sqrt_pi_i = static_cast<Real>(2.0 * G.alpha / sqrt(kPi));
+    Real const pref = static_cast<Real>(G.prefactor);
+    Real fx = Real(0), fy = Real(0), fz = Real(0);
+    int const cnt = nb_cnt[a];
+    for (int k = 0; k < cnt; ++k) {
+      int const b = nb[static_cast<long long>(k) * n + a];
+      double4 const pb = spq[b];
+      Real const d0 = static_cast<Real>(mi_d(pa.x - pb.x, G.box[0], G.box_i[0]));
+      Real const d1 = static_cast<Real>(mi_d(pa.y - pb.y, G.box[1], G.box_i[1]));
+      Real const d2v = static_cast<Real>(mi_d(pa.z - pb.z, G.box[2], G.box_i[2]));
+      Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
+      Real const dist = sqrt_r(dist2);
+      Real fc = Real(0), ec = Real(0);
+      Real const q1q2 = static_cast<Real>(pa.w * pb.w);
+      if (q1q2 != Real(0) && dist < r_cut && dist > Real(0)) {
+        Real const adist = alpha * dist;
+        Real const ex = exp_r(-adist * adist);
+        Real const erfc_part_ri = as_erfc_part(adist) / dist;
+        fc = pref * q1q2 * (ex * (erfc_part_ri + two_a_sqrt_pi_i) / dist2);
+        ec = pref * q1q2 * erfc_part_ri * ex;
+      }
+      Real fn = Real(0), en = Real(0);
+      PairIA const &p = ia[ta * ntypes + stype[b]];
+      if (p.ia_cut != -1.0) {
+        Real const lcut = static_cast<Real>(p.lj_cut + p.lj_offset);
+        Real const lmin = static_cast<Real>(p.lj_min + p.lj_offset);
+        if (dist < lcut && dist > lmin) {
+          Real const r_off = dist - static_cast<Real>(p.lj_offset);
+          Real const s = static_cast<Real>(p.lj_sig) / r_off;
+          Real const s2 = s * s;
+          Real const f6 = s2 * s2 * s2;
+          Real const eps = static_cast<Real>(p.lj_eps);
+          fn += Real(48) * eps * f6 * (f6 - Real(0.5)) / (r_off * dist);
+          en += Real(4) * eps * (f6 * f6 - f6 + static_cast<Real>(p.lj_shift));
+        }
+        if (dist < static_cast<Real>(p.wca_cut)) {
+          Real const s = static_cast<Real>(p.wca_sig) / dist;
+          Real const s2 = s * s;
+          Real const f6 = s2 * s2 * s2;
+          Real const eps = static_cast<Real>(p.wca_eps);
+          fn += Real(48) * eps * f6 * (f6 - Real(0.5)) / dist2;
+          en += Real(4) * eps * (f6 * f6 - f6 + Real(0.25));
+        }
+      }
+      Real const ft = fc + fn;
+      fx += ft * d0;
+      fy += ft * d1;
+      fz += ft * d2v;
+      if (want_ev) {
+        double const dd[3] = {double(d0), double(d1), double(d2v)};
+        ev[0] += 0.5 * double(ec);
+        ev[1] += 0.5 * double(en);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
+            ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
+          }
+      }
+    }
+    int const i = perm[a];
+    if (overwrite) {
+      f[3 * i + 0] = double(fx);
+      f[3 * i + 1] = double(fy);
+      f[3 * i + 2] = double(fz);
+    } else {
+      f[3 * i + 0] += double(fx);
+      f[3 * i + 1] += double(fy);
+      f[3 * i + 2] += double(fz);
+    }
+  }
+  if (want_ev) {
+    __shared__ double red[20][8];
+    int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 20; ++k) {
+      double v = ev[k];
+      for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0)
+        red[k][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 20) {
+      double s = 0.0;
+      for (int w = 0; w < (blockDim.x >> 5); ++w)
+        s += red[threadIdx.x][w];
+      partials[static_cast<long long>(blockIdx.x) * 20 + threadIdx.x] = s;
+    }
+  }
+}
+
+// Largest squared displacement since the last list build, as a flag:
+// set when any particle moved more than skin/2 (check_resort_required,
+// CellStructure.hpp:393-401).
+__global__ void k_displacement_check(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                                     const double *__restrict__ pos, const double *__restrict__ pos_ref,
+                                     long long n, int *__restrict__ flag) {
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  RepGeom const &G = reps[rep_of[i]];
+  double d2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double const dx = pos[3 * i + d] - pos_ref[3 * i + d];
+    d2 += dx * dx;
+  }
+  double const lim = 0.5 * G.skin;
+  if (d2 > lim * lim)
+    atomicOr(flag, 1);
+}
+
+} // namespace p3mx

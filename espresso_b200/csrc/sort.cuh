@@ -1,0 +1,174 @@
+// Exclusive scan and deterministic counting sort (device primitives).
+//
+// The counting sort orders items by an integer key (mesh-corner bin or link
+// cell) and then restores, inside every key bucket, ascending item order, so
+// the permutation is a pure function of the keys: the same input gives the
+// same bitwise output on every run, whatever the atomic order was.
+#pragma once
+
+#include "common.cuh"
+
+namespace p3mx {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ inline int warp_incl_scan(int v) {
+  unsigned const lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int const t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= static_cast<unsigned>(o))
+      v += t;
+  }
+  return v;
+}
+
+// Block-wide exclusive scan of one int per thread; returns the block total.
+__device__ inline int block_excl_scan(int v, int &total) {
+  __shared__ int warp_sums[32];
+  int const incl = warp_incl_scan(v);
+  int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 31)
+    warp_sums[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int const nw = (blockDim.x + 31) >> 5;
+    int s = (lane < nw) ? warp_sums[lane] : 0;
+    s = warp_incl_scan(s);
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  int const warp_off = (wid > 0) ? warp_sums[wid - 1] : 0;
+  total = warp_sums[((blockDim.x + 31) >> 5) - 1];
+  __syncthreads();
+  return warp_off + incl - v;
+}
+
+// Pass 1: tile-local exclusive scan, tile totals to tile_sums.
+__global__ void k_scan_tiles(const int *__restrict__ in, int *__restrict__ out,
+                             int *__restrict__ tile_sums, long long n,
+                             const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const base = static_cast<long long>(blockIdx.x) * kScanTile +
+                         static_cast<long long>(threadIdx.x) * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  int total;
+  int run = block_excl_scan(s, total);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n)
+      out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0)
+    tile_sums[blockIdx.x] = total;
+}
+
+// Pass 2: exclusive scan of the tile totals by one block; writes the grand
+// total to out[n].
+__global__ void k_scan_tile_sums(int *__restrict__ tile_sums, int ntiles,
+                                 int *__restrict__ out, long long n,
+                                 const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  int const per = (ntiles + blockDim.x - 1) / blockDim.x;
+  int const b0 = threadIdx.x * per;
+  int s = 0;
+  for (int k = 0; k < per; ++k)
+    if (b0 + k < ntiles)
+      s += tile_sums[b0 + k];
+  int total;
+  int run = block_excl_scan(s, total);
+  for (int k = 0; k < per; ++k) {
+    if (b0 + k < ntiles) {
+      int const t = tile_sums[b0 + k];
+      tile_sums[b0 + k] = run;
+      run += t;
+    }
+  }
+  if (threadIdx.x == 0)
+    out[n] = total;
+}
+
+// Pass 3: add tile offsets.
+__global__ void k_scan_add(int *__restrict__ out, const int *__restrict__ tile_sums,
+                           long long n, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n)
+    out[i] += tile_sums[i / kScanTile];
+}
+
+// Place every item at start[key] + slot (slot from the counting atomics).
+__global__ void k_place(const int *__restrict__ key, const int *__restrict__ slot,
+                        const int *__restrict__ start, int *__restrict__ perm,
+                        long long n, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n)
+    perm[start[key[i]] + slot[i]] = static_cast<int>(i);
+}
+
+// Restore ascending item order inside each bucket (buckets are short:
+// insertion sort), making the permutation independent of atomic order.
+__global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ perm,
+                              long long nbuckets, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const b = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= nbuckets)
+    return;
+  int const s0 = start[b], s1 = start[b + 1];
+  if (s1 - s0 < 2)
+    return;
+  for (int i = s0 + 1; i < s1; ++i) {
+    int const v = perm[i];
+    int j = i - 1;
+    while (j >= s0 && perm[j] > v) {
+      perm[j + 1] = perm[j];
+      --j;
+    }
+    perm[j + 1] = v;
+  }
+}
+
+// Host driver of the three-pass exclusive scan (out has n+1 entries).
+// `cond` (device int, may be NULL) skips the whole scan when zero, so the
+// scan can sit inside a captured CUDA graph behind a device-side decision.
+inline void exclusive_scan(const int *in, int *out, int *tile_buf, long long n,
+                           cudaStream_t st, const int *cond = nullptr) {
+  int const ntiles = ceil_div(n, kScanTile);
+  k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(in, out, tile_buf, n, cond);
+  k_scan_tile_sums<<<1, 1024, 0, st>>>(tile_buf, ntiles, out, n, cond);
+  k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, tile_buf, n, cond);
+}
+
+// Conditional fill / copy helpers for graph-captured paths.
+__global__ void k_fill_int(int *__restrict__ p, int v, long long n, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+__global__ void k_copy_f64(double *__restrict__ dst, const double *__restrict__ src, long long n,
+                           const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
+} // namespace p3mx

@@ -1,0 +1,212 @@
+/*
+ * p3mx -- B200-native P3M electrostatics + short-range pair engine.
+ *
+ * C ABI of the drop-in boundary.  Every entry point returns 0 on success or
+ * a non-zero P3MX_E* status; the message of the last failure is available
+ * from p3mx_last_error().  Nothing here throws or calls exit() (the
+ * reference exits the process on CUDA errors, src/core/cuda/utils.cuh:64-80).
+ *
+ * Pointers: positions/charges/forces are plain FP64 arrays in AoS layout
+ * (x0 y0 z0 x1 ...), as ESPResSo's Particle::pos()/force() hold them.  With
+ * P3MX_DEVICE_PTRS in `flags` they are device pointers already resident in
+ * HBM; otherwise they are host pointers and the call copies them in and out
+ * (the GpuParticleData gather/scatter of system/GpuParticleData.cpp:85-184).
+ * `stream` is a cudaStream_t (NULL = the handle's own stream).
+ */
+#ifndef P3MX_H
+#define P3MX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P3MX_OK 0
+#define P3MX_EDOMAIN 1    /* parameter outside its domain (std::domain_error) */
+#define P3MX_ERUNTIME 2   /* state error (std::runtime_error in the reference) */
+#define P3MX_ECUDA 3      /* CUDA runtime error */
+#define P3MX_ENOMEM 4     /* device allocation failed */
+#define P3MX_EHANDLE 5    /* NULL or destroyed handle */
+
+#define P3MX_DEVICE_PTRS 1u   /* pos/q/f/type are device pointers */
+#define P3MX_FORCES 2u        /* compute forces (added to f) */
+#define P3MX_ENERGY 4u        /* compute energy */
+#define P3MX_VIRIAL 8u        /* compute the 3x3 virial / pressure tensor */
+#define P3MX_OVERWRITE 16u    /* f is overwritten instead of accumulated */
+
+typedef struct p3mx_handle p3mx_handle;
+
+/* Actor parameters: the kwargs of espressomd.electrostatics.P3M / P3MGPU
+ * (src/python/espressomd/electrostatics.py:129-284) and the
+ * P3MParameters constructor (src/core/p3m/common.hpp:59-150).  -1 marks a
+ * value left to the tuner. */
+typedef struct {
+  double prefactor;
+  double accuracy;
+  int mesh[3];
+  int cao;
+  double r_cut;
+  double alpha;
+  double epsilon;       /* 0 = metallic */
+  double mesh_off[3];   /* -1 = P3M_MESHOFF (0.5) */
+  int tune;             /* bool */
+  int timings;          /* force evaluations timed per tuning trial */
+  int verbose;          /* print the tuning log */
+  int single_precision; /* 1 = FP32-mixed mesh/FFT path, 0 = plain FP64 */
+  int check_neutrality;
+  double charge_neutrality_tolerance; /* reference default 2e-12 */
+} p3mx_params;
+
+/* Geometry and cell-system settings (BoxGeometry + CellStructure skin). */
+typedef struct {
+  double box[3];
+  double skin;
+  int periodic[3];
+} p3mx_system;
+
+/* Read-only parameter view: the getters of CoulombP3M<Arch>
+ * (src/script_interface/electrostatics/CoulombP3M.hpp:67-99). */
+typedef struct {
+  int mesh[3];
+  int cao;
+  double r_cut, alpha, r_cut_iL, alpha_L, accuracy, epsilon;
+  double mesh_off[3];
+  double a[3];
+  int is_tuned;
+  int single_precision;
+  double rs_error, ks_error;
+} p3mx_tuned;
+
+/* LJ and WCA parameters of one type pair
+ * (src/core/nonbonded_interactions/lj.cpp:33-46, wca.cpp:31-42). */
+typedef struct {
+  double lj_eps, lj_sig, lj_cut, lj_shift, lj_offset, lj_min;
+  double wca_eps, wca_sig;
+} p3mx_pair_params;
+
+/* --- actor life cycle ------------------------------------------------- */
+
+/* Validates and stores the parameters; replaces the constructor path
+ * CoulombP3M<Arch>::do_construct + new_p3m_handle
+ * (script_interface/electrostatics/CoulombP3M.hpp:102-142,
+ *  core/electrostatics/p3m.impl.hpp:390-401). */
+int p3mx_create(const p3mx_params *params, p3mx_handle **out);
+void p3mx_destroy(p3mx_handle *h);
+const char *p3mx_last_error(const p3mx_handle *h);
+/* Version and build string ("p3mx <ver> sm_100a ..."). */
+const char *p3mx_version(void);
+
+/* Box / skin change: CoulombP3M::on_boxl_change -> scaleby_box_l
+ * (electrostatics/p3m.cpp:856-865) and the cell-system rebuild. */
+int p3mx_set_system(p3mx_handle *h, const p3mx_system *sys);
+
+/* Activation: sanity checks + charge counting + (optional) tuning + init,
+ * CoulombP3MImpl::on_activation / tune / init
+ * (p3m.impl.hpp:328-343, p3m.cpp:758-791, p3m.cpp:246-280 and
+ *  p3m_gpu_init, p3m_gpu_cuda.cu:549-667).  Positions/charges are needed
+ * for the charge count and the timed tuning trials. */
+int p3mx_activate(p3mx_handle *h, size_t n, const double *pos,
+                  const double *q, unsigned flags);
+int p3mx_get_tuned(const p3mx_handle *h, p3mx_tuned *out);
+
+/* --- force / energy / pressure ---------------------------------------- */
+
+/* k-space part: replaces CoulombP3MImpl::add_long_range_forces,
+ * long_range_energy and long_range_pressure (p3m.impl.hpp:345-358,
+ * p3m.cpp:394-592) and the GPU entry p3m_gpu_add_farfield_force
+ * (p3m_gpu_cuda.cuh:31-35).  energy: 1 double; virial9: 3x3 k-space
+ * pressure tensor times volume (as long_range_pressure returns it). */
+int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos,
+                    const double *q, double *f, double *energy,
+                    double *virial9, unsigned flags, void *stream);
+
+/* Short-range part over the cell system: real-space Coulomb
+ * (CoulombP3M::pair_force / pair_energy, electrostatics/p3m.hpp:146-180)
+ * plus LJ/WCA (lj.hpp:41-60, wca.hpp:39-55) through the Verlet list
+ * (CellStructure::verlet_list_loop, CellStructure.hpp:612-646).
+ * energy2 = {coulomb real space, non-bonded}; virial18 = two 3x3 tensors
+ * (coulomb, non-bonded), each sum over pairs of F (x) d. */
+int p3mx_set_pair_params(p3mx_handle *h, int ntypes,
+                         const p3mx_pair_params *table);
+int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos,
+                     const double *q, const int *type, double *f,
+                     double *energy2, double *virial18, unsigned flags,
+                     void *stream);
+
+/* Full force evaluation in one call: one upload of pos/q/type, the
+ * k-space and short-range pipelines, one download of the forces --
+ * System::calculate_forces for the non-bonded + electrostatic part
+ * (forces.cpp:121-249 with gpu.update / copy_forces_to_host at :129, :225).
+ * energy3 = {coulomb real, coulomb k-space, non-bonded};
+ * virial27 = {coulomb real, coulomb k-space, non-bonded} 3x3 each. */
+int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q,
+                const int *type, double *f, double *energy3, double *virial27,
+                unsigned flags, void *stream);
+
+/* Cell-system introspection for parity tests: the cell grid and the cell
+ * index of each particle as RegularDecomposition::position_to_cell_index
+ * returns it (RegularDecomposition.cpp:51-80, 289-385), and the Verlet pair
+ * set as non_bonded_loop_trace reports it (core/cells.cpp:178-188). */
+int p3mx_cell_grid(p3mx_handle *h, int *cell_grid, double *cell_size);
+int p3mx_cell_index(p3mx_handle *h, size_t n, const double *pos, int *cell);
+/* Writes up to `cap` pairs (i<j) into pairs (2*cap ints); *count gets the
+ * total pair count (may exceed cap). */
+int p3mx_verlet_pairs(p3mx_handle *h, size_t n, const double *pos,
+                      const double *q, const int *type, int *pairs,
+                      size_t cap, size_t *count);
+
+/* Charge-assignment mesh of the last long-range call (M0*M1*M2, FP64 copy
+ * of the device mesh) for element-wise parity checks. */
+int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap);
+
+/* Tuning error estimates (p3m.cpp:187-243; GPU k-space sum of
+ * p3m_gpu_error_cuda.cu:87-143). */
+int p3mx_error_estimate(const int *mesh, int cao, int n_c_part,
+                        double sum_q2, double alpha_L, double r_cut_iL,
+                        const double *box, double prefactor, double *rs_err,
+                        double *ks_err);
+
+/* --- batched replicas -------------------------------------------------- */
+
+/* Many independent cubic or orthorhombic systems advanced by one launch
+ * per kernel (the reference has no batched path; each replica otherwise is
+ * one ESPResSo System).  Per-replica arrays have n_rep entries; particles
+ * of replica r occupy [offset[r], offset[r+1]) of the global arrays. */
+typedef struct {
+  int n_rep;
+  const double *box;       /* 3*n_rep */
+  const double *prefactor; /* n_rep (Bjerrum length * kT) */
+  const long long *offset; /* n_rep+1 */
+  double accuracy;         /* common target accuracy */
+  double skin;
+  int single_precision;
+  int mesh_min, mesh_max;  /* autotuner mesh range (per dimension) */
+  int cao_min, cao_max;
+} p3mx_batch_desc;
+
+typedef struct p3mx_batch p3mx_batch;
+
+/* Creates the batch, uploads positions/charges/types, tunes every replica
+ * (mesh, cao, r_cut, alpha by the error estimate plus timed trials). */
+int p3mx_batch_create(const p3mx_batch_desc *d, const double *pos,
+                      const double *q, const int *type, int ntypes,
+                      const p3mx_pair_params *table, p3mx_batch **out);
+void p3mx_batch_destroy(p3mx_batch *b);
+const char *p3mx_batch_last_error(const p3mx_batch *b);
+/* Tuned parameters of replica r. */
+int p3mx_batch_get_tuned(const p3mx_batch *b, int r, p3mx_tuned *out);
+/* One force evaluation for all replicas (forces overwritten, device
+ * resident); optional per-replica energies (n_rep doubles, host). */
+int p3mx_batch_forces(p3mx_batch *b, double *energy_out);
+/* Velocity-Verlet + Langevin (kT, gamma, dt) for `steps` steps, captured
+ * in a CUDA graph after the first step.  Positions stay FP64 on device. */
+int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT,
+                   double gamma, unsigned long long seed);
+/* Copy positions / forces (3*N doubles, host) of all replicas. */
+int p3mx_batch_get(p3mx_batch *b, double *pos, double *f, double *vel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,277 @@
+"""GPU parity tests of the P3M + short-range path through the C ABI.
+
+Structure follows the reference tests (testsuite/python/coulomb_cloud_wall.py,
+electrostatic_interactions.py, p3m_madelung.py, coulomb_tuning.py, lj.py):
+the same systems and tolerances against the golden fixtures, plus tighter
+element-wise comparisons with the FP64 oracle.  Tolerances: the plain FP64
+GPU path must agree with the oracle to 1e-9 (relative to the force scale);
+the FP32-mixed path to 2e-5 relative (FP32 mesh/FFT arithmetic).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import espresso_b200 as eb
+from espresso_b200 import _lib
+from espresso_b200.electrostatics import P3M, P3MGPU
+from oracle import oracle as O
+from tests.golden_systems import jittered_lattice, known, load, madelung_system
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-9
+FP32_RTOL = 2e-5
+
+
+def make_system(box, pos, q, skin=0.4):
+    s = eb.System(box_l=box)
+    s.time_step = 0.01
+    s.cell_system.skin = skin
+    s.part.add(pos=pos, q=q)
+    return s
+
+
+def oracle_total(box, pos, q, mesh, cao, alpha, r_cut, pref, epsilon=0.0):
+    p = O.make_params(box, mesh, cao, alpha, r_cut, pref, epsilon=epsilon)
+    fk, ek, vk = O.p3m_kspace(p, pos, q)
+    fr, er, vc, _ = O.short_range(p, pos, q)
+    return fk + fr, ek + er[0], vk + vc
+
+
+@pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
+def test_cloud_wall(cls, rtol):
+    g = load("coulomb_cloud_wall.npz")
+    pref = 3.0 if cls is P3M else 2.2
+    s = make_system(g["box"], g["pos"], g["q"])
+    s.electrostatics.solver = cls(prefactor=pref, accuracy=float(g["accuracy"]),
+                                  mesh=[int(m) for m in g["mesh"]], cao=int(g["cao"]),
+                                  alpha=float(g["alpha"]), r_cut=float(g["r_cut"]), tune=False)
+    s.integrator.run(0)
+    f = s.part.all().f
+    e = s.analysis.energy()["total"]
+    # reference test tolerances against the stored data
+    np.testing.assert_allclose(f / pref, g["forces"], atol=float(g["force_atol"]))
+    assert abs(e / pref - float(g["energy"])) < float(g["energy_atol"])
+    # element-wise against the oracle
+    fo, eo, _ = oracle_total(g["box"], g["pos"], g["q"], g["mesh"], int(g["cao"]),
+                             float(g["alpha"]), float(g["r_cut"]), pref)
+    scale = np.abs(fo).max()
+    np.testing.assert_allclose(f, fo, atol=rtol * scale, rtol=0)
+    assert abs(e - eo) <= rtol * abs(eo) + 1e-12
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_two_charges_metallic_and_dipole(cls):
+    ka = known()["two_charges"]
+    pref = ka["prefactor"]
+    pos, q = np.array(ka["pos"]), np.array(ka["q"])
+    s = make_system(ka["box"], pos, q)
+    kw = dict(prefactor=pref, accuracy=ka["accuracy"], mesh=[ka["mesh"]] * 3, cao=ka["cao"],
+              r_cut=ka["r_cut"], alpha=ka["alpha"], tune=False)
+    s.electrostatics.solver = cls(epsilon="metallic", **kw)
+    s.integrator.run(0)
+    e_met = s.analysis.energy()["coulomb"]
+    f_met = s.part.all().f
+    assert abs(e_met - ka["energy_per_prefactor"] * pref) < ka["tol"]
+    np.testing.assert_allclose(f_met[0], [ka["force_x_per_prefactor"] * pref, 0, 0], atol=ka["tol"])
+    np.testing.assert_allclose(f_met[1], [-ka["force_x_per_prefactor"] * pref, 0, 0], atol=ka["tol"])
+    if cls is P3MGPU:
+        return
+    V = ka["box"] ** 3
+    dip = q @ pos
+    for eps in 10.0 ** np.arange(-4, 5):
+        s.electrostatics.clear()
+        s.electrostatics.solver = cls(epsilon=float(eps), **kw)
+        s.integrator.run(0)
+        corr = 4 * np.pi / V / (1 + 2 * eps)
+        e = s.analysis.energy()["coulomb"]
+        np.testing.assert_allclose(e, e_met + pref * corr * dip @ dip, atol=ka["dipole_tol"])
+        np.testing.assert_allclose(s.part.all().f, f_met - pref * np.outer(q, corr * dip),
+                                   atol=ka["dipole_tol"])
+
+
+@pytest.mark.parametrize("kind", ["wire", "sheet", "cube"])
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_madelung(kind, cls):
+    box, pos, q, ka = madelung_system(kind)
+    params = dict(mesh=ka["mesh"], cao=ka["cao"], r_cut=ka["r_cut"], alpha=ka["alpha"],
+                  accuracy=ka["accuracy"])
+    if kind == "cube" and cls is P3MGPU:
+        params = dict(ka["gpu_params"])
+    s = make_system(box, pos, q)
+    s.electrostatics.solver = cls(prefactor=1.0, tune=False, **params)
+    n = len(q)
+    V = float(np.prod(box))
+    energy = 2.0 * s.analysis.energy()["coulomb"] / n
+    p_tensor = 2.0 * s.analysis.pressure_tensor()["coulomb"] * V / n
+    p_scalar = 2.0 * s.analysis.pressure()["coulomb"] * V / n
+    base = np.array(ka["base"], float)
+    ref_p = ka["madelung"] * np.diag(base) / base.sum()
+    np.testing.assert_allclose(energy, ka["madelung"], atol=0, rtol=ka["energy_rtol"])
+    np.testing.assert_allclose(p_scalar, np.trace(ref_p) / 3.0, atol=1e-12, rtol=ka["pressure_rtol"])
+    np.testing.assert_allclose(p_tensor, ref_p, atol=5e-9, rtol=ka["pressure_rtol"])
+
+
+def _handle_compute(cls, box, pos, q, mesh, cao, alpha, r_cut, pref=1.0):
+    act = cls(prefactor=pref, accuracy=1e-4, mesh=mesh, cao=cao, alpha=alpha, r_cut=r_cut,
+              tune=False, check_neutrality=False)
+    act._set_system(np.broadcast_to(box, (3,)), 0.4, (True, True, True))
+    act._activate(pos, q)
+    lib = _lib.load()
+    f = np.zeros((len(q), 3))
+    e = np.zeros(1)
+    v = np.zeros(9)
+    rc = lib.p3mx_long_range(act._handle, len(q), _lib.dptr(_lib.as_f64(pos)),
+                             _lib.dptr(_lib.as_f64(q)), _lib.dptr(f),
+                             e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             _lib.P3MX_FORCES | _lib.P3MX_ENERGY | _lib.P3MX_VIRIAL |
+                             _lib.P3MX_OVERWRITE, None)
+    _lib.check(rc, act._handle)
+    mesh_out = np.zeros(int(np.prod(np.broadcast_to(mesh, (3,)))))
+    _lib.check(lib.p3mx_copy_mesh(act._handle, mesh_out.ctypes.data_as(
+        ctypes.POINTER(ctypes.c_double)), mesh_out.size), act._handle)
+    return act, f, e[0], v.reshape(3, 3), mesh_out
+
+
+@pytest.mark.parametrize("cao", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
+def test_kspace_elementwise_vs_oracle(cao, cls, rtol):
+    """Charge mesh, k-space forces, energy and virial vs the FP64 oracle on a
+    ragged non-cubic mesh (16 x 22 x 18; 22 and 18 exercise radix 11 and 3)."""
+    box = np.array([10.0, 12.0, 11.0])
+    rng = np.random.default_rng(cao)
+    n = 333
+    pos = rng.uniform(-1.0, 1.0, (n, 3)) * box + box / 2  # some outside the box
+    q = rng.choice([-1.0, 1.0, 2.0, -2.0, 0.0], n)
+    q -= q.mean()
+    mesh = [16, 22, 18]
+    _, f, e, v, mesh_gpu = _handle_compute(cls, box, pos, q, mesh, cao, 1.1, 2.5)
+    p = O.make_params(box, mesh, cao, 1.1, 2.5, 1.0)
+    fo, eo, vo, rho = O.p3m_kspace(p, pos, q, want_mesh=True)
+    np.testing.assert_allclose(mesh_gpu, rho.ravel(), atol=rtol * np.abs(rho).max() * 10, rtol=0)
+    np.testing.assert_allclose(f, fo, atol=rtol * np.abs(fo).max(), rtol=0)
+    assert abs(e - eo) <= rtol * abs(eo) * 10 + 1e-12
+    np.testing.assert_allclose(v, vo, atol=rtol * np.abs(vo).max() * 10, rtol=0)
+
+
+def test_assignment_is_deterministic():
+    box = 20.0
+    pos, q = jittered_lattice(12, box, 0.2, seed=7)
+    act, f1, e1, _, m1 = _handle_compute(P3MGPU, box, pos, q, 32, 7, 1.0, 3.0)
+    lib = _lib.load()
+    for _ in range(2):
+        f2 = np.zeros_like(f1)
+        rc = lib.p3mx_long_range(act._handle, len(q), _lib.dptr(_lib.as_f64(pos)),
+                                 _lib.dptr(_lib.as_f64(q)), _lib.dptr(f2), None, None,
+                                 _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE, None)
+        _lib.check(rc, act._handle)
+        m2 = np.zeros_like(m1)
+        lib.p3mx_copy_mesh(act._handle, m2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), m2.size)
+        assert np.array_equal(m1, m2)
+        assert np.array_equal(f1, f2)
+
+
+def test_lj_system():
+    g = load("lj_system.npz")
+    s = eb.System(box_l=[float(g["box"])] * 3)
+    s.time_step = 0.1
+    s.cell_system.skin = float(g["skin"])
+    s.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0,
+                                                      cutoff=float(g["cut"]), shift="auto")
+    s.part.add(pos=g["pos"])
+    for _ in range(2):  # build the Verlet list, then reuse it
+        s.integrator.run(0, recalc_forces=True)
+        f = s.part.all().f
+        assert np.linalg.norm(f - g["forces"], axis=1).mean() < 1e-7
+        assert np.abs(f - g["forces"]).max() < 1e-5
+
+
+def test_cell_index_bit_exact_and_pair_set():
+    """Cell assignment equals position_to_cell_index; the Verlet pair set
+    equals the oracle's link-cell pair set (check_non_bonded_loop_trace)."""
+    box = 20.0
+    rng = np.random.default_rng(11)
+    n = 3000
+    pos = rng.uniform(0, box, (n, 3))
+    pos[:5] = [[0.0, 0.0, 0.0], [box - 1e-12, 5.0, 5.0], [4.0, 4.0, 4.0], [8.0, 12.0, 16.0],
+               [19.999999999, 0.0, 3.4]]
+    q = rng.choice([-1.0, 1.0], n)
+    s = make_system([box] * 3, pos, q)
+    act = P3M(prefactor=1.0, accuracy=1e-3, mesh=16, cao=3, alpha=1.0, r_cut=3.0, tune=False,
+              check_neutrality=False)
+    s.electrostatics.solver = act
+    lib = _lib.load()
+    cell = np.zeros(n, dtype=np.int32)
+    _lib.check(lib.p3mx_cell_index(act._handle, n, pos.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   cell.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), act._handle)
+    cg = np.zeros(3, dtype=np.int32)
+    cs = np.zeros(3)
+    lib.p3mx_cell_grid(act._handle, cg.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                       cs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    cg_o, cs_o = O.cell_grid(np.array([box] * 3), 3.0 + 0.4)
+    assert list(cg) == list(cg_o)
+    np.testing.assert_array_equal(cell, O.cell_index(np.array([box] * 3), 3.4, pos))
+    cap = 200 * n
+    pairs = np.zeros(2 * cap, dtype=np.int32)
+    cnt = ctypes.c_size_t()
+    _lib.check(lib.p3mx_verlet_pairs(act._handle, n, pos.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None,
+                                     pairs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cap,
+                                     ctypes.byref(cnt)), act._handle)
+    mine = {tuple(p) for p in pairs[:2 * cnt.value].reshape(-1, 2)}
+    ref = {tuple(sorted(p)) for p in O.verlet_pairs([box] * 3, 0.4, 3.0, pos, q)}
+    assert mine == ref
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_tuning(cls):
+    """coulomb_tuning.py: tune to accuracy 5e-4, forces within 2e-3."""
+    g = load("coulomb_tuning.npz")
+    s = make_system(g["box"], g["pos"], g["q"])
+    act = cls(prefactor=1.0, accuracy=float(g["accuracy"]), tune=True, verbose=False)
+    s.electrostatics.solver = act
+    assert act.is_tuned
+    assert act.get_params()["accuracy"] <= float(g["accuracy"])
+    s.integrator.run(0)
+    np.testing.assert_allclose(s.part.all().f, g["forces"], atol=float(g["force_atol"]))
+
+
+def test_error_estimate_matches_oracle():
+    lib = _lib.load()
+    box = np.array([20.0, 20.0, 20.0])
+    for mesh, cao, aL, rcL in [(32, 5, 12.0, 0.15), (22, 7, 7.75, 0.445), (64, 3, 30.0, 0.05)]:
+        m = np.array([mesh] * 3, dtype=np.int32)
+        rs = ctypes.c_double()
+        ks = ctypes.c_double()
+        rc = lib.p3mx_error_estimate(m.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cao, 2000,
+                                     2000.0, aL, rcL, box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     1.0, ctypes.byref(rs), ctypes.byref(ks))
+        assert rc == 0
+        np.testing.assert_allclose(ks.value, O.ks_error(1.0, mesh, cao, 2000, 2000.0, aL, box),
+                                   rtol=1e-12)
+        np.testing.assert_allclose(rs.value, O.rs_error(1.0, rcL, 2000, 2000.0, aL, box), rtol=1e-14)
+
+
+def test_fp32_accuracy_vs_ewald_c1_like():
+    """2000 ions, L=20, mesh 32, cao 5, r_cut 3 at accuracy 1e-4: the
+    FP32-mixed path's rms force error against the FP64 Ewald sum stays at the
+    P3M error level (<= 1e-4 * the tuning estimate margin)."""
+    box = 20.0
+    pos, q = jittered_lattice(10, box, 0.2, seed=1)  # 1000 ions
+    pos2, q2 = jittered_lattice(10, box, 0.2, seed=2)
+    pos = np.vstack([pos, pos2 + 0.5 * box / 10])
+    q = np.concatenate([q, -q2])
+    s = make_system([box] * 3, pos, q)
+    act = P3MGPU(prefactor=1.0, accuracy=1e-4, mesh=32, cao=5, r_cut=3.0, tune=True, verbose=False)
+    s.electrostatics.solver = act
+    s.integrator.run(0)
+    f = s.part.all().f
+    fe, ee = O.ewald([box] * 3, pos, q, 1.0, 0.35, 9.9, 18)
+    rms = np.sqrt(((f - fe) ** 2).sum(1).mean())
+    est = act.get_params()["accuracy"]
+    assert rms < 3 * max(est, 1e-4)
+    fo, _, _ = oracle_total([box] * 3, pos, q, 32, 5, act.alpha, act.r_cut, 1.0)
+    rms_o = np.sqrt(((fo - fe) ** 2).sum(1).mean())
+    assert abs(rms - rms_o) < 0.05 * rms_o + 1e-6
