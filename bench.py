@@ -1,0 +1,408 @@
+"""Benchmark of the P3M + short-range force path (particle-steps/s).
+
+Workload (default): the single large system of 2^20 monovalent ions (half
++1, half -1) at number density 0.5 in a cubic box of side 128 on a jittered
+lattice, LJ eps=1 sigma=1 cutoff 2.5 (shift auto), P3M cao 7, r_cut 3.5 and
+a 256^3 mesh with alpha tuned for an rms force error estimate <= 1e-4 (at
+r_cut 3.5 the 128^3 mesh bottoms out at 3.9e-3), FP32-mixed
+mesh/FFT path.  One step = one full force evaluation (k-space + real-space
+Coulomb + LJ through the Verlet list) of the whole system; positions stay
+fixed, so the Verlet list is reused (its rebuild cost is reported apart).
+Inputs (>= 1 GB resident with the neighbour list) exceed the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the
+workload on its own GPU (replicas only: the path has no exchange step);
+value = all particles of all ranks / max-over-ranks time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at rms force err <=1e-4 (FP32-mixed P3M+LJ force evaluation)"
+HBM_FALLBACK = 6650.0
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mesh", type=int, default=256)
+    ap.add_argument("--cao", type=int, default=7)
+    ap.add_argument("--r_cut", type=float, default=3.5)
+    ap.add_argument("--accuracy", type=float, default=1e-4)
+    ap.add_argument("--fp64", action="store_true", help="plain FP64 path instead of FP32-mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="setup + a few evaluations, no JSON (for ncu captures)")
+    return ap.parse_args()
+
+
+def make_workload(seed=0, n_target=2 ** 20, box=128.0, n_side=102, jitter=0.2):
+    """Jittered simple-cubic lattice at density 0.5 with alternating charges,
+    thinned symmetrically to exactly n_target neutral ions."""
+    rng = np.random.default_rng(seed)
+    a = box / n_side
+    idx = np.stack(np.meshgrid(*[np.arange(n_side)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    q = np.where(idx.sum(1) % 2 == 0, 1.0, -1.0)
+    pos = (idx + 0.5) * a + rng.uniform(-jitter, jitter, idx.shape)
+    drop = (len(q) - n_target) // 2
+    plus = np.flatnonzero(q > 0)
+    minus = np.flatnonzero(q < 0)
+    keep = np.ones(len(q), bool)
+    keep[rng.choice(plus, drop, replace=False)] = False
+    keep[rng.choice(minus, drop, replace=False)] = False
+    return pos[keep].copy(), q[keep].copy(), box
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    def __init__(self, index=0):
+        self.samples = []
+        self.index = index
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 2 + k and s[2 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def cpu_reference_step(pos, q, box, mesh, cao, alpha, r_cut, tab):
+    from oracle import oracle as O
+    p = O.make_params(box, mesh, cao, alpha, r_cut, 1.0)
+    t0 = time.perf_counter()
+    fk, _, _ = O.p3m_kspace(p, pos, q)
+    fr, _, _, _ = O.short_range(p, pos, q, None, 1, tab)
+    return time.perf_counter() - t0
+
+
+def lj_table_oracle():
+    from oracle import oracle as O
+    cut = 2.5
+    shift = -((1 / cut) ** 12 - (1 / cut) ** 6)
+    return O.pair_table(1, {(0, 0): dict(lj_eps=1.0, lj_sig=1.0, lj_cut=cut, lj_shift=shift)})
+
+
+def config_dict(args, n, alpha, nranks):
+    return {"workload": f"single system: 2^20 ions, density 0.5, box 128, LJ 2.5, "
+                        f"P3M mesh {args.mesh}^3 cao {args.cao} r_cut {args.r_cut}",
+            "n_particles_per_rank": int(n), "box": 128.0, "mesh": args.mesh, "cao": args.cao,
+            "r_cut": args.r_cut, "alpha": alpha, "accuracy_target": args.accuracy,
+            "lj": {"epsilon": 1.0, "sigma": 1.0, "cutoff": 2.5},
+            "precision": "fp64" if args.fp64 else "fp32-mixed",
+            "step": "one full force evaluation, Verlet list reused",
+            "l2": "inputs larger than L2 (neighbour list ~1 GB)",
+            "parallelism": f"replicas x{nranks}" if nranks > 1 else "single GPU"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    pos, q, box = make_workload()
+    n = len(q)
+    # alpha of the tuned GPU configuration (same error-estimate formula)
+    alpha = tuned_alpha(args, n, float(np.sum(q * q)), box)
+    tab = lj_table_oracle()
+    for _ in range(args.warmup):
+        cpu_reference_step(pos, q, box, args.mesh, args.cao, alpha, args.r_cut, tab)
+    times = [cpu_reference_step(pos, q, box, args.mesh, args.cao, alpha, args.r_cut, tab)
+             for _ in range(args.steps)]
+    t = float(np.mean(times))
+    v = n / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(args, n, alpha, 1),
+        "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": ncores, "kind": "port",
+                         "sample": "full workload per step: FP64 CPU restatement of the "
+                                   "reference CPU P3M + link-cell LJ/real-space (OpenMP)"},
+        "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def tuned_alpha(args, n, sum_q2, box):
+    """alpha_L from calculate_accuracy (p3m.cpp:636-655) at fixed r_cut."""
+    from math import log, sqrt
+    L = box
+    r_iL = args.r_cut / L
+    V = L ** 3
+    rs0 = 2.0 * sum_q2 / sqrt(n * r_iL * L * V)
+    aL = sqrt(log(sqrt(2.0) * rs0 / args.accuracy)) / r_iL if sqrt(2.0) * rs0 > args.accuracy else 0.1
+    return aL / L
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(local)
+    import espresso_b200 as eb
+    from espresso_b200 import _lib
+    from espresso_b200.electrostatics import P3M, P3MGPU
+
+    lib = _lib.load()
+    pos, q, box = make_workload(seed=rank)
+    n = len(q)
+    cls = P3M if args.fp64 else P3MGPU
+    act = cls(prefactor=1.0, accuracy=args.accuracy, mesh=args.mesh, cao=args.cao,
+              r_cut=args.r_cut, tune=True, timings=2, verbose=False)
+    s = eb.System(box_l=[box] * 3)
+    s.time_step = 0.01
+    s.cell_system.skin = 0.4
+    s.part.add(pos=pos, q=q)
+    s.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0, cutoff=2.5,
+                                                      shift="auto")
+    s.electrostatics.solver = act
+    prm = act.get_params()
+    h = act._handle
+    types = np.zeros(n, dtype=np.int32)
+    s._sync_pairs(h, types)
+    dev = torch.device("cuda", local)
+    pos_d = torch.from_numpy(pos).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    t_d = torch.from_numpy(types).to(dev)
+    f_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    flags = _lib.P3MX_DEVICE_PTRS | _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE
+
+    def step():
+        rc = lib.p3mx_forces(h, n, _lib.dptr(pos_d), _lib.dptr(q_d), _lib.dptr(t_d), _lib.dptr(f_d),
+                             None, None, flags, sp)
+        if rc:
+            _lib.check(rc, h)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    if args.profile_only:
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        return
+    # stage profile (CUDA events between stages, same stream as the launches)
+    names = (ctypes.c_char_p * 32)()
+    ms = (ctypes.c_double * 32)()
+    nst = ctypes.c_int()
+    _lib.check(lib.p3mx_profile(h, 5, ms, names, 32, ctypes.byref(nst)), h)
+    stages = {names[k].decode(): ms[k] for k in range(nst.value)}
+    # rebuild cost: one evaluation with a forced Verlet rebuild
+    lc0 = ctypes.c_longlong()
+    lc1 = ctypes.c_longlong()
+    # timed region
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    lib.p3mx_launch_count(h, ctypes.byref(lc0))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    lib.p3mx_launch_count(h, ctypes.byref(lc1))
+    if dist is not None:
+        dist.barrier()
+    t_ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = n * world / (t_ms * 1e-3)
+
+    # end to end through the C ABI with host buffers (pinned staging inside)
+    pos_h = np.ascontiguousarray(pos)
+    q_h = np.ascontiguousarray(q)
+    f_h = np.zeros((n, 3))
+    hflags = _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE
+
+    def step_host():
+        rc = lib.p3mx_forces(h, n, _lib.dptr(pos_h), _lib.dptr(q_h), _lib.dptr(types),
+                             _lib.dptr(f_h), None, None, hflags, sp)
+        if rc:
+            _lib.check(rc, h)
+
+    for _ in range(2):
+        step_host()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    k_e2e = max(3, args.steps // 3)
+    for _ in range(k_e2e):
+        step_host()
+    torch.cuda.synchronize(dev)
+    t_e2e = (time.perf_counter() - t0) / k_e2e
+    if dist is not None:
+        tt = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = n * world / t_e2e
+
+    # FP32-mixed vs FP64 force difference on the same configuration
+    fp_diff = None
+    if not args.fp64:
+        f32 = f_d.cpu().numpy()
+        ref_act = P3M(prefactor=1.0, accuracy=args.accuracy, mesh=args.mesh, cao=args.cao,
+                      r_cut=args.r_cut, alpha=prm["alpha"], tune=False)
+        s.electrostatics.clear()
+        s.electrostatics.solver = ref_act
+        s._sync_pairs(ref_act._handle, types)
+        f64 = np.zeros((n, 3))
+        _lib.check(lib.p3mx_forces(ref_act._handle, n, _lib.dptr(pos_h), _lib.dptr(q_h),
+                                   _lib.dptr(types), _lib.dptr(f64), None, None, hflags, None),
+                   ref_act._handle)
+        fp_diff = float(np.sqrt(((f32 - f64) ** 2).sum(1).mean()))
+        del ref_act
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    hbm, hbm_kind = peaks()
+    # roofline of the dominant stage
+    N = n
+    M3 = float(args.mesh) ** 3
+    K = args.mesh * args.mesh * (args.mesh // 2 + 1)
+    c = args.cao
+    rc_eff = args.r_cut + 0.4
+    nb_full = 4.18879 * rc_eff ** 3 * 0.5
+    bytes_alg = {
+        "p3m_assign": 28 * N + 4 * M3,
+        "p3m_interp": 28 * N + 12 * M3 + 24 * N,
+        "fft_fwd_zy": 4 * M3 + 8 * K + 8 * K + 8 * K,
+        "fft_x_kspace": 8 * K + 4 * K + 3 * 8 * K,
+        "fft_inv_yz": 3 * (8 * K + 8 * K) + 3 * (8 * K + 4 * M3),
+        "pair_forces": N * nb_full * 4 + 32 * N + 24 * N,
+        "p3m_sort": 2 * (24 + 4 + 4) * N + 8 * M3,
+        "p3m_weights": 24 * N + 8 * N + 3 * 4 * c * N,
+    }
+    dom = max(stages, key=stages.get)
+    dom_ms = stages[dom]
+    alg = bytes_alg.get(dom)
+    achieved = alg / (dom_ms * 1e-3) / 1e9 if alg else None
+    traffic = ncu_traffic().get(dom)
+    flops_alg = {"p3m_assign": 2 * c ** 3 * N + 30 * c * N, "p3m_interp": 6 * c ** 3 * N,
+                 "pair_forces": N * nb_full * 8 + N * 0.5 * 4.18879 * args.r_cut ** 3 * 25}
+    fp32 = None
+    if dom in flops_alg:
+        tf = flops_alg[dom] / (dom_ms * 1e-3) / 1e12
+        fp32 = {"achieved": tf, "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                "frac": tf / FP32_NOMINAL_TFLOPS, "peak_kind": "nominal 148 SM x 128 x 2 x 1965 MHz"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        ncores = os.cpu_count() or 1
+        tab = lj_table_oracle()
+        t_cpu = cpu_reference_step(pos, q, box, args.mesh, args.cao, prm["alpha"], args.r_cut, tab)
+        cpu = {"value": n / t_cpu, "unit": "particle-steps/s", "cores": ncores, "kind": "port",
+               "sample": "one full force evaluation of the same workload on the FP64 CPU "
+                         "restatement of the reference path (OpenMP, all host cores)"}
+    n_launch = lc1.value - lc0.value
+    out = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.fp64 else "f32-mixed (f64 positions/accumulators)",
+        "data": "synthetic", "config": config_dict(args, n, prm["alpha"], world),
+        "e2e": {"value": e2e, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(n * (24 + 8 + 4)), "d2h_bytes_per_step": int(n * 24)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                     "traffic": traffic, "peak_kind": hbm_kind,
+                     "algorithmic_bytes": alg, "launch_ms": dom_ms, "fp32": fp32},
+        "stages_ms": stages,
+        "accuracy": {"rms_force_err_estimate": prm["accuracy"],
+                     "fp32_vs_fp64_rms_force_diff": fp_diff},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": int(n_launch),
+    }
+    print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -16,6 +16,7 @@ P3MX_FORCES = 2
 P3MX_ENERGY = 4
 P3MX_VIRIAL = 8
 P3MX_OVERWRITE = 16
+P3MX_MIXED_OBSERVABLES = 32
 
 STATUS = {0: "OK", 1: "EDOMAIN", 2: "ERUNTIME", 3: "ECUDA", 4: "ENOMEM", 5: "EHANDLE"}
 
@@ -84,6 +85,9 @@ SIGNATURES = {
     "p3mx_cell_index": (ctypes.c_int, [_vp, _sz, _dp, _ip]),
     "p3mx_verlet_pairs": (ctypes.c_int, [_vp, _sz, _dp, _dp, _ip, _ip, _sz, ctypes.POINTER(_sz)]),
     "p3mx_copy_mesh": (ctypes.c_int, [_vp, _dp, _sz]),
+    "p3mx_profile": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_char_p),
+                                    ctypes.c_int, _ip]),
+    "p3mx_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "p3mx_error_estimate": (ctypes.c_int, [_ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, _dp, ctypes.c_double,
                                            _dp, _dp]),

@@ -72,6 +72,10 @@ struct p3mx_handle {
   bool is_tuned = false, activated = false;
   double rs_err = 0, ks_err = 0;
   std::unique_ptr<Engine> eng;
+  // FP64 engine for the observables of the FP32-mixed actor: energies and
+  // pressures are evaluated in FP64, as the reference GPU actor evaluates
+  // them with its double-precision CPU kernels (p3m.impl.hpp:328-343)
+  std::unique_ptr<Engine> eng64;
   size_t n = 0;
   int ntypes = 1;
   std::vector<PairIA> table{PairIA{0, 0, 0, 0, 0, 0, 0, 0, 0, -1.0}};
@@ -164,6 +168,27 @@ void configure_engine(p3mx_handle *h) {
   c.np = static_cast<long long>(h->n);
   h->eng->set_pair_table(h->ntypes, h->table);
   h->eng->configure({c}, static_cast<long long>(h->n));
+  h->eng64.reset();
+}
+
+Engine &observables_engine(p3mx_handle *h) {
+  if (!h->eng64) {
+    h->eng64 = std::make_unique<Engine>(false);
+    ReplicaConf c = h->eng->conf(0);
+    h->eng64->set_pair_table(h->ntypes, h->table);
+    h->eng64->configure({c}, static_cast<long long>(h->n));
+  }
+  return *h->eng64;
+}
+
+// k-space energy / virial of the FP32-mixed actor in FP64 (see eng64).
+void fp64_kspace_observables(p3mx_handle *h, cudaStream_t st, bool want_e, bool want_v,
+                             std::vector<double> &en, std::vector<double> &vir) {
+  Engine &e = *h->eng;
+  Engine &e64 = observables_engine(h);
+  e64.upload(e.d_pos(), e.d_q(), e.d_type(), true, st);
+  e64.census(st);
+  e64.long_range(nullptr, true, want_e, want_v, st, &en, &vir);
 }
 
 // sanity_checks_boxl (p3m.cpp:793-818) and the non-metallic cubic-box rule.
@@ -761,8 +786,12 @@ int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q
     if ((flags & P3MX_FORCES) && f)
       fd = dev ? f : e.d_force();
     std::vector<double> en, vir;
-    e.long_range(fd, dev ? ow : true, energy && (flags & P3MX_ENERGY), virial9 && (flags & P3MX_VIRIAL),
-                 st, &en, &vir);
+    bool const want_e = energy && (flags & P3MX_ENERGY);
+    bool const want_v = virial9 && (flags & P3MX_VIRIAL);
+    bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
+    e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &en, &vir);
+    if (obs64 && (want_e || want_v))
+      fp64_kspace_observables(h, st, want_e, want_v, en, vir);
     if (energy && (flags & P3MX_ENERGY))
       *energy = en.empty() ? 0. : en[0];
     if (virial9 && (flags & P3MX_VIRIAL))
@@ -788,12 +817,15 @@ int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos, const double *
       fd = dev ? f : e.d_force();
     bool const want = (energy2 && (flags & P3MX_ENERGY)) || (virial18 && (flags & P3MX_VIRIAL));
     std::vector<double> en, vir;
+    bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
     if (fd) {
-      e.short_range(fd, dev ? ow : true, want, st, &en, &vir);
-    } else {
+      e.short_range(fd, dev ? ow : true, want && !obs64, st, &en, &vir);
+    } else if (!(want && obs64)) {
       // energies only: compute into the scratch force buffer
       e.short_range(e.d_force(), true, want, st, &en, &vir);
     }
+    if (want && obs64)
+      e.short_range(observables_engine(h).d_force(), true, true, st, &en, &vir, true);
     if (energy2 && (flags & P3MX_ENERGY))
       for (int k = 0; k < 2; ++k)
         energy2[k] = en.empty() ? 0. : en[k];
@@ -821,8 +853,13 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
       e.census(st);
     double *fd = (dev && f) ? f : e.d_force();
     std::vector<double> enk, virk, ens, virs;
-    e.long_range(fd, dev ? ow : true, want_e, want_v, st, &enk, &virk);
-    e.short_range(fd, false, want_e || want_v, st, &ens, &virs);
+    bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
+    e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &enk, &virk);
+    e.short_range(fd, false, (want_e || want_v) && !obs64, st, &ens, &virs);
+    if (obs64 && (want_e || want_v)) {
+      fp64_kspace_observables(h, st, want_e, want_v, enk, virk);
+      e.short_range(observables_engine(h).d_force(), true, true, st, &ens, &virs, true);
+    }
     if (want_e) {
       energy3[0] = ens[0];
       energy3[1] = enk[0];
@@ -881,6 +918,35 @@ int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap) {
       throw Error(P3MX_EDOMAIN, "output buffer too small for the mesh");
     std::memcpy(out, v.data(), v.size() * sizeof(double));
   });
+}
+
+int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names, int cap,
+                 int *nstages) {
+  return guarded(h, [&] {
+    if (!h->eng || !h->activated)
+      throw Error(P3MX_ERUNTIME, "actor not activated");
+    static std::vector<std::string> keep;
+    auto prof = h->eng->profile(std::max(1, reps), h->eng->stream());
+    keep.clear();
+    for (auto const &p : prof)
+      keep.push_back(p.first);
+    int const n = static_cast<int>(prof.size());
+    if (nstages)
+      *nstages = n;
+    for (int k = 0; k < std::min(n, cap); ++k) {
+      if (ms)
+        ms[k] = prof[k].second;
+      if (names)
+        names[k] = keep[k].c_str();
+    }
+  });
+}
+
+int p3mx_launch_count(const p3mx_handle *h, long long *count) {
+  if (!h || !count)
+    return P3MX_EHANDLE;
+  *count = (h->eng ? h->eng->launches() : 0) + (h->eng64 ? h->eng64->launches() : 0);
+  return P3MX_OK;
 }
 
 int p3mx_error_estimate(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,

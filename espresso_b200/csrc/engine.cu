@@ -385,10 +385,10 @@ void Engine::upload_positions(const double *pos, bool device_ptrs, cudaStream_t 
 void Engine::census(cudaStream_t st) {
   int const R = n_rep();
   k_census<<<m_n_blk_census, 256, 0, st>>>(m_blk_census.as<int2>(), m_geom_d.as<RepGeom>(),
-                                           d_pos(), d_q(), m_part_census.as<double>());
+                                           d_pos(), d_q(), m_part_census.as<double>()); ++m_launches;
   k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_census.as<double>(), 6,
                                                       m_blk_census_start_d.as<int>(), R,
-                                                      m_sums_census.as<double>());
+                                                      m_sums_census.as<double>()); ++m_launches;
   m_census_h.assign(static_cast<size_t>(R) * 6, 0.0);
   P3MX_CUDA(cudaMemcpyAsync(m_census_h.data(), m_sums_census.p, R * 6 * sizeof(double),
                             cudaMemcpyDeviceToHost, st));
@@ -407,8 +407,9 @@ void Engine::census(cudaStream_t st) {
 void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
                        cudaStream_t st, const int *cond) {
   exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
-  k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond);
-  k_fix_buckets<<<ceil_div(nkeys, 256), 256, 0, st>>>(start, perm, nkeys, cond);
+  m_launches += 3;
+  k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
+  k_fix_buckets<<<ceil_div(nkeys, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
 }
 
 #define P3MX_CAO_DISPATCH(cao, KERNEL_CALL)                                    \
@@ -435,21 +436,25 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
       throw Error(1, "replicas of one batch must share the charge-assignment order");
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   if (!m_ginf_valid) {
-    k_influence<Real><<<m_n_blk_cplx, 256, 0, st>>>(geom, m_blk_cplx.as<int2>(), m_ginf.as<Real>());
+    k_influence<Real><<<m_n_blk_cplx, 256, 0, st>>>(geom, m_blk_cplx.as<int2>(), m_ginf.as<Real>()); ++m_launches;
     m_ginf_valid = true;
   }
+  mark("start", st);
   // 1. corner binning + deterministic counting sort
   P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_bins + 1) * sizeof(int), st));
   int const nb = ceil_div(m_n, 256);
   if (m_n > 0) {
     k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
-                                        m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>());
+                                        m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>()); ++m_launches;
     sort_keys(m_key.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
               m_perm.as<int>(), m_bins, st);
+    mark("p3m_sort", st);
     P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
                                m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_scz.as<int>(),
                                m_skey.as<int>())));
+    ++m_launches;
+    mark("p3m_weights", st);
   } else {
     P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_bins + 1) * sizeof(int), st));
   }
@@ -457,36 +462,45 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   P3MX_CAO_DISPATCH(cao, (k_p3m_assign<Real, P><<<m_n_blk_mesh, 256, 0, st>>>(
                              geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
                              m_scz.as<int>(), m_rho.as<Real>())));
+  ++m_launches;
+  mark("p3m_assign", st);
   // 3. forward FFT z (r2c) and y
   C const *tw = m_tw.as<C>();
   k_fft_z_fwd<Real><<<m_n_blk_zf, 256, m_smem_zf, st>>>(geom, m_blk_zf.as<Blk>(), m_rho.as<Real>(),
-                                                        m_ck.as<C>(), tw);
+                                                        m_ck.as<C>(), tw); ++m_launches;
   k_fft_y<Real><<<dim3(m_n_blk_y, 1), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_ck.as<C>(), 0,
-                                                          m_tile_y, false, tw);
+                                                          m_tile_y, false, tw); ++m_launches;
+  mark("fft_fwd_zy", st);
   // 4. x pass fused with the k-space operator (+ energy/virial partials)
   bool const want_f = (f != nullptr);
   bool const want_ev = want_e || want_v;
   k_fft_x_kspace<Real><<<m_n_blk_x, 256, m_smem_x, st>>>(
       geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx, m_tile_x,
-      want_f ? 1 : 0, want_ev ? 1 : 0, m_part_x.as<double>(), tw);
-  if (want_ev)
+      want_f ? 1 : 0, want_ev ? 1 : 0, m_part_x.as<double>(), tw); ++m_launches;
+  if (want_ev) {
     k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_x.as<double>(), 8,
                                                         m_blk_x_start_d.as<int>(), R,
                                                         m_sums_x.as<double>());
+    ++m_launches;
+  }
+  mark("fft_x_kspace", st);
   if (!want_f)
     return;
   // 5. backward FFT y (3 fields), z (c2r, 3 fields)
   k_fft_y<Real><<<dim3(m_n_blk_y, 3), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_field.as<C>(),
-                                                          m_cplx, m_tile_y, true, tw);
+                                                          m_cplx, m_tile_y, true, tw); ++m_launches;
   k_fft_z_inv3<Real><<<m_n_blk_zi, 256, m_smem_zi, st>>>(geom, m_blk_zi.as<Blk>(), m_field.as<C>(),
-                                                         m_cplx, m_E.as<Real>(), m_bins, tw);
+                                                         m_cplx, m_E.as<Real>(), m_bins, tw); ++m_launches;
+  mark("fft_inv_yz", st);
   // 6. force back-interpolation
   if (m_n > 0) {
     P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
                                m_W.as<Real>(), m_E.as<Real>(), m_bins, d_q(), m_dipole.as<double>(),
                                m_n, f, overwrite ? 1 : 0)));
+    ++m_launches;
   }
+  mark("p3m_interp", st);
 }
 
 void Engine::long_range(double *f, bool overwrite, bool want_energy, bool want_virial,
@@ -545,11 +559,11 @@ void Engine::build_lists(cudaStream_t st) {
   int const nb = ceil_div(m_n, 256);
   P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr);
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st);
   k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr);
+                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr); ++m_launches;
   if (m_max_nb == 0) {
     // neighbour estimate from the densest replica plus margin
     double est = 16.0;
@@ -566,7 +580,7 @@ void Engine::build_lists(cudaStream_t st) {
     k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                        m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
-                                       m_overflow.as<int>(), nullptr);
+                                       m_overflow.as<int>(), nullptr); ++m_launches;
     int ov = 0;
     P3MX_CUDA(cudaMemcpyAsync(&ov, m_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
@@ -595,7 +609,7 @@ __global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__res
 void Engine::refresh_sorted_positions(cudaStream_t st) {
   k_refresh_spq<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(),
                                                     m_cperm.as<int>(), d_pos(), d_q(), m_n,
-                                                    m_spq.as<double4>());
+                                                    m_spq.as<double4>()); ++m_launches;
 }
 
 template <typename Real>
@@ -608,27 +622,31 @@ void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t
   if (!rebuild) {
     P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
     k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                             m_n, m_flag.as<int>());
+                                             m_n, m_flag.as<int>()); ++m_launches;
     int flag = 0;
     P3MX_CUDA(cudaMemcpyAsync(&flag, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
     rebuild = (flag != 0);
   }
+  mark("sr_check", st);
   if (rebuild)
     build_lists(st);
   else
     refresh_sorted_positions(st);
+  mark(rebuild ? "sr_rebuild" : "sr_refresh", st);
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
   k_pair_forces<Real><<<m_n_blk_pair, 256, smem, st>>>(geom, m_blk_pair.as<int2>(), m_spq.as<double4>(),
                                              m_stype.as<int>(), m_cperm.as<int>(), m_ia_d.as<PairIA>(),
                                              m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
                                              overwrite ? 1 : 0, want_ev ? 1 : 0,
-                                             m_part_pair.as<double>());
+                                             m_part_pair.as<double>()); ++m_launches;
+  mark("pair_forces", st);
 }
 
 void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,
-                         std::vector<double> *energies, std::vector<double> *virials) {
-  if (m_fp32)
+                         std::vector<double> *energies, std::vector<double> *virials,
+                         bool fp64_math) {
+  if (m_fp32 && !fp64_math)
     short_range_t<float>(f, overwrite, want_ev, st);
   else
     short_range_t<double>(f, overwrite, want_ev, st);
@@ -637,7 +655,7 @@ void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t s
     int const R = n_rep();
     k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_pair.as<double>(), 20,
                                                         m_blk_pair_start_d.as<int>(), R,
-                                                        m_sums_pair.as<double>());
+                                                        m_sums_pair.as<double>()); ++m_launches;
     std::vector<double> sums(static_cast<size_t>(R) * 20);
     P3MX_CUDA(cudaMemcpyAsync(sums.data(), m_sums_pair.p, sums.size() * sizeof(double),
                               cudaMemcpyDeviceToHost, st));
@@ -668,21 +686,21 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
   int *flag = m_flag.as<int>();
-  k_fill_int<<<1, 32, 0, st>>>(flag, 0, 1, nullptr);
+  k_fill_int<<<1, 32, 0, st>>>(flag, 0, 1, nullptr); ++m_launches;
   k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                           m_n, flag);
-  k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag);
+                                           m_n, flag); ++m_launches;
+  k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag); ++m_launches;
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag);
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st, flag);
   k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), flag);
+                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
   k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
-                                     m_overflow.as<int>(), flag);
-  k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag);
+                                     m_overflow.as<int>(), flag); ++m_launches;
+  k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag); ++m_launches;
   refresh_sorted_positions(st);
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
   if (m_fp32)
@@ -695,6 +713,7 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
         geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
         m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0, 0,
         m_part_pair.as<double>());
+  ++m_launches;
 }
 
 int Engine::list_overflow(cudaStream_t st) {
@@ -732,7 +751,7 @@ std::vector<int> Engine::cell_index_ghost(cudaStream_t st) {
   k_cell_bin<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(),
                                                  d_q(), m_n, m_ckey.as<int>(), m_cslot.as<int>(),
                                                  m_ccnt.as<int>(), m_pq.as<double4>(), gi.as<int>(),
-                                                 nullptr);
+                                                 nullptr); ++m_launches;
   P3MX_CUDA(cudaMemcpyAsync(out.data(), gi.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));
   m_lists_valid = false;
@@ -791,7 +810,7 @@ double Engine::ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, d
   int const nblk = 296;
   m_ks_part.ensure(nblk * sizeof(double));
   k_ks_error<<<nblk, 256, 0, m_stream>>>(mesh[0], mesh[1], mesh[2], cao, alpha_L,
-                                         m_ks_part.as<double>());
+                                         m_ks_part.as<double>()); ++m_launches;
   std::vector<double> part(nblk);
   P3MX_CUDA(cudaMemcpyAsync(part.data(), m_ks_part.p, nblk * sizeof(double), cudaMemcpyDeviceToHost,
                             m_stream));
@@ -800,6 +819,41 @@ double Engine::ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, d
   for (double v : part)
     he_q += v;
   return 2. * prefactor * sum_q2 * std::sqrt(he_q / static_cast<double>(n_c_part)) / (box[1] * box[2]);
+}
+
+void Engine::mark(const char *name, cudaStream_t st) {
+  if (!m_profiling)
+    return;
+  cudaEvent_t e;
+  P3MX_CUDA(cudaEventCreate(&e));
+  P3MX_CUDA(cudaEventRecord(e, st));
+  m_marks.emplace_back(name, e);
+}
+
+std::vector<std::pair<std::string, double>> Engine::profile(int reps, cudaStream_t st) {
+  std::vector<std::pair<std::string, double>> acc;
+  for (int r = 0; r < reps; ++r) {
+    m_marks.clear();
+    m_profiling = true;
+    long_range(d_force(), true, false, false, st, nullptr, nullptr);
+    short_range(d_force(), false, false, st, nullptr, nullptr);
+    m_profiling = false;
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    for (size_t k = 1; k < m_marks.size(); ++k) {
+      float ms = 0.f;
+      P3MX_CUDA(cudaEventElapsedTime(&ms, m_marks[k - 1].second, m_marks[k].second));
+      std::string const &name = m_marks[k].first;
+      auto it = std::find_if(acc.begin(), acc.end(), [&](auto const &p) { return p.first == name; });
+      if (it == acc.end())
+        acc.emplace_back(name, ms / reps);
+      else
+        it->second += ms / reps;
+    }
+    for (auto &m : m_marks)
+      cudaEventDestroy(m.second);
+    m_marks.clear();
+  }
+  return acc;
 }
 
 } // namespace p3mx

@@ -8,6 +8,8 @@
 #include "pair.cuh"
 
 #include <memory>
+#include <string>
+#include <utility>
 #include <vector>
 
 namespace p3mx {
@@ -93,8 +95,11 @@ public:
                   cudaStream_t st, std::vector<double> *energies,
                   std::vector<double> *virials);
   // Real-space + LJ/WCA over Verlet lists.  energies[r*2], virials[r*18].
+  // fp64_math runs the pair arithmetic in FP64 even on an FP32-mixed engine
+  // (observables of the FP32-mixed actor are evaluated in FP64).
   void short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,
-                   std::vector<double> *energies, std::vector<double> *virials);
+                   std::vector<double> *energies, std::vector<double> *virials,
+                   bool fp64_math = false);
   // Graph-capturable short-range evaluation (device-side rebuild decision).
   void short_range_graph(double *f, bool overwrite, cudaStream_t st);
   // Build lists now if invalid (capacity margin factor for graph use).
@@ -110,6 +115,12 @@ public:
   std::vector<double> mesh_copy(int r, cudaStream_t st);
   void cell_grid(int r, int *cg, double *cs) const;
 
+  // Per-stage device times (ms, mean of reps) of one full force evaluation,
+  // measured with CUDA events between the stages on the stream.
+  std::vector<std::pair<std::string, double>> profile(int reps, cudaStream_t st);
+  // Number of kernels launched by this engine so far.
+  long long launches() const { return m_launches; }
+
   // k-space error sum (device, FP64) for tuning.
   double ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,
                   const double *box, double prefactor);
@@ -124,8 +135,13 @@ private:
   void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
                  cudaStream_t st, const int *cond = nullptr);
 
+  void mark(const char *name, cudaStream_t st);
+
   bool m_fp32;
   cudaStream_t m_stream = nullptr;
+  long long m_launches = 0;
+  bool m_profiling = false;
+  std::vector<std::pair<std::string, cudaEvent_t>> m_marks;
   std::vector<ReplicaConf> m_conf;
   std::vector<RepGeom> m_geom;
   long long m_n = 0;

@@ -34,6 +34,10 @@ extern "C" {
 #define P3MX_ENERGY 4u        /* compute energy */
 #define P3MX_VIRIAL 8u        /* compute the 3x3 virial / pressure tensor */
 #define P3MX_OVERWRITE 16u    /* f is overwritten instead of accumulated */
+/* FP32-mixed actor only: evaluate energy/virial with the FP32 pipeline too.
+ * By default the FP32-mixed actor evaluates these observables in FP64, as
+ * the reference GPU actor does with its double-precision CPU kernels. */
+#define P3MX_MIXED_OBSERVABLES 32u
 
 typedef struct p3mx_handle p3mx_handle;
 
@@ -159,6 +163,15 @@ int p3mx_verlet_pairs(p3mx_handle *h, size_t n, const double *pos,
 /* Charge-assignment mesh of the last long-range call (M0*M1*M2, FP64 copy
  * of the device mesh) for element-wise parity checks. */
 int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap);
+
+/* Stage profile of one force evaluation with the current particles (no
+ * counterpart in the reference, which has no GPU timers): per-stage mean
+ * device time in ms over `reps` evaluations, stage names in
+ * names[k] (static strings).  *nstages receives the stage count. */
+int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names,
+                 int cap, int *nstages);
+/* Total number of kernels launched by the handle's engines so far. */
+int p3mx_launch_count(const p3mx_handle *h, long long *count);
 
 /* Tuning error estimates (p3m.cpp:187-243; GPU k-space sum of
  * p3m_gpu_error_cuda.cu:87-143). */

@@ -793,6 +793,7 @@ int oracle_short_range(const oracle_p3m_params *pp, long n, const double *pos,
   if (cl.build(p.box, max_cut + p.skin, n, pf.data()))
     return 2;
   double const alpha = p.alpha;
+  double const max_cut2 = max_cut * max_cut;
   double const two_a_sqrt_pi_i = 2.0 * alpha * (1.0 / std::sqrt(PI));
   long const nc = long(cl.cg[0]) * cl.cg[1] * cl.cg[2];
   int nthreads = 1;
@@ -823,6 +824,8 @@ int oracle_short_range(const oracle_p3m_params *pp, long n, const double *pos,
             d[k] = mi(pf[3 * i + k] - pf[3 * j + k], p.box[k]);
             d2 += d[k] * d[k];
           }
+          if (d2 >= max_cut2)
+            continue; // beyond every cutoff: all kernels return zero
           double const dist = std::sqrt(d2);
           double fc[3] = {0, 0, 0}, fnb[3] = {0, 0, 0};
           double ec = 0.0, en = 0.0;
