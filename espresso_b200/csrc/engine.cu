@@ -218,12 +218,16 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   size_t const cap = m_fp32 ? 4096 : 2048; // complex elements per smem buffer
   {
     std::vector<int2> bm, bc, bcen, bp;
+    m_run = 4;
+    for (int r = 0; r < R; ++r)
+      if (m_geom[r].mesh[2] % 4)
+        m_run = 2;
     m_blk_census_start.assign(1, 0);
     m_blk_pair_start.assign(1, 0);
     for (int r = 0; r < R; ++r) {
       long long const ms = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].mesh[2];
       long long const cs2 = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].hp;
-      for (int b = 0; b < ceil_div(ms, 256); ++b)
+      for (int b = 0; b < ceil_div(ms / m_run, 256); ++b)
         bm.push_back(int2{r, b});
       for (int b = 0; b < ceil_div(cs2, 256); ++b)
         bc.push_back(int2{r, b});
@@ -327,7 +331,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_start.ensure((m_bins + 1) * sizeof(int));
   m_scan_tiles.ensure((ceil_div(std::max(m_bins, m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
-  m_W.ensure(3 * 7 * n * rsz);
+  m_W.ensure((3 * 7 + 2 * 3) * n * rsz);
   m_scz.ensure(n * sizeof(int));
   m_skey.ensure(n * sizeof(int));
   m_rho.ensure(m_bins * rsz);
@@ -412,7 +416,7 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   k_fix_buckets<<<ceil_div(nkeys, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
 }
 
-#define P3MX_CAO_DISPATCH(cao, KERNEL_CALL)                                    \
+#define P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                  \
   switch (cao) {                                                               \
   case 1: { constexpr int P = 1; KERNEL_CALL; } break;                         \
   case 2: { constexpr int P = 2; KERNEL_CALL; } break;                         \
@@ -421,6 +425,16 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   case 5: { constexpr int P = 5; KERNEL_CALL; } break;                         \
   case 6: { constexpr int P = 6; KERNEL_CALL; } break;                         \
   default: { constexpr int P = 7; KERNEL_CALL; } break;                        \
+  }
+// cao (template P) x z-run length of the assignment (template R: 4 when
+// every mesh has M2 % 4 == 0, else 2)
+#define P3MX_CAO_DISPATCH(cao, KERNEL_CALL)                                    \
+  if (m_run == 4) {                                                            \
+    constexpr int R = 4;                                                       \
+    P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                      \
+  } else {                                                                     \
+    constexpr int R = 2;                                                       \
+    P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                      \
   }
 
 template <typename Real>
@@ -449,7 +463,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
     sort_keys(m_key.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
               m_perm.as<int>(), m_bins, st);
     mark("p3m_sort", st);
-    P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P><<<nb, 256, 0, st>>>(
+    P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P, R><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
                                m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_scz.as<int>(),
                                m_skey.as<int>())));
@@ -459,7 +473,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
     P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_bins + 1) * sizeof(int), st));
   }
   // 2. gather-based charge assignment
-  P3MX_CAO_DISPATCH(cao, (k_p3m_assign<Real, P><<<m_n_blk_mesh, 256, 0, st>>>(
+  P3MX_CAO_DISPATCH(cao, (k_p3m_assign<Real, P, R><<<m_n_blk_mesh, 256, 0, st>>>(
                              geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
                              m_scz.as<int>(), m_rho.as<Real>())));
   ++m_launches;
@@ -494,7 +508,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   mark("fft_inv_yz", st);
   // 6. force back-interpolation
   if (m_n > 0) {
-    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P><<<nb, 256, 0, st>>>(
+    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P, R><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
                                m_W.as<Real>(), m_E.as<Real>(), m_bins, d_q(), m_dipole.as<double>(),
                                m_n, f, overwrite ? 1 : 0)));

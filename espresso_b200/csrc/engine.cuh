@@ -158,6 +158,7 @@ private:
   int m_n_blk_mesh = 0, m_n_blk_cplx = 0, m_n_blk_census = 0, m_n_blk_pair = 0;
   int m_n_blk_zf = 0, m_n_blk_y = 0, m_n_blk_x = 0, m_n_blk_zi = 0;
   int m_tile_y = 16, m_tile_x = 16;
+  int m_run = 4; // z points per thread of the charge assignment
   size_t m_smem_zf = 0, m_smem_y = 0, m_smem_x = 0, m_smem_zi = 0;
 
   // particles

@@ -75,9 +75,16 @@ __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restric
   slot[i] = atomicAdd(&cnt[k], 1);
 }
 
-// Weights in corner-sorted order: W[s] = {q*wx[0..P), wy[0..P), wz[0..P)};
-// also the z corner and the corner key of every sorted particle.
-template <typename Real, int P>
+// Per-particle weight record stride for order P and z-run length R:
+// {q*wx[0..P), wy[0..P), 0[R-1], wz[0..P), 0[R-1]}.  The zero padding lets a
+// thread that owns R consecutive z points read the weight of every point of
+// its run without a branch (out-of-stencil points read zero).
+template <int P, int R> __host__ __device__ constexpr int wstride() { return 3 * P + 2 * (R - 1); }
+template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
+
+// Weights in corner-sorted order; also the z corner and the corner key of
+// every sorted particle.
+template <typename Real, int P, int R>
 __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
                               const int *__restrict__ key, const Real *__restrict__ dist,
                               const double *__restrict__ q, const int *__restrict__ rep_of,
@@ -93,12 +100,17 @@ __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__res
   bspline_weights<P>(dist[3 * i + 1], w[1]);
   bspline_weights<P>(dist[3 * i + 2], w[2]);
   Real const qi = static_cast<Real>(q[i]);
-  Real *o = W + s * (3 * P);
+  Real *o = W + s * wstride<P, R>();
 #pragma unroll
   for (int k = 0; k < P; ++k) {
     o[k] = qi * w[0][k];
     o[P + k] = w[1][k];
-    o[2 * P + k] = w[2][k];
+    o[wz_off<P, R>() + k] = w[2][k];
+  }
+#pragma unroll
+  for (int k = 0; k < R - 1; ++k) {
+    o[2 * P + k] = Real(0);
+    o[wz_off<P, R>() + P + k] = Real(0);
   }
   int const loc = key[i] - static_cast<int>(G.rm_off);
   s_key[s] = loc;
@@ -114,29 +126,42 @@ template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v
   c += err;
 }
 
-// Gather-based charge assignment: one thread per mesh point g sums, in a
-// fixed order, the contributions q*wx*wy*wz of every particle whose stencil
-// covers g (corners in [g-P+1, g] per axis, periodic).  No atomics: the
-// result is bitwise reproducible.  For FP32 the column sums are combined
-// with compensated (two-sum) accumulation.
-template <typename Real, int P>
+// Gather-based charge assignment.  One thread owns R consecutive mesh
+// points along z of one (x, y) line and sums, in a fixed order, the
+// contributions q*wx*wy*wz of every particle whose stencil covers them: for
+// each of the P^2 corner columns (x-kx, y-ky) the particles with z corners
+// in [z0-P+1, z0+R-1] form one contiguous range of the corner-sorted order
+// (two ranges across the periodic wrap), so a thread does 2 P^2 range
+// lookups for R points.  No atomics: the result is bitwise reproducible.
+// For FP32 the per-column partial sums are combined with compensated
+// (two-sum) accumulation.
+template <typename Real, int P, int R>
 __global__ void __launch_bounds__(256)
 k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
              const int *__restrict__ start, const Real *__restrict__ W,
              const int *__restrict__ s_cz, Real *__restrict__ rho) {
+  constexpr int WS = wstride<P, R>();
+  constexpr int WZ = wz_off<P, R>();
   int2 const bk = blk[blockIdx.x];
   RepGeom const &G = reps[bk.x];
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const runs = M2 / R;
   long long const local = static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
-  long long const msize = static_cast<long long>(M0) * M1 * M2;
-  if (local >= msize)
+  if (local >= static_cast<long long>(M0) * M1 * runs)
     return;
-  int const gz = static_cast<int>(local % M2);
-  int const gy = static_cast<int>((local / M2) % M1);
-  int const gx = static_cast<int>(local / (static_cast<long long>(M1) * M2));
+  int const zr = static_cast<int>(local % runs);
+  int const gy = static_cast<int>((local / runs) % M1);
+  int const gx = static_cast<int>(local / (static_cast<long long>(runs) * M1));
+  int const z0 = zr * R;
+  int const z_lo = z0 - (P - 1);
+  int const z_hi = z0 + R - 1;
   const int *st = start + G.rm_off;
-  Real sum = Real(0), comp = Real(0);
-  int const z_lo = gz - (P - 1);
+  Real acc[R], comp[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    acc[j] = Real(0);
+    comp[j] = Real(0);
+  }
 #pragma unroll 1
   for (int kx = 0; kx < P; ++kx) {
     int cx = gx - kx;
@@ -148,42 +173,56 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
       if (cy < 0)
         cy += M1;
       int const row = (cx * M1 + cy) * M2;
-      Real col = Real(0);
-      // corner z in [z_lo, gz], split at the periodic wrap
-      int r0a, r0b, r1a = 0, r1b = 0;
-      if (z_lo >= 0) {
-        r0a = st[row + z_lo];
-        r0b = st[row + gz + 1];
-      } else {
-        r1a = st[row + M2 + z_lo];
-        r1b = st[row + M2];
-        r0a = st[row];
-        r0b = st[row + gz + 1];
+      // [wrap range with corners cz - M2 in [z_lo, 0)] + [main range]
+      int a0 = 0, a1 = 0;
+      if (z_lo < 0) {
+        a0 = st[row + M2 + z_lo];
+        a1 = st[row + M2];
       }
-      for (int s = r1a; s < r1b; ++s) {
-        int const kz = gz - (s_cz[s] - M2);
-        const Real *w = W + static_cast<long long>(s) * (3 * P);
-        col += w[kx] * w[P + ky] * w[2 * P + kz];
+      int const b0 = st[row + max(z_lo, 0)];
+      int const b1 = st[row + z_hi + 1];
+      Real col[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+        col[j] = Real(0);
+      for (int s = a0; s < a1; ++s) {
+        const Real *w = W + static_cast<long long>(s) * WS;
+        int const d = s_cz[s] - M2 - z0;
+        Real const wxy = w[kx] * w[P + ky];
+        const Real *wz = w + WZ - d;
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+          col[j] += wxy * wz[j];
       }
-      for (int s = r0a; s < r0b; ++s) {
-        int const kz = gz - s_cz[s];
-        const Real *w = W + static_cast<long long>(s) * (3 * P);
-        col += w[kx] * w[P + ky] * w[2 * P + kz];
+      for (int s = b0; s < b1; ++s) {
+        const Real *w = W + static_cast<long long>(s) * WS;
+        int const d = s_cz[s] - z0;
+        Real const wxy = w[kx] * w[P + ky];
+        const Real *wz = w + WZ - d;
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+          col[j] += wxy * wz[j];
       }
-      if constexpr (sizeof(Real) == 4)
-        two_sum(sum, comp, col);
-      else
-        sum += col;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        if constexpr (sizeof(Real) == 4)
+          two_sum(acc[j], comp[j], col[j]);
+        else
+          acc[j] += col[j];
+      }
     }
   }
-  rho[G.rm_off + local] = sum + comp;
+  Real *out = rho + G.rm_off + (static_cast<long long>(gx) * M1 + gy) * M2 + z0;
+#pragma unroll
+  for (int j = 0; j < R; ++j)
+    out[j] = acc[j] + comp[j];
 }
 
 // Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373):
 // per sorted particle F -= prefactor/V * sum_{stencil} (q wx wy wz) E, FP32
 // row sums accumulated in FP64; plus the dipole term for epsilon != 0
 // (p3m.cpp:540-547).  Writes (or adds) to f[3*i] of the original index.
-template <typename Real, int P>
+template <typename Real, int P, int R>
 __global__ void __launch_bounds__(256)
 k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
              const int *__restrict__ rep_of, const int *__restrict__ s_key,
@@ -202,10 +241,13 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
   int const cy = (loc / M2) % M1;
   int const cx = loc / (M1 * M2);
   Real wv[3 * P];
-  const Real *w = W + s * (3 * P);
+  const Real *w = W + s * wstride<P, R>();
 #pragma unroll
-  for (int k = 0; k < 3 * P; ++k)
+  for (int k = 0; k < 2 * P; ++k)
     wv[k] = w[k];
+#pragma unroll
+  for (int k = 0; k < P; ++k)
+    wv[2 * P + k] = w[wz_off<P, R>() + k];
   int zi[P];
 #pragma unroll
   for (int k = 0; k < P; ++k) {
