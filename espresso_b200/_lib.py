@@ -91,6 +91,10 @@ SIGNATURES = {
     "p3mx_error_estimate": (ctypes.c_int, [_ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, _dp, ctypes.c_double,
                                            _dp, _dp]),
+    "p3mx_error_estimate_noalloc": (ctypes.c_int, [_ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_double, _dp,
+                                                   ctypes.c_double, _dp, _dp, _vp, ctypes.c_char_p,
+                                                   _sz]),
     "p3mx_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchDesc), _dp, _dp, _ip, ctypes.c_int,
                                          ctypes.POINTER(PairParams), ctypes.POINTER(_vp)]),
     "p3mx_batch_destroy": (None, [_vp]),

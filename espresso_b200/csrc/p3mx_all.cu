@@ -3,3 +3,4 @@
 #include "engine.cu"
 #include "api.cu"
 #include "batch.cu"
+#include "noalloc.cu"

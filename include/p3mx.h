@@ -180,6 +180,23 @@ int p3mx_error_estimate(const int *mesh, int cao, int n_c_part,
                         const double *box, double prefactor, double *rs_err,
                         double *ks_err);
 
+/* Allocation-free k-space / real-space error estimate (no counterpart in
+ * the reference).  For callers that must not allocate device memory while
+ * they run -- engines that hand all GPU memory to their own pool at start-up,
+ * or loops that cannot take the device synchronisation cudaMalloc/cudaFree
+ * may imply.  Same results as p3mx_error_estimate, but the scratch is a
+ * fixed 32 KiB device array inside the library (held on every GPU that loads
+ * it until exit): meshes above 4096*16384 points are rejected with
+ * P3MX_EDOMAIN and a message in errbuf.  The first call on a device looks up
+ * the array's address (make it before any stream capture); all calls share
+ * the array, so calls that overlap on the GPU race.  stream: cudaStream_t or
+ * NULL; errbuf/errbuf_len may be NULL/0. */
+int p3mx_error_estimate_noalloc(const int *mesh, int cao, int n_c_part,
+                                double sum_q2, double alpha_L, double r_cut_iL,
+                                const double *box, double prefactor,
+                                double *rs_err, double *ks_err, void *stream,
+                                char *errbuf, size_t errbuf_len);
+
 /* --- batched replicas -------------------------------------------------- */
 
 /* Many independent cubic or orthorhombic systems advanced by one launch
