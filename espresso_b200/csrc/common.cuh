@@ -32,6 +32,14 @@ template <typename Real> struct CplxOf;
 template <> struct CplxOf<float> { using type = float2; };
 template <> struct CplxOf<double> { using type = double2; };
 
+template <typename Real> struct Real4Of;
+template <> struct Real4Of<float> { using type = float4; };
+// 32-byte aligned four-double record
+struct __align__(32) double4a {
+  double x, y, z, w;
+};
+template <> struct Real4Of<double> { using type = double4a; };
+
 template <typename C> __host__ __device__ inline C cmul(C a, C b) {
   return C{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }

@@ -284,8 +284,8 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     }
     m_smem_zf = smem_zf;
     m_smem_zi = smem_zi;
-    m_smem_y = 2 * static_cast<size_t>(m_tile_y) * maxM1 * csz;
-    m_smem_x = 2 * 3 * static_cast<size_t>(m_tile_x) * maxM0 * csz;
+    m_smem_y = 2 * static_cast<size_t>(m_tile_y) * (maxM1 + 1) * csz;
+    m_smem_x = 2 * 3 * static_cast<size_t>(m_tile_x) * (maxM0 + 1) * csz;
     m_n_blk_zf = static_cast<int>(zf.size());
     m_n_blk_y = static_cast<int>(y.size());
     m_n_blk_x = static_cast<int>(x.size());
@@ -335,7 +335,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_scz.ensure(n * sizeof(int));
   m_skey.ensure(n * sizeof(int));
   m_rho.ensure(m_bins * rsz);
-  m_E.ensure(3 * m_bins * rsz);
+  m_E.ensure(4 * m_bins * rsz);
   m_ck.ensure(m_cplx * csz);
   m_field.ensure(3 * m_cplx * csz);
   m_ginf.ensure(m_cplx * rsz);
@@ -504,13 +504,13 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   k_fft_y<Real><<<dim3(m_n_blk_y, 3), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_field.as<C>(),
                                                           m_cplx, m_tile_y, true, tw); ++m_launches;
   k_fft_z_inv3<Real><<<m_n_blk_zi, 256, m_smem_zi, st>>>(geom, m_blk_zi.as<Blk>(), m_field.as<C>(),
-                                                         m_cplx, m_E.as<Real>(), m_bins, tw); ++m_launches;
+                                                         m_cplx, m_E.as<Real>(), tw); ++m_launches;
   mark("fft_inv_yz", st);
   // 6. force back-interpolation
   if (m_n > 0) {
     P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P, R><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
-                               m_W.as<Real>(), m_E.as<Real>(), m_bins, d_q(), m_dipole.as<double>(),
+                               m_W.as<Real>(), m_E.as<Real>(), d_q(), m_dipole.as<double>(),
                                m_n, f, overwrite ? 1 : 0)));
     ++m_launches;
   }
@@ -649,11 +649,17 @@ void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t
     refresh_sorted_positions(st);
   mark(rebuild ? "sr_rebuild" : "sr_refresh", st);
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
-  k_pair_forces<Real><<<m_n_blk_pair, 256, smem, st>>>(geom, m_blk_pair.as<int2>(), m_spq.as<double4>(),
-                                             m_stype.as<int>(), m_cperm.as<int>(), m_ia_d.as<PairIA>(),
-                                             m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
-                                             overwrite ? 1 : 0, want_ev ? 1 : 0,
-                                             m_part_pair.as<double>()); ++m_launches;
+  if (want_ev)
+    k_pair_forces<Real, true><<<m_n_blk_pair, 256, smem, st>>>(
+        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
+        m_part_pair.as<double>());
+  else
+    k_pair_forces<Real, false><<<m_n_blk_pair, 256, smem, st>>>(
+        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
+        m_part_pair.as<double>());
+  ++m_launches;
   mark("pair_forces", st);
 }
 
@@ -718,14 +724,14 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   refresh_sorted_positions(st);
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
   if (m_fp32)
-    k_pair_forces<float><<<m_n_blk_pair, 256, smem, st>>>(
+    k_pair_forces<float, false><<<m_n_blk_pair, 256, smem, st>>>(
         geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0, 0,
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
         m_part_pair.as<double>());
   else
-    k_pair_forces<double><<<m_n_blk_pair, 256, smem, st>>>(
+    k_pair_forces<double, false><<<m_n_blk_pair, 256, smem, st>>>(
         geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0, 0,
+        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
         m_part_pair.as<double>());
   ++m_launches;
 }

@@ -84,28 +84,43 @@ __device__ inline void dft_dyn(C *v, int R, const C *__restrict__ tw, int n, boo
     v[m] = out[m];
 }
 
-// One Stockham stage over `nlines` lines of length n held in shared memory.
+// Quotient of small non-negative ints (< 2^24) by a runtime divisor via the
+// FP32 reciprocal plus one correction step (replaces the ~20-instruction
+// integer division in the FFT index maps).
+__device__ inline int qdiv(int a, int b, float rb) {
+  int q = __float2int_rz(__int2float_rn(a) * rb);
+  int const r = a - q * b;
+  q += (r >= b) - (r < 0);
+  return q;
+}
+
+// One Stockham stage over `nlines` lines of length n held in shared memory
+// with line stride ld (ld > n pads the lines against bank conflicts).
+// Twiddle index r*jm*tstride < n, so no modulo is needed.
 template <typename C, int R>
-__device__ inline void fft_stage_t(const C *src, C *dst, int n, int nlines, int Ns,
+__device__ inline void fft_stage_t(const C *src, C *dst, int n, int ld, int nlines, int Ns,
                                    const C *__restrict__ tw, bool inv) {
   int const nb = n / R;
   int const total = nb * nlines;
   int const tstride = n / (Ns * R);
+  float const rnb = 1.0f / static_cast<float>(nb);
+  float const rNs = 1.0f / static_cast<float>(Ns);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int const line = t / nb;
+    int const line = qdiv(t, nb, rnb);
     int const j = t - line * nb;
-    C const *s = src + line * n;
-    C *d = dst + line * n;
-    int const jm = j % Ns;
+    C const *s = src + line * ld;
+    C *d = dst + line * ld;
+    int const jq = qdiv(j, Ns, rNs);
+    int const jm = j - jq * Ns;
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       v[r] = s[j + r * nb];
       if (r > 0 && jm != 0)
-        v[r] = cmul(v[r], ld_tw(tw, (r * jm * tstride) % n, inv));
+        v[r] = cmul(v[r], ld_tw(tw, r * jm * tstride, inv));
     }
     dft_small<C, R>(v, tw, n, inv);
-    int const base = (j / Ns) * Ns * R + jm;
+    int const base = jq * Ns * R + jm;
 #pragma unroll
     for (int r = 0; r < R; ++r)
       d[base + r * Ns] = v[r];
@@ -113,7 +128,7 @@ __device__ inline void fft_stage_t(const C *src, C *dst, int n, int nlines, int 
 }
 
 template <typename C>
-__device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int nlines, int Ns,
+__device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int ld, int nlines, int Ns,
                                      int R, const C *__restrict__ tw, bool inv) {
   int const nb = n / R;
   int const total = nb * nlines;
@@ -121,14 +136,14 @@ __device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int nlines, in
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int const line = t / nb;
     int const j = t - line * nb;
-    C const *s = src + line * n;
-    C *d = dst + line * n;
+    C const *s = src + line * ld;
+    C *d = dst + line * ld;
     int const jm = j % Ns;
     C v[32];
     for (int r = 0; r < R; ++r) {
       v[r] = s[j + r * nb];
       if (r > 0 && jm != 0)
-        v[r] = cmul(v[r], ld_tw(tw, (r * jm * tstride) % n, inv));
+        v[r] = cmul(v[r], ld_tw(tw, r * jm * tstride, inv));
     }
     dft_dyn(v, R, tw, n, inv);
     int const base = (j / Ns) * Ns * R + jm;
@@ -140,7 +155,7 @@ __device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int nlines, in
 // Full transform of nlines lines in `a` (scratch `b`); returns the buffer
 // holding the result.  All threads of the block must call it.
 template <typename C>
-__device__ C *fft_lines(C *a, C *b, int nlines, AxisPlan const &pl,
+__device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
                         const C *__restrict__ twtab, bool inv) {
   int const n = pl.n;
   const C *tw = twtab + pl.tw_off;
@@ -149,12 +164,12 @@ __device__ C *fft_lines(C *a, C *b, int nlines, AxisPlan const &pl,
   for (int s = 0; s < pl.nstages; ++s) {
     int const R = pl.radix[s];
     switch (R) {
-    case 2: fft_stage_t<C, 2>(src, dst, n, nlines, Ns, tw, inv); break;
-    case 3: fft_stage_t<C, 3>(src, dst, n, nlines, Ns, tw, inv); break;
-    case 4: fft_stage_t<C, 4>(src, dst, n, nlines, Ns, tw, inv); break;
-    case 5: fft_stage_t<C, 5>(src, dst, n, nlines, Ns, tw, inv); break;
-    case 7: fft_stage_t<C, 7>(src, dst, n, nlines, Ns, tw, inv); break;
-    default: fft_stage_dyn<C>(src, dst, n, nlines, Ns, R, tw, inv); break;
+    case 2: fft_stage_t<C, 2>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 3: fft_stage_t<C, 3>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 4: fft_stage_t<C, 4>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 5: fft_stage_t<C, 5>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 7: fft_stage_t<C, 7>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    default: fft_stage_dyn<C>(src, dst, n, ld, nlines, Ns, R, tw, inv); break;
     }
     __syncthreads();
     Ns *= R;
@@ -184,7 +199,7 @@ __global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restr
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x)
     a[e] = C{src[e], Real(0)};
   __syncthreads();
-  C *res = fft_lines<C>(a, b, nl, G.plan[2], twtab, false);
+  C *res = fft_lines<C>(a, b, nl, n, G.plan[2], twtab, false);
   int const H = n / 2 + 1;
   for (int e = threadIdx.x; e < nl * G.hp; e += blockDim.x) {
     int const l = e / G.hp, k = e - l * G.hp;
@@ -208,18 +223,19 @@ __global__ void k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict_
   int const H = G.mesh[2] / 2 + 1;
   int const x = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
+  int const ld = M1 + 1; // padded line stride: conflict-free transposed staging
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + T * M1;
+  C *b = a + T * ld;
   long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp;
   for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
     int const y = e / T, t = e - y * T;
-    a[t * M1 + y] = cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t];
+    a[t * ld + y] = cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t];
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, T, G.plan[1], twtab, inv);
+  C *res = fft_lines<C>(a, b, T, ld, G.plan[1], twtab, inv);
   for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
     int const y = e / T, t = e - y * T;
-    cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t] = res[t * M1 + y];
+    cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t] = res[t * ld + y];
   }
 }
 
@@ -242,17 +258,18 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   int const H = M2 / 2 + 1;
   int const y = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
-  int const L = T * M0;
+  int const ld = M0 + 1; // padded line stride
+  int const L = T * ld;
   C *a = reinterpret_cast<C *>(smem_raw);
   C *b = a + 3 * L; // scratch of the same size (3 fields)
   long long const stride_x = static_cast<long long>(M1) * G.hp;
   long long const base = G.km_off + static_cast<long long>(y) * G.hp + kz0;
-  for (int e = threadIdx.x; e < L; e += blockDim.x) {
+  for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
     int const x = e / T, t = e - x * T;
-    a[t * M0 + x] = rho_hat[base + x * stride_x + t];
+    a[t * ld + x] = rho_hat[base + x * stride_x + t];
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, T, G.plan[0], twtab, false);
+  C *res = fft_lines<C>(a, b, T, ld, G.plan[0], twtab, false);
   // k-space operator
   double const wv[3] = {2.0 * kPi * G.box_i[0], 2.0 * kPi * G.box_i[1],
                         2.0 * kPi * G.box_i[2]};
@@ -262,10 +279,10 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   // d_op (Nyquist zeroed) integer shift of index i in a mesh of size m
   auto dop = [](int i, int m) { return (i == m / 2) ? 0 : (i < m / 2 ? i : i - m); };
   int const kyd = dop(y, M1);
-  for (int e = threadIdx.x; e < L; e += blockDim.x) {
+  for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
     int const t = e / M0, x = e - t * M0;
     int const kz = kz0 + t;
-    C const rh = res[t * M0 + x];
+    C const rh = res[t * ld + x];
     Real const g = ginf[base + x * stride_x + t];
     int const kxd = dop(x, M0), kzd = dop(kz, M2);
     if (want_ev) {
@@ -291,9 +308,9 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
       Real const k0 = static_cast<Real>(kxd) * static_cast<Real>(wv[0]);
       Real const k1 = static_cast<Real>(kyd) * static_cast<Real>(wv[1]);
       Real const k2 = static_cast<Real>(kzd) * static_cast<Real>(wv[2]);
-      fbuf[0 * L + t * M0 + x] = C{-k0 * phi.y, k0 * phi.x};
-      fbuf[1 * L + t * M0 + x] = C{-k1 * phi.y, k1 * phi.x};
-      fbuf[2 * L + t * M0 + x] = C{-k2 * phi.y, k2 * phi.x};
+      fbuf[0 * L + t * ld + x] = C{-k0 * phi.y, k0 * phi.x};
+      fbuf[1 * L + t * ld + x] = C{-k1 * phi.y, k1 * phi.x};
+      fbuf[2 * L + t * ld + x] = C{-k2 * phi.y, k2 * phi.x};
     }
   }
   if (want_ev) {
@@ -322,11 +339,13 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
     return;
   __syncthreads();
   C *scratch = (fbuf == a) ? b : a;
-  C *fres = fft_lines<C>(fbuf, scratch, 3 * T, G.plan[0], twtab, true);
-  for (int e = threadIdx.x; e < 3 * L; e += blockDim.x) {
-    int const d = e / L, r = e - d * L;
+  // the three field blocks are 3T consecutive lines of stride ld
+  C *fres = fft_lines<C>(fbuf, scratch, 3 * T, ld, G.plan[0], twtab, true);
+  int const TM = T * M0;
+  for (int e = threadIdx.x; e < 3 * TM; e += blockDim.x) {
+    int const d = e / TM, r = e - d * TM;
     int const x = r / T, t = r - x * T;
-    field0[field_stride * d + base + x * stride_x + t] = fres[d * L + t * M0 + x];
+    field0[field_stride * d + base + x * stride_x + t] = fres[d * L + t * ld + x];
   }
 }
 
@@ -335,7 +354,6 @@ template <typename Real>
 __global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
                              const typename CplxOf<Real>::type *__restrict__ field0,
                              long long field_stride, Real *__restrict__ efield,
-                             long long efield_stride,
                              const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -360,11 +378,18 @@ __global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__rest
     a[e] = v;
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, 3 * nl, G.plan[2], twtab, true);
-  for (int e = threadIdx.x; e < 3 * nl * n; e += blockDim.x) {
-    int const dl = e / n, z = e - dl * n;
-    int const d = dl / nl, l = dl - d * nl;
-    efield[efield_stride * d + G.rm_off + (line0 + l) * n + z] = res[e].x;
+  C *res = fft_lines<C>(a, b, 3 * nl, n, G.plan[2], twtab, true);
+  // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
+  // interpolation gathers one 16-byte (FP32) record per stencil point
+  using R4 = typename Real4Of<Real>::type;
+  R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
+  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+    R4 v;
+    v.x = res[e].x;
+    v.y = res[nl * n + e].x;
+    v.z = res[2 * nl * n + e].x;
+    v.w = Real(0);
+    out[e] = v;
   }
 }
 

@@ -219,14 +219,14 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
 }
 
 // Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373):
-// per sorted particle F -= prefactor/V * sum_{stencil} (q wx wy wz) E, FP32
+// reads the packed (Ex, Ey, Ez, 0) field mesh; per sorted particle F -= prefactor/V * sum_{stencil} (q wx wy wz) E, FP32
 // row sums accumulated in FP64; plus the dipole term for epsilon != 0
 // (p3m.cpp:540-547).  Writes (or adds) to f[3*i] of the original index.
 template <typename Real, int P, int R>
 __global__ void __launch_bounds__(256)
 k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
              const int *__restrict__ rep_of, const int *__restrict__ s_key,
-             const Real *__restrict__ W, const Real *__restrict__ E, long long estride,
+             const Real *__restrict__ W, const Real *__restrict__ E,
              const double *__restrict__ q, const double *__restrict__ dipole,
              long long n, double *__restrict__ f, int overwrite) {
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -254,9 +254,8 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
     int z = cz + k;
     zi[k] = (z >= M2) ? z - M2 : z;
   }
-  const Real *E0 = E + G.rm_off;
-  const Real *E1 = E0 + estride;
-  const Real *E2 = E1 + estride;
+  using R4 = typename Real4Of<Real>::type;
+  const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off;
   double fx = 0.0, fy = 0.0, fz = 0.0;
 #pragma unroll 1
   for (int kx = 0; kx < P; ++kx) {
@@ -273,11 +272,11 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
       Real ax = Real(0), ay = Real(0), az = Real(0);
 #pragma unroll
       for (int kz = 0; kz < P; ++kz) {
-        long long const idx = row + zi[kz];
+        R4 const e = E4[row + zi[kz]];
         Real const wt = wxy * wv[2 * P + kz];
-        ax += wt * E0[idx];
-        ay += wt * E1[idx];
-        az += wt * E2[idx];
+        ax += wt * e.x;
+        ay += wt * e.y;
+        az += wt * e.z;
       }
       fx += static_cast<double>(ax);
       fy += static_cast<double>(ay);

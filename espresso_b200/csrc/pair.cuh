@@ -171,21 +171,66 @@ template <typename Real> __device__ inline Real sqrt_r(Real x);
 template <> __device__ inline float sqrt_r<float>(float x) { return sqrtf(x); }
 template <> __device__ inline double sqrt_r<double>(double x) { return sqrt(x); }
 
+// Reciprocal / reciprocal square root in the working precision: FP32 uses
+// the hardware approximations refined to ~1 ulp (the FP32-mixed path
+// tolerates ulp-level differences); FP64 keeps IEEE division and sqrt.
+template <typename Real> __device__ inline Real rcp_r(Real x);
+template <> __device__ inline float rcp_r<float>(float x) { return __frcp_rn(x); }
+template <> __device__ inline double rcp_r<double>(double x) { return 1.0 / x; }
+template <typename Real> __device__ inline Real rsqrt_r(Real x);
+template <> __device__ inline float rsqrt_r<float>(float x) { return rsqrtf(x); }
+template <> __device__ inline double rsqrt_r<double>(double x) { return 1.0 / sqrt(x); }
+
+// LJ/WCA parameters of one type pair in the working precision.
+template <typename Real> struct PairR {
+  Real lcut, lmin, loff, lsig, leps, lshift, wcut, wsig, weps;
+  bool active;
+  __device__ explicit PairR(PairIA const &p)
+      : lcut(static_cast<Real>(p.lj_cut + p.lj_offset)),
+        lmin(static_cast<Real>(p.lj_min + p.lj_offset)), loff(static_cast<Real>(p.lj_offset)),
+        lsig(static_cast<Real>(p.lj_sig)), leps(static_cast<Real>(p.lj_eps)),
+        lshift(static_cast<Real>(p.lj_shift)), wcut(static_cast<Real>(p.wca_cut)),
+        wsig(static_cast<Real>(p.wca_sig)), weps(static_cast<Real>(p.wca_eps)),
+        active(p.ia_cut != -1.0) {}
+};
+
+// LJ + WCA force factor and energy of one pair (lj.hpp:41-60, wca.hpp:39-55).
+template <typename Real>
+__device__ inline void lj_wca(PairR<Real> const &p, Real dist, Real inv_d, Real &fn, Real &en) {
+  if (dist < p.lcut && dist > p.lmin) {
+    Real const r_off = dist - p.loff;
+    Real const inv_off = rcp_r(r_off);
+    Real const s = p.lsig * inv_off;
+    Real const s2 = s * s;
+    Real const f6 = s2 * s2 * s2;
+    fn += Real(48) * p.leps * f6 * (f6 - Real(0.5)) * (inv_off * inv_d);
+    en += Real(4) * p.leps * (f6 * f6 - f6 + p.lshift);
+  }
+  if (dist < p.wcut) {
+    Real const s = p.wsig * inv_d;
+    Real const s2 = s * s;
+    Real const f6 = s2 * s2 * s2;
+    fn += Real(48) * p.weps * f6 * (f6 - Real(0.5)) * (inv_d * inv_d);
+    en += Real(4) * p.weps * (f6 * f6 - f6 + Real(0.25));
+  }
+}
+
 // Pair kernel over the Verlet list: real-space Coulomb
 // (CoulombP3M::pair_force / pair_energy, p3m.hpp:146-180) plus LJ and WCA
-// (lj.hpp:41-60, wca.hpp:39-55), minimum-image distance in FP64, pair
+// (lj.hpp:41-60, wca.hpp:39-55).  Minimum-image difference in FP64, pair
 // arithmetic in Real, per-particle accumulation in Real (no atomics: each
-// particle owns its force).  Energies/virials: each pair is seen from both
-// ends, so per-particle sums are halved; per-block FP64 partials
-// {E_coul, E_nb, Vc[9], Vn[9]} (width 20).
-template <typename Real>
-__global__ void __launch_bounds__(256)
+// particle owns its force, full list).  EV adds energies and virials: each
+// pair is seen from both ends, so per-particle sums are halved; per-block
+// FP64 partials {E_coul, E_nb, Vc[9], Vn[9]} (width 20).  Blocks map to
+// replicas through the block table so partials never straddle replicas.
+// Neighbour loads are issued two entries ahead of their use.
+template <typename Real, bool EV>
+__global__ void __launch_bounds__(256, (sizeof(Real) == 4 && !EV) ? 4 : 1)
 k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
               const double4 *__restrict__ spq, const int *__restrict__ stype,
               const int *__restrict__ perm, const PairIA *__restrict__ ia_g, int ntypes,
               long long n, const int *__restrict__ nb, const int *__restrict__ nb_cnt,
-              double *__restrict__ f, int overwrite, int want_ev,
-              double *__restrict__ partials) {
+              double *__restrict__ f, int overwrite, double *__restrict__ partials) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PairIA *ia = reinterpret_cast<PairIA *>(smem_raw);
   for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
@@ -194,64 +239,68 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
   int2 const bk = blk[blockIdx.x];
   RepGeom const &G = reps[bk.x];
   long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
-  double ev[20];
+  double ev[EV ? 20 : 1];
 #pragma unroll
-  for (int k = 0; k < 20; ++k)
+  for (int k = 0; k < (EV ? 20 : 1); ++k)
     ev[k] = 0.0;
   if (a < G.p0 + G.np) {
     double4 const pa = spq[a];
     int const ta = stype[a];
+    double const L0 = G.box[0], L1 = G.box[1], L2 = G.box[2];
+    double const Li0 = G.box_i[0], Li1 = G.box_i[1], Li2 = G.box_i[2];
     Real const alpha = static_cast<Real>(G.alpha);
     Real const r_cut = static_cast<Real>(G.r_cut);
     Real const two_a_sqrt_pi_i = static_cast<Real>(2.0 * G.alpha / sqrt(kPi));
-    Real const pref = static_cast<Real>(G.prefactor);
+    Real const pref_qa = static_cast<Real>(G.prefactor * pa.w);
+    bool const one_type = (ntypes == 1);
+    PairR<Real> const p0(ia[0]);
     Real fx = Real(0), fy = Real(0), fz = Real(0);
     int const cnt = nb_cnt[a];
+    const int *nbp = nb + a;
+    int b_next = (cnt > 0) ? nbp[0] : 0;
+    double4 p_next = (cnt > 0) ? spq[b_next] : pa;
     for (int k = 0; k < cnt; ++k) {
-      int const b = nb[static_cast<long long>(k) * n + a];
-      double4 const pb = spq[b];
-      Real const d0 = static_cast<Real>(mi_d(pa.x - pb.x, G.box[0], G.box_i[0]));
-      Real const d1 = static_cast<Real>(mi_d(pa.y - pb.y, G.box[1], G.box_i[1]));
-      Real const d2v = static_cast<Real>(mi_d(pa.z - pb.z, G.box[2], G.box_i[2]));
+      int const b = b_next;
+      double4 const pb = p_next;
+      if (k + 1 < cnt) {
+        b_next = nbp[static_cast<long long>(k + 1) * n];
+        p_next = spq[b_next];
+      }
+      Real const d0 = static_cast<Real>(mi_d(pa.x - pb.x, L0, Li0));
+      Real const d1 = static_cast<Real>(mi_d(pa.y - pb.y, L1, Li1));
+      Real const d2v = static_cast<Real>(mi_d(pa.z - pb.z, L2, Li2));
       Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
-      Real const dist = sqrt_r(dist2);
+      Real const inv_d = rsqrt_r(dist2);
+      Real const dist = dist2 * inv_d;
       Real fc = Real(0), ec = Real(0);
-      Real const q1q2 = static_cast<Real>(pa.w * pb.w);
-      if (q1q2 != Real(0) && dist < r_cut && dist > Real(0)) {
+      Real const qb = static_cast<Real>(pb.w);
+      if (qb != Real(0) && pref_qa != Real(0) && dist < r_cut && dist > Real(0)) {
         Real const adist = alpha * dist;
         Real const ex = exp_r(-adist * adist);
-        Real const erfc_part_ri = as_erfc_part(adist) / dist;
-        fc = pref * q1q2 * (ex * (erfc_part_ri + two_a_sqrt_pi_i) / dist2);
-        ec = pref * q1q2 * erfc_part_ri * ex;
+        Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
+        Real const asp = t * (Real(0.254829592) +
+                              t * (Real(-0.284496736) +
+                                   t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
+        Real const erfc_part_ri = asp * inv_d;
+        Real const pq = pref_qa * qb;
+        fc = pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d));
+        if constexpr (EV)
+          ec = pq * erfc_part_ri * ex;
       }
       Real fn = Real(0), en = Real(0);
-      PairIA const &p = ia[ta * ntypes + stype[b]];
-      if (p.ia_cut != -1.0) {
-        Real const lcut = static_cast<Real>(p.lj_cut + p.lj_offset);
-        Real const lmin = static_cast<Real>(p.lj_min + p.lj_offset);
-        if (dist < lcut && dist > lmin) {
-          Real const r_off = dist - static_cast<Real>(p.lj_offset);
-          Real const s = static_cast<Real>(p.lj_sig) / r_off;
-          Real const s2 = s * s;
-          Real const f6 = s2 * s2 * s2;
-          Real const eps = static_cast<Real>(p.lj_eps);
-          fn += Real(48) * eps * f6 * (f6 - Real(0.5)) / (r_off * dist);
-          en += Real(4) * eps * (f6 * f6 - f6 + static_cast<Real>(p.lj_shift));
-        }
-        if (dist < static_cast<Real>(p.wca_cut)) {
-          Real const s = static_cast<Real>(p.wca_sig) / dist;
-          Real const s2 = s * s;
-          Real const f6 = s2 * s2 * s2;
-          Real const eps = static_cast<Real>(p.wca_eps);
-          fn += Real(48) * eps * f6 * (f6 - Real(0.5)) / dist2;
-          en += Real(4) * eps * (f6 * f6 - f6 + Real(0.25));
-        }
+      if (one_type) {
+        if (p0.active)
+          lj_wca(p0, dist, inv_d, fn, en);
+      } else {
+        PairR<Real> const p(ia[ta * ntypes + stype[b]]);
+        if (p.active)
+          lj_wca(p, dist, inv_d, fn, en);
       }
       Real const ft = fc + fn;
       fx += ft * d0;
       fy += ft * d1;
       fz += ft * d2v;
-      if (want_ev) {
+      if constexpr (EV) {
         double const dd[3] = {double(d0), double(d1), double(d2v)};
         ev[0] += 0.5 * double(ec);
         ev[1] += 0.5 * double(en);
@@ -275,7 +324,7 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
       f[3 * i + 2] += double(fz);
     }
   }
-  if (want_ev) {
+  if constexpr (EV) {
     __shared__ double red[20][8];
     int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
