@@ -1,0 +1,149 @@
+"""GPU tests of the batched-replica API (p3mx_batch_*): many independent
+systems of uneven size, box and Bjerrum length advanced by one launch per
+kernel.  Forces of every replica are checked against the FP64 oracle with the
+parameters the batch autotuner chose; the graph-captured Langevin run is
+checked for reproducibility and equipartition.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from espresso_b200 import _lib
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+_P = ctypes.POINTER
+
+
+def make_replicas(seed=5, n_rep=5):
+    rng = np.random.default_rng(seed)
+    boxes, prefs, pos, q, offs = [], [], [], [], [0]
+    for r in range(n_rep):
+        n = int(rng.integers(200, 900)) * 2
+        L = (n / 0.3) ** (1 / 3)
+        nval = n // 2
+        val = rng.choice([1.0, 2.0])
+        qq = np.concatenate([np.full(nval, val), np.full(nval, -val)])
+        # keep ions apart: jittered lattice with random assignment of charges
+        side = int(np.ceil(n ** (1 / 3)))
+        grid = np.stack(np.meshgrid(*[np.arange(side)] * 3, indexing="ij"), -1).reshape(-1, 3)
+        sel = rng.choice(len(grid), n, replace=False)
+        p = (grid[sel] + 0.5) * (L / side) + rng.uniform(-0.1, 0.1, (n, 3))
+        rng.shuffle(qq)
+        boxes.append([L, L, L])
+        prefs.append(float(rng.uniform(0.5, 4.0)))
+        pos.append(p)
+        q.append(qq)
+        offs.append(offs[-1] + n)
+    return (np.array(boxes), np.array(prefs), np.vstack(pos), np.concatenate(q),
+            np.array(offs, dtype=np.int64))
+
+
+def wca_table():
+    tab = (_lib.PairParams * 1)()
+    tab[0].wca_eps = 1.0
+    tab[0].wca_sig = 1.0
+    return tab
+
+
+def create(boxes, prefs, pos, q, offs, acc=1e-3, single=1):
+    lib = _lib.load()
+    d = _lib.BatchDesc()
+    d.n_rep = len(prefs)
+    boxes = np.ascontiguousarray(boxes, dtype=np.float64)
+    prefs = np.ascontiguousarray(prefs, dtype=np.float64)
+    offs = np.ascontiguousarray(offs, dtype=np.int64)
+    d.box = boxes.ctypes.data_as(_P(ctypes.c_double))
+    d.prefactor = prefs.ctypes.data_as(_P(ctypes.c_double))
+    d.offset = offs.ctypes.data_as(_P(ctypes.c_longlong))
+    d.accuracy = acc
+    d.skin = 0.4
+    d.single_precision = single
+    d.mesh_min, d.mesh_max, d.cao_min, d.cao_max = 8, 32, 3, 7
+    h = ctypes.c_void_p()
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    types = np.zeros(len(q), dtype=np.int32)
+    rc = lib.p3mx_batch_create(ctypes.byref(d), pos.ctypes.data_as(_P(ctypes.c_double)),
+                               q.ctypes.data_as(_P(ctypes.c_double)),
+                               types.ctypes.data_as(_P(ctypes.c_int)), 1, wca_table(),
+                               ctypes.byref(h))
+    if rc:
+        msg = lib.p3mx_batch_last_error(h).decode() if h.value else ""
+        raise RuntimeError(f"batch create failed {rc}: {msg}")
+    # keep the arrays referenced by the descriptor alive for the call only
+    return h
+
+
+def tuned(h, r):
+    t = _lib.Tuned()
+    assert _lib.load().p3mx_batch_get_tuned(h, r, ctypes.byref(t)) == 0
+    return t
+
+
+def test_batch_forces_match_oracle_per_replica():
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas()
+    h = create(boxes, prefs, pos, q, offs)
+    try:
+        R = len(prefs)
+        en = np.zeros(R)
+        assert lib.p3mx_batch_forces(h, en.ctypes.data_as(_P(ctypes.c_double))) == 0
+        f = np.zeros_like(pos)
+        assert lib.p3mx_batch_get(h, None, f.ctypes.data_as(_P(ctypes.c_double)), None) == 0
+        tab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
+        caos = set()
+        for r in range(R):
+            t = tuned(h, r)
+            caos.add(t.cao)
+            assert t.accuracy <= 1e-3
+            sl = slice(offs[r], offs[r + 1])
+            p = O.make_params(boxes[r], list(t.mesh), t.cao, t.alpha, t.r_cut, prefs[r])
+            fk, ek, _ = O.p3m_kspace(p, pos[sl], q[sl])
+            fr, er, _, _ = O.short_range(p, pos[sl], q[sl], None, 1, tab)
+            ref = fk + fr
+            scale = np.abs(ref).max()
+            np.testing.assert_allclose(f[sl], ref, atol=3e-5 * scale, rtol=0)
+            e_ref = ek + er[0] + er[1]
+            assert abs(en[r] - e_ref) <= 1e-4 * (abs(e_ref) + np.abs(ek) + 1.0)
+        assert len(caos) == 1  # one cao per batch
+    finally:
+        lib.p3mx_batch_destroy(h)
+
+
+def test_batch_langevin_run_is_reproducible_and_thermalises():
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas(seed=9, n_rep=3)
+    outs = []
+    for _ in range(2):
+        h = create(boxes, prefs, pos, q, offs)
+        try:
+            assert lib.p3mx_batch_run(h, 400, 0.005, 1.0, 1.0, 1234) == 0
+            x = np.zeros_like(pos)
+            v = np.zeros_like(pos)
+            assert lib.p3mx_batch_get(h, x.ctypes.data_as(_P(ctypes.c_double)), None,
+                                      v.ctypes.data_as(_P(ctypes.c_double))) == 0
+            outs.append((x, v))
+        finally:
+            lib.p3mx_batch_destroy(h)
+    # same seed and inputs: bitwise identical trajectories
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    x, v = outs[0]
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(v))
+    # equipartition within sampling noise: <v^2> per component ~ kT
+    assert 0.8 < np.mean(v ** 2) < 1.2
+
+
+def test_batch_rejects_bad_descriptors():
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas(n_rep=2)
+    with pytest.raises(RuntimeError, match="prefactor"):
+        create(boxes, -prefs, pos, q, offs)
+    bad = boxes.copy()
+    bad[0, 1] *= 1.1
+    with pytest.raises(RuntimeError, match="cubic"):
+        create(bad, prefs, pos, q, offs)
+    del lib
