@@ -103,6 +103,8 @@ SIGNATURES = {
     "p3mx_batch_forces": (ctypes.c_int, [_vp, _dp]),
     "p3mx_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_ulonglong]),
+    "p3mx_batch_stream": (ctypes.c_void_p, [_vp]),
+    "p3mx_batch_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "p3mx_batch_get": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
 }
 

@@ -124,6 +124,7 @@ __global__ void k_ks_error_batch(const int2 *__restrict__ mc, const double *__re
 
 struct p3mx_batch {
   p3mx_batch_desc d{};
+  long long graph_nodes = 0, graph_launches = 0;
   std::vector<double> box, pref;
   std::vector<long long> off;
   std::vector<int> n_charged;
@@ -580,6 +581,9 @@ int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT, double gamma,
       k_vv_step2<<<ceil_div(n3, 256), 256, 0, st>>>(b->vel.as<double>(), e.d_force(), n3, dt);
       k_step_inc<<<1, 1, 0, st>>>(stp);
       P3MX_CUDA(cudaStreamEndCapture(st, &gr));
+      size_t nodes = 0;
+      P3MX_CUDA(cudaGraphGetNodes(gr, nullptr, &nodes));
+      b->graph_nodes = static_cast<long long>(nodes);
       P3MX_CUDA(cudaGraphInstantiate(&b->graph, gr, 0));
       cudaGraphDestroy(gr);
       b->g_dt = dt;
@@ -589,10 +593,24 @@ int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT, double gamma,
     }
     for (int s = 0; s < steps; ++s)
       P3MX_CUDA(cudaGraphLaunch(b->graph, st));
+    b->graph_launches += steps;
     P3MX_CUDA(cudaStreamSynchronize(st));
     if (e.list_overflow(st))
       throw Error(P3MX_ERUNTIME, "Verlet list capacity exceeded during the graph run");
   });
+}
+
+void *p3mx_batch_stream(const p3mx_batch *b) {
+  return (b && b->eng) ? static_cast<void *>(b->eng->stream()) : nullptr;
+}
+
+int p3mx_batch_launch_count(const p3mx_batch *b, long long *count) {
+  if (!b || !count || !b->eng)
+    return P3MX_EHANDLE;
+  // kernel nodes of the captured step (memset nodes included) times launches,
+  // plus the kernels launched outside graphs
+  *count = b->eng->launches() + b->graph_nodes * b->graph_launches;
+  return P3MX_OK;
 }
 
 int p3mx_batch_get(p3mx_batch *b, double *pos, double *f, double *vel) {

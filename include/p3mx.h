@@ -233,6 +233,11 @@ int p3mx_batch_forces(p3mx_batch *b, double *energy_out);
  * in a CUDA graph after the first step.  Positions stay FP64 on device. */
 int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT,
                    double gamma, unsigned long long seed);
+/* The CUDA stream (cudaStream_t) the batch launches its work and graphs on,
+ * for callers that time or order work around p3mx_batch_run. */
+void *p3mx_batch_stream(const p3mx_batch *b);
+/* Kernels launched by the batch so far (graph launches count their nodes). */
+int p3mx_batch_launch_count(const p3mx_batch *b, long long *count);
 /* Copy positions / forces (3*N doubles, host) of all replicas. */
 int p3mx_batch_get(p3mx_batch *b, double *pos, double *f, double *vel);
 
