@@ -84,6 +84,10 @@ struct RepGeom {
   double inv_cs[3];
   long long cell_off;
   double max_cut, skin, coulomb_cut;
+  // Verlet list of this replica: neighbour k of particle p0+i at
+  // nb[nb_off + k*np + i], capacity max_nb per particle
+  long long nb_off;
+  int max_nb;
 };
 
 inline int ceil_div(long long a, long long b) {

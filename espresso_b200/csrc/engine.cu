@@ -126,6 +126,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_n = n_total;
   int const R = static_cast<int>(conf.size());
   m_geom.assign(R, RepGeom{});
+  m_cap.clear();
   // twiddle tables for every distinct axis length
   std::map<int, int> tw_off;
   std::vector<std::complex<double>> tw;
@@ -354,7 +355,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_stype.ensure(n * sizeof(int));
   m_scell.ensure(n * sizeof(int));
   m_nb_cnt.ensure(n * sizeof(int));
-  m_overflow.ensure(sizeof(int));
+  m_overflow.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_flag.ensure(sizeof(int));
   m_pos_ref.ensure(3 * n * sizeof(double));
   m_part_pair.ensure(static_cast<size_t>(m_n_blk_pair) * 20 * sizeof(double));
@@ -508,7 +509,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   mark("fft_inv_yz", st);
   // 6. force back-interpolation
   if (m_n > 0) {
-    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P, R><<<nb, 256, 0, st>>>(
+    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P, R><<<ceil_div(8 * m_n, 256), 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
                                m_W.as<Real>(), m_E.as<Real>(), d_q(), m_dipole.as<double>(),
                                m_n, f, overwrite ? 1 : 0)));
@@ -578,31 +579,29 @@ void Engine::build_lists(cudaStream_t st) {
             m_cperm.as<int>(), m_cells, st);
   k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
                                     m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr); ++m_launches;
-  if (m_max_nb == 0) {
-    // neighbour estimate from the densest replica plus margin
-    double est = 16.0;
-    for (auto const &G : m_geom) {
-      double const rc = G.max_cut + G.skin;
-      double const rho = G.np / G.V;
-      est = std::max(est, 1.5 * 4.18879 * rc * rc * rc * rho + 32.0);
-    }
-    m_max_nb = static_cast<int>(est);
-  }
+  if (m_cap.size() != m_geom.size())
+    set_list_capacity(1.5);
+  int const R = n_rep();
   for (int attempt = 0; attempt < 4; ++attempt) {
-    m_nb.ensure(static_cast<size_t>(m_max_nb) * std::max<long long>(1, m_n) * sizeof(int));
-    P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, sizeof(int), st));
+    P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, R * sizeof(int), st));
     k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
-                                       m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
+                                       m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                        m_overflow.as<int>(), nullptr); ++m_launches;
-    int ov = 0;
-    P3MX_CUDA(cudaMemcpyAsync(&ov, m_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    std::vector<int> ov(R);
+    P3MX_CUDA(cudaMemcpyAsync(ov.data(), m_overflow.p, R * sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
-    if (ov == 0)
+    bool grown = false;
+    for (int r = 0; r < R; ++r)
+      if (ov[r] > 0) {
+        m_cap[r] = ov[r] + ov[r] / 4 + 16;
+        grown = true;
+      }
+    if (!grown)
       break;
-    m_max_nb = ov + ov / 4 + 16;
     if (attempt == 3)
       throw Error(2, "Verlet list overflow");
+    layout_lists(st);
   }
   P3MX_CUDA(cudaMemcpyAsync(m_pos_ref.p, d_pos(), 3 * m_n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   m_lists_valid = true;
@@ -718,7 +717,7 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
                                     m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
   k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
-                                     m_ntypes, m_n, m_max_nb, m_nb.as<int>(), m_nb_cnt.as<int>(),
+                                     m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                      m_overflow.as<int>(), flag); ++m_launches;
   k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag); ++m_launches;
   refresh_sorted_positions(st);
@@ -737,26 +736,44 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
 }
 
 int Engine::list_overflow(cudaStream_t st) {
-  int ov = 0;
-  P3MX_CUDA(cudaMemcpyAsync(&ov, m_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  std::vector<int> ov(std::max(1, n_rep()));
+  P3MX_CUDA(cudaMemcpyAsync(ov.data(), m_overflow.p, ov.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));
-  return ov;
+  return *std::max_element(ov.begin(), ov.end());
+}
+
+// Per-replica neighbour capacity from the densest local estimate
+// margin * 4/3 pi (max_cut + skin)^3 rho + 48, never shrinking an existing one.
+void Engine::set_list_capacity(double margin) {
+  int const R = n_rep();
+  m_cap.resize(R, 0);
+  for (int r = 0; r < R; ++r) {
+    auto const &G = m_geom[r];
+    double const rc = G.max_cut + G.skin;
+    double const est = margin * 4.18879 * rc * rc * rc * (G.np / G.V) + 48.0;
+    m_cap[r] = std::max(m_cap[r], static_cast<int>(std::min(est, double(std::max<long long>(G.np, 1)))) + 1);
+  }
+  layout_lists(m_stream);
+}
+
+void Engine::layout_lists(cudaStream_t st) {
+  long long off = 0;
+  for (int r = 0; r < n_rep(); ++r) {
+    m_geom[r].nb_off = off;
+    m_geom[r].max_nb = m_cap[r];
+    off += static_cast<long long>(m_cap[r]) * m_geom[r].np;
+  }
+  m_nb.ensure(static_cast<size_t>(std::max<long long>(off, 1)) * sizeof(int));
+  upload_vec(m_geom_d, m_geom, st);
+  m_lists_valid = false;
 }
 
 void Engine::ensure_lists(cudaStream_t st, double nb_margin) {
-  int want = m_max_nb;
-  if (nb_margin > 1.0) {
-    double est = 16.0;
-    for (auto const &G : m_geom) {
-      double const rc = G.max_cut + G.skin;
-      est = std::max(est, nb_margin * 4.18879 * rc * rc * rc * (G.np / G.V) + 48.0);
-    }
-    want = std::max(want, static_cast<int>(est));
-  }
-  if (want != m_max_nb) {
-    m_max_nb = want;
+  std::vector<int> before = m_cap;
+  if (m_cap.size() != m_geom.size() || nb_margin > 1.0)
+    set_list_capacity(std::max(nb_margin, 1.5));
+  if (m_cap != before)
     m_lists_valid = false;
-  }
   if (!m_lists_valid)
     build_lists(st);
 }
@@ -781,21 +798,25 @@ std::vector<int> Engine::cell_index_ghost(cudaStream_t st) {
 std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
   build_lists(st);
   std::vector<int> cnt(m_n), perm(m_n);
-  std::vector<int> nbh(static_cast<size_t>(m_max_nb) * m_n);
+  long long total = 0;
+  for (auto const &G : m_geom)
+    total += static_cast<long long>(G.max_nb) * G.np;
+  std::vector<int> nbh(total);
   P3MX_CUDA(cudaMemcpyAsync(cnt.data(), m_nb_cnt.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaMemcpyAsync(perm.data(), m_cperm.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaMemcpyAsync(nbh.data(), m_nb.p, nbh.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));
   std::vector<int> pairs;
-  for (long long a = 0; a < m_n; ++a)
-    for (int k = 0; k < cnt[a]; ++k) {
-      int const b = nbh[static_cast<size_t>(k) * m_n + a];
-      int const i = perm[a], j = perm[b];
-      if (i < j) {
-        pairs.push_back(i);
-        pairs.push_back(j);
+  for (auto const &G : m_geom)
+    for (long long a = G.p0; a < G.p0 + G.np; ++a)
+      for (int k = 0; k < cnt[a]; ++k) {
+        int const b = nbh[G.nb_off + static_cast<long long>(k) * G.np + (a - G.p0)];
+        int const i = perm[a], j = perm[b];
+        if (i < j) {
+          pairs.push_back(i);
+          pairs.push_back(j);
+        }
       }
-    }
   return pairs;
 }
 

@@ -131,6 +131,8 @@ private:
   template <typename Real> void short_range_t(double *f, bool overwrite, bool want_ev,
                                               cudaStream_t st);
   void build_lists(cudaStream_t st);
+  void set_list_capacity(double margin);
+  void layout_lists(cudaStream_t st);
   void refresh_sorted_positions(cudaStream_t st);
   void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
                  cudaStream_t st, const int *cond = nullptr);
@@ -173,7 +175,7 @@ private:
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_stype, m_scell;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_part_pair, m_sums_pair;
-  int m_max_nb = 0;
+  std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;
   // misc host staging
   DevBuf m_ks_part;

@@ -218,10 +218,15 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     out[j] = acc[j] + comp[j];
 }
 
-// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373):
-// reads the packed (Ex, Ey, Ez, 0) field mesh; per sorted particle F -= prefactor/V * sum_{stencil} (q wx wy wz) E, FP32
-// row sums accumulated in FP64; plus the dipole term for epsilon != 0
-// (p3m.cpp:540-547).  Writes (or adds) to f[3*i] of the original index.
+// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373).
+// Eight lanes serve one corner-sorted particle: lane kz owns the stencil
+// z-offset kz and walks the P^2 (x, y) rows, so the lanes of a group read
+// P consecutive (Ex, Ey, Ez, 0) records of one row together (one or two
+// cache lines per group instead of one line per lane).  Lane sums are FP32
+// over the P^2 rows; the group reduction is FP64 in a fixed shuffle order.
+// F -= prefactor/V * sum (q wx wy wz) E, plus the dipole term for
+// epsilon != 0 (p3m.cpp:540-547).  Writes (or adds) f[3*i] of the original
+// particle index.
 template <typename Real, int P, int R>
 __global__ void __launch_bounds__(256)
 k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
@@ -229,60 +234,65 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
              const Real *__restrict__ W, const Real *__restrict__ E,
              const double *__restrict__ q, const double *__restrict__ dipole,
              long long n, double *__restrict__ f, int overwrite) {
-  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= n)
-    return;
-  int const i = perm[s];
-  int const r = rep_of[i];
-  RepGeom const &G = reps[r];
-  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-  int const loc = s_key[s];
-  int const cz = loc % M2;
-  int const cy = (loc / M2) % M1;
-  int const cx = loc / (M1 * M2);
-  Real wv[3 * P];
-  const Real *w = W + s * wstride<P, R>();
-#pragma unroll
-  for (int k = 0; k < 2 * P; ++k)
-    wv[k] = w[k];
-#pragma unroll
-  for (int k = 0; k < P; ++k)
-    wv[2 * P + k] = w[wz_off<P, R>() + k];
-  int zi[P];
-#pragma unroll
-  for (int k = 0; k < P; ++k) {
-    int z = cz + k;
-    zi[k] = (z >= M2) ? z - M2 : z;
+  static_assert(P <= 8, "one lane per stencil z offset");
+  long long const s = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+  int const kz = threadIdx.x & 7;
+  bool const live = s < n;
+  int i = 0, r = 0;
+  if (live) {
+    i = perm[s];
+    r = rep_of[i];
   }
-  using R4 = typename Real4Of<Real>::type;
-  const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off;
-  double fx = 0.0, fy = 0.0, fz = 0.0;
+  RepGeom const &G = reps[r];
+  Real ax = Real(0), ay = Real(0), az = Real(0);
+  if (live && kz < P) {
+    int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+    int const loc = s_key[s];
+    int const cz = loc % M2;
+    int const cy = (loc / M2) % M1;
+    int const cx = loc / (M1 * M2);
+    const Real *w = W + s * wstride<P, R>();
+    Real wx[P], wy[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      wx[k] = w[k];
+      wy[k] = w[P + k];
+    }
+    Real const wzk = w[wz_off<P, R>() + kz];
+    int z = cz + kz;
+    if (z >= M2)
+      z -= M2;
+    using R4 = typename Real4Of<Real>::type;
+    const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off + z;
 #pragma unroll 1
-  for (int kx = 0; kx < P; ++kx) {
-    int gx = cx + kx;
-    if (gx >= M0)
-      gx -= M0;
+    for (int kx = 0; kx < P; ++kx) {
+      int gx = cx + kx;
+      if (gx >= M0)
+        gx -= M0;
+      Real const wxz = wx[kx] * wzk;
+      long long const xrow = static_cast<long long>(gx) * M1;
 #pragma unroll
-    for (int ky = 0; ky < P; ++ky) {
-      int gy = cy + ky;
-      if (gy >= M1)
-        gy -= M1;
-      long long const row = (static_cast<long long>(gx) * M1 + gy) * M2;
-      Real const wxy = wv[kx] * wv[P + ky];
-      Real ax = Real(0), ay = Real(0), az = Real(0);
-#pragma unroll
-      for (int kz = 0; kz < P; ++kz) {
-        R4 const e = E4[row + zi[kz]];
-        Real const wt = wxy * wv[2 * P + kz];
+      for (int ky = 0; ky < P; ++ky) {
+        int gy = cy + ky;
+        if (gy >= M1)
+          gy -= M1;
+        R4 const e = E4[(xrow + gy) * M2];
+        Real const wt = wxz * wy[ky];
         ax += wt * e.x;
         ay += wt * e.y;
         az += wt * e.z;
       }
-      fx += static_cast<double>(ax);
-      fy += static_cast<double>(ay);
-      fz += static_cast<double>(az);
     }
   }
+  double fx = static_cast<double>(ax), fy = static_cast<double>(ay), fz = static_cast<double>(az);
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (!live || kz != 0)
+    return;
   double const pref = G.prefactor / G.V;
   double ox = -pref * fx, oy = -pref * fy, oz = -pref * fz;
   if (G.epsilon != 0.0) {

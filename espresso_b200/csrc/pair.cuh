@@ -86,19 +86,25 @@ __device__ inline double mi_d(double dx, double L, double Li) {
 // partners b != a in the 27 (unique) neighbour cells with the
 // VerletCriterion (VerletCriterion.hpp:68-97): d^2 <= (max_cut+skin)^2 and
 // (both charged and d^2 <= (r_cut+skin)^2, or the type pair is active and
-// d^2 <= (ia_cut+skin)^2).  Neighbour k of a is stored at nb[k*n + a].
+// d^2 <= (ia_cut+skin)^2).  Neighbour k of a is stored at
+// nb[G.nb_off + k*G.np + (a - G.p0)] (per-replica capacity G.max_nb); a
+// replica whose capacity is exceeded reports its largest count in
+// overflow[replica].
 __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
                                const double4 *__restrict__ spq, const int *__restrict__ stype,
                                const int *__restrict__ scell, const int *__restrict__ cstart,
                                const PairIA *__restrict__ ia, int ntypes, long long n,
-                               int max_nb, int *__restrict__ nb, int *__restrict__ nb_cnt,
+                               int *__restrict__ nb, int *__restrict__ nb_cnt,
                                int *__restrict__ overflow, const int *__restrict__ cond) {
   if (cond && !*cond)
     return;
   long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (a >= n)
     return;
-  RepGeom const &G = reps[rep_of_sorted[a]];
+  int const rep = rep_of_sorted[a];
+  RepGeom const &G = reps[rep];
+  int const max_nb = G.max_nb;
+  int *nbp = nb + G.nb_off + (a - G.p0);
   double4 const pa = spq[a];
   int const ta = stype[a];
   int const loc = scell[a] - static_cast<int>(G.cell_off);
@@ -143,7 +149,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
           }
           if (take) {
             if (count < max_nb)
-              nb[static_cast<long long>(count) * n + a] = b;
+              nbp[static_cast<long long>(count) * G.np] = b;
             ++count;
           }
         }
@@ -152,7 +158,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
   }
   nb_cnt[a] = min(count, max_nb);
   if (count > max_nb)
-    atomicMax(overflow, count);
+    atomicMax(&overflow[rep], count);
 }
 
 // A&S 7.1.26 approximation of exp(d^2) erfc(d), as the reference's real-
@@ -218,7 +224,7 @@ __device__ inline void lj_wca(PairR<Real> const &p, Real dist, Real inv_d, Real 
 // Pair kernel over the Verlet list: real-space Coulomb
 // (CoulombP3M::pair_force / pair_energy, p3m.hpp:146-180) plus LJ and WCA
 // (lj.hpp:41-60, wca.hpp:39-55).  Minimum-image difference in FP64, pair
-// arithmetic in Real, per-particle accumulation in Real (no atomics: each
+// arithmetic in Real, per-particle accumulation in FP64 (no atomics: each
 // particle owns its force, full list).  EV adds energies and virials: each
 // pair is seen from both ends, so per-particle sums are halved; per-block
 // FP64 partials {E_coul, E_nb, Vc[9], Vn[9]} (width 20).  Blocks map to
@@ -254,22 +260,23 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     Real const pref_qa = static_cast<Real>(G.prefactor * pa.w);
     bool const one_type = (ntypes == 1);
     PairR<Real> const p0(ia[0]);
-    Real fx = Real(0), fy = Real(0), fz = Real(0);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
     int const cnt = nb_cnt[a];
-    const int *nbp = nb + a;
+    const int *nbp = nb + G.nb_off + (a - G.p0);
     int b_next = (cnt > 0) ? nbp[0] : 0;
     double4 p_next = (cnt > 0) ? spq[b_next] : pa;
     for (int k = 0; k < cnt; ++k) {
       int const b = b_next;
       double4 const pb = p_next;
       if (k + 1 < cnt) {
-        b_next = nbp[static_cast<long long>(k + 1) * n];
+        b_next = nbp[static_cast<long long>(k + 1) * G.np];
         p_next = spq[b_next];
       }
-      Real const d0 = static_cast<Real>(mi_d(pa.x - pb.x, L0, Li0));
-      Real const d1 = static_cast<Real>(mi_d(pa.y - pb.y, L1, Li1));
-      Real const d2v = static_cast<Real>(mi_d(pa.z - pb.z, L2, Li2));
-      Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
+      // geometry in FP64 (two conversions per pair instead of four)
+      double const d0 = mi_d(pa.x - pb.x, L0, Li0);
+      double const d1 = mi_d(pa.y - pb.y, L1, Li1);
+      double const d2v = mi_d(pa.z - pb.z, L2, Li2);
+      Real const dist2 = static_cast<Real>(d0 * d0 + d1 * d1 + d2v * d2v);
       Real const inv_d = rsqrt_r(dist2);
       Real const dist = dist2 * inv_d;
       Real fc = Real(0), ec = Real(0);
@@ -296,12 +303,12 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
         if (p.active)
           lj_wca(p, dist, inv_d, fn, en);
       }
-      Real const ft = fc + fn;
+      double const ft = static_cast<double>(fc + fn);
       fx += ft * d0;
       fy += ft * d1;
       fz += ft * d2v;
       if constexpr (EV) {
-        double const dd[3] = {double(d0), double(d1), double(d2v)};
+        double const dd[3] = {d0, d1, d2v};
         ev[0] += 0.5 * double(ec);
         ev[1] += 0.5 * double(en);
 #pragma unroll
@@ -315,13 +322,13 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     }
     int const i = perm[a];
     if (overwrite) {
-      f[3 * i + 0] = double(fx);
-      f[3 * i + 1] = double(fy);
-      f[3 * i + 2] = double(fz);
+      f[3 * i + 0] = fx;
+      f[3 * i + 1] = fy;
+      f[3 * i + 2] = fz;
     } else {
-      f[3 * i + 0] += double(fx);
-      f[3 * i + 1] += double(fy);
-      f[3 * i + 2] += double(fz);
+      f[3 * i + 0] += fx;
+      f[3 * i + 1] += fy;
+      f[3 * i + 2] += fz;
     }
   }
   if constexpr (EV) {
