@@ -76,7 +76,10 @@ struct RepGeom {
   int hp;  // padded length of the r2c axis (>= mesh[2]/2+1, multiple of 4)
   int cao;
   long long p0, np;  // particle range
-  long long rm_off;  // real mesh / corner-bin offset (elements)
+  long long rm_off;  // real mesh offset (elements)
+  long long bin_off; // corner-bin (sort key) offset: bricks of brick^3 bins
+  int brick;         // brick edge (corner units) of the charge assignment
+  int nbx, nby, nbz; // bricks per dimension
   long long km_off;  // complex half mesh offset (elements)
   AxisPlan plan[3];
   // short-range cell system

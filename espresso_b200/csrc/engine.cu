@@ -143,7 +143,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   double max_ia = -1.0;
   for (auto const &e : m_ia)
     max_ia = std::max(max_ia, e.ia_cut);
-  m_bins = m_cplx = m_cells = 0;
+  m_bins = m_cplx = m_cells = m_nkeys = 0;
   for (int r = 0; r < R; ++r) {
     auto const &c = conf[r];
     auto &G = m_geom[r];
@@ -172,6 +172,13 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       G.plan[d] = make_plan(c.mesh[d], twoff(c.mesh[d]));
     }
     G.hp = ((c.mesh[2] / 2 + 1) + 3) / 4 * 4;
+    // assignment bricks: edge >= cao-1 so that same-colour tiles never overlap
+    G.brick = (c.cao <= 5) ? 4 : 8;
+    G.nbx = (c.mesh[0] + G.brick - 1) / G.brick;
+    G.nby = (c.mesh[1] + G.brick - 1) / G.brick;
+    G.nbz = (c.mesh[2] + G.brick - 1) / G.brick;
+    G.bin_off = m_nkeys;
+    m_nkeys += static_cast<long long>(G.nbx) * G.nby * G.nbz * G.brick * G.brick * G.brick;
     G.rm_off = m_bins;
     G.km_off = m_cplx;
     m_bins += static_cast<long long>(c.mesh[0]) * c.mesh[1] * c.mesh[2];
@@ -189,7 +196,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     G.cell_off = m_cells;
     m_cells += static_cast<long long>(G.cg[0]) * G.cg[1] * G.cg[2];
   }
-  if (m_bins >= (1LL << 31) || m_n >= (1LL << 31))
+  if (m_nkeys >= (1LL << 31) || m_bins >= (1LL << 31) || m_n >= (1LL << 31))
     throw Error(1, "batch too large for 32-bit bin/particle indices");
   cudaStream_t st = m_stream;
   upload_vec(m_geom_d, m_geom, st);
@@ -228,8 +235,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     for (int r = 0; r < R; ++r) {
       long long const ms = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].mesh[2];
       long long const cs2 = static_cast<long long>(m_geom[r].mesh[0]) * m_geom[r].mesh[1] * m_geom[r].hp;
-      for (int b = 0; b < ceil_div(ms / m_run, 256); ++b)
-        bm.push_back(int2{r, b});
+      (void)ms;
       for (int b = 0; b < ceil_div(cs2, 256); ++b)
         bc.push_back(int2{r, b});
       for (int b = 0; b < std::max(1, ceil_div(conf[r].np, 2048)); ++b)
@@ -238,6 +244,28 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       for (int b = 0; b < std::max(1, ceil_div(conf[r].np, 256)); ++b)
         bp.push_back(int2{r, b});
       m_blk_pair_start.push_back(static_cast<int>(bp.size()));
+    }
+    // bricks of the assignment grouped by colour (3 colours per dimension)
+    {
+      std::vector<std::vector<int2>> phase(27);
+      auto colour = [](int b, int nb) { return (nb % 2 == 1 && nb > 1 && b == nb - 1) ? 2 : b % 2; };
+      m_tile_cap = 1;
+      for (int r = 0; r < R; ++r) {
+        auto const &G = m_geom[r];
+        int const E = G.brick + G.cao - 1;
+        m_tile_cap = std::max(m_tile_cap, E * E * E);
+        for (int bx = 0; bx < G.nbx; ++bx)
+          for (int by = 0; by < G.nby; ++by)
+            for (int bz = 0; bz < G.nbz; ++bz) {
+              int const p = colour(bx, G.nbx) + 3 * (colour(by, G.nby) + 3 * colour(bz, G.nbz));
+              phase[p].push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
+            }
+      }
+      m_phase_off.assign(1, 0);
+      for (auto const &ph : phase) {
+        bm.insert(bm.end(), ph.begin(), ph.end());
+        m_phase_off.push_back(static_cast<int>(bm.size()));
+      }
     }
     m_n_blk_mesh = static_cast<int>(bm.size());
     m_n_blk_cplx = static_cast<int>(bc.size());
@@ -306,6 +334,22 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(limit)));
     };
+    {
+      // assignment tiles: 2 (hi, lo) x (brick + cao - 1)^3 per warp
+      auto aset = [&](auto kern) {
+        P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(limit)));
+      };
+      if (m_fp32) {
+        aset(k_p3m_assign<float, 1>); aset(k_p3m_assign<float, 2>); aset(k_p3m_assign<float, 3>);
+        aset(k_p3m_assign<float, 4>); aset(k_p3m_assign<float, 5>); aset(k_p3m_assign<float, 6>);
+        aset(k_p3m_assign<float, 7>);
+      } else {
+        aset(k_p3m_assign<double, 1>); aset(k_p3m_assign<double, 2>); aset(k_p3m_assign<double, 3>);
+        aset(k_p3m_assign<double, 4>); aset(k_p3m_assign<double, 5>); aset(k_p3m_assign<double, 6>);
+        aset(k_p3m_assign<double, 7>);
+      }
+    }
     if (m_fp32) {
       attr(k_fft_z_fwd<float>, m_smem_zf);
       attr(k_fft_y<float>, m_smem_y);
@@ -328,12 +372,11 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_key.ensure(n * sizeof(int));
   m_slot.ensure(n * sizeof(int));
   m_perm.ensure(n * sizeof(int));
-  m_cnt.ensure((m_bins + 1) * sizeof(int));
-  m_start.ensure((m_bins + 1) * sizeof(int));
-  m_scan_tiles.ensure((ceil_div(std::max(m_bins, m_cells) + 1, kScanTile) + 1) * sizeof(int));
+  m_cnt.ensure((m_nkeys + 1) * sizeof(int));
+  m_start.ensure((m_nkeys + 1) * sizeof(int));
+  m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
   m_W.ensure((3 * 7 + 2 * 3) * n * rsz);
-  m_scz.ensure(n * sizeof(int));
   m_skey.ensure(n * sizeof(int));
   m_rho.ensure(m_bins * rsz);
   m_E.ensure(4 * m_bins * rsz);
@@ -456,28 +499,38 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   }
   mark("start", st);
   // 1. corner binning + deterministic counting sort
-  P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_bins + 1) * sizeof(int), st));
+  P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_nkeys + 1) * sizeof(int), st));
   int const nb = ceil_div(m_n, 256);
   if (m_n > 0) {
     k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
                                         m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>()); ++m_launches;
     sort_keys(m_key.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
-              m_perm.as<int>(), m_bins, st);
+              m_perm.as<int>(), m_nkeys, st);
     mark("p3m_sort", st);
     P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P, R><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
-                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_scz.as<int>(),
-                               m_skey.as<int>())));
+                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_skey.as<int>())));
     ++m_launches;
     mark("p3m_weights", st);
   } else {
-    P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_bins + 1) * sizeof(int), st));
+    P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_nkeys + 1) * sizeof(int), st));
   }
-  // 2. gather-based charge assignment
-  P3MX_CAO_DISPATCH(cao, (k_p3m_assign<Real, P, R><<<m_n_blk_mesh, 256, 0, st>>>(
-                             geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
-                             m_scz.as<int>(), m_rho.as<Real>())));
-  ++m_launches;
+  // 2. charge assignment: one warp per brick, colour by colour
+  P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
+  {
+    int const wpb = (sizeof(Real) == 4) ? 4 : 2;
+    size_t const smem = static_cast<size_t>(wpb) * 2 * m_tile_cap * sizeof(Real);
+    for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
+      int const cnt = m_phase_off[p + 1] - m_phase_off[p];
+      if (cnt == 0)
+        continue;
+      int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
+      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<ceil_div(cnt, wpb), 32 * wpb, smem, st>>>(
+                                   geom, tab, cnt, m_tile_cap, m_start.as<int>(), m_W.as<Real>(),
+                                   m_skey.as<int>(), m_rho.as<Real>())));
+      ++m_launches;
+    }
+  }
   mark("p3m_assign", st);
   // 3. forward FFT z (r2c) and y
   C const *tw = m_tw.as<C>();

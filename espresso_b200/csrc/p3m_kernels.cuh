@@ -47,7 +47,9 @@ __device__ inline void bspline_weights(Real x, Real *w) {
 // Per particle: nearest-mesh-point corner and the distance to it, following
 // p3m_calculate_interpolation_weights (p3m/interpolation.hpp:138-178) with
 // the single-rank CA-mesh origin of P3MLocalMesh (p3m/common.cpp:34-106).
-// key = corner bin (replica mesh offset + (cx*M1+cy)*M2+cz).
+// key = corner bin, brick-major: bin_off + brick*B^3 + (lx*B + ly)*B + lz
+// with brick = (bx*nby + by)*nbz + bz and (lx, ly, lz) the corner inside it,
+// so the particles of one brick form one contiguous range of the sorted order.
 template <typename Real>
 __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                           const double *__restrict__ pos, long long n,
@@ -70,7 +72,10 @@ __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restric
     g[d] = c;
     dist[3 * i + d] = static_cast<Real>(ds);
   }
-  int const k = static_cast<int>(G.rm_off) + (g[0] * G.mesh[1] + g[1]) * G.mesh[2] + g[2];
+  int const B = G.brick;
+  int const brick = ((g[0] / B) * G.nby + g[1] / B) * G.nbz + g[2] / B;
+  int const k = static_cast<int>(G.bin_off) + brick * B * B * B +
+                ((g[0] % B) * B + g[1] % B) * B + g[2] % B;
   key[i] = k;
   slot[i] = atomicAdd(&cnt[k], 1);
 }
@@ -82,14 +87,13 @@ __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restric
 template <int P, int R> __host__ __device__ constexpr int wstride() { return 3 * P + 2 * (R - 1); }
 template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
 
-// Weights in corner-sorted order; also the z corner and the corner key of
-// every sorted particle.
+// Weights in corner-sorted order; also the brick-local corner key of every
+// sorted particle.
 template <typename Real, int P, int R>
 __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
                               const int *__restrict__ key, const Real *__restrict__ dist,
                               const double *__restrict__ q, const int *__restrict__ rep_of,
-                              long long n, Real *__restrict__ W, int *__restrict__ s_cz,
-                              int *__restrict__ s_key) {
+                              long long n, Real *__restrict__ W, int *__restrict__ s_key) {
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
@@ -112,9 +116,7 @@ __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__res
     o[2 * P + k] = Real(0);
     o[wz_off<P, R>() + P + k] = Real(0);
   }
-  int const loc = key[i] - static_cast<int>(G.rm_off);
-  s_key[s] = loc;
-  s_cz[s] = loc % G.mesh[2];
+  s_key[s] = key[i] - static_cast<int>(G.bin_off);
 }
 
 // Two-sum (Knuth): exact error term of a + b, for compensated summation.
@@ -126,96 +128,112 @@ template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v
   c += err;
 }
 
-// Gather-based charge assignment.  One thread owns R consecutive mesh
-// points along z of one (x, y) line and sums, in a fixed order, the
-// contributions q*wx*wy*wz of every particle whose stencil covers them: for
-// each of the P^2 corner columns (x-kx, y-ky) the particles with z corners
-// in [z0-P+1, z0+R-1] form one contiguous range of the corner-sorted order
-// (two ranges across the periodic wrap), so a thread does 2 P^2 range
-// lookups for R points.  No atomics: the result is bitwise reproducible.
-// For FP32 the per-column partial sums are combined with compensated
-// (two-sum) accumulation.
-template <typename Real, int P, int R>
-__global__ void __launch_bounds__(256)
-k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
-             const int *__restrict__ start, const Real *__restrict__ W,
-             const int *__restrict__ s_cz, Real *__restrict__ rho) {
+// Corner (cx, cy, cz) of a brick-local key.
+__device__ inline void corner_of(RepGeom const &G, int loc, int &cx, int &cy, int &cz) {
+  int const B = G.brick, B3 = B * B * B;
+  int const brick = loc / B3, l = loc - brick * B3;
+  int const bz = brick % G.nbz, by = (brick / G.nbz) % G.nby, bx = brick / (G.nbz * G.nby);
+  cx = bx * B + l / (B * B);
+  cy = by * B + (l / B) % B;
+  cz = bz * B + l % B;
+}
+
+// Deterministic charge assignment, one warp per brick.  The particles of a
+// brick (corners in a B^3 block, one contiguous range of the brick-major
+// sorted order) are taken one at a time in sorted order; the 32 lanes cover
+// the particle's P^3 stencil points, each lane adding q*wx*wy*wz into the
+// brick's shared-memory tile ((B+P-1)^3 points) -- no two lanes of one
+// round touch the same point, so the tile needs no atomics and the sum order
+// is fixed.  Tile accumulation is compensated (two-sum hi/lo).  Tiles are
+// then added to the mesh; bricks of one launch share a colour (parity per
+// dimension, a third colour for the last brick of an odd count), so the
+// tiles of one launch never overlap and plain read-add-write is race-free;
+// colours run in a fixed order, making the mesh bitwise reproducible.
+template <typename Real, int P>
+__global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks,
+                             int nbricks, int tile_cap, const int *__restrict__ start,
+                             const Real *__restrict__ W, const int *__restrict__ s_key,
+                             Real *__restrict__ rho) {
+  constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
-  int2 const bk = blk[blockIdx.x];
+  constexpr int P3 = P * P * P;
+  constexpr int NR = (P3 + 31) / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const bi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (bi >= nbricks)
+    return; // whole warp
+  int2 const bk = bricks[bi];
   RepGeom const &G = reps[bk.x];
-  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-  int const runs = M2 / R;
-  long long const local = static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
-  if (local >= static_cast<long long>(M0) * M1 * runs)
-    return;
-  int const zr = static_cast<int>(local % runs);
-  int const gy = static_cast<int>((local / runs) % M1);
-  int const gx = static_cast<int>(local / (static_cast<long long>(runs) * M1));
-  int const z0 = zr * R;
-  int const z_lo = z0 - (P - 1);
-  int const z_hi = z0 + R - 1;
-  const int *st = start + G.rm_off;
-  Real acc[R], comp[R];
-#pragma unroll
-  for (int j = 0; j < R; ++j) {
-    acc[j] = Real(0);
-    comp[j] = Real(0);
+  int const B = G.brick, B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
+  Real *hi = reinterpret_cast<Real *>(smem_raw) + static_cast<long long>(warp) * 2 * tile_cap;
+  Real *lo = hi + tile_cap;
+  for (int t = lane; t < E3; t += 32) {
+    hi[t] = Real(0);
+    lo[t] = Real(0);
   }
-#pragma unroll 1
-  for (int kx = 0; kx < P; ++kx) {
-    int cx = gx - kx;
-    if (cx < 0)
-      cx += M0;
-#pragma unroll 1
-    for (int ky = 0; ky < P; ++ky) {
-      int cy = gy - ky;
-      if (cy < 0)
-        cy += M1;
-      int const row = (cx * M1 + cy) * M2;
-      // [wrap range with corners cz - M2 in [z_lo, 0)] + [main range]
-      int a0 = 0, a1 = 0;
-      if (z_lo < 0) {
-        a0 = st[row + M2 + z_lo];
-        a1 = st[row + M2];
-      }
-      int const b0 = st[row + max(z_lo, 0)];
-      int const b1 = st[row + z_hi + 1];
-      Real col[R];
+  // per-lane stencil point of each round and its tile offset
+  int off[NR], wi[NR], wj[NR], wk[NR];
 #pragma unroll
-      for (int j = 0; j < R; ++j)
-        col[j] = Real(0);
-      for (int s = a0; s < a1; ++s) {
-        const Real *w = W + static_cast<long long>(s) * WS;
-        int const d = s_cz[s] - M2 - z0;
-        Real const wxy = w[kx] * w[P + ky];
-        const Real *wz = w + WZ - d;
+  for (int r = 0; r < NR; ++r) {
+    int const t = lane + 32 * r;
+    int const tt = (t < P3) ? t : 0;
+    wi[r] = tt / (P * P);
+    wj[r] = (tt / P) % P;
+    wk[r] = tt % P;
+    off[r] = (wi[r] * E + wj[r]) * E + wk[r];
+  }
+  __syncwarp();
+  const int *st = start + G.bin_off;
+  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
+  for (int s = s0; s < s1; ++s) {
+    int const l = s_key[s] - bk.y * B3;
+    int const base = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
+    const Real *w = W + static_cast<long long>(s) * WS;
 #pragma unroll
-        for (int j = 0; j < R; ++j)
-          col[j] += wxy * wz[j];
-      }
-      for (int s = b0; s < b1; ++s) {
-        const Real *w = W + static_cast<long long>(s) * WS;
-        int const d = s_cz[s] - z0;
-        Real const wxy = w[kx] * w[P + ky];
-        const Real *wz = w + WZ - d;
-#pragma unroll
-        for (int j = 0; j < R; ++j)
-          col[j] += wxy * wz[j];
-      }
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        if constexpr (sizeof(Real) == 4)
-          two_sum(acc[j], comp[j], col[j]);
-        else
-          acc[j] += col[j];
+    for (int r = 0; r < NR; ++r) {
+      if (lane + 32 * r < P3) {
+        Real const v = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
+        int const idx = base + off[r];
+        Real h = hi[idx], c = lo[idx];
+        two_sum(h, c, v);
+        hi[idx] = h;
+        lo[idx] = c;
       }
     }
+    __syncwarp();
   }
-  Real *out = rho + G.rm_off + (static_cast<long long>(gx) * M1 + gy) * M2 + z0;
-#pragma unroll
-  for (int j = 0; j < R; ++j)
-    out[j] = acc[j] + comp[j];
+  // add the tile to the mesh: real extent of the brick plus the stencil
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
+  int const x0 = bx * B, y0 = by * B, z0 = bz * B;
+  int const ex = min(B, M0 - x0) + P - 1, ey = min(B, M1 - y0) + P - 1, ez = min(B, M2 - z0) + P - 1;
+  Real *mesh = rho + G.rm_off;
+  // a tile wider than the mesh maps two tile points onto one mesh point:
+  // add such points in separate passes (one per wrap class)
+  bool const self_wrap = (ex > M0) || (ey > M1) || (ez > M2);
+  int const passes = self_wrap ? 8 : 1;
+  int const n = ex * ey * ez;
+  for (int pass = 0; pass < passes; ++pass) {
+    for (int t = lane; t < n; t += 32) {
+      int const x = t / (ey * ez), y = (t / ez) % ey, z = t % ez;
+      int gx = x0 + x, gy = y0 + y, gz = z0 + z;
+      int cls = 0;
+      if (gx >= M0) { gx -= M0; cls |= 1; }
+      if (gx >= M0) gx -= M0;
+      if (gy >= M1) { gy -= M1; cls |= 2; }
+      if (gy >= M1) gy -= M1;
+      if (gz >= M2) { gz -= M2; cls |= 4; }
+      if (gz >= M2) gz -= M2;
+      if (self_wrap && cls != pass)
+        continue;
+      int const ti = (x * E + y) * E + z;
+      long long const g = (static_cast<long long>(gx) * M1 + gy) * M2 + gz;
+      mesh[g] += hi[ti] + lo[ti];
+    }
+    __syncwarp();
+  }
 }
 
 // Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373).
@@ -247,10 +265,8 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
   Real ax = Real(0), ay = Real(0), az = Real(0);
   if (live && kz < P) {
     int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-    int const loc = s_key[s];
-    int const cz = loc % M2;
-    int const cy = (loc / M2) % M1;
-    int const cx = loc / (M1 * M2);
+    int cx, cy, cz;
+    corner_of(G, s_key[s], cx, cy, cz);
     const Real *w = W + s * wstride<P, R>();
     Real wx[P], wy[P];
 #pragma unroll
