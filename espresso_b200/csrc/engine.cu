@@ -245,19 +245,53 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         bp.push_back(int2{r, b});
       m_blk_pair_start.push_back(static_cast<int>(bp.size()));
     }
-    // bricks of the assignment grouped by colour (3 colours per dimension)
+    // bricks of the assignment grouped by colour: per dimension, the tile
+    // intervals [bB, bB + min(B, M - bB) + cao - 1) on the periodic axis are
+    // coloured greedily so that intervals of one colour never intersect
+    // (modulo M); bricks sharing the colour triple then have disjoint tiles
     {
-      std::vector<std::vector<int2>> phase(27);
-      auto colour = [](int b, int nb) { return (nb % 2 == 1 && nb > 1 && b == nb - 1) ? 2 : b % 2; };
+      auto colours = [](int M, int B, int P) {
+        int const nb = (M + B - 1) / B;
+        std::vector<int> s(nb), e(nb), col(nb, -1);
+        for (int b = 0; b < nb; ++b) {
+          s[b] = b * B;
+          e[b] = s[b] + std::min(B, M - s[b]) + P - 1;
+        }
+        auto hit = [&](int a, int b) {
+          if (e[a] - s[a] >= M || e[b] - s[b] >= M)
+            return true;
+          for (int k = -1; k <= 1; ++k)
+            if (s[a] < e[b] + k * M && s[b] + k * M < e[a])
+              return true;
+          return false;
+        };
+        for (int b = 0; b < nb; ++b) {
+          std::vector<char> used(nb + 1, 0);
+          for (int a = 0; a < nb; ++a)
+            if (a != b && col[a] >= 0 && hit(a, b))
+              used[col[a]] = 1;
+          int c = 0;
+          while (used[c])
+            ++c;
+          col[b] = c;
+        }
+        return col;
+      };
+      std::vector<std::vector<int2>> phase;
       m_tile_cap = 1;
       for (int r = 0; r < R; ++r) {
         auto const &G = m_geom[r];
         int const E = G.brick + G.cao - 1;
         m_tile_cap = std::max(m_tile_cap, E * E * E);
+        auto const cxv = colours(G.mesh[0], G.brick, G.cao);
+        auto const cyv = colours(G.mesh[1], G.brick, G.cao);
+        auto const czv = colours(G.mesh[2], G.brick, G.cao);
         for (int bx = 0; bx < G.nbx; ++bx)
           for (int by = 0; by < G.nby; ++by)
             for (int bz = 0; bz < G.nbz; ++bz) {
-              int const p = colour(bx, G.nbx) + 3 * (colour(by, G.nby) + 3 * colour(bz, G.nbz));
+              int const p = cxv[bx] + 8 * (cyv[by] + 8 * czv[bz]);
+              if (static_cast<int>(phase.size()) <= p)
+                phase.resize(p + 1);
               phase[p].push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
             }
       }

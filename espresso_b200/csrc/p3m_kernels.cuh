@@ -191,15 +191,23 @@ __global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__res
     int const l = s_key[s] - bk.y * B3;
     int const base = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
     const Real *w = W + static_cast<long long>(s) * WS;
+    // all loads of the particle's rounds first (the rounds touch distinct
+    // tile points), then the compensated adds, then the stores
+    Real v[NR], h[NR], c[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      v[r] = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
+      h[r] = hi[base + off[r]];
+      c[r] = lo[base + off[r]];
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      two_sum(h[r], c[r], v[r]);
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       if (lane + 32 * r < P3) {
-        Real const v = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
-        int const idx = base + off[r];
-        Real h = hi[idx], c = lo[idx];
-        two_sum(h, c, v);
-        hi[idx] = h;
-        lo[idx] = c;
+        hi[base + off[r]] = h[r];
+        lo[base + off[r]] = c[r];
       }
     }
     __syncwarp();
@@ -214,23 +222,37 @@ __global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__res
   // add such points in separate passes (one per wrap class)
   bool const self_wrap = (ex > M0) || (ey > M1) || (ez > M2);
   int const passes = self_wrap ? 8 : 1;
-  int const n = ex * ey * ez;
+  // each lane owns fixed (y, z) slots of the tile's yz plane; loop over x
+  constexpr int EMAX = 8 + P - 1;
+  constexpr int NS = (EMAX * EMAX + 31) / 32;
+  int yzt[NS], yzg[NS], ycls[NS];
+  int const nyz = ey * ez;
+#pragma unroll
+  for (int k2 = 0; k2 < NS; ++k2) {
+    int const t = lane + 32 * k2;
+    int const y = (t < nyz) ? t / ez : 0, z = (t < nyz) ? t - (t / ez) * ez : 0;
+    int gy = y0 + y, gz = z0 + z, cls = 0;
+    if (gy >= M1) { gy -= M1; cls |= 2; }
+    if (gy >= M1) gy -= M1;
+    if (gz >= M2) { gz -= M2; cls |= 4; }
+    if (gz >= M2) gz -= M2;
+    yzt[k2] = (t < nyz) ? y * E + z : -1;
+    yzg[k2] = gy * M2 + gz;
+    ycls[k2] = cls;
+  }
   for (int pass = 0; pass < passes; ++pass) {
-    for (int t = lane; t < n; t += 32) {
-      int const x = t / (ey * ez), y = (t / ez) % ey, z = t % ez;
-      int gx = x0 + x, gy = y0 + y, gz = z0 + z;
-      int cls = 0;
-      if (gx >= M0) { gx -= M0; cls |= 1; }
+    for (int x = 0; x < ex; ++x) {
+      int gx = x0 + x, xcls = 0;
+      if (gx >= M0) { gx -= M0; xcls = 1; }
       if (gx >= M0) gx -= M0;
-      if (gy >= M1) { gy -= M1; cls |= 2; }
-      if (gy >= M1) gy -= M1;
-      if (gz >= M2) { gz -= M2; cls |= 4; }
-      if (gz >= M2) gz -= M2;
-      if (self_wrap && cls != pass)
-        continue;
-      int const ti = (x * E + y) * E + z;
-      long long const g = (static_cast<long long>(gx) * M1 + gy) * M2 + gz;
-      mesh[g] += hi[ti] + lo[ti];
+      long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+      for (int k2 = 0; k2 < NS; ++k2) {
+        if (yzt[k2] < 0 || (self_wrap && (xcls | ycls[k2]) != pass))
+          continue;
+        int const ti = x * E * E + yzt[k2];
+        mesh[gbase + yzg[k2]] += hi[ti] + lo[ti];
+      }
     }
     __syncwarp();
   }
