@@ -226,10 +226,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   size_t const cap = m_fp32 ? 4096 : 2048; // complex elements per smem buffer
   {
     std::vector<int2> bm, bc, bcen, bp;
-    m_run = 4;
-    for (int r = 0; r < R; ++r)
-      if (m_geom[r].mesh[2] % 4)
-        m_run = 2;
+    m_run = 4; // weight-record padding (R) used by every assignment/interp kernel
     m_blk_census_start.assign(1, 0);
     m_blk_pair_start.assign(1, 0);
     for (int r = 0; r < R; ++r) {
