@@ -3,6 +3,7 @@
 // host<->device staging.  No exception crosses the ABI.
 #include "../../include/p3mx.h"
 #include "engine.cuh"
+#include "host_pool.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -48,6 +49,34 @@ struct Pinned {
   template <typename T> T *as() { return static_cast<T *>(p); }
 };
 
+// Events marking the chunks of a pipelined device->host copy.
+struct ChunkEvents {
+  std::vector<cudaEvent_t> ev;
+  ~ChunkEvents() {
+    for (auto e : ev)
+      cudaEventDestroy(e);
+  }
+  cudaEvent_t get(size_t i) {
+    while (ev.size() <= i) {
+      cudaEvent_t e;
+      P3MX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev.push_back(e);
+    }
+    return ev[i];
+  }
+};
+
+// Chunk of the host<->device staging pipeline (bytes).
+constexpr size_t kStageChunk = size_t(4) << 20;
+
+// Process-wide host worker pool; calls from different handles take turns.
+HostPool &host_pool(std::unique_lock<std::mutex> &lk) {
+  static HostPool pool;
+  static std::mutex mu;
+  lk = std::unique_lock<std::mutex>(mu);
+  return pool;
+}
+
 bool mesh_fft_ok(int m) {
   if (m < 2 || (m % 2))
     return false;
@@ -81,6 +110,7 @@ struct p3mx_handle {
   std::vector<PairIA> table{PairIA{0, 0, 0, 0, 0, 0, 0, 0, 0, -1.0}};
   std::string err;
   Pinned h_in, h_out;
+  ChunkEvents out_events;
   // charge census
   int n_charged = 0;
   double sum_q2 = 0, sum_q = 0;
@@ -739,17 +769,28 @@ static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *
     e.upload(pos, q, type, true, st);
     return;
   }
+  // host arrays -> pinned staging (parallel host copies) -> device, chunk by
+  // chunk: the DMA of one chunk overlaps the host copy of the next
   size_t const bytes = n * (4 * sizeof(double) + sizeof(int));
   h->h_in.ensure(bytes);
-  double *pp = h->h_in.as<double>();
-  std::memcpy(pp, pos, 3 * n * sizeof(double));
-  std::memcpy(pp + 3 * n, q, n * sizeof(double));
-  int *tt = reinterpret_cast<int *>(pp + 4 * n);
+  char *pinned = h->h_in.as<char>();
+  std::unique_lock<std::mutex> lk;
+  HostPool &pool = host_pool(lk);
+  auto push = [&](const void *src, void *dst, size_t nbytes) {
+    for (size_t b0 = 0; b0 < nbytes; b0 += kStageChunk) {
+      size_t const nb = std::min(kStageChunk, nbytes - b0);
+      pool.copy(pinned + b0, static_cast<const char *>(src) + b0, nb);
+      P3MX_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + b0, pinned + b0, nb,
+                                cudaMemcpyHostToDevice, st));
+    }
+    pinned += nbytes;
+  };
+  push(pos, e.d_pos(), 3 * n * sizeof(double));
+  push(q, e.d_q(), n * sizeof(double));
   if (type)
-    std::memcpy(tt, type, n * sizeof(int));
+    push(type, e.d_type(), n * sizeof(int));
   else
-    std::memset(tt, 0, n * sizeof(int));
-  e.upload(pp, pp + 3 * n, tt, false, st);
+    P3MX_CUDA(cudaMemsetAsync(e.d_type(), 0, n * sizeof(int), st));
 }
 
 static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwrite,
@@ -761,15 +802,36 @@ static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwr
     // device destination: forces were computed straight into f
     return;
   }
-  h->h_out.ensure(3 * n * sizeof(double));
+  // device -> pinned staging in chunks, each chunk copied (or added) to the
+  // user's array by the host pool while the next chunk is in flight
+  size_t const bytes = 3 * n * sizeof(double);
+  h->h_out.ensure(bytes);
   double *o = h->h_out.as<double>();
-  P3MX_CUDA(cudaMemcpyAsync(o, e.d_force(), 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
-  P3MX_CUDA(cudaStreamSynchronize(st));
-  if (overwrite)
-    std::memcpy(f, o, 3 * n * sizeof(double));
-  else
-    for (size_t k = 0; k < 3 * n; ++k)
-      f[k] += o[k];
+  size_t const nch = (bytes + kStageChunk - 1) / kStageChunk;
+  for (size_t c = 0; c < nch; ++c) {
+    size_t const b0 = c * kStageChunk, nb = std::min(kStageChunk, bytes - b0);
+    P3MX_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(o) + b0,
+                              reinterpret_cast<const char *>(e.d_force()) + b0, nb,
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaEventRecord(h->out_events.get(c), st));
+  }
+  std::unique_lock<std::mutex> lk;
+  HostPool &pool = host_pool(lk);
+  for (size_t c = 0; c < nch; ++c) {
+    size_t const b0 = c * kStageChunk, nb = std::min(kStageChunk, bytes - b0);
+    P3MX_CUDA(cudaEventSynchronize(h->out_events.get(c)));
+    if (overwrite) {
+      pool.copy(reinterpret_cast<char *>(f) + b0, reinterpret_cast<const char *>(o) + b0, nb);
+    } else {
+      size_t const k0 = b0 / sizeof(double), nk = nb / sizeof(double);
+      size_t const piece = std::max<size_t>(32768, (nk + pool.size() - 1) / pool.size());
+      pool.run(static_cast<int>((nk + piece - 1) / piece), [&](int i) {
+        size_t const a0 = k0 + i * piece, a1 = std::min(k0 + nk, a0 + piece);
+        for (size_t k = a0; k < a1; ++k)
+          f[k] += o[k];
+      });
+    }
+  }
 }
 
 int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q, double *f,

@@ -366,7 +366,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
                                      static_cast<int>(limit)));
     };
     {
-      // assignment tiles: 2 (hi, lo) x (brick + cao - 1)^3 per warp
+      // assignment tiles: (brick + cao - 1)^3 fixed-point points per block
       auto aset = [&](auto kern) {
         P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(limit)));
@@ -549,15 +549,14 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 2. charge assignment: one warp per brick, colour by colour
   P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
   {
-    int const wpb = (sizeof(Real) == 4) ? 4 : 2;
-    size_t const smem = static_cast<size_t>(wpb) * 2 * m_tile_cap * sizeof(Real);
+    size_t const smem = static_cast<size_t>(m_tile_cap) * sizeof(unsigned long long);
     for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
       int const cnt = m_phase_off[p + 1] - m_phase_off[p];
       if (cnt == 0)
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<ceil_div(cnt, wpb), 32 * wpb, smem, st>>>(
-                                   geom, tab, cnt, m_tile_cap, m_start.as<int>(), m_W.as<Real>(),
+      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps, smem, st>>>(
+                                   geom, tab, cnt, m_start.as<int>(), m_W.as<Real>(),
                                    m_skey.as<int>(), m_rho.as<Real>())));
       ++m_launches;
     }

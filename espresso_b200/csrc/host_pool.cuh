@@ -1,0 +1,132 @@
+// Persistent host worker pool for the host-pointer staging path: parallel
+// copies between user buffers and pinned staging, chunked so that each chunk's
+// DMA overlaps the host copy of the next one.
+#pragma once
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace p3mx {
+
+class HostPool {
+public:
+  // Threads: P3MX_HOST_THREADS if set, else min(hardware threads, 16).
+  HostPool() {
+    int n = static_cast<int>(std::thread::hardware_concurrency());
+    if (const char *s = std::getenv("P3MX_HOST_THREADS"))
+      n = std::atoi(s);
+    n = std::clamp(n, 1, 16);
+    for (int i = 1; i < n; ++i) // the caller is the n-th worker
+      m_workers.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_mu);
+      m_stop = true;
+    }
+    m_cv.notify_all();
+    for (auto &t : m_workers)
+      t.join();
+  }
+  HostPool(HostPool const &) = delete;
+  HostPool &operator=(HostPool const &) = delete;
+
+  int size() const { return static_cast<int>(m_workers.size()) + 1; }
+
+  // Run fn(i) for i in [0, n_tasks) on the pool and the caller; returns when
+  // every task has finished.
+  void run(int n_tasks, std::function<void(int)> const &fn) {
+    if (n_tasks <= 0)
+      return;
+    if (m_workers.empty() || n_tasks == 1) {
+      for (int i = 0; i < n_tasks; ++i)
+        fn(i);
+      return;
+    }
+    unsigned gen;
+    {
+      std::lock_guard<std::mutex> lk(m_mu);
+      m_fn = &fn;
+      m_n = n_tasks;
+      m_done = 0;
+      gen = ++m_gen;
+      m_next.store(static_cast<unsigned long long>(gen) << 32);
+    }
+    m_cv.notify_all();
+    int const mine = work(gen, n_tasks, &fn);
+    std::unique_lock<std::mutex> lk(m_mu);
+    m_done += mine;
+    m_done_cv.wait(lk, [&] { return m_done == m_n; });
+    m_fn = nullptr;
+  }
+
+  // Parallel memcpy, split into pieces of at least 256 KB.
+  void copy(void *dst, const void *src, size_t bytes) {
+    size_t const piece = std::max<size_t>(256 << 10, (bytes + size() - 1) / size());
+    int const n = static_cast<int>((bytes + piece - 1) / piece);
+    run(n, [&](int i) {
+      size_t const b0 = i * piece, b1 = std::min(bytes, b0 + piece);
+      std::memcpy(static_cast<char *>(dst) + b0, static_cast<const char *>(src) + b0, b1 - b0);
+    });
+  }
+
+private:
+  // Claim tasks of generation gen: the counter holds (generation << 32 |
+  // next index), so a worker holding a stale generation claims nothing.
+  int work(unsigned gen, int n, std::function<void(int)> const *fn) {
+    int count = 0;
+    for (;;) {
+      unsigned long long v = m_next.load();
+      for (;;) {
+        if ((v >> 32) != gen || static_cast<int>(v & 0xffffffffull) >= n)
+          return count;
+        if (m_next.compare_exchange_weak(v, v + 1))
+          break;
+      }
+      (*fn)(static_cast<int>(v & 0xffffffffull));
+      ++count;
+    }
+  }
+  void loop() {
+    unsigned seen = 0;
+    for (;;) {
+      unsigned gen;
+      int n;
+      std::function<void(int)> const *fn;
+      {
+        std::unique_lock<std::mutex> lk(m_mu);
+        m_cv.wait(lk, [&] { return m_stop || m_gen != seen; });
+        if (m_stop)
+          return;
+        seen = gen = m_gen;
+        n = m_n;
+        fn = m_fn;
+      }
+      int const mine = work(gen, n, fn);
+      std::lock_guard<std::mutex> lk(m_mu);
+      if (gen == m_gen) {
+        m_done += mine;
+        if (m_done == m_n)
+          m_done_cv.notify_all();
+      }
+    }
+  }
+
+  std::vector<std::thread> m_workers;
+  std::mutex m_mu;
+  std::condition_variable m_cv, m_done_cv;
+  std::function<void(int)> const *m_fn = nullptr;
+  int m_n = 0, m_done = 0;
+  std::atomic<unsigned long long> m_next{0};
+  unsigned m_gen = 0;
+  bool m_stop = false;
+};
+
+} // namespace p3mx

@@ -138,41 +138,82 @@ __device__ inline void corner_of(RepGeom const &G, int loc, int &cx, int &cy, in
   cz = bz * B + l % B;
 }
 
-// Deterministic charge assignment, one warp per brick.  The particles of a
-// brick (corners in a B^3 block, one contiguous range of the brick-major
-// sorted order) are taken one at a time in sorted order; the 32 lanes cover
-// the particle's P^3 stencil points, each lane adding q*wx*wy*wz into the
-// brick's shared-memory tile ((B+P-1)^3 points) -- no two lanes of one
-// round touch the same point, so the tile needs no atomics and the sum order
-// is fixed.  Tile accumulation is compensated (two-sum hi/lo).  Tiles are
-// then added to the mesh; bricks of one launch share a colour (parity per
-// dimension, a third colour for the last brick of an odd count), so the
-// tiles of one launch never overlap and plain read-add-write is race-free;
-// colours run in a fixed order, making the mesh bitwise reproducible.
+// Warps per brick (block) of the charge assignment.
+constexpr int kAssignWarps = 4;
+
+// Real -> 64-bit fixed point (round to nearest) and back.
+__device__ inline long long to_fixed(float v) { return __float2ll_rn(v); }
+__device__ inline long long to_fixed(double v) { return __double2ll_rn(v); }
+template <typename Real> __device__ inline Real from_fixed(long long v);
+template <> __device__ inline float from_fixed<float>(long long v) { return __ll2float_rn(v); }
+template <> __device__ inline double from_fixed<double>(long long v) { return __ll2double_rn(v); }
+
+// Deterministic charge assignment (AssignCharges, p3m.cpp:225-265), one
+// block of kAssignWarps warps per brick.  The particles of a brick (corners
+// in a B^3 block: one contiguous range of the brick-major sorted order) are
+// spread over the warps; for each particle the 32 lanes cover its P^3 stencil
+// points and add q*wx*wy*wz into the brick's shared-memory tile of
+// (B+P-1)^3 points.  The tile holds 64-bit fixed point with a power-of-two
+// scale S chosen from the brick's total |q| (every tile sum stays below 2^62),
+// so the shared-memory atomic adds are exact and order-independent: the tile
+// is bitwise reproducible although the warps run concurrently.  The tile is
+// then converted back (one rounding per point) and added to the mesh; bricks
+// of one launch share a colour (greedy interval colouring per dimension), so
+// the tiles of one launch never overlap and plain read-add-write is
+// race-free; colours run in a fixed order, making the mesh reproducible.
 template <typename Real, int P>
-__global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks,
-                             int nbricks, int tile_cap, const int *__restrict__ start,
-                             const Real *__restrict__ W, const int *__restrict__ s_key,
-                             Real *__restrict__ rho) {
+__global__ void __launch_bounds__(32 * kAssignWarps)
+k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
+             const int *__restrict__ start, const Real *__restrict__ W,
+             const int *__restrict__ s_key, Real *__restrict__ rho) {
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
   constexpr int P3 = P * P * P;
   constexpr int NR = (P3 + 31) / 32;
+  constexpr int NT = 32 * kAssignWarps;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int const bi = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (bi >= nbricks)
-    return; // whole warp
-  int2 const bk = bricks[bi];
+  __shared__ double s_red[kAssignWarps];
+  if (static_cast<int>(blockIdx.x) >= nbricks)
+    return; // whole block
+  int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
   int const B = G.brick, B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
-  Real *hi = reinterpret_cast<Real *>(smem_raw) + static_cast<long long>(warp) * 2 * tile_cap;
-  Real *lo = hi + tile_cap;
-  for (int t = lane; t < E3; t += 32) {
-    hi[t] = Real(0);
-    lo[t] = Real(0);
+  const int *st = start + G.bin_off;
+  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
+  if (s0 == s1)
+    return; // empty brick: nothing to add
+  unsigned long long *tile = reinterpret_cast<unsigned long long *>(smem_raw);
+  for (int t = tid; t < E3; t += NT)
+    tile[t] = 0ull;
+  // total |q| of the brick: the x weights of a record are q*wx with wx >= 0
+  // summing to 1, so sum_k |q wx_k| = |q|
+  double aq = 0.0;
+  for (int s = s0 + tid; s < s1; s += NT) {
+    const Real *w = W + static_cast<long long>(s) * WS;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+      aq += fabs(static_cast<double>(w[k]));
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    aq += __shfl_xor_sync(0xffffffffu, aq, o);
+  if (lane == 0)
+    s_red[warp] = aq;
+  __syncthreads();
+  double qabs = 0.0;
+#pragma unroll
+  for (int k = 0; k < kAssignWarps; ++k)
+    qabs += s_red[k];
+  if (qabs == 0.0)
+    return; // all charges zero: the tile would stay zero
+  // S = 2^(61 - ex) with qabs < 2^ex: |tile sum| <= qabs*S + count/2 < 2^62
+  int ex;
+  frexp(qabs * (1.0 + 1e-12), &ex);
+  int const es = min(max(61 - ex, -100), 100);
+  Real const S = static_cast<Real>(ldexp(1.0, es));
+  Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
   // per-lane stencil point of each round and its tile offset
   int off[NR], wi[NR], wj[NR], wk[NR];
 #pragma unroll
@@ -184,52 +225,38 @@ __global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__res
     wk[r] = tt % P;
     off[r] = (wi[r] * E + wj[r]) * E + wk[r];
   }
-  __syncwarp();
-  const int *st = start + G.bin_off;
-  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
-  for (int s = s0; s < s1; ++s) {
+  __syncthreads(); // tile zeroed
+  for (int s = s0 + warp; s < s1; s += kAssignWarps) {
     int const l = s_key[s] - bk.y * B3;
     int const base = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
     const Real *w = W + static_cast<long long>(s) * WS;
-    // all loads of the particle's rounds first (the rounds touch distinct
-    // tile points), then the compensated adds, then the stores
-    Real v[NR], h[NR], c[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      v[r] = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
-      h[r] = hi[base + off[r]];
-      c[r] = lo[base + off[r]];
-    }
-#pragma unroll
-    for (int r = 0; r < NR; ++r)
-      two_sum(h[r], c[r], v[r]);
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       if (lane + 32 * r < P3) {
-        hi[base + off[r]] = h[r];
-        lo[base + off[r]] = c[r];
+        Real const v = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
+        atomicAdd(&tile[base + off[r]], static_cast<unsigned long long>(to_fixed(v * S)));
       }
     }
-    __syncwarp();
   }
+  __syncthreads();
   // add the tile to the mesh: real extent of the brick plus the stencil
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
   int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
   int const x0 = bx * B, y0 = by * B, z0 = bz * B;
-  int const ex = min(B, M0 - x0) + P - 1, ey = min(B, M1 - y0) + P - 1, ez = min(B, M2 - z0) + P - 1;
+  int const ex0 = min(B, M0 - x0) + P - 1, ey = min(B, M1 - y0) + P - 1, ez = min(B, M2 - z0) + P - 1;
   Real *mesh = rho + G.rm_off;
   // a tile wider than the mesh maps two tile points onto one mesh point:
   // add such points in separate passes (one per wrap class)
-  bool const self_wrap = (ex > M0) || (ey > M1) || (ez > M2);
+  bool const self_wrap = (ex0 > M0) || (ey > M1) || (ez > M2);
   int const passes = self_wrap ? 8 : 1;
-  // each lane owns fixed (y, z) slots of the tile's yz plane; loop over x
+  // each thread owns fixed (y, z) slots of the tile's yz plane; loop over x
   constexpr int EMAX = 8 + P - 1;
-  constexpr int NS = (EMAX * EMAX + 31) / 32;
+  constexpr int NS = (EMAX * EMAX + NT - 1) / NT;
   int yzt[NS], yzg[NS], ycls[NS];
   int const nyz = ey * ez;
 #pragma unroll
   for (int k2 = 0; k2 < NS; ++k2) {
-    int const t = lane + 32 * k2;
+    int const t = tid + NT * k2;
     int const y = (t < nyz) ? t / ez : 0, z = (t < nyz) ? t - (t / ez) * ez : 0;
     int gy = y0 + y, gz = z0 + z, cls = 0;
     if (gy >= M1) { gy -= M1; cls |= 2; }
@@ -241,7 +268,7 @@ __global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__res
     ycls[k2] = cls;
   }
   for (int pass = 0; pass < passes; ++pass) {
-    for (int x = 0; x < ex; ++x) {
+    for (int x = 0; x < ex0; ++x) {
       int gx = x0 + x, xcls = 0;
       if (gx >= M0) { gx -= M0; xcls = 1; }
       if (gx >= M0) gx -= M0;
@@ -251,10 +278,10 @@ __global__ void k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__res
         if (yzt[k2] < 0 || (self_wrap && (xcls | ycls[k2]) != pass))
           continue;
         int const ti = x * E * E + yzt[k2];
-        mesh[gbase + yzg[k2]] += hi[ti] + lo[ti];
+        mesh[gbase + yzg[k2]] += from_fixed<Real>(static_cast<long long>(tile[ti])) * inv_S;
       }
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
