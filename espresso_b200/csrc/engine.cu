@@ -549,14 +549,14 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 2. charge assignment: one warp per brick, colour by colour
   P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
   {
-    size_t const smem = static_cast<size_t>(m_tile_cap) * sizeof(unsigned long long);
     for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
       int const cnt = m_phase_off[p + 1] - m_phase_off[p];
       if (cnt == 0)
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps, smem, st>>>(
-                                   geom, tab, cnt, m_start.as<int>(), m_W.as<Real>(),
+      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps,
+                                   assign_smem<Real, P>(m_tile_cap), st>>>(
+                                   geom, tab, cnt, m_tile_cap, m_start.as<int>(), m_W.as<Real>(),
                                    m_skey.as<int>(), m_rho.as<Real>())));
       ++m_launches;
     }

@@ -138,33 +138,52 @@ __device__ inline void corner_of(RepGeom const &G, int loc, int &cx, int &cy, in
   cz = bz * B + l % B;
 }
 
-// Warps per brick (block) of the charge assignment.
+// Warps per brick (block) of the charge assignment, and particles whose
+// weight records are staged in shared memory at a time.
 constexpr int kAssignWarps = 4;
+constexpr int kAssignChunk = 64;
 
-// Real -> 64-bit fixed point (round to nearest) and back.
-__device__ inline long long to_fixed(float v) { return __float2ll_rn(v); }
-__device__ inline long long to_fixed(double v) { return __double2ll_rn(v); }
-template <typename Real> __device__ inline Real from_fixed(long long v);
-template <> __device__ inline float from_fixed<float>(long long v) { return __ll2float_rn(v); }
-template <> __device__ inline double from_fixed<double>(long long v) { return __ll2double_rn(v); }
+// Bytes of dynamic shared memory of one assignment block: the split
+// fixed-point tile (two 32-bit words per point) and one staged chunk of
+// weight records and tile offsets.
+template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem(int tile_cap) {
+  return 2 * sizeof(int) * static_cast<size_t>(tile_cap) +
+         sizeof(Real) * kAssignChunk * wstride<P, 4>() + sizeof(int) * kAssignChunk;
+}
+
+template <typename Real> __device__ inline Real floor_r(Real v);
+template <> __device__ inline float floor_r<float>(float v) { return floorf(v); }
+template <> __device__ inline double floor_r<double>(double v) { return floor(v); }
+__device__ inline unsigned to_u32_rn(float v) { return __float2uint_rn(v); }
+__device__ inline unsigned to_u32_rn(double v) { return __double2uint_rn(v); }
+template <typename Real> __device__ inline Real from_ll(long long v);
+template <> __device__ inline float from_ll<float>(long long v) { return __ll2float_rn(v); }
+template <> __device__ inline double from_ll<double>(long long v) { return __ll2double_rn(v); }
 
 // Deterministic charge assignment (AssignCharges, p3m.cpp:225-265), one
 // block of kAssignWarps warps per brick.  The particles of a brick (corners
 // in a B^3 block: one contiguous range of the brick-major sorted order) are
 // spread over the warps; for each particle the 32 lanes cover its P^3 stencil
 // points and add q*wx*wy*wz into the brick's shared-memory tile of
-// (B+P-1)^3 points.  The tile holds 64-bit fixed point with a power-of-two
-// scale S chosen from the brick's total |q| (every tile sum stays below 2^62),
-// so the shared-memory atomic adds are exact and order-independent: the tile
-// is bitwise reproducible although the warps run concurrently.  The tile is
-// then converted back (one rounding per point) and added to the mesh; bricks
-// of one launch share a colour (greedy interval colouring per dimension), so
-// the tiles of one launch never overlap and plain read-add-write is
-// race-free; colours run in a fixed order, making the mesh reproducible.
+// (B+P-1)^3 points.
+//
+// The tile holds fixed point: a contribution t = v*S (S a power of two) is
+// split exactly into hi = floor(t / 2^kb) and lo = t - hi*2^kb in [0, 2^kb],
+// added with 32-bit integer atomics to two words per point.  With n
+// particles in the brick, kb = 32 - ceil(log2(n+1)) keeps every lo sum below
+// 2^32, and S = 2^(30+kb-ex) with sum|q| < 2^ex keeps every hi sum below
+// 2^31; the point value is (hi*2^kb + lo)/S.  Integer sums do not depend on
+// the order of the adds, so the tile is bitwise reproducible although the
+// warps run concurrently; the quantum is 2^-(30+kb) of the brick's sum|q|.
+//
+// Tiles are then added to the mesh; bricks of one launch share a colour
+// (greedy interval colouring per dimension), so the tiles of one launch never
+// overlap and plain read-add-write is race-free; colours run in a fixed
+// order, making the mesh reproducible.
 template <typename Real, int P>
 __global__ void __launch_bounds__(32 * kAssignWarps)
 k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
-             const int *__restrict__ start, const Real *__restrict__ W,
+             int tile_cap, const int *__restrict__ start, const Real *__restrict__ W,
              const int *__restrict__ s_key, Real *__restrict__ rho) {
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
@@ -172,6 +191,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   constexpr int P3 = P * P * P;
   constexpr int NR = (P3 + 31) / 32;
   constexpr int NT = 32 * kAssignWarps;
+  constexpr int CH = kAssignChunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[kAssignWarps];
   if (static_cast<int>(blockIdx.x) >= nbricks)
@@ -184,9 +204,14 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
   if (s0 == s1)
     return; // empty brick: nothing to add
-  unsigned long long *tile = reinterpret_cast<unsigned long long *>(smem_raw);
-  for (int t = tid; t < E3; t += NT)
-    tile[t] = 0ull;
+  int *t_hi = reinterpret_cast<int *>(smem_raw);
+  unsigned *t_lo = reinterpret_cast<unsigned *>(t_hi + tile_cap);
+  Real *rec = reinterpret_cast<Real *>(t_lo + tile_cap);
+  int *rbase = reinterpret_cast<int *>(rec + CH * WS);
+  for (int t = tid; t < E3; t += NT) {
+    t_hi[t] = 0;
+    t_lo[t] = 0u;
+  }
   // total |q| of the brick: the x weights of a record are q*wx with wx >= 0
   // summing to 1, so sum_k |q wx_k| = |q|
   double aq = 0.0;
@@ -208,12 +233,14 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     qabs += s_red[k];
   if (qabs == 0.0)
     return; // all charges zero: the tile would stay zero
-  // S = 2^(61 - ex) with qabs < 2^ex: |tile sum| <= qabs*S + count/2 < 2^62
+  int const cnt = s1 - s0;
+  int const kb = min(24, 32 - (32 - __clz(cnt))); // cnt < 2^(32-kb)
   int ex;
   frexp(qabs * (1.0 + 1e-12), &ex);
-  int const es = min(max(61 - ex, -100), 100);
+  int const es = min(max(30 + kb - ex, -100), 100);
   Real const S = static_cast<Real>(ldexp(1.0, es));
-  Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
+  Real const two_kb = static_cast<Real>(1u << kb);
+  Real const inv_two_kb = static_cast<Real>(1.0 / (1u << kb));
   // per-lane stencil point of each round and its tile offset
   int off[NR], wi[NR], wj[NR], wk[NR];
 #pragma unroll
@@ -225,20 +252,36 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     wk[r] = tt % P;
     off[r] = (wi[r] * E + wj[r]) * E + wk[r];
   }
-  __syncthreads(); // tile zeroed
-  for (int s = s0 + warp; s < s1; s += kAssignWarps) {
-    int const l = s_key[s] - bk.y * B3;
-    int const base = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
-    const Real *w = W + static_cast<long long>(s) * WS;
+  for (int c0 = s0; c0 < s1; c0 += CH) {
+    int const cn = min(CH, s1 - c0);
+    __syncthreads(); // tile zeroed / previous chunk consumed
+    // stage the chunk: records are contiguous, so the block copies them with
+    // coalesced loads, plus each particle's tile base offset
+    const Real *src = W + static_cast<long long>(c0) * WS;
+    for (int e = tid; e < cn * WS; e += NT)
+      rec[e] = src[e];
+    for (int j = tid; j < cn; j += NT) {
+      int const l = s_key[c0 + j] - bk.y * B3;
+      rbase[j] = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
+    }
+    __syncthreads();
+    for (int j = warp; j < cn; j += kAssignWarps) {
+      int const base = rbase[j];
+      const Real *w = rec + j * WS;
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (lane + 32 * r < P3) {
-        Real const v = w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]];
-        atomicAdd(&tile[base + off[r]], static_cast<unsigned long long>(to_fixed(v * S)));
+      for (int r = 0; r < NR; ++r) {
+        if (lane + 32 * r < P3) {
+          Real const t = (w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]]) * S;
+          Real const hf = floor_r(t * inv_two_kb);
+          Real const lf = t - hf * two_kb;
+          atomicAdd(&t_hi[base + off[r]], static_cast<int>(hf));
+          atomicAdd(&t_lo[base + off[r]], to_u32_rn(lf));
+        }
       }
     }
   }
   __syncthreads();
+  Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
   // add the tile to the mesh: real extent of the brick plus the stencil
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
   int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
@@ -278,7 +321,8 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
         if (yzt[k2] < 0 || (self_wrap && (xcls | ycls[k2]) != pass))
           continue;
         int const ti = x * E * E + yzt[k2];
-        mesh[gbase + yzg[k2]] += from_fixed<Real>(static_cast<long long>(tile[ti])) * inv_S;
+        long long const v = static_cast<long long>(t_hi[ti]) * (1ll << kb) + t_lo[ti];
+        mesh[gbase + yzg[k2]] += from_ll<Real>(v) * inv_S;
       }
     }
     __syncthreads();
