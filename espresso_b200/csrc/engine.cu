@@ -13,22 +13,24 @@ namespace p3mx {
 
 namespace {
 
-// Radix factorisation of an FFT length: 4s first, then 2, 3, 5, 7 and any
-// remaining prime (handled by the generic radix, up to 31).
+// Radix factorisation of an FFT length: the power of two as radix-16 stages
+// (then one 8, 4 or 2), then 3, 5, 7 and any remaining prime (handled by the
+// generic radix, up to 31).
 AxisPlan make_plan(int n, int tw_off) {
   AxisPlan pl{};
   pl.n = n;
   pl.tw_off = tw_off;
   int m = n;
   std::vector<int> f;
-  while (m % 4 == 0) {
-    f.push_back(4);
-    m /= 4;
+  while (m % 16 == 0) {
+    f.push_back(16);
+    m /= 16;
   }
-  while (m % 2 == 0) {
-    f.push_back(2);
-    m /= 2;
-  }
+  for (int r : {8, 4, 2})
+    if (m % r == 0) {
+      f.push_back(r);
+      m /= r;
+    }
   for (int p = 3; m > 1; p += 2) {
     while (m % p == 0) {
       f.push_back(p);
@@ -319,21 +321,28 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       maxM2 = std::max(maxM2, G.mesh[2]);
     }
     m_tile_y = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / maxM1)));
-    m_tile_x = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / (3 * maxM0))));
+    // x pass: three line buffers (phi, field lines, scratch) of T kz columns
+    size_t const x_budget = 96 * 1024;
+    m_tile_x = static_cast<int>(std::max<size_t>(
+        1, std::min<size_t>(16, x_budget / (3 * static_cast<size_t>(maxM0 + 1) * csz))));
     size_t smem_zf = 0, smem_zi = 0;
     for (int r = 0; r < R; ++r) {
       auto const &G = m_geom[r];
       int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
       int const H = M2 / 2 + 1;
       int const lines = M0 * M1;
-      int const lz = static_cast<int>(std::max<size_t>(1, cap / M2));
+      // forward z: two real lines per complex transform
+      int const lz = static_cast<int>(std::max<size_t>(1, cap / M2)) * 2;
       for (int l = 0; l < lines; l += lz)
         zf.push_back(Blk{r, l, std::min(lz, lines - l), 0});
-      smem_zf = std::max(smem_zf, 2 * static_cast<size_t>(std::min(lz, lines)) * M2 * csz);
-      int const lzi = static_cast<int>(std::max<size_t>(1, cap / (3 * M2)));
+      smem_zf = std::max(smem_zf,
+                         2 * static_cast<size_t>((std::min(lz, lines) + 1) / 2) * M2 * csz);
+      // backward z: nl lines -> nl (Ex, Ey) + ceil(nl/2) (Ez pairs) transforms
+      int const lzi = static_cast<int>(std::max<size_t>(1, 2 * (cap / M2) / 3));
       for (int l = 0; l < lines; l += lzi)
         zi.push_back(Blk{r, l, std::min(lzi, lines - l), 0});
-      smem_zi = std::max(smem_zi, 2 * 3 * static_cast<size_t>(std::min(lzi, lines)) * M2 * csz);
+      int const nzi = std::min(lzi, lines);
+      smem_zi = std::max(smem_zi, 2 * static_cast<size_t>(nzi + (nzi + 1) / 2) * M2 * csz);
       for (int xx = 0; xx < M0; ++xx)
         for (int k0 = 0; k0 < H; k0 += m_tile_y)
           y.push_back(Blk{r, xx, k0, 0});
@@ -345,7 +354,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     m_smem_zf = smem_zf;
     m_smem_zi = smem_zi;
     m_smem_y = 2 * static_cast<size_t>(m_tile_y) * (maxM1 + 1) * csz;
-    m_smem_x = 2 * 3 * static_cast<size_t>(m_tile_x) * (maxM0 + 1) * csz;
+    m_smem_x = 3 * static_cast<size_t>(m_tile_x) * (maxM0 + 1) * csz;
     m_n_blk_zf = static_cast<int>(zf.size());
     m_n_blk_y = static_cast<int>(y.size());
     m_n_blk_x = static_cast<int>(x.size());

@@ -33,9 +33,83 @@ template <typename C> __device__ inline C ld_tw(const C *__restrict__ tw, int k,
   return w;
 }
 
+// cos(2 pi k / 16) and sin(2 pi k / 16), k = 0..15 (exact constants of the
+// sixteenth roots of unity: 1, cos(pi/8), sqrt(1/2), sin(pi/8), 0).
+__host__ __device__ constexpr double cos16(int k) {
+  constexpr double c1 = 0.92387953251128675613, c2 = 0.70710678118654752440,
+                   c3 = 0.38268343236508977173;
+  switch (k & 15) {
+  case 0: return 1.0;
+  case 1: return c1;
+  case 2: return c2;
+  case 3: return c3;
+  case 4: return 0.0;
+  case 5: return -c3;
+  case 6: return -c2;
+  case 7: return -c1;
+  case 8: return -1.0;
+  case 9: return -c1;
+  case 10: return -c2;
+  case 11: return -c3;
+  case 12: return 0.0;
+  case 13: return c3;
+  case 14: return c2;
+  default: return c1;
+  }
+}
+__host__ __device__ constexpr double sin16(int k) { return cos16(k - 4); }
+
+// In-register DFT of a power-of-two length R <= 16 (radix-2 decimation in
+// time on top of the radix-4 kernel), constant twiddles.
+template <typename C, int R> __device__ __forceinline__ void dft_pow2(C *v, bool inv) {
+  using Real = decltype(v[0].x);
+  if constexpr (R == 2) {
+    C const a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    C const s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]);
+    C const s2 = cadd(v[1], v[3]), s3 = csub(v[1], v[3]);
+    C const s3r = inv ? C{-s3.y, s3.x} : C{s3.y, -s3.x};
+    v[0] = cadd(s0, s2);
+    v[2] = csub(s0, s2);
+    v[1] = cadd(s1, s3r);
+    v[3] = csub(s1, s3r);
+  } else {
+    constexpr int H = R / 2;
+    C e[H], o[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    dft_pow2<C, H>(e, inv);
+    dft_pow2<C, H>(o, inv);
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      C t;
+      if (k == 0) {
+        t = o[0];
+      } else if (2 * k == H) {
+        // exp(-+ i pi/2) = -+i
+        t = inv ? C{-o[k].y, o[k].x} : C{o[k].y, -o[k].x};
+      } else {
+        Real const wr = static_cast<Real>(cos16(k * (16 / R)));
+        Real const ws = static_cast<Real>(sin16(k * (16 / R)));
+        Real const wi = inv ? ws : -ws;
+        t = C{o[k].x * wr - o[k].y * wi, o[k].x * wi + o[k].y * wr};
+      }
+      v[k] = cadd(e[k], t);
+      v[k + H] = csub(e[k], t);
+    }
+  }
+}
+
 template <typename C, int R>
 __device__ inline void dft_small(C *v, const C *__restrict__ tw, int n, bool inv) {
-  if constexpr (R == 2) {
+  if constexpr (R == 8 || R == 16) {
+    dft_pow2<C, R>(v, inv);
+  } else if constexpr (R == 2) {
     C const a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
@@ -167,6 +241,8 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
     case 2: fft_stage_t<C, 2>(src, dst, n, ld, nlines, Ns, tw, inv); break;
     case 3: fft_stage_t<C, 3>(src, dst, n, ld, nlines, Ns, tw, inv); break;
     case 4: fft_stage_t<C, 4>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 8: fft_stage_t<C, 8>(src, dst, n, ld, nlines, Ns, tw, inv); break;
+    case 16: fft_stage_t<C, 16>(src, dst, n, ld, nlines, Ns, tw, inv); break;
     case 5: fft_stage_t<C, 5>(src, dst, n, ld, nlines, Ns, tw, inv); break;
     case 7: fft_stage_t<C, 7>(src, dst, n, ld, nlines, Ns, tw, inv); break;
     default: fft_stage_dyn<C>(src, dst, n, ld, nlines, Ns, R, tw, inv); break;
@@ -181,6 +257,9 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
 }
 
 // ---- pass z, forward: real lines -> complex half lines -----------------
+// Two real lines per complex transform: Z = x0 + i x1, then
+// X0[k] = (Z[k] + conj Z[n-k]) / 2 and X1[k] = -i (Z[k] - conj Z[n-k]) / 2.
+// bk.b real lines per block (an odd last line is paired with zeros).
 template <typename Real>
 __global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
                             const Real *__restrict__ rmesh,
@@ -191,20 +270,34 @@ __global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restr
   Blk const bk = blks[blockIdx.x];
   RepGeom const &G = reps[bk.rep];
   int const n = G.mesh[2];
-  int const nl = bk.b; // lines in this block
+  int const nl = bk.b;            // real lines in this block
+  int const np = (nl + 1) >> 1;   // complex lines
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + nl * n;
+  C *b = a + np * n;
   long long const line0 = bk.a;
   const Real *src = rmesh + G.rm_off + line0 * n;
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x)
-    a[e] = C{src[e], Real(0)};
+  for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
+    int const j = e / n, k = e - j * n;
+    Real const re = src[(2 * j) * n + k];
+    Real const im = (2 * j + 1 < nl) ? src[(2 * j + 1) * n + k] : Real(0);
+    a[e] = C{re, im};
+  }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, nl, n, G.plan[2], twtab, false);
+  C *res = fft_lines<C>(a, b, np, n, G.plan[2], twtab, false);
   int const H = n / 2 + 1;
-  for (int e = threadIdx.x; e < nl * G.hp; e += blockDim.x) {
-    int const l = e / G.hp, k = e - l * G.hp;
-    C v = (k < H) ? res[l * n + k] : C{Real(0), Real(0)};
-    cmesh[G.km_off + (line0 + l) * G.hp + k] = v;
+  int const hp = G.hp;
+  for (int e = threadIdx.x; e < nl * hp; e += blockDim.x) {
+    int const l = e / hp, k = e - l * hp;
+    C v{Real(0), Real(0)};
+    if (k < H) {
+      C const z = res[(l >> 1) * n + k];
+      C const zc = res[(l >> 1) * n + ((n - k) % n)];
+      if ((l & 1) == 0)
+        v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
+      else
+        v = C{Real(0.5) * (z.y + zc.y), Real(0.5) * (zc.x - z.x)};
+    }
+    cmesh[G.km_off + (line0 + l) * hp + k] = v;
   }
 }
 
@@ -261,7 +354,8 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   int const ld = M0 + 1; // padded line stride
   int const L = T * ld;
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + 3 * L; // scratch of the same size (3 fields)
+  C *b = a + L;
+  C *c = b + L; // three line buffers: phi, field lines, FFT scratch
   long long const stride_x = static_cast<long long>(M1) * G.hp;
   long long const base = G.km_off + static_cast<long long>(y) * G.hp + kz0;
   for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
@@ -270,12 +364,12 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   }
   __syncthreads();
   C *res = fft_lines<C>(a, b, T, ld, G.plan[0], twtab, false);
+  C *fb = (res == a) ? b : a; // field lines go to the free buffer
   // k-space operator
   double const wv[3] = {2.0 * kPi * G.box_i[0], 2.0 * kPi * G.box_i[1],
                         2.0 * kPi * G.box_i[2]};
   double const hai2 = (1.0 / 2.0 / G.alpha) * (1.0 / 2.0 / G.alpha);
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  C *fbuf = (res == a) ? b : a; // the three field lines go to the free buffer
   // d_op (Nyquist zeroed) integer shift of index i in a mesh of size m
   auto dop = [](int i, int m) { return (i == m / 2) ? 0 : (i < m / 2 ? i : i - m); };
   int const kyd = dop(y, M1);
@@ -303,15 +397,8 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
         acc[7] += ek;
       }
     }
-    if (want_fields) {
-      C const phi{g * rh.x, g * rh.y};
-      Real const k0 = static_cast<Real>(kxd) * static_cast<Real>(wv[0]);
-      Real const k1 = static_cast<Real>(kyd) * static_cast<Real>(wv[1]);
-      Real const k2 = static_cast<Real>(kzd) * static_cast<Real>(wv[2]);
-      fbuf[0 * L + t * ld + x] = C{-k0 * phi.y, k0 * phi.x};
-      fbuf[1 * L + t * ld + x] = C{-k1 * phi.y, k1 * phi.x};
-      fbuf[2 * L + t * ld + x] = C{-k2 * phi.y, k2 * phi.x};
-    }
+    // phi = G rho_hat replaces rho_hat in place (same thread, same point)
+    res[t * ld + x] = C{g * rh.x, g * rh.y};
   }
   if (want_ev) {
     // block reduction of the 8 partial sums (fixed order -> deterministic)
@@ -337,19 +424,33 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   }
   if (!want_fields)
     return;
-  __syncthreads();
-  C *scratch = (fbuf == a) ? b : a;
-  // the three field blocks are 3T consecutive lines of stride ld
-  C *fres = fft_lines<C>(fbuf, scratch, 3 * T, ld, G.plan[0], twtab, true);
-  int const TM = T * M0;
-  for (int e = threadIdx.x; e < 3 * TM; e += blockDim.x) {
-    int const d = e / TM, r = e - d * TM;
-    int const x = r / T, t = r - x * T;
-    field0[field_stride * d + base + x * stride_x + t] = fres[d * L + t * ld + x];
+  // the three field components, one after another: E_d = i k_d phi, then
+  // the backward x transform of its T lines
+  int const kvec_y = kyd;
+  for (int d = 0; d < 3; ++d) {
+    __syncthreads(); // phi complete / previous component stored
+    Real const wd = static_cast<Real>(wv[d]);
+    for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
+      int const t = e / M0, x = e - t * M0;
+      int const kd = (d == 0) ? dop(x, M0) : (d == 1 ? kvec_y : dop(kz0 + t, M2));
+      Real const k = static_cast<Real>(kd) * wd;
+      C const phi = res[t * ld + x];
+      fb[t * ld + x] = C{-k * phi.y, k * phi.x};
+    }
+    __syncthreads();
+    C *fres = fft_lines<C>(fb, c, T, ld, G.plan[0], twtab, true);
+    for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
+      int const x = e / T, t = e - x * T;
+      field0[field_stride * d + base + x * stride_x + t] = fres[t * ld + x];
+    }
   }
 }
 
 // ---- pass z, backward for the 3 field components -> real fields --------
+// Two real outputs per complex transform: slot l < nl carries Ex + i Ey of
+// line l, slot nl + j carries Ez of lines 2j and 2j+1.  Each half row is
+// extended by Hermitian symmetry with the imaginary parts of the k = 0 and
+// k = n/2 entries dropped (c2r semantics), so both packed outputs are real.
 template <typename Real>
 __global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
                              const typename CplxOf<Real>::type *__restrict__ field0,
@@ -362,32 +463,49 @@ __global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__rest
   int const n = G.mesh[2];
   int const H = n / 2 + 1;
   int const nl = bk.b;
+  int const nz = (nl + 1) >> 1;
+  int const nc = nl + nz;
   long long const line0 = bk.a;
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + 3 * nl * n;
-  for (int e = threadIdx.x; e < 3 * nl * n; e += blockDim.x) {
-    int const dl = e / n, k = e - dl * n; // dl = d * nl + l
-    int const d = dl / nl, l = dl - d * nl;
+  C *b = a + nc * n;
+  // Hermitian-extended entry k of field d, line l of this block
+  auto herm = [&](int d, int l, int k) -> C {
     const C *src = field0 + field_stride * d + G.km_off + (line0 + l) * G.hp;
-    C v;
     if (k < H) {
-      v = src[k];
-    } else {
-      v = cconj(src[n - k]);
+      C v = src[k];
+      if (k == 0 || 2 * k == n)
+        v.y = Real(0);
+      return v;
     }
-    a[e] = v;
+    return cconj(src[n - k]);
+  };
+  for (int e = threadIdx.x; e < nc * n; e += blockDim.x) {
+    int const j = e / n, k = e - j * n;
+    C X, Y;
+    if (j < nl) {
+      X = herm(0, j, k);
+      Y = herm(1, j, k);
+    } else {
+      int const l0 = 2 * (j - nl);
+      X = herm(2, l0, k);
+      Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
+    }
+    a[e] = C{X.x - Y.y, X.y + Y.x};
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, 3 * nl, n, G.plan[2], twtab, true);
+  C *res = fft_lines<C>(a, b, nc, n, G.plan[2], twtab, true);
   // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
   // interpolation gathers one 16-byte (FP32) record per stencil point
   using R4 = typename Real4Of<Real>::type;
   R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+    int const l = e / n, k = e - l * n;
+    C const xy = res[e];
+    C const zz = res[(nl + (l >> 1)) * n + k];
     R4 v;
-    v.x = res[e].x;
-    v.y = res[nl * n + e].x;
-    v.z = res[2 * nl * n + e].x;
+    v.x = xy.x;
+    v.y = xy.y;
+    v.z = (l & 1) ? zz.y : zz.x;
     v.w = Real(0);
     out[e] = v;
   }
