@@ -320,29 +320,34 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       maxM1 = std::max(maxM1, G.mesh[1]);
       maxM2 = std::max(maxM2, G.mesh[2]);
     }
-    m_tile_y = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / maxM1)));
+    // staged lines are padded (line_ld); every pass also holds its axis
+    // twiddle table (n complex) in shared memory
+    size_t const ldy = line_ld(maxM1), ldx = line_ld(maxM0);
+    m_tile_y = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / ldy)));
     // x pass: three line buffers (phi, field lines, scratch) of T kz columns
     size_t const x_budget = 96 * 1024;
-    m_tile_x = static_cast<int>(std::max<size_t>(
-        1, std::min<size_t>(16, x_budget / (3 * static_cast<size_t>(maxM0 + 1) * csz))));
+    m_tile_x = static_cast<int>(
+        std::max<size_t>(1, std::min<size_t>(16, x_budget / (3 * ldx * csz))));
     size_t smem_zf = 0, smem_zi = 0;
     for (int r = 0; r < R; ++r) {
       auto const &G = m_geom[r];
       int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
       int const H = M2 / 2 + 1;
       int const lines = M0 * M1;
+      int const ldz = line_ld(M2);
       // forward z: two real lines per complex transform
-      int const lz = static_cast<int>(std::max<size_t>(1, cap / M2)) * 2;
+      int const lz = static_cast<int>(std::max<size_t>(1, cap / ldz)) * 2;
       for (int l = 0; l < lines; l += lz)
         zf.push_back(Blk{r, l, std::min(lz, lines - l), 0});
       smem_zf = std::max(smem_zf,
-                         2 * static_cast<size_t>((std::min(lz, lines) + 1) / 2) * M2 * csz);
+                         (2 * static_cast<size_t>((std::min(lz, lines) + 1) / 2) * ldz + M2) * csz);
       // backward z: nl lines -> nl (Ex, Ey) + ceil(nl/2) (Ez pairs) transforms
-      int const lzi = static_cast<int>(std::max<size_t>(1, 2 * (cap / M2) / 3));
+      int const lzi = static_cast<int>(std::max<size_t>(1, 2 * (cap / ldz) / 3));
       for (int l = 0; l < lines; l += lzi)
         zi.push_back(Blk{r, l, std::min(lzi, lines - l), 0});
       int const nzi = std::min(lzi, lines);
-      smem_zi = std::max(smem_zi, 2 * static_cast<size_t>(nzi + (nzi + 1) / 2) * M2 * csz);
+      size_t const nci = nzi + (nzi + 1) / 2;
+      smem_zi = std::max(smem_zi, (nci * ldz + z_inv_b_size(nzi, M2) + M2) * csz);
       for (int xx = 0; xx < M0; ++xx)
         for (int k0 = 0; k0 < H; k0 += m_tile_y)
           y.push_back(Blk{r, xx, k0, 0});
@@ -353,8 +358,8 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     }
     m_smem_zf = smem_zf;
     m_smem_zi = smem_zi;
-    m_smem_y = 2 * static_cast<size_t>(m_tile_y) * (maxM1 + 1) * csz;
-    m_smem_x = 3 * static_cast<size_t>(m_tile_x) * (maxM0 + 1) * csz;
+    m_smem_y = (2 * static_cast<size_t>(m_tile_y) * ldy + maxM1) * csz;
+    m_smem_x = (3 * static_cast<size_t>(m_tile_x) * ldx + maxM0) * csz;
     m_n_blk_zf = static_cast<int>(zf.size());
     m_n_blk_y = static_cast<int>(y.size());
     m_n_blk_x = static_cast<int>(x.size());

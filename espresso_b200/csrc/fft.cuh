@@ -26,6 +26,44 @@ struct Blk {
   int pad;
 };
 
+// Shared-memory position of element i of a staged line: one pad slot per 16
+// elements, so the stride-R accesses of the early Stockham stages (and the
+// stride-16 transposed loads) fall into distinct banks.
+__host__ __device__ inline int pix(int i) { return i + (i >> 4); }
+// Line stride (elements) of staged lines of length n: padded length, odd so
+// that consecutive lines start in different banks.
+__host__ __device__ inline int line_ld(int n) { return (n + ((n - 1) >> 4)) | 1; }
+
+// Batched global -> shared copy: each thread issues U loads before its
+// stores, so U loads are in flight per thread.
+template <int U, typename L, typename S>
+__device__ inline void staged_copy(int total, L const &load, S const &store) {
+  for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
+    decltype(load(0)) v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      int const e = e0 + u * blockDim.x;
+      if (e < total)
+        v[u] = load(e);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      int const e = e0 + u * blockDim.x;
+      if (e < total)
+        store(e, v[u]);
+    }
+  }
+}
+
+// Copy the twiddle table exp(-2 pi i k / n), k < n, of one axis to shared
+// memory (caller synchronises).
+template <typename C>
+__device__ inline void load_twiddles(C *dst, const C *__restrict__ twtab, AxisPlan const &pl) {
+  const C *src = twtab + pl.tw_off;
+  for (int k = threadIdx.x; k < pl.n; k += blockDim.x)
+    dst[k] = src[k];
+}
+
 template <typename C> __device__ inline C ld_tw(const C *__restrict__ tw, int k, bool inv) {
   C w = tw[k];
   if (inv)
@@ -189,7 +227,7 @@ __device__ inline void fft_stage_t(const C *src, C *dst, int n, int ld, int nlin
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      v[r] = s[j + r * nb];
+      v[r] = s[pix(j + r * nb)];
       if (r > 0 && jm != 0)
         v[r] = cmul(v[r], ld_tw(tw, r * jm * tstride, inv));
     }
@@ -197,7 +235,7 @@ __device__ inline void fft_stage_t(const C *src, C *dst, int n, int ld, int nlin
     int const base = jq * Ns * R + jm;
 #pragma unroll
     for (int r = 0; r < R; ++r)
-      d[base + r * Ns] = v[r];
+      d[pix(base + r * Ns)] = v[r];
   }
 }
 
@@ -215,24 +253,24 @@ __device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int ld, int nl
     int const jm = j % Ns;
     C v[32];
     for (int r = 0; r < R; ++r) {
-      v[r] = s[j + r * nb];
+      v[r] = s[pix(j + r * nb)];
       if (r > 0 && jm != 0)
         v[r] = cmul(v[r], ld_tw(tw, r * jm * tstride, inv));
     }
     dft_dyn(v, R, tw, n, inv);
     int const base = (j / Ns) * Ns * R + jm;
     for (int r = 0; r < R; ++r)
-      d[base + r * Ns] = v[r];
+      d[pix(base + r * Ns)] = v[r];
   }
 }
 
-// Full transform of nlines lines in `a` (scratch `b`); returns the buffer
-// holding the result.  All threads of the block must call it.
+// Full transform of nlines lines in `a` (scratch `b`; element i of line l at
+// l*ld + pix(i)); tw = the axis twiddle table (shared memory).  Returns the
+// buffer holding the result.  All threads of the block must call it.
 template <typename C>
 __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
-                        const C *__restrict__ twtab, bool inv) {
+                        const C *__restrict__ tw, bool inv) {
   int const n = pl.n;
-  const C *tw = twtab + pl.tw_off;
   int Ns = 1;
   C *src = a, *dst = b;
   for (int s = 0; s < pl.nstages; ++s) {
@@ -260,38 +298,47 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
 // Two real lines per complex transform: Z = x0 + i x1, then
 // X0[k] = (Z[k] + conj Z[n-k]) / 2 and X1[k] = -i (Z[k] - conj Z[n-k]) / 2.
 // bk.b real lines per block (an odd last line is paired with zeros).
+// Shared memory: 2 x ceil(bk.b/2) staged lines of line_ld(n), twiddles (n).
 template <typename Real>
-__global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
-                            const Real *__restrict__ rmesh,
-                            typename CplxOf<Real>::type *__restrict__ cmesh,
-                            const typename CplxOf<Real>::type *__restrict__ twtab) {
+__global__ void __launch_bounds__(256)
+k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+            const Real *__restrict__ rmesh, typename CplxOf<Real>::type *__restrict__ cmesh,
+            const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
   RepGeom const &G = reps[bk.rep];
   int const n = G.mesh[2];
-  int const nl = bk.b;            // real lines in this block
-  int const np = (nl + 1) >> 1;   // complex lines
+  int const ld = line_ld(n);
+  int const nl = bk.b;          // real lines in this block
+  int const np = (nl + 1) >> 1; // complex lines
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + np * n;
+  C *b = a + np * ld;
+  C *tw = b + np * ld;
+  load_twiddles(tw, twtab, G.plan[2]);
   long long const line0 = bk.a;
   const Real *src = rmesh + G.rm_off + line0 * n;
-  for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
-    int const j = e / n, k = e - j * n;
-    Real const re = src[(2 * j) * n + k];
-    Real const im = (2 * j + 1 < nl) ? src[(2 * j + 1) * n + k] : Real(0);
-    a[e] = C{re, im};
-  }
+  // real line element e = l*n + k -> real or imaginary part of slot l/2
+  Real *ar = reinterpret_cast<Real *>(a);
+  staged_copy<8>(
+      nl * n, [&](int e) { return src[e]; },
+      [&](int e, Real v) {
+        int const l = e / n, k = e - l * n;
+        ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = v;
+      });
+  if (nl & 1) // odd count: zero imaginary parts of the last slot
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+      ar[2 * ((np - 1) * ld + pix(k)) + 1] = Real(0);
   __syncthreads();
-  C *res = fft_lines<C>(a, b, np, n, G.plan[2], twtab, false);
+  C *res = fft_lines<C>(a, b, np, ld, G.plan[2], tw, false);
   int const H = n / 2 + 1;
   int const hp = G.hp;
   for (int e = threadIdx.x; e < nl * hp; e += blockDim.x) {
     int const l = e / hp, k = e - l * hp;
     C v{Real(0), Real(0)};
     if (k < H) {
-      C const z = res[(l >> 1) * n + k];
-      C const zc = res[(l >> 1) * n + ((n - k) % n)];
+      C const z = res[(l >> 1) * ld + pix(k)];
+      C const zc = res[(l >> 1) * ld + pix((n - k) % n)];
       if ((l & 1) == 0)
         v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
       else
@@ -302,11 +349,12 @@ __global__ void k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restr
 }
 
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
+// Shared memory: 2 x tile staged lines of line_ld(M1), twiddles (M1).
 template <typename Real>
-__global__ void k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
-                        typename CplxOf<Real>::type *__restrict__ c0,
-                        long long field_stride, int tile, bool inv,
-                        const typename CplxOf<Real>::type *__restrict__ twtab) {
+__global__ void __launch_bounds__(256)
+k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+        typename CplxOf<Real>::type *__restrict__ c0, long long field_stride, int tile,
+        bool inv, const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
@@ -316,33 +364,44 @@ __global__ void k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict_
   int const H = G.mesh[2] / 2 + 1;
   int const x = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
-  int const ld = M1 + 1; // padded line stride: conflict-free transposed staging
+  int const ld = line_ld(M1);
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + T * ld;
-  long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp;
-  for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
-    int const y = e / T, t = e - y * T;
-    a[t * ld + y] = cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t];
-  }
+  C *b = a + tile * ld;
+  C *tw = b + tile * ld;
+  load_twiddles(tw, twtab, G.plan[1]);
+  long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp + kz0;
+  long long const hp = G.hp;
+  staged_copy<8>(
+      T * M1,
+      [&](int e) {
+        int const y = e / T, t = e - y * T;
+        return cm[rowbase + y * hp + t];
+      },
+      [&](int e, C v) {
+        int const y = e / T, t = e - y * T;
+        a[t * ld + pix(y)] = v;
+      });
   __syncthreads();
-  C *res = fft_lines<C>(a, b, T, ld, G.plan[1], twtab, inv);
+  C *res = fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
   for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
     int const y = e / T, t = e - y * T;
-    cm[rowbase + static_cast<long long>(y) * G.hp + kz0 + t] = res[t * ld + y];
+    cm[rowbase + y * hp + t] = res[t * ld + pix(y)];
   }
 }
 
 // ---- pass x fused with the k-space operator -----------------------------
 // Per block: one ky, a tile of kz; partials[blk*8 + {E, Pxx, Pxy, Pxz, Pyy,
 // Pyz, Pzz, diag}] in FP64 (Hermitian weights 1 for kz = 0, M2/2, else 2).
+// Shared memory: 3 x tile staged lines of line_ld(M0) (phi, field lines,
+// scratch), twiddles (M0).
 template <typename Real>
-__global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
-                               const typename CplxOf<Real>::type *__restrict__ rho_hat,
-                               const Real *__restrict__ ginf,
-                               typename CplxOf<Real>::type *__restrict__ field0,
-                               long long field_stride, int tile, int want_fields,
-                               int want_ev, double *__restrict__ partials,
-                               const typename CplxOf<Real>::type *__restrict__ twtab) {
+__global__ void __launch_bounds__(256)
+k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+               const typename CplxOf<Real>::type *__restrict__ rho_hat,
+               const Real *__restrict__ ginf, typename CplxOf<Real>::type *__restrict__ field0,
+               long long field_stride, int tile, int want_fields, int want_ev,
+               double *__restrict__ partials,
+               const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
@@ -351,19 +410,27 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   int const H = M2 / 2 + 1;
   int const y = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
-  int const ld = M0 + 1; // padded line stride
-  int const L = T * ld;
+  int const ld = line_ld(M0);
+  int const L = tile * ld;
   C *a = reinterpret_cast<C *>(smem_raw);
   C *b = a + L;
   C *c = b + L; // three line buffers: phi, field lines, FFT scratch
+  C *tw = c + L;
+  load_twiddles(tw, twtab, G.plan[0]);
   long long const stride_x = static_cast<long long>(M1) * G.hp;
   long long const base = G.km_off + static_cast<long long>(y) * G.hp + kz0;
-  for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
-    int const x = e / T, t = e - x * T;
-    a[t * ld + x] = rho_hat[base + x * stride_x + t];
-  }
+  staged_copy<8>(
+      T * M0,
+      [&](int e) {
+        int const x = e / T, t = e - x * T;
+        return rho_hat[base + x * stride_x + t];
+      },
+      [&](int e, C v) {
+        int const x = e / T, t = e - x * T;
+        a[t * ld + pix(x)] = v;
+      });
   __syncthreads();
-  C *res = fft_lines<C>(a, b, T, ld, G.plan[0], twtab, false);
+  C *res = fft_lines<C>(a, b, T, ld, G.plan[0], tw, false);
   C *fb = (res == a) ? b : a; // field lines go to the free buffer
   // k-space operator
   double const wv[3] = {2.0 * kPi * G.box_i[0], 2.0 * kPi * G.box_i[1],
@@ -374,9 +441,10 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
   auto dop = [](int i, int m) { return (i == m / 2) ? 0 : (i < m / 2 ? i : i - m); };
   int const kyd = dop(y, M1);
   for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
-    int const t = e / M0, x = e - t * M0;
+    // t fastest: the influence-function reads are T-contiguous rows
+    int const x = e / T, t = e - x * T;
     int const kz = kz0 + t;
-    C const rh = res[t * ld + x];
+    C const rh = res[t * ld + pix(x)];
     Real const g = ginf[base + x * stride_x + t];
     int const kxd = dop(x, M0), kzd = dop(kz, M2);
     if (want_ev) {
@@ -398,7 +466,7 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
       }
     }
     // phi = G rho_hat replaces rho_hat in place (same thread, same point)
-    res[t * ld + x] = C{g * rh.x, g * rh.y};
+    res[t * ld + pix(x)] = C{g * rh.x, g * rh.y};
   }
   if (want_ev) {
     // block reduction of the 8 partial sums (fixed order -> deterministic)
@@ -434,50 +502,80 @@ __global__ void k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__re
       int const t = e / M0, x = e - t * M0;
       int const kd = (d == 0) ? dop(x, M0) : (d == 1 ? kvec_y : dop(kz0 + t, M2));
       Real const k = static_cast<Real>(kd) * wd;
-      C const phi = res[t * ld + x];
-      fb[t * ld + x] = C{-k * phi.y, k * phi.x};
+      C const phi = res[t * ld + pix(x)];
+      fb[t * ld + pix(x)] = C{-k * phi.y, k * phi.x};
     }
     __syncthreads();
-    C *fres = fft_lines<C>(fb, c, T, ld, G.plan[0], twtab, true);
+    C *fres = fft_lines<C>(fb, c, T, ld, G.plan[0], tw, true);
     for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
       int const x = e / T, t = e - x * T;
-      field0[field_stride * d + base + x * stride_x + t] = fres[t * ld + x];
+      field0[field_stride * d + base + x * stride_x + t] = fres[t * ld + pix(x)];
     }
   }
 }
 
 // ---- pass z, backward for the 3 field components -> real fields --------
+// Stride of a staged half row and size (elements) of the second buffer,
+// which holds either the FFT scratch lines or the 3 nl staged half rows.
+__host__ __device__ inline int z_inv_half_ld(int n) { return (n / 2 + 2) | 1; }
+__host__ __device__ inline int z_inv_b_size(int nl, int n) {
+  int const nc = nl + (nl + 1) / 2;
+  int const s1 = nc * line_ld(n), s2 = 3 * nl * z_inv_half_ld(n);
+  return s1 > s2 ? s1 : s2;
+}
+
 // Two real outputs per complex transform: slot l < nl carries Ex + i Ey of
 // line l, slot nl + j carries Ez of lines 2j and 2j+1.  Each half row is
 // extended by Hermitian symmetry with the imaginary parts of the k = 0 and
 // k = n/2 entries dropped (c2r semantics), so both packed outputs are real.
+// Shared memory: 2 x (nl + ceil(nl/2)) staged lines of line_ld(n),
+// twiddles (n).
 template <typename Real>
-__global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
-                             const typename CplxOf<Real>::type *__restrict__ field0,
-                             long long field_stride, Real *__restrict__ efield,
-                             const typename CplxOf<Real>::type *__restrict__ twtab) {
+__global__ void __launch_bounds__(256)
+k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
+             const typename CplxOf<Real>::type *__restrict__ field0, long long field_stride,
+             Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
   RepGeom const &G = reps[bk.rep];
   int const n = G.mesh[2];
   int const H = n / 2 + 1;
+  int const ld = line_ld(n);
   int const nl = bk.b;
   int const nz = (nl + 1) >> 1;
   int const nc = nl + nz;
   long long const line0 = bk.a;
+  // b doubles as the staging area of the 3 nl half rows (stride hl)
+  int const hl = z_inv_half_ld(n);
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + nc * n;
-  // Hermitian-extended entry k of field d, line l of this block
+  C *b = a + nc * ld;
+  C *tw = b + z_inv_b_size(nl, n);
+  load_twiddles(tw, twtab, G.plan[2]);
+  // stage the half rows (H entries of each of 3 nl rows; field d, line l at
+  // b[(d * nl + l) * hl]), then build the packed lines in a
+  const C *fsrc = field0 + G.km_off + line0 * G.hp;
+  staged_copy<8>(
+      3 * nl * H,
+      [&](int e) {
+        int const dl = e / H, k = e - dl * H;
+        int const d = dl / nl, l = dl - d * nl;
+        return fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
+      },
+      [&](int e, C v) {
+        int const dl = e / H, k = e - dl * H;
+        b[dl * hl + k] = v;
+      });
+  __syncthreads();
   auto herm = [&](int d, int l, int k) -> C {
-    const C *src = field0 + field_stride * d + G.km_off + (line0 + l) * G.hp;
+    const C *row = b + (d * nl + l) * hl;
     if (k < H) {
-      C v = src[k];
+      C v = row[k];
       if (k == 0 || 2 * k == n)
         v.y = Real(0);
       return v;
     }
-    return cconj(src[n - k]);
+    return cconj(row[n - k]);
   };
   for (int e = threadIdx.x; e < nc * n; e += blockDim.x) {
     int const j = e / n, k = e - j * n;
@@ -490,18 +588,18 @@ __global__ void k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__rest
       X = herm(2, l0, k);
       Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
     }
-    a[e] = C{X.x - Y.y, X.y + Y.x};
+    a[j * ld + pix(k)] = C{X.x - Y.y, X.y + Y.x};
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, nc, n, G.plan[2], twtab, true);
+  C *res = fft_lines<C>(a, b, nc, ld, G.plan[2], tw, true);
   // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
   // interpolation gathers one 16-byte (FP32) record per stencil point
   using R4 = typename Real4Of<Real>::type;
   R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
     int const l = e / n, k = e - l * n;
-    C const xy = res[e];
-    C const zz = res[(nl + (l >> 1)) * n + k];
+    C const xy = res[l * ld + pix(k)];
+    C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
     R4 v;
     v.x = xy.x;
     v.y = xy.y;
