@@ -93,6 +93,27 @@ struct RepGeom {
   int max_nb;
 };
 
+// Batched global -> shared copy: each thread issues U loads before its
+// stores, so U loads are in flight per thread.
+template <int U, typename L, typename S>
+__device__ inline void staged_copy(int total, L const &load, S const &store) {
+  for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
+    decltype(load(0)) v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      int const e = e0 + u * blockDim.x;
+      if (e < total)
+        v[u] = load(e);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      int const e = e0 + u * blockDim.x;
+      if (e < total)
+        store(e, v[u]);
+    }
+  }
+}
+
 inline int ceil_div(long long a, long long b) {
   return static_cast<int>((a + b - 1) / b);
 }

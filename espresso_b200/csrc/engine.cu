@@ -227,7 +227,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   size_t const csz = m_fp32 ? sizeof(float2) : sizeof(double2);
   size_t const cap = m_fp32 ? 4096 : 2048; // complex elements per smem buffer
   {
-    std::vector<int2> bm, bc, bcen, bp;
+    std::vector<int2> bm, bc, bcen, bp, nat;
     m_run = 4; // weight-record padding (R) used by every assignment/interp kernel
     m_blk_census_start.assign(1, 0);
     m_blk_pair_start.assign(1, 0);
@@ -277,6 +277,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         return col;
       };
       std::vector<std::vector<int2>> phase;
+      nat.clear();
       m_tile_cap = 1;
       for (int r = 0; r < R; ++r) {
         auto const &G = m_geom[r];
@@ -292,6 +293,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
               if (static_cast<int>(phase.size()) <= p)
                 phase.resize(p + 1);
               phase[p].push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
+              nat.push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
             }
       }
       m_phase_off.assign(1, 0);
@@ -305,6 +307,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     m_n_blk_census = static_cast<int>(bcen.size());
     m_n_blk_pair = static_cast<int>(bp.size());
     upload_vec(m_blk_mesh, bm, st);
+    upload_vec(m_blk_brick, nat, st);
     upload_vec(m_blk_cplx, bc, st);
     upload_vec(m_blk_census, bcen, st);
     upload_vec(m_blk_pair, bp, st);
@@ -389,10 +392,16 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         aset(k_p3m_assign<float, 1>); aset(k_p3m_assign<float, 2>); aset(k_p3m_assign<float, 3>);
         aset(k_p3m_assign<float, 4>); aset(k_p3m_assign<float, 5>); aset(k_p3m_assign<float, 6>);
         aset(k_p3m_assign<float, 7>);
+        aset(k_p3m_interp<float, 1>); aset(k_p3m_interp<float, 2>); aset(k_p3m_interp<float, 3>);
+        aset(k_p3m_interp<float, 4>); aset(k_p3m_interp<float, 5>); aset(k_p3m_interp<float, 6>);
+        aset(k_p3m_interp<float, 7>);
       } else {
         aset(k_p3m_assign<double, 1>); aset(k_p3m_assign<double, 2>); aset(k_p3m_assign<double, 3>);
         aset(k_p3m_assign<double, 4>); aset(k_p3m_assign<double, 5>); aset(k_p3m_assign<double, 6>);
         aset(k_p3m_assign<double, 7>);
+        aset(k_p3m_interp<double, 1>); aset(k_p3m_interp<double, 2>); aset(k_p3m_interp<double, 3>);
+        aset(k_p3m_interp<double, 4>); aset(k_p3m_interp<double, 5>); aset(k_p3m_interp<double, 6>);
+        aset(k_p3m_interp<double, 7>);
       }
     }
     if (m_fp32) {
@@ -606,10 +615,14 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   mark("fft_inv_yz", st);
   // 6. force back-interpolation
   if (m_n > 0) {
-    P3MX_CAO_DISPATCH(cao, (k_p3m_interp<Real, P, R><<<ceil_div(8 * m_n, 256), 256, 0, st>>>(
-                               geom, m_perm.as<int>(), m_rep_of.as<int>(), m_skey.as<int>(),
-                               m_W.as<Real>(), m_E.as<Real>(), d_q(), m_dipole.as<double>(),
-                               m_n, f, overwrite ? 1 : 0)));
+    using R4 = typename Real4Of<Real>::type;
+    int const nbr = m_phase_off.back();
+    P3MX_CAO_DISPATCH_R(cao, (k_p3m_interp<Real, P><<<nbr, 32 * kAssignWarps,
+                                 static_cast<size_t>(m_tile_cap) * sizeof(R4), st>>>(
+                                 geom, m_blk_brick.as<int2>(), nbr, m_start.as<int>(),
+                                 m_perm.as<int>(), m_skey.as<int>(), m_W.as<Real>(),
+                                 m_E.as<Real>(), d_q(), m_dipole.as<double>(), f,
+                                 overwrite ? 1 : 0)));
     ++m_launches;
   }
   mark("p3m_interp", st);

@@ -156,6 +156,7 @@ private:
   // tables
   DevBuf m_geom_d, m_rep_of, m_tw, m_ia_d;
   DevBuf m_blk_mesh, m_blk_cplx, m_blk_census, m_blk_pair;
+  DevBuf m_blk_brick; // all bricks in spatial order (interpolation)
   DevBuf m_blk_zf, m_blk_y, m_blk_x, m_blk_zi;
   std::vector<int> m_blk_x_start, m_blk_census_start, m_blk_pair_start;
   DevBuf m_blk_x_start_d, m_blk_census_start_d, m_blk_pair_start_d;

@@ -34,27 +34,6 @@ __host__ __device__ inline int pix(int i) { return i + (i >> 4); }
 // that consecutive lines start in different banks.
 __host__ __device__ inline int line_ld(int n) { return (n + ((n - 1) >> 4)) | 1; }
 
-// Batched global -> shared copy: each thread issues U loads before its
-// stores, so U loads are in flight per thread.
-template <int U, typename L, typename S>
-__device__ inline void staged_copy(int total, L const &load, S const &store) {
-  for (int e0 = threadIdx.x; e0 < total; e0 += U * blockDim.x) {
-    decltype(load(0)) v[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      int const e = e0 + u * blockDim.x;
-      if (e < total)
-        v[u] = load(e);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      int const e = e0 + u * blockDim.x;
-      if (e < total)
-        store(e, v[u]);
-    }
-  }
-}
-
 // Copy the twiddle table exp(-2 pi i k / n), k < n, of one axis to shared
 // memory (caller synchronises).
 template <typename C>

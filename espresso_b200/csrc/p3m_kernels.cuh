@@ -329,96 +329,137 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   }
 }
 
-// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373).
-// Eight lanes serve one corner-sorted particle: lane kz owns the stencil
-// z-offset kz and walks the P^2 (x, y) rows, so the lanes of a group read
-// P consecutive (Ex, Ey, Ez, 0) records of one row together (one or two
-// cache lines per group instead of one line per lane).  Lane sums are FP32
-// over the P^2 rows; the group reduction is FP64 in a fixed shuffle order.
-// F -= prefactor/V * sum (q wx wy wz) E, plus the dipole term for
-// epsilon != 0 (p3m.cpp:540-547).  Writes (or adds) f[3*i] of the original
-// particle index.
-template <typename Real, int P, int R>
-__global__ void __launch_bounds__(256)
-k_p3m_interp(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
-             const int *__restrict__ rep_of, const int *__restrict__ s_key,
-             const Real *__restrict__ W, const Real *__restrict__ E,
-             const double *__restrict__ q, const double *__restrict__ dipole,
-             long long n, double *__restrict__ f, int overwrite) {
+// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373),
+// one block of kAssignWarps warps per brick.  The block first copies the
+// brick's field tile -- (B+P-1)^3 packed (Ex, Ey, Ez, 0) records around the
+// brick, periodic images folded in -- into shared memory with batched
+// coalesced loads; the particles of the brick (one contiguous range of the
+// brick-major order) then read only shared memory.  Eight lanes serve one
+// particle: lane kz owns the stencil z offset kz and walks the P^2 (x, y)
+// rows; lane sums are FP32, the group reduction is FP64 in a fixed shuffle
+// order (deterministic).  F -= prefactor/V * sum (q wx wy wz) E, plus the
+// dipole term for epsilon != 0 (p3m.cpp:540-547).  Writes (or adds) f[3*i] of
+// the original particle index.
+template <typename Real, int P>
+__global__ void __launch_bounds__(32 * kAssignWarps)
+k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
+             const int *__restrict__ start, const int *__restrict__ perm,
+             const int *__restrict__ s_key, const Real *__restrict__ W,
+             const Real *__restrict__ E, const double *__restrict__ q,
+             const double *__restrict__ dipole, double *__restrict__ f, int overwrite) {
   static_assert(P <= 8, "one lane per stencil z offset");
-  long long const s = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
-  int const kz = threadIdx.x & 7;
-  bool const live = s < n;
-  int i = 0, r = 0;
-  if (live) {
-    i = perm[s];
-    r = rep_of[i];
-  }
-  RepGeom const &G = reps[r];
-  Real ax = Real(0), ay = Real(0), az = Real(0);
-  if (live && kz < P) {
-    int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-    int cx, cy, cz;
-    corner_of(G, s_key[s], cx, cy, cz);
-    const Real *w = W + s * wstride<P, R>();
-    Real wx[P], wy[P];
+  constexpr int R = 4;
+  constexpr int WS = wstride<P, R>();
+  constexpr int WZ = wz_off<P, R>();
+  constexpr int NT = 32 * kAssignWarps;
+  using R4 = typename Real4Of<Real>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (static_cast<int>(blockIdx.x) >= nbricks)
+    return; // whole block
+  int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int2 const bk = bricks[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  int const B = G.brick, B3 = B * B * B, Ed = B + P - 1, E2 = Ed * Ed;
+  const int *st = start + G.bin_off;
+  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
+  if (s0 == s1)
+    return; // no particles in this brick
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
+  int const x0 = bx * B, y0 = by * B, z0 = bz * B;
+  R4 *tile = reinterpret_cast<R4 *>(smem_raw);
+  const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off;
+  auto wrap = [](int v, int m) {
+    while (v >= m)
+      v -= m;
+    return v;
+  };
+  // tile rows (x, y) of Ed records along z; lane groups of gs lanes copy one
+  // row each with asynchronous 16-byte copies (cp.async, L2 only), all in
+  // flight together
+  int const gs = (Ed <= 8) ? 8 : (Ed <= 16 ? 16 : 32);
+  int const rpw = 32 / gs;
+  int const zl = lane & (gs - 1);
+  int const gz = wrap(z0 + zl, M2);
+  for (int row = warp * rpw + lane / gs; row < E2; row += kAssignWarps * rpw) {
+    int const x = row / Ed, y = row - x * Ed;
+    if (zl < Ed) {
+      long long const gx = wrap(x0 + x, M0), gy = wrap(y0 + y, M1);
+      const R4 *src = E4 + (gx * M1 + gy) * M2 + gz;
+      R4 *dst = tile + row * Ed + zl;
 #pragma unroll
-    for (int k = 0; k < P; ++k) {
-      wx[k] = w[k];
-      wy[k] = w[P + k];
+      for (int h = 0; h < static_cast<int>(sizeof(R4) / 16); ++h)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                         static_cast<unsigned>(__cvta_generic_to_shared(
+                             reinterpret_cast<char *>(dst) + 16 * h))),
+                     "l"(reinterpret_cast<const char *>(src) + 16 * h)
+                     : "memory");
     }
-    Real const wzk = w[wz_off<P, R>() + kz];
-    int z = cz + kz;
-    if (z >= M2)
-      z -= M2;
-    using R4 = typename Real4Of<Real>::type;
-    const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off + z;
-#pragma unroll 1
-    for (int kx = 0; kx < P; ++kx) {
-      int gx = cx + kx;
-      if (gx >= M0)
-        gx -= M0;
-      Real const wxz = wx[kx] * wzk;
-      long long const xrow = static_cast<long long>(gx) * M1;
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  int const g = lane >> 3, kz = lane & 7;
+  double const pref = G.prefactor / G.V;
+  double const cdip = (G.epsilon != 0.0)
+                          ? G.prefactor * 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0)
+                          : 0.0;
+  // four particles per warp (one per 8-lane group), warps interleaved
+  for (int sb = s0 + 4 * warp; sb < s1; sb += 4 * kAssignWarps) {
+    int const s = sb + g;
+    bool const live = s < s1;
+    Real ax = Real(0), ay = Real(0), az = Real(0);
+    if (live && kz < P) {
+      int const l = s_key[s] - bk.y * B3;
+      int const lx = l / (B * B), ly = (l / B) % B, lz = l % B;
+      const Real *w = W + static_cast<long long>(s) * WS;
+      Real wx[P], wy[P];
 #pragma unroll
-      for (int ky = 0; ky < P; ++ky) {
-        int gy = cy + ky;
-        if (gy >= M1)
-          gy -= M1;
-        R4 const e = E4[(xrow + gy) * M2];
-        Real const wt = wxz * wy[ky];
-        ax += wt * e.x;
-        ay += wt * e.y;
-        az += wt * e.z;
+      for (int k = 0; k < P; ++k) {
+        wx[k] = w[k];
+        wy[k] = w[P + k];
+      }
+      Real const wzk = w[WZ + kz];
+      const R4 *tp = tile + (lx * Ed + ly) * Ed + lz + kz;
+#pragma unroll
+      for (int kx = 0; kx < P; ++kx) {
+        Real const wxz = wx[kx] * wzk;
+#pragma unroll
+        for (int ky = 0; ky < P; ++ky) {
+          R4 const e = tp[(kx * Ed + ky) * Ed];
+          Real const wt = wxz * wy[ky];
+          ax += wt * e.x;
+          ay += wt * e.y;
+          az += wt * e.z;
+        }
       }
     }
-  }
-  double fx = static_cast<double>(ax), fy = static_cast<double>(ay), fz = static_cast<double>(az);
+    double fx = static_cast<double>(ax), fy = static_cast<double>(ay),
+           fz = static_cast<double>(az);
 #pragma unroll
-  for (int o = 1; o < 8; o <<= 1) {
-    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-    fz += __shfl_xor_sync(0xffffffffu, fz, o);
-  }
-  if (!live || kz != 0)
-    return;
-  double const pref = G.prefactor / G.V;
-  double ox = -pref * fx, oy = -pref * fy, oz = -pref * fz;
-  if (G.epsilon != 0.0) {
-    double const qi = q[i];
-    double const c = G.prefactor * 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0);
-    ox -= qi * c * dipole[3 * r + 0];
-    oy -= qi * c * dipole[3 * r + 1];
-    oz -= qi * c * dipole[3 * r + 2];
-  }
-  if (overwrite) {
-    f[3 * i + 0] = ox;
-    f[3 * i + 1] = oy;
-    f[3 * i + 2] = oz;
-  } else {
-    f[3 * i + 0] += ox;
-    f[3 * i + 1] += oy;
-    f[3 * i + 2] += oz;
+    for (int o = 1; o < 8; o <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+      fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (live && kz == 0) {
+      int const i = perm[s];
+      double ox = -pref * fx, oy = -pref * fy, oz = -pref * fz;
+      if (cdip != 0.0) {
+        double const qi = q[i];
+        ox -= qi * cdip * dipole[3 * bk.x + 0];
+        oy -= qi * cdip * dipole[3 * bk.x + 1];
+        oz -= qi * cdip * dipole[3 * bk.x + 2];
+      }
+      if (overwrite) {
+        f[3 * i + 0] = ox;
+        f[3 * i + 1] = oy;
+        f[3 * i + 2] = oz;
+      } else {
+        f[3 * i + 0] += ox;
+        f[3 * i + 1] += oy;
+        f[3 * i + 2] += oz;
+      }
+    }
   }
 }
 
