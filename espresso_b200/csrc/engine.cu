@@ -430,7 +430,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_start.ensure((m_nkeys + 1) * sizeof(int));
   m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
-  m_W.ensure((3 * 7 + 2 * 3) * n * rsz);
+  m_W.ensure(static_cast<size_t>(wstride<7, 4>()) * n * rsz);
   m_skey.ensure(n * sizeof(int));
   m_rho.ensure(m_bins * rsz);
   m_E.ensure(4 * m_bins * rsz);

@@ -84,7 +84,11 @@ __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restric
 // {q*wx[0..P), wy[0..P), 0[R-1], wz[0..P), 0[R-1]}.  The zero padding lets a
 // thread that owns R consecutive z points read the weight of every point of
 // its run without a branch (out-of-stencil points read zero).
-template <int P, int R> __host__ __device__ constexpr int wstride() { return 3 * P + 2 * (R - 1); }
+// Record stride, padded to a multiple of 4 elements (16 bytes in FP32, 32 in
+// FP64) so that runs of records are legal 16-byte asynchronous copies.
+template <int P, int R> __host__ __device__ constexpr int wstride() {
+  return (3 * P + 2 * (R - 1) + 3) / 4 * 4;
+}
 template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
 
 // Weights in corner-sorted order; also the brick-local corner key of every
@@ -146,9 +150,12 @@ constexpr int kAssignChunk = 64;
 // Bytes of dynamic shared memory of one assignment block: the split
 // fixed-point tile (two 32-bit words per point) and one staged chunk of
 // weight records and tile offsets.
+__host__ __device__ constexpr size_t assign_tile_bytes(int tile_cap) {
+  return (2 * sizeof(int) * static_cast<size_t>(tile_cap) + 15) / 16 * 16;
+}
 template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem(int tile_cap) {
-  return 2 * sizeof(int) * static_cast<size_t>(tile_cap) +
-         sizeof(Real) * kAssignChunk * wstride<P, 4>() + sizeof(int) * kAssignChunk;
+  return assign_tile_bytes(tile_cap) + sizeof(Real) * kAssignChunk * wstride<P, 4>() +
+         sizeof(int) * kAssignChunk;
 }
 
 template <typename Real> __device__ inline Real floor_r(Real v);
@@ -206,17 +213,35 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     return; // empty brick: nothing to add
   int *t_hi = reinterpret_cast<int *>(smem_raw);
   unsigned *t_lo = reinterpret_cast<unsigned *>(t_hi + tile_cap);
-  Real *rec = reinterpret_cast<Real *>(t_lo + tile_cap);
+  Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes(tile_cap));
   int *rbase = reinterpret_cast<int *>(rec + CH * WS);
   for (int t = tid; t < E3; t += NT) {
     t_hi[t] = 0;
     t_lo[t] = 0u;
   }
+  // stage a chunk of records (contiguous; asynchronous 16-byte copies) and
+  // each particle's tile base offset
+  auto stage = [&](int c0, int cn) {
+    const char *src = reinterpret_cast<const char *>(W + static_cast<long long>(c0) * WS);
+    unsigned const dst = static_cast<unsigned>(__cvta_generic_to_shared(rec));
+    int const nbytes = cn * WS * static_cast<int>(sizeof(Real));
+    for (int o = 16 * tid; o < nbytes; o += 16 * NT)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + o), "l"(src + o)
+                   : "memory");
+    for (int j = tid; j < cn; j += NT) {
+      int const l = s_key[c0 + j] - bk.y * B3;
+      rbase[j] = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  };
+  int const cnt = s1 - s0;
+  stage(s0, min(CH, cnt));
+  __syncthreads(); // tile zeroed, first chunk staged
   // total |q| of the brick: the x weights of a record are q*wx with wx >= 0
   // summing to 1, so sum_k |q wx_k| = |q|
   double aq = 0.0;
   for (int s = s0 + tid; s < s1; s += NT) {
-    const Real *w = W + static_cast<long long>(s) * WS;
+    const Real *w = (s - s0 < CH) ? rec + (s - s0) * WS : W + static_cast<long long>(s) * WS;
 #pragma unroll
     for (int k = 0; k < P; ++k)
       aq += fabs(static_cast<double>(w[k]));
@@ -233,7 +258,6 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     qabs += s_red[k];
   if (qabs == 0.0)
     return; // all charges zero: the tile would stay zero
-  int const cnt = s1 - s0;
   int const kb = min(24, 32 - (32 - __clz(cnt))); // cnt < 2^(32-kb)
   int ex;
   frexp(qabs * (1.0 + 1e-12), &ex);
@@ -254,17 +278,11 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   }
   for (int c0 = s0; c0 < s1; c0 += CH) {
     int const cn = min(CH, s1 - c0);
-    __syncthreads(); // tile zeroed / previous chunk consumed
-    // stage the chunk: records are contiguous, so the block copies them with
-    // coalesced loads, plus each particle's tile base offset
-    const Real *src = W + static_cast<long long>(c0) * WS;
-    for (int e = tid; e < cn * WS; e += NT)
-      rec[e] = src[e];
-    for (int j = tid; j < cn; j += NT) {
-      int const l = s_key[c0 + j] - bk.y * B3;
-      rbase[j] = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
+    if (c0 != s0) {
+      __syncthreads(); // previous chunk consumed
+      stage(c0, cn);
+      __syncthreads();
     }
-    __syncthreads();
     for (int j = warp; j < cn; j += kAssignWarps) {
       int const base = rbase[j];
       const Real *w = rec + j * WS;
@@ -310,6 +328,42 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     yzg[k2] = gy * M2 + gz;
     ycls[k2] = cls;
   }
+  auto tile_val = [&](int ti) {
+    long long const v = static_cast<long long>(t_hi[ti]) * (1ll << kb) + t_lo[ti];
+    return from_ll<Real>(v) * inv_S;
+  };
+  if (!self_wrap) {
+    // every tile point maps to its own mesh point: issue all of the
+    // thread's mesh loads first, then the adds and stores
+    Real old[EMAX][NS];
+#pragma unroll
+    for (int x = 0; x < EMAX; ++x) {
+      if (x < ex0) {
+        int gx = x0 + x;
+        if (gx >= M0)
+          gx -= M0;
+        long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+          if (yzt[k2] >= 0)
+            old[x][k2] = mesh[gbase + yzg[k2]];
+      }
+    }
+#pragma unroll
+    for (int x = 0; x < EMAX; ++x) {
+      if (x < ex0) {
+        int gx = x0 + x;
+        if (gx >= M0)
+          gx -= M0;
+        long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+          if (yzt[k2] >= 0)
+            mesh[gbase + yzg[k2]] = old[x][k2] + tile_val(x * E * E + yzt[k2]);
+      }
+    }
+    return;
+  }
   for (int pass = 0; pass < passes; ++pass) {
     for (int x = 0; x < ex0; ++x) {
       int gx = x0 + x, xcls = 0;
@@ -318,11 +372,9 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
       long long const gbase = static_cast<long long>(gx) * M1 * M2;
 #pragma unroll
       for (int k2 = 0; k2 < NS; ++k2) {
-        if (yzt[k2] < 0 || (self_wrap && (xcls | ycls[k2]) != pass))
+        if (yzt[k2] < 0 || (xcls | ycls[k2]) != pass)
           continue;
-        int const ti = x * E * E + yzt[k2];
-        long long const v = static_cast<long long>(t_hi[ti]) * (1ll << kb) + t_lo[ti];
-        mesh[gbase + yzg[k2]] += from_ll<Real>(v) * inv_S;
+        mesh[gbase + yzg[k2]] += tile_val(x * E * E + yzt[k2]);
       }
     }
     __syncthreads();
