@@ -916,8 +916,13 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     double *fd = (dev && f) ? f : e.d_force();
     std::vector<double> enk, virk, ens, virs;
     bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
-    e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &enk, &virk);
-    e.short_range(fd, false, (want_e || want_v) && !obs64, st, &ens, &virs);
+    if (!want_e && !want_v) {
+      // forces only: real-space pairs concurrent with the k-space chain
+      e.forces_overlapped(fd, dev ? ow : true, st);
+    } else {
+      e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &enk, &virk);
+      e.short_range(fd, false, (want_e || want_v) && !obs64, st, &ens, &virs);
+    }
     if (obs64 && (want_e || want_v)) {
       fp64_kspace_observables(h, st, want_e, want_v, enk, virk);
       e.short_range(observables_engine(h).d_force(), true, true, st, &ens, &virs, true);

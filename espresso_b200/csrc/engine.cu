@@ -108,6 +108,14 @@ Engine::Engine(bool fp32) : m_fp32(fp32) {
 }
 
 Engine::~Engine() {
+  if (m_side)
+    cudaStreamSynchronize(m_side);
+  if (m_ev_fork)
+    cudaEventDestroy(m_ev_fork);
+  if (m_ev_join)
+    cudaEventDestroy(m_ev_join);
+  if (m_side)
+    cudaStreamDestroy(m_side);
   if (m_stream)
     cudaStreamDestroy(m_stream);
 }
@@ -613,7 +621,9 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   k_fft_z_inv3<Real><<<m_n_blk_zi, 256, m_smem_zi, st>>>(geom, m_blk_zi.as<Blk>(), m_field.as<C>(),
                                                          m_cplx, m_E.as<Real>(), tw); ++m_launches;
   mark("fft_inv_yz", st);
-  // 6. force back-interpolation
+  // 6. force back-interpolation (after the concurrent pair kernel, if any)
+  if (m_interp_wait)
+    P3MX_CUDA(cudaStreamWaitEvent(st, m_interp_wait, 0));
   if (m_n > 0) {
     using R4 = typename Real4Of<Real>::type;
     int const nbr = m_phase_off.back();
@@ -735,10 +745,9 @@ void Engine::refresh_sorted_positions(cudaStream_t st) {
                                                     m_spq.as<double4>()); ++m_launches;
 }
 
-template <typename Real>
-void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
-  if (m_n == 0)
-    return;
+// Displacement check (host decision) and list rebuild or sorted-position
+// refresh: after it the pair kernel can run.
+void Engine::prepare_short_range(cudaStream_t st) {
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
   bool rebuild = !m_lists_valid;
@@ -757,6 +766,11 @@ void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t
   else
     refresh_sorted_positions(st);
   mark(rebuild ? "sr_rebuild" : "sr_refresh", st);
+}
+
+template <typename Real>
+void Engine::launch_pair(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
   if (want_ev)
     k_pair_forces<Real, true><<<m_n_blk_pair, 256, smem, st>>>(
@@ -769,7 +783,45 @@ void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t
         m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
         m_part_pair.as<double>());
   ++m_launches;
+}
+
+template <typename Real>
+void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
+  if (m_n == 0)
+    return;
+  prepare_short_range(st);
+  launch_pair<Real>(f, overwrite, want_ev, st);
   mark("pair_forces", st);
+}
+
+// Forces only (no energies or virials): the pair kernel runs on a side
+// stream, concurrently with the k-space chain (sort, assignment, FFTs); the
+// interpolation waits for it and adds the k-space forces on top.
+void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
+  if (m_n == 0 || m_profiling) {
+    long_range(f, overwrite, false, false, st, nullptr, nullptr);
+    short_range(f, false, false, st, nullptr, nullptr);
+    return;
+  }
+  if (m_side == nullptr) {
+    P3MX_CUDA(cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking));
+    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_fork, cudaEventDisableTiming));
+    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_join, cudaEventDisableTiming));
+  }
+  prepare_short_range(st);
+  P3MX_CUDA(cudaEventRecord(m_ev_fork, st));
+  P3MX_CUDA(cudaStreamWaitEvent(m_side, m_ev_fork, 0));
+  if (m_fp32)
+    launch_pair<float>(f, overwrite, false, m_side);
+  else
+    launch_pair<double>(f, overwrite, false, m_side);
+  P3MX_CUDA(cudaEventRecord(m_ev_join, m_side));
+  struct Reset {
+    cudaEvent_t &ev;
+    ~Reset() { ev = nullptr; }
+  } reset{m_interp_wait};
+  m_interp_wait = m_ev_join;
+  long_range(f, false, false, false, st, nullptr, nullptr);
 }
 
 void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,

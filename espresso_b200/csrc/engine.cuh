@@ -100,6 +100,9 @@ public:
   void short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,
                    std::vector<double> *energies, std::vector<double> *virials,
                    bool fp64_math = false);
+  // Forces of the whole path (k-space + real-space + LJ/WCA), no energies:
+  // the pair kernel overlaps the k-space chain on a side stream.
+  void forces_overlapped(double *f, bool overwrite, cudaStream_t st);
   // Graph-capturable short-range evaluation (device-side rebuild decision).
   void short_range_graph(double *f, bool overwrite, cudaStream_t st);
   // Build lists now if invalid (capacity margin factor for graph use).
@@ -130,6 +133,9 @@ private:
                                              cudaStream_t st);
   template <typename Real> void short_range_t(double *f, bool overwrite, bool want_ev,
                                               cudaStream_t st);
+  template <typename Real> void launch_pair(double *f, bool overwrite, bool want_ev,
+                                            cudaStream_t st);
+  void prepare_short_range(cudaStream_t st);
   void build_lists(cudaStream_t st);
   void set_list_capacity(double margin);
   void layout_lists(cudaStream_t st);
@@ -143,6 +149,9 @@ private:
   cudaStream_t m_stream = nullptr;
   long long m_launches = 0;
   bool m_profiling = false;
+  cudaStream_t m_side = nullptr;          // pair kernel of forces_overlapped
+  cudaEvent_t m_ev_fork = nullptr, m_ev_join = nullptr;
+  cudaEvent_t m_interp_wait = nullptr;    // event the interpolation waits for
   std::vector<std::pair<std::string, cudaEvent_t>> m_marks;
   std::vector<ReplicaConf> m_conf;
   std::vector<RepGeom> m_geom;
