@@ -77,7 +77,8 @@ struct RepGeom {
   int cao;
   long long p0, np;  // particle range
   long long rm_off;  // real mesh offset (elements)
-  long long bin_off; // corner-bin (sort key) offset: bricks of brick^3 bins
+  long long bin_off; // corner key offset: bricks of brick^3 corners
+  long long brk_off; // brick (sort key) offset
   int brick;         // brick edge (corner units) of the charge assignment
   int nbx, nby, nbz; // bricks per dimension
   long long km_off;  // complex half mesh offset (elements)

@@ -153,7 +153,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   double max_ia = -1.0;
   for (auto const &e : m_ia)
     max_ia = std::max(max_ia, e.ia_cut);
-  m_bins = m_cplx = m_cells = m_nkeys = 0;
+  m_bins = m_cplx = m_cells = m_nkeys = m_ncorner = 0;
   for (int r = 0; r < R; ++r) {
     auto const &c = conf[r];
     auto &G = m_geom[r];
@@ -187,8 +187,10 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     G.nbx = (c.mesh[0] + G.brick - 1) / G.brick;
     G.nby = (c.mesh[1] + G.brick - 1) / G.brick;
     G.nbz = (c.mesh[2] + G.brick - 1) / G.brick;
-    G.bin_off = m_nkeys;
-    m_nkeys += static_cast<long long>(G.nbx) * G.nby * G.nbz * G.brick * G.brick * G.brick;
+    G.bin_off = m_ncorner;
+    m_ncorner += static_cast<long long>(G.nbx) * G.nby * G.nbz * G.brick * G.brick * G.brick;
+    G.brk_off = m_nkeys;
+    m_nkeys += static_cast<long long>(G.nbx) * G.nby * G.nbz;
     G.rm_off = m_bins;
     G.km_off = m_cplx;
     m_bins += static_cast<long long>(c.mesh[0]) * c.mesh[1] * c.mesh[2];
@@ -206,7 +208,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     G.cell_off = m_cells;
     m_cells += static_cast<long long>(G.cg[0]) * G.cg[1] * G.cg[2];
   }
-  if (m_nkeys >= (1LL << 31) || m_bins >= (1LL << 31) || m_n >= (1LL << 31))
+  if (m_ncorner >= (1LL << 31) || m_bins >= (1LL << 31) || m_n >= (1LL << 31))
     throw Error(1, "batch too large for 32-bit bin/particle indices");
   cudaStream_t st = m_stream;
   upload_vec(m_geom_d, m_geom, st);
@@ -432,6 +434,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_type.ensure(n * sizeof(int));
   m_force.ensure(3 * n * sizeof(double));
   m_key.ensure(n * sizeof(int));
+  m_bkey.ensure(n * sizeof(int));
   m_slot.ensure(n * sizeof(int));
   m_perm.ensure(n * sizeof(int));
   m_cnt.ensure((m_nkeys + 1) * sizeof(int));
@@ -565,8 +568,9 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   int const nb = ceil_div(m_n, 256);
   if (m_n > 0) {
     k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
+                                        m_bkey.as<int>(),
                                         m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>()); ++m_launches;
-    sort_keys(m_key.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
+    sort_keys(m_bkey.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
               m_perm.as<int>(), m_nkeys, st);
     mark("p3m_sort", st);
     P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P, R><<<nb, 256, 0, st>>>(

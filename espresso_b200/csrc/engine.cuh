@@ -156,7 +156,8 @@ private:
   std::vector<ReplicaConf> m_conf;
   std::vector<RepGeom> m_geom;
   long long m_n = 0;
-  long long m_bins = 0, m_cplx = 0, m_cells = 0, m_nkeys = 0;
+  long long m_bins = 0, m_cplx = 0, m_cells = 0, m_nkeys = 0; // m_nkeys: bricks (sort keys)
+  long long m_ncorner = 0; // corner keys (bricks x brick^3)
   std::vector<int> m_phase_off; // assignment brick table offsets per colour
   int m_tile_cap = 1;           // largest assignment tile (points)
   int m_ntypes = 1;
@@ -178,7 +179,7 @@ private:
   // particles
   DevBuf m_pos, m_q, m_type, m_force;
   // p3m
-  DevBuf m_key, m_slot, m_cnt, m_start, m_perm, m_scan_tiles;
+  DevBuf m_key, m_bkey, m_slot, m_cnt, m_start, m_perm, m_scan_tiles;
   DevBuf m_dist, m_W, m_skey;
   DevBuf m_rho, m_ck, m_field, m_E, m_ginf;
   DevBuf m_part_x, m_part_census, m_sums_x, m_sums_census, m_dipole;

@@ -47,13 +47,14 @@ __device__ inline void bspline_weights(Real x, Real *w) {
 // Per particle: nearest-mesh-point corner and the distance to it, following
 // p3m_calculate_interpolation_weights (p3m/interpolation.hpp:138-178) with
 // the single-rank CA-mesh origin of P3MLocalMesh (p3m/common.cpp:34-106).
-// key = corner bin, brick-major: bin_off + brick*B^3 + (lx*B + ly)*B + lz
-// with brick = (bx*nby + by)*nbz + bz and (lx, ly, lz) the corner inside it,
-// so the particles of one brick form one contiguous range of the sorted order.
+// key = corner, brick-major: bin_off + brick*B^3 + (lx*B + ly)*B + lz with
+// brick = (bx*nby + by)*nbz + bz and (lx, ly, lz) the corner inside it; the
+// sort key bkey = brk_off + brick, so the particles of one brick form one
+// contiguous range of the sorted order (particle index order inside it).
 template <typename Real>
 __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                           const double *__restrict__ pos, long long n,
-                          int *__restrict__ key, int *__restrict__ slot,
+                          int *__restrict__ key, int *__restrict__ bkey, int *__restrict__ slot,
                           int *__restrict__ cnt, Real *__restrict__ dist) {
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n)
@@ -77,22 +78,23 @@ __global__ void k_p3m_bin(const RepGeom *__restrict__ reps, const int *__restric
   int const k = static_cast<int>(G.bin_off) + brick * B * B * B +
                 ((g[0] % B) * B + g[1] % B) * B + g[2] % B;
   key[i] = k;
-  slot[i] = atomicAdd(&cnt[k], 1);
+  int const b = static_cast<int>(G.brk_off) + brick;
+  bkey[i] = b;
+  slot[i] = atomicAdd(&cnt[b], 1);
 }
 
-// Per-particle weight record stride for order P and z-run length R:
-// {q*wx[0..P), wy[0..P), 0[R-1], wz[0..P), 0[R-1]}.  The zero padding lets a
-// thread that owns R consecutive z points read the weight of every point of
-// its run without a branch (out-of-stencil points read zero).
-// Record stride, padded to a multiple of 4 elements (16 bytes in FP32, 32 in
-// FP64) so that runs of records are legal 16-byte asynchronous copies.
+// Per-particle weight record for order P (R = 4):
+// {q*wx[0..P), wy[0..P), 0[R-1], wz[0..P), 0[R-1]}, zero-padded; the stride
+// is a multiple of 4 elements (16 bytes in FP32, 32 in FP64) so that records
+// are stored as vectors and runs of records are legal 16-byte asynchronous
+// copies.
 template <int P, int R> __host__ __device__ constexpr int wstride() {
   return (3 * P + 2 * (R - 1) + 3) / 4 * 4;
 }
 template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
 
-// Weights in corner-sorted order; also the brick-local corner key of every
-// sorted particle.
+// Weights in brick-sorted order; also the corner key (relative to the
+// replica's corner range) of every sorted particle.
 template <typename Real, int P, int R>
 __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
                               const int *__restrict__ key, const Real *__restrict__ dist,
@@ -108,17 +110,29 @@ __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__res
   bspline_weights<P>(dist[3 * i + 1], w[1]);
   bspline_weights<P>(dist[3 * i + 2], w[2]);
   Real const qi = static_cast<Real>(q[i]);
-  Real *o = W + s * wstride<P, R>();
+  // assemble the record in registers, then store it as 16- or 32-byte
+  // vectors (the stride is a multiple of 4 elements)
+  constexpr int WS = wstride<P, R>();
+  Real rec[WS];
+#pragma unroll
+  for (int k = 0; k < WS; ++k)
+    rec[k] = Real(0);
 #pragma unroll
   for (int k = 0; k < P; ++k) {
-    o[k] = qi * w[0][k];
-    o[P + k] = w[1][k];
-    o[wz_off<P, R>() + k] = w[2][k];
+    rec[k] = qi * w[0][k];
+    rec[P + k] = w[1][k];
+    rec[wz_off<P, R>() + k] = w[2][k];
   }
+  using R4 = typename Real4Of<Real>::type;
+  R4 *o = reinterpret_cast<R4 *>(W + s * WS);
 #pragma unroll
-  for (int k = 0; k < R - 1; ++k) {
-    o[2 * P + k] = Real(0);
-    o[wz_off<P, R>() + P + k] = Real(0);
+  for (int k = 0; k < WS / 4; ++k) {
+    R4 v;
+    v.x = rec[4 * k];
+    v.y = rec[4 * k + 1];
+    v.z = rec[4 * k + 2];
+    v.w = rec[4 * k + 3];
+    o[k] = v;
   }
   s_key[s] = key[i] - static_cast<int>(G.bin_off);
 }
@@ -207,8 +221,8 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
   int const B = G.brick, B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
-  const int *st = start + G.bin_off;
-  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
+  const int *st = start + G.brk_off;
+  int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)
     return; // empty brick: nothing to add
   int *t_hi = reinterpret_cast<int *>(smem_raw);
@@ -412,8 +426,8 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
   int const B = G.brick, B3 = B * B * B, Ed = B + P - 1, E2 = Ed * Ed;
-  const int *st = start + G.bin_off;
-  int const s0 = st[bk.y * B3], s1 = st[(bk.y + 1) * B3];
+  const int *st = start + G.brk_off;
+  int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)
     return; // no particles in this brick
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
