@@ -522,7 +522,7 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
   m_launches += 3;
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
-  k_fix_buckets<<<ceil_div(nkeys, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
+  k_fix_buckets<<<ceil_div(nkeys * 32, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
 }
 
 #define P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                  \

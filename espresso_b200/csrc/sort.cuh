@@ -1,12 +1,14 @@
 // Exclusive scan and deterministic counting sort (device primitives).
 //
-// The counting sort orders items by an integer key (mesh-corner bin or link
+// The counting sort orders items by an integer key (assignment brick or link
 // cell) and then restores, inside every key bucket, ascending item order, so
 // the permutation is a pure function of the keys: the same input gives the
 // same bitwise output on every run, whatever the atomic order was.
 #pragma once
 
 #include "common.cuh"
+
+#include <climits>
 
 namespace p3mx {
 
@@ -120,27 +122,61 @@ __global__ void k_place(const int *__restrict__ key, const int *__restrict__ slo
     perm[start[key[i]] + slot[i]] = static_cast<int>(i);
 }
 
-// Restore ascending item order inside each bucket (buckets are short:
-// insertion sort), making the permutation independent of atomic order.
+// Restore particle-index order inside every bucket (the atomic slots of the
+// binning pass arrive in any order): one warp per bucket.  Buckets of up to
+// 128 entries are held in registers (4 per lane) and every entry's rank is
+// counted by shuffle comparisons against all others (entries are distinct
+// particle indices, so ranks are unique); larger buckets fall back to an
+// insertion sort by lane 0.
 __global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ perm,
                               long long nbuckets, const int *__restrict__ cond) {
   if (cond && !*cond)
     return;
-  long long const b = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  constexpr int NV = 4;
+  long long const b = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  int const lane = threadIdx.x & 31;
   if (b >= nbuckets)
-    return;
+    return; // whole warp
   int const s0 = start[b], s1 = start[b + 1];
-  if (s1 - s0 < 2)
+  int const n = s1 - s0;
+  if (n < 2)
     return;
-  for (int i = s0 + 1; i < s1; ++i) {
-    int const v = perm[i];
-    int j = i - 1;
-    while (j >= s0 && perm[j] > v) {
-      perm[j + 1] = perm[j];
-      --j;
-    }
-    perm[j + 1] = v;
+  if (n > 32 * NV) {
+    if (lane == 0)
+      for (int i = s0 + 1; i < s1; ++i) {
+        int const v = perm[i];
+        int j = i - 1;
+        while (j >= s0 && perm[j] > v) {
+          perm[j + 1] = perm[j];
+          --j;
+        }
+        perm[j + 1] = v;
+      }
+    return;
   }
+  int v[NV], rank[NV];
+#pragma unroll
+  for (int u = 0; u < NV; ++u) {
+    int const idx = u * 32 + lane;
+    v[u] = (idx < n) ? perm[s0 + idx] : INT_MAX;
+    rank[u] = 0;
+  }
+#pragma unroll
+  for (int u2 = 0; u2 < NV; ++u2) {
+    if (u2 * 32 >= n)
+      break; // warp-uniform
+    for (int k = 0; k < 32; ++k) {
+      int const o = __shfl_sync(0xffffffffu, v[u2], k);
+#pragma unroll
+      for (int u = 0; u < NV; ++u)
+        rank[u] += (o < v[u]) ? 1 : 0;
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < NV; ++u)
+    if (u * 32 + lane < n)
+      perm[s0 + rank[u]] = v[u];
 }
 
 // Host driver of the three-pass exclusive scan (out has n+1 entries).
