@@ -244,7 +244,8 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
                    : "memory");
     for (int j = tid; j < cn; j += NT) {
       int const l = s_key[c0 + j] - bk.y * B3;
-      rbase[j] = ((l / (B * B)) * E + (l / B) % B) * E + l % B;
+      int const lb = __ffs(B) - 1; // B is a power of two
+      rbase[j] = ((l >> (2 * lb)) * E + ((l >> lb) & (B - 1))) * E + (l & (B - 1));
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
   };
@@ -440,26 +441,38 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
       v -= m;
     return v;
   };
+  // mesh offsets of the tile's x planes and y rows (periodic images folded)
+  __shared__ int s_xo[16], s_yo[16];
+  if (tid < Ed)
+    s_xo[tid] = wrap(x0 + tid, M0) * M1 * M2;
+  else if (tid >= 32 && tid - 32 < Ed)
+    s_yo[tid - 32] = wrap(y0 + tid - 32, M1) * M2;
+  __syncthreads();
   // tile rows (x, y) of Ed records along z; lane groups of gs lanes copy one
   // row each with asynchronous 16-byte copies (cp.async, L2 only), all in
-  // flight together
+  // flight together; rows advance by increment (no division)
   int const gs = (Ed <= 8) ? 8 : (Ed <= 16 ? 16 : 32);
   int const rpw = 32 / gs;
   int const zl = lane & (gs - 1);
-  int const gz = wrap(z0 + zl, M2);
-  for (int row = warp * rpw + lane / gs; row < E2; row += kAssignWarps * rpw) {
-    int const x = row / Ed, y = row - x * Ed;
+  int const zo = wrap(z0 + zl, M2);
+  int const step = kAssignWarps * rpw;
+  int row = warp * rpw + lane / gs;
+  int x = row / Ed, y = row - (row / Ed) * Ed;
+  unsigned const tbase = static_cast<unsigned>(__cvta_generic_to_shared(tile));
+  for (; row < E2; row += step) {
     if (zl < Ed) {
-      long long const gx = wrap(x0 + x, M0), gy = wrap(y0 + y, M1);
-      const R4 *src = E4 + (gx * M1 + gy) * M2 + gz;
-      R4 *dst = tile + row * Ed + zl;
+      const R4 *src = E4 + (s_xo[x] + s_yo[y] + zo);
+      unsigned const dst = tbase + static_cast<unsigned>((row * Ed + zl) * sizeof(R4));
 #pragma unroll
       for (int h = 0; h < static_cast<int>(sizeof(R4) / 16); ++h)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                         static_cast<unsigned>(__cvta_generic_to_shared(
-                             reinterpret_cast<char *>(dst) + 16 * h))),
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * h),
                      "l"(reinterpret_cast<const char *>(src) + 16 * h)
                      : "memory");
+    }
+    y += step;
+    while (y >= Ed) {
+      y -= Ed;
+      ++x;
     }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
@@ -476,7 +489,8 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     Real ax = Real(0), ay = Real(0), az = Real(0);
     if (live && kz < P) {
       int const l = s_key[s] - bk.y * B3;
-      int const lx = l / (B * B), ly = (l / B) % B, lz = l % B;
+      int const lb = __ffs(B) - 1; // B is a power of two
+      int const lx = l >> (2 * lb), ly = (l >> lb) & (B - 1), lz = l & (B - 1);
       const Real *w = W + static_cast<long long>(s) * WS;
       Real wx[P], wy[P];
 #pragma unroll
