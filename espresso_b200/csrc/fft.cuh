@@ -243,6 +243,49 @@ __device__ inline void fft_stage_dyn(const C *src, C *dst, int n, int ld, int nl
   }
 }
 
+// Power-of-two line length N = N1 * N2 (N1, N2 <= 16) in two register
+// steps (n = t + N2 m, k = k1 + N1 k2):
+//   step 1, item (line, t): Y[t][k1] = w_N^(t k1) * DFT_N1 over m of x[t + N2 m],
+//           written in place at t + N2 k1;
+//   step 2, item (line, k1): X[k1 + N1 k2] = DFT_N2 over t of Y[t][k1],
+//           written to `b` in natural order.
+// Strides are compile-time constants; the padded layout (pix) keeps both
+// steps free of bank conflicts.  Returns b.
+template <typename C, int N1, int N2>
+__device__ C *fft_2step(C *a, C *b, int nlines, int ld, const C *__restrict__ tw, bool inv) {
+  for (int it = threadIdx.x; it < nlines * N2; it += blockDim.x) {
+    int const l = it / N2, t = it - l * N2;
+    C *s = a + l * ld;
+    C v[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m)
+      v[m] = s[pix(t + N2 * m)];
+    dft_pow2<C, N1>(v, inv);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      v[k1] = cmul(v[k1], ld_tw(tw, t * k1, inv));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1)
+      s[pix(t + N2 * k1)] = v[k1];
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < nlines * N1; it += blockDim.x) {
+    int const l = it / N1, k1 = it - l * N1;
+    const C *s = a + l * ld;
+    C *d = b + l * ld;
+    C v[N2];
+#pragma unroll
+    for (int t = 0; t < N2; ++t)
+      v[t] = s[pix(t + N2 * k1)];
+    dft_pow2<C, N2>(v, inv);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2)
+      d[pix(k1 + N1 * k2)] = v[k2];
+  }
+  __syncthreads();
+  return b;
+}
+
 // Full transform of nlines lines in `a` (scratch `b`; element i of line l at
 // l*ld + pix(i)); tw = the axis twiddle table (shared memory).  Returns the
 // buffer holding the result.  All threads of the block must call it.
@@ -250,6 +293,13 @@ template <typename C>
 __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
                         const C *__restrict__ tw, bool inv) {
   int const n = pl.n;
+  switch (n) {
+  case 32: return fft_2step<C, 16, 2>(a, b, nlines, ld, tw, inv);
+  case 64: return fft_2step<C, 16, 4>(a, b, nlines, ld, tw, inv);
+  case 128: return fft_2step<C, 16, 8>(a, b, nlines, ld, tw, inv);
+  case 256: return fft_2step<C, 16, 16>(a, b, nlines, ld, tw, inv);
+  default: break;
+  }
   int Ns = 1;
   C *src = a, *dst = b;
   for (int s = 0; s < pl.nstages; ++s) {
@@ -279,7 +329,7 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
 // bk.b real lines per block (an odd last line is paired with zeros).
 // Shared memory: 2 x ceil(bk.b/2) staged lines of line_ld(n), twiddles (n).
 template <typename Real>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
 k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
             const Real *__restrict__ rmesh, typename CplxOf<Real>::type *__restrict__ cmesh,
             const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -330,7 +380,7 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
 // Shared memory: 2 x tile staged lines of line_ld(M1), twiddles (M1).
 template <typename Real>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
 k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
         typename CplxOf<Real>::type *__restrict__ c0, long long field_stride, int tile,
         bool inv, const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -510,7 +560,7 @@ __host__ __device__ inline int z_inv_b_size(int nl, int n) {
 // Shared memory: 2 x (nl + ceil(nl/2)) staged lines of line_ld(n),
 // twiddles (n).
 template <typename Real>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
 k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
              const typename CplxOf<Real>::type *__restrict__ field0, long long field_stride,
              Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab) {
