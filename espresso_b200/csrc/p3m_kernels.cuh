@@ -172,11 +172,24 @@ template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem
          sizeof(int) * kAssignChunk;
 }
 
-template <typename Real> __device__ inline Real floor_r(Real v);
-template <> __device__ inline float floor_r<float>(float v) { return floorf(v); }
-template <> __device__ inline double floor_r<double>(double v) { return floor(v); }
-__device__ inline unsigned to_u32_rn(float v) { return __float2uint_rn(v); }
-__device__ inline unsigned to_u32_rn(double v) { return __double2uint_rn(v); }
+// Round-to-nearest split of a fixed-point contribution t (|t| <= 2^(22+kb))
+// into hi = rint(t / 2^kb) and lo = rint(t - hi 2^kb), both |.| <= 2^22.
+// FP32: the 1.5 * 2^23 magic-add rounding keeps the work on the FMA and ALU
+// pipes (no conversion instructions); t - hi 2^kb is exact (Sterbenz).
+__device__ inline void split_fixed(float t, float two_kb, float inv_two_kb, int &hi, int &lo) {
+  float const magic = 12582912.0f; // 1.5 * 2^23
+  float const hs = t * inv_two_kb + magic;
+  float const hf = hs - magic;
+  float const lf = fmaf(-hf, two_kb, t);
+  float const ls = lf + magic;
+  hi = __float_as_int(hs) - 0x4B400000;
+  lo = __float_as_int(ls) - 0x4B400000;
+}
+__device__ inline void split_fixed(double t, double two_kb, double inv_two_kb, int &hi, int &lo) {
+  double const hf = rint(t * inv_two_kb);
+  hi = static_cast<int>(hf);
+  lo = __double2int_rn(fma(-hf, two_kb, t));
+}
 template <typename Real> __device__ inline Real from_ll(long long v);
 template <> __device__ inline float from_ll<float>(long long v) { return __ll2float_rn(v); }
 template <> __device__ inline double from_ll<double>(long long v) { return __ll2double_rn(v); }
@@ -189,13 +202,14 @@ template <> __device__ inline double from_ll<double>(long long v) { return __ll2
 // (B+P-1)^3 points.
 //
 // The tile holds fixed point: a contribution t = v*S (S a power of two) is
-// split exactly into hi = floor(t / 2^kb) and lo = t - hi*2^kb in [0, 2^kb],
+// split into hi = rint(t / 2^kb) and lo = rint(t - hi*2^kb), |lo| <= 2^(kb-1),
 // added with 32-bit integer atomics to two words per point.  With n
-// particles in the brick, kb = 32 - ceil(log2(n+1)) keeps every lo sum below
-// 2^32, and S = 2^(30+kb-ex) with sum|q| < 2^ex keeps every hi sum below
-// 2^31; the point value is (hi*2^kb + lo)/S.  Integer sums do not depend on
-// the order of the adds, so the tile is bitwise reproducible although the
-// warps run concurrently; the quantum is 2^-(30+kb) of the brick's sum|q|.
+// particles in the brick, kb = min(23, 32 - bits(n)) keeps every lo sum
+// inside int32, and S = 2^(22+kb-ex) with sum|q| < 2^ex keeps |t| < 2^(22+kb)
+// (so |hi| < 2^22) and every hi sum inside int32; the point value is
+// (hi*2^kb + lo)/S.  Integer sums do not depend on the order of the adds, so
+// the tile is bitwise reproducible although the warps run concurrently; the
+// quantum is 2^-(22+kb) (at most 2^-45) of the brick's sum|q|.
 //
 // Tiles are then added to the mesh; bricks of one launch share a colour
 // (greedy interval colouring per dimension), so the tiles of one launch never
@@ -226,12 +240,12 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   if (s0 == s1)
     return; // empty brick: nothing to add
   int *t_hi = reinterpret_cast<int *>(smem_raw);
-  unsigned *t_lo = reinterpret_cast<unsigned *>(t_hi + tile_cap);
+  int *t_lo = t_hi + tile_cap;
   Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes(tile_cap));
   int *rbase = reinterpret_cast<int *>(rec + CH * WS);
   for (int t = tid; t < E3; t += NT) {
     t_hi[t] = 0;
-    t_lo[t] = 0u;
+    t_lo[t] = 0;
   }
   // stage a chunk of records (contiguous; asynchronous 16-byte copies) and
   // each particle's tile base offset
@@ -273,10 +287,10 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     qabs += s_red[k];
   if (qabs == 0.0)
     return; // all charges zero: the tile would stay zero
-  int const kb = min(24, 32 - (32 - __clz(cnt))); // cnt < 2^(32-kb)
+  int const kb = min(23, 32 - (32 - __clz(cnt))); // cnt < 2^(32-kb)
   int ex;
   frexp(qabs * (1.0 + 1e-12), &ex);
-  int const es = min(max(30 + kb - ex, -100), 100);
+  int const es = min(max(22 + kb - ex, -100), 100);
   Real const S = static_cast<Real>(ldexp(1.0, es));
   Real const two_kb = static_cast<Real>(1u << kb);
   Real const inv_two_kb = static_cast<Real>(1.0 / (1u << kb));
@@ -305,10 +319,10 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
       for (int r = 0; r < NR; ++r) {
         if (lane + 32 * r < P3) {
           Real const t = (w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]]) * S;
-          Real const hf = floor_r(t * inv_two_kb);
-          Real const lf = t - hf * two_kb;
-          atomicAdd(&t_hi[base + off[r]], static_cast<int>(hf));
-          atomicAdd(&t_lo[base + off[r]], to_u32_rn(lf));
+          int hi, lo;
+          split_fixed(t, two_kb, inv_two_kb, hi, lo);
+          atomicAdd(&t_hi[base + off[r]], hi);
+          atomicAdd(&t_lo[base + off[r]], lo);
         }
       }
     }
