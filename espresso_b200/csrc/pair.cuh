@@ -170,18 +170,37 @@ template <typename Real> __device__ inline Real as_erfc_part(Real d) {
   return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5))));
 }
 
+// FP32 exp(x) for the real-space kernel (x = -(alpha r)^2 in [-88, 0]):
+// e^x = 2^y with y = x log2(e) split error-free into y_hi + y_lo (the FMA
+// residual of the product, Dekker's TwoProduct, plus the low part of the
+// constant), then 2^y = 2^y_hi (hardware ex2.approx, ~2 ulp) * (1 + y_lo ln 2).
+// Relative error ~2^-21 over the range, against ~2^-24 * |y| for a plain
+// ex2(x * log2 e).
+__device__ inline float exp_fast(float x) {
+  float const l2e_hi = 1.44269502162933349609375f;    // log2(e) rounded to FP32
+  float const l2e_lo = 1.9259629911266175e-8f;        // log2(e) - l2e_hi
+  float const y_hi = x * l2e_hi;
+  float const y_lo = fmaf(x, l2e_hi, -y_hi) + x * l2e_lo;
+  float e;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(y_hi));
+  return fmaf(e, y_lo * 0.693147180559945309f, e);
+}
 template <typename Real> __device__ inline Real exp_r(Real x);
-template <> __device__ inline float exp_r<float>(float x) { return expf(x); }
+template <> __device__ inline float exp_r<float>(float x) { return exp_fast(x); }
 template <> __device__ inline double exp_r<double>(double x) { return exp(x); }
 template <typename Real> __device__ inline Real sqrt_r(Real x);
 template <> __device__ inline float sqrt_r<float>(float x) { return sqrtf(x); }
 template <> __device__ inline double sqrt_r<double>(double x) { return sqrt(x); }
 
 // Reciprocal / reciprocal square root in the working precision: FP32 uses
-// the hardware approximations refined to ~1 ulp (the FP32-mixed path
-// tolerates ulp-level differences); FP64 keeps IEEE division and sqrt.
+// the hardware approximations (~1 ulp; the FP32-mixed path tolerates
+// ulp-level differences); FP64 keeps IEEE division and sqrt.
 template <typename Real> __device__ inline Real rcp_r(Real x);
-template <> __device__ inline float rcp_r<float>(float x) { return __frcp_rn(x); }
+template <> __device__ inline float rcp_r<float>(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 template <> __device__ inline double rcp_r<double>(double x) { return 1.0 / x; }
 template <typename Real> __device__ inline Real rsqrt_r(Real x);
 template <> __device__ inline float rsqrt_r<float>(float x) { return rsqrtf(x); }
