@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdlib>
 #include <cstring>
@@ -30,6 +31,7 @@ public:
     {
       std::lock_guard<std::mutex> lk(m_mu);
       m_stop = true;
+      m_stop_pub.store(true);
     }
     m_cv.notify_all();
     for (auto &t : m_workers)
@@ -55,15 +57,18 @@ public:
       std::lock_guard<std::mutex> lk(m_mu);
       m_fn = &fn;
       m_n = n_tasks;
-      m_done = 0;
+      m_done_pub.store(0);
       gen = ++m_gen;
       m_next.store(static_cast<unsigned long long>(gen) << 32);
+      m_gen_pub.store(gen, std::memory_order_release);
     }
     m_cv.notify_all();
     int const mine = work(gen, n_tasks, &fn);
-    std::unique_lock<std::mutex> lk(m_mu);
-    m_done += mine;
-    m_done_cv.wait(lk, [&] { return m_done == m_n; });
+    // tasks finish within microseconds of each other: spin on the count
+    int done = m_done_pub.fetch_add(mine, std::memory_order_acq_rel) + mine;
+    while (done < n_tasks)
+      done = m_done_pub.load(std::memory_order_acquire);
+    std::lock_guard<std::mutex> lk(m_mu);
     m_fn = nullptr;
   }
 
@@ -100,6 +105,13 @@ private:
       unsigned gen;
       int n;
       std::function<void(int)> const *fn;
+      // chunks of one staging call follow each other within microseconds:
+      // spin on the generation counter for a while before sleeping, so a
+      // hot pool picks up the next chunk without a wake-up
+      auto const t_spin = std::chrono::steady_clock::now() + std::chrono::microseconds(300);
+      while (m_gen_pub.load(std::memory_order_acquire) == seen && !m_stop_pub.load() &&
+             std::chrono::steady_clock::now() < t_spin) {
+      }
       {
         std::unique_lock<std::mutex> lk(m_mu);
         m_cv.wait(lk, [&] { return m_stop || m_gen != seen; });
@@ -110,23 +122,23 @@ private:
         fn = m_fn;
       }
       int const mine = work(gen, n, fn);
-      std::lock_guard<std::mutex> lk(m_mu);
-      if (gen == m_gen) {
-        m_done += mine;
-        if (m_done == m_n)
-          m_done_cv.notify_all();
-      }
+      // a stale generation claimed no task (mine == 0): nothing to report
+      if (mine > 0)
+        m_done_pub.fetch_add(mine, std::memory_order_acq_rel);
     }
   }
 
   std::vector<std::thread> m_workers;
   std::mutex m_mu;
-  std::condition_variable m_cv, m_done_cv;
+  std::condition_variable m_cv;
   std::function<void(int)> const *m_fn = nullptr;
-  int m_n = 0, m_done = 0;
+  int m_n = 0;
+  std::atomic<int> m_done_pub{0}; // finished tasks of the current generation
   std::atomic<unsigned long long> m_next{0};
   unsigned m_gen = 0;
   bool m_stop = false;
+  std::atomic<unsigned> m_gen_pub{0}; // m_gen, readable without the lock
+  std::atomic<bool> m_stop_pub{false};
 };
 
 } // namespace p3mx
