@@ -287,6 +287,11 @@ def run_batched(args):
         tuned.append((t.mesh[0], t.cao, t.r_cut, t.accuracy))
     meshes = np.array([x[0] for x in tuned])
     acc = np.array([x[3] for x in tuned])
+    rcs = np.array([x[2] for x in tuned])
+    nrep = np.diff(offs).astype(float)
+    # full-list Verlet candidates per step: N (4/3) pi (r_cut + skin)^3 rho
+    pair_cand = float((nrep * 4.18879 * (np.maximum(rcs, 2 ** (1 / 6)) + 0.4) ** 3 *
+                       nrep / boxes[:, 0] ** 3).sum())
     cpu = None
     if not args.no_cpu_baseline:
         # sample: the first 8 replicas, one force evaluation each, FP64 oracle
@@ -320,7 +325,9 @@ def run_batched(args):
                                f"CUDA graph per step",
                    "total_particles": int(n), "tuning_s": t_tune,
                    "mesh_hist": {int(m): int((meshes == m).sum()) for m in np.unique(meshes)},
-                   "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max())},
+                   "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max()),
+                   "r_cut_range": [float(rcs.min()), float(rcs.max())],
+                   "verlet_candidates_per_step_est": pair_cand},
         "cpu_baseline": cpu, "clocks": clk.summary(),
         "gpu_launches": int(lc1.value - lc0.value)}))
 

@@ -314,3 +314,24 @@ def test_host_staging_chunks_accumulate_and_device_pointers():
                                None, None, flags | _lib.P3MX_DEVICE_PTRS, None), act._handle)
     torch.cuda.synchronize()
     assert np.array_equal(df.cpu().numpy(), f_ow)
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_headline_parameters_rms_error_vs_ewald(cls):
+    """The P3M parameters of the 2^20-ion headline workload (mesh spacing 0.5,
+    cao 7, r_cut 3.5, alpha 0.87024 from its tuning to accuracy 1e-4) on a
+    box-24 system of the same construction and density (6912 ions, mesh 48):
+    the rms Coulomb force error against the FP64 direct Ewald sum stays below
+    the 1e-4 target that the headline metric is quoted at."""
+    import bench
+    pos, q, box = bench.make_workload(seed=3, box=24.0)
+    s = make_system([box] * 3, pos, q)
+    s.electrostatics.solver = cls(prefactor=1.0, accuracy=1e-4, mesh=48, cao=7, r_cut=3.5,
+                                  alpha=0.8702383472846797, tune=False)
+    s.integrator.run(0)
+    f = s.part.all().f
+    # Ewald: real space erfc(0.35 * 9.9) ~ 1e-6, k space exp(-k^2/4a^2) < 1e-15
+    fe, _ = O.ewald([box] * 3, pos, q, 1.0, 0.35, 9.9, 16)
+    rms = np.sqrt(((f - fe) ** 2).sum(1).mean())
+    assert rms < 1e-4
+    assert rms > 1e-6  # the comparison resolves the P3M discretisation error
