@@ -210,6 +210,9 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   }
   if (m_ncorner >= (1LL << 31) || m_bins >= (1LL << 31) || m_n >= (1LL << 31))
     throw Error(1, "batch too large for 32-bit bin/particle indices");
+  for (auto const &G : m_geom)
+    if (G.np >= (1LL << kNbIndexBits))
+      throw Error(1, "a replica holds more than 2^26 particles (Verlet list index limit)");
   cudaStream_t st = m_stream;
   upload_vec(m_geom_d, m_geom, st);
   {
@@ -460,6 +463,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_cperm.ensure(n * sizeof(int));
   m_pq.ensure(n * sizeof(double4));
   m_spq.ensure(n * sizeof(double4));
+  m_spf.ensure(n * sizeof(float4));
   m_stype.ensure(n * sizeof(int));
   m_scell.ensure(n * sizeof(int));
   m_nb_cnt.ensure(n * sizeof(int));
@@ -523,6 +527,8 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   m_launches += 3;
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
   k_fix_buckets<<<ceil_div(nkeys * 32, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
+  k_fix_big_buckets<<<static_cast<int>(std::min<long long>(nkeys, 4096)), 256, 0, st>>>(
+      start, perm, nkeys, cond); ++m_launches;
 }
 
 #define P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                  \
@@ -701,14 +707,15 @@ void Engine::build_lists(cudaStream_t st) {
                                  m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st);
-  k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr); ++m_launches;
+  k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
+                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr); ++m_launches;
   if (m_cap.size() != m_geom.size())
     set_list_capacity(1.5);
   int const R = n_rep();
   for (int attempt = 0; attempt < 4; ++attempt) {
     P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, R * sizeof(int), st));
-    k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
+    k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+                                       m_spf.as<float4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                        m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                        m_overflow.as<int>(), nullptr); ++m_launches;
@@ -733,20 +740,28 @@ void Engine::build_lists(cudaStream_t st) {
 
 __global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                               const int *__restrict__ perm, const double *__restrict__ pos,
-                              const double *__restrict__ q, long long n, double4 *__restrict__ spq) {
+                              const double *__restrict__ q, const int *__restrict__ scell,
+                              const double *__restrict__ pos_ref, long long n,
+                              double4 *__restrict__ spq, float4 *__restrict__ spf) {
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
   int const i = perm[s];
   RepGeom const &G = reps[rep_of[i]];
-  spq[s] = make_double4(fold_coord(pos[3 * i], G.box[0]), fold_coord(pos[3 * i + 1], G.box[1]),
-                        fold_coord(pos[3 * i + 2], G.box[2]), q[i]);
+  double4 const v = make_double4(fold_coord(pos[3 * i], G.box[0]),
+                                 fold_coord(pos[3 * i + 1], G.box[1]),
+                                 fold_coord(pos[3 * i + 2], G.box[2]), q[i]);
+  spq[s] = v;
+  spf[s] = cell_offset(G, scell[s] - static_cast<int>(G.cell_off), pos_ref + 3 * i, pos + 3 * i,
+                       v.w);
 }
 
 void Engine::refresh_sorted_positions(cudaStream_t st) {
   k_refresh_spq<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(),
-                                                    m_cperm.as<int>(), d_pos(), d_q(), m_n,
-                                                    m_spq.as<double4>()); ++m_launches;
+                                                    m_cperm.as<int>(), d_pos(), d_q(),
+                                                    m_scell.as<int>(), m_pos_ref.as<double>(),
+                                                    m_n, m_spq.as<double4>(),
+                                                    m_spf.as<float4>()); ++m_launches;
 }
 
 // Displacement check (host decision) and list rebuild or sorted-position
@@ -776,17 +791,33 @@ template <typename Real>
 void Engine::launch_pair(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
-  if (want_ev)
-    k_pair_forces<Real, true><<<m_n_blk_pair, 256, smem, st>>>(
-        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
-        m_part_pair.as<double>());
-  else
-    k_pair_forces<Real, false><<<m_n_blk_pair, 256, smem, st>>>(
-        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
-        m_part_pair.as<double>());
-  ++m_launches;
+  if constexpr (sizeof(Real) == 4) {
+    // FP32-mixed: cell-relative FP32 geometry
+    if (want_ev)
+      k_pair_forces_rel<true><<<m_n_blk_pair, 256, smem, st>>>(
+          geom, m_blk_pair.as<int2>(), m_spf.as<float4>(), m_stype.as<int>(), m_cperm.as<int>(),
+          m_ia_d.as<PairIA>(), m_ntypes, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+          overwrite ? 1 : 0, m_part_pair.as<double>());
+    else
+      k_pair_forces_rel<false><<<m_n_blk_pair, 256, smem, st>>>(
+          geom, m_blk_pair.as<int2>(), m_spf.as<float4>(), m_stype.as<int>(), m_cperm.as<int>(),
+          m_ia_d.as<PairIA>(), m_ntypes, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+          overwrite ? 1 : 0, m_part_pair.as<double>());
+    ++m_launches;
+  } else {
+    // FP64: FP64 geometry (minimum image on absolute positions)
+    if (want_ev)
+      k_pair_forces<Real, true><<<m_n_blk_pair, 256, smem, st>>>(
+          geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+          m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+          overwrite ? 1 : 0, m_part_pair.as<double>());
+    else
+      k_pair_forces<Real, false><<<m_n_blk_pair, 256, smem, st>>>(
+          geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
+          m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+          overwrite ? 1 : 0, m_part_pair.as<double>());
+    ++m_launches;
+  }
 }
 
 template <typename Real>
@@ -879,26 +910,19 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
                                  m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st, flag);
-  k_cell_gather<<<nb, 256, 0, st>>>(m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
-  k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(), m_stype.as<int>(),
+  k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
+                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
+  k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+                                       m_spf.as<float4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                      m_overflow.as<int>(), flag); ++m_launches;
   k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag); ++m_launches;
   refresh_sorted_positions(st);
-  size_t const smem = static_cast<size_t>(m_ntypes) * m_ntypes * sizeof(PairIA);
   if (m_fp32)
-    k_pair_forces<float, false><<<m_n_blk_pair, 256, smem, st>>>(
-        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
-        m_part_pair.as<double>());
+    launch_pair<float>(f, overwrite, false, st);
   else
-    k_pair_forces<double, false><<<m_n_blk_pair, 256, smem, st>>>(
-        geom, m_blk_pair.as<int2>(), m_spq.as<double4>(), m_stype.as<int>(), m_cperm.as<int>(),
-        m_ia_d.as<PairIA>(), m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(), f, overwrite ? 1 : 0,
-        m_part_pair.as<double>());
-  ++m_launches;
+    launch_pair<double>(f, overwrite, false, st);
 }
 
 int Engine::list_overflow(cudaStream_t st) {
@@ -912,14 +936,20 @@ int Engine::list_overflow(cudaStream_t st) {
 // margin * 4/3 pi (max_cut + skin)^3 rho + 48, never shrinking an existing one.
 void Engine::set_list_capacity(double margin) {
   int const R = n_rep();
+  bool changed = (static_cast<int>(m_cap.size()) != R) || m_nb.p == nullptr;
   m_cap.resize(R, 0);
   for (int r = 0; r < R; ++r) {
     auto const &G = m_geom[r];
     double const rc = G.max_cut + G.skin;
     double const est = margin * 4.18879 * rc * rc * rc * (G.np / G.V) + 48.0;
-    m_cap[r] = std::max(m_cap[r], static_cast<int>(std::min(est, double(std::max<long long>(G.np, 1)))) + 1);
+    int const cap = std::max(
+        m_cap[r], static_cast<int>(std::min(est, double(std::max<long long>(G.np, 1)))) + 1);
+    changed = changed || (cap != m_cap[r]);
+    m_cap[r] = cap;
   }
-  layout_lists(m_stream);
+  // a new layout invalidates the lists; an unchanged one keeps them
+  if (changed)
+    layout_lists(m_stream);
 }
 
 void Engine::layout_lists(cudaStream_t st) {
@@ -927,7 +957,8 @@ void Engine::layout_lists(cudaStream_t st) {
   for (int r = 0; r < n_rep(); ++r) {
     m_geom[r].nb_off = off;
     m_geom[r].max_nb = m_cap[r];
-    off += static_cast<long long>(m_cap[r]) * m_geom[r].np;
+    // warp tiles of 32 particles (nb_base)
+    off += static_cast<long long>(m_cap[r]) * ((m_geom[r].np + 31) / 32 * 32);
   }
   m_nb.ensure(static_cast<size_t>(std::max<long long>(off, 1)) * sizeof(int));
   upload_vec(m_geom_d, m_geom, st);
@@ -966,7 +997,7 @@ std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
   std::vector<int> cnt(m_n), perm(m_n);
   long long total = 0;
   for (auto const &G : m_geom)
-    total += static_cast<long long>(G.max_nb) * G.np;
+    total += static_cast<long long>(G.max_nb) * ((G.np + 31) / 32 * 32);
   std::vector<int> nbh(total);
   P3MX_CUDA(cudaMemcpyAsync(cnt.data(), m_nb_cnt.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaMemcpyAsync(perm.data(), m_cperm.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -976,7 +1007,9 @@ std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
   for (auto const &G : m_geom)
     for (long long a = G.p0; a < G.p0 + G.np; ++a)
       for (int k = 0; k < cnt[a]; ++k) {
-        int const b = nbh[G.nb_off + static_cast<long long>(k) * G.np + (a - G.p0)];
+        unsigned const ent = static_cast<unsigned>(
+            nbh[nb_base(G.nb_off, G.max_nb, a - G.p0) + (static_cast<long long>(k) << 5)]);
+        int const b = static_cast<int>(G.p0 + (ent & kNbIndexMask));
         int const i = perm[a], j = perm[b];
         if (i < j) {
           pairs.push_back(i);

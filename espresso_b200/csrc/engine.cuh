@@ -186,7 +186,7 @@ private:
   bool m_ginf_valid = false;
   std::vector<double> m_census_h;
   // short range
-  DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_stype, m_scell;
+  DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_part_pair, m_sums_pair;
   std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;

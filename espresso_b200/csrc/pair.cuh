@@ -14,6 +14,27 @@ struct PairIA {
   double ia_cut; // max of active cutoffs, -1 when inactive
 };
 
+// FP32 offset of a particle from the corner of cell `loc` (cell index inside
+// the replica) that it was binned into at the last list build: the folded
+// build-time position minus the corner, plus the minimum-image displacement
+// since the build (below skin/2 by the Verlet rebuild rule), so the offset
+// stays continuous when the particle leaves its cell or crosses the box
+// boundary, for any cell grid.  At build time xref = x.
+__device__ inline float4 cell_offset(RepGeom const &G, int loc, const double *xref,
+                                     const double *x, double q) {
+  int const c[3] = {loc % G.cg[0], (loc / G.cg[0]) % G.cg[1], loc / (G.cg[0] * G.cg[1])};
+  float o[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double const cs = G.box[d] / G.cg[d];
+    double const v = fold_coord(xref[d], G.box[d]) - c[d] * cs;
+    double dd = x[d] - xref[d];
+    dd -= G.box[d] * rint(dd * G.box_i[d]);
+    o[d] = static_cast<float>(v + dd);
+  }
+  return make_float4(o[0], o[1], o[2], static_cast<float>(q));
+}
+
 // Cell of a folded position, position_to_cell_index
 // (RegularDecomposition.cpp:51-80) on a single rank: floor(x/cell)+1,
 // clamped to the grid for x < L.  Returns interior coordinates 0..cg-1.
@@ -60,19 +81,25 @@ __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restri
 }
 
 // Gather particle data into cell-sorted order.
-__global__ void k_cell_gather(const int *__restrict__ perm, const double4 *__restrict__ pq,
+__global__ void k_cell_gather(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                              const int *__restrict__ perm, const double4 *__restrict__ pq,
                               const int *__restrict__ type, const int *__restrict__ key,
-                              long long n, double4 *__restrict__ spq, int *__restrict__ stype,
-                              int *__restrict__ scell, const int *__restrict__ cond) {
+                              long long n, double4 *__restrict__ spq, float4 *__restrict__ spf,
+                              int *__restrict__ stype, int *__restrict__ scell,
+                              const int *__restrict__ cond) {
   if (cond && !*cond)
     return;
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
   int const i = perm[s];
-  spq[s] = pq[i];
+  double4 const v = pq[i];
+  spq[s] = v;
   stype[s] = type ? type[i] : 0;
   scell[s] = key[i];
+  RepGeom const &G = reps[rep_of[i]];
+  double const xv[3] = {v.x, v.y, v.z};
+  spf[s] = cell_offset(G, key[i] - static_cast<int>(G.cell_off), xv, xv, v.w);
 }
 
 __device__ inline double mi_d(double dx, double L, double Li) {
@@ -82,16 +109,27 @@ __device__ inline double mi_d(double dx, double L, double Li) {
   return dx;
 }
 
+// Verlet list layout, warp-tiled: the lists of 32 consecutive particles of a
+// replica (one warp of the pair kernel) form one contiguous block, neighbour
+// slot k of local particle la at nb_off + ((la/32) * max_nb + k) * 32 + la%32,
+// so a warp streams through its own block.  An entry packs the partner's
+// index inside the replica (26 bits) and its cell offset code (cell_offset).
+constexpr int kNbIndexBits = 26;
+constexpr unsigned kNbIndexMask = (1u << kNbIndexBits) - 1u;
+__host__ __device__ inline long long nb_base(long long nb_off, int max_nb, long long la) {
+  return nb_off + (((la >> 5) * max_nb) << 5) + (la & 31);
+}
+
 // Verlet list (full, both directions) of every cell-sorted particle a:
 // partners b != a in the 27 (unique) neighbour cells with the
 // VerletCriterion (VerletCriterion.hpp:68-97): d^2 <= (max_cut+skin)^2 and
 // (both charged and d^2 <= (r_cut+skin)^2, or the type pair is active and
-// d^2 <= (ia_cut+skin)^2).  Neighbour k of a is stored at
-// nb[G.nb_off + k*G.np + (a - G.p0)] (per-replica capacity G.max_nb); a
-// replica whose capacity is exceeded reports its largest count in
-// overflow[replica].
+// d^2 <= (ia_cut+skin)^2).  Stored in the warp-tiled layout above
+// (per-replica capacity G.max_nb); a replica whose capacity is exceeded
+// reports its largest count in overflow[replica].
 __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
-                               const double4 *__restrict__ spq, const int *__restrict__ stype,
+                               const double4 *__restrict__ spq, const float4 *__restrict__ spf,
+                               const int *__restrict__ stype,
                                const int *__restrict__ scell, const int *__restrict__ cstart,
                                const PairIA *__restrict__ ia, int ntypes, long long n,
                                int *__restrict__ nb, int *__restrict__ nb_cnt,
@@ -104,14 +142,24 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
   int const rep = rep_of_sorted[a];
   RepGeom const &G = reps[rep];
   int const max_nb = G.max_nb;
-  int *nbp = nb + G.nb_off + (a - G.p0);
+  int *nbp = nb + nb_base(G.nb_off, max_nb, a - G.p0);
   double4 const pa = spq[a];
+  double const cs[3] = {G.box[0] / G.cg[0], G.box[1] / G.cg[1], G.box[2] / G.cg[2]};
+  double const ics[3] = {G.cg[0] * G.box_i[0], G.cg[1] * G.box_i[1], G.cg[2] * G.box_i[2]};
+  bool const small_grid = (G.cg[0] < 3) || (G.cg[1] < 3) || (G.cg[2] < 3);
+  // FP32 pre-check on the cell-relative offsets (exact geometry up to FP32
+  // rounding): candidates clearly beyond the list range are dropped before
+  // the FP64 minimum-image test, which alone decides membership
+  float4 const pfa = spf[a];
+  float const csf[3] = {static_cast<float>(cs[0]), static_cast<float>(cs[1]),
+                        static_cast<float>(cs[2])};
   int const ta = stype[a];
   int const loc = scell[a] - static_cast<int>(G.cell_off);
   int const c0 = loc % G.cg[0];
   int const c1 = (loc / G.cg[0]) % G.cg[1];
   int const c2 = loc / (G.cg[0] * G.cg[1]);
   double const emax2 = (G.max_cut + G.skin) * (G.max_cut + G.skin);
+  float const emax2_pre = static_cast<float>(emax2 * (1.0 + 1e-4));
   double const ecoul2 = (G.coulomb_cut > 0.0) ? (G.coulomb_cut + G.skin) * (G.coulomb_cut + G.skin) : -1.0;
   double const Li[3] = {G.box_i[0], G.box_i[1], G.box_i[2]};
   int count = 0;
@@ -132,25 +180,78 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
         int x = c0 + dx;
         x = (x < 0) ? x + G.cg[0] : (x >= G.cg[0] ? x - G.cg[0] : x);
         int const cell = static_cast<int>(G.cell_off) + x + G.cg[0] * (y + G.cg[1] * z);
-        for (int b = cstart[cell]; b < cstart[cell + 1]; ++b) {
-          if (b == a)
-            continue;
-          double4 const pb = spq[b];
-          double const d0 = mi_d(pa.x - pb.x, G.box[0], Li[0]);
-          double const d1 = mi_d(pa.y - pb.y, G.box[1], Li[1]);
-          double const d2v = mi_d(pa.z - pb.z, G.box[2], Li[2]);
-          double const d2 = d0 * d0 + d1 * d1 + d2v * d2v;
-          if (d2 > emax2)
-            continue;
-          bool take = (ecoul2 >= 0.0 && d2 <= ecoul2 && pa.w != 0.0 && pb.w != 0.0);
-          if (!take) {
-            double const ic = ia[ta * ntypes + stype[b]].ia_cut;
-            take = (ic != -1.0) && d2 <= (ic + G.skin) * (ic + G.skin);
-          }
-          if (take) {
-            if (count < max_nb)
-              nbp[static_cast<long long>(count) * G.np] = b;
-            ++count;
+        float const shx = -dx * csf[0], shy = -dy * csf[1], shz = -dz * csf[2];
+        // exact (FP64 minimum-image) test and store of one candidate
+        auto consider = [&](int b) {
+            double4 const pb = spq[b];
+            double const d0 = mi_d(pa.x - pb.x, G.box[0], Li[0]);
+            double const d1 = mi_d(pa.y - pb.y, G.box[1], Li[1]);
+            double const d2v = mi_d(pa.z - pb.z, G.box[2], Li[2]);
+            double const d2 = d0 * d0 + d1 * d1 + d2v * d2v;
+            if (d2 > emax2)
+              return;
+            bool take = (ecoul2 >= 0.0 && d2 <= ecoul2 && pa.w != 0.0 && pb.w != 0.0);
+            if (!take) {
+              double const ic = ia[ta * ntypes + stype[b]].ia_cut;
+              take = (ic != -1.0) && d2 <= (ic + G.skin) * (ic + G.skin);
+            }
+            if (take) {
+              if (count < max_nb) {
+                // cell offset dc of the partner's image: x_b' - x_a = dc cs +
+                // (off_b - off_a), an exact multiple of the cell size; with
+                // cells >= the list range, dc is -1, 0 or +1 per axis.  With
+                // 3 or more cells along an axis the minimum image is the image
+                // in the visited neighbour cell, so dc is the loop offset;
+                // with 1 or 2 cells it follows from the minimum-image vector.
+                int dcv[3] = {dx, dy, dz};
+                if (small_grid) {
+                  int const lb = scell[b] - static_cast<int>(G.cell_off);
+                  int const cb[3] = {lb % G.cg[0], (lb / G.cg[0]) % G.cg[1],
+                                     lb / (G.cg[0] * G.cg[1])};
+                  int const ca[3] = {c0, c1, c2};
+                  double const xa[3] = {pa.x, pa.y, pa.z}, xb[3] = {pb.x, pb.y, pb.z};
+                  double const dmi[3] = {-d0, -d1, -d2v};
+#pragma unroll
+                  for (int d = 0; d < 3; ++d)
+                    if (G.cg[d] < 3) {
+                      double const oa = xa[d] - ca[d] * cs[d], ob = xb[d] - cb[d] * cs[d];
+                      dcv[d] = static_cast<int>(rint((dmi[d] - (ob - oa)) * ics[d]));
+                    }
+                }
+                int const code = (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1);
+                nbp[static_cast<long long>(count) << 5] =
+                    static_cast<int>(static_cast<unsigned>(b - G.p0) |
+                                     (static_cast<unsigned>(code) << kNbIndexBits));
+              }
+              ++count;
+            }
+        };
+        int const b_lo = cstart[cell], b_hi = cstart[cell + 1];
+        if (small_grid) {
+          for (int b = b_lo; b < b_hi; ++b)
+            if (b != a)
+              consider(b);
+        } else {
+          // FP32 pre-check, four candidates per round (loads issued together)
+          for (int b0 = b_lo; b0 < b_hi; b0 += 4) {
+            float4 pf[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              pf[u] = (b0 + u < b_hi) ? spf[b0 + u] : pfa;
+            unsigned keep = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              float const e0 = (pfa.x - pf[u].x) + shx, e1 = (pfa.y - pf[u].y) + shy,
+                          e2 = (pfa.z - pf[u].z) + shz;
+              bool const in = (b0 + u < b_hi) && (b0 + u != a) &&
+                              (e0 * e0 + e1 * e1 + e2 * e2 <= emax2_pre);
+              keep |= (in ? 1u : 0u) << u;
+            }
+            while (keep) {
+              int const u = __ffs(keep) - 1;
+              keep &= keep - 1;
+              consider(b0 + u);
+            }
           }
         }
       }
@@ -249,6 +350,158 @@ __device__ inline void lj_wca(PairR<Real> const &p, Real dist, Real inv_d, Real 
 // FP64 partials {E_coul, E_nb, Vc[9], Vn[9]} (width 20).  Blocks map to
 // replicas through the block table so partials never straddle replicas.
 // Neighbour loads are issued two entries ahead of their use.
+// FP32-mixed real-space kernel over the same Verlet lists: positions are
+// FP32 offsets from each particle's build-time cell corner (cell_offset), the
+// list stores every partner's cell offset code, so
+//   d = x_a - x_b' = (off_a - off_b) - dc * cs
+// is formed in FP32 from small numbers (no minimum-image arithmetic, 16-byte
+// gathers); the geometry error is about one ulp of the cell size.  Pair
+// physics as k_pair_forces; per-particle force sums are FP32 over runs of 8
+// partners and FP64 across runs.
+template <bool EV>
+__global__ void __launch_bounds__(256, EV ? 1 : 4)
+k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+                  const float4 *__restrict__ spf, const int *__restrict__ stype,
+                  const int *__restrict__ perm, const PairIA *__restrict__ ia_g, int ntypes,
+                  const int *__restrict__ nb, const int *__restrict__ nb_cnt,
+                  double *__restrict__ f, int overwrite,
+                  double *__restrict__ partials) {
+  using Real = float;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float4 shift[27];
+  PairIA *ia = reinterpret_cast<PairIA *>(smem_raw);
+  for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
+    ia[k] = ia_g[k];
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  if (threadIdx.x < 27) {
+    int const c = threadIdx.x;
+    int const dc[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
+    shift[c] = make_float4(static_cast<float>(-dc[0] * (G.box[0] / G.cg[0])),
+                           static_cast<float>(-dc[1] * (G.box[1] / G.cg[1])),
+                           static_cast<float>(-dc[2] * (G.box[2] / G.cg[2])), 0.f);
+  }
+  __syncthreads();
+  long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  double ev[EV ? 20 : 1];
+#pragma unroll
+  for (int k = 0; k < (EV ? 20 : 1); ++k)
+    ev[k] = 0.0;
+  if (a < G.p0 + G.np) {
+    float4 const pa = spf[a];
+    int const ta = stype[a];
+    Real const alpha = static_cast<Real>(G.alpha);
+    Real const r_cut = static_cast<Real>(G.r_cut);
+    Real const two_a_sqrt_pi_i = static_cast<Real>(2.0 * G.alpha / sqrt(kPi));
+    Real const pref_qa = static_cast<Real>(G.prefactor) * pa.w;
+    bool const one_type = (ntypes == 1);
+    PairR<Real> const p0(ia[0]);
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    int const cnt = nb_cnt[a];
+    const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
+    long long const base0 = G.p0;
+    unsigned e_next = (cnt > 0) ? static_cast<unsigned>(nbp[0]) : 13u << kNbIndexBits;
+    float4 p_next = (cnt > 0) ? spf[base0 + (e_next & kNbIndexMask)] : pa;
+    for (int k = 0; k < cnt; ++k) {
+      unsigned const e = e_next;
+      int const b = static_cast<int>(base0 + (e & kNbIndexMask));
+      int const code = static_cast<int>(e >> kNbIndexBits);
+      float4 const pb = p_next;
+      if (k + 1 < cnt) {
+        e_next = static_cast<unsigned>(nbp[static_cast<long long>(k + 1) << 5]);
+        p_next = spf[base0 + (e_next & kNbIndexMask)];
+      }
+      float4 const sh = shift[code];
+      Real const d0 = (pa.x - pb.x) + sh.x;
+      Real const d1 = (pa.y - pb.y) + sh.y;
+      Real const d2v = (pa.z - pb.z) + sh.z;
+      Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
+      Real const inv_d = rsqrt_r(dist2);
+      Real const dist = dist2 * inv_d;
+      Real fc = Real(0), ec = Real(0);
+      Real const qb = pb.w;
+      if (qb != Real(0) && pref_qa != Real(0) && dist < r_cut && dist > Real(0)) {
+        Real const adist = alpha * dist;
+        Real const ex = exp_r(-adist * adist);
+        Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
+        Real const asp =
+            t * (Real(0.254829592) +
+                 t * (Real(-0.284496736) +
+                      t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
+        Real const erfc_part_ri = asp * inv_d;
+        Real const pq = pref_qa * qb;
+        fc = pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d));
+        if constexpr (EV)
+          ec = pq * erfc_part_ri * ex;
+      }
+      Real fn = Real(0), en = Real(0);
+      if (one_type) {
+        if (p0.active)
+          lj_wca(p0, dist, inv_d, fn, en);
+      } else {
+        PairR<Real> const p(ia[ta * ntypes + stype[b]]);
+        if (p.active)
+          lj_wca(p, dist, inv_d, fn, en);
+      }
+      Real const ft = fc + fn;
+      sx += ft * d0;
+      sy += ft * d1;
+      sz += ft * d2v;
+      if ((k & 7) == 7) {
+        fx += static_cast<double>(sx);
+        fy += static_cast<double>(sy);
+        fz += static_cast<double>(sz);
+        sx = sy = sz = 0.f;
+      }
+      if constexpr (EV) {
+        double const dd[3] = {d0, d1, d2v};
+        ev[0] += 0.5 * double(ec);
+        ev[1] += 0.5 * double(en);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
+            ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
+          }
+      }
+    }
+    fx += static_cast<double>(sx);
+    fy += static_cast<double>(sy);
+    fz += static_cast<double>(sz);
+    int const i = perm[a];
+    if (overwrite) {
+      f[3 * i + 0] = fx;
+      f[3 * i + 1] = fy;
+      f[3 * i + 2] = fz;
+    } else {
+      f[3 * i + 0] += fx;
+      f[3 * i + 1] += fy;
+      f[3 * i + 2] += fz;
+    }
+  }
+  if constexpr (EV) {
+    __shared__ double red[20][8];
+    int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 20; ++k) {
+      double v = ev[k];
+      for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0)
+        red[k][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 20) {
+      double s = 0.0;
+      for (int w = 0; w < (blockDim.x >> 5); ++w)
+        s += red[threadIdx.x][w];
+      partials[static_cast<long long>(blockIdx.x) * 20 + threadIdx.x] = s;
+    }
+  }
+}
+
 template <typename Real, bool EV>
 __global__ void __launch_bounds__(256, (sizeof(Real) == 4 && !EV) ? 4 : 1)
 k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
@@ -281,14 +534,18 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     PairR<Real> const p0(ia[0]);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     int const cnt = nb_cnt[a];
-    const int *nbp = nb + G.nb_off + (a - G.p0);
-    int b_next = (cnt > 0) ? nbp[0] : 0;
+    const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
+    int const base0 = static_cast<int>(G.p0);
+    int b_next =
+        (cnt > 0) ? base0 + static_cast<int>(static_cast<unsigned>(nbp[0]) & kNbIndexMask) : 0;
     double4 p_next = (cnt > 0) ? spq[b_next] : pa;
     for (int k = 0; k < cnt; ++k) {
       int const b = b_next;
       double4 const pb = p_next;
       if (k + 1 < cnt) {
-        b_next = nbp[static_cast<long long>(k + 1) * G.np];
+        b_next = base0 + static_cast<int>(
+                             static_cast<unsigned>(nbp[static_cast<long long>(k + 1) << 5]) &
+                             kNbIndexMask);
         p_next = spq[b_next];
       }
       // geometry in FP64 (two conversions per pair instead of four)

@@ -126,8 +126,8 @@ __global__ void k_place(const int *__restrict__ key, const int *__restrict__ slo
 // binning pass arrive in any order): one warp per bucket.  Buckets of up to
 // 128 entries are held in registers (4 per lane) and every entry's rank is
 // counted by shuffle comparisons against all others (entries are distinct
-// particle indices, so ranks are unique); larger buckets fall back to an
-// insertion sort by lane 0.
+// particle indices, so ranks are unique); larger buckets are left to
+// k_fix_big_buckets.
 __global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ perm,
                               long long nbuckets, const int *__restrict__ cond) {
   if (cond && !*cond)
@@ -141,19 +141,8 @@ __global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ p
   int const n = s1 - s0;
   if (n < 2)
     return;
-  if (n > 32 * NV) {
-    if (lane == 0)
-      for (int i = s0 + 1; i < s1; ++i) {
-        int const v = perm[i];
-        int j = i - 1;
-        while (j >= s0 && perm[j] > v) {
-          perm[j + 1] = perm[j];
-          --j;
-        }
-        perm[j + 1] = v;
-      }
-    return;
-  }
+  if (n > 32 * NV)
+    return; // large bucket: k_fix_big_buckets
   int v[NV], rank[NV];
 #pragma unroll
   for (int u = 0; u < NV; ++u) {
@@ -177,6 +166,50 @@ __global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ p
   for (int u = 0; u < NV; ++u)
     if (u * 32 + lane < n)
       perm[s0 + rank[u]] = v[u];
+}
+
+// Large buckets (> 128 entries), one block each: the bucket is copied to
+// shared memory and every thread counts the rank of its entries against the
+// whole bucket (O(n^2 / threads)); buckets beyond kBigBucket entries fall
+// back to an insertion sort by thread 0.
+constexpr int kBigBucket = 8192;
+__global__ void __launch_bounds__(256)
+k_fix_big_buckets(const int *__restrict__ start, int *__restrict__ perm, long long nbuckets,
+                  const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  __shared__ int sv[kBigBucket];
+  for (long long b = blockIdx.x; b < nbuckets; b += gridDim.x) {
+    int const s0 = start[b], s1 = start[b + 1];
+    int const n = s1 - s0;
+    if (n <= 128)
+      continue; // block-uniform
+    if (n > kBigBucket) {
+      if (threadIdx.x == 0)
+        for (int i = s0 + 1; i < s1; ++i) {
+          int const v = perm[i];
+          int j = i - 1;
+          while (j >= s0 && perm[j] > v) {
+            perm[j + 1] = perm[j];
+            --j;
+          }
+          perm[j + 1] = v;
+        }
+      __syncthreads();
+      continue;
+    }
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+      sv[k] = perm[s0 + k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      int const v = sv[k];
+      int r = 0;
+      for (int m = 0; m < n; ++m)
+        r += (sv[m] < v) ? 1 : 0;
+      perm[s0 + r] = v;
+    }
+    __syncthreads();
+  }
 }
 
 // Host driver of the three-pass exclusive scan (out has n+1 entries).
