@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--workload", default="single", choices=["single", "batched"],
                     help="single large system (default) or batched replicas")
     ap.add_argument("--replicas", type=int, default=512)
+    ap.add_argument("--skin", type=float, default=None,
+                    help="Verlet skin (default 0.4 single system; 0.8 batched: the fastest of "
+                         "0.4/0.6/0.8/1.0 in timed trials of the batched Langevin run, as a "
+                         "skin tuning would choose)")
     ap.add_argument("--profile-only", action="store_true",
                     help="setup + a few evaluations, no JSON (for ncu captures)")
     return ap.parse_args()
@@ -249,7 +253,7 @@ def run_batched(args):
     d.prefactor = prefs.ctypes.data_as(P(ctypes.c_double))
     d.offset = offs.ctypes.data_as(P(ctypes.c_longlong))
     d.accuracy = args.accuracy
-    d.skin = 0.4
+    d.skin = args.skin if args.skin is not None else 0.8
     d.single_precision = 0 if args.fp64 else 1
     d.mesh_min, d.mesh_max, d.cao_min, d.cao_max = 16, 64, 3, 7
     tab = (_lib.PairParams * 1)()
@@ -290,7 +294,7 @@ def run_batched(args):
     rcs = np.array([x[2] for x in tuned])
     nrep = np.diff(offs).astype(float)
     # full-list Verlet candidates per step: N (4/3) pi (r_cut + skin)^3 rho
-    pair_cand = float((nrep * 4.18879 * (np.maximum(rcs, 2 ** (1 / 6)) + 0.4) ** 3 *
+    pair_cand = float((nrep * 4.18879 * (np.maximum(rcs, 2 ** (1 / 6)) + d.skin) ** 3 *
                        nrep / boxes[:, 0] ** 3).sum())
     cpu = None
     if not args.no_cpu_baseline:
@@ -322,7 +326,7 @@ def run_batched(args):
                                f"[1e3, 5e4] (total {n}), density 0.3, +/-1 or +/-2 ions, "
                                f"l_B U[0.5, 4], WCA, P3M accuracy {args.accuracy}, meshes "
                                f"16-64 and cao 3-7 autotuned, Langevin VV dt 0.01 in one "
-                               f"CUDA graph per step",
+                               f"CUDA graph per step, Verlet skin {d.skin:g}",
                    "total_particles": int(n), "tuning_s": t_tune,
                    "mesh_hist": {int(m): int((meshes == m).sum()) for m in np.unique(meshes)},
                    "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max()),
@@ -364,7 +368,7 @@ def main():
               r_cut=args.r_cut, tune=True, timings=2, verbose=False)
     s = eb.System(box_l=[box] * 3)
     s.time_step = 0.01
-    s.cell_system.skin = 0.4
+    s.cell_system.skin = args.skin if args.skin is not None else 0.4
     s.part.add(pos=pos, q=q)
     s.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0, cutoff=2.5,
                                                       shift="auto")

@@ -232,15 +232,16 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
             if (b != a)
               consider(b);
         } else {
-          // FP32 pre-check, four candidates per round (loads issued together)
-          for (int b0 = b_lo; b0 < b_hi; b0 += 4) {
-            float4 pf[4];
+          // FP32 pre-check, kPre candidates per round (loads issued together)
+          constexpr int kPre = 8;
+          for (int b0 = b_lo; b0 < b_hi; b0 += kPre) {
+            float4 pf[kPre];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < kPre; ++u)
               pf[u] = (b0 + u < b_hi) ? spf[b0 + u] : pfa;
             unsigned keep = 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kPre; ++u) {
               float const e0 = (pfa.x - pf[u].x) + shx, e1 = (pfa.y - pf[u].y) + shy,
                           e2 = (pfa.z - pf[u].z) + shz;
               bool const in = (b0 + u < b_hi) && (b0 + u != a) &&
