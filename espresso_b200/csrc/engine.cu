@@ -527,7 +527,9 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   m_launches += 3;
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
   k_fix_buckets<<<ceil_div(nkeys * 32, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
-  k_fix_big_buckets<<<static_cast<int>(std::min<long long>(nkeys, 4096)), 256, 0, st>>>(
+  // block-uniform walk over the buckets, two blocks per SM (most buckets
+  // are small and skipped)
+  k_fix_big_buckets<<<static_cast<int>(std::min<long long>(nkeys, 296)), 256, 0, st>>>(
       start, perm, nkeys, cond); ++m_launches;
 }
 
