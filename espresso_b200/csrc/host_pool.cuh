@@ -82,6 +82,20 @@ public:
     });
   }
 
+  // Parallel memcmp: true when the two byte ranges are equal.
+  bool equal(const void *a, const void *b, size_t bytes) {
+    size_t const piece = std::max<size_t>(256 << 10, (bytes + size() - 1) / size());
+    int const n = static_cast<int>((bytes + piece - 1) / piece);
+    std::atomic<bool> same{true};
+    run(n, [&](int i) {
+      size_t const b0 = i * piece, b1 = std::min(bytes, b0 + piece);
+      if (std::memcmp(static_cast<const char *>(a) + b0, static_cast<const char *>(b) + b0,
+                      b1 - b0) != 0)
+        same.store(false, std::memory_order_relaxed);
+    });
+    return same.load();
+  }
+
 private:
   // Claim tasks of generation gen: the counter holds (generation << 32 |
   // next index), so a worker holding a stale generation claims nothing.

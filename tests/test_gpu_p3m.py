@@ -314,6 +314,27 @@ def test_host_staging_chunks_accumulate_and_device_pointers():
                                None, None, flags | _lib.P3MX_DEVICE_PTRS, None), act._handle)
     torch.cuda.synchronize()
     assert np.array_equal(df.cpu().numpy(), f_ow)
+    # unchanged charges are not staged again: a changed chunk must be sent
+    # (one + and one - ion swap sign, in different 4 MB chunks)
+    q2 = q.copy()
+    i_plus = int(np.flatnonzero(q2 > 0)[1000])
+    i_minus = int(np.flatnonzero(q2 < 0)[-1000])
+    q2[i_plus], q2[i_minus] = -q2[i_plus], -q2[i_minus]
+    f2 = np.zeros((n, 3))
+    _lib.check(lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q2), None,
+                               _lib.dptr(f2), None, None, flags, None), act._handle)
+    dq2 = torch.from_numpy(q2).cuda()
+    torch.cuda.synchronize()
+    _lib.check(lib.p3mx_forces(act._handle, n, dp.data_ptr(), dq2.data_ptr(), None, df.data_ptr(),
+                               None, None, flags | _lib.P3MX_DEVICE_PTRS, None), act._handle)
+    torch.cuda.synchronize()
+    assert not np.array_equal(f2, f_ow)
+    assert np.array_equal(df.cpu().numpy(), f2)
+    # and back to the original charges through the host path again
+    f3 = np.zeros((n, 3))
+    _lib.check(lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q), None,
+                               _lib.dptr(f3), None, None, flags, None), act._handle)
+    assert np.array_equal(f3, f_ow)
 
 
 @pytest.mark.parametrize("cls", [P3M, P3MGPU])
