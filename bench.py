@@ -406,6 +406,30 @@ def main():
     nst = ctypes.c_int()
     _lib.check(lib.p3mx_profile(h, 5, ms, names, 32, ctypes.byref(nst)), h)
     stages = {names[k].decode(): ms[k] for k in range(nst.value)}
+    # timed comparison (not used by the path): cuFFT through torch.fft on the
+    # same mesh, one r2c and three c2r transforms as one force evaluation
+    # needs, against the hand-written FFT stages above
+    cufft_ms = None
+    if rank == 0 and not args.fp64:
+        M = args.mesh
+        xr = torch.randn((M, M, M), dtype=torch.float32, device=dev)
+        xc = torch.fft.rfftn(xr)
+        for _ in range(3):
+            torch.fft.rfftn(xr)
+            torch.fft.irfftn(xc, s=(M, M, M))
+        torch.cuda.synchronize(dev)
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record()
+        for _ in range(5):
+            torch.fft.rfftn(xr)
+            for _ in range(3):
+                torch.fft.irfftn(xc, s=(M, M, M))
+        c1.record()
+        torch.cuda.synchronize(dev)
+        cufft_ms = c0.elapsed_time(c1) / 5
+        del xr, xc
+        torch.cuda.empty_cache()
     # rebuild cost: one evaluation with a forced Verlet rebuild
     lc0 = ctypes.c_longlong()
     lc1 = ctypes.c_longlong()
@@ -543,6 +567,12 @@ def main():
                      "traffic": traffic, "peak_kind": hbm_kind,
                      "algorithmic_bytes": alg, "launch_ms": dom_ms, "fp32": fp32},
         "stages_ms": stages,
+        "fft_comparison": None if cufft_ms is None else {
+            "cufft_r2c_plus_3_c2r_ms": cufft_ms,
+            "own_fft_stages_ms": stages.get("fft_fwd_zy", 0) + stages.get("fft_x_kspace", 0) +
+                                 stages.get("fft_inv_yz", 0),
+            "note": "own stages include the influence function, ik-differentiation, "
+                    "energy/virial sums and the packed field-mesh output"},
         "accuracy": {"rms_force_err_estimate": prm["accuracy"],
                      "fp32_vs_fp64_rms_coulomb_force_diff": fp_diff,
                      "rms_coulomb_force": f_rms},

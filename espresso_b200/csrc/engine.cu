@@ -527,9 +527,8 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
   m_launches += 3;
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
   k_fix_buckets<<<ceil_div(nkeys * 32, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
-  // block-uniform walk over the buckets, two blocks per SM (most buckets
-  // are small and skipped)
-  k_fix_big_buckets<<<static_cast<int>(std::min<long long>(nkeys, 296)), 256, 0, st>>>(
+  k_fix_big_buckets<<<static_cast<int>(std::min<long long>(ceil_div(nkeys, 256), 296)), 256, 0,
+                      st>>>(
       start, perm, nkeys, cond); ++m_launches;
 }
 
@@ -750,25 +749,25 @@ __global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__res
     return;
   int const i = perm[s];
   RepGeom const &G = reps[rep_of[i]];
-  double4 const v = make_double4(fold_coord(pos[3 * i], G.box[0]),
-                                 fold_coord(pos[3 * i + 1], G.box[1]),
-                                 fold_coord(pos[3 * i + 2], G.box[2]), q[i]);
-  spq[s] = v;
+  double const qi = q[i];
+  if (spq) // FP64 pair kernel positions, only when that kernel runs next
+    spq[s] = make_double4(fold_coord(pos[3 * i], G.box[0]), fold_coord(pos[3 * i + 1], G.box[1]),
+                          fold_coord(pos[3 * i + 2], G.box[2]), qi);
   spf[s] = cell_offset(G, scell[s] - static_cast<int>(G.cell_off), pos_ref + 3 * i, pos + 3 * i,
-                       v.w);
+                       qi);
 }
 
-void Engine::refresh_sorted_positions(cudaStream_t st) {
+void Engine::refresh_sorted_positions(cudaStream_t st, bool want_spq) {
   k_refresh_spq<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(),
                                                     m_cperm.as<int>(), d_pos(), d_q(),
                                                     m_scell.as<int>(), m_pos_ref.as<double>(),
-                                                    m_n, m_spq.as<double4>(),
+                                                    m_n, want_spq ? m_spq.as<double4>() : nullptr,
                                                     m_spf.as<float4>()); ++m_launches;
 }
 
 // Displacement check (host decision) and list rebuild or sorted-position
 // refresh: after it the pair kernel can run.
-void Engine::prepare_short_range(cudaStream_t st) {
+void Engine::prepare_short_range(cudaStream_t st, bool need_spq) {
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
   bool rebuild = !m_lists_valid;
@@ -785,7 +784,7 @@ void Engine::prepare_short_range(cudaStream_t st) {
   if (rebuild)
     build_lists(st);
   else
-    refresh_sorted_positions(st);
+    refresh_sorted_positions(st, need_spq);
   mark(rebuild ? "sr_rebuild" : "sr_refresh", st);
 }
 
@@ -826,7 +825,7 @@ template <typename Real>
 void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t st) {
   if (m_n == 0)
     return;
-  prepare_short_range(st);
+  prepare_short_range(st, sizeof(Real) == 8);
   launch_pair<Real>(f, overwrite, want_ev, st);
   mark("pair_forces", st);
 }
@@ -845,7 +844,7 @@ void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
     P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_fork, cudaEventDisableTiming));
     P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_join, cudaEventDisableTiming));
   }
-  prepare_short_range(st);
+  prepare_short_range(st, !m_fp32);
   P3MX_CUDA(cudaEventRecord(m_ev_fork, st));
   P3MX_CUDA(cudaStreamWaitEvent(m_side, m_ev_fork, 0));
   if (m_fp32)
@@ -920,7 +919,7 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                      m_overflow.as<int>(), flag); ++m_launches;
   k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag); ++m_launches;
-  refresh_sorted_positions(st);
+  refresh_sorted_positions(st, !m_fp32);
   if (m_fp32)
     launch_pair<float>(f, overwrite, false, st);
   else

@@ -135,11 +135,12 @@ private:
                                               cudaStream_t st);
   template <typename Real> void launch_pair(double *f, bool overwrite, bool want_ev,
                                             cudaStream_t st);
-  void prepare_short_range(cudaStream_t st);
+  void prepare_short_range(cudaStream_t st, bool need_spq);
   void build_lists(cudaStream_t st);
   void set_list_capacity(double margin);
   void layout_lists(cudaStream_t st);
-  void refresh_sorted_positions(cudaStream_t st);
+  // want_spq: also the FP64 double4 positions (FP64 pair kernel)
+  void refresh_sorted_positions(cudaStream_t st, bool want_spq = true);
   void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
                  cudaStream_t st, const int *cond = nullptr);
 

@@ -168,10 +168,11 @@ __global__ void k_fix_buckets(const int *__restrict__ start, int *__restrict__ p
       perm[s0 + rank[u]] = v[u];
 }
 
-// Large buckets (> 128 entries), one block each: the bucket is copied to
-// shared memory and every thread counts the rank of its entries against the
-// whole bucket (O(n^2 / threads)); buckets beyond kBigBucket entries fall
-// back to an insertion sort by thread 0.
+// Large buckets (> 128 entries): each thread checks one bucket, the block
+// collects the large ones and sorts them one after another: the bucket is
+// copied to shared memory and every thread counts the rank of its entries
+// against the whole bucket (O(n^2 / threads)); buckets beyond kBigBucket
+// entries fall back to an insertion sort by thread 0.
 constexpr int kBigBucket = 8192;
 __global__ void __launch_bounds__(256)
 k_fix_big_buckets(const int *__restrict__ start, int *__restrict__ perm, long long nbuckets,
@@ -179,36 +180,49 @@ k_fix_big_buckets(const int *__restrict__ start, int *__restrict__ perm, long lo
   if (cond && !*cond)
     return;
   __shared__ int sv[kBigBucket];
-  for (long long b = blockIdx.x; b < nbuckets; b += gridDim.x) {
-    int const s0 = start[b], s1 = start[b + 1];
-    int const n = s1 - s0;
-    if (n <= 128)
-      continue; // block-uniform
-    if (n > kBigBucket) {
-      if (threadIdx.x == 0)
-        for (int i = s0 + 1; i < s1; ++i) {
-          int const v = perm[i];
-          int j = i - 1;
-          while (j >= s0 && perm[j] > v) {
-            perm[j + 1] = perm[j];
-            --j;
+  __shared__ long long list[256];
+  __shared__ int nlist;
+  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < nbuckets;
+       base += static_cast<long long>(gridDim.x) * blockDim.x) {
+    // every thread checks one bucket; the large ones are handled by the block
+    if (threadIdx.x == 0)
+      nlist = 0;
+    __syncthreads();
+    long long const bt = base + threadIdx.x;
+    if (bt < nbuckets && start[bt + 1] - start[bt] > 128)
+      list[atomicAdd(&nlist, 1)] = bt;
+    __syncthreads();
+    int const nl = nlist;
+    for (int li = 0; li < nl; ++li) {
+      long long const b = list[li];
+      int const s0 = start[b], s1 = start[b + 1];
+      int const n = s1 - s0;
+      if (n > kBigBucket) {
+        if (threadIdx.x == 0)
+          for (int i = s0 + 1; i < s1; ++i) {
+            int const v = perm[i];
+            int j = i - 1;
+            while (j >= s0 && perm[j] > v) {
+              perm[j + 1] = perm[j];
+              --j;
+            }
+            perm[j + 1] = v;
           }
-          perm[j + 1] = v;
-        }
+        __syncthreads();
+        continue;
+      }
+      for (int k = threadIdx.x; k < n; k += blockDim.x)
+        sv[k] = perm[s0 + k];
       __syncthreads();
-      continue;
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        int const v = sv[k];
+        int r = 0;
+        for (int m = 0; m < n; ++m)
+          r += (sv[m] < v) ? 1 : 0;
+        perm[s0 + r] = v;
+      }
+      __syncthreads();
     }
-    for (int k = threadIdx.x; k < n; k += blockDim.x)
-      sv[k] = perm[s0 + k];
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      int const v = sv[k];
-      int r = 0;
-      for (int m = 0; m < n; ++m)
-        r += (sv[m] < v) ? 1 : 0;
-      perm[s0 + r] = v;
-    }
-    __syncthreads();
   }
 }
 
