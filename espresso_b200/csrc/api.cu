@@ -813,6 +813,13 @@ static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *
   h->staged_type = (type != nullptr);
 }
 
+// Raise the error of a kernel whose bounded wait ran out (both engines).
+static void check_kernels(p3mx_handle *h, cudaStream_t st) {
+  h->eng->check_kernel_error(st);
+  if (h->eng64)
+    h->eng64->check_kernel_error(st);
+}
+
 static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwrite,
                       cudaStream_t st) {
   Engine &e = *h->eng;
@@ -882,6 +889,7 @@ int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q
     if (fd)
       stage_out(h, n, f, dev, ow, st);
     P3MX_CUDA(cudaStreamSynchronize(st));
+    check_kernels(h, st);
   });
 }
 
@@ -961,6 +969,7 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     if (f)
       stage_out(h, n, f, dev, ow, st);
     P3MX_CUDA(cudaStreamSynchronize(st));
+    check_kernels(h, st);
   });
 }
 

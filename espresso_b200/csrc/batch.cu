@@ -539,6 +539,7 @@ int p3mx_batch_forces(p3mx_batch *b, double *energy_out) {
       for (int r = 0; r < R; ++r)
         energy_out[r] = ek[r] + es[2 * r] + es[2 * r + 1];
     P3MX_CUDA(cudaStreamSynchronize(st));
+    e.check_kernel_error(st);
     b->forces_valid = true;
   });
 }
@@ -595,6 +596,7 @@ int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT, double gamma,
       P3MX_CUDA(cudaGraphLaunch(b->graph, st));
     b->graph_launches += steps;
     P3MX_CUDA(cudaStreamSynchronize(st));
+    e.check_kernel_error(st);
     if (e.list_overflow(st))
       throw Error(P3MX_ERUNTIME, "Verlet list capacity exceeded during the graph run");
   });

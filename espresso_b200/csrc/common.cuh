@@ -115,6 +115,49 @@ __device__ inline void staged_copy(int total, L const &load, S const &store) {
   }
 }
 
+// ---- bulk-copy engine (TMA) helpers: cp.async.bulk global -> shared with
+// completion on an mbarrier (transaction bytes); waits are bounded.
+__device__ inline unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ inline void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Arrive (one of the barrier's expected arrivals) and add `bytes` to the
+// transaction count of the current phase.
+__device__ inline void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned).
+__device__ inline void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Wait until the phase with the given parity completes; false when the
+// iteration limit ran out (the caller reports it and bails out).
+__device__ inline bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done)
+      return true;
+  }
+  return false;
+}
+
 inline int ceil_div(long long a, long long b) {
   return static_cast<int>((a + b - 1) / b);
 }

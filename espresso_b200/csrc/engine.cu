@@ -469,6 +469,10 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_nb_cnt.ensure(n * sizeof(int));
   m_overflow.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_flag.ensure(sizeof(int));
+  if (m_kerr.p == nullptr) {
+    m_kerr.ensure(sizeof(int));
+    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(int), st));
+  }
   m_pos_ref.ensure(3 * n * sizeof(double));
   m_part_pair.ensure(static_cast<size_t>(m_n_blk_pair) * 20 * sizeof(double));
   m_sums_pair.ensure(static_cast<size_t>(R) * 20 * sizeof(double));
@@ -599,7 +603,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
       P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps,
                                    assign_smem<Real, P>(m_tile_cap), st>>>(
                                    geom, tab, cnt, m_tile_cap, m_start.as<int>(), m_W.as<Real>(),
-                                   m_skey.as<int>(), m_rho.as<Real>())));
+                                   m_skey.as<int>(), m_rho.as<Real>(), m_kerr.as<int>())));
       ++m_launches;
     }
   }
@@ -643,7 +647,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
                                  geom, m_blk_brick.as<int2>(), nbr, m_start.as<int>(),
                                  m_perm.as<int>(), m_skey.as<int>(), m_W.as<Real>(),
                                  m_E.as<Real>(), d_q(), m_dipole.as<double>(), f,
-                                 overwrite ? 1 : 0)));
+                                 overwrite ? 1 : 0, m_kerr.as<int>())));
     ++m_launches;
   }
   mark("p3m_interp", st);
@@ -1060,6 +1064,18 @@ double Engine::ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, d
   for (double v : part)
     he_q += v;
   return 2. * prefactor * sum_q2 * std::sqrt(he_q / static_cast<double>(n_c_part)) / (box[1] * box[2]);
+}
+
+void Engine::check_kernel_error(cudaStream_t st) {
+  if (m_kerr.p == nullptr)
+    return;
+  int flag = 0;
+  P3MX_CUDA(cudaMemcpyAsync(&flag, m_kerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  if (flag) {
+    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(int), st));
+    throw Error(3, "a bulk copy into shared memory did not complete within the wait limit");
+  }
 }
 
 void Engine::mark(const char *name, cudaStream_t st) {

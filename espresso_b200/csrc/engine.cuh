@@ -121,6 +121,8 @@ public:
   // Per-stage device times (ms, mean of reps) of one full force evaluation,
   // measured with CUDA events between the stages on the stream.
   std::vector<std::pair<std::string, double>> profile(int reps, cudaStream_t st);
+  // Throws if a kernel reported that a bounded wait ran out (synchronises st).
+  void check_kernel_error(cudaStream_t st);
   // Number of kernels launched by this engine so far.
   long long launches() const { return m_launches; }
 
@@ -189,6 +191,7 @@ private:
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_part_pair, m_sums_pair;
+  DevBuf m_kerr; // set by a kernel whose bounded wait ran out
   std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;
   // misc host staging

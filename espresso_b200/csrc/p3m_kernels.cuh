@@ -219,7 +219,7 @@ template <typename Real, int P>
 __global__ void __launch_bounds__(32 * kAssignWarps)
 k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
              int tile_cap, const int *__restrict__ start, const Real *__restrict__ W,
-             const int *__restrict__ s_key, Real *__restrict__ rho) {
+             const int *__restrict__ s_key, Real *__restrict__ rho, int *__restrict__ err) {
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
@@ -229,6 +229,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   constexpr int CH = kAssignChunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[kAssignWarps];
+  __shared__ __align__(8) unsigned long long bar;
   if (static_cast<int>(blockIdx.x) >= nbricks)
     return; // whole block
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -243,29 +244,47 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int *t_lo = t_hi + tile_cap;
   Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes(tile_cap));
   int *rbase = reinterpret_cast<int *>(rec + CH * WS);
+  if (tid == 0)
+    mbar_init(&bar, 1);
   for (int t = tid; t < E3; t += NT) {
     t_hi[t] = 0;
     t_lo[t] = 0;
   }
-  // stage a chunk of records (contiguous; asynchronous 16-byte copies) and
-  // each particle's tile base offset
-  auto stage = [&](int c0, int cn) {
-    const char *src = reinterpret_cast<const char *>(W + static_cast<long long>(c0) * WS);
-    unsigned const dst = static_cast<unsigned>(__cvta_generic_to_shared(rec));
-    int const nbytes = cn * WS * static_cast<int>(sizeof(Real));
-    for (int o = 16 * tid; o < nbytes; o += 16 * NT)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + o), "l"(src + o)
-                   : "memory");
+  __syncthreads(); // barrier initialised
+  // stage a chunk of records (contiguous, 16-byte aligned: one bulk copy by
+  // the TMA engine, completing on the mbarrier) and each particle's tile base
+  // offset; false when the copy did not land within the wait limit
+  unsigned parity = 0;
+  auto stage = [&](int c0, int cn) -> bool {
+    if (tid == 0) {
+      unsigned const nbytes = static_cast<unsigned>(cn * WS * sizeof(Real));
+      // the records of the previous chunk were read through the generic
+      // proxy: order those reads before the asynchronous-proxy writes
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_expect_tx(&bar, nbytes);
+      bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
+    }
     for (int j = tid; j < cn; j += NT) {
       int const l = s_key[c0 + j] - bk.y * B3;
       int const lb = __ffs(B) - 1; // B is a power of two
       rbase[j] = ((l >> (2 * lb)) * E + ((l >> lb) & (B - 1))) * E + (l & (B - 1));
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    bool const ok = mbar_wait(&bar, parity);
+    parity ^= 1u;
+    // the whole block leaves together if any thread gave up
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        mbar_wait(&bar, parity ^ 1u); // second bounded wait for the copy in flight
+      }
+      return false;
+    }
+    return true;
   };
   int const cnt = s1 - s0;
-  stage(s0, min(CH, cnt));
-  __syncthreads(); // tile zeroed, first chunk staged
+  if (!stage(s0, min(CH, cnt)))
+    return;
+  // (the vote inside stage() also orders the tile zeroing and the first chunk)
   // total |q| of the brick: the x weights of a record are q*wx with wx >= 0
   // summing to 1, so sum_k |q wx_k| = |q|
   double aq = 0.0;
@@ -309,8 +328,8 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     int const cn = min(CH, s1 - c0);
     if (c0 != s0) {
       __syncthreads(); // previous chunk consumed
-      stage(c0, cn);
-      __syncthreads();
+      if (!stage(c0, cn))
+        return;
     }
     for (int j = warp; j < cn; j += kAssignWarps) {
       int const base = rbase[j];
@@ -427,7 +446,8 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
              const int *__restrict__ start, const int *__restrict__ perm,
              const int *__restrict__ s_key, const Real *__restrict__ W,
              const Real *__restrict__ E, const double *__restrict__ q,
-             const double *__restrict__ dipole, double *__restrict__ f, int overwrite) {
+             const double *__restrict__ dipole, double *__restrict__ f, int overwrite,
+             int *__restrict__ err) {
   static_assert(P <= 8, "one lane per stencil z offset");
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
@@ -462,35 +482,37 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   else if (tid >= 32 && tid - 32 < Ed)
     s_yo[tid - 32] = wrap(y0 + tid - 32, M1) * M2;
   __syncthreads();
-  // tile rows (x, y) of Ed records along z; lane groups of gs lanes copy one
-  // row each with asynchronous 16-byte copies (cp.async, L2 only), all in
-  // flight together; rows advance by increment (no division)
-  int const gs = (Ed <= 8) ? 8 : (Ed <= 16 ? 16 : 32);
-  int const rpw = 32 / gs;
-  int const zl = lane & (gs - 1);
-  int const zo = wrap(z0 + zl, M2);
-  int const step = kAssignWarps * rpw;
-  int row = warp * rpw + lane / gs;
-  int x = row / Ed, y = row - (row / Ed) * Ed;
-  unsigned const tbase = static_cast<unsigned>(__cvta_generic_to_shared(tile));
-  for (; row < E2; row += step) {
-    if (zl < Ed) {
-      const R4 *src = E4 + (s_xo[x] + s_yo[y] + zo);
-      unsigned const dst = tbase + static_cast<unsigned>((row * Ed + zl) * sizeof(R4));
-#pragma unroll
-      for (int h = 0; h < static_cast<int>(sizeof(R4) / 16); ++h)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * h),
-                     "l"(reinterpret_cast<const char *>(src) + 16 * h)
-                     : "memory");
-    }
-    y += step;
-    while (y >= Ed) {
-      y -= Ed;
-      ++x;
+  // tile rows (x, y) of Ed records along z are contiguous in the field mesh
+  // (two pieces when the row wraps around z): one bulk copy (TMA engine) per
+  // piece, all completing on one mbarrier that expects the whole tile
+  __shared__ __align__(8) unsigned long long bar;
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, static_cast<unsigned>(E2 * Ed * sizeof(R4)));
+  }
+  __syncthreads();
+  for (int row = tid; row < E2; row += NT) {
+    int const x = row / Ed, y = row - x * Ed;
+    const R4 *src = E4 + (s_xo[x] + s_yo[y]);
+    R4 *dst = tile + row * Ed;
+    // pieces of the row up to each z wrap (several when the mesh is shorter
+    // than the tile along z); each piece stays inside its mesh row
+    int z = z0, done = 0;
+    while (done < Ed) {
+      int const len = min(Ed - done, M2 - z);
+      bulk_g2s(dst + done, src + z, static_cast<unsigned>(len * sizeof(R4)), &bar);
+      done += len;
+      z = 0;
     }
   }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  __syncthreads();
+  bool const ok = mbar_wait(&bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      mbar_wait(&bar, 0); // second bounded wait for the copies in flight
+    }
+    return;
+  }
   int const g = lane >> 3, kz = lane & 7;
   double const pref = G.prefactor / G.V;
   double const cdip = (G.epsilon != 0.0)
