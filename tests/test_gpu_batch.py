@@ -150,3 +150,33 @@ def test_batch_rejects_bad_descriptors():
     with pytest.raises(RuntimeError, match="cubic"):
         create(bad, prefs, pos, q, offs)
     del lib
+
+
+def test_batch_forces_after_langevin_run_match_oracle():
+    """After 60 graph-captured Langevin steps (device-side Verlet rebuilds,
+    particles crossing cell and box boundaries), a force evaluation at the
+    current positions matches the FP64 oracle per replica."""
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas(seed=13, n_rep=4)
+    h = create(boxes, prefs, pos, q, offs, cao=(5, 5))
+    try:
+        assert lib.p3mx_batch_run(h, 60, 0.005, 1.0, 1.0, 99) == 0
+        R = len(prefs)
+        en = np.zeros(R)
+        assert lib.p3mx_batch_forces(h, en.ctypes.data_as(_P(ctypes.c_double))) == 0
+        x = np.zeros_like(pos)
+        f = np.zeros_like(pos)
+        assert lib.p3mx_batch_get(h, x.ctypes.data_as(_P(ctypes.c_double)),
+                                  f.ctypes.data_as(_P(ctypes.c_double)), None) == 0
+        assert np.abs(x - pos).max() > 0.05  # the particles did move
+        tab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
+        for r in range(R):
+            t = tuned(h, r)
+            sl = slice(offs[r], offs[r + 1])
+            p = O.make_params(boxes[r], list(t.mesh), t.cao, t.alpha, t.r_cut, prefs[r])
+            fk, _, _ = O.p3m_kspace(p, x[sl], q[sl])
+            fr, _, _, _ = O.short_range(p, x[sl], q[sl], None, 1, tab)
+            ref = fk + fr
+            np.testing.assert_allclose(f[sl], ref, atol=3e-5 * np.abs(ref).max(), rtol=0)
+    finally:
+        lib.p3mx_batch_destroy(h)

@@ -356,3 +356,40 @@ def test_headline_parameters_rms_error_vs_ewald(cls):
     rms = np.sqrt(((f - fe) ** 2).sum(1).mean())
     assert rms < 1e-4
     assert rms > 1e-6  # the comparison resolves the P3M discretisation error
+
+
+@pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
+def test_forces_after_moves_across_the_boundary(cls, rtol):
+    """Forces after moves that keep the Verlet list (below skin/2) or force
+    a rebuild, with ions crossing the periodic boundary and unfolded input
+    coordinates, equal the oracle's on the moved configuration: the
+    FP32-mixed kernel's cell-relative geometry must follow the particles."""
+    box = 12.0
+    pos, q = jittered_lattice(8, box, 0.2, seed=21)  # 512 ions
+    pos[:8, 0] = box - 0.03
+    pos[8:16, 1] = 0.02
+    pos[16:24, 2] = box - 0.01
+    s = make_system([box] * 3, pos, q)
+    s.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0, cutoff=2.5,
+                                                      shift="auto")
+    s.electrostatics.solver = cls(prefactor=1.0, accuracy=1e-3, mesh=24, cao=5, alpha=1.0,
+                                  r_cut=3.0, tune=False)
+    s.integrator.run(0, recalc_forces=True)
+    shift = -((1.0 / 2.5) ** 12 - (1.0 / 2.5) ** 6)
+    tab = O.pair_table(1, {(0, 0): dict(lj_eps=1.0, lj_sig=1.0, lj_cut=2.5, lj_shift=shift)})
+    p = O.make_params([box] * 3, [24] * 3, 5, 1.0, 3.0, 1.0)
+    rng = np.random.default_rng(5)
+    cur = pos.copy()
+    for step in range(4):
+        d = rng.uniform(-0.05, 0.05, cur.shape)
+        d[:8, 0] = 0.06    # across x = box
+        d[8:16, 1] = -0.05  # across y = 0
+        d[16:24, 2] = 0.04  # across z = box
+        cur = cur + d       # unfolded coordinates, outside [0, box) for some
+        s.part.all().pos = cur
+        s.integrator.run(0, recalc_forces=True)
+        f = s.part.all().f
+        fk, _, _ = O.p3m_kspace(p, cur, q)
+        fr, _, _, _ = O.short_range(p, cur, q, None, 1, tab)
+        ref = fk + fr
+        np.testing.assert_allclose(f, ref, atol=rtol * np.abs(ref).max() * 10, rtol=0)
