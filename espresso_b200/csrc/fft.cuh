@@ -347,34 +347,40 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   load_twiddles(tw, twtab, G.plan[2]);
   long long const line0 = bk.a;
   const Real *src = rmesh + G.rm_off + line0 * n;
-  // real line element e = l*n + k -> real or imaginary part of slot l/2
+  // real line l, element k -> real or imaginary part of slot l/2 (line by
+  // line, four lines of loads in flight)
   Real *ar = reinterpret_cast<Real *>(a);
-  staged_copy<8>(
-      nl * n, [&](int e) { return src[e]; },
-      [&](int e, Real v) {
-        int const l = e / n, k = e - l * n;
-        ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = v;
-      });
-  if (nl & 1) // odd count: zero imaginary parts of the last slot
-    for (int k = threadIdx.x; k < n; k += blockDim.x)
-      ar[2 * ((np - 1) * ld + pix(k)) + 1] = Real(0);
+  for (int l0 = 0; l0 < nl; l0 += 4) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      Real v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        v[u] = (l0 + u < nl) ? src[(l0 + u) * n + k] : Real(0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        int const l = l0 + u;
+        if (l < nl || (l == nl && (nl & 1))) // odd count: zero imaginary part
+          ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = v[u];
+      }
+    }
+  }
   __syncthreads();
   C *res = fft_lines<C>(a, b, np, ld, G.plan[2], tw, false);
   int const H = n / 2 + 1;
   int const hp = G.hp;
-  for (int e = threadIdx.x; e < nl * hp; e += blockDim.x) {
-    int const l = e / hp, k = e - l * hp;
-    C v{Real(0), Real(0)};
-    if (k < H) {
-      C const z = res[(l >> 1) * ld + pix(k)];
-      C const zc = res[(l >> 1) * ld + pix((n - k) % n)];
-      if ((l & 1) == 0)
-        v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
-      else
-        v = C{Real(0.5) * (z.y + zc.y), Real(0.5) * (zc.x - z.x)};
+  for (int l = 0; l < nl; ++l)
+    for (int k = threadIdx.x; k < hp; k += blockDim.x) {
+      C v{Real(0), Real(0)};
+      if (k < H) {
+        C const z = res[(l >> 1) * ld + pix(k)];
+        C const zc = res[(l >> 1) * ld + pix(k == 0 ? 0 : n - k)];
+        if ((l & 1) == 0)
+          v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
+        else
+          v = C{Real(0.5) * (z.y + zc.y), Real(0.5) * (zc.x - z.x)};
+      }
+      cmesh[G.km_off + (line0 + l) * hp + k] = v;
     }
-    cmesh[G.km_off + (line0 + l) * hp + k] = v;
-  }
 }
 
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
@@ -400,22 +406,29 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   load_twiddles(tw, twtab, G.plan[1]);
   long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp + kz0;
   long long const hp = G.hp;
-  staged_copy<8>(
-      T * M1,
-      [&](int e) {
-        int const y = e / T, t = e - y * T;
-        return cm[rowbase + y * hp + t];
-      },
-      [&](int e, C v) {
-        int const y = e / T, t = e - y * T;
-        a[t * ld + pix(y)] = v;
-      });
+  // 16 x 16 thread mapping (tile <= 16 columns): column tq, rows yq + 16 i
+  int const tq = threadIdx.x & 15, yq = threadIdx.x >> 4;
+  bool const col = tq < T;
+  for (int y0 = yq; y0 < M1; y0 += 64) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int const y = y0 + 16 * u;
+      if (col && y < M1)
+        v[u] = cm[rowbase + y * hp + tq];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int const y = y0 + 16 * u;
+      if (col && y < M1)
+        a[tq * ld + pix(y)] = v[u];
+    }
+  }
   __syncthreads();
   C *res = fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
-  for (int e = threadIdx.x; e < T * M1; e += blockDim.x) {
-    int const y = e / T, t = e - y * T;
-    cm[rowbase + y * hp + t] = res[t * ld + pix(y)];
-  }
+  if (col)
+    for (int y = yq; y < M1; y += 16)
+      cm[rowbase + y * hp + tq] = res[tq * ld + pix(y)];
 }
 
 // ---- pass x fused with the k-space operator -----------------------------
@@ -448,16 +461,24 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   load_twiddles(tw, twtab, G.plan[0]);
   long long const stride_x = static_cast<long long>(M1) * G.hp;
   long long const base = G.km_off + static_cast<long long>(y) * G.hp + kz0;
-  staged_copy<8>(
-      T * M0,
-      [&](int e) {
-        int const x = e / T, t = e - x * T;
-        return rho_hat[base + x * stride_x + t];
-      },
-      [&](int e, C v) {
-        int const x = e / T, t = e - x * T;
-        a[t * ld + pix(x)] = v;
-      });
+  // 16 x 16 thread mapping (tile <= 16 columns): column tq, rows xq + 16 i
+  int const tq = threadIdx.x & 15, xq = threadIdx.x >> 4;
+  bool const col = tq < T;
+  for (int x0 = xq; x0 < M0; x0 += 64) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int const x = x0 + 16 * u;
+      if (col && x < M0)
+        v[u] = rho_hat[base + x * stride_x + tq];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int const x = x0 + 16 * u;
+      if (col && x < M0)
+        a[tq * ld + pix(x)] = v[u];
+    }
+  }
   __syncthreads();
   C *res = fft_lines<C>(a, b, T, ld, G.plan[0], tw, false);
   C *fb = (res == a) ? b : a; // field lines go to the free buffer
@@ -469,9 +490,9 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   // d_op (Nyquist zeroed) integer shift of index i in a mesh of size m
   auto dop = [](int i, int m) { return (i == m / 2) ? 0 : (i < m / 2 ? i : i - m); };
   int const kyd = dop(y, M1);
-  for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
-    // t fastest: the influence-function reads are T-contiguous rows
-    int const x = e / T, t = e - x * T;
+  for (int x = xq; col && x < M0; x += 16) {
+    // t fastest across lanes: the influence-function reads are T-contiguous
+    int const t = tq;
     int const kz = kz0 + t;
     C const rh = res[t * ld + pix(x)];
     Real const g = ginf[base + x * stride_x + t];
@@ -527,8 +548,8 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   for (int d = 0; d < 3; ++d) {
     __syncthreads(); // phi complete / previous component stored
     Real const wd = static_cast<Real>(wv[d]);
-    for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
-      int const t = e / M0, x = e - t * M0;
+    for (int x = xq; col && x < M0; x += 16) {
+      int const t = tq;
       int const kd = (d == 0) ? dop(x, M0) : (d == 1 ? kvec_y : dop(kz0 + t, M2));
       Real const k = static_cast<Real>(kd) * wd;
       C const phi = res[t * ld + pix(x)];
@@ -536,10 +557,9 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     }
     __syncthreads();
     C *fres = fft_lines<C>(fb, c, T, ld, G.plan[0], tw, true);
-    for (int e = threadIdx.x; e < T * M0; e += blockDim.x) {
-      int const x = e / T, t = e - x * T;
-      field0[field_stride * d + base + x * stride_x + t] = fres[t * ld + pix(x)];
-    }
+    if (col)
+      for (int x = xq; x < M0; x += 16)
+        field0[field_stride * d + base + x * stride_x + tq] = fres[tq * ld + pix(x)];
   }
 }
 
@@ -584,17 +604,24 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   // stage the half rows (H entries of each of 3 nl rows; field d, line l at
   // b[(d * nl + l) * hl]), then build the packed lines in a
   const C *fsrc = field0 + G.km_off + line0 * G.hp;
-  staged_copy<8>(
-      3 * nl * H,
-      [&](int e) {
-        int const dl = e / H, k = e - dl * H;
-        int const d = dl / nl, l = dl - d * nl;
-        return fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
-      },
-      [&](int e, C v) {
-        int const dl = e / H, k = e - dl * H;
-        b[dl * hl + k] = v;
-      });
+  // row dl = d * nl + l, four rows of loads in flight
+  for (int dl0 = 0; dl0 < 3 * nl; dl0 += 4) {
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        int const dl = dl0 + u;
+        if (dl < 3 * nl) {
+          int const d = dl / nl, l = dl - d * nl;
+          v[u] = fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (dl0 + u < 3 * nl)
+          b[(dl0 + u) * hl + k] = v[u];
+    }
+  }
   __syncthreads();
   auto herm = [&](int d, int l, int k) -> C {
     const C *row = b + (d * nl + l) * hl;
@@ -606,36 +633,36 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     }
     return cconj(row[n - k]);
   };
-  for (int e = threadIdx.x; e < nc * n; e += blockDim.x) {
-    int const j = e / n, k = e - j * n;
-    C X, Y;
-    if (j < nl) {
-      X = herm(0, j, k);
-      Y = herm(1, j, k);
-    } else {
-      int const l0 = 2 * (j - nl);
-      X = herm(2, l0, k);
-      Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
+  for (int j = 0; j < nc; ++j)
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      C X, Y;
+      if (j < nl) {
+        X = herm(0, j, k);
+        Y = herm(1, j, k);
+      } else {
+        int const l0 = 2 * (j - nl);
+        X = herm(2, l0, k);
+        Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
+      }
+      a[j * ld + pix(k)] = C{X.x - Y.y, X.y + Y.x};
     }
-    a[j * ld + pix(k)] = C{X.x - Y.y, X.y + Y.x};
-  }
   __syncthreads();
   C *res = fft_lines<C>(a, b, nc, ld, G.plan[2], tw, true);
   // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
   // interpolation gathers one 16-byte (FP32) record per stencil point
   using R4 = typename Real4Of<Real>::type;
   R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    int const l = e / n, k = e - l * n;
-    C const xy = res[l * ld + pix(k)];
-    C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
-    R4 v;
-    v.x = xy.x;
-    v.y = xy.y;
-    v.z = (l & 1) ? zz.y : zz.x;
-    v.w = Real(0);
-    out[e] = v;
-  }
+  for (int l = 0; l < nl; ++l)
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      C const xy = res[l * ld + pix(k)];
+      C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
+      R4 v;
+      v.x = xy.x;
+      v.y = xy.y;
+      v.z = (l & 1) ? zz.y : zz.x;
+      v.w = Real(0);
+      out[l * n + k] = v;
+    }
 }
 
 } // namespace p3mx
