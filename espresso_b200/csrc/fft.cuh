@@ -34,6 +34,22 @@ __host__ __device__ inline int pix(int i) { return i + (i >> 4); }
 // that consecutive lines start in different banks.
 __host__ __device__ inline int line_ld(int n) { return (n + ((n - 1) >> 4)) | 1; }
 
+// body(l, k) for l < nl, k < n over the block: lines shorter than the block
+// run several at a time (one division per thread, not per element).
+template <typename F> __device__ inline void for_lines(int nl, int n, F const &body) {
+  int const per = blockDim.x / n;
+  if (per > 0) {
+    int const lq = threadIdx.x / n, k = threadIdx.x - lq * n;
+    if (lq < per)
+      for (int l = lq; l < nl; l += per)
+        body(l, k);
+  } else {
+    for (int l = 0; l < nl; ++l)
+      for (int k = threadIdx.x; k < n; k += blockDim.x)
+        body(l, k);
+  }
+}
+
 // Copy the twiddle table exp(-2 pi i k / n), k < n, of one axis to shared
 // memory (caller synchronises).
 template <typename C>
@@ -329,7 +345,7 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
 // bk.b real lines per block (an odd last line is paired with zeros).
 // Shared memory: 2 x ceil(bk.b/2) staged lines of line_ld(n), twiddles (n).
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
 k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
             const Real *__restrict__ rmesh, typename CplxOf<Real>::type *__restrict__ cmesh,
             const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -350,43 +366,32 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   // real line l, element k -> real or imaginary part of slot l/2 (line by
   // line, four lines of loads in flight)
   Real *ar = reinterpret_cast<Real *>(a);
-  for (int l0 = 0; l0 < nl; l0 += 4) {
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      Real v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        v[u] = (l0 + u < nl) ? src[(l0 + u) * n + k] : Real(0);
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        int const l = l0 + u;
-        if (l < nl || (l == nl && (nl & 1))) // odd count: zero imaginary part
-          ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = v[u];
-      }
-    }
-  }
+  // odd count: the last slot's imaginary part is line nl, all zeros
+  for_lines(nl + (nl & 1), n, [&](int l, int k) {
+    ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = (l < nl) ? src[l * n + k] : Real(0);
+  });
   __syncthreads();
   C *res = fft_lines<C>(a, b, np, ld, G.plan[2], tw, false);
   int const H = n / 2 + 1;
   int const hp = G.hp;
-  for (int l = 0; l < nl; ++l)
-    for (int k = threadIdx.x; k < hp; k += blockDim.x) {
-      C v{Real(0), Real(0)};
-      if (k < H) {
-        C const z = res[(l >> 1) * ld + pix(k)];
-        C const zc = res[(l >> 1) * ld + pix(k == 0 ? 0 : n - k)];
-        if ((l & 1) == 0)
-          v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
-        else
-          v = C{Real(0.5) * (z.y + zc.y), Real(0.5) * (zc.x - z.x)};
-      }
-      cmesh[G.km_off + (line0 + l) * hp + k] = v;
+  for_lines(nl, hp, [&](int l, int k) {
+    C v{Real(0), Real(0)};
+    if (k < H) {
+      C const z = res[(l >> 1) * ld + pix(k)];
+      C const zc = res[(l >> 1) * ld + pix(k == 0 ? 0 : n - k)];
+      if ((l & 1) == 0)
+        v = C{Real(0.5) * (z.x + zc.x), Real(0.5) * (z.y - zc.y)};
+      else
+        v = C{Real(0.5) * (z.y + zc.y), Real(0.5) * (zc.x - z.x)};
     }
+    cmesh[G.km_off + (line0 + l) * hp + k] = v;
+  });
 }
 
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
 // Shared memory: 2 x tile staged lines of line_ld(M1), twiddles (M1).
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
 k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
         typename CplxOf<Real>::type *__restrict__ c0, long long field_stride, int tile,
         bool inv, const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -580,7 +585,7 @@ __host__ __device__ inline int z_inv_b_size(int nl, int n) {
 // Shared memory: 2 x (nl + ceil(nl/2)) staged lines of line_ld(n),
 // twiddles (n).
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
 k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
              const typename CplxOf<Real>::type *__restrict__ field0, long long field_stride,
              Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -604,24 +609,11 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   // stage the half rows (H entries of each of 3 nl rows; field d, line l at
   // b[(d * nl + l) * hl]), then build the packed lines in a
   const C *fsrc = field0 + G.km_off + line0 * G.hp;
-  // row dl = d * nl + l, four rows of loads in flight
-  for (int dl0 = 0; dl0 < 3 * nl; dl0 += 4) {
-    for (int k = threadIdx.x; k < H; k += blockDim.x) {
-      C v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        int const dl = dl0 + u;
-        if (dl < 3 * nl) {
-          int const d = dl / nl, l = dl - d * nl;
-          v[u] = fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (dl0 + u < 3 * nl)
-          b[(dl0 + u) * hl + k] = v[u];
-    }
-  }
+  // row dl = d * nl + l of the three fields
+  for_lines(3 * nl, H, [&](int dl, int k) {
+    int const d = (dl >= 2 * nl) ? 2 : (dl >= nl ? 1 : 0), l = dl - d * nl;
+    b[dl * hl + k] = fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
+  });
   __syncthreads();
   auto herm = [&](int d, int l, int k) -> C {
     const C *row = b + (d * nl + l) * hl;
@@ -633,36 +625,34 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     }
     return cconj(row[n - k]);
   };
-  for (int j = 0; j < nc; ++j)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      C X, Y;
-      if (j < nl) {
-        X = herm(0, j, k);
-        Y = herm(1, j, k);
-      } else {
-        int const l0 = 2 * (j - nl);
-        X = herm(2, l0, k);
-        Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
-      }
-      a[j * ld + pix(k)] = C{X.x - Y.y, X.y + Y.x};
+  for_lines(nc, n, [&](int j, int k) {
+    C X, Y;
+    if (j < nl) {
+      X = herm(0, j, k);
+      Y = herm(1, j, k);
+    } else {
+      int const l0 = 2 * (j - nl);
+      X = herm(2, l0, k);
+      Y = (l0 + 1 < nl) ? herm(2, l0 + 1, k) : C{Real(0), Real(0)};
     }
+    a[j * ld + pix(k)] = C{X.x - Y.y, X.y + Y.x};
+  });
   __syncthreads();
   C *res = fft_lines<C>(a, b, nc, ld, G.plan[2], tw, true);
   // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
   // interpolation gathers one 16-byte (FP32) record per stencil point
   using R4 = typename Real4Of<Real>::type;
   R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
-  for (int l = 0; l < nl; ++l)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      C const xy = res[l * ld + pix(k)];
-      C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
-      R4 v;
-      v.x = xy.x;
-      v.y = xy.y;
-      v.z = (l & 1) ? zz.y : zz.x;
-      v.w = Real(0);
-      out[l * n + k] = v;
-    }
+  for_lines(nl, n, [&](int l, int k) {
+    C const xy = res[l * ld + pix(k)];
+    C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
+    R4 v;
+    v.x = xy.x;
+    v.y = xy.y;
+    v.z = (l & 1) ? zz.y : zz.x;
+    v.w = Real(0);
+    out[l * n + k] = v;
+  });
 }
 
 } // namespace p3mx
