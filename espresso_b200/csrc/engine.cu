@@ -183,7 +183,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     }
     G.hp = ((c.mesh[2] / 2 + 1) + 3) / 4 * 4;
     // assignment bricks: edge >= cao-1 so that same-colour tiles never overlap
-    G.brick = (c.cao <= 5) ? 4 : 8;
+    G.brick = (c.cao <= 5) ? 4 : 8; // brick_edge<cao>() of the kernels
     G.nbx = (c.mesh[0] + G.brick - 1) / G.brick;
     G.nby = (c.mesh[1] + G.brick - 1) / G.brick;
     G.nbz = (c.mesh[2] + G.brick - 1) / G.brick;

@@ -146,15 +146,10 @@ template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v
   c += err;
 }
 
-// Corner (cx, cy, cz) of a brick-local key.
-__device__ inline void corner_of(RepGeom const &G, int loc, int &cx, int &cy, int &cz) {
-  int const B = G.brick, B3 = B * B * B;
-  int const brick = loc / B3, l = loc - brick * B3;
-  int const bz = brick % G.nbz, by = (brick / G.nbz) % G.nby, bx = brick / (G.nbz * G.nby);
-  cx = bx * B + l / (B * B);
-  cy = by * B + (l / B) % B;
-  cz = bz * B + l % B;
-}
+// Brick edge (mesh points) of the charge assignment for order P: at least
+// P - 1 so that the tiles of one colour never overlap (the engine sets
+// RepGeom::brick by the same rule).
+template <int P> __host__ __device__ constexpr int brick_edge() { return (P <= 5) ? 4 : 8; }
 
 // Warps per brick (block) of the charge assignment, and particles whose
 // weight records are staged in shared memory at a time.
@@ -235,7 +230,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
-  int const B = G.brick, B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
   const int *st = start + G.brk_off;
   int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)
@@ -460,7 +455,7 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
-  int const B = G.brick, B3 = B * B * B, Ed = B + P - 1, E2 = Ed * Ed;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B, Ed = B + P - 1, E2 = Ed * Ed;
   const int *st = start + G.brk_off;
   int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)
