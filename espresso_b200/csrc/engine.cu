@@ -730,7 +730,7 @@ void Engine::build_lists(cudaStream_t st) {
     bool grown = false;
     for (int r = 0; r < R; ++r)
       if (ov[r] > 0) {
-        m_cap[r] = ov[r] + ov[r] / 4 + 16;
+        m_cap[r] = (ov[r] + ov[r] / 4 + 16 + 7) / 8 * 8; // whole groups of 8
         grown = true;
       }
     if (!grown)
@@ -948,7 +948,8 @@ void Engine::set_list_capacity(double margin) {
     double const rc = G.max_cut + G.skin;
     double const est = margin * 4.18879 * rc * rc * rc * (G.np / G.V) + 48.0;
     int const cap = std::max(
-        m_cap[r], static_cast<int>(std::min(est, double(std::max<long long>(G.np, 1)))) + 1);
+        m_cap[r],
+        (static_cast<int>(std::min(est, double(std::max<long long>(G.np, 1)))) + 1 + 7) / 8 * 8);
     changed = changed || (cap != m_cap[r]);
     m_cap[r] = cap;
   }
@@ -962,7 +963,7 @@ void Engine::layout_lists(cudaStream_t st) {
   for (int r = 0; r < n_rep(); ++r) {
     m_geom[r].nb_off = off;
     m_geom[r].max_nb = m_cap[r];
-    // warp tiles of 32 particles (nb_base)
+    // warp tiles of 32 particles, capacity in groups of 8 (nb_base)
     off += static_cast<long long>(m_cap[r]) * ((m_geom[r].np + 31) / 32 * 32);
   }
   m_nb.ensure(static_cast<size_t>(std::max<long long>(off, 1)) * sizeof(int));
@@ -1012,8 +1013,8 @@ std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
   for (auto const &G : m_geom)
     for (long long a = G.p0; a < G.p0 + G.np; ++a)
       for (int k = 0; k < cnt[a]; ++k) {
-        unsigned const ent = static_cast<unsigned>(
-            nbh[nb_base(G.nb_off, G.max_nb, a - G.p0) + (static_cast<long long>(k) << 5)]);
+        unsigned const ent =
+            static_cast<unsigned>(nbh[nb_entry(nb_base(G.nb_off, G.max_nb, a - G.p0), k)]);
         int const b = static_cast<int>(G.p0 + (ent & kNbIndexMask));
         int const i = perm[a], j = perm[b];
         if (i < j) {

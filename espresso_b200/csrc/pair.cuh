@@ -109,15 +109,27 @@ __device__ inline double mi_d(double dx, double L, double Li) {
   return dx;
 }
 
-// Verlet list layout, warp-tiled: the lists of 32 consecutive particles of a
-// replica (one warp of the pair kernel) form one contiguous block, neighbour
-// slot k of local particle la at nb_off + ((la/32) * max_nb + k) * 32 + la%32,
-// so a warp streams through its own block.  An entry packs the partner's
-// index inside the replica (26 bits) and its cell offset code (cell_offset).
+// Verlet list layout: per warp tile of 32 consecutive particles of a replica,
+// each particle's entries in groups of 8 (one 32-byte sector), the groups of
+// the 32 particles interleaved: entry k of local particle la at
+//   nb_off + ((la/32) * (cap/8) + k/8) * 256 + (la%32) * 8 + k%8
+// (cap, the per-replica capacity, a multiple of 8).  The build writes whole
+// groups with vector stores and the pair kernels read whole groups with
+// vector loads.  An entry packs the partner's index inside the replica
+// (26 bits) and its cell offset code (cell_offset).
 constexpr int kNbIndexBits = 26;
 constexpr unsigned kNbIndexMask = (1u << kNbIndexBits) - 1u;
-__host__ __device__ inline long long nb_base(long long nb_off, int max_nb, long long la) {
-  return nb_off + (((la >> 5) * max_nb) << 5) + (la & 31);
+// First entry (group 0) of local particle la; group g at + g * 256.
+__host__ __device__ inline long long nb_base(long long nb_off, int cap, long long la) {
+  return nb_off + (((la >> 5) * (cap >> 3)) << 8) + ((la & 31) << 3);
+}
+__host__ __device__ inline long long nb_entry(long long base, int k) {
+  return base + (static_cast<long long>(k >> 3) << 8) + (k & 7);
+}
+
+__device__ inline void store_group(int *p, const int *g) {
+  reinterpret_cast<int4 *>(p)[0] = make_int4(g[0], g[1], g[2], g[3]);
+  reinterpret_cast<int4 *>(p)[1] = make_int4(g[4], g[5], g[6], g[7]);
 }
 
 // Verlet list (full, both directions) of every cell-sorted particle a:
@@ -143,6 +155,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
   RepGeom const &G = reps[rep];
   int const max_nb = G.max_nb;
   int *nbp = nb + nb_base(G.nb_off, max_nb, a - G.p0);
+  int gbuf[8] = {0, 0, 0, 0, 0, 0, 0, 0}; // the group being filled
   double4 const pa = spq[a];
   double const cs[3] = {G.box[0] / G.cg[0], G.box[1] / G.cg[1], G.box[2] / G.cg[2]};
   double const ics[3] = {G.cg[0] * G.box_i[0], G.cg[1] * G.box_i[1], G.cg[2] * G.box_i[2]};
@@ -180,6 +193,16 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
         int x = c0 + dx;
         x = (x < 0) ? x + G.cg[0] : (x >= G.cg[0] ? x - G.cg[0] : x);
         int const cell = static_cast<int>(G.cell_off) + x + G.cg[0] * (y + G.cg[1] * z);
+        if (!small_grid) {
+          // skip a neighbour cell lying wholly beyond the list range: distance
+          // from the particle (cell-relative offset) to the cell's box
+          float const ax = (dx == 0) ? 0.f : (dx > 0 ? csf[0] - pfa.x : pfa.x);
+          float const ay = (dy == 0) ? 0.f : (dy > 0 ? csf[1] - pfa.y : pfa.y);
+          float const az = (dz == 0) ? 0.f : (dz > 0 ? csf[2] - pfa.z : pfa.z);
+          float const bx = fmaxf(ax, 0.f), by = fmaxf(ay, 0.f), bz = fmaxf(az, 0.f);
+          if (bx * bx + by * by + bz * bz > emax2_pre)
+            continue;
+        }
         float const shx = -dx * csf[0], shy = -dy * csf[1], shz = -dz * csf[2];
         // exact (FP64 minimum-image) test and store of one candidate
         auto consider = [&](int b) {
@@ -219,9 +242,15 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
                     }
                 }
                 int const code = (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1);
-                nbp[static_cast<long long>(count) << 5] =
-                    static_cast<int>(static_cast<unsigned>(b - G.p0) |
-                                     (static_cast<unsigned>(code) << kNbIndexBits));
+                int const ent = static_cast<int>(static_cast<unsigned>(b - G.p0) |
+                                                 (static_cast<unsigned>(code) << kNbIndexBits));
+                int const slot = count & 7;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                  if (u == slot)
+                    gbuf[u] = ent;
+                if (slot == 7)
+                  store_group(nbp + (static_cast<long long>(count >> 3) << 8), gbuf);
               }
               ++count;
             }
@@ -258,7 +287,10 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
       }
     }
   }
-  nb_cnt[a] = min(count, max_nb);
+  int const stored = min(count, max_nb);
+  if (stored & 7) // last partial group (entries beyond the count are never read)
+    store_group(nbp + (static_cast<long long>(stored >> 3) << 8), gbuf);
+  nb_cnt[a] = stored;
   if (count > max_nb)
     atomicMax(&overflow[rep], count);
 }
@@ -402,75 +434,86 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
     int const cnt = nb_cnt[a];
     const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
     long long const base0 = G.p0;
-    unsigned e_next = (cnt > 0) ? static_cast<unsigned>(nbp[0]) : 13u << kNbIndexBits;
-    float4 p_next = (cnt > 0) ? spf[base0 + (e_next & kNbIndexMask)] : pa;
-    for (int k = 0; k < cnt; ++k) {
-      unsigned const e = e_next;
-      int const b = static_cast<int>(base0 + (e & kNbIndexMask));
-      int const code = static_cast<int>(e >> kNbIndexBits);
-      float4 const pb = p_next;
-      if (k + 1 < cnt) {
-        e_next = static_cast<unsigned>(nbp[static_cast<long long>(k + 1) << 5]);
-        p_next = spf[base0 + (e_next & kNbIndexMask)];
-      }
-      float4 const sh = shift[code];
-      Real const d0 = (pa.x - pb.x) + sh.x;
-      Real const d1 = (pa.y - pb.y) + sh.y;
-      Real const d2v = (pa.z - pb.z) + sh.z;
-      Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
-      Real const inv_d = rsqrt_r(dist2);
-      Real const dist = dist2 * inv_d;
-      Real fc = Real(0), ec = Real(0);
-      Real const qb = pb.w;
-      if (qb != Real(0) && pref_qa != Real(0) && dist < r_cut && dist > Real(0)) {
-        Real const adist = alpha * dist;
-        Real const ex = exp_r(-adist * adist);
-        Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
-        Real const asp =
-            t * (Real(0.254829592) +
-                 t * (Real(-0.284496736) +
-                      t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
-        Real const erfc_part_ri = asp * inv_d;
-        Real const pq = pref_qa * qb;
-        fc = pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d));
-        if constexpr (EV)
-          ec = pq * erfc_part_ri * ex;
-      }
-      Real fn = Real(0), en = Real(0);
-      if (one_type) {
-        if (p0.active)
-          lj_wca(p0, dist, inv_d, fn, en);
-      } else {
-        PairR<Real> const p(ia[ta * ntypes + stype[b]]);
-        if (p.active)
-          lj_wca(p, dist, inv_d, fn, en);
-      }
-      Real const ft = fc + fn;
-      sx += ft * d0;
-      sy += ft * d1;
-      sz += ft * d2v;
-      if ((k & 7) == 7) {
-        fx += static_cast<double>(sx);
-        fy += static_cast<double>(sy);
-        fz += static_cast<double>(sz);
-        sx = sy = sz = 0.f;
-      }
-      if constexpr (EV) {
-        double const dd[3] = {d0, d1, d2v};
-        ev[0] += 0.5 * double(ec);
-        ev[1] += 0.5 * double(en);
+    for (int k0 = 0; k0 < cnt; k0 += 8) {
+      // one group of 8 entries: two 16-byte loads
+      const int4 *gp = reinterpret_cast<const int4 *>(nbp + (static_cast<long long>(k0 >> 3) << 8));
+      int4 const g0 = gp[0], g1 = gp[1];
+      unsigned const ent[8] = {static_cast<unsigned>(g0.x), static_cast<unsigned>(g0.y),
+                               static_cast<unsigned>(g0.z), static_cast<unsigned>(g0.w),
+                               static_cast<unsigned>(g1.x), static_cast<unsigned>(g1.y),
+                               static_cast<unsigned>(g1.z), static_cast<unsigned>(g1.w)};
+      int const kn = min(8, cnt - k0);
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+      for (int h = 0; h < 8; h += 4) {
+        // the partners' positions, four gathers in flight
+        float4 pbv[4];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
-            ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
+        for (int u = 0; u < 4; ++u)
+          pbv[u] = (h + u < kn) ? spf[base0 + (ent[h + u] & kNbIndexMask)] : pa;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (h + u >= kn)
+            continue;
+          unsigned const e = ent[h + u];
+          int const b = static_cast<int>(base0 + (e & kNbIndexMask));
+          int const code = static_cast<int>(e >> kNbIndexBits);
+          float4 const pb = pbv[u];
+          float4 const sh = shift[code];
+          Real const d0 = (pa.x - pb.x) + sh.x;
+          Real const d1 = (pa.y - pb.y) + sh.y;
+          Real const d2v = (pa.z - pb.z) + sh.z;
+          Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
+          Real const inv_d = rsqrt_r(dist2);
+          Real const dist = dist2 * inv_d;
+          Real fc = Real(0), ec = Real(0);
+          Real const qb = pb.w;
+          if (qb != Real(0) && pref_qa != Real(0) && dist < r_cut && dist > Real(0)) {
+            Real const adist = alpha * dist;
+            Real const ex = exp_r(-adist * adist);
+            Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
+            Real const asp =
+                t * (Real(0.254829592) +
+                     t * (Real(-0.284496736) +
+                          t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
+            Real const erfc_part_ri = asp * inv_d;
+            Real const pq = pref_qa * qb;
+            fc = pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d));
+            if constexpr (EV)
+              ec = pq * erfc_part_ri * ex;
           }
+          Real fn = Real(0), en = Real(0);
+          if (one_type) {
+            if (p0.active)
+              lj_wca(p0, dist, inv_d, fn, en);
+          } else {
+            PairR<Real> const p(ia[ta * ntypes + stype[b]]);
+            if (p.active)
+              lj_wca(p, dist, inv_d, fn, en);
+          }
+          Real const ft = fc + fn;
+          sx += ft * d0;
+          sy += ft * d1;
+          sz += ft * d2v;
+          if constexpr (EV) {
+            double const dd[3] = {d0, d1, d2v};
+            ev[0] += 0.5 * double(ec);
+            ev[1] += 0.5 * double(en);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
+                ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
+              }
+          }
+        }
       }
+      // FP32 sums of this group into the FP64 accumulators
+      fx += static_cast<double>(sx);
+      fy += static_cast<double>(sy);
+      fz += static_cast<double>(sz);
+      sx = sy = sz = 0.f;
     }
-    fx += static_cast<double>(sx);
-    fy += static_cast<double>(sy);
-    fz += static_cast<double>(sz);
     int const i = perm[a];
     if (overwrite) {
       f[3 * i + 0] = fx;
@@ -544,9 +587,8 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
       int const b = b_next;
       double4 const pb = p_next;
       if (k + 1 < cnt) {
-        b_next = base0 + static_cast<int>(
-                             static_cast<unsigned>(nbp[static_cast<long long>(k + 1) << 5]) &
-                             kNbIndexMask);
+        b_next = base0 + static_cast<int>(static_cast<unsigned>(nbp[nb_entry(0, k + 1)]) &
+                                          kNbIndexMask);
         p_next = spq[b_next];
       }
       // geometry in FP64 (two conversions per pair instead of four)
