@@ -127,9 +127,10 @@ __host__ __device__ inline long long nb_entry(long long base, int k) {
   return base + (static_cast<long long>(k >> 3) << 8) + (k & 7);
 }
 
+// Copy one group of 8 entries (32 bytes, 16-byte aligned on both sides).
 __device__ inline void store_group(int *p, const int *g) {
-  reinterpret_cast<int4 *>(p)[0] = make_int4(g[0], g[1], g[2], g[3]);
-  reinterpret_cast<int4 *>(p)[1] = make_int4(g[4], g[5], g[6], g[7]);
+  reinterpret_cast<int4 *>(p)[0] = reinterpret_cast<const int4 *>(g)[0];
+  reinterpret_cast<int4 *>(p)[1] = reinterpret_cast<const int4 *>(g)[1];
 }
 
 // Verlet list (full, both directions) of every cell-sorted particle a:
@@ -139,7 +140,7 @@ __device__ inline void store_group(int *p, const int *g) {
 // d^2 <= (ia_cut+skin)^2).  Stored in the warp-tiled layout above
 // (per-replica capacity G.max_nb); a replica whose capacity is exceeded
 // reports its largest count in overflow[replica].
-__global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
+__global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
                                const double4 *__restrict__ spq, const float4 *__restrict__ spf,
                                const int *__restrict__ stype,
                                const int *__restrict__ scell, const int *__restrict__ cstart,
@@ -148,6 +149,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
                                int *__restrict__ overflow, const int *__restrict__ cond) {
   if (cond && !*cond)
     return;
+  __shared__ __align__(16) int s_group[256 * 8];
   long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (a >= n)
     return;
@@ -155,7 +157,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
   RepGeom const &G = reps[rep];
   int const max_nb = G.max_nb;
   int *nbp = nb + nb_base(G.nb_off, max_nb, a - G.p0);
-  int gbuf[8] = {0, 0, 0, 0, 0, 0, 0, 0}; // the group being filled
+  int *gbuf = s_group + threadIdx.x * 8; // the group being filled (shared memory)
   double4 const pa = spq[a];
   double const cs[3] = {G.box[0] / G.cg[0], G.box[1] / G.cg[1], G.box[2] / G.cg[2]};
   double const ics[3] = {G.cg[0] * G.box_i[0], G.cg[1] * G.box_i[1], G.cg[2] * G.box_i[2]};
@@ -245,10 +247,7 @@ __global__ void k_verlet_build(const RepGeom *__restrict__ reps, const int *__re
                 int const ent = static_cast<int>(static_cast<unsigned>(b - G.p0) |
                                                  (static_cast<unsigned>(code) << kNbIndexBits));
                 int const slot = count & 7;
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                  if (u == slot)
-                    gbuf[u] = ent;
+                gbuf[slot] = ent;
                 if (slot == 7)
                   store_group(nbp + (static_cast<long long>(count >> 3) << 8), gbuf);
               }
