@@ -468,6 +468,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_scell.ensure(n * sizeof(int));
   m_nb_cnt.ensure(n * sizeof(int));
   m_overflow.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
+  m_rflag.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_flag.ensure(sizeof(int));
   if (m_kerr.p == nullptr) {
     m_kerr.ensure(sizeof(int));
@@ -709,7 +710,8 @@ void Engine::build_lists(cudaStream_t st) {
   int const nb = ceil_div(m_n, 256);
   P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr); ++m_launches;
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr,
+                                 nullptr); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
@@ -723,7 +725,7 @@ void Engine::build_lists(cudaStream_t st) {
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                        m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
-                                       m_overflow.as<int>(), nullptr); ++m_launches;
+                                       m_overflow.as<int>(), nullptr, nullptr); ++m_launches;
     std::vector<int> ov(R);
     P3MX_CUDA(cudaMemcpyAsync(ov.data(), m_overflow.p, R * sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
@@ -778,7 +780,7 @@ void Engine::prepare_short_range(cudaStream_t st, bool need_spq) {
   if (!rebuild) {
     P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
     k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                             m_n, m_flag.as<int>()); ++m_launches;
+                                             m_n, m_flag.as<int>(), nullptr); ++m_launches;
     int flag = 0;
     P3MX_CUDA(cudaMemcpyAsync(&flag, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
@@ -898,21 +900,27 @@ void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t s
 }
 
 // Graph-capturable short-range step: the displacement check raises a device
-// flag, and the whole rebuild chain (cell binning, counting sort, gather,
-// Verlet build, reference positions) runs only when it is set, so no host
-// decision is needed between steps.
+// flag (and one per replica), and the rebuild chain (cell binning, counting
+// sort, gather, Verlet build, reference positions) runs only when it is set,
+// so no host decision is needed between steps.  Only the replicas whose
+// particles moved more than skin/2 rebuild: the others keep their cell keys,
+// hence their sorted order, lists and reference positions.
 void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   if (m_n == 0)
     return;
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
+  int const R = n_rep();
   int *flag = m_flag.as<int>();
+  int *rflag = m_rflag.as<int>();
   k_fill_int<<<1, 32, 0, st>>>(flag, 0, 1, nullptr); ++m_launches;
+  k_fill_int<<<ceil_div(R, 256), 256, 0, st>>>(rflag, 0, R, nullptr); ++m_launches;
   k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                           m_n, flag); ++m_launches;
+                                           m_n, flag, rflag); ++m_launches;
   k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag); ++m_launches;
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag); ++m_launches;
+                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag,
+                                 rflag); ++m_launches;
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st, flag);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
@@ -921,8 +929,9 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
-                                     m_overflow.as<int>(), flag); ++m_launches;
-  k_copy_f64<<<ceil_div(3 * m_n, 256), 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), 3 * m_n, flag); ++m_launches;
+                                     m_overflow.as<int>(), flag, rflag); ++m_launches;
+  k_copy_pos_ref<<<nb, 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), m_rep_of.as<int>(), rflag, m_n,
+                                     flag); ++m_launches;
   refresh_sorted_positions(st, !m_fp32);
   if (m_fp32)
     launch_pair<float>(f, overwrite, false, st);
@@ -991,7 +1000,7 @@ std::vector<int> Engine::cell_index_ghost(cudaStream_t st) {
   k_cell_bin<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(),
                                                  d_q(), m_n, m_ckey.as<int>(), m_cslot.as<int>(),
                                                  m_ccnt.as<int>(), m_pq.as<double4>(), gi.as<int>(),
-                                                 nullptr); ++m_launches;
+                                                 nullptr, nullptr); ++m_launches;
   P3MX_CUDA(cudaMemcpyAsync(out.data(), gi.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));
   m_lists_valid = false;

@@ -57,7 +57,8 @@ __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restri
                            const double *__restrict__ pos, const double *__restrict__ q,
                            long long n, int *__restrict__ key, int *__restrict__ slot,
                            int *__restrict__ cnt, double4 *__restrict__ pq,
-                           int *__restrict__ ghost_index, const int *__restrict__ cond) {
+                           int *__restrict__ ghost_index, const int *__restrict__ cond,
+                           const int *__restrict__ rflag) {
   if (cond && !*cond)
     return;
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -70,8 +71,14 @@ __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restri
     xf[d] = fold_coord(pos[3 * i + d], G.box[d]);
   int c[3];
   cell_coords(G, xf, c);
-  int const k = static_cast<int>(G.cell_off) + c[0] + G.cg[0] * (c[1] + G.cg[1] * c[2]);
-  key[i] = k;
+  int k;
+  if (rflag && !rflag[rep_of[i]]) {
+    // replica keeps its lists: same cells, hence the same sorted order
+    k = key[i];
+  } else {
+    k = static_cast<int>(G.cell_off) + c[0] + G.cg[0] * (c[1] + G.cg[1] * c[2]);
+    key[i] = k;
+  }
   slot[i] = atomicAdd(&cnt[k], 1);
   pq[i] = make_double4(xf[0], xf[1], xf[2], q[i]);
   if (ghost_index) {
@@ -146,7 +153,8 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
                                const int *__restrict__ scell, const int *__restrict__ cstart,
                                const PairIA *__restrict__ ia, int ntypes, long long n,
                                int *__restrict__ nb, int *__restrict__ nb_cnt,
-                               int *__restrict__ overflow, const int *__restrict__ cond) {
+                               int *__restrict__ overflow, const int *__restrict__ cond,
+                               const int *__restrict__ rflag) {
   if (cond && !*cond)
     return;
   __shared__ __align__(16) int s_group[256 * 8];
@@ -154,6 +162,8 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
   if (a >= n)
     return;
   int const rep = rep_of_sorted[a];
+  if (rflag && !rflag[rep])
+    return; // this replica keeps its list
   RepGeom const &G = reps[rep];
   int const max_nb = G.max_nb;
   int *nbp = nb + nb_base(G.nb_off, max_nb, a - G.p0);
@@ -675,11 +685,13 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
 // CellStructure.hpp:393-401).
 __global__ void k_displacement_check(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                                      const double *__restrict__ pos, const double *__restrict__ pos_ref,
-                                     long long n, int *__restrict__ flag) {
+                                     long long n, int *__restrict__ flag,
+                                     int *__restrict__ rflag) {
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n)
     return;
-  RepGeom const &G = reps[rep_of[i]];
+  int const r = rep_of[i];
+  RepGeom const &G = reps[r];
   double d2 = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -687,8 +699,25 @@ __global__ void k_displacement_check(const RepGeom *__restrict__ reps, const int
     d2 += dx * dx;
   }
   double const lim = 0.5 * G.skin;
-  if (d2 > lim * lim)
+  if (d2 > lim * lim) {
     atomicOr(flag, 1);
+    if (rflag) // per-replica decision: only this replica rebuilds
+      atomicOr(&rflag[r], 1);
+  }
+}
+
+// Reference positions of the replicas that rebuilt (all when rflag is null).
+__global__ void k_copy_pos_ref(double *__restrict__ pos_ref, const double *__restrict__ pos,
+                               const int *__restrict__ rep_of, const int *__restrict__ rflag,
+                               long long n, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n || (rflag && !rflag[rep_of[i]]))
+    return;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    pos_ref[3 * i + d] = pos[3 * i + d];
 }
 
 } // namespace p3mx

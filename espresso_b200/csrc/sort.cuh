@@ -237,21 +237,4 @@ inline void exclusive_scan(const int *in, int *out, int *tile_buf, long long n,
   k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, tile_buf, n, cond);
 }
 
-// Conditional fill / copy helpers for graph-captured paths.
-__global__ void k_fill_int(int *__restrict__ p, int v, long long n, const int *__restrict__ cond) {
-  if (cond && !*cond)
-    return;
-  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<long long>(gridDim.x) * blockDim.x)
-    p[i] = v;
-}
-__global__ void k_copy_f64(double *__restrict__ dst, const double *__restrict__ src, long long n,
-                           const int *__restrict__ cond) {
-  if (cond && !*cond)
-    return;
-  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<long long>(gridDim.x) * blockDim.x)
-    dst[i] = src[i];
-}
-
 } // namespace p3mx
