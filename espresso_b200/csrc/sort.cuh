@@ -226,6 +226,15 @@ k_fix_big_buckets(const int *__restrict__ start, int *__restrict__ perm, long lo
   }
 }
 
+// Conditional fill for graph-captured paths (no-op when *cond is zero).
+__global__ void k_fill_int(int *__restrict__ p, int v, long long n, const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
 // Host driver of the three-pass exclusive scan (out has n+1 entries).
 // `cond` (device int, may be NULL) skips the whole scan when zero, so the
 // scan can sit inside a captured CUDA graph behind a device-side decision.
