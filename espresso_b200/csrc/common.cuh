@@ -1,6 +1,7 @@
 // Shared definitions of the p3mx CUDA engine (sm_100a).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -77,6 +78,8 @@ struct RepGeom {
   int cao;
   long long p0, np;  // particle range
   long long rm_off;  // real mesh offset (elements)
+  long long re_off;  // field mesh offset (records of 4 values)
+  int epad[3];       // field mesh extent: mesh plus high-side ghost layers
   long long bin_off; // corner key offset: bricks of brick^3 corners
   long long brk_off; // brick (sort key) offset
   int brick;         // brick edge (corner units) of the charge assignment
@@ -140,6 +143,24 @@ __device__ inline void bulk_g2s(void *dst, const void *src, unsigned bytes,
           "r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
+}
+// Tiled 3-d tensor copy global -> shared (TMA engine) of the box at
+// coordinates (c0 innermost, c1, c2) of the tensor map, completing on the
+// mbarrier; the shared destination is 128-byte aligned and c0 times the
+// element size a multiple of 16 bytes.
+__device__ inline void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                   unsigned long long *bar) {
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+               " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+               "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2),
+               "r"(smem_u32(bar))
+               : "memory");
+}
+// Acquire a tensor map that lives in global memory for the tensor proxy.
+__device__ inline void tensormap_acquire(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<unsigned long long>(map))
+               : "memory");
 }
 // Wait until the phase with the given parity completes; false when the
 // iteration limit ran out (the caller reports it and bails out).

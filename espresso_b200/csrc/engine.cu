@@ -4,7 +4,10 @@
 #include "p3m_kernels.cuh"
 #include "sort.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -153,7 +156,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   double max_ia = -1.0;
   for (auto const &e : m_ia)
     max_ia = std::max(max_ia, e.ia_cut);
-  m_bins = m_cplx = m_cells = m_nkeys = m_ncorner = 0;
+  m_bins = m_cplx = m_cells = m_nkeys = m_ncorner = m_ebins = 0;
   for (int r = 0; r < R; ++r) {
     auto const &c = conf[r];
     auto &G = m_geom[r];
@@ -193,6 +196,16 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     m_nkeys += static_cast<long long>(G.nbx) * G.nby * G.nbz;
     G.rm_off = m_bins;
     G.km_off = m_cplx;
+    // field mesh: ghost layers (periodic images) on the high side, so that
+    // the interpolation tile of every brick (brick + cao - 1 points from the
+    // brick origin) is one box of the padded mesh
+    {
+      int const nb[3] = {G.nbx, G.nby, G.nbz};
+      for (int d = 0; d < 3; ++d)
+        G.epad[d] = std::max(c.mesh[d], (nb[d] - 1) * G.brick + G.brick + c.cao - 1);
+      G.re_off = m_ebins;
+      m_ebins += static_cast<long long>(G.epad[0]) * G.epad[1] * G.epad[2];
+    }
     m_bins += static_cast<long long>(c.mesh[0]) * c.mesh[1] * c.mesh[2];
     m_cplx += static_cast<long long>(c.mesh[0]) * c.mesh[1] * G.hp;
     // short-range cell system
@@ -439,15 +452,17 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_key.ensure(n * sizeof(int));
   m_bkey.ensure(n * sizeof(int));
   m_slot.ensure(n * sizeof(int));
-  m_perm.ensure(n * sizeof(int));
+  // + 8: the back-interpolation copies 16-byte aligned windows of these
+  m_perm.ensure((n + 8) * sizeof(int));
   m_cnt.ensure((m_nkeys + 1) * sizeof(int));
   m_start.ensure((m_nkeys + 1) * sizeof(int));
   m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
   m_W.ensure(static_cast<size_t>(wstride<7, 4>()) * n * rsz);
-  m_skey.ensure(n * sizeof(int));
+  m_skey.ensure((n + 8) * sizeof(int));
   m_rho.ensure(m_bins * rsz);
-  m_E.ensure(4 * m_bins * rsz);
+  m_E.ensure(4 * m_ebins * rsz);
+  encode_field_maps(st);
   m_ck.ensure(m_cplx * csz);
   m_field.ensure(3 * m_cplx * csz);
   m_ginf.ensure(m_cplx * rsz);
@@ -536,6 +551,72 @@ void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, lon
                       st>>>(
       start, perm, nkeys, cond); ++m_launches;
 }
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 const fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult res = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &res) !=
+            cudaSuccess ||
+        res != cudaDriverEntryPointSuccess || p == nullptr) {
+      cudaGetLastError();
+      throw Error(4, "cuTensorMapEncodeTiled is not available from the CUDA driver");
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+} // namespace
+
+// One tensor map per replica over its packed, ghost-padded field mesh E (4
+// values per point): dims (4 E2, E1, E0) with E = epad, box (4 Ed, Ed, Ed)
+// with Ed = brick + cao - 1 (<= epad by construction).
+void Engine::encode_field_maps(cudaStream_t st) {
+  auto enc = tensor_map_encoder();
+  size_t const es = m_fp32 ? sizeof(float) : sizeof(double);
+  std::vector<CUtensorMap> maps(m_geom.size());
+  for (size_t r = 0; r < m_geom.size(); ++r) {
+    RepGeom const &G = m_geom[r];
+    cuuint32_t const Ed = static_cast<cuuint32_t>(G.brick + G.cao - 1);
+    cuuint64_t const E0 = G.epad[0], E1 = G.epad[1], E2 = G.epad[2];
+    if (Ed > E0 || Ed > E1 || Ed > E2 || 4 * Ed > 256)
+      throw Error(1, "interpolation tile larger than the field mesh box limits");
+    cuuint64_t dims[3] = {4 * E2, E1, E0};
+    cuuint64_t strides[2] = {4 * E2 * es, 4 * E2 * E1 * es};
+    cuuint32_t box[3] = {4 * Ed, Ed, Ed};
+    cuuint32_t estr[3] = {1, 1, 1};
+    void *base = static_cast<char *>(m_E.p) + 4 * static_cast<size_t>(G.re_off) * es;
+    CUresult const rc =
+        enc(&maps[r], m_fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+            3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS)
+      throw Error(4, "tensor map encoding of the field mesh failed (" + std::to_string(rc) + ")");
+  }
+  upload_vec(m_tmap, maps, st);
+}
+
+namespace {
+// Persistent grid of the back-interpolation pipeline: resident blocks per
+// SM times the SM count (computed once per kernel instance and process),
+// at most one block per brick.
+template <typename Real, int P> int interp_grid(int nbricks) {
+  static std::atomic<int> blocks{0};
+  int b = blocks.load(std::memory_order_relaxed);
+  if (b == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    P3MX_CUDA(cudaGetDevice(&dev));
+    P3MX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    P3MX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_p3m_interp<Real, P>, 32 * (1 + kInterpWarps), interp_smem<Real, P>()));
+    b = std::max(1, per_sm) * std::max(1, sms);
+    blocks.store(b, std::memory_order_relaxed);
+  }
+  return std::max(1, std::min(nbricks, b));
+}
+} // namespace
 
 #define P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                  \
   switch (cao) {                                                               \
@@ -641,13 +722,13 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   if (m_interp_wait)
     P3MX_CUDA(cudaStreamWaitEvent(st, m_interp_wait, 0));
   if (m_n > 0) {
-    using R4 = typename Real4Of<Real>::type;
     int const nbr = m_phase_off.back();
-    P3MX_CAO_DISPATCH_R(cao, (k_p3m_interp<Real, P><<<nbr, 32 * kAssignWarps,
-                                 static_cast<size_t>(m_tile_cap) * sizeof(R4), st>>>(
+    P3MX_CAO_DISPATCH_R(cao, (k_p3m_interp<Real, P><<<interp_grid<Real, P>(nbr),
+                                 32 * (1 + kInterpWarps), interp_smem<Real, P>(), st>>>(
                                  geom, m_blk_brick.as<int2>(), nbr, m_start.as<int>(),
                                  m_perm.as<int>(), m_skey.as<int>(), m_W.as<Real>(),
-                                 m_E.as<Real>(), d_q(), m_dipole.as<double>(), f,
+                                 m_E.as<Real>(), m_tmap.as<CUtensorMap>(), d_q(),
+                                 m_dipole.as<double>(), f,
                                  overwrite ? 1 : 0, m_kerr.as<int>())));
     ++m_launches;
   }

@@ -141,6 +141,7 @@ private:
   void build_lists(cudaStream_t st);
   void set_list_capacity(double margin);
   void layout_lists(cudaStream_t st);
+  void encode_field_maps(cudaStream_t st);
   // want_spq: also the FP64 double4 positions (FP64 pair kernel)
   void refresh_sorted_positions(cudaStream_t st, bool want_spq = true);
   void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
@@ -160,6 +161,7 @@ private:
   std::vector<RepGeom> m_geom;
   long long m_n = 0;
   long long m_bins = 0, m_cplx = 0, m_cells = 0, m_nkeys = 0; // m_nkeys: bricks (sort keys)
+  long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
   std::vector<int> m_phase_off; // assignment brick table offsets per colour
   int m_tile_cap = 1;           // largest assignment tile (points)
@@ -185,6 +187,7 @@ private:
   DevBuf m_key, m_bkey, m_slot, m_cnt, m_start, m_perm, m_scan_tiles;
   DevBuf m_dist, m_W, m_skey;
   DevBuf m_rho, m_ck, m_field, m_E, m_ginf;
+  DevBuf m_tmap; // per replica: tensor map of its field mesh (interpolation tiles)
   DevBuf m_part_x, m_part_census, m_sums_x, m_sums_census, m_dipole;
   bool m_ginf_valid = false;
   std::vector<double> m_census_h;

@@ -641,8 +641,13 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   C *res = fft_lines<C>(a, b, nc, ld, G.plan[2], tw, true);
   // packed field mesh: one (Ex, Ey, Ez, 0) record per mesh point, so the
   // interpolation gathers one 16-byte (FP32) record per stencil point
+  // (ghost-padded: every record also goes to its periodic images in the
+  // high-side ghost layers of extent epad)
   using R4 = typename Real4Of<Real>::type;
-  R4 *out = reinterpret_cast<R4 *>(efield) + G.rm_off + line0 * n;
+  R4 *out = reinterpret_cast<R4 *>(efield) + G.re_off;
+  int const M1 = G.mesh[1], M0 = G.mesh[0];
+  int const P0 = G.epad[0], P1 = G.epad[1], P2 = G.epad[2];
+  int const x0 = static_cast<int>(line0 / M1), y0 = static_cast<int>(line0 - static_cast<long long>(x0) * M1);
   for_lines(nl, n, [&](int l, int k) {
     C const xy = res[l * ld + pix(k)];
     C const zz = res[(nl + (l >> 1)) * ld + pix(k)];
@@ -651,7 +656,17 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     v.y = xy.y;
     v.z = (l & 1) ? zz.y : zz.x;
     v.w = Real(0);
-    out[l * n + k] = v;
+    int x = x0, y = y0 + l;
+    while (y >= M1) {
+      y -= M1;
+      ++x;
+    }
+    for (int xg = x; xg < P0; xg += M0)
+      for (int yg = y; yg < P1; yg += M1) {
+        R4 *row = out + (static_cast<long long>(xg) * P1 + yg) * P2;
+        for (int zg = k; zg < P2; zg += n)
+          row[zg] = v;
+      }
   });
 }
 

@@ -424,153 +424,277 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   }
 }
 
-// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373),
-// one block of kAssignWarps warps per brick.  The block first copies the
-// brick's field tile -- (B+P-1)^3 packed (Ex, Ey, Ez, 0) records around the
-// brick, periodic images folded in -- into shared memory with batched
-// coalesced loads; the particles of the brick (one contiguous range of the
-// brick-major order) then read only shared memory.  Eight lanes serve one
-// particle: lane kz owns the stencil z offset kz and walks the P^2 (x, y)
-// rows; lane sums are FP32, the group reduction is FP64 in a fixed shuffle
-// order (deterministic).  F -= prefactor/V * sum (q wx wy wz) E, plus the
-// dipole term for epsilon != 0 (p3m.cpp:540-547).  Writes (or adds) f[3*i] of
-// the original particle index.
+// Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373) as
+// a warp-specialised pipeline over bricks.  Each block takes the bricks
+// blockIdx.x, blockIdx.x + gridDim.x, ... (a persistent grid); its warp 0
+// (the producer) fills kInterpStages shared-memory stages ahead of the
+// kInterpWarps consumer warps.  A stage holds one brick's field tile --
+// (B+P-1)^3 packed (Ex, Ey, Ez, 0) records from the brick origin, one 3-d
+// tensor copy (TMA engine) from the replica's ghost-padded field mesh, whose
+// high-side ghost layers hold the periodic images -- and the weight records,
+// sort keys and source indices of up to kInterpCap of the brick's particles
+// (contiguous in the brick-major order: one bulk copy each).  A full barrier
+// per stage counts the producer lanes' arrivals and the copied bytes; an
+// empty barrier per stage counts the consumer warps that finished with it.
+// Consumers read shared memory only (particles past the cap of a dense brick
+// read their records from global memory) and store the forces.
+//
+// Eight lanes serve one particle: lane kz owns the stencil z offset kz and
+// walks the P^2 (x, y) rows; lane sums are FP32 (FP64 for the FP64 path),
+// the group reduction is FP64 in a fixed shuffle order (deterministic).
+// F -= prefactor/V * sum (q wx wy wz) E, plus the dipole term for
+// epsilon != 0 (p3m.cpp:540-547).  Writes (or adds) f[3*i] of the original
+// particle index.  Every barrier wait is bounded: on a timeout the kernel
+// sets *err, the producer waits (bounded) for its copies in flight, and the
+// block returns.
+constexpr int kInterpStages = 2;
+constexpr int kInterpWarps = 8; // consumer warps
+constexpr int kInterpCap = 64;  // particles per stage with staged records
+
+template <typename Real, int P> struct InterpStage {
+  using R4 = typename Real4Of<Real>::type;
+  static constexpr int Ed = brick_edge<P>() + P - 1;
+  static constexpr size_t tile = sizeof(R4) * Ed * Ed * Ed;
+  static constexpr size_t rec = sizeof(Real) * kInterpCap * wstride<P, 4>();
+  // key / index window: the 16-byte aligned superset of the staged range
+  static constexpr size_t ids = sizeof(int) * (kInterpCap + 8);
+  // stages start on 128-byte boundaries (tensor copy destinations)
+  static constexpr size_t bytes = (tile + rec + 2 * ids + 127) / 128 * 128;
+  static_assert(tile % 16 == 0 && rec % 16 == 0 && ids % 16 == 0, "bulk copy alignment");
+};
+// (+ 128: the kernel rounds the dynamic shared-memory base up to 128 bytes)
+template <typename Real, int P> __host__ __device__ constexpr size_t interp_smem() {
+  return kInterpStages * InterpStage<Real, P>::bytes + 128;
+}
+
+struct InterpInfo {
+  int rep, brick, s0, s1; // rep < 0: no more bricks
+  double pref, cdip;
+};
+
+__device__ inline void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 template <typename Real, int P>
-__global__ void __launch_bounds__(32 * kAssignWarps)
+__global__ void __launch_bounds__(32 * (1 + kInterpWarps), sizeof(Real) == 4 ? 2 : 1)
 k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
              const int *__restrict__ start, const int *__restrict__ perm,
              const int *__restrict__ s_key, const Real *__restrict__ W,
-             const Real *__restrict__ E, const double *__restrict__ q,
-             const double *__restrict__ dipole, double *__restrict__ f, int overwrite,
-             int *__restrict__ err) {
+             const Real *__restrict__ E, const CUtensorMap *__restrict__ tmaps,
+             const double *__restrict__ q, const double *__restrict__ dipole,
+             double *__restrict__ f, int overwrite, int *__restrict__ err) {
   static_assert(P <= 8, "one lane per stencil z offset");
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
-  constexpr int NT = 32 * kAssignWarps;
-  using R4 = typename Real4Of<Real>::type;
+  constexpr int S = kInterpStages, CW = kInterpWarps, CAP = kInterpCap;
+  using L = InterpStage<Real, P>;
+  using R4 = typename L::R4;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B, Ed = L::Ed, E2 = Ed * Ed;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  if (static_cast<int>(blockIdx.x) >= nbricks)
-    return; // whole block
+  __shared__ __align__(8) unsigned long long full[S], empty[S];
+  __shared__ InterpInfo s_info[S];
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int2 const bk = bricks[blockIdx.x];
-  RepGeom const &G = reps[bk.x];
-  constexpr int B = brick_edge<P>(), B3 = B * B * B, Ed = B + P - 1, E2 = Ed * Ed;
-  const int *st = start + G.brk_off;
-  int const s0 = st[bk.y], s1 = st[bk.y + 1];
-  if (s0 == s1)
-    return; // no particles in this brick
-  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-  int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
-  int const x0 = bx * B, y0 = by * B, z0 = bz * B;
-  R4 *tile = reinterpret_cast<R4 *>(smem_raw);
-  const R4 *E4 = reinterpret_cast<const R4 *>(E) + G.rm_off;
-  auto wrap = [](int v, int m) {
-    while (v >= m)
-      v -= m;
-    return v;
-  };
-  // mesh offsets of the tile's x planes and y rows (periodic images folded)
-  __shared__ int s_xo[16], s_yo[16];
-  if (tid < Ed)
-    s_xo[tid] = wrap(x0 + tid, M0) * M1 * M2;
-  else if (tid >= 32 && tid - 32 < Ed)
-    s_yo[tid - 32] = wrap(y0 + tid - 32, M1) * M2;
-  __syncthreads();
-  // tile rows (x, y) of Ed records along z are contiguous in the field mesh
-  // (two pieces when the row wraps around z): one bulk copy (TMA engine) per
-  // piece, all completing on one mbarrier that expects the whole tile
-  __shared__ __align__(8) unsigned long long bar;
   if (tid == 0) {
-    mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, static_cast<unsigned>(E2 * Ed * sizeof(R4)));
-  }
-  __syncthreads();
-  for (int row = tid; row < E2; row += NT) {
-    int const x = row / Ed, y = row - x * Ed;
-    const R4 *src = E4 + (s_xo[x] + s_yo[y]);
-    R4 *dst = tile + row * Ed;
-    // pieces of the row up to each z wrap (several when the mesh is shorter
-    // than the tile along z); each piece stays inside its mesh row
-    int z = z0, done = 0;
-    while (done < Ed) {
-      int const len = min(Ed - done, M2 - z);
-      bulk_g2s(dst + done, src + z, static_cast<unsigned>(len * sizeof(R4)), &bar);
-      done += len;
-      z = 0;
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+      mbar_init(&full[k], 32);  // the producer's lanes
+      mbar_init(&empty[k], CW); // one arrival per consumer warp
     }
   }
-  bool const ok = mbar_wait(&bar, 0);
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0) {
-      atomicExch(err, 1);
-      mbar_wait(&bar, 0); // second bounded wait for the copies in flight
+  __syncthreads();
+  unsigned char *const smem_base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  auto stage_ptr = [&](int k) { return smem_base + static_cast<size_t>(k) * L::bytes; };
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    // the next brick's table entry and particle range are fetched one brick
+    // ahead, so their load latency overlaps the copies of the current one
+    int it = 0, last_rep = -1;
+    bool ok = true;
+    int n = blockIdx.x;
+    int2 bk = make_int2(0, 0);
+    int s0 = 0, s1 = 0;
+    if (n < nbricks) {
+      bk = bricks[n];
+      const int *st = start + reps[bk.x].brk_off;
+      s0 = st[bk.y];
+      s1 = st[bk.y + 1];
+    }
+    for (; n < nbricks; n += gridDim.x) {
+      int const nn = n + gridDim.x;
+      int2 const bkn = (nn < nbricks) ? bricks[nn] : make_int2(0, 0);
+      if (s0 != s1) {
+        RepGeom const &G = reps[bk.x];
+        int const k = it % S;
+        bool const got = mbar_wait(&empty[k], ((it / S) & 1) ^ 1u);
+        if (!__all_sync(0xffffffffu, got)) {
+          ok = false;
+          break;
+        }
+        unsigned char *sp = stage_ptr(k);
+        R4 *tile = reinterpret_cast<R4 *>(sp);
+        Real *rec = reinterpret_cast<Real *>(sp + L::tile);
+        int *keys = reinterpret_cast<int *>(sp + L::tile + L::rec);
+        int *pm = reinterpret_cast<int *>(sp + L::tile + L::rec + L::ids);
+        int const cn = min(s1 - s0, CAP);
+        int const a0 = s0 & ~3, a1 = (s0 + cn + 3) & ~3;
+        if (lane == 0) {
+          InterpInfo inf;
+          inf.rep = bk.x;
+          inf.brick = bk.y;
+          inf.s0 = s0;
+          inf.s1 = s1;
+          inf.pref = G.prefactor / G.V;
+          inf.cdip = (G.epsilon != 0.0)
+                         ? G.prefactor * 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0)
+                         : 0.0;
+          s_info[k] = inf;
+        }
+        // the consumers' reads of the stage were generic-proxy accesses:
+        // order them before the asynchronous-proxy writes that refill it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
+        // lane 0: the tile; lanes 1..3: one particle array each
+        unsigned bytes = 0;
+        if (lane == 0)
+          bytes = static_cast<unsigned>(E2 * Ed * sizeof(R4));
+        else if (lane == 1)
+          bytes = static_cast<unsigned>(cn * WS * sizeof(Real));
+        else if (lane == 2 || lane == 3)
+          bytes = static_cast<unsigned>((a1 - a0) * sizeof(int));
+        mbar_arrive_expect_tx(&full[k], bytes);
+        if (lane == 0) {
+          if (bk.x != last_rep) {
+            tensormap_acquire(&tmaps[bk.x]);
+            last_rep = bk.x;
+          }
+          tma_load_3d(tile, &tmaps[bk.x], 4 * bz * B, by * B, bx * B, &full[k]);
+        } else if (lane == 1) {
+          bulk_g2s(rec, W + static_cast<long long>(s0) * WS,
+                   static_cast<unsigned>(cn * WS * sizeof(Real)), &full[k]);
+        } else if (lane == 2) {
+          bulk_g2s(keys, s_key + a0, static_cast<unsigned>((a1 - a0) * sizeof(int)), &full[k]);
+        } else if (lane == 3) {
+          bulk_g2s(pm, perm + a0, static_cast<unsigned>((a1 - a0) * sizeof(int)), &full[k]);
+        }
+        ++it;
+      }
+      int s0n = 0, s1n = 0;
+      if (nn < nbricks) {
+        const int *st = start + reps[bkn.x].brk_off;
+        s0n = st[bkn.y];
+        s1n = st[bkn.y + 1];
+      }
+      bk = bkn;
+      s0 = s0n;
+      s1 = s1n;
+    }
+    // end marker for the consumers
+    if (ok) {
+      int const k = it % S;
+      bool const got = mbar_wait(&empty[k], ((it / S) & 1) ^ 1u);
+      if (__all_sync(0xffffffffu, got)) {
+        if (lane == 0)
+          s_info[k].rep = -1;
+        mbar_arrive(&full[k]);
+      } else {
+        ok = false;
+      }
+    }
+    if (!ok) {
+      if (lane == 0)
+        atomicExch(err, 1);
+      // bounded wait for the fills that may still be in flight
+      for (int j = max(0, it - S); j < it; ++j)
+        mbar_wait(&full[j % S], (j / S) & 1);
     }
     return;
   }
-  int const g = lane >> 3, kz = lane & 7;
-  double const pref = G.prefactor / G.V;
-  double const cdip = (G.epsilon != 0.0)
-                          ? G.prefactor * 4.0 * kPi / G.V / (2.0 * G.epsilon + 1.0)
-                          : 0.0;
-  // four particles per warp (one per 8-lane group), warps interleaved
-  for (int sb = s0 + 4 * warp; sb < s1; sb += 4 * kAssignWarps) {
-    int const s = sb + g;
-    bool const live = s < s1;
-    Real ax = Real(0), ay = Real(0), az = Real(0);
-    if (live && kz < P) {
-      int const l = s_key[s] - bk.y * B3;
-      int const lb = __ffs(B) - 1; // B is a power of two
-      int const lx = l >> (2 * lb), ly = (l >> lb) & (B - 1), lz = l & (B - 1);
-      const Real *w = W + static_cast<long long>(s) * WS;
-      Real wx[P], wy[P];
+
+  // ---------------- consumers ----------------
+  int const cw = warp - 1, g = lane >> 3, kz = lane & 7;
+  for (int it = 0;; ++it) {
+    int const k = it % S;
+    bool const got = mbar_wait(&full[k], (it / S) & 1);
+    if (!__all_sync(0xffffffffu, got)) {
+      if (lane == 0)
+        atomicExch(err, 1);
+      return;
+    }
+    InterpInfo const inf = s_info[k];
+    if (inf.rep < 0)
+      return;
+    unsigned char *sp = stage_ptr(k);
+    const R4 *tile = reinterpret_cast<const R4 *>(sp);
+    const Real *rec = reinterpret_cast<const Real *>(sp + L::tile);
+    const int *keys = reinterpret_cast<const int *>(sp + L::tile + L::rec);
+    const int *pm = reinterpret_cast<const int *>(sp + L::tile + L::rec + L::ids);
+    int const s0 = inf.s0, s1 = inf.s1, a0 = s0 & ~3;
+    // four particles per warp (one per 8-lane group), warps interleaved
+    for (int sb = s0 + 4 * cw; sb < s1; sb += 4 * CW) {
+      int const s = sb + g, j = s - s0;
+      bool const live = s < s1;
+      Real ax = Real(0), ay = Real(0), az = Real(0);
+      if (live && kz < P) {
+        bool const staged = j < CAP;
+        int const l = (staged ? keys[s - a0] : s_key[s]) - inf.brick * B3;
+        int const lb = __ffs(B) - 1; // B is a power of two
+        int const lx = l >> (2 * lb), ly = (l >> lb) & (B - 1), lz = l & (B - 1);
+        const Real *w = staged ? rec + j * WS : W + static_cast<long long>(s) * WS;
+        Real wx[P], wy[P];
 #pragma unroll
-      for (int k = 0; k < P; ++k) {
-        wx[k] = w[k];
-        wy[k] = w[P + k];
+        for (int kk = 0; kk < P; ++kk) {
+          wx[kk] = w[kk];
+          wy[kk] = w[P + kk];
+        }
+        Real const wzk = w[WZ + kz];
+        const R4 *tp = tile + (lx * Ed + ly) * Ed + lz + kz;
+#pragma unroll
+        for (int kx = 0; kx < P; ++kx) {
+          Real const wxz = wx[kx] * wzk;
+#pragma unroll
+          for (int ky = 0; ky < P; ++ky) {
+            R4 const e = tp[(kx * Ed + ky) * Ed];
+            Real const wt = wxz * wy[ky];
+            ax += wt * e.x;
+            ay += wt * e.y;
+            az += wt * e.z;
+          }
+        }
       }
-      Real const wzk = w[WZ + kz];
-      const R4 *tp = tile + (lx * Ed + ly) * Ed + lz + kz;
+      double fx = static_cast<double>(ax), fy = static_cast<double>(ay),
+             fz = static_cast<double>(az);
 #pragma unroll
-      for (int kx = 0; kx < P; ++kx) {
-        Real const wxz = wx[kx] * wzk;
-#pragma unroll
-        for (int ky = 0; ky < P; ++ky) {
-          R4 const e = tp[(kx * Ed + ky) * Ed];
-          Real const wt = wxz * wy[ky];
-          ax += wt * e.x;
-          ay += wt * e.y;
-          az += wt * e.z;
+      for (int o = 1; o < 8; o <<= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+      }
+      if (live && kz == 0) {
+        int const i = (j < CAP) ? pm[s - a0] : perm[s];
+        double ox = -inf.pref * fx, oy = -inf.pref * fy, oz = -inf.pref * fz;
+        if (inf.cdip != 0.0) {
+          double const qi = q[i];
+          ox -= qi * inf.cdip * dipole[3 * inf.rep + 0];
+          oy -= qi * inf.cdip * dipole[3 * inf.rep + 1];
+          oz -= qi * inf.cdip * dipole[3 * inf.rep + 2];
+        }
+        if (overwrite) {
+          f[3 * i + 0] = ox;
+          f[3 * i + 1] = oy;
+          f[3 * i + 2] = oz;
+        } else {
+          f[3 * i + 0] += ox;
+          f[3 * i + 1] += oy;
+          f[3 * i + 2] += oz;
         }
       }
     }
-    double fx = static_cast<double>(ax), fy = static_cast<double>(ay),
-           fz = static_cast<double>(az);
-#pragma unroll
-    for (int o = 1; o < 8; o <<= 1) {
-      fx += __shfl_xor_sync(0xffffffffu, fx, o);
-      fy += __shfl_xor_sync(0xffffffffu, fy, o);
-      fz += __shfl_xor_sync(0xffffffffu, fz, o);
-    }
-    if (live && kz == 0) {
-      int const i = perm[s];
-      double ox = -pref * fx, oy = -pref * fy, oz = -pref * fz;
-      if (cdip != 0.0) {
-        double const qi = q[i];
-        ox -= qi * cdip * dipole[3 * bk.x + 0];
-        oy -= qi * cdip * dipole[3 * bk.x + 1];
-        oz -= qi * cdip * dipole[3 * bk.x + 2];
-      }
-      if (overwrite) {
-        f[3 * i + 0] = ox;
-        f[3 * i + 1] = oy;
-        f[3 * i + 2] = oz;
-      } else {
-        f[3 * i + 0] += ox;
-        f[3 * i + 1] += oy;
-        f[3 * i + 2] += oz;
-      }
-    }
+    __syncwarp();
+    if (lane == 0)
+      mbar_arrive(&empty[k]);
   }
 }
 
