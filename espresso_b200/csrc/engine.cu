@@ -304,11 +304,8 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       };
       std::vector<std::vector<int2>> phase;
       nat.clear();
-      m_tile_cap = 1;
       for (int r = 0; r < R; ++r) {
         auto const &G = m_geom[r];
-        int const E = G.brick + G.cao - 1;
-        m_tile_cap = std::max(m_tile_cap, E * E * E);
         auto const cxv = colours(G.mesh[0], G.brick, G.cao);
         auto const cyv = colours(G.mesh[1], G.brick, G.cao);
         auto const czv = colours(G.mesh[2], G.brick, G.cao);
@@ -683,8 +680,8 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
       P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps,
-                                   assign_smem<Real, P>(m_tile_cap), st>>>(
-                                   geom, tab, cnt, m_tile_cap, m_start.as<int>(), m_W.as<Real>(),
+                                   assign_smem<Real, P>(), st>>>(
+                                   geom, tab, cnt, m_start.as<int>(), m_W.as<Real>(),
                                    m_skey.as<int>(), m_rho.as<Real>(), m_kerr.as<int>())));
       ++m_launches;
     }

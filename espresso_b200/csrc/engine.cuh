@@ -164,7 +164,6 @@ private:
   long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
   std::vector<int> m_phase_off; // assignment brick table offsets per colour
-  int m_tile_cap = 1;           // largest assignment tile (points)
   int m_ntypes = 1;
   std::vector<PairIA> m_ia;
 

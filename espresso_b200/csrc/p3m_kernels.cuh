@@ -151,6 +151,40 @@ template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v
 // RepGeom::brick by the same rule).
 template <int P> __host__ __device__ constexpr int brick_edge() { return (P <= 5) ? 4 : 8; }
 
+// Strides of the charge-assignment tile [x][y][z] (z contiguous): the
+// smallest y stride >= E and x stride >= E * (y stride) for which the lanes of
+// a warp, one (x, y) stencil row each (row s = lane + 32 q, x = s / P,
+// y = s % P), hit distinct shared-memory banks.
+struct TileStrides {
+  int sy, sx;
+};
+template <int P> __host__ __device__ constexpr TileStrides assign_strides() {
+  constexpr int E = brick_edge<P>() + P - 1;
+  for (int sy = E; sy < E + 16; ++sy)
+    for (int sx = E * sy; sx < E * sy + 64; ++sx) {
+      bool ok = true;
+      for (int q = 0; q * 32 < P * P && ok; ++q) {
+        unsigned used = 0;
+        for (int lane = 0; lane < 32 && lane + 32 * q < P * P; ++lane) {
+          int const r = lane + 32 * q;
+          unsigned const bit = 1u << (((r / P) * sx + (r % P) * sy) % 32);
+          if (used & bit) {
+            ok = false;
+            break;
+          }
+          used |= bit;
+        }
+      }
+      if (ok)
+        return TileStrides{sy, sx};
+    }
+  return TileStrides{E, E * E};
+}
+// Points (per word array) of the assignment tile for interpolation order P.
+template <int P> __host__ __device__ constexpr int assign_tile_points() {
+  return (brick_edge<P>() + P - 1) * assign_strides<P>().sx;
+}
+
 // Warps per brick (block) of the charge assignment, and particles whose
 // weight records are staged in shared memory at a time.
 constexpr int kAssignWarps = 4;
@@ -159,11 +193,11 @@ constexpr int kAssignChunk = 64;
 // Bytes of dynamic shared memory of one assignment block: the split
 // fixed-point tile (two 32-bit words per point) and one staged chunk of
 // weight records and tile offsets.
-__host__ __device__ constexpr size_t assign_tile_bytes(int tile_cap) {
-  return (2 * sizeof(int) * static_cast<size_t>(tile_cap) + 15) / 16 * 16;
+template <int P> __host__ __device__ constexpr size_t assign_tile_bytes() {
+  return (2 * sizeof(int) * static_cast<size_t>(assign_tile_points<P>()) + 15) / 16 * 16;
 }
-template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem(int tile_cap) {
-  return assign_tile_bytes(tile_cap) + sizeof(Real) * kAssignChunk * wstride<P, 4>() +
+template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem() {
+  return assign_tile_bytes<P>() + sizeof(Real) * kAssignChunk * wstride<P, 4>() +
          sizeof(int) * kAssignChunk;
 }
 
@@ -213,14 +247,16 @@ template <> __device__ inline double from_ll<double>(long long v) { return __ll2
 template <typename Real, int P>
 __global__ void __launch_bounds__(32 * kAssignWarps)
 k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
-             int tile_cap, const int *__restrict__ start, const Real *__restrict__ W,
+             const int *__restrict__ start, const Real *__restrict__ W,
              const int *__restrict__ s_key, Real *__restrict__ rho, int *__restrict__ err) {
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
-  constexpr int P3 = P * P * P;
-  constexpr int NR = (P3 + 31) / 32;
+  constexpr int P2 = P * P;
+  constexpr int NQ = (P2 + 31) / 32; // rounds of (x, y) stencil rows
   constexpr int NT = 32 * kAssignWarps;
+  constexpr int TP = assign_tile_points<P>();
+  constexpr int SY = assign_strides<P>().sy, SX = assign_strides<P>().sx;
   constexpr int CH = kAssignChunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[kAssignWarps];
@@ -230,20 +266,21 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
-  constexpr int B = brick_edge<P>(), B3 = B * B * B, E = B + P - 1, E3 = E * E * E;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B, E = B + P - 1;
   const int *st = start + G.brk_off;
   int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)
     return; // empty brick: nothing to add
   int *t_hi = reinterpret_cast<int *>(smem_raw);
-  int *t_lo = t_hi + tile_cap;
-  Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes(tile_cap));
+  int *t_lo = t_hi + TP;
+  Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes<P>());
   int *rbase = reinterpret_cast<int *>(rec + CH * WS);
   if (tid == 0)
     mbar_init(&bar, 1);
-  for (int t = tid; t < E3; t += NT) {
-    t_hi[t] = 0;
-    t_lo[t] = 0;
+  {
+    int4 *z4 = reinterpret_cast<int4 *>(smem_raw);
+    for (int t = tid; t < static_cast<int>(assign_tile_bytes<P>() / 16); t += NT)
+      z4[t] = make_int4(0, 0, 0, 0);
   }
   __syncthreads(); // barrier initialised
   // stage a chunk of records (contiguous, 16-byte aligned: one bulk copy by
@@ -262,7 +299,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     for (int j = tid; j < cn; j += NT) {
       int const l = s_key[c0 + j] - bk.y * B3;
       int const lb = __ffs(B) - 1; // B is a power of two
-      rbase[j] = ((l >> (2 * lb)) * E + ((l >> lb) & (B - 1))) * E + (l & (B - 1));
+      rbase[j] = (l >> (2 * lb)) * SX + ((l >> lb) & (B - 1)) * SY + (l & (B - 1));
     }
     bool const ok = mbar_wait(&bar, parity);
     parity ^= 1u;
@@ -308,16 +345,15 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   Real const S = static_cast<Real>(ldexp(1.0, es));
   Real const two_kb = static_cast<Real>(1u << kb);
   Real const inv_two_kb = static_cast<Real>(1.0 / (1u << kb));
-  // per-lane stencil point of each round and its tile offset
-  int off[NR], wi[NR], wj[NR], wk[NR];
+  // per-lane (x, y) stencil row of each round and its tile offset
+  int qx[NQ], qy[NQ], qoff[NQ];
 #pragma unroll
-  for (int r = 0; r < NR; ++r) {
-    int const t = lane + 32 * r;
-    int const tt = (t < P3) ? t : 0;
-    wi[r] = tt / (P * P);
-    wj[r] = (tt / P) % P;
-    wk[r] = tt % P;
-    off[r] = (wi[r] * E + wj[r]) * E + wk[r];
+  for (int q = 0; q < NQ; ++q) {
+    int const r = lane + 32 * q;
+    int const rr = (r < P2) ? r : 0;
+    qx[q] = rr / P;
+    qy[q] = rr % P;
+    qoff[q] = qx[q] * SX + qy[q] * SY;
   }
   for (int c0 = s0; c0 < s1; c0 += CH) {
     int const cn = min(CH, s1 - c0);
@@ -329,14 +365,24 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     for (int j = warp; j < cn; j += kAssignWarps) {
       int const base = rbase[j];
       const Real *w = rec + j * WS;
+      Real wz[P];
 #pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        if (lane + 32 * r < P3) {
-          Real const t = (w[wi[r]] * w[P + wj[r]] * w[WZ + wk[r]]) * S;
-          int hi, lo;
-          split_fixed(t, two_kb, inv_two_kb, hi, lo);
-          atomicAdd(&t_hi[base + off[r]], hi);
-          atomicAdd(&t_lo[base + off[r]], lo);
+      for (int k = 0; k < P; ++k)
+        wz[k] = w[WZ + k];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        if (lane + 32 * q < P2) {
+          // the lane's row: P consecutive z points of one (x, y)
+          Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
+          int *const ph = t_hi + base + qoff[q];
+          int *const pl = t_lo + base + qoff[q];
+#pragma unroll
+          for (int k = 0; k < P; ++k) {
+            int hi, lo;
+            split_fixed(wxy * wz[k], two_kb, inv_two_kb, hi, lo);
+            atomicAdd(ph + k, hi);
+            atomicAdd(pl + k, lo);
+          }
         }
       }
     }
@@ -367,7 +413,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
     if (gy >= M1) gy -= M1;
     if (gz >= M2) { gz -= M2; cls |= 4; }
     if (gz >= M2) gz -= M2;
-    yzt[k2] = (t < nyz) ? y * E + z : -1;
+    yzt[k2] = (t < nyz) ? y * SY + z : -1;
     yzg[k2] = gy * M2 + gz;
     ycls[k2] = cls;
   }
@@ -402,7 +448,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
 #pragma unroll
         for (int k2 = 0; k2 < NS; ++k2)
           if (yzt[k2] >= 0)
-            mesh[gbase + yzg[k2]] = old[x][k2] + tile_val(x * E * E + yzt[k2]);
+            mesh[gbase + yzg[k2]] = old[x][k2] + tile_val(x * SX + yzt[k2]);
       }
     }
     return;
@@ -417,7 +463,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
       for (int k2 = 0; k2 < NS; ++k2) {
         if (yzt[k2] < 0 || (xcls | ycls[k2]) != pass)
           continue;
-        mesh[gbase + yzg[k2]] += tile_val(x * E * E + yzt[k2]);
+        mesh[gbase + yzg[k2]] += tile_val(x * SX + yzt[k2]);
       }
     }
     __syncthreads();
