@@ -457,7 +457,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_dist.ensure(3 * n * rsz);
   m_W.ensure(static_cast<size_t>(wstride<7, 4>()) * n * rsz);
   m_skey.ensure((n + 8) * sizeof(int));
-  m_rho.ensure(m_bins * rsz);
+  m_rho.ensure(m_bins * rsz + 64); // + slack: bulk copies of 16-byte aligned supersets
   m_E.ensure(4 * m_ebins * rsz);
   encode_field_maps(st);
   m_ck.ensure(m_cplx * csz);
@@ -690,7 +690,8 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 3. forward FFT z (r2c) and y
   C const *tw = m_tw.as<C>();
   k_fft_z_fwd<Real><<<m_n_blk_zf, 256, m_smem_zf, st>>>(geom, m_blk_zf.as<Blk>(), m_rho.as<Real>(),
-                                                        m_ck.as<C>(), tw); ++m_launches;
+                                                        m_ck.as<C>(), tw, m_kerr.as<int>());
+  ++m_launches;
   k_fft_y<Real><<<dim3(m_n_blk_y, 1), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_ck.as<C>(), 0,
                                                           m_tile_y, false, tw); ++m_launches;
   mark("fft_fwd_zy", st);
@@ -713,7 +714,8 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   k_fft_y<Real><<<dim3(m_n_blk_y, 3), 256, m_smem_y, st>>>(geom, m_blk_y.as<Blk>(), m_field.as<C>(),
                                                           m_cplx, m_tile_y, true, tw); ++m_launches;
   k_fft_z_inv3<Real><<<m_n_blk_zi, 256, m_smem_zi, st>>>(geom, m_blk_zi.as<Blk>(), m_field.as<C>(),
-                                                         m_cplx, m_E.as<Real>(), tw); ++m_launches;
+                                                         m_cplx, m_E.as<Real>(), tw, m_kerr.as<int>());
+  ++m_launches;
   mark("fft_inv_yz", st);
   // 6. force back-interpolation (after the concurrent pair kernel, if any)
   if (m_interp_wait)

@@ -339,6 +339,43 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
   return src;
 }
 
+// Copy the contiguous global range [src, src + count) to shared memory with
+// one bulk copy (TMA engine) when its 16-byte aligned superset fits in the
+// `room` bytes at `area`.  Returns the shared-memory copy of src, or nullptr
+// when the range does not fit (nothing copied; the decision is uniform over
+// the block).  Called by all threads of the block; the copy has landed when
+// it returns.  A wait that runs out sets *err and `failed` (the caller
+// returns).  The aligned superset may reach up to 15 bytes past the range:
+// the buffer behind src is allocated with that slack.
+template <typename T>
+__device__ inline const T *bulk_stage(const T *src, long long count, unsigned char *area,
+                                      size_t room, unsigned long long *bar, int *err,
+                                      bool &failed) {
+  uintptr_t const g0 = reinterpret_cast<uintptr_t>(src) & ~uintptr_t(15);
+  uintptr_t const g1 = (reinterpret_cast<uintptr_t>(src + count) + 15) & ~uintptr_t(15);
+  unsigned const pad = (16u - (smem_u32(area) & 15u)) & 15u;
+  size_t const bytes = g1 - g0;
+  if (pad + bytes > room || bytes >= (1u << 20))
+    return nullptr;
+  unsigned char *dst = area + pad;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, static_cast<unsigned>(bytes));
+    bulk_g2s(dst, reinterpret_cast<const void *>(g0), static_cast<unsigned>(bytes), bar);
+  }
+  __syncthreads(); // barrier initialised before anyone waits on it
+  bool const ok = mbar_wait(bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(err, 1);
+      mbar_wait(bar, 0); // second bounded wait for the copy in flight
+    }
+    failed = true;
+    return nullptr;
+  }
+  return reinterpret_cast<const T *>(dst + (reinterpret_cast<uintptr_t>(src) - g0));
+}
+
 // ---- pass z, forward: real lines -> complex half lines -----------------
 // Two real lines per complex transform: Z = x0 + i x1, then
 // X0[k] = (Z[k] + conj Z[n-k]) / 2 and X1[k] = -i (Z[k] - conj Z[n-k]) / 2.
@@ -348,7 +385,7 @@ template <typename Real>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
 k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
             const Real *__restrict__ rmesh, typename CplxOf<Real>::type *__restrict__ cmesh,
-            const typename CplxOf<Real>::type *__restrict__ twtab) {
+            const typename CplxOf<Real>::type *__restrict__ twtab, int *__restrict__ err) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
@@ -363,12 +400,22 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   load_twiddles(tw, twtab, G.plan[2]);
   long long const line0 = bk.a;
   const Real *src = rmesh + G.rm_off + line0 * n;
-  // real line l, element k -> real or imaginary part of slot l/2 (line by
-  // line, four lines of loads in flight)
+  // the block's nl real lines are one contiguous range of the mesh: stage it
+  // in b (the FFT scratch) with one bulk copy when it fits there
+  __shared__ __align__(8) unsigned long long bar;
+  bool failed = false;
+  const Real *sv = bulk_stage(src, static_cast<long long>(nl) * n,
+                              reinterpret_cast<unsigned char *>(b), np * ld * sizeof(C), &bar,
+                              err, failed);
+  if (failed)
+    return;
+  if (sv == nullptr)
+    sv = src;
+  // real line l, element k -> real or imaginary part of slot l/2
   Real *ar = reinterpret_cast<Real *>(a);
   // odd count: the last slot's imaginary part is line nl, all zeros
   for_lines(nl + (nl & 1), n, [&](int l, int k) {
-    ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = (l < nl) ? src[l * n + k] : Real(0);
+    ar[2 * ((l >> 1) * ld + pix(k)) + (l & 1)] = (l < nl) ? sv[l * n + k] : Real(0);
   });
   __syncthreads();
   C *res = fft_lines<C>(a, b, np, ld, G.plan[2], tw, false);
@@ -588,7 +635,8 @@ template <typename Real>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
 k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
              const typename CplxOf<Real>::type *__restrict__ field0, long long field_stride,
-             Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab) {
+             Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab,
+             int *__restrict__ err) {
   using C = typename CplxOf<Real>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Blk const bk = blks[blockIdx.x];
@@ -606,17 +654,49 @@ k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   C *b = a + nc * ld;
   C *tw = b + z_inv_b_size(nl, n);
   load_twiddles(tw, twtab, G.plan[2]);
-  // stage the half rows (H entries of each of 3 nl rows; field d, line l at
-  // b[(d * nl + l) * hl]), then build the packed lines in a
+  // stage the half rows of the 3 fields (field d, line l at
+  // sb[(d * nl + l) * hs]), then build the packed lines in a.  A field's nl
+  // rows are one contiguous range (row stride hp): one bulk copy (TMA
+  // engine) per field when the three fit in b, else plain loads (stride hl)
   const C *fsrc = field0 + G.km_off + line0 * G.hp;
-  // row dl = d * nl + l of the three fields
-  for_lines(3 * nl, H, [&](int dl, int k) {
-    int const d = (dl >= 2 * nl) ? 2 : (dl >= nl ? 1 : 0), l = dl - d * nl;
-    b[dl * hl + k] = fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
-  });
-  __syncthreads();
+  __shared__ __align__(8) unsigned long long bar;
+  size_t const rb = static_cast<size_t>(nl) * G.hp * sizeof(C);
+  unsigned char *const bb = reinterpret_cast<unsigned char *>(b);
+  unsigned const pad = (16u - (smem_u32(bb) & 15u)) & 15u;
+  bool const bulk =
+      ((reinterpret_cast<uintptr_t>(fsrc) | static_cast<uintptr_t>(field_stride * sizeof(C))) &
+       15u) == 0 &&
+      rb % 16 == 0 && pad + 3 * rb <= z_inv_b_size(nl, n) * sizeof(C) && 3 * rb < (1u << 20);
+  C *sb = b;
+  int hs = hl;
+  if (bulk) {
+    sb = reinterpret_cast<C *>(bb + pad);
+    hs = G.hp;
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      mbar_arrive_expect_tx(&bar, static_cast<unsigned>(3 * rb));
+      for (int d = 0; d < 3; ++d)
+        bulk_g2s(bb + pad + d * rb, fsrc + field_stride * d, static_cast<unsigned>(rb), &bar);
+    }
+    __syncthreads(); // barrier initialised before anyone waits on it
+    bool const ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait(&bar, 0); // second bounded wait for the copies in flight
+      }
+      return;
+    }
+  } else {
+    // row dl = d * nl + l of the three fields
+    for_lines(3 * nl, H, [&](int dl, int k) {
+      int const d = (dl >= 2 * nl) ? 2 : (dl >= nl ? 1 : 0), l = dl - d * nl;
+      b[dl * hl + k] = fsrc[field_stride * d + static_cast<long long>(l) * G.hp + k];
+    });
+    __syncthreads();
+  }
   auto herm = [&](int d, int l, int k) -> C {
-    const C *row = b + (d * nl + l) * hl;
+    const C *row = sb + (d * nl + l) * hs;
     if (k < H) {
       C v = row[k];
       if (k == 0 || 2 * k == n)
