@@ -66,8 +66,28 @@ struct ChunkEvents {
   }
 };
 
-// Chunk of the host<->device staging pipeline (bytes).
+// Chunks of the host<->device staging pipeline (bytes): sizes double from
+// kStageFirst up to kStageChunk, so that the host copy of the first chunk
+// (before any DMA can start) and of the last one (after the last DMA) are
+// short.
 constexpr size_t kStageChunk = size_t(4) << 20;
+constexpr size_t kStageFirst = size_t(512) << 10;
+
+// Chunk sizes of a transfer of `bytes`: ramping up from kStageFirst
+// (host -> device) or, reversed, ramping down to it (device -> host).
+std::vector<size_t> stage_chunks(size_t bytes, bool ramp_up) {
+  std::vector<size_t> sizes;
+  size_t c = kStageFirst;
+  for (size_t left = bytes; left > 0;) {
+    size_t const nb = std::min(c, left);
+    sizes.push_back(nb);
+    left -= nb;
+    c = std::min(2 * c, kStageChunk);
+  }
+  if (!ramp_up)
+    std::reverse(sizes.begin(), sizes.end());
+  return sizes;
+}
 
 // Process-wide host worker pool; calls from different handles take turns.
 HostPool &host_pool(std::unique_lock<std::mutex> &lk) {
@@ -790,14 +810,15 @@ static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *
   std::unique_lock<std::mutex> lk;
   HostPool &pool = host_pool(lk);
   auto push = [&](const void *src, void *dst, size_t nbytes, bool cached) {
-    for (size_t b0 = 0; b0 < nbytes; b0 += kStageChunk) {
-      size_t const nb = std::min(kStageChunk, nbytes - b0);
+    size_t b0 = 0;
+    for (size_t const nb : stage_chunks(nbytes, true)) {
       const char *s = static_cast<const char *>(src) + b0;
-      if (cached && pool.equal(pinned + b0, s, nb))
-        continue;
-      pool.copy(pinned + b0, s, nb);
-      P3MX_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + b0, pinned + b0, nb,
-                                cudaMemcpyHostToDevice, st));
+      if (!(cached && pool.equal(pinned + b0, s, nb))) {
+        pool.copy(pinned + b0, s, nb);
+        P3MX_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + b0, pinned + b0, nb,
+                                  cudaMemcpyHostToDevice, st));
+      }
+      b0 += nb;
     }
     pinned += nbytes;
   };
@@ -834,18 +855,21 @@ static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwr
   size_t const bytes = 3 * n * sizeof(double);
   h->h_out.ensure(bytes);
   double *o = h->h_out.as<double>();
-  size_t const nch = (bytes + kStageChunk - 1) / kStageChunk;
+  std::vector<size_t> const sizes = stage_chunks(bytes, false);
+  size_t const nch = sizes.size();
+  std::vector<size_t> off(nch + 1, 0);
+  for (size_t c = 0; c < nch; ++c)
+    off[c + 1] = off[c] + sizes[c];
   for (size_t c = 0; c < nch; ++c) {
-    size_t const b0 = c * kStageChunk, nb = std::min(kStageChunk, bytes - b0);
-    P3MX_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(o) + b0,
-                              reinterpret_cast<const char *>(e.d_force()) + b0, nb,
+    P3MX_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(o) + off[c],
+                              reinterpret_cast<const char *>(e.d_force()) + off[c], sizes[c],
                               cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaEventRecord(h->out_events.get(c), st));
   }
   std::unique_lock<std::mutex> lk;
   HostPool &pool = host_pool(lk);
   for (size_t c = 0; c < nch; ++c) {
-    size_t const b0 = c * kStageChunk, nb = std::min(kStageChunk, bytes - b0);
+    size_t const b0 = off[c], nb = sizes[c];
     P3MX_CUDA(cudaEventSynchronize(h->out_events.get(c)));
     if (overwrite) {
       pool.copy(reinterpret_cast<char *>(f) + b0, reinterpret_cast<const char *>(o) + b0, nb);

@@ -349,6 +349,11 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     // staged lines are padded (line_ld); every pass also holds its axis
     // twiddle table (n complex) in shared memory
     size_t const ldy = line_ld(maxM1), ldx = line_ld(maxM0);
+    // y pass: power-of-two lines of 32..256 transform in place (no scratch
+    // buffer)
+    bool yin = true;
+    for (auto const &G : m_geom)
+      yin = yin && fft_inplace_ok(G.mesh[1], 16, 256);
     m_tile_y = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, cap / ldy)));
     // x pass: three line buffers (phi, field lines, scratch) of T kz columns
     size_t const x_budget = 96 * 1024;
@@ -384,7 +389,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     }
     m_smem_zf = smem_zf;
     m_smem_zi = smem_zi;
-    m_smem_y = (2 * static_cast<size_t>(m_tile_y) * ldy + maxM1) * csz;
+    m_smem_y = ((yin ? 1 : 2) * static_cast<size_t>(m_tile_y) * ldy + maxM1) * csz;
     m_smem_x = (3 * static_cast<size_t>(m_tile_x) * ldx + maxM0) * csz;
     m_n_blk_zf = static_cast<int>(zf.size());
     m_n_blk_y = static_cast<int>(y.size());

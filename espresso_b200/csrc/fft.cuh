@@ -302,13 +302,71 @@ __device__ C *fft_2step(C *a, C *b, int nlines, int ld, const C *__restrict__ tw
   return b;
 }
 
+// In-place form of fft_2step for nlines * 16 <= blockDim.x (one item per
+// thread and step): step 2 reads its column into registers, the block
+// synchronises, then every thread writes its outputs back to `a`.
+template <typename C, int N1, int N2>
+__device__ C *fft_2step_inplace(C *a, int nlines, int ld, const C *__restrict__ tw, bool inv) {
+  int const it = threadIdx.x;
+  if (it < nlines * N2) {
+    int const l = it / N2, t = it - l * N2;
+    C *s = a + l * ld;
+    C v[N1];
+#pragma unroll
+    for (int m = 0; m < N1; ++m)
+      v[m] = s[pix(t + N2 * m)];
+    dft_pow2<C, N1>(v, inv);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      v[k1] = cmul(v[k1], ld_tw(tw, t * k1, inv));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1)
+      s[pix(t + N2 * k1)] = v[k1];
+  }
+  __syncthreads();
+  bool const act = it < nlines * N1;
+  int const l = it / N1, k1 = it - l * N1;
+  C v[N2];
+  if (act) {
+    const C *s = a + l * ld;
+#pragma unroll
+    for (int t = 0; t < N2; ++t)
+      v[t] = s[pix(t + N2 * k1)];
+    dft_pow2<C, N2>(v, inv);
+  }
+  __syncthreads();
+  if (act) {
+    C *d = a + l * ld;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2)
+      d[pix(k1 + N1 * k2)] = v[k2];
+  }
+  __syncthreads();
+  return a;
+}
+
+// True when lines of length n transform in place (fft_lines with b ==
+// nullptr): n a power of two in 32..256 and nlines * 16 <= threads.
+__host__ __device__ inline bool fft_inplace_ok(int n, int nlines, int threads) {
+  return (n == 32 || n == 64 || n == 128 || n == 256) && nlines * 16 <= threads;
+}
+
 // Full transform of nlines lines in `a` (scratch `b`; element i of line l at
 // l*ld + pix(i)); tw = the axis twiddle table (shared memory).  Returns the
-// buffer holding the result.  All threads of the block must call it.
+// buffer holding the result.  b == nullptr transforms in place (requires
+// fft_inplace_ok).  All threads of the block must call it.
 template <typename C>
 __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
                         const C *__restrict__ tw, bool inv) {
   int const n = pl.n;
+  if (b == nullptr) {
+    switch (n) {
+    case 32: return fft_2step_inplace<C, 16, 2>(a, nlines, ld, tw, inv);
+    case 64: return fft_2step_inplace<C, 16, 4>(a, nlines, ld, tw, inv);
+    case 128: return fft_2step_inplace<C, 16, 8>(a, nlines, ld, tw, inv);
+    default: return fft_2step_inplace<C, 16, 16>(a, nlines, ld, tw, inv);
+    }
+  }
   switch (n) {
   case 32: return fft_2step<C, 16, 2>(a, b, nlines, ld, tw, inv);
   case 64: return fft_2step<C, 16, 4>(a, b, nlines, ld, tw, inv);
@@ -436,9 +494,10 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
 }
 
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
-// Shared memory: 2 x tile staged lines of line_ld(M1), twiddles (M1).
+// Shared memory: tile staged lines of line_ld(M1) (two sets unless the
+// lines transform in place), twiddles (M1).
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2)
 k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
         typename CplxOf<Real>::type *__restrict__ c0, long long field_stride, int tile,
         bool inv, const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -452,9 +511,10 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   int const x = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
   int const ld = line_ld(M1);
+  bool const inplace = fft_inplace_ok(M1, tile, blockDim.x);
   C *a = reinterpret_cast<C *>(smem_raw);
-  C *b = a + tile * ld;
-  C *tw = b + tile * ld;
+  C *b = inplace ? nullptr : a + tile * ld;
+  C *tw = a + (inplace ? 1 : 2) * tile * ld;
   load_twiddles(tw, twtab, G.plan[1]);
   long long const rowbase = G.km_off + static_cast<long long>(x) * M1 * G.hp + kz0;
   long long const hp = G.hp;

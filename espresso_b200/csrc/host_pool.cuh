@@ -72,9 +72,9 @@ public:
     m_fn = nullptr;
   }
 
-  // Parallel memcpy, split into pieces of at least 256 KB.
+  // Parallel memcpy, split into pieces of at least 64 KB.
   void copy(void *dst, const void *src, size_t bytes) {
-    size_t const piece = std::max<size_t>(256 << 10, (bytes + size() - 1) / size());
+    size_t const piece = std::max<size_t>(64 << 10, (bytes + size() - 1) / size());
     int const n = static_cast<int>((bytes + piece - 1) / piece);
     run(n, [&](int i) {
       size_t const b0 = i * piece, b1 = std::min(bytes, b0 + piece);
@@ -84,7 +84,7 @@ public:
 
   // Parallel memcmp: true when the two byte ranges are equal.
   bool equal(const void *a, const void *b, size_t bytes) {
-    size_t const piece = std::max<size_t>(256 << 10, (bytes + size() - 1) / size());
+    size_t const piece = std::max<size_t>(64 << 10, (bytes + size() - 1) / size());
     int const n = static_cast<int>((bytes + piece - 1) / piece);
     std::atomic<bool> same{true};
     run(n, [&](int i) {

@@ -266,7 +266,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int2 const bk = bricks[blockIdx.x];
   RepGeom const &G = reps[bk.x];
-  constexpr int B = brick_edge<P>(), B3 = B * B * B, E = B + P - 1;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B;
   const int *st = start + G.brk_off;
   int const s0 = st[bk.y], s1 = st[bk.y + 1];
   if (s0 == s1)

@@ -383,6 +383,37 @@ __device__ inline void lj_wca(PairR<Real> const &p, Real dist, Real inv_d, Real 
   }
 }
 
+// Branch-free form of lj_wca for the FP32 kernel: every term is evaluated
+// and selected by its range test (the lanes of a warp, different particles,
+// would otherwise diverge on the tests); WCA only when the pair has it.
+__device__ inline void lj_wca_sel(PairR<float> const &p, float dist, float inv_d, float &fn,
+                                  float &en) {
+  {
+    float const r_off = dist - p.loff;
+    float const inv_off = rcp_r(r_off);
+    float const s = p.lsig * inv_off;
+    float const s2 = s * s;
+    float const f6 = s2 * s2 * s2;
+    bool const in = dist < p.lcut && dist > p.lmin;
+    fn += in ? 48.f * p.leps * f6 * (f6 - 0.5f) * (inv_off * inv_d) : 0.f;
+    en += in ? 4.f * p.leps * (f6 * f6 - f6 + p.lshift) : 0.f;
+  }
+  if (p.wcut > 0.f) {
+    float const s = p.wsig * inv_d;
+    float const s2 = s * s;
+    float const f6 = s2 * s2 * s2;
+    bool const in = dist < p.wcut;
+    fn += in ? 48.f * p.weps * f6 * (f6 - 0.5f) * (inv_d * inv_d) : 0.f;
+    en += in ? 4.f * p.weps * (f6 * f6 - f6 + 0.25f) : 0.f;
+  }
+}
+
+__device__ inline float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Pair kernel over the Verlet list: real-space Coulomb
 // (CoulombP3M::pair_force / pair_energy, p3m.hpp:146-180) plus LJ and WCA
 // (lj.hpp:41-60, wca.hpp:39-55).  Minimum-image difference in FP64, pair
@@ -443,6 +474,9 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
     int const cnt = nb_cnt[a];
     const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
     long long const base0 = G.p0;
+    // the particle itself with the zero cell offset (code 13: dc = 0)
+    unsigned const self_ent =
+        static_cast<unsigned>(a - G.p0) | (13u << kNbIndexBits);
     for (int k0 = 0; k0 < cnt; k0 += 8) {
       // one group of 8 entries: two 16-byte loads
       const int4 *gp = reinterpret_cast<const int4 *>(nbp + (static_cast<long long>(k0 >> 3) << 8));
@@ -454,17 +488,19 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
       int const kn = min(8, cnt - k0);
 #pragma unroll
       for (int h = 0; h < 8; h += 4) {
-        // the partners' positions, four gathers in flight
+        // entries past the count stand for the particle itself (zero
+        // distance: no term passes its range test), so no lane branches on
+        // the count; the partners' positions, four gathers in flight
+        unsigned eu[4];
         float4 pbv[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-          pbv[u] = (h + u < kn) ? spf[base0 + (ent[h + u] & kNbIndexMask)] : pa;
+        for (int u = 0; u < 4; ++u) {
+          eu[u] = (h + u < kn) ? ent[h + u] : self_ent;
+          pbv[u] = spf[base0 + (eu[u] & kNbIndexMask)];
+        }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          if (h + u >= kn)
-            continue;
-          unsigned const e = ent[h + u];
-          int const b = static_cast<int>(base0 + (e & kNbIndexMask));
+          unsigned const e = eu[u];
           int const code = static_cast<int>(e >> kNbIndexBits);
           float4 const pb = pbv[u];
           float4 const sh = shift[code];
@@ -472,33 +508,36 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
           Real const d1 = (pa.y - pb.y) + sh.y;
           Real const d2v = (pa.z - pb.z) + sh.z;
           Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
-          Real const inv_d = rsqrt_r(dist2);
+          Real const inv_d = rsqrt_approx(dist2);
           Real const dist = dist2 * inv_d;
-          Real fc = Real(0), ec = Real(0);
-          Real const qb = pb.w;
-          if (qb != Real(0) && pref_qa != Real(0) && dist < r_cut && dist > Real(0)) {
-            Real const adist = alpha * dist;
-            Real const ex = exp_r(-adist * adist);
-            Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
-            Real const asp =
-                t * (Real(0.254829592) +
-                     t * (Real(-0.284496736) +
-                          t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
-            Real const erfc_part_ri = asp * inv_d;
-            Real const pq = pref_qa * qb;
-            fc = pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d));
-            if constexpr (EV)
-              ec = pq * erfc_part_ri * ex;
-          }
+          bool const pos = dist2 > Real(0);
+          // Coulomb, evaluated for every entry and selected
+          Real const adist = alpha * dist;
+          Real const ex = exp_r(-adist * adist);
+          Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
+          Real const asp =
+              t * (Real(0.254829592) +
+                   t * (Real(-0.284496736) +
+                        t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
+          Real const erfc_part_ri = asp * inv_d;
+          Real const pq = pref_qa * pb.w;
+          bool const in_c = pos && dist < r_cut;
+          Real const fc = in_c ? pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d)) : Real(0);
+          Real ec = Real(0);
+          if constexpr (EV)
+            ec = in_c ? pq * erfc_part_ri * ex : Real(0);
           Real fn = Real(0), en = Real(0);
           if (one_type) {
             if (p0.active)
-              lj_wca(p0, dist, inv_d, fn, en);
+              lj_wca_sel(p0, dist, inv_d, fn, en);
           } else {
+            int const b = static_cast<int>(base0 + (e & kNbIndexMask));
             PairR<Real> const p(ia[ta * ntypes + stype[b]]);
             if (p.active)
-              lj_wca(p, dist, inv_d, fn, en);
+              lj_wca_sel(p, dist, inv_d, fn, en);
           }
+          fn = pos ? fn : Real(0);
+          en = pos ? en : Real(0);
           Real const ft = fc + fn;
           sx += ft * d0;
           sy += ft * d1;
