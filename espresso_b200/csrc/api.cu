@@ -789,8 +789,10 @@ int p3mx_set_pair_params(p3mx_handle *h, int ntypes, const p3mx_pair_params *tab
   });
 }
 
+// want_pos / want_qt select the positions and/or the charges and types (a
+// split used by the speculative path of p3mx_forces).
 static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *q, const int *type,
-                     bool dev, cudaStream_t st) {
+                     bool dev, cudaStream_t st, bool want_pos = true, bool want_qt = true) {
   Engine &e = *h->eng;
   if (dev || n == 0) {
     e.upload(pos, q, type, true, st);
@@ -822,7 +824,12 @@ static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *
     }
     pinned += nbytes;
   };
-  push(pos, e.d_pos(), 3 * n * sizeof(double), false);
+  if (want_pos)
+    push(pos, e.d_pos(), 3 * n * sizeof(double), false);
+  else
+    pinned += 3 * n * sizeof(double);
+  if (!want_qt)
+    return;
   push(q, e.d_q(), n * sizeof(double), h->staged_q);
   if (type) {
     push(type, e.d_type(), n * sizeof(int), h->staged_type);
@@ -832,6 +839,20 @@ static void stage_in(p3mx_handle *h, size_t n, const double *pos, const double *
   h->staged_n = n;
   h->staged_q = true;
   h->staged_type = (type != nullptr);
+}
+
+// True when the host arrays q and type (nullptr: all zero) equal the
+// staged copies of the last call, which are also on the device.
+static bool staged_match(p3mx_handle *h, size_t n, const double *q, const int *type) {
+  if (h->h_in.p == nullptr || h->staged_n != n || !h->staged_q ||
+      (type != nullptr) != h->staged_type)
+    return false;
+  const char *pinned = h->h_in.as<char>() + 3 * n * sizeof(double);
+  std::unique_lock<std::mutex> lk;
+  HostPool &pool = host_pool(lk);
+  if (!pool.equal(pinned, q, n * sizeof(double)))
+    return false;
+  return type == nullptr || pool.equal(pinned + n * sizeof(double), type, n * sizeof(int));
 }
 
 // Raise the error of a kernel whose bounded wait ran out (both engines).
@@ -960,12 +981,37 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
     bool const dev = flags & P3MX_DEVICE_PTRS;
     bool const ow = flags & P3MX_OVERWRITE;
-    stage_in(h, n, pos, q, type, dev, st);
     bool const want_e = energy3 && (flags & P3MX_ENERGY);
     bool const want_v = virial27 && (flags & P3MX_VIRIAL);
+    double *fd = (dev && f) ? f : e.d_force();
+    // Forces only from host arrays, with charges and types staged by an
+    // earlier call: the device computes with the staged copies while the
+    // host compares them with q and type; on a difference the changed
+    // chunks are uploaded and the forces computed again.  The comparison
+    // is thereby off the critical path of the common case (unchanged
+    // charges and types).
+    bool const spec = !dev && f && !want_e && !want_v && n > 0 && h->h_in.p &&
+                      h->staged_n == n && h->staged_q && (type != nullptr) == h->staged_type;
+    stage_in(h, n, pos, q, type, dev, st, true, !spec);
+    if (spec) {
+      auto forces = [&] {
+        if (h->prm.epsilon != 0.)
+          e.census(st);
+        e.forces_overlapped(fd, true, st);
+      };
+      forces();
+      if (!staged_match(h, n, q, type)) {
+        P3MX_CUDA(cudaStreamSynchronize(st));
+        stage_in(h, n, pos, q, type, dev, st, false, true);
+        forces();
+      }
+      stage_out(h, n, f, dev, ow, st);
+      P3MX_CUDA(cudaStreamSynchronize(st));
+      check_kernels(h, st);
+      return;
+    }
     if (want_e || h->prm.epsilon != 0.)
       e.census(st);
-    double *fd = (dev && f) ? f : e.d_force();
     std::vector<double> enk, virk, ens, virs;
     bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
     if (!want_e && !want_v) {

@@ -492,6 +492,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(int), st));
   }
   m_pos_ref.ensure(3 * n * sizeof(double));
+  m_type_ref.ensure(n * sizeof(int));
   m_part_pair.ensure(static_cast<size_t>(m_n_blk_pair) * 20 * sizeof(double));
   m_sums_pair.ensure(static_cast<size_t>(R) * 20 * sizeof(double));
   if (m_ia_d.p == nullptr)
@@ -827,6 +828,7 @@ void Engine::build_lists(cudaStream_t st) {
     layout_lists(st);
   }
   P3MX_CUDA(cudaMemcpyAsync(m_pos_ref.p, d_pos(), 3 * m_n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  P3MX_CUDA(cudaMemcpyAsync(m_type_ref.p, d_type(), m_n * sizeof(int), cudaMemcpyDeviceToDevice, st));
   m_lists_valid = true;
 }
 
@@ -865,7 +867,8 @@ void Engine::prepare_short_range(cudaStream_t st, bool need_spq) {
   if (!rebuild) {
     P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
     k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                             m_n, m_flag.as<int>(), nullptr); ++m_launches;
+                                             d_type(), m_type_ref.as<int>(), m_n,
+                                             m_flag.as<int>(), nullptr); ++m_launches;
     int flag = 0;
     P3MX_CUDA(cudaMemcpyAsync(&flag, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
@@ -1001,7 +1004,8 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   k_fill_int<<<1, 32, 0, st>>>(flag, 0, 1, nullptr); ++m_launches;
   k_fill_int<<<ceil_div(R, 256), 256, 0, st>>>(rflag, 0, R, nullptr); ++m_launches;
   k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                           m_n, flag, rflag); ++m_launches;
+                                           d_type(), m_type_ref.as<int>(), m_n, flag, rflag);
+  ++m_launches;
   k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag); ++m_launches;
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
                                  m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag,
@@ -1015,7 +1019,8 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
                                      m_overflow.as<int>(), flag, rflag); ++m_launches;
-  k_copy_pos_ref<<<nb, 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), m_rep_of.as<int>(), rflag, m_n,
+  k_copy_pos_ref<<<nb, 256, 0, st>>>(m_pos_ref.as<double>(), d_pos(), m_type_ref.as<int>(),
+                                     d_type(), m_rep_of.as<int>(), rflag, m_n,
                                      flag); ++m_launches;
   refresh_sorted_positions(st, !m_fp32);
   if (m_fp32)

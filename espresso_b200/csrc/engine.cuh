@@ -193,6 +193,7 @@ private:
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_rflag, m_part_pair, m_sums_pair;
+  DevBuf m_type_ref; // types at the last list build (a change triggers a rebuild)
   DevBuf m_kerr; // set by a kernel whose bounded wait ran out
   std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;

@@ -722,10 +722,14 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
 // Largest squared displacement since the last list build, as a flag:
 // set when any particle moved more than skin/2 (check_resort_required,
 // CellStructure.hpp:393-401).
+// A particle whose type differs from its type at the last build also
+// triggers the rebuild: the lists hold per-type-pair cutoffs and the sorted
+// types (as the reference resorts on a particle type change).
 __global__ void k_displacement_check(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                                      const double *__restrict__ pos, const double *__restrict__ pos_ref,
-                                     long long n, int *__restrict__ flag,
-                                     int *__restrict__ rflag) {
+                                     const int *__restrict__ type,
+                                     const int *__restrict__ type_ref, long long n,
+                                     int *__restrict__ flag, int *__restrict__ rflag) {
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n)
     return;
@@ -738,15 +742,17 @@ __global__ void k_displacement_check(const RepGeom *__restrict__ reps, const int
     d2 += dx * dx;
   }
   double const lim = 0.5 * G.skin;
-  if (d2 > lim * lim) {
+  if (d2 > lim * lim || type[i] != type_ref[i]) {
     atomicOr(flag, 1);
     if (rflag) // per-replica decision: only this replica rebuilds
       atomicOr(&rflag[r], 1);
   }
 }
 
-// Reference positions of the replicas that rebuilt (all when rflag is null).
+// Reference positions and types of the replicas that rebuilt (all when
+// rflag is null).
 __global__ void k_copy_pos_ref(double *__restrict__ pos_ref, const double *__restrict__ pos,
+                               int *__restrict__ type_ref, const int *__restrict__ type,
                                const int *__restrict__ rep_of, const int *__restrict__ rflag,
                                long long n, const int *__restrict__ cond) {
   if (cond && !*cond)
@@ -757,6 +763,7 @@ __global__ void k_copy_pos_ref(double *__restrict__ pos_ref, const double *__res
 #pragma unroll
   for (int d = 0; d < 3; ++d)
     pos_ref[3 * i + d] = pos[3 * i + d];
+  type_ref[i] = type[i];
 }
 
 } // namespace p3mx

@@ -320,9 +320,17 @@ def test_host_staging_chunks_accumulate_and_device_pointers():
     i_plus = int(np.flatnonzero(q2 > 0)[1000])
     i_minus = int(np.flatnonzero(q2 < 0)[-1000])
     q2[i_plus], q2[i_minus] = -q2[i_plus], -q2[i_minus]
+    # host call right after a host call: computed first with the staged
+    # charges, found changed, computed again
+    _lib.check(lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q), None,
+                               _lib.dptr(f_acc), None, None, flags, None), act._handle)
+    f2s = np.zeros((n, 3))
+    _lib.check(lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q2), None,
+                               _lib.dptr(f2s), None, None, flags, None), act._handle)
     f2 = np.zeros((n, 3))
     _lib.check(lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q2), None,
                                _lib.dptr(f2), None, None, flags, None), act._handle)
+    assert np.array_equal(f2s, f2)
     dq2 = torch.from_numpy(q2).cuda()
     torch.cuda.synchronize()
     _lib.check(lib.p3mx_forces(act._handle, n, dp.data_ptr(), dq2.data_ptr(), None, df.data_ptr(),
@@ -393,3 +401,44 @@ def test_forces_after_moves_across_the_boundary(cls, rtol):
         fr, _, _, _ = O.short_range(p, cur, q, None, 1, tab)
         ref = fk + fr
         np.testing.assert_allclose(f, ref, atol=rtol * np.abs(ref).max() * 10, rtol=0)
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_changed_types_and_charges_between_host_calls(cls):
+    """Host-pointer force calls compute first with the charges and types
+    staged by the previous call and compare them with the new arrays on the
+    host meanwhile; changed types or charges must still give, bit for bit,
+    the forces of a fresh system built with the new values."""
+    box = 10.0
+    pos, q = jittered_lattice(8, box, 0.2, seed=31)  # 512 ions
+    rng = np.random.default_rng(8)
+    t1 = rng.integers(0, 2, len(q)).astype(np.int32)
+    t2 = t1.copy()
+    t2[:40] = 1 - t2[:40]
+    q2 = q.copy()
+    q2[100:110] = -q2[100:110]
+
+    def system(types, charges):
+        s = make_system([box] * 3, pos, charges)
+        s.part.all().type = types
+        for (a, b), eps in {(0, 0): 1.0, (0, 1): 0.5, (1, 1): 2.0}.items():
+            s.non_bonded_inter[a, b].lennard_jones.set_params(epsilon=eps, sigma=1.0,
+                                                              cutoff=2.5, shift="auto")
+        s.electrostatics.solver = cls(prefactor=1.0, accuracy=1e-3, mesh=20, cao=5, alpha=1.0,
+                                      r_cut=3.0, tune=False)
+        return s
+
+    def forces(s):
+        s.integrator.run(0, recalc_forces=True)
+        return s.part.all().f.copy()
+
+    s = system(t1, q)
+    forces(s)
+    forces(s)  # staged charges and types unchanged
+    s.part.all().type = t2
+    f_t = forces(s)
+    assert np.array_equal(f_t, forces(system(t2, q)))
+    s.part.all().q = q2
+    f_q = forces(s)
+    assert np.array_equal(f_q, forces(system(t2, q2)))
+    assert not np.array_equal(f_t, f_q)
