@@ -468,13 +468,13 @@ def main():
         if rc:
             _lib.check(rc, h)
 
-    for _ in range(2):
+    for _ in range(3):
         step_host()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    k_e2e = max(3, args.steps // 3)
+    k_e2e = max(5, args.steps // 2)
     for _ in range(k_e2e):
         step_host()
     torch.cuda.synchronize(dev)

@@ -8,13 +8,40 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
+#if defined(__x86_64__) || defined(_M_X64)
+#include <emmintrin.h>
+#endif
 
 namespace p3mx {
+
+// memcpy with non-temporal (streaming) stores: the destination lines are
+// not read first, so a large copy moves 2 bytes of memory traffic per byte
+// instead of 3.  The stores are fenced before return.
+inline void copy_stream(void *dst, const void *src, size_t bytes) {
+#if defined(__x86_64__) || defined(_M_X64)
+  char *d = static_cast<char *>(dst);
+  const char *s = static_cast<const char *>(src);
+  size_t const head = std::min(bytes, (16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15);
+  std::memcpy(d, s, head);
+  d += head;
+  s += head;
+  bytes -= head;
+  size_t const n16 = bytes / 16;
+  for (size_t i = 0; i < n16; ++i)
+    _mm_stream_si128(reinterpret_cast<__m128i *>(d) + i,
+                     _mm_loadu_si128(reinterpret_cast<const __m128i *>(s) + i));
+  std::memcpy(d + 16 * n16, s + 16 * n16, bytes - 16 * n16);
+  _mm_sfence();
+#else
+  std::memcpy(dst, src, bytes);
+#endif
+}
 
 class HostPool {
 public:
@@ -72,13 +99,13 @@ public:
     m_fn = nullptr;
   }
 
-  // Parallel memcpy, split into pieces of at least 64 KB.
+  // Parallel copy with streaming stores, split into pieces of at least 64 KB.
   void copy(void *dst, const void *src, size_t bytes) {
     size_t const piece = std::max<size_t>(64 << 10, (bytes + size() - 1) / size());
     int const n = static_cast<int>((bytes + piece - 1) / piece);
     run(n, [&](int i) {
       size_t const b0 = i * piece, b1 = std::min(bytes, b0 + piece);
-      std::memcpy(static_cast<char *>(dst) + b0, static_cast<const char *>(src) + b0, b1 - b0);
+      copy_stream(static_cast<char *>(dst) + b0, static_cast<const char *>(src) + b0, b1 - b0);
     });
   }
 
