@@ -345,28 +345,33 @@ __device__ C *fft_2step_inplace(C *a, int nlines, int ld, const C *__restrict__ 
   return a;
 }
 
-// True when lines of length n transform in place (fft_lines with b ==
-// nullptr): n a power of two in 32..256 and nlines * 16 <= threads.
+// True when lines of length n transform in place (fft_lines_inplace): n a
+// power of two in 32..256 and nlines * 16 <= threads.
 __host__ __device__ inline bool fft_inplace_ok(int n, int nlines, int threads) {
   return (n == 32 || n == 64 || n == 128 || n == 256) && nlines * 16 <= threads;
 }
 
+// In-place transform of nlines lines in `a` (requires fft_inplace_ok);
+// returns a.  A separate function from fft_lines, so that kernels that never
+// transform in place do not carry its code (and registers).
+template <typename C>
+__device__ C *fft_lines_inplace(C *a, int nlines, int ld, AxisPlan const &pl,
+                                const C *__restrict__ tw, bool inv) {
+  switch (pl.n) {
+  case 32: return fft_2step_inplace<C, 16, 2>(a, nlines, ld, tw, inv);
+  case 64: return fft_2step_inplace<C, 16, 4>(a, nlines, ld, tw, inv);
+  case 128: return fft_2step_inplace<C, 16, 8>(a, nlines, ld, tw, inv);
+  default: return fft_2step_inplace<C, 16, 16>(a, nlines, ld, tw, inv);
+  }
+}
+
 // Full transform of nlines lines in `a` (scratch `b`; element i of line l at
 // l*ld + pix(i)); tw = the axis twiddle table (shared memory).  Returns the
-// buffer holding the result.  b == nullptr transforms in place (requires
-// fft_inplace_ok).  All threads of the block must call it.
+// buffer holding the result.  All threads of the block must call it.
 template <typename C>
 __device__ C *fft_lines(C *a, C *b, int nlines, int ld, AxisPlan const &pl,
                         const C *__restrict__ tw, bool inv) {
   int const n = pl.n;
-  if (b == nullptr) {
-    switch (n) {
-    case 32: return fft_2step_inplace<C, 16, 2>(a, nlines, ld, tw, inv);
-    case 64: return fft_2step_inplace<C, 16, 4>(a, nlines, ld, tw, inv);
-    case 128: return fft_2step_inplace<C, 16, 8>(a, nlines, ld, tw, inv);
-    default: return fft_2step_inplace<C, 16, 16>(a, nlines, ld, tw, inv);
-    }
-  }
   switch (n) {
   case 32: return fft_2step<C, 16, 2>(a, b, nlines, ld, tw, inv);
   case 64: return fft_2step<C, 16, 4>(a, b, nlines, ld, tw, inv);
@@ -537,7 +542,8 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     }
   }
   __syncthreads();
-  C *res = fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
+  C *res = inplace ? fft_lines_inplace<C>(a, T, ld, G.plan[1], tw, inv)
+                   : fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
   if (col)
     for (int y = yq; y < M1; y += 16)
       cm[rowbase + y * hp + tq] = res[tq * ld + pix(y)];
