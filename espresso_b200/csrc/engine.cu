@@ -602,6 +602,25 @@ void Engine::encode_field_maps(cudaStream_t st) {
 }
 
 namespace {
+// One colour launch of the charge assignment; `chained` launches it as a
+// programmatic dependent of the previous colour (see k_p3m_assign).
+template <typename Real, int P>
+void launch_assign(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
+                   int const *start, Real const *W, int const *s_key, Real *rho, int *err) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(cnt));
+  cfg.blockDim = dim3(32 * kAssignWarps);
+  cfg.dynamicSmemBytes = assign_smem<Real, P>();
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = chained ? 1 : 0;
+  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign<Real, P>, geom, tab, cnt, start, W, s_key, rho,
+                               err));
+}
+
 // Persistent grid of the back-interpolation pipeline: resident blocks per
 // SM times the SM count (computed once per kernel instance and process),
 // at most one block per brick.
@@ -680,15 +699,17 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 2. charge assignment: one warp per brick, colour by colour
   P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
   {
+    bool chained = false; // the first colour waits for the mesh memset normally
     for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
       int const cnt = m_phase_off[p + 1] - m_phase_off[p];
       if (cnt == 0)
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign<Real, P><<<cnt, 32 * kAssignWarps,
-                                   assign_smem<Real, P>(), st>>>(
-                                   geom, tab, cnt, m_start.as<int>(), m_W.as<Real>(),
-                                   m_skey.as<int>(), m_rho.as<Real>(), m_kerr.as<int>())));
+      P3MX_CAO_DISPATCH_R(cao, (launch_assign<Real, P>(chained, cnt, st, geom, tab,
+                                                       m_start.as<int>(), m_W.as<Real>(),
+                                                       m_skey.as<int>(), m_rho.as<Real>(),
+                                                       m_kerr.as<int>())));
+      chained = true;
       ++m_launches;
     }
   }

@@ -243,7 +243,12 @@ template <> __device__ inline double from_ll<double>(long long v) { return __ll2
 // Tiles are then added to the mesh; bricks of one launch share a colour
 // (greedy interval colouring per dimension), so the tiles of one launch never
 // overlap and plain read-add-write is race-free; colours run in a fixed
-// order, making the mesh reproducible.
+// order, making the mesh reproducible.  The colour launches are chained by
+// programmatic dependent launch: each block lets the next colour's grid start
+// (griddepcontrol.launch_dependents) as soon as it runs, so that grid fills
+// its tiles while this one drains, and waits (griddepcontrol.wait, the
+// completion and memory flush of the previous colour) only before its own
+// read-add-write of the mesh.
 template <typename Real, int P>
 __global__ void __launch_bounds__(32 * kAssignWarps)
 k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
@@ -261,6 +266,7 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[kAssignWarps];
   __shared__ __align__(8) unsigned long long bar;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (static_cast<int>(blockIdx.x) >= nbricks)
     return; // whole block
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -389,6 +395,8 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   }
   __syncthreads();
   Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
+  // the previous colour's flush has completed and is visible
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   // add the tile to the mesh: real extent of the brick plus the stencil
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
   int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
