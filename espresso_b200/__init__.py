@@ -6,7 +6,8 @@ the ctypes binding, the actor mirror (``electrostatics``), a minimal
 ``System`` for scripting and tests, and the batched-replica driver.
 """
 from . import electrostatics  # noqa: F401
+from . import interactions  # noqa: F401
 from ._lib import load as load_library  # noqa: F401
 from .system import System  # noqa: F401
 
-__all__ = ["System", "electrostatics", "load_library"]
+__all__ = ["System", "electrostatics", "interactions", "load_library"]

@@ -54,6 +54,15 @@ class PairParams(ctypes.Structure):
                 ("wca_eps", ctypes.c_double), ("wca_sig", ctypes.c_double)]
 
 
+P3MX_BOND_FENE = 1
+P3MX_BOND_HARMONIC = 2
+
+
+class BondParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("k", ctypes.c_double), ("r0", ctypes.c_double),
+                ("r_max", ctypes.c_double)]
+
+
 class BatchDesc(ctypes.Structure):
     _fields_ = [("n_rep", ctypes.c_int), ("box", ctypes.POINTER(ctypes.c_double)),
                 ("prefactor", ctypes.POINTER(ctypes.c_double)),
@@ -79,6 +88,9 @@ SIGNATURES = {
     "p3mx_get_tuned": (ctypes.c_int, [_vp, ctypes.POINTER(Tuned)]),
     "p3mx_long_range": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_set_pair_params": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(PairParams)]),
+    "p3mx_set_bonds": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(BondParams), _sz,
+                                      ctypes.POINTER(ctypes.c_int)]),
+    "p3mx_bond_observables": (ctypes.c_int, [_vp, _sz, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_short_range": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_forces": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_cell_grid": (ctypes.c_int, [_vp, _ip, _dp]),

@@ -135,6 +135,11 @@ struct p3mx_handle {
   // the device (unchanged chunks are not uploaded again)
   size_t staged_n = 0;
   bool staged_q = false, staged_type = false;
+  // pair bonds (p3mx_set_bonds): built into the engine's lists on the next
+  // call after a change (or after the engine was configured anew)
+  std::vector<BondParam> bond_types;
+  std::vector<int> bonds;
+  bool bonds_dirty = false;
   // charge census
   int n_charged = 0;
   double sum_q2 = 0, sum_q = 0;
@@ -620,6 +625,11 @@ void ensure_ready(p3mx_handle *h, size_t n) {
   if (n != h->n || !h->eng) {
     h->n = n;
     configure_engine(h);
+    h->bonds_dirty = !h->bonds.empty();
+  }
+  if (h->bonds_dirty) {
+    h->eng->set_bonds(h->bond_types, h->bonds, h->eng->stream());
+    h->bonds_dirty = false;
   }
 }
 
@@ -743,6 +753,53 @@ int p3mx_get_tuned(const p3mx_handle *h, p3mx_tuned *out) {
   out->rs_error = h->rs_err;
   out->ks_error = h->ks_err;
   return P3MX_OK;
+}
+
+int p3mx_set_bonds(p3mx_handle *h, int n_types, const p3mx_bond_params *types, size_t n_bonds,
+                   const int *bonds) {
+  return guarded(h, [&] {
+    if (n_types < 0 || (n_types > 0 && !types) || (n_bonds > 0 && !bonds))
+      throw Error(P3MX_EDOMAIN, "bond arrays missing");
+    std::vector<BondParam> t(static_cast<size_t>(n_types));
+    for (int k = 0; k < n_types; ++k) {
+      auto const &s = types[k];
+      if (s.kind != P3MX_BOND_FENE && s.kind != P3MX_BOND_HARMONIC)
+        throw Error(P3MX_EDOMAIN, "unknown bond kind " + std::to_string(s.kind));
+      if (s.kind == P3MX_BOND_FENE && !(s.r_max > 0.))
+        throw Error(P3MX_EDOMAIN, "FENE parameter 'd_r_max' has to be > 0");
+      if (s.r_max < 0. || s.r0 < 0.)
+        throw Error(P3MX_EDOMAIN, "bond lengths have to be >= 0");
+      t[k] = BondParam{s.kind == P3MX_BOND_FENE ? kBondFene : kBondHarmonic, s.k, s.r0, s.r_max};
+    }
+    for (size_t b = 0; b < n_bonds; ++b)
+      if (bonds[3 * b] < 0 || bonds[3 * b] >= n_types)
+        throw Error(P3MX_EDOMAIN, "bond type " + std::to_string(bonds[3 * b]) + " is not defined");
+    h->bond_types = std::move(t);
+    h->bonds.assign(bonds, bonds + 3 * n_bonds);
+    h->bonds_dirty = true;
+    if (h->eng && h->activated) {
+      h->eng->set_bonds(h->bond_types, h->bonds, h->eng->stream());
+      h->bonds_dirty = false;
+    }
+  });
+}
+
+int p3mx_bond_observables(p3mx_handle *h, size_t n, const double *pos, double *energy,
+                          double *virial9, unsigned flags, void *stream) {
+  return guarded(h, [&] {
+    ensure_ready(h, n);
+    Engine &e = *h->eng;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
+    double en = 0.0, vir[9];
+    if (n > 0)
+      e.upload_positions(pos, flags & P3MX_DEVICE_PTRS, st);
+    e.bond_observables(st, &en, vir);
+    if (energy)
+      *energy = en;
+    if (virial9)
+      for (int k = 0; k < 9; ++k)
+        virial9[k] = vir[k];
+  });
 }
 
 int p3mx_set_pair_params(p3mx_handle *h, int ntypes, const p3mx_pair_params *table) {
@@ -955,6 +1012,7 @@ int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos, const double *
     bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
     if (fd) {
       e.short_range(fd, dev ? ow : true, want && !obs64, st, &en, &vir);
+      e.bond_forces(fd, st);
     } else if (!(want && obs64)) {
       // energies only: compute into the scratch force buffer
       e.short_range(e.d_force(), true, want, st, &en, &vir);
@@ -970,6 +1028,7 @@ int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos, const double *
     if (fd)
       stage_out(h, n, f, dev, ow, st);
     P3MX_CUDA(cudaStreamSynchronize(st));
+    check_kernels(h, st);
   });
 }
 
@@ -1020,6 +1079,7 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     } else {
       e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &enk, &virk);
       e.short_range(fd, false, (want_e || want_v) && !obs64, st, &ens, &virs);
+      e.bond_forces(fd, st);
     }
     if (obs64 && (want_e || want_v)) {
       fp64_kspace_observables(h, st, want_e, want_v, enk, virk);

@@ -488,8 +488,8 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_rflag.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_flag.ensure(sizeof(int));
   if (m_kerr.p == nullptr) {
-    m_kerr.ensure(sizeof(int));
-    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(int), st));
+    m_kerr.ensure(4 * sizeof(int));
+    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, 4 * sizeof(int), st));
   }
   m_pos_ref.ensure(3 * n * sizeof(double));
   m_type_ref.ensure(n * sizeof(int));
@@ -952,6 +952,7 @@ void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
   if (m_n == 0 || m_profiling) {
     long_range(f, overwrite, false, false, st, nullptr, nullptr);
     short_range(f, false, false, st, nullptr, nullptr);
+    bond_forces(f, st);
     return;
   }
   if (m_side == nullptr) {
@@ -966,6 +967,7 @@ void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
     launch_pair<float>(f, overwrite, false, m_side);
   else
     launch_pair<double>(f, overwrite, false, m_side);
+  bond_forces(f, m_side);
   P3MX_CUDA(cudaEventRecord(m_ev_join, m_side));
   struct Reset {
     cudaEvent_t &ev;
@@ -1190,12 +1192,92 @@ double Engine::ks_error(const int *mesh, int cao, int n_c_part, double sum_q2, d
 void Engine::check_kernel_error(cudaStream_t st) {
   if (m_kerr.p == nullptr)
     return;
-  int flag = 0;
-  P3MX_CUDA(cudaMemcpyAsync(&flag, m_kerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int w[4] = {0, 0, 0, 0};
+  P3MX_CUDA(cudaMemcpyAsync(w, m_kerr.p, sizeof(w), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));
-  if (flag) {
-    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(int), st));
-    throw Error(3, "a bulk copy into shared memory did not complete within the wait limit");
+  if (w[0] || w[1]) {
+    P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, sizeof(w), st));
+    if (w[0])
+      throw Error(3, "a bulk copy into shared memory did not complete within the wait limit");
+    // bond_error.cpp:28-35 and the zero-distance messages of fene.hpp /
+    // harmonic.hpp (runtime errors in the reference)
+    if (w[1] == 1)
+      throw Error(2, "bond broken between particles " + std::to_string(w[2]) + ", " +
+                         std::to_string(w[3]));
+    throw Error(2, "Bond: Particles " + std::to_string(w[2]) + " and " + std::to_string(w[3]) +
+                       " have zero distance. This is most likely an error in the system "
+                       "setup.");
+  }
+}
+
+void Engine::set_bonds(std::vector<BondParam> const &types, std::vector<int> const &bonds,
+                       cudaStream_t st) {
+  long long const nb = static_cast<long long>(bonds.size() / 3);
+  m_nbonds = 0;
+  if (nb == 0)
+    return;
+  // CSR over particles, both ends of every bond, entries in bond order
+  std::vector<int> cnt(static_cast<size_t>(m_n) + 1, 0);
+  for (long long b = 0; b < nb; ++b) {
+    int const t = bonds[3 * b], i = bonds[3 * b + 1], j = bonds[3 * b + 2];
+    if (t < 0 || t >= static_cast<int>(types.size()))
+      throw Error(1, "bond type " + std::to_string(t) + " is not defined");
+    if (i < 0 || j < 0 || i >= m_n || j >= m_n || i == j)
+      throw Error(1, "bond between invalid particles " + std::to_string(i) + ", " +
+                         std::to_string(j));
+    ++cnt[i + 1];
+    ++cnt[j + 1];
+  }
+  for (long long i = 0; i < m_n; ++i)
+    cnt[i + 1] += cnt[i];
+  std::vector<int2> ent(static_cast<size_t>(2 * nb));
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  for (long long b = 0; b < nb; ++b) {
+    int const t = bonds[3 * b], i = bonds[3 * b + 1], j = bonds[3 * b + 2];
+    ent[fill[i]++] = make_int2(j, t);
+    ent[fill[j]++] = make_int2(i, t);
+  }
+  upload_vec(m_bstart, cnt, st);
+  upload_vec(m_bent, ent, st);
+  upload_vec(m_bparam, types, st);
+  m_bpart.ensure(static_cast<size_t>(ceil_div(m_n, 256)) * 10 * sizeof(double));
+  m_nbonds = nb;
+  m_bond_n = m_n;
+}
+
+void Engine::bond_forces(double *f, cudaStream_t st) {
+  if (m_nbonds == 0)
+    return;
+  if (m_bond_n != m_n)
+    throw Error(2, "bonds were set for a different particle count");
+  k_bond_forces<<<ceil_div(m_n, 256), 256, 0, st>>>(
+      m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(), m_bstart.as<int>(), m_bent.as<int2>(),
+      m_bparam.as<BondParam>(), m_n, f, m_kerr.as<int>());
+  ++m_launches;
+}
+
+void Engine::bond_observables(cudaStream_t st, double *energy, double *virial9) {
+  for (int k = 0; k < 9; ++k)
+    virial9[k] = 0.0;
+  *energy = 0.0;
+  if (m_nbonds == 0)
+    return;
+  if (m_bond_n != m_n)
+    throw Error(2, "bonds were set for a different particle count");
+  int const nblk = static_cast<int>(ceil_div(m_n, 256));
+  k_bond_observables<<<nblk, 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(),
+                                           m_bstart.as<int>(), m_bent.as<int2>(),
+                                           m_bparam.as<BondParam>(), m_n, m_bpart.as<double>(),
+                                           m_kerr.as<int>());
+  ++m_launches;
+  std::vector<double> part(static_cast<size_t>(nblk) * 10);
+  P3MX_CUDA(cudaMemcpyAsync(part.data(), m_bpart.p, part.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  check_kernel_error(st); // synchronises
+  for (int b = 0; b < nblk; ++b) {
+    *energy += part[10 * b];
+    for (int k = 0; k < 9; ++k)
+      virial9[k] += part[10 * b + 1 + k];
   }
 }
 

@@ -6,6 +6,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 #include "pair.cuh"
+#include "bonds.cuh"
 
 #include <memory>
 #include <string>
@@ -123,6 +124,13 @@ public:
   std::vector<std::pair<std::string, double>> profile(int reps, cudaStream_t st);
   // Throws if a kernel reported that a bounded wait ran out (synchronises st).
   void check_kernel_error(cudaStream_t st);
+  // Pair bonds (bonds.cuh): `bonds` holds (type, i, j) triples of particle
+  // indices; forces are added by the force paths, observables on request.
+  void set_bonds(std::vector<BondParam> const &types, std::vector<int> const &bonds,
+                 cudaStream_t st);
+  void bond_forces(double *f, cudaStream_t st);
+  void bond_observables(cudaStream_t st, double *energy, double *virial9);
+  bool has_bonds() const { return m_nbonds > 0; }
   // Number of kernels launched by this engine so far.
   long long launches() const { return m_launches; }
 
@@ -194,7 +202,11 @@ private:
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_rflag, m_part_pair, m_sums_pair;
   DevBuf m_type_ref; // types at the last list build (a change triggers a rebuild)
-  DevBuf m_kerr; // set by a kernel whose bounded wait ran out
+  // kernel error word: [0] a bounded wait ran out; [1] bond status (1 broken,
+  // 2 zero length), [2], [3] the two particles of the first failing bond
+  DevBuf m_kerr;
+  long long m_nbonds = 0, m_bond_n = 0; // bonds, particle count they were set for
+  DevBuf m_bstart, m_bent, m_bparam, m_bpart;
   std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;
   // misc host staging

@@ -1,6 +1,7 @@
 """Minimal host-side system mirroring the slice of ``espressomd.System`` that
 the P3M + short-range force path needs: particles (pos, q, type, v, f), box,
-periodicity, Verlet skin, LJ/WCA parameters, the electrostatics container,
+periodicity, Verlet skin, LJ/WCA parameters, FENE / harmonic bonds, the
+electrostatics container,
 ``integrator.run`` and ``analysis.energy/pressure/pressure_tensor``.
 
 Every force, energy and virial comes from libp3mx.so through the C ABI
@@ -16,6 +17,7 @@ import numpy as np
 
 from . import _lib
 from .electrostatics import P3M, _P3MBase
+from .interactions import BondedInteractions
 
 
 class CellSystem:
@@ -136,6 +138,35 @@ class ParticleHandle:
     def id(self):
         return int(np.atleast_1d(self._idx)[0]) if np.ndim(self._idx) == 0 else None
 
+    def _index(self):
+        if isinstance(self._idx, slice) or np.ndim(self._idx) != 0:
+            raise ValueError("bonds belong to single particles")
+        return int(self._idx)
+
+    def add_bond(self, bond):
+        """bond = (bond object, partner particle or id), as in espressomd."""
+        obj, partner = bond
+        j = partner._index() if isinstance(partner, ParticleHandle) else int(partner)
+        self._pl._system.bonded_inter._id(obj)
+        i = self._index()
+        if not 0 <= j < len(self._pl):
+            raise ValueError("bond partner %d does not exist" % j)
+        self._pl._bonds.append((obj, i, j))
+        self._pl._system._bonds_changed()
+
+    @property
+    def bonds(self):
+        i = self._index()
+        return tuple((obj, j) for obj, a, j in self._pl._bonds if a == i)
+
+    @bonds.setter
+    def bonds(self, value):
+        i = self._index()
+        self._pl._bonds = [b for b in self._pl._bonds if b[1] != i]
+        self._pl._system._bonds_changed()
+        for bond in value:
+            self.add_bond(bond)
+
 
 class ParticleList:
     def __init__(self, system):
@@ -149,7 +180,10 @@ class ParticleList:
         self._q = np.zeros(0)
         self._type = np.zeros(0, dtype=np.int32)
         self._mass = np.zeros(0)
+        self._bonds = []  # (bond object, owner index, partner index)
         self._system._touch("all")
+        if hasattr(self._system, "_bond_version"):
+            self._system._bonds_changed()
 
     def add(self, pos, q=None, type=None, v=None, mass=None):
         pos = np.asarray(pos, dtype=float)
@@ -241,9 +275,10 @@ class Analysis:
         s = self._system
         e3, _ = s._calc_observables(energy=True)
         kin = 0.5 * float((s.part._mass[:, None] * s.part._v ** 2).sum())
+        eb, _ = s._bond_observables()
         out = {"kinetic": kin, "coulomb": e3[0] + e3[1], "non_bonded": e3[2],
-               "bonded": 0.0}
-        out["total"] = kin + out["coulomb"] + out["non_bonded"]
+               "bonded": eb}
+        out["total"] = kin + out["coulomb"] + out["non_bonded"] + out["bonded"]
         return out
 
     def pressure_tensor(self):
@@ -251,9 +286,10 @@ class Analysis:
         _, v27 = s._calc_observables(virial=True)
         V = float(np.prod(s.box_l))
         kin = np.einsum("i,ij,ik->jk", s.part._mass, s.part._v, s.part._v)
+        _, vb = s._bond_observables()
         out = {"kinetic": kin / V, "coulomb": (v27[0] + v27[1]) / V,
-               "non_bonded": v27[2] / V, "bonded": np.zeros((3, 3))}
-        out["total"] = out["kinetic"] + out["coulomb"] + out["non_bonded"]
+               "non_bonded": v27[2] / V, "bonded": vb / V}
+        out["total"] = out["kinetic"] + out["coulomb"] + out["non_bonded"] + out["bonded"]
         return out
 
     def pressure(self):
@@ -270,7 +306,9 @@ class System:
         self.cell_system = CellSystem()
         self._sr_handle = None
         self._pairs_dirty = True
+        self._bond_version = 0
         self.part = ParticleList(self)
+        self.bonded_inter = BondedInteractions(self)
         self.non_bonded_inter = NonBondedInteractions(self)
         self.electrostatics = Electrostatics(self)
         self.integrator = Integrator(self)
@@ -293,6 +331,53 @@ class System:
 
     def _touch(self, what):
         pass
+
+    def _bonds_changed(self):
+        self._bond_version += 1
+
+    def _sync_bonds(self, actor):
+        """Send the bond list to the actor's handle when it changed since the
+        last call on that actor (p3mx_set_bonds)."""
+        if getattr(actor, "_bonds_of", None) is self and actor._bond_version == self._bond_version:
+            return
+        handle = actor._handle
+        bonds = self.part._bonds
+        kinds = self.bonded_inter
+        types = (_lib.BondParams * max(1, len(kinds)))()
+        for t in range(len(kinds)):
+            types[t] = kinds[t].c_params()
+        trip = np.array([(kinds._id(o), i, j) for o, i, j in bonds], dtype=np.int32).reshape(-1)
+        rc = _lib.load().p3mx_set_bonds(
+            handle, len(kinds), types, len(bonds),
+            trip.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if len(bonds) else None)
+        _lib.check(rc, handle)
+        actor._bonds_of, actor._bond_version = self, self._bond_version
+
+    def _force_actor(self):
+        """Actor whose handle takes the force calls: the Coulomb solver, else
+        the short-range one when pair or bonded interactions exist."""
+        if self.electrostatics.solver is not None:
+            return self.electrostatics.solver
+        if (self.non_bonded_inter.active() or self.part._bonds) and len(self.part) > 0:
+            return self._short_range_handle()
+        return None
+
+    def _bond_observables(self):
+        """Bonded energy and virial tensor (sum of F (x) d)."""
+        if not self.part._bonds:
+            return 0.0, np.zeros((3, 3))
+        act = self._force_actor()
+        self._sync_bonds(act)
+        h = act._handle
+        pos = _lib.as_f64(self.part._pos)
+        e = np.zeros(1)
+        v = np.zeros(9)
+        rc = _lib.load().p3mx_bond_observables(h, len(self.part), _lib.dptr(pos),
+                                               e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               0, None)
+        _lib.check(rc, h)
+        return float(e[0]), v.reshape(3, 3)
 
     # -- force engine plumbing --------------------------------------------
     def _short_range_handle(self):
@@ -325,14 +410,16 @@ class System:
         if solver is not None:
             h = solver._handle
             self._sync_pairs(h, t)
+            self._sync_bonds(solver)
             rc = lib.p3mx_forces(h, n, _lib.dptr(pos), _lib.dptr(q), _lib.dptr(t), _lib.dptr(f),
                                  e3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                  v27.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), flags, None)
             _lib.check(rc, h)
-        elif self.non_bonded_inter.active() and n > 0:
+        elif (self.non_bonded_inter.active() or self.part._bonds) and n > 0:
             act = self._short_range_handle()
             h = act._handle
             self._sync_pairs(h, t)
+            self._sync_bonds(act)
             e2 = np.zeros(2)
             v18 = np.zeros(18)
             zero_q = np.zeros(n)

@@ -138,6 +138,33 @@ int p3mx_short_range(p3mx_handle *h, size_t n, const double *pos,
                      double *energy2, double *virial18, unsigned flags,
                      void *stream);
 
+/* Pair bonds: FENE (bonded_interactions/fene.hpp:37-105) and harmonic
+ * (harmonic.hpp:35-93) over the minimum-image vector d = x_i - x_j, i
+ * getting F(d) and j -F(d) (add_bonded_two_body_force,
+ * forces_inline.hpp:320-350).  types[t] describes bond type t; bonds[3b] =
+ * type, bonds[3b+1] = i, bonds[3b+2] = j (particle indices).  The call
+ * replaces the bonds set before (n_bonds 0 clears them).  p3mx_forces and
+ * p3mx_short_range add the bond forces; a bond stretched past its range
+ * fails the call with P3MX_ERUNTIME and "bond broken between particles i,
+ * j" (bond_error.cpp:28-35), a zero-length bond with r0 > 0 likewise (the
+ * reference's zero-distance runtime error).  No counterpart in the
+ * reference's GPU path, which has no bonded kernels. */
+#define P3MX_BOND_FENE 1
+#define P3MX_BOND_HARMONIC 2
+typedef struct {
+  int kind;     /* P3MX_BOND_FENE or P3MX_BOND_HARMONIC */
+  double k;     /* spring constant */
+  double r0;    /* equilibrium length */
+  double r_max; /* FENE: d_r_max (largest r - r0); harmonic: r_cut (0: none) */
+} p3mx_bond_params;
+int p3mx_set_bonds(p3mx_handle *h, int n_types, const p3mx_bond_params *types,
+                   size_t n_bonds, const int *bonds);
+/* Bonded energy and virial (sum over bonds of F (x) d, 3x3) of the
+ * configuration pos (device pointer with P3MX_DEVICE_PTRS in flags). */
+int p3mx_bond_observables(p3mx_handle *h, size_t n, const double *pos,
+                          double *energy, double *virial9, unsigned flags,
+                          void *stream);
+
 /* Full force evaluation in one call: one upload of pos/q/type, the
  * k-space and short-range pipelines, one download of the forces --
  * System::calculate_forces for the non-bonded + electrostatic part

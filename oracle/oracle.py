@@ -231,3 +231,55 @@ def ewald(box, pos, q, prefactor, alpha, r_cut, kmax, epsilon=0.0):
     lib.oracle_ewald(_d(box), len(q), _d(pos), _d(q), prefactor, alpha, r_cut,
                      int(kmax), epsilon, _d(f), _d(e))
     return f, e[0]
+
+
+BOND_FENE = 1
+BOND_HARMONIC = 2
+
+
+def bonds(box, pos, bond_types, bond_list):
+    """Pair bonds, restated from the reference in FP64 numpy: FENE
+    (bonded_interactions/fene.hpp:67-103), harmonic (harmonic.hpp:62-92),
+    applied as add_bonded_two_body_force does (forces_inline.hpp:320-350):
+    d = get_mi_vector(x_i, x_j) (BoxGeometry.hpp:47-60), F = fac(|d|) d on i,
+    -F on j, virial sum F (x) d (pressure.cpp bonded contribution).
+
+    bond_types: list of (kind, k, r0, r_max) with kind BOND_FENE (r_max =
+    d_r_max) or BOND_HARMONIC (r_max = r_cut, 0 for none); bond_list: (B, 3)
+    ints (type, i, j).  Returns forces (N, 3), energy, virial (3, 3); raises
+    RuntimeError("bond broken ...") for a bond past its range and for a
+    zero-length bond with r0 > 0, as the reference's runtime errors do.
+    """
+    box = np.asarray(box, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    bl = np.asarray(bond_list, dtype=np.int64).reshape(-1, 3)
+    f = np.zeros_like(pos)
+    energy = 0.0
+    vir = np.zeros((3, 3))
+    for t, i, j in bl:
+        kind, k, r0, r_max = bond_types[t]
+        d = pos[i] - pos[j]
+        far = np.abs(d) > 0.5 * box
+        d = np.where(far, d - np.rint(d / box) * box, d)
+        ln = np.sqrt(d @ d)
+        dr = ln - r0
+        if kind == BOND_FENE:
+            if dr >= r_max:
+                raise RuntimeError("bond broken between particles %d, %d" % (i, j))
+            fac = -k * dr / (1.0 - dr * dr / r_max ** 2)
+            e = -0.5 * k * r_max ** 2 * np.log(1.0 - dr * dr / r_max ** 2)
+        else:
+            if r_max > 0.0 and ln > r_max:
+                raise RuntimeError("bond broken between particles %d, %d" % (i, j))
+            fac = -k * dr
+            e = 0.5 * k * dr * dr
+        if ln > 1e-14:
+            fac /= ln
+        elif r0 > 0.0:
+            raise RuntimeError("particles %d, %d have zero distance" % (i, j))
+        force = fac * d
+        f[i] += force
+        f[j] -= force
+        energy += e
+        vir += np.outer(force, d)
+    return f, energy, vir
