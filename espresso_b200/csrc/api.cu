@@ -2,6 +2,7 @@
 // parameter validation with the reference's messages, the P3M tuner, and
 // host<->device staging.  No exception crosses the ABI.
 #include "../../include/p3mx.h"
+#include "bond_abi.cuh"
 #include "engine.cuh"
 #include "host_pool.cuh"
 
@@ -758,23 +759,7 @@ int p3mx_get_tuned(const p3mx_handle *h, p3mx_tuned *out) {
 int p3mx_set_bonds(p3mx_handle *h, int n_types, const p3mx_bond_params *types, size_t n_bonds,
                    const int *bonds) {
   return guarded(h, [&] {
-    if (n_types < 0 || (n_types > 0 && !types) || (n_bonds > 0 && !bonds))
-      throw Error(P3MX_EDOMAIN, "bond arrays missing");
-    std::vector<BondParam> t(static_cast<size_t>(n_types));
-    for (int k = 0; k < n_types; ++k) {
-      auto const &s = types[k];
-      if (s.kind != P3MX_BOND_FENE && s.kind != P3MX_BOND_HARMONIC)
-        throw Error(P3MX_EDOMAIN, "unknown bond kind " + std::to_string(s.kind));
-      if (s.kind == P3MX_BOND_FENE && !(s.r_max > 0.))
-        throw Error(P3MX_EDOMAIN, "FENE parameter 'd_r_max' has to be > 0");
-      if (s.r_max < 0. || s.r0 < 0.)
-        throw Error(P3MX_EDOMAIN, "bond lengths have to be >= 0");
-      t[k] = BondParam{s.kind == P3MX_BOND_FENE ? kBondFene : kBondHarmonic, s.k, s.r0, s.r_max};
-    }
-    for (size_t b = 0; b < n_bonds; ++b)
-      if (bonds[3 * b] < 0 || bonds[3 * b] >= n_types)
-        throw Error(P3MX_EDOMAIN, "bond type " + std::to_string(bonds[3 * b]) + " is not defined");
-    h->bond_types = std::move(t);
+    h->bond_types = bond_types_from_abi(n_types, types, n_bonds, bonds);
     h->bonds.assign(bonds, bonds + 3 * n_bonds);
     h->bonds_dirty = true;
     if (h->eng && h->activated) {

@@ -4,6 +4,7 @@
 // (The reference has no batched path: every replica would be one ESPResSo
 // System running its own MPI job.)
 #include "../../include/p3mx.h"
+#include "bond_abi.cuh"
 #include "engine.cuh"
 
 #include <algorithm>
@@ -370,6 +371,7 @@ void batch_forces(p3mx_batch *b, cudaStream_t st, bool graph_mode) {
     e.short_range_graph(e.d_force(), false, st);
   else
     e.short_range(e.d_force(), false, false, st, nullptr, nullptr);
+  e.bond_forces(e.d_force(), st);
 }
 
 } // namespace
@@ -535,9 +537,12 @@ int p3mx_batch_forces(p3mx_batch *b, double *energy_out) {
     std::vector<double> ek, es;
     e.long_range(e.d_force(), true, energy_out != nullptr, false, st, &ek, nullptr);
     e.short_range(e.d_force(), false, energy_out != nullptr, st, &es, nullptr);
-    if (energy_out)
+    e.bond_forces(e.d_force(), st);
+    if (energy_out) {
+      std::vector<double> const eb = e.bond_energies(st);
       for (int r = 0; r < R; ++r)
-        energy_out[r] = ek[r] + es[2 * r] + es[2 * r + 1];
+        energy_out[r] = ek[r] + es[2 * r] + es[2 * r + 1] + eb[r];
+    }
     P3MX_CUDA(cudaStreamSynchronize(st));
     e.check_kernel_error(st);
     b->forces_valid = true;
@@ -599,6 +604,32 @@ int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT, double gamma,
     e.check_kernel_error(st);
     if (e.list_overflow(st))
       throw Error(P3MX_ERUNTIME, "Verlet list capacity exceeded during the graph run");
+  });
+}
+
+int p3mx_batch_set_bonds(p3mx_batch *b, int n_types, const p3mx_bond_params *types,
+                         size_t n_bonds, const int *bonds) {
+  return bguard(b, [&] {
+    std::vector<BondParam> const t = bond_types_from_abi(n_types, types, n_bonds, bonds);
+    // both partners of a bond in one replica (offsets are replica starts)
+    auto rep = [&](int i) {
+      return static_cast<int>(std::upper_bound(b->off.begin(), b->off.end(),
+                                               static_cast<long long>(i)) -
+                              b->off.begin()) - 1;
+    };
+    for (size_t k = 0; k < n_bonds; ++k)
+      if (rep(bonds[3 * k + 1]) != rep(bonds[3 * k + 2]))
+        throw Error(P3MX_EDOMAIN, "bond between particles " + std::to_string(bonds[3 * k + 1]) +
+                                      " and " + std::to_string(bonds[3 * k + 2]) +
+                                      " of different replicas");
+    Engine &e = *b->eng;
+    e.set_bonds(t, std::vector<int>(bonds, bonds + 3 * n_bonds), e.stream());
+    // the captured step holds the old bond tables (or none): capture anew
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->forces_valid = false;
   });
 }
 

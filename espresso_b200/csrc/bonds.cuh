@@ -105,6 +105,33 @@ __global__ void k_bond_forces(const RepGeom *__restrict__ reps, const int *__res
   f[3 * i + 2] += fz;
 }
 
+// Bond energy of every particle (half of each of its bonds; a bond is seen
+// from both ends), for per-replica sums on the host.
+__global__ void k_bond_energy_pp(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                                 const double *__restrict__ pos, const int *__restrict__ bstart,
+                                 const int2 *__restrict__ bent, const BondParam *__restrict__ bp,
+                                 long long n, double *__restrict__ e_pp, int *__restrict__ err) {
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  RepGeom const &G = reps[rep_of[i]];
+  double acc = 0.0;
+  for (int e = bstart[i]; e < bstart[i + 1]; ++e) {
+    int2 const en = bent[e];
+    double d[3];
+    bond_vector(G, pos, i, en.x, d);
+    double const len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double fac = 0.0, energy = 0.0;
+    int const st = bond_eval(bp[en.y], len, fac, energy);
+    if (st != 0) {
+      bond_report(err, st, static_cast<int>(i), en.x);
+      continue;
+    }
+    acc += 0.5 * energy;
+  }
+  e_pp[i] = acc;
+}
+
 // Bonded energy and virial (sum over bonds of F (x) d): each bond is seen
 // from both ends with the same F (x) d, so every end adds half.  Per-block
 // partials[block * 10 + {E, V00..V22}], reduced in a fixed order.

@@ -1256,6 +1256,28 @@ void Engine::bond_forces(double *f, cudaStream_t st) {
   ++m_launches;
 }
 
+std::vector<double> Engine::bond_energies(cudaStream_t st) {
+  std::vector<double> out(m_geom.size(), 0.0);
+  if (m_nbonds == 0)
+    return out;
+  if (m_bond_n != m_n)
+    throw Error(2, "bonds were set for a different particle count");
+  DevBuf e_pp;
+  e_pp.ensure(static_cast<size_t>(m_n) * sizeof(double));
+  k_bond_energy_pp<<<ceil_div(m_n, 256), 256, 0, st>>>(
+      m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(), m_bstart.as<int>(), m_bent.as<int2>(),
+      m_bparam.as<BondParam>(), m_n, e_pp.as<double>(), m_kerr.as<int>());
+  ++m_launches;
+  std::vector<double> h(static_cast<size_t>(m_n));
+  P3MX_CUDA(cudaMemcpyAsync(h.data(), e_pp.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            st));
+  check_kernel_error(st); // synchronises
+  for (size_t r = 0; r < m_geom.size(); ++r)
+    for (long long i = m_geom[r].p0; i < m_geom[r].p0 + m_geom[r].np; ++i)
+      out[r] += h[static_cast<size_t>(i)];
+  return out;
+}
+
 void Engine::bond_observables(cudaStream_t st, double *energy, double *virial9) {
   for (int k = 0; k < 9; ++k)
     virial9[k] = 0.0;

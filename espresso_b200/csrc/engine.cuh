@@ -130,6 +130,8 @@ public:
                  cudaStream_t st);
   void bond_forces(double *f, cudaStream_t st);
   void bond_observables(cudaStream_t st, double *energy, double *virial9);
+  // bonded energy of every replica (zeros without bonds); synchronises
+  std::vector<double> bond_energies(cudaStream_t st);
   bool has_bonds() const { return m_nbonds > 0; }
   // Number of kernels launched by this engine so far.
   long long launches() const { return m_launches; }

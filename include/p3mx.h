@@ -256,6 +256,13 @@ int p3mx_batch_get_tuned(const p3mx_batch *b, int r, p3mx_tuned *out);
 /* One force evaluation for all replicas (forces overwritten, device
  * resident); optional per-replica energies (n_rep doubles, host). */
 int p3mx_batch_forces(p3mx_batch *b, double *energy_out);
+/* Pair bonds of the batch, as p3mx_set_bonds with particle indices over the
+ * whole batch (both partners in one replica); forces enter
+ * p3mx_batch_forces and the graph step of p3mx_batch_run (captured anew
+ * after this call), bonded energies the per-replica energy_out. */
+int p3mx_batch_set_bonds(p3mx_batch *b, int n_types,
+                         const p3mx_bond_params *types, size_t n_bonds,
+                         const int *bonds);
 /* Velocity-Verlet + Langevin (kT, gamma, dt) for `steps` steps, captured
  * in a CUDA graph after the first step.  Positions stay FP64 on device. */
 int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT,

@@ -180,3 +180,64 @@ def test_batch_forces_after_langevin_run_match_oracle():
             np.testing.assert_allclose(f[sl], ref, atol=3e-5 * np.abs(ref).max(), rtol=0)
     finally:
         lib.p3mx_batch_destroy(h)
+
+
+def _nearest_bonds(pos, offs, boxes):
+    """One bond per particle of the first half of every replica, to its
+    nearest neighbour in the replica (minimum image); global indices."""
+    out = []
+    for r in range(len(offs) - 1):
+        a, b = int(offs[r]), int(offs[r + 1])
+        p = pos[a:b]
+        L = boxes[r]
+        for i in range((b - a) // 2):
+            d = p - p[i]
+            d -= np.rint(d / L) * L
+            d2 = (d * d).sum(1)
+            d2[i] = np.inf
+            out.append((0, a + i, a + int(np.argmin(d2))))
+    return np.array(out, dtype=np.int32)
+
+
+def test_batch_bonds_in_the_graph_step_match_oracle():
+    """FENE bonds inside every replica: p3mx_batch_set_bonds, 40 graph-captured
+    Langevin steps, then forces and per-replica energies (bonded included)
+    against the FP64 oracle; a bond across replicas is rejected."""
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas(seed=21, n_rep=3)
+    h = create(boxes, prefs, pos, q, offs, cao=(5, 5))
+    try:
+        bonds = _nearest_bonds(pos, offs, boxes)
+        kf, drmax = 10.0, 2.5
+        types = (_lib.BondParams * 1)()
+        types[0] = _lib.BondParams(_lib.P3MX_BOND_FENE, kf, 0.0, drmax)
+        bad = np.array([0, int(offs[0]), int(offs[1])], dtype=np.int32)
+        assert lib.p3mx_batch_set_bonds(h, 1, types, 1, bad.ctypes.data_as(_P(ctypes.c_int))) != 0
+        assert lib.p3mx_batch_set_bonds(h, 1, types, len(bonds),
+                                        bonds.ctypes.data_as(_P(ctypes.c_int))) == 0
+        assert lib.p3mx_batch_run(h, 40, 0.005, 1.0, 1.0, 7) == 0
+        R = len(prefs)
+        en = np.zeros(R)
+        assert lib.p3mx_batch_forces(h, en.ctypes.data_as(_P(ctypes.c_double))) == 0
+        x = np.zeros_like(pos)
+        f = np.zeros_like(pos)
+        assert lib.p3mx_batch_get(h, x.ctypes.data_as(_P(ctypes.c_double)),
+                                  f.ctypes.data_as(_P(ctypes.c_double)), None) == 0
+        assert np.abs(x - pos).max() > 0.05
+        tab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
+        for r in range(R):
+            t = tuned(h, r)
+            a, b = int(offs[r]), int(offs[r + 1])
+            sl = slice(a, b)
+            mine = bonds[(bonds[:, 1] >= a) & (bonds[:, 1] < b)].copy()
+            mine[:, 1:] -= a
+            p = O.make_params(boxes[r], list(t.mesh), t.cao, t.alpha, t.r_cut, prefs[r])
+            fk, ek, _ = O.p3m_kspace(p, x[sl], q[sl])
+            fr, er, _, _ = O.short_range(p, x[sl], q[sl], None, 1, tab)
+            fb, eb, _ = O.bonds(boxes[r], x[sl], [(O.BOND_FENE, kf, 0.0, drmax)], mine)
+            ref = fk + fr + fb
+            np.testing.assert_allclose(f[sl], ref, atol=3e-5 * np.abs(ref).max(), rtol=0)
+            e_ref = ek + er[0] + er[1] + eb
+            assert abs(en[r] - e_ref) <= 1e-4 * (abs(e_ref) + np.abs(ek) + 1.0)
+    finally:
+        lib.p3mx_batch_destroy(h)
