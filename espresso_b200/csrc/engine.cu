@@ -117,6 +117,8 @@ Engine::~Engine() {
     cudaEventDestroy(m_ev_fork);
   if (m_ev_join)
     cudaEventDestroy(m_ev_join);
+  if (m_ev_kdone)
+    cudaEventDestroy(m_ev_kdone);
   if (m_side)
     cudaStreamDestroy(m_side);
   if (m_stream)
@@ -956,25 +958,35 @@ void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
     return;
   }
   if (m_side == nullptr) {
-    P3MX_CUDA(cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking));
+    // the k-space chain (many dependent launches, each with a tail) runs at
+    // the highest stream priority; the pair kernel's blocks fill the SMs
+    // its tails and launch gaps leave free
+    int lo = 0, hi = 0;
+    P3MX_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    P3MX_CUDA(cudaStreamCreateWithPriority(&m_side, cudaStreamNonBlocking, hi));
     P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_fork, cudaEventDisableTiming));
     P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_join, cudaEventDisableTiming));
+    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_kdone, cudaEventDisableTiming));
   }
   prepare_short_range(st, !m_fp32);
   P3MX_CUDA(cudaEventRecord(m_ev_fork, st));
   P3MX_CUDA(cudaStreamWaitEvent(m_side, m_ev_fork, 0));
+  // pair (+ bond) forces on the caller's stream; the interpolation, which
+  // adds onto them, waits for m_ev_join
   if (m_fp32)
-    launch_pair<float>(f, overwrite, false, m_side);
+    launch_pair<float>(f, overwrite, false, st);
   else
-    launch_pair<double>(f, overwrite, false, m_side);
-  bond_forces(f, m_side);
-  P3MX_CUDA(cudaEventRecord(m_ev_join, m_side));
+    launch_pair<double>(f, overwrite, false, st);
+  bond_forces(f, st);
+  P3MX_CUDA(cudaEventRecord(m_ev_join, st));
   struct Reset {
     cudaEvent_t &ev;
     ~Reset() { ev = nullptr; }
   } reset{m_interp_wait};
   m_interp_wait = m_ev_join;
-  long_range(f, false, false, false, st, nullptr, nullptr);
+  long_range(f, false, false, false, m_side, nullptr, nullptr);
+  P3MX_CUDA(cudaEventRecord(m_ev_kdone, m_side));
+  P3MX_CUDA(cudaStreamWaitEvent(st, m_ev_kdone, 0));
 }
 
 void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,

@@ -163,8 +163,8 @@ private:
   cudaStream_t m_stream = nullptr;
   long long m_launches = 0;
   bool m_profiling = false;
-  cudaStream_t m_side = nullptr;          // pair kernel of forces_overlapped
-  cudaEvent_t m_ev_fork = nullptr, m_ev_join = nullptr;
+  cudaStream_t m_side = nullptr;          // k-space chain of forces_overlapped (high priority)
+  cudaEvent_t m_ev_fork = nullptr, m_ev_join = nullptr, m_ev_kdone = nullptr;
   cudaEvent_t m_interp_wait = nullptr;    // event the interpolation waits for
   std::vector<std::pair<std::string, cudaEvent_t>> m_marks;
   std::vector<ReplicaConf> m_conf;
