@@ -125,6 +125,20 @@ class _P3MBase:
             return self._params[name]
         raise AttributeError(name)
 
+    # --- checkpointing ----------------------------------------------------
+    # As the reference's script-interface checkpoints, a pickled actor keeps
+    # its parameters with the tuned values (mesh, cao, r_cut, alpha,
+    # mesh_off, achieved accuracy); the restored actor does not tune again.
+    def __reduce__(self):
+        p = dict(self._params)
+        if self._handle is not None and self._handle.value:
+            t = self._tuned()
+            if t.is_tuned:
+                p.update(mesh=[int(m) for m in t.mesh], cao=int(t.cao), r_cut=float(t.r_cut),
+                         alpha=float(t.alpha), mesh_off=[float(x) for x in t.mesh_off],
+                         accuracy=float(t.accuracy), tune=False)
+        return (_restore_actor, (type(self), p))
+
     # --- engine-facing calls ---------------------------------------------
     def _set_system(self, box_l, skin, periodicity):
         s = _lib.SystemDesc()
@@ -151,3 +165,7 @@ class P3MGPU(_P3MBase):
     """P3M electrostatics solver with the FP32-mixed GPU path by default."""
     _so_name = "Coulomb::CoulombP3MGPU"
     _single_precision_default = True
+
+
+def _restore_actor(cls, params):
+    return cls(**params)

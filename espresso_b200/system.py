@@ -329,6 +329,21 @@ class System:
     def volume(self):
         return float(np.prod(self._box_l))
 
+    # checkpointing: particles, interactions and the solver's (tuned)
+    # parameters; the restored system activates its solver anew
+    def __getstate__(self):
+        st = dict(self.__dict__)
+        st["_sr_handle"] = None
+        st["_restore_solver"] = self.electrostatics._solver
+        return st
+
+    def __setstate__(self, st):
+        solver = st.pop("_restore_solver")
+        self.__dict__.update(st)
+        self.electrostatics._solver = None
+        if solver is not None:
+            self.electrostatics.solver = solver
+
     def _touch(self, what):
         pass
 

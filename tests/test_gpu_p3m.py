@@ -442,3 +442,31 @@ def test_changed_types_and_charges_between_host_calls(cls):
     f_q = forces(s)
     assert np.array_equal(f_q, forces(system(t2, q2)))
     assert not np.array_equal(f_t, f_q)
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_checkpoint_keeps_tuned_parameters(cls):
+    """A pickled system (as the reference's checkpointing) restores the
+    solver with its tuned parameters, without tuning again, and gives the
+    same forces bit for bit."""
+    import pickle
+    from espresso_b200.interactions import FeneBond
+    box = 12.0
+    pos, q = jittered_lattice(8, box, 0.2, seed=41)
+    s = make_system([box] * 3, pos, q)
+    s.non_bonded_inter[0, 0].wca.set_params(epsilon=1.0, sigma=1.0)
+    fene = FeneBond(k=10.0, d_r_max=2.0)
+    s.bonded_inter.add(fene)
+    s.part.by_id(0).add_bond((fene, 1))
+    s.electrostatics.solver = cls(prefactor=1.0, accuracy=1e-3, tune=True, verbose=False,
+                                  timings=2)
+    s.integrator.run(0, recalc_forces=True)
+    f0 = s.part.all().f
+    s2 = pickle.loads(pickle.dumps(s))
+    p1, p2 = s.electrostatics.solver.get_params(), s2.electrostatics.solver.get_params()
+    for k in ("mesh", "cao", "r_cut", "alpha", "mesh_off", "prefactor", "accuracy"):
+        assert p1[k] == p2[k], k
+    assert p1["is_tuned"] and p2["is_tuned"] and p2["tune"] is False
+    s2.integrator.run(0, recalc_forces=True)
+    assert np.array_equal(s2.part.all().f, f0)
+    assert len(s2.part.by_id(0).bonds) == 1
