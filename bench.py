@@ -284,6 +284,14 @@ def run_batched(args):
         torch.cuda.synchronize()
     lib.p3mx_batch_launch_count(h, ctypes.byref(lc1))
     t_ms = e0.elapsed_time(e1) / args.steps
+    # stage profile of one force evaluation of the whole batch (outside the
+    # timed region)
+    names = (ctypes.c_char_p * 32)()
+    sms = (ctypes.c_double * 32)()
+    nst = ctypes.c_int()
+    _lib.check(lib.p3mx_batch_profile(h, 3, sms, names, 32, ctypes.byref(nst)), h,
+               lib.p3mx_batch_last_error)
+    stages = {names[k].decode(): sms[k] for k in range(nst.value)}
     tuned = []
     for r in range(len(prefs)):
         t = _lib.Tuned()
@@ -332,7 +340,7 @@ def run_batched(args):
                    "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max()),
                    "r_cut_range": [float(rcs.min()), float(rcs.max())],
                    "verlet_candidates_per_step_est": pair_cand},
-        "cpu_baseline": cpu, "clocks": clk.summary(),
+        "stages_ms": stages, "cpu_baseline": cpu, "clocks": clk.summary(),
         "gpu_launches": int(lc1.value - lc0.value)}))
 
 

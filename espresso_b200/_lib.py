@@ -93,6 +93,9 @@ SIGNATURES = {
     "p3mx_bond_observables": (ctypes.c_int, [_vp, _sz, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_batch_set_bonds": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(BondParams), _sz,
                                             ctypes.POINTER(ctypes.c_int)]),
+    "p3mx_batch_profile": (ctypes.c_int, [_vp, ctypes.c_int, _dp,
+                                          ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int)]),
     "p3mx_short_range": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_forces": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_cell_grid": (ctypes.c_int, [_vp, _ip, _dp]),

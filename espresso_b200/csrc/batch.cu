@@ -633,6 +633,29 @@ int p3mx_batch_set_bonds(p3mx_batch *b, int n_types, const p3mx_bond_params *typ
   });
 }
 
+int p3mx_batch_profile(p3mx_batch *b, int reps, double *ms, const char **names, int cap,
+                       int *nstages) {
+  return bguard(b, [&] {
+    static std::vector<std::string> keep;
+    Engine &e = *b->eng;
+    e.ensure_lists(e.stream(), 2.0);
+    auto prof = e.profile(std::max(1, reps), e.stream());
+    keep.clear();
+    for (auto const &p : prof)
+      keep.push_back(p.first);
+    int const n = static_cast<int>(prof.size());
+    if (nstages)
+      *nstages = n;
+    for (int k = 0; k < std::min(n, cap); ++k) {
+      if (ms)
+        ms[k] = prof[k].second;
+      if (names)
+        names[k] = keep[k].c_str();
+    }
+    b->forces_valid = false;
+  });
+}
+
 void *p3mx_batch_stream(const p3mx_batch *b) {
   return (b && b->eng) ? static_cast<void *>(b->eng->stream()) : nullptr;
 }

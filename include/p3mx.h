@@ -256,6 +256,10 @@ int p3mx_batch_get_tuned(const p3mx_batch *b, int r, p3mx_tuned *out);
 /* One force evaluation for all replicas (forces overwritten, device
  * resident); optional per-replica energies (n_rep doubles, host). */
 int p3mx_batch_forces(p3mx_batch *b, double *energy_out);
+/* Stage profile of one force evaluation of the whole batch, as
+ * p3mx_profile (no counterpart in the reference). */
+int p3mx_batch_profile(p3mx_batch *b, int reps, double *ms, const char **names,
+                       int cap, int *nstages);
 /* Pair bonds of the batch, as p3mx_set_bonds with particle indices over the
  * whole batch (both partners in one replica); forces enter
  * p3mx_batch_forces and the graph step of p3mx_batch_run (captured anew
