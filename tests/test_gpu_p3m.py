@@ -470,3 +470,25 @@ def test_checkpoint_keeps_tuned_parameters(cls):
     s2.integrator.run(0, recalc_forces=True)
     assert np.array_equal(s2.part.all().f, f0)
     assert len(s2.part.by_id(0).bonds) == 1
+
+
+@pytest.mark.parametrize("mesh,cao", [([8, 10, 12], 7), ([6, 8, 10], 5), ([8, 8, 8], 8 - 1)])
+@pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
+def test_kspace_meshes_smaller_than_a_brick_tile(mesh, cao, cls, rtol):
+    """Meshes smaller than one brick tile (brick + cao - 1 points): the
+    assignment tiles overlap themselves (multi-pass flush by wrap class) and
+    the ghost layers of the field mesh cover most of it; charge mesh, forces
+    and energy still match the FP64 oracle."""
+    box = np.array([7.0, 8.0, 9.0])
+    rng = np.random.default_rng(cao + mesh[0])
+    n = 150
+    pos = rng.uniform(0.0, 1.0, (n, 3)) * box
+    q = rng.choice([-1.0, 1.0], n)
+    q -= q.mean()
+    _, f, e, v, mesh_gpu = _handle_compute(cls, box, pos, q, mesh, cao, 0.9, 2.0)
+    p = O.make_params(box, mesh, cao, 0.9, 2.0, 1.0)
+    fo, eo, vo, rho = O.p3m_kspace(p, pos, q, want_mesh=True)
+    np.testing.assert_allclose(mesh_gpu, rho.ravel(), atol=rtol * np.abs(rho).max() * 10, rtol=0)
+    np.testing.assert_allclose(f, fo, atol=rtol * np.abs(fo).max() * 10, rtol=0)
+    assert abs(e - eo) <= rtol * abs(eo) * 10 + 1e-12
+    np.testing.assert_allclose(v, vo, atol=rtol * np.abs(vo).max() * 10, rtol=0)
