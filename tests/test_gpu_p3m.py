@@ -492,3 +492,39 @@ def test_kspace_meshes_smaller_than_a_brick_tile(mesh, cao, cls, rtol):
     np.testing.assert_allclose(f, fo, atol=rtol * np.abs(fo).max() * 10, rtol=0)
     assert abs(e - eo) <= rtol * abs(eo) * 10 + 1e-12
     np.testing.assert_allclose(v, vo, atol=rtol * np.abs(vo).max() * 10, rtol=0)
+
+
+def test_degenerate_inputs():
+    """Edge cases of the reference's own checks and of empty work: tuning
+    without charged particles raises its runtime error (p3m.cpp:769-771);
+    an untuned actor on all-zero charges gives the LJ forces alone; a
+    single ion (neutrality check off) gets a finite force; a system without
+    particles runs."""
+    box = 10.0
+    pos, _ = jittered_lattice(6, box, 0.2, seed=51)  # 216 particles
+    zero = np.zeros(len(pos))
+    s = make_system([box] * 3, pos, zero)
+    with pytest.raises(Exception, match="no charged particles"):
+        s.electrostatics.solver = P3MGPU(prefactor=1.0, accuracy=1e-3, tune=True, verbose=False)
+    s.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0, cutoff=2.5,
+                                                      shift="auto")
+    s.integrator.run(0, recalc_forces=True)
+    f_lj = s.part.all().f
+    # (the FP32-mixed actor evaluates LJ in FP32 too)
+    for cls, tol in ((P3M, 1e-12), (P3MGPU, FP32_RTOL * np.abs(f_lj).max())):
+        s.electrostatics.solver = cls(prefactor=1.0, accuracy=1e-3, mesh=16, cao=5, alpha=1.0,
+                                      r_cut=2.5, tune=False, check_neutrality=False)
+        s.integrator.run(0, recalc_forces=True)
+        np.testing.assert_allclose(s.part.all().f, f_lj, rtol=0, atol=tol)
+        s.electrostatics.clear()
+    one = make_system([box] * 3, np.array([[1.0, 2.0, 3.0]]), np.array([1.0]))
+    one.electrostatics.solver = P3MGPU(prefactor=1.0, accuracy=1e-3, mesh=16, cao=5, alpha=1.0,
+                                       r_cut=2.5, tune=False, check_neutrality=False)
+    one.integrator.run(0, recalc_forces=True)
+    assert np.all(np.isfinite(one.part.all().f))
+    assert np.abs(one.part.all().f).max() < 1e-3  # the self force of one ion vanishes
+    empty = eb.System(box_l=[box] * 3)
+    empty.time_step = 0.01
+    empty.non_bonded_inter[0, 0].lennard_jones.set_params(epsilon=1.0, sigma=1.0, cutoff=2.5)
+    empty.integrator.run(2)
+    assert empty.analysis.energy()["total"] == 0.0
