@@ -873,6 +873,41 @@ __global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__res
                        qi);
 }
 
+// Displacement check fused with the sorted-position refresh, over the
+// cell-sorted order: sets *flag when a particle moved more than skin/2 or
+// changed type since the last build (k_displacement_check's test) and
+// writes the pair kernel's sorted records as k_refresh_spq does (a rebuild
+// that follows rewrites them).  One pass over the gathered positions
+// instead of two.
+__global__ void k_check_refresh(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
+                                const int *__restrict__ perm, const double *__restrict__ pos,
+                                const double *__restrict__ q, const int *__restrict__ scell,
+                                const double *__restrict__ pos_ref, const int *__restrict__ type,
+                                const int *__restrict__ type_ref, long long n,
+                                double4 *__restrict__ spq, float4 *__restrict__ spf,
+                                int *__restrict__ flag) {
+  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= n)
+    return;
+  int const i = perm[s];
+  RepGeom const &G = reps[rep_of[i]];
+  double d2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double const dx = pos[3 * i + d] - pos_ref[3 * i + d];
+    d2 += dx * dx;
+  }
+  double const lim = 0.5 * G.skin;
+  if (d2 > lim * lim || type[i] != type_ref[i])
+    atomicOr(flag, 1);
+  double const qi = q[i];
+  if (spq)
+    spq[s] = make_double4(fold_coord(pos[3 * i], G.box[0]), fold_coord(pos[3 * i + 1], G.box[1]),
+                          fold_coord(pos[3 * i + 2], G.box[2]), qi);
+  spf[s] = cell_offset(G, scell[s] - static_cast<int>(G.cell_off), pos_ref + 3 * i, pos + 3 * i,
+                       qi);
+}
+
 void Engine::refresh_sorted_positions(cudaStream_t st, bool want_spq) {
   k_refresh_spq<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(),
                                                     m_cperm.as<int>(), d_pos(), d_q(),
@@ -888,21 +923,25 @@ void Engine::prepare_short_range(cudaStream_t st, bool need_spq) {
   int const nb = ceil_div(m_n, 256);
   bool rebuild = !m_lists_valid;
   if (!rebuild) {
+    // check and refresh in one pass; the records it writes stand unless a
+    // rebuild follows
     P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
-    k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
-                                             d_type(), m_type_ref.as<int>(), m_n,
-                                             m_flag.as<int>(), nullptr); ++m_launches;
+    k_check_refresh<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), d_pos(), d_q(),
+                                        m_scell.as<int>(), m_pos_ref.as<double>(), d_type(),
+                                        m_type_ref.as<int>(), m_n,
+                                        need_spq ? m_spq.as<double4>() : nullptr,
+                                        m_spf.as<float4>(), m_flag.as<int>());
+    ++m_launches;
     int flag = 0;
     P3MX_CUDA(cudaMemcpyAsync(&flag, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     P3MX_CUDA(cudaStreamSynchronize(st));
     rebuild = (flag != 0);
   }
   mark("sr_check", st);
-  if (rebuild)
+  if (rebuild) {
     build_lists(st);
-  else
-    refresh_sorted_positions(st, need_spq);
-  mark(rebuild ? "sr_rebuild" : "sr_refresh", st);
+    mark("sr_rebuild", st);
+  }
 }
 
 template <typename Real>
