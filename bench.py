@@ -4,7 +4,8 @@ Workload (default): the single large system of 2^20 monovalent ions (half
 +1, half -1) at number density 0.5 in a cubic box of side 128 on a jittered
 lattice, LJ eps=1 sigma=1 cutoff 2.5 (shift auto), P3M cao 7, r_cut 3.5 and
 a 256^3 mesh with alpha tuned for an rms force error estimate <= 1e-4 (at
-r_cut 3.5 the 128^3 mesh bottoms out at 3.9e-3), FP32-mixed
+r_cut 3.5 and cao 7 the error estimate of a 128^3 mesh bottoms out at
+3.9e-3 whatever alpha, so 256^3 is the smallest mesh reaching 1e-4), FP32-mixed
 mesh/FFT path.  One step = one full force evaluation (k-space + real-space
 Coulomb + LJ through the Verlet list) of the whole system; positions stay
 fixed, so the Verlet list is reused (its rebuild cost is reported apart).
