@@ -437,12 +437,15 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     if (m_fp32) {
       attr(k_fft_z_fwd<float>, m_smem_zf);
       attr(k_fft_y<float>, m_smem_y);
-      attr(k_fft_x_kspace<float>, m_smem_x);
+      attr(k_fft_x_kspace<float, true>, m_smem_x);
+      attr(k_fft_x_kspace<float, false>, m_smem_x);
+      attr(k_fft_x_kspace<float, false, 3>, m_smem_x);
       attr(k_fft_z_inv3<float>, m_smem_zi);
     } else {
       attr(k_fft_z_fwd<double>, m_smem_zf);
       attr(k_fft_y<double>, m_smem_y);
-      attr(k_fft_x_kspace<double>, m_smem_x);
+      attr(k_fft_x_kspace<double, true>, m_smem_x);
+      attr(k_fft_x_kspace<double, false>, m_smem_x);
       attr(k_fft_z_inv3<double>, m_smem_zi);
     }
   }
@@ -727,9 +730,21 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 4. x pass fused with the k-space operator (+ energy/virial partials)
   bool const want_f = (f != nullptr);
   bool const want_ev = want_e || want_v;
-  k_fft_x_kspace<Real><<<m_n_blk_x, 256, m_smem_x, st>>>(
-      geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx, m_tile_x,
-      want_f ? 1 : 0, want_ev ? 1 : 0, m_part_x.as<double>(), tw); ++m_launches;
+  if (want_ev)
+    k_fft_x_kspace<Real, true><<<m_n_blk_x, 256, m_smem_x, st>>>(
+        geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx,
+        m_tile_x, want_f ? 1 : 0, m_part_x.as<double>(), tw);
+  else if (sizeof(Real) == 4 && 3 * (m_smem_x + 1024) <= 228 * 1024)
+    // the shared memory leaves room for three blocks per SM: the instance
+    // whose registers allow them
+    k_fft_x_kspace<Real, false, 3><<<m_n_blk_x, 256, m_smem_x, st>>>(
+        geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx,
+        m_tile_x, want_f ? 1 : 0, m_part_x.as<double>(), tw);
+  else
+    k_fft_x_kspace<Real, false><<<m_n_blk_x, 256, m_smem_x, st>>>(
+        geom, m_blk_x.as<Blk>(), m_ck.as<C>(), m_ginf.as<Real>(), m_field.as<C>(), m_cplx,
+        m_tile_x, want_f ? 1 : 0, m_part_x.as<double>(), tw);
+  ++m_launches;
   if (want_ev) {
     k_reduce_partials<<<ceil_div(R, 128), 128, 0, st>>>(m_part_x.as<double>(), 8,
                                                         m_blk_x_start_d.as<int>(), R,

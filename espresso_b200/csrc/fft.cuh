@@ -554,12 +554,16 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
 // Pyz, Pzz, diag}] in FP64 (Hermitian weights 1 for kz = 0, M2/2, else 2).
 // Shared memory: 3 x tile staged lines of line_ld(M0) (phi, field lines,
 // scratch), twiddles (M0).
-template <typename Real>
-__global__ void __launch_bounds__(256)
+// EV: energy / virial partials (a template parameter, so that the
+// forces-only instance carries none of their registers).  MINB: blocks per
+// SM the registers are sized for -- 3 pays where the shared memory of a
+// launch (small meshes) leaves room for a third block.
+template <typename Real, bool EV, int MINB = 2>
+__global__ void __launch_bounds__(256, MINB)
 k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
                const typename CplxOf<Real>::type *__restrict__ rho_hat,
                const Real *__restrict__ ginf, typename CplxOf<Real>::type *__restrict__ field0,
-               long long field_stride, int tile, int want_fields, int want_ev,
+               long long field_stride, int tile, int want_fields,
                double *__restrict__ partials,
                const typename CplxOf<Real>::type *__restrict__ twtab) {
   using C = typename CplxOf<Real>::type;
@@ -615,7 +619,7 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     C const rh = res[t * ld + pix(x)];
     Real const g = ginf[base + x * stride_x + t];
     int const kxd = dop(x, M0), kzd = dop(kz, M2);
-    if (want_ev) {
+    if constexpr (EV) {
       double const wgt = (kz == 0 || kz == M2 / 2) ? 1.0 : 2.0;
       double const ek = wgt * static_cast<double>(g) *
                         (static_cast<double>(rh.x) * rh.x + static_cast<double>(rh.y) * rh.y);
@@ -636,7 +640,7 @@ k_fft_x_kspace(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     // phi = G rho_hat replaces rho_hat in place (same thread, same point)
     res[t * ld + pix(x)] = C{g * rh.x, g * rh.y};
   }
-  if (want_ev) {
+  if constexpr (EV) {
     // block reduction of the 8 partial sums (fixed order -> deterministic)
     __shared__ double red[8][32];
     int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
