@@ -283,3 +283,133 @@ def bonds(box, pos, bond_types, bond_list):
         energy += e
         vir += np.outer(force, d)
     return f, energy, vir
+
+
+def elc_far_cut(box, box_h, max_pw_error):
+    """ELC far-formula cutoff from the maximal pairwise error, restating
+    ElectrostaticLayerCorrection::tune_far_cut (electrostatics/elc.cpp:942-973)
+    without dielectric contrasts (lz = box_l[2]).  Raises RuntimeError when no
+    cutoff below 50 meets the bound, as the reference does."""
+    ux, uy = 1.0 / box[0], 1.0 / box[1]
+    umin = min(ux, uy)
+    lz = box[2]
+    fc = umin
+    while True:
+        pref = 2.0 * np.pi * fc
+        s = pref + 2.0 * (ux + uy)
+        den = -np.expm1(-pref * lz)
+        num1 = np.exp(pref * (box_h - lz))
+        num2 = np.exp(-pref * (box_h + lz))
+        err = 0.5 / den * (num1 * (s + 1.0 / (lz - box_h)) / (lz - box_h) +
+                           num2 * (s + 1.0 / (lz + box_h)) / (lz + box_h))
+        fc += umin
+        if not (err > max_pw_error and fc < 50.0):
+            break
+    if fc >= 50.0:
+        raise RuntimeError("ELC tuning failed: maxPWerror too small")
+    return fc - umin
+
+
+def elc_modes(box, far_cut):
+    """The (p, q) frequencies ELC sums over, in the reference's loop order
+    (elc.cpp:830-883): p-modes (q = 0), q-modes (p = 0), then p-major pq
+    modes; each as (kind, p, q, omega) with kind 0 = x, 1 = y, 2 = pq."""
+    ux, uy = 1.0 / box[0], 1.0 / box[1]
+    nfx = int(np.ceil(far_cut * box[0]) + 1.0)
+    nfy = int(np.ceil(far_cut * box[1]) + 1.0)
+    modes = []
+    p = 1
+    while ux * (p - 1) < far_cut and p <= nfx:
+        modes.append((0, p, 0, 2.0 * np.pi * ux * p))
+        p += 1
+    q = 1
+    while uy * (q - 1) < far_cut and q <= nfy:
+        modes.append((1, 0, q, 2.0 * np.pi * uy * q))
+        q += 1
+    p = 1
+    while ux * (p - 1) < far_cut and p <= nfx:
+        q = 1
+        while (ux * (p - 1)) ** 2 + (uy * (q - 1)) ** 2 < far_cut * far_cut and q <= nfy:
+            modes.append((2, p, q, 2.0 * np.pi * np.sqrt((ux * p) ** 2 + (uy * q) ** 2)))
+            q += 1
+        p += 1
+    return modes
+
+
+def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True):
+    """ELC correction forces and energy without dielectric contrasts, in FP64
+    numpy, restating electrostatics/elc.cpp: the dipole force and energy
+    (add_dipole_force :201-264, dipole_energy :267-343), the per-frequency
+    product decomposition (setup_PoQ :501-598, add_PoQ_force :601-618,
+    PoQ_energy :620-634, setup_PQ :641-769, add_PQ_force :771-810,
+    PQ_energy :812-828) and their sums (add_force :830-883, calc_energy
+    :885-940, which halves the total).  Positions are folded into the box
+    first, as the reference's particle positions are.  Returns (forces
+    (N, 3), energy); raises RuntimeError for a charged particle in the gap.
+    """
+    box = np.asarray(box, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    pos = pos - np.floor(pos / box) * box
+    x, y, z = pos[:, 0], pos[:, 1], pos[:, 2]
+    lz = box[2]
+    box_h = lz - gap_size
+    bad = (q != 0.0) & ((z < 0.0) | (z > box_h))
+    if bad.any():
+        i = int(np.flatnonzero(bad)[0])
+        dz = z[i] if z[i] < 0.0 else z[i] - box_h
+        raise RuntimeError("Particle %d entered ELC gap region by %r" % (i, dz))
+    f = np.zeros_like(pos)
+    vol = box[0] * box[1] * box[2]
+    shift = 0.5 * lz
+    # dipole force (elc.cpp:201-264), no dielectric contrast / const_pot
+    pref = prefactor * 4.0 * np.pi / vol
+    g0 = pref * np.sum(q * (z - shift))
+    g2 = pref * np.sum(q)
+    f[:, 2] -= g0 * q
+    if not neutralize:
+        f[:, 2] += g2 * q * (z - shift)
+    # dipole energy (elc.cpp:267-343)
+    pref = prefactor * 2.0 * np.pi / vol
+    s0 = np.sum(q)
+    s2 = np.sum(q * (z - shift))
+    s4 = np.sum(q * (z - shift) ** 2)
+    energy = 2.0 * pref * s2 * s2
+    if not neutralize:
+        energy += 2.0 * pref * (-s0 * s4 - (0.25 - 0.5 / 3.0) * (s0 * lz) ** 2)
+    area_inv = 1.0 / (box[0] * box[1])
+    ux, uy = 1.0 / box[0], 1.0 / box[1]
+    for kind, p, qq, omega in elc_modes(box, far_cut):
+        e = np.exp(omega * z)
+        if kind < 2:
+            c = x if kind == 0 else y
+            u = ux if kind == 0 else uy
+            arg = (2.0 * np.pi * u * (p if kind == 0 else qq)) * c
+            s, co = np.sin(arg), np.cos(arg)
+            pb = np.stack([q * s * e, q * co * e, q * s / e, q * co / e])  # SP CP SM CM
+            pref = -(prefactor * 4.0 * np.pi * area_inv) / np.expm1(omega * lz)
+            G = pref * pb.sum(axis=1)
+            SP, CP, SM, CM = pb
+            f[:, kind] += SM * G[1] - CM * G[0] + SP * G[3] - CP * G[2]
+            f[:, 2] += CM * G[1] + SM * G[0] - CP * G[3] - SP * G[2]
+            energy += np.sum(CM * G[1] + SM * G[0] + CP * G[3] + SP * G[2]) / omega
+        else:
+            ax = (2.0 * np.pi * ux * p) * x
+            ay = (2.0 * np.pi * uy * qq) * y
+            sx, cx, sy, cy = np.sin(ax), np.cos(ax), np.sin(ay), np.cos(ay)
+            pb = np.stack([sx * sy * q * e, sx * cy * q * e, cx * sy * q * e, cx * cy * q * e,
+                           sx * sy * q / e, sx * cy * q / e, cx * sy * q / e, cx * cy * q / e])
+            pref = -(prefactor * 8.0 * np.pi * area_inv) / np.expm1(omega * lz)
+            G = pref * pb.sum(axis=1)
+            SSP, SCP, CSP, CCP, SSM, SCM, CSM, CCM = pb
+            px = 2.0 * np.pi * ux * p / omega
+            py = 2.0 * np.pi * uy * qq / omega
+            f[:, 0] += px * (SCM * G[3] + SSM * G[2] - CCM * G[1] - CSM * G[0] +
+                             SCP * G[7] + SSP * G[6] - CCP * G[5] - CSP * G[4])
+            f[:, 1] += py * (CSM * G[3] + SSM * G[1] - CCM * G[2] - SCM * G[0] +
+                             CSP * G[7] + SSP * G[5] - CCP * G[6] - SCP * G[4])
+            f[:, 2] += (CCM * G[3] + CSM * G[2] + SCM * G[1] + SSM * G[0] -
+                        CCP * G[7] - CSP * G[6] - SCP * G[5] - SSP * G[4])
+            energy += np.sum(CCM * G[3] + CSM * G[2] + SCM * G[1] + SSM * G[0] +
+                             CCP * G[7] + CSP * G[6] + SCP * G[5] + SSP * G[4]) / omega
+    return f, 0.5 * energy

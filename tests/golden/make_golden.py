@@ -10,6 +10,9 @@ Sources (paths relative to the ESPResSo tree):
     with the parameters and energy of testsuite/python/coulomb_cloud_wall.py:40-47
   * testsuite/python/data/coulomb_tuning_system.npz (coulomb_tuning.py:37-47)
   * testsuite/python/data/lj_system.dat (lj.py:28-47)
+  * testsuite/python/data/coulomb_mixed_periodicity_system.data (id pos q f,
+    forces from MMM2D) with the parameters and the MMM2D energy of
+    testsuite/python/coulomb_mixed_periodicity.py:30-40, 84-121 (ELC)
   * known answers written in testsuite/python/electrostatic_interactions.py:81-124
     and testsuite/python/p3m_madelung.py:202-313 (parameters and constants)
   * values of the reference's own math headers (bspline.hpp, AS_erfc_part.hpp,
@@ -49,6 +52,14 @@ def main():
                         eps=1.0, sig=1.0, cut=1.12246, skin=0.4,
                         shift=0.2499999999700293)
 
+    mp = np.genfromtxt(os.path.join(DATA, "coulomb_mixed_periodicity_system.data"))
+    np.savez_compressed(
+        os.path.join(HERE, "coulomb_mixed_periodicity.npz"),
+        pos=mp[:, 1:4], q=mp[:, 4], forces=mp[:, 5:8],
+        box=np.array([10., 10., 12.]), mesh=np.array([42, 42, 50]), r_cut=3.0,
+        accuracy=1e-6, max_pw_error=1e-6, gap_size=3.0, energy=216.640984711,
+        force_atol=1e-5, energy_atol=1e-4)
+
     known = {
         "two_charges": {
             "source": "testsuite/python/electrostatic_interactions.py:81-124",
@@ -69,7 +80,8 @@ def main():
             "n_pairs": 24, "mesh": 48, "cao": 7, "r_cut": 22.0,
             "alpha": 0.179719, "accuracy": 1e-8,
             "madelung": -1.6155426267128247, "base": [1, 1, 0],
-            "energy_rtol": 1e-7, "pressure_rtol": 5e-7},
+            "energy_rtol": 1e-7, "pressure_rtol": 5e-7,
+            "elc": {"maxPWerror": 1e-6, "gap_size": 16.0}},
         "madelung_cube": {
             "source": "testsuite/python/p3m_madelung.py:279-313",
             "n_pairs": 6, "mesh": 72, "cao": 7, "r_cut": 5.6,
