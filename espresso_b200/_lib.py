@@ -63,6 +63,13 @@ class BondParams(ctypes.Structure):
                 ("r_max", ctypes.c_double)]
 
 
+class ElcParams(ctypes.Structure):
+    _fields_ = [("maxPWerror", ctypes.c_double), ("gap_size", ctypes.c_double),
+                ("far_cut", ctypes.c_double), ("neutralize", ctypes.c_int),
+                ("delta_mid_top", ctypes.c_double), ("delta_mid_bot", ctypes.c_double),
+                ("const_pot", ctypes.c_int), ("pot_diff", ctypes.c_double)]
+
+
 class BatchDesc(ctypes.Structure):
     _fields_ = [("n_rep", ctypes.c_int), ("box", ctypes.POINTER(ctypes.c_double)),
                 ("prefactor", ctypes.POINTER(ctypes.c_double)),
@@ -91,6 +98,8 @@ SIGNATURES = {
     "p3mx_set_bonds": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(BondParams), _sz,
                                       ctypes.POINTER(ctypes.c_int)]),
     "p3mx_bond_observables": (ctypes.c_int, [_vp, _sz, _vp, _dp, _dp, ctypes.c_uint, _vp]),
+    "p3mx_set_elc": (ctypes.c_int, [_vp, ctypes.POINTER(ElcParams)]),
+    "p3mx_get_elc": (ctypes.c_int, [_vp, _dp, _dp]),
     "p3mx_batch_set_bonds": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(BondParams), _sz,
                                             ctypes.POINTER(ctypes.c_int)]),
     "p3mx_batch_profile": (ctypes.c_int, [_vp, ctypes.c_int, _dp,

@@ -3,6 +3,7 @@
 // host<->device staging.  No exception crosses the ABI.
 #include "../../include/p3mx.h"
 #include "bond_abi.cuh"
+#include "elc_host.cuh"
 #include "engine.cuh"
 #include "host_pool.cuh"
 
@@ -144,6 +145,8 @@ struct p3mx_handle {
   // charge census
   int n_charged = 0;
   double sum_q2 = 0, sum_q = 0;
+  // electrostatic layer correction attached to the actor (p3mx_set_elc)
+  std::unique_ptr<ElcState> elc;
 };
 
 namespace {
@@ -948,6 +951,49 @@ static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwr
   }
 }
 
+// ELC correction of the staged particles into the device forces fd
+// (ElectrostaticLayerCorrection::add_long_range_forces :1231-1254 after the
+// P3M forces; long_range_energy :1189-1229 adds calc_energy).
+static void elc_add(p3mx_handle *h, double *fd, double *energy, cudaStream_t st) {
+  Engine &e = *h->eng;
+  elc_apply(*h->elc, h->sys.box, h->prm.prefactor, static_cast<long long>(h->n), e.d_pos(),
+            e.d_q(), fd, energy, nullptr, st);
+}
+
+int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p) {
+  return guarded(h, [&] {
+    if (!p) {
+      h->elc.reset();
+      return;
+    }
+    elc_validate(*p);
+    if (h->sys_set && !(h->sys.periodic[0] && h->sys.periodic[1] && h->sys.periodic[2]))
+      throw Error(P3MX_ERUNTIME, "ELC: requires periodicity (True, True, True)");
+    auto s = std::make_unique<ElcState>();
+    s->prm = *p;
+    s->far_calculated = (p->far_cut == -1.0);
+    // adapt_epsilon_elc (p3m.impl.hpp:112-114): the base P3M is metallic
+    h->prm.epsilon = 0.0;
+    if (h->sys_set) {
+      Engine *e = h->eng.get();
+      elc_prepare(*s, h->sys.box, h->prm.prefactor, e ? e->stream() : nullptr);
+    }
+    h->elc = std::move(s);
+  });
+}
+
+int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h) {
+  if (!h)
+    return P3MX_EHANDLE;
+  if (!h->elc)
+    return P3MX_ERUNTIME;
+  if (far_cut)
+    *far_cut = h->elc->far_cut;
+  if (box_h)
+    *box_h = h->elc->box_h;
+  return 0;
+}
+
 int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q, double *f,
                     double *energy, double *virial9, unsigned flags, void *stream) {
   return guarded(h, [&] {
@@ -968,8 +1014,13 @@ int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q
     e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &en, &vir);
     if (obs64 && (want_e || want_v))
       fp64_kspace_observables(h, st, want_e, want_v, en, vir);
+    double e_elc = 0.0;
+    if (h->elc) {
+      elc_add(h, fd ? fd : e.d_force(), want_e ? &e_elc : nullptr, st);
+      vir.assign(9, 0.0);
+    }
     if (energy && (flags & P3MX_ENERGY))
-      *energy = en.empty() ? 0. : en[0];
+      *energy = (en.empty() ? 0. : en[0]) + e_elc;
     if (virial9 && (flags & P3MX_VIRIAL))
       for (int k = 0; k < 9; ++k)
         virial9[k] = vir.empty() ? 0. : vir[k];
@@ -1042,6 +1093,8 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
         if (h->prm.epsilon != 0.)
           e.census(st);
         e.forces_overlapped(fd, true, st);
+        if (h->elc)
+          elc_add(h, fd, nullptr, st);
       };
       forces();
       if (!staged_match(h, n, q, type)) {
@@ -1070,9 +1123,17 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
       fp64_kspace_observables(h, st, want_e, want_v, enk, virk);
       e.short_range(observables_engine(h).d_force(), true, true, st, &ens, &virs, true);
     }
+    double e_elc = 0.0;
+    if (h->elc) {
+      // ELC: correction forces and energy; no k-space pressure (the
+      // reference warns and reports zero, coulomb.cpp:124-131)
+      elc_add(h, fd, want_e ? &e_elc : nullptr, st);
+      for (auto &v : virk)
+        v = 0.0;
+    }
     if (want_e) {
       energy3[0] = ens[0];
-      energy3[1] = enk[0];
+      energy3[1] = enk[0] + e_elc;
       energy3[2] = ens[1];
     }
     if (want_v)

@@ -1,0 +1,217 @@
+// Host side of the electrostatic layer correction: parameter checks
+// (elc_data::elc_data, core/electrostatics/elc.cpp:1056-1102), slab height
+// and far-formula cutoff (recalc_box_h :1020-1030, tune_far_cut :942-973),
+// the mode table in the reference's loop order (add_force :830-883) and the
+// kernel chain of elc.cuh on a caller's stream.
+#pragma once
+
+#include "../../include/p3mx.h"
+#include "elc.cuh"
+#include "engine.cuh"
+
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+namespace p3mx {
+
+struct ElcState {
+  p3mx_elc_params prm{};
+  bool far_calculated = false;
+  double far_cut = 0.0, box_h = 0.0;
+  double built_box[3] = {0, 0, 0};
+  double built_prefactor = 0.0;
+  std::vector<ElcMode> modes;
+  int nfx = 0, nfy = 0;
+  DevBuf d_modes, d_sc, d_part, d_G, d_epart, d_err;
+  std::vector<double> h_epart;
+};
+
+// elc_data::elc_data (elc.cpp:1056-1102); dielectric contrasts and the
+// constant-potential option are not part of this library.
+inline void elc_validate(p3mx_elc_params const &p) {
+  double const delta_range = 1.0 + std::sqrt(1e-14);
+  bool const far_calc = (p.far_cut == -1.0);
+  if (p.far_cut <= 0.0 && !far_calc)
+    throw Error(P3MX_EDOMAIN, "Parameter 'far_cut' must be > 0");
+  if (p.maxPWerror <= 0.0)
+    throw Error(P3MX_EDOMAIN, "Parameter 'maxPWerror' must be > 0");
+  if (p.gap_size <= 0.0)
+    throw Error(P3MX_EDOMAIN, "Parameter 'gap_size' must be > 0");
+  if (p.pot_diff != 0.0 && !p.const_pot)
+    throw Error(P3MX_EDOMAIN, "Parameter 'const_pot' must be True when 'pot_diff' is non-zero");
+  if (p.delta_mid_top < -delta_range || p.delta_mid_top > delta_range)
+    throw Error(P3MX_EDOMAIN, "Parameter 'delta_mid_top' must be >= -1 and <= +1");
+  if (p.delta_mid_bot < -delta_range || p.delta_mid_bot > delta_range)
+    throw Error(P3MX_EDOMAIN, "Parameter 'delta_mid_bot' must be >= -1 and <= +1");
+  if (p.delta_mid_top != 0.0 || p.delta_mid_bot != 0.0)
+    throw Error(P3MX_ERUNTIME, "ELC: dielectric contrasts (delta_mid_top / delta_mid_bot "
+                               "!= 0) are not supported by this library");
+}
+
+// tune_far_cut (elc.cpp:942-973) without dielectric contrasts (lz = L_z).
+inline double elc_tune_far_cut(double const box[3], double box_h, double max_pw_error) {
+  double const maximal_far_cut = 50.0;
+  double const ux = 1.0 / box[0], uy = 1.0 / box[1];
+  double const umin = std::min(ux, uy);
+  double const lz = box[2];
+  double fc = umin, err;
+  do {
+    double const pref = 2.0 * kPi * fc;
+    double const sum = pref + 2.0 * (ux + uy);
+    double const den = -std::expm1(-pref * lz);
+    double const num1 = std::exp(pref * (box_h - lz));
+    double const num2 = std::exp(-pref * (box_h + lz));
+    err = 0.5 / den *
+          (num1 * (sum + 1.0 / (lz - box_h)) / (lz - box_h) +
+           num2 * (sum + 1.0 / (lz + box_h)) / (lz + box_h));
+    fc += umin;
+  } while (err > max_pw_error && fc < maximal_far_cut);
+  if (fc >= maximal_far_cut)
+    throw Error(P3MX_ERUNTIME, "ELC tuning failed: maxPWerror too small");
+  return fc - umin;
+}
+
+// box_h, far_cut and the mode table for the box and prefactor (again only
+// when either changed: on_boxl_change -> recalc_box_h, recalc_far_cut).
+inline void elc_prepare(ElcState &s, double const box[3], double prefactor, cudaStream_t st) {
+  if (box[0] == s.built_box[0] && box[1] == s.built_box[1] && box[2] == s.built_box[2] &&
+      prefactor == s.built_prefactor && !s.modes.empty())
+    return;
+  double const bh = box[2] - s.prm.gap_size;
+  if (bh < 0.0) {
+    char m[160];
+    std::snprintf(m, sizeof m, "ELC gap size (%f) larger than box length in z-direction (%f)",
+                  s.prm.gap_size, box[2]);
+    throw Error(P3MX_ERUNTIME, m);
+  }
+  s.box_h = bh;
+  s.far_cut = s.far_calculated ? elc_tune_far_cut(box, bh, s.prm.maxPWerror) : s.prm.far_cut;
+  double const fc = s.far_cut, fc2 = fc * fc;
+  double const ux = 1.0 / box[0], uy = 1.0 / box[1];
+  s.nfx = static_cast<int>(std::ceil(fc * box[0]) + 1.0);
+  s.nfy = static_cast<int>(std::ceil(fc * box[1]) + 1.0);
+  double const area_inv = ux * uy;
+  s.modes.clear();
+  auto add = [&](int kind, int p, int q, double omega) {
+    ElcMode m{};
+    m.kind = kind;
+    m.p = p;
+    m.q = q;
+    m.omega = omega;
+    double const pref_di = prefactor * (kind < 2 ? 4.0 : 8.0) * kPi * area_inv;
+    m.pref = -pref_di / std::expm1(omega * box[2]);
+    m.px = 2.0 * kPi * ux * static_cast<double>(p) / omega;
+    m.py = 2.0 * kPi * uy * static_cast<double>(q) / omega;
+    s.modes.push_back(m);
+  };
+  for (int p = 1; ux * static_cast<double>(p - 1) < fc && p <= s.nfx; ++p)
+    add(0, p, 0, 2.0 * kPi * ux * static_cast<double>(p));
+  for (int q = 1; uy * static_cast<double>(q - 1) < fc && q <= s.nfy; ++q)
+    add(1, 0, q, 2.0 * kPi * uy * static_cast<double>(q));
+  for (int p = 1; ux * static_cast<double>(p - 1) < fc && p <= s.nfx; ++p)
+    for (int q = 1; (ux * static_cast<double>(p - 1)) * (ux * static_cast<double>(p - 1)) +
+                            (uy * static_cast<double>(q - 1)) * (uy * static_cast<double>(q - 1)) <
+                        fc2 &&
+                    q <= s.nfy;
+         ++q)
+      add(2, p, q,
+          2.0 * kPi * std::sqrt((ux * p) * (ux * p) + (uy * q) * (uy * q)));
+  s.d_modes.ensure(s.modes.size() * sizeof(ElcMode));
+  P3MX_CUDA(cudaMemcpyAsync(s.d_modes.p, s.modes.data(), s.modes.size() * sizeof(ElcMode),
+                            cudaMemcpyHostToDevice, st));
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  for (int d = 0; d < 3; ++d)
+    s.built_box[d] = box[d];
+  s.built_prefactor = prefactor;
+}
+
+// Adds the ELC forces to f (device, 3n FP64, original particle order) for
+// the positions and charges on the device; with energy != nullptr also the
+// ELC energy (calc_energy :885-940: dipole + mode terms, halved).  Ends with
+// a stream synchronisation: a charged particle in the gap raises the
+// reference's runtime error (check_gap :184-194).
+inline void elc_apply(ElcState &s, double const box[3], double prefactor, long long n,
+                      const double *pos, const double *q, double *f, double *energy,
+                      long long *launches, cudaStream_t st) {
+  elc_prepare(s, box, prefactor, st);
+  if (energy)
+    *energy = 0.0;
+  if (n == 0)
+    return;
+  ElcGeom g{};
+  for (int d = 0; d < 3; ++d)
+    g.box[d] = box[d];
+  g.box_h = s.box_h;
+  g.shift = 0.5 * box[2];
+  g.pref_dip = prefactor * 4.0 * kPi / (box[0] * box[1] * box[2]);
+  g.n = n;
+  g.nmodes = static_cast<int>(s.modes.size());
+  g.nfx = s.nfx;
+  g.nfy = s.nfy;
+  g.neutralize = s.prm.neutralize ? 1 : 0;
+  long long const nsc = (static_cast<long long>(s.nfx) + s.nfy) * n;
+  int const nbp = static_cast<int>((n + kElcThreads * kElcPPT - 1) / (kElcThreads * kElcPPT));
+  int const nbf = static_cast<int>((n + kElcThreads - 1) / kElcThreads);
+  s.d_sc.ensure(static_cast<size_t>(nsc) * sizeof(double2));
+  s.d_part.ensure(static_cast<size_t>(nbp) * (g.nmodes * 8 + 3) * sizeof(double));
+  s.d_G.ensure(static_cast<size_t>(g.nmodes * 8 + 3) * sizeof(double));
+  s.d_epart.ensure(static_cast<size_t>(nbf) * sizeof(double));
+  s.d_err.ensure(sizeof(int));
+  P3MX_CUDA(cudaMemsetAsync(s.d_err.p, 0x7f, sizeof(int), st));
+  k_elc_sc<<<static_cast<unsigned>((nsc + kElcThreads - 1) / kElcThreads), kElcThreads, 0, st>>>(
+      g, pos, s.d_sc.as<double2>());
+  dim3 const gs(nbp, std::max(1, (g.nmodes + kElcModesPerBlock - 1) / kElcModesPerBlock));
+  k_elc_sums<<<gs, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                         s.d_sc.as<double2>(), s.d_part.as<double>(),
+                                         s.d_err.as<int>());
+  int const nred = g.nmodes * 8 + 3;
+  k_elc_reduce<<<(nred + 255) / 256, 256, 0, st>>>(g, s.d_modes.as<ElcMode>(), s.d_part.as<double>(),
+                                                   nbp, s.d_G.as<double>());
+  if (energy)
+    k_elc_forces<true><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                                    s.d_sc.as<double2>(), s.d_G.as<double>(), f,
+                                                    s.d_epart.as<double>());
+  else
+    k_elc_forces<false><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                                     s.d_sc.as<double2>(), s.d_G.as<double>(), f,
+                                                     nullptr);
+  P3MX_CUDA(cudaGetLastError());
+  if (launches)
+    *launches += 4;
+  int bad = INT_MAX;
+  double dip[3] = {0, 0, 0};
+  P3MX_CUDA(cudaMemcpyAsync(&bad, s.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (energy) {
+    s.h_epart.assign(nbf, 0.0);
+    P3MX_CUDA(cudaMemcpyAsync(s.h_epart.data(), s.d_epart.p, nbf * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaMemcpyAsync(dip, s.d_G.as<double>() + g.nmodes * 8, 3 * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+  }
+  P3MX_CUDA(cudaStreamSynchronize(st));
+  if (bad >= 0 && bad < n) {
+    double zb[3];
+    P3MX_CUDA(cudaMemcpy(zb, pos + 3 * static_cast<long long>(bad), sizeof zb,
+                         cudaMemcpyDeviceToHost));
+    double const z = zb[2] - std::floor(zb[2] / box[2]) * box[2];
+    char m[160];
+    std::snprintf(m, sizeof m, "Particle %d entered ELC gap region by %g", bad,
+                  z < 0.0 ? z : z - s.box_h);
+    throw Error(P3MX_ERUNTIME, m);
+  }
+  if (energy) {
+    // dipole_energy (elc.cpp:267-343): sums {q (z - L/2), q, q (z - L/2)^2}
+    double const pref = prefactor * 2.0 * kPi / (box[0] * box[1] * box[2]);
+    double e = 2.0 * pref * dip[0] * dip[0];
+    if (!s.prm.neutralize)
+      e += 2.0 * pref *
+           (-dip[1] * dip[2] - (0.25 - 0.5 / 3.0) * (dip[1] * box[2]) * (dip[1] * box[2]));
+    for (double v : s.h_epart)
+      e += v;
+    *energy = 0.5 * e;
+  }
+}
+
+} // namespace p3mx

@@ -154,6 +154,10 @@ class _P3MBase:
         rc = _lib.load().p3mx_activate(self._handle, len(q), _lib.dptr(pos), _lib.dptr(q), 0)
         _lib.check(rc, self._handle)
 
+    def _detach_layer_correction(self):
+        # the actor used on its own again: no ELC on its handle
+        _lib.check(_lib.load().p3mx_set_elc(self._handle, None), self._handle)
+
 
 class P3M(_P3MBase):
     """P3M electrostatics solver (plain FP64 path unless single_precision)."""
@@ -169,3 +173,91 @@ class P3MGPU(_P3MBase):
 
 def _restore_actor(cls, params):
     return cls(**params)
+
+
+def _real(x):
+    return isinstance(x, (float, int, np.floating, np.integer)) and not isinstance(x, bool)
+
+
+class ELC:
+    """Electrostatic layer correction for slab systems (2D-periodic, with an
+    empty gap along z), a mirror of ``espressomd.electrostatics.ELC``
+    (src/python/espressomd/electrostatics.py:288-365): same keyword
+    arguments, defaults and checks.  The base ``actor`` (P3M or P3MGPU)
+    computes the 3D-periodic solution and the correction runs in FP64 CUDA
+    kernels of libp3mx.so.  Dielectric contrasts (``delta_mid_top`` /
+    ``delta_mid_bot`` != 0) are not supported and raise RuntimeError.
+    """
+    _so_name = "Coulomb::ElectrostaticLayerCorrection"
+    _defaults = {"far_cut": -1., "delta_mid_top": 0., "delta_mid_bot": 0.,
+                 "const_pot": False, "pot_diff": 0., "neutralize": True,
+                 "check_neutrality": True}
+    _required = ("actor", "gap_size", "maxPWerror")
+
+    def __init__(self, **kwargs):
+        if any(k not in kwargs for k in self._required):
+            raise ValueError(f"At least the following keys have to be given as keyword "
+                             f"arguments: {sorted(self._required)}, got {sorted(kwargs)}")
+        p = dict(self._defaults)
+        p.update(kwargs)
+        for key in ("maxPWerror", "gap_size", "far_cut"):
+            if not _real(p[key]):
+                raise TypeError(f"{key} has to be a float")
+        if not isinstance(p["neutralize"], (bool, np.bool_)):
+            raise TypeError("neutralize has to be a bool")
+        if not isinstance(p["actor"], _P3MBase):
+            raise TypeError("ELC requires a P3M or P3MGPU actor")
+        self._params = p
+        self._attach()
+
+    @property
+    def actor(self):
+        return self._params["actor"]
+
+    @property
+    def _handle(self):
+        return self.actor._handle
+
+    def _attach(self):
+        p = self._params
+        c = _lib.ElcParams()
+        c.maxPWerror = float(p["maxPWerror"])
+        c.gap_size = float(p["gap_size"])
+        c.far_cut = float(p["far_cut"])
+        c.neutralize = 1 if p["neutralize"] else 0
+        c.delta_mid_top = float(p["delta_mid_top"])
+        c.delta_mid_bot = float(p["delta_mid_bot"])
+        c.const_pot = 1 if p["const_pot"] else 0
+        c.pot_diff = float(p["pot_diff"])
+        _lib.check(_lib.load().p3mx_set_elc(self._handle, ctypes.byref(c)), self._handle)
+        # adapt_epsilon_elc: the base actor is metallic from now on
+        self.actor._params["epsilon"] = _METALLIC
+
+    def get_params(self):
+        out = dict(self._params)
+        fc = ctypes.c_double()
+        if _lib.load().p3mx_get_elc(self._handle, ctypes.byref(fc), None) == 0:
+            out["far_cut"] = fc.value
+        return out
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        params = self.__dict__.get("_params", {})
+        if name == "far_cut":
+            return self.get_params()["far_cut"]
+        if name in params:
+            return params[name]
+        raise AttributeError(name)
+
+    def __reduce__(self):
+        return (_restore_actor, (type(self), dict(self._params)))
+
+    # --- engine-facing calls: the base actor's, then ELC's activation
+    # (ElectrostaticLayerCorrection::on_activation: checks, box_h, far_cut)
+    def _set_system(self, box_l, skin, periodicity):
+        self.actor._set_system(box_l, skin, periodicity)
+
+    def _activate(self, pos, q):
+        self.actor._activate(pos, q)
+        self._attach()

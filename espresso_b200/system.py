@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .electrostatics import P3M, _P3MBase
+from .electrostatics import ELC, P3M, _P3MBase
 from .interactions import BondedInteractions
 
 
@@ -234,11 +234,13 @@ class Electrostatics:
         if actor is None:
             self.clear()
             return
-        if not isinstance(actor, _P3MBase):
-            raise TypeError("only P3M / P3MGPU actors are supported")
+        if not isinstance(actor, (_P3MBase, ELC)):
+            raise TypeError("only P3M / P3MGPU / ELC actors are supported")
         s = self._system
         if s.time_step is None:
             raise RuntimeError("time_step not set")
+        if isinstance(actor, _P3MBase):
+            actor._detach_layer_correction()
         actor._set_system(s.box_l, s.cell_system.skin, s.periodicity)
         actor._activate(s.part._pos, s.part._q)  # raises and leaves no solver on failure
         self._solver = actor

@@ -175,6 +175,39 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q,
                 const int *type, double *f, double *energy3, double *virial27,
                 unsigned flags, void *stream);
 
+/* --- electrostatic layer correction (slab geometry) -------------------- */
+
+/* Parameters of espressomd.electrostatics.ELC (src/python/espressomd/
+ * electrostatics.py:288-365) as the elc_data constructor takes them
+ * (src/core/electrostatics/elc.cpp:1056-1102).  Dielectric contrasts are not
+ * supported: delta_mid_top and delta_mid_bot must be 0 (const_pot then has
+ * no effect, as in the reference, where it needs a contrast). */
+typedef struct {
+  double maxPWerror;
+  double gap_size;
+  double far_cut;       /* -1: tuned from maxPWerror (tune_far_cut) */
+  int neutralize;       /* bool; reference default 1 */
+  double delta_mid_top; /* must be 0 */
+  double delta_mid_bot; /* must be 0 */
+  int const_pot;        /* bool */
+  double pot_diff;
+} p3mx_elc_params;
+
+/* Attaches ELC to the actor, replacing the ElectrostaticLayerCorrection
+ * constructor and activation (elc.hpp ElectrostaticLayerCorrection,
+ * elc.cpp:1104-1109, on_activation): parameter checks, the base P3M set to
+ * metallic (adapt_epsilon_elc, p3m.impl.hpp:112-114), slab height and
+ * far cutoff (recalc_box_h elc.cpp:1020-1030, tune_far_cut :942-973).  NULL
+ * detaches.  While attached, p3mx_forces and p3mx_long_range add the ELC
+ * forces and energy (add_long_range_forces :1231-1254, long_range_energy
+ * :1189-1229) and report a zero k-space virial (the reference computes no
+ * ELC pressure, electrostatics/coulomb.cpp:124-131).  A charged particle in
+ * the gap fails the call with "Particle <i> entered ELC gap region by <dz>"
+ * (check_gap :184-194). */
+int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p);
+/* The far-formula cutoff in use and the slab height L_z - gap_size. */
+int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h);
+
 /* Cell-system introspection for parity tests: the cell grid and the cell
  * index of each particle as RegularDecomposition::position_to_cell_index
  * returns it (RegularDecomposition.cpp:51-80, 289-385), and the Verlet pair

@@ -1,0 +1,135 @@
+"""GPU tests of the electrostatic layer correction (ELC) through the C ABI.
+
+* the reference's testsuite/python/coulomb_mixed_periodicity.py:84-121: 285
+  charges in a 10 x 10 x 12 box with a 3-unit gap; P3M (accuracy 1e-6, mesh
+  42 x 42 x 50, r_cut 3, alpha and cao tuned) + ELC (maxPWerror 1e-6) against
+  the MMM2D forces (1e-5) and energy (1e-4); resizing the box and back
+  leaves forces and energy unchanged (1e-9);
+* testsuite/python/p3m_madelung.py:236-277: ionic sheet with ELC, energy
+  per ion equal to the square-lattice Madelung constant (rtol 1e-7);
+* the ELC part alone (ELC run minus the bare P3M run) against the oracle's
+  FP64 restatement, neutral and non-neutral, neutralize on and off
+  (1e-9 of the largest force; energy 1e-9 relative);
+* the gap check of testsuite/python/elc.py:92-104 (a charge in the gap,
+  above and below, raises "entered ELC gap region").
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import espresso_b200 as eb
+from espresso_b200.electrostatics import ELC, P3M, P3MGPU
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _system(box, pos, q):
+    s = eb.System(box_l=list(box))
+    s.time_step = 0.01
+    s.cell_system.skin = 0.0
+    s.part.add(pos=pos, q=q)
+    return s
+
+
+@pytest.mark.parametrize("cls,ftol", [(P3M, None), (P3MGPU, 5e-5)])
+def test_elc_vs_mmm2d_golden(cls, ftol):
+    g = np.load(os.path.join(GOLD, "coulomb_mixed_periodicity.npz"))
+    s = _system(g["box"], g["pos"], g["q"])
+    p3m = cls(prefactor=1.0, accuracy=float(g["accuracy"]), mesh=[int(m) for m in g["mesh"]],
+              r_cut=float(g["r_cut"]))
+    elc = ELC(actor=p3m, maxPWerror=float(g["max_pw_error"]), gap_size=float(g["gap_size"]))
+    s.electrostatics.solver = elc
+    s.integrator.run(0)
+    f1 = np.copy(s.part.all().f)
+    e1 = s.analysis.energy()["total"]
+    np.testing.assert_allclose(f1, g["forces"], atol=ftol or float(g["force_atol"]), rtol=0)
+    assert abs(e1 - float(g["energy"])) < float(g["energy_atol"])
+    # re-initialisation through a box change and back (coulomb_mixed_periodicity.py:67-82)
+    box0 = np.copy(s.box_l)
+    pos0 = np.copy(s.part.all().pos)
+    for d in range(3):
+        b = np.copy(box0)
+        b[d] *= 1.05
+        s.box_l = b
+        s.part.all().pos = pos0 * (b / box0)
+        s.integrator.run(0)
+    s.box_l = box0
+    s.part.all().pos = pos0
+    s.integrator.run(0)
+    np.testing.assert_allclose(s.part.all().f, f1, rtol=1e-9, atol=1e-12)
+    assert abs(s.analysis.energy()["total"] - e1) <= 1e-9 * abs(e1)
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_elc_ionic_sheet_madelung(cls):
+    k = json.load(open(os.path.join(GOLD, "known_answers.json")))["madelung_sheet"]
+    n = 2 * k["n_pairs"]
+    jj, kk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    pos = np.stack([jj.ravel(), kk.ravel(), np.zeros(n * n)], axis=1).astype(float)
+    q = (-1.0) ** (jj.ravel() + kk.ravel())
+    s = _system([n, n, 2.0 * n], pos, q)
+    p3m = cls(prefactor=1.0, accuracy=k["accuracy"], mesh=k["mesh"], r_cut=k["r_cut"],
+              cao=k["cao"], alpha=k["alpha"], tune=False)
+    s.electrostatics.solver = ELC(actor=p3m, **k["elc"])
+    e_ion = 2.0 * s.analysis.energy()["coulomb"] / len(q)
+    np.testing.assert_allclose(e_ion, k["madelung"], rtol=k["energy_rtol"], atol=0)
+
+
+@pytest.mark.parametrize("neutral,neutralize", [(True, True), (False, True), (False, False)])
+def test_elc_part_vs_oracle(neutral, neutralize):
+    rng = np.random.default_rng(7)
+    box = np.array([9.0, 11.0, 14.0])
+    gap = 3.5
+    n = 400
+    pos = rng.uniform([0, 0, 0.2], [box[0], box[1], box[2] - gap - 0.2], (n, 3))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    if not neutral:
+        q[:3] = 2.0
+    s = _system(box, pos, q)
+    p3m = P3M(prefactor=1.7, accuracy=1e-4, mesh=32, cao=5, r_cut=2.5, alpha=1.3, tune=False,
+              check_neutrality=False)
+    s.electrostatics.solver = p3m
+    s.integrator.run(0)
+    f0 = np.copy(s.part.all().f)
+    e0 = s.analysis.energy()["coulomb"]
+    elc = ELC(actor=p3m, maxPWerror=1e-7, gap_size=gap, neutralize=neutralize)
+    s.electrostatics.solver = elc
+    s.integrator.run(0)
+    f1 = np.copy(s.part.all().f)
+    e1 = s.analysis.energy()["coulomb"]
+    fc = elc.far_cut
+    assert fc == pytest.approx(O.elc_far_cut(box, box[2] - gap, 1e-7), rel=1e-12)
+    fo, eo = O.elc(box, gap, pos, q, 1.7, fc, neutralize=neutralize)
+    np.testing.assert_allclose(f1 - f0, fo, atol=1e-9 * np.abs(fo).max(), rtol=0)
+    assert abs((e1 - e0) - eo) <= 1e-9 * max(abs(eo), 1.0)
+    # the bare actor again: no correction left on it
+    s.electrostatics.solver = p3m
+    s.integrator.run(0)
+    np.testing.assert_allclose(s.part.all().f, f0, rtol=0, atol=1e-12)
+
+
+def test_elc_gap_error():
+    box = np.array([10.0, 10.0, 13.0])
+    gap = 3.0
+    s = _system(box, [[1.0, 1.0, 1.0], [5.0, 5.0, 9.0]], [1.0, -1.0])
+    p3m = P3M(prefactor=1.0, accuracy=1e-3, mesh=32, cao=5, r_cut=2.0, alpha=1.5, tune=False)
+    s.electrostatics.solver = ELC(actor=p3m, maxPWerror=1e-3, gap_size=gap)
+    s.integrator.run(0)
+    p1 = s.part.by_id(0)
+    # positive direction (elc.py:92-97)
+    p1.pos = [box[0] / 2, box[1] / 2, box[2] - gap / 2]
+    with pytest.raises(Exception):
+        s.analysis.energy()
+    with pytest.raises(Exception, match="entered ELC gap region"):
+        s.integrator.run(2)
+    # negative direction (folded into the gap from below; elc.py:98-104)
+    p1.pos = [box[0] / 2, box[1] / 2, -gap / 2]
+    with pytest.raises(Exception, match="entered ELC gap region"):
+        s.integrator.run(0)
+    # back in the slab: usable again
+    p1.pos = [1.0, 1.0, 1.0]
+    s.integrator.run(0)
