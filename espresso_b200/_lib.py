@@ -99,7 +99,7 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_int)]),
     "p3mx_bond_observables": (ctypes.c_int, [_vp, _sz, _vp, _dp, _dp, ctypes.c_uint, _vp]),
     "p3mx_set_elc": (ctypes.c_int, [_vp, ctypes.POINTER(ElcParams)]),
-    "p3mx_get_elc": (ctypes.c_int, [_vp, _dp, _dp]),
+    "p3mx_get_elc": (ctypes.c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int)]),
     "p3mx_batch_set_bonds": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(BondParams), _sz,
                                             ctypes.POINTER(ctypes.c_int)]),
     "p3mx_batch_profile": (ctypes.c_int, [_vp, ctypes.c_int, _dp,

@@ -982,7 +982,7 @@ int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p) {
   });
 }
 
-int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h) {
+int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h, int *n_modes) {
   if (!h)
     return P3MX_EHANDLE;
   if (!h->elc)
@@ -991,6 +991,8 @@ int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h) {
     *far_cut = h->elc->far_cut;
   if (box_h)
     *box_h = h->elc->box_h;
+  if (n_modes)
+    *n_modes = static_cast<int>(h->elc->modes.size());
   return 0;
 }
 
@@ -1200,6 +1202,12 @@ int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names, int c
       throw Error(P3MX_ERUNTIME, "actor not activated");
     static std::vector<std::string> keep;
     auto prof = h->eng->profile(std::max(1, reps), h->eng->stream());
+    if (h->elc) {
+      Engine &e = *h->eng;
+      auto pe = elc_profile(*h->elc, h->sys.box, h->prm.prefactor, static_cast<long long>(h->n),
+                            e.d_pos(), e.d_q(), e.d_force(), std::max(1, reps), e.stream());
+      prof.insert(prof.end(), pe.begin(), pe.end());
+    }
     keep.clear();
     for (auto const &p : prof)
       keep.push_back(p.first);

@@ -12,12 +12,15 @@
 // energy (PoQ_energy :620-634, PQ_energy :812-828).  The dipole term
 // (add_dipole_force :201-264, dipole_energy :267-343) is three more sums.
 //
+// The sin / cos of a particle's x and y phases at frequency k (the
+// reference caches them per particle, calc_sc_cache :107-125) are carried in
+// registers from mode to mode: the next frequency is one rotation by the
+// unit phase (4 FMA), a new p or a chunk start takes one sincos.  Modes run
+// p-major, so a pq-mode block needs one x sincos per p and rotations in q.
+//
 // Device layout (all FP64):
-//   sc   : per frequency f and particle i, (sin, cos) of 2 pi f x_i / L_x
-//          (f = 1..nfx) then of 2 pi f y_i / L_y (f = 1..nfy), [f][i]
-//          (calc_sc_cache :107-125);
-//   part : per particle tile b and mode m, the 8 product sums
-//          [b][m][8], then per tile the 3 dipole sums [b][3];
+//   part : per mode m and component c, the product sums of every particle
+//          tile b, [m * 8 + c][b]; then the 3 dipole sums [nm8 + c][b];
 //   G    : per mode the 8 sums over all tiles times the mode prefactor, then
 //          the 3 dipole sums;
 //   epart: per block of the force kernel, its energy sum (EV only).
@@ -47,61 +50,103 @@ struct ElcGeom {
 };
 
 constexpr int kElcThreads = 256;
-constexpr int kElcPPT = 4;            // particles per thread in the sums kernel
+constexpr int kElcPPT = 2;            // particles per thread in the sums kernel
 constexpr int kElcModesPerBlock = 16; // modes per block of the sums kernel
 
 __device__ __forceinline__ double elc_fold(double x, double l) { return x - floor(x / l) * l; }
 
-// sin / cos of the x and y phases of every particle at every frequency.
-__global__ void __launch_bounds__(kElcThreads)
-k_elc_sc(ElcGeom g, const double *__restrict__ pos, double2 *__restrict__ sc) {
-  long long const t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  long long const nf = static_cast<long long>(g.nfx) + g.nfy;
-  if (t >= nf * g.n)
+// sin / cos of the phase 2 pi k u x at frequency k, from the state of the
+// previous mode: kept (same k), rotated by the unit phase (k - 1), the unit
+// phase itself (k = 1) or computed (c2pu = 2 pi u, as the reference forms
+// its argument (2 pi u k) x).
+struct ElcPhase {
+  int k;
+  double s, c;
+};
+
+__device__ __forceinline__ void elc_phase(ElcPhase &ph, int k, double s1, double c1, double c2pu,
+                                          double x) {
+  if (ph.k == k)
     return;
-  long long const f = t / g.n, i = t - f * g.n;
-  int const dir = f < g.nfx ? 0 : 1;
-  int const freq = static_cast<int>(dir == 0 ? f + 1 : f - g.nfx + 1);
-  double const c = elc_fold(pos[3 * i + dir], g.box[dir]);
-  double const pref = 2.0 * kPi * (1.0 / g.box[dir]) * static_cast<double>(freq);
-  double s, co;
-  sincos(pref * c, &s, &co);
-  sc[t] = make_double2(s, co);
+  if (ph.k == k - 1) {
+    double const sn = ph.s * c1 + ph.c * s1;
+    double const cn = ph.c * c1 - ph.s * s1;
+    ph.s = sn;
+    ph.c = cn;
+  } else if (k == 1) {
+    ph.s = s1;
+    ph.c = c1;
+  } else {
+    sincos((c2pu * static_cast<double>(k)) * x, &ph.s, &ph.c);
+  }
+  ph.k = k;
 }
 
-// the 4 / 8 products of particle i for mode md (z folded, e = exp(omega z))
-__device__ __forceinline__ int elc_products(ElcMode const &md, ElcGeom const &g,
-                                            const double2 *__restrict__ sc, long long i,
-                                            double q, double z, double v[8]) {
-  double const e = exp(md.omega * z);
+// One particle's state: folded position, charge, unit phases and the
+// current x / y phases.
+struct ElcPart {
+  double x, y, z, q;
+  double s1x, c1x, s1y, c1y;
+  ElcPhase px, py;
+};
+
+__device__ __forceinline__ void elc_part_init(ElcPart &P, ElcGeom const &g,
+                                              const double *__restrict__ pos, double q) {
+  P.x = elc_fold(pos[0], g.box[0]);
+  P.y = elc_fold(pos[1], g.box[1]);
+  P.z = elc_fold(pos[2], g.box[2]);
+  P.q = q;
+  sincos((2.0 * kPi * (1.0 / g.box[0])) * P.x, &P.s1x, &P.c1x);
+  sincos((2.0 * kPi * (1.0 / g.box[1])) * P.y, &P.s1y, &P.c1y);
+  P.px.k = P.py.k = -1;
+  P.px.s = P.px.c = P.py.s = P.py.c = 0.0;
+}
+
+// the 4 / 8 products of the particle for mode md (e = exp(omega z); the
+// reference divides by e, here one reciprocal is multiplied in)
+__device__ __forceinline__ int elc_products(ElcMode const &md, ElcGeom const &g, ElcPart &P,
+                                            double v[8]) {
+  double const e = exp(md.omega * P.z);
+  double const ie = 1.0 / e;
+  double const q = P.q;
   if (md.kind < 2) {
-    long long const f = (md.kind == 0) ? (md.p - 1) : (g.nfx + md.q - 1);
-    double2 const a = sc[f * g.n + i];
+    double sn, cs;
+    if (md.kind == 0) {
+      elc_phase(P.px, md.p, P.s1x, P.c1x, 2.0 * kPi * (1.0 / g.box[0]), P.x);
+      sn = P.px.s;
+      cs = P.px.c;
+    } else {
+      elc_phase(P.py, md.q, P.s1y, P.c1y, 2.0 * kPi * (1.0 / g.box[1]), P.y);
+      sn = P.py.s;
+      cs = P.py.c;
+    }
     // POQESP, POQECP, POQESM, POQECM
-    v[0] = q * a.x * e;
-    v[1] = q * a.y * e;
-    v[2] = q * a.x / e;
-    v[3] = q * a.y / e;
+    v[0] = q * sn * e;
+    v[1] = q * cs * e;
+    v[2] = q * sn * ie;
+    v[3] = q * cs * ie;
     return 4;
   }
-  double2 const ax = sc[static_cast<long long>(md.p - 1) * g.n + i];
-  double2 const ay = sc[static_cast<long long>(g.nfx + md.q - 1) * g.n + i];
+  elc_phase(P.px, md.p, P.s1x, P.c1x, 2.0 * kPi * (1.0 / g.box[0]), P.x);
+  elc_phase(P.py, md.q, P.s1y, P.c1y, 2.0 * kPi * (1.0 / g.box[1]), P.y);
+  double const sx = P.px.s, cx = P.px.c, sy = P.py.s, cy = P.py.c;
   // PQESSP, PQESCP, PQECSP, PQECCP, PQESSM, PQESCM, PQECSM, PQECCM
-  v[0] = ax.x * ay.x * q * e;
-  v[1] = ax.x * ay.y * q * e;
-  v[2] = ax.y * ay.x * q * e;
-  v[3] = ax.y * ay.y * q * e;
-  v[4] = ax.x * ay.x * q / e;
-  v[5] = ax.x * ay.y * q / e;
-  v[6] = ax.y * ay.x * q / e;
-  v[7] = ax.y * ay.y * q / e;
+  v[0] = sx * sy * q * e;
+  v[1] = sx * cy * q * e;
+  v[2] = cx * sy * q * e;
+  v[3] = cx * cy * q * e;
+  v[4] = sx * sy * q * ie;
+  v[5] = sx * cy * q * ie;
+  v[6] = cx * sy * q * ie;
+  v[7] = cx * cy * q * ie;
   return 8;
 }
 
 // sum of v over the block (256 threads) in a fixed order, written by threads
-// 0..W-1 to out[0..W); red: scratch of [8 warps][W] doubles.
+// 0..W-1 to out[c * stride] for c < W; red: scratch of [8 warps][W] doubles.
 template <int W>
-__device__ __forceinline__ void elc_block_sum(double (&v)[W], double *red, double *out) {
+__device__ __forceinline__ void elc_block_sum(double (&v)[W], double *red, double *out,
+                                              long long stride = 1) {
   int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int c = 0; c < W; ++c) {
@@ -117,7 +162,7 @@ __device__ __forceinline__ void elc_block_sum(double (&v)[W], double *red, doubl
     double s = 0.0;
     for (int w = 0; w < kElcThreads / 32; ++w)
       s += red[w * W + threadIdx.x];
-    out[threadIdx.x] = s;
+    out[threadIdx.x * stride] = s;
   }
   __syncthreads();
 }
@@ -127,17 +172,15 @@ __device__ __forceinline__ void elc_block_sum(double (&v)[W], double *red, doubl
 // (check_gap :184-194: a charged particle below 0 or above L_z - gap).
 __global__ void __launch_bounds__(kElcThreads)
 k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ pos,
-           const double *__restrict__ qv, const double2 *__restrict__ sc,
-           double *__restrict__ part, int *__restrict__ gap_err) {
+           const double *__restrict__ qv, double *__restrict__ part, int *__restrict__ gap_err) {
   __shared__ double red[(kElcThreads / 32) * 8];
   long long const tile0 = static_cast<long long>(blockIdx.x) * kElcThreads * kElcPPT;
-  double zz[kElcPPT], qq[kElcPPT];
+  ElcPart P[kElcPPT];
 #pragma unroll
   for (int k = 0; k < kElcPPT; ++k) {
     long long const i = tile0 + k * kElcThreads + threadIdx.x;
-    bool const ok = i < g.n;
-    qq[k] = ok ? qv[i] : 0.0;
-    zz[k] = ok ? elc_fold(pos[3 * i + 2], g.box[2]) : 0.0;
+    long long const ic = i < g.n ? i : 0;
+    elc_part_init(P[k], g, pos + 3 * ic, i < g.n ? qv[i] : 0.0);
   }
   int const m0 = blockIdx.y * kElcModesPerBlock;
   int const m1 = min(g.nmodes, m0 + kElcModesPerBlock);
@@ -146,52 +189,49 @@ k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restric
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < kElcPPT; ++k) {
-      long long const i = tile0 + k * kElcThreads + threadIdx.x;
-      if (i < g.n && qq[k] != 0.0) {
-        double v[8];
-        int const w = elc_products(md, g, sc, i, qq[k], zz[k], v);
-        for (int c = 0; c < w; ++c)
-          acc[c] += v[c];
-      }
+      // uncharged particles and the tile's tail add zeros (q = 0)
+      double v[8];
+      int const w = elc_products(md, g, P[k], v);
+      for (int c = 0; c < w; ++c)
+        acc[c] += v[c];
     }
-    elc_block_sum<8>(acc, red, part + (static_cast<long long>(blockIdx.x) * g.nmodes + m) * 8);
+    elc_block_sum<8>(acc, red, part + static_cast<long long>(m) * 8 * gridDim.x + blockIdx.x,
+                     gridDim.x);
   }
   if (blockIdx.y == 0) {
     double d[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < kElcPPT; ++k) {
       long long const i = tile0 + k * kElcThreads + threadIdx.x;
-      if (i < g.n && qq[k] != 0.0) {
-        double const dz = zz[k] - g.shift;
-        d[0] += qq[k] * dz;
-        d[1] += qq[k];
-        d[2] += qq[k] * dz * dz;
-        if (zz[k] < 0.0 || zz[k] > g.box_h)
+      if (i < g.n && P[k].q != 0.0) {
+        double const dz = P[k].z - g.shift;
+        d[0] += P[k].q * dz;
+        d[1] += P[k].q;
+        d[2] += P[k].q * dz * dz;
+        if (P[k].z < 0.0 || P[k].z > g.box_h)
           atomicMin(gap_err, static_cast<int>(i));
       }
     }
     long long const nbp = gridDim.x;
-    elc_block_sum<3>(d, red, part + nbp * g.nmodes * 8 + static_cast<long long>(blockIdx.x) * 3);
+    elc_block_sum<3>(d, red, part + nbp * g.nmodes * 8 + blockIdx.x, nbp);
   }
 }
 
-// G[m][c] = pref_m * sum over tiles (fixed order); the dipole sums after them.
-__global__ void k_elc_reduce(ElcGeom g, const ElcMode *__restrict__ modes,
-                             const double *__restrict__ part, int nbp, double *__restrict__ G) {
-  int const t = blockIdx.x * blockDim.x + threadIdx.x;
-  int const nm8 = g.nmodes * 8;
-  if (t < nm8) {
-    double s = 0.0;
-    for (int b = 0; b < nbp; ++b)
-      s += part[static_cast<long long>(b) * nm8 + t];
-    G[t] = modes[t >> 3].pref * s;
-  } else if (t < nm8 + 3) {
-    int const c = t - nm8;
-    double s = 0.0;
-    for (int b = 0; b < nbp; ++b)
-      s += part[static_cast<long long>(nbp) * nm8 + static_cast<long long>(b) * 3 + c];
-    G[t] = s;
-  }
+// G[m * 8 + c] = pref_m * (sum over tiles), one block per sum, tiles read
+// contiguously and added in a fixed order; the 3 dipole sums after them.
+__global__ void __launch_bounds__(kElcThreads)
+k_elc_reduce(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ part,
+             int nbp, double *__restrict__ G) {
+  __shared__ double red[kElcThreads / 32];
+  int const t = blockIdx.x;
+  const double *row = part + static_cast<long long>(t) * nbp;
+  double v[1] = {0.0};
+  for (int b = threadIdx.x; b < nbp; b += kElcThreads)
+    v[0] += row[b];
+  __shared__ double out[1];
+  elc_block_sum<1>(v, red, out);
+  if (threadIdx.x == 0)
+    G[t] = (t < g.nmodes * 8) ? modes[t >> 3].pref * out[0] : out[0];
 }
 
 // Per particle: the mode forces from the global sums (add_PoQ_force,
@@ -200,19 +240,20 @@ __global__ void k_elc_reduce(ElcGeom g, const ElcMode *__restrict__ modes,
 template <bool EV>
 __global__ void __launch_bounds__(kElcThreads)
 k_elc_forces(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ pos,
-             const double *__restrict__ qv, const double2 *__restrict__ sc,
-             const double *__restrict__ G, double *__restrict__ f, double *__restrict__ epart) {
+             const double *__restrict__ qv, const double *__restrict__ G, double *__restrict__ f,
+             double *__restrict__ epart) {
   __shared__ double red[(kElcThreads / 32) * 8];
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   double en[1] = {0.0};
   if (i < g.n && qv[i] != 0.0) {
-    double const q = qv[i];
-    double const z = elc_fold(pos[3 * i + 2], g.box[2]);
+    ElcPart P;
+    elc_part_init(P, g, pos + 3 * i, qv[i]);
+    double const q = P.q, z = P.z;
     double fx = 0.0, fy = 0.0, fz = 0.0;
     for (int m = 0; m < g.nmodes; ++m) {
       ElcMode const md = modes[m];
       double v[8];
-      elc_products(md, g, sc, i, q, z, v);
+      elc_products(md, g, P, v);
       const double *Gm = G + static_cast<long long>(m) * 8;
       if (md.kind < 2) {
         double const ft = v[2] * Gm[1] - v[3] * Gm[0] + v[0] * Gm[3] - v[1] * Gm[2];

@@ -12,6 +12,8 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <string>
+#include <utility>
 #include <vector>
 
 namespace p3mx {
@@ -24,7 +26,7 @@ struct ElcState {
   double built_prefactor = 0.0;
   std::vector<ElcMode> modes;
   int nfx = 0, nfy = 0;
-  DevBuf d_modes, d_sc, d_part, d_G, d_epart, d_err;
+  DevBuf d_modes, d_part, d_G, d_epart, d_err;
   std::vector<double> h_epart;
 };
 
@@ -127,6 +129,85 @@ inline void elc_prepare(ElcState &s, double const box[3], double prefactor, cuda
   s.built_prefactor = prefactor;
 }
 
+// Kernel geometry of one ELC evaluation of n particles.
+inline ElcGeom elc_geom(ElcState const &s, double const box[3], double prefactor, long long n) {
+  ElcGeom g{};
+  for (int d = 0; d < 3; ++d)
+    g.box[d] = box[d];
+  g.box_h = s.box_h;
+  g.shift = 0.5 * box[2];
+  g.pref_dip = prefactor * 4.0 * kPi / (box[0] * box[1] * box[2]);
+  g.n = n;
+  g.nmodes = static_cast<int>(s.modes.size());
+  g.nfx = s.nfx;
+  g.nfy = s.nfy;
+  g.neutralize = s.prm.neutralize ? 1 : 0;
+  return g;
+}
+
+// The three kernels of one evaluation on st; ev (4 events or nullptr) is
+// recorded before, between and after them for the stage profile.
+inline void elc_launch(ElcState &s, ElcGeom const &g, const double *pos, const double *q,
+                       double *f, bool want_e, cudaStream_t st, cudaEvent_t *ev) {
+  long long const n = g.n;
+  int const nbp = static_cast<int>((n + kElcThreads * kElcPPT - 1) / (kElcThreads * kElcPPT));
+  int const nbf = static_cast<int>((n + kElcThreads - 1) / kElcThreads);
+  s.d_part.ensure(static_cast<size_t>(nbp) * (g.nmodes * 8 + 3) * sizeof(double));
+  s.d_G.ensure(static_cast<size_t>(g.nmodes * 8 + 3) * sizeof(double));
+  s.d_epart.ensure(static_cast<size_t>(nbf) * sizeof(double));
+  s.d_err.ensure(sizeof(int));
+  P3MX_CUDA(cudaMemsetAsync(s.d_err.p, 0x7f, sizeof(int), st));
+  if (ev)
+    P3MX_CUDA(cudaEventRecord(ev[0], st));
+  dim3 const gs(nbp, std::max(1, (g.nmodes + kElcModesPerBlock - 1) / kElcModesPerBlock));
+  k_elc_sums<<<gs, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                         s.d_part.as<double>(), s.d_err.as<int>());
+  if (ev)
+    P3MX_CUDA(cudaEventRecord(ev[1], st));
+  int const nred = g.nmodes * 8 + 3;
+  k_elc_reduce<<<nred, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), s.d_part.as<double>(),
+                                             nbp, s.d_G.as<double>());
+  if (ev)
+    P3MX_CUDA(cudaEventRecord(ev[2], st));
+  if (want_e)
+    k_elc_forces<true><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                                    s.d_G.as<double>(), f, s.d_epart.as<double>());
+  else
+    k_elc_forces<false><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
+                                                     s.d_G.as<double>(), f, nullptr);
+  if (ev)
+    P3MX_CUDA(cudaEventRecord(ev[3], st));
+  P3MX_CUDA(cudaGetLastError());
+}
+
+// Mean device time (ms) of each ELC kernel over reps evaluations of the
+// forces (no energy) into f; names elc_sums, elc_reduce, elc_forces.
+inline std::vector<std::pair<std::string, double>>
+elc_profile(ElcState &s, double const box[3], double prefactor, long long n, const double *pos,
+            const double *q, double *f, int reps, cudaStream_t st) {
+  elc_prepare(s, box, prefactor, st);
+  std::vector<std::pair<std::string, double>> out = {
+      {"elc_sums", 0.0}, {"elc_reduce", 0.0}, {"elc_forces", 0.0}};
+  if (n == 0)
+    return out;
+  ElcGeom const g = elc_geom(s, box, prefactor, n);
+  cudaEvent_t ev[4];
+  for (auto &e : ev)
+    P3MX_CUDA(cudaEventCreate(&e));
+  for (int r = 0; r < reps; ++r) {
+    elc_launch(s, g, pos, q, f, false, st, ev);
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < 3; ++k) {
+      float ms = 0.f;
+      P3MX_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      out[k].second += ms / reps;
+    }
+  }
+  for (auto &e : ev)
+    cudaEventDestroy(e);
+  return out;
+}
+
 // Adds the ELC forces to f (device, 3n FP64, original particle order) for
 // the positions and charges on the device; with energy != nullptr also the
 // ELC energy (calc_energy :885-940: dipole + mode terms, halved).  Ends with
@@ -140,46 +221,11 @@ inline void elc_apply(ElcState &s, double const box[3], double prefactor, long l
     *energy = 0.0;
   if (n == 0)
     return;
-  ElcGeom g{};
-  for (int d = 0; d < 3; ++d)
-    g.box[d] = box[d];
-  g.box_h = s.box_h;
-  g.shift = 0.5 * box[2];
-  g.pref_dip = prefactor * 4.0 * kPi / (box[0] * box[1] * box[2]);
-  g.n = n;
-  g.nmodes = static_cast<int>(s.modes.size());
-  g.nfx = s.nfx;
-  g.nfy = s.nfy;
-  g.neutralize = s.prm.neutralize ? 1 : 0;
-  long long const nsc = (static_cast<long long>(s.nfx) + s.nfy) * n;
-  int const nbp = static_cast<int>((n + kElcThreads * kElcPPT - 1) / (kElcThreads * kElcPPT));
+  ElcGeom const g = elc_geom(s, box, prefactor, n);
   int const nbf = static_cast<int>((n + kElcThreads - 1) / kElcThreads);
-  s.d_sc.ensure(static_cast<size_t>(nsc) * sizeof(double2));
-  s.d_part.ensure(static_cast<size_t>(nbp) * (g.nmodes * 8 + 3) * sizeof(double));
-  s.d_G.ensure(static_cast<size_t>(g.nmodes * 8 + 3) * sizeof(double));
-  s.d_epart.ensure(static_cast<size_t>(nbf) * sizeof(double));
-  s.d_err.ensure(sizeof(int));
-  P3MX_CUDA(cudaMemsetAsync(s.d_err.p, 0x7f, sizeof(int), st));
-  k_elc_sc<<<static_cast<unsigned>((nsc + kElcThreads - 1) / kElcThreads), kElcThreads, 0, st>>>(
-      g, pos, s.d_sc.as<double2>());
-  dim3 const gs(nbp, std::max(1, (g.nmodes + kElcModesPerBlock - 1) / kElcModesPerBlock));
-  k_elc_sums<<<gs, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
-                                         s.d_sc.as<double2>(), s.d_part.as<double>(),
-                                         s.d_err.as<int>());
-  int const nred = g.nmodes * 8 + 3;
-  k_elc_reduce<<<(nred + 255) / 256, 256, 0, st>>>(g, s.d_modes.as<ElcMode>(), s.d_part.as<double>(),
-                                                   nbp, s.d_G.as<double>());
-  if (energy)
-    k_elc_forces<true><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
-                                                    s.d_sc.as<double2>(), s.d_G.as<double>(), f,
-                                                    s.d_epart.as<double>());
-  else
-    k_elc_forces<false><<<nbf, kElcThreads, 0, st>>>(g, s.d_modes.as<ElcMode>(), pos, q,
-                                                     s.d_sc.as<double2>(), s.d_G.as<double>(), f,
-                                                     nullptr);
-  P3MX_CUDA(cudaGetLastError());
+  elc_launch(s, g, pos, q, f, energy != nullptr, st, nullptr);
   if (launches)
-    *launches += 4;
+    *launches += 3;
   int bad = INT_MAX;
   double dip[3] = {0, 0, 0};
   P3MX_CUDA(cudaMemcpyAsync(&bad, s.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));

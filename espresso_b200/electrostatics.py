@@ -236,7 +236,7 @@ class ELC:
     def get_params(self):
         out = dict(self._params)
         fc = ctypes.c_double()
-        if _lib.load().p3mx_get_elc(self._handle, ctypes.byref(fc), None) == 0:
+        if _lib.load().p3mx_get_elc(self._handle, ctypes.byref(fc), None, None) == 0:
             out["far_cut"] = fc.value
         return out
 

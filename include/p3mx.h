@@ -205,8 +205,9 @@ typedef struct {
  * the gap fails the call with "Particle <i> entered ELC gap region by <dz>"
  * (check_gap :184-194). */
 int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p);
-/* The far-formula cutoff in use and the slab height L_z - gap_size. */
-int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h);
+/* The far-formula cutoff in use, the slab height L_z - gap_size and the
+ * number of Fourier modes summed (each may be NULL). */
+int p3mx_get_elc(const p3mx_handle *h, double *far_cut, double *box_h, int *n_modes);
 
 /* Cell-system introspection for parity tests: the cell grid and the cell
  * index of each particle as RegularDecomposition::position_to_cell_index
@@ -227,7 +228,9 @@ int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap);
 /* Stage profile of one force evaluation with the current particles (no
  * counterpart in the reference, which has no GPU timers): per-stage mean
  * device time in ms over `reps` evaluations, stage names in
- * names[k] (static strings).  *nstages receives the stage count. */
+ * names[k] (static strings).  *nstages receives the stage count.  With ELC
+ * attached (p3mx_set_elc) its three kernels follow: elc_sums, elc_reduce,
+ * elc_forces. */
 int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names,
                  int cap, int *nstages);
 /* Total number of kernels launched by the handle's engines so far. */

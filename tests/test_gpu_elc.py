@@ -13,6 +13,7 @@
 * the gap check of testsuite/python/elc.py:92-104 (a charge in the gap,
   above and below, raises "entered ELC gap region").
 """
+import ctypes
 import json
 import os
 
@@ -20,6 +21,7 @@ import numpy as np
 import pytest
 
 import espresso_b200 as eb
+from espresso_b200 import _lib
 from espresso_b200.electrostatics import ELC, P3M, P3MGPU
 from oracle import oracle as O
 
@@ -103,6 +105,9 @@ def test_elc_part_vs_oracle(neutral, neutralize):
     e1 = s.analysis.energy()["coulomb"]
     fc = elc.far_cut
     assert fc == pytest.approx(O.elc_far_cut(box, box[2] - gap, 1e-7), rel=1e-12)
+    nm = ctypes.c_int()
+    assert _lib.load().p3mx_get_elc(elc._handle, None, None, ctypes.byref(nm)) == 0
+    assert nm.value == len(O.elc_modes(box, fc)) > 20
     fo, eo = O.elc(box, gap, pos, q, 1.7, fc, neutralize=neutralize)
     np.testing.assert_allclose(f1 - f0, fo, atol=1e-9 * np.abs(fo).max(), rtol=0)
     assert abs((e1 - e0) - eo) <= 1e-9 * max(abs(eo), 1.0)
