@@ -40,3 +40,15 @@ def test_required_keys_and_defaults(p3m):
     assert p3m.epsilon == 0.0
     # const_pot without a dielectric contrast has no effect (elc.cpp:1063)
     ELC(actor=p3m, gap_size=2.0, maxPWerror=1e-4, const_pot=True, pot_diff=1.0)
+
+
+def test_pickle_round_trip(p3m):
+    """A pickled ELC actor restores its parameters and its base actor
+    (checkpointing as the reference's script interface does)."""
+    import pickle
+    elc = ELC(actor=p3m, gap_size=2.5, maxPWerror=1e-5, far_cut=0.3, neutralize=False)
+    back = pickle.loads(pickle.dumps(elc))
+    assert isinstance(back, ELC) and back is not elc
+    for key in ("gap_size", "maxPWerror", "far_cut", "neutralize", "delta_mid_top"):
+        assert back.get_params()[key] == elc.get_params()[key]
+    assert type(back.actor) is type(p3m) and back.actor.prefactor == p3m.prefactor
