@@ -167,6 +167,38 @@ __device__ __forceinline__ void elc_block_sum(double (&v)[W], double *red, doubl
   __syncthreads();
 }
 
+// Warp sum of 8 values with 9 shuffles: three halving exchanges (lanes
+// l and l ^ 16 / 8 / 4 each keep one half of the values and add the half the
+// partner sends), then two butterfly steps over l ^ 2, l ^ 1.  Lane l with
+// (l & 3) == 0 ends with the warp total of value ((l >> 2) & 7) (bit 4 of l
+// selects values 4-7, bit 3 values +2, bit 2 value +1); fixed order.
+__device__ __forceinline__ double elc_warp_sum8(double const (&v)[8]) {
+  int const lane = threadIdx.x & 31;
+  bool const b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  double w[4], x[2];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double const send = b4 ? v[j] : v[j + 4];
+    double const keep = b4 ? v[j + 4] : v[j];
+    w[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    double const send = b3 ? w[j] : w[j + 2];
+    double const keep = b3 ? w[j + 2] : w[j];
+    x[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  double y;
+  {
+    double const send = b2 ? x[0] : x[1];
+    double const keep = b2 ? x[1] : x[0];
+    y = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  y += __shfl_xor_sync(0xffffffffu, y, 2);
+  y += __shfl_xor_sync(0xffffffffu, y, 1);
+  return y;
+}
+
 // Per particle tile (blockIdx.x) and mode chunk (blockIdx.y): the product sums
 // of each mode; chunk 0 also takes the dipole sums and the gap check
 // (check_gap :184-194: a charged particle below 0 or above L_z - gap).
@@ -174,7 +206,10 @@ __global__ void __launch_bounds__(kElcThreads)
 k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ pos,
            const double *__restrict__ qv, double *__restrict__ part, int *__restrict__ gap_err) {
   __shared__ double red[(kElcThreads / 32) * 8];
+  // per mode of the chunk, per warp, the 8 warp sums (one barrier per chunk)
+  __shared__ double wsum[kElcModesPerBlock][kElcThreads / 32][8];
   long long const tile0 = static_cast<long long>(blockIdx.x) * kElcThreads * kElcPPT;
+  int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   ElcPart P[kElcPPT];
 #pragma unroll
   for (int k = 0; k < kElcPPT; ++k) {
@@ -195,8 +230,18 @@ k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restric
       for (int c = 0; c < w; ++c)
         acc[c] += v[c];
     }
-    elc_block_sum<8>(acc, red, part + static_cast<long long>(m) * 8 * gridDim.x + blockIdx.x,
-                     gridDim.x);
+    double const ws = elc_warp_sum8(acc);
+    if ((lane & 3) == 0)
+      wsum[m - m0][wid][lane >> 2] = ws;
+  }
+  __syncthreads();
+  for (int o = threadIdx.x; o < (m1 - m0) * 8; o += kElcThreads) {
+    int const mm = o >> 3, c = o & 7;
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < kElcThreads / 32; ++w)
+      t += wsum[mm][w][c];
+    part[static_cast<long long>((m0 + mm) * 8 + c) * gridDim.x + blockIdx.x] = t;
   }
   if (blockIdx.y == 0) {
     double d[3] = {0, 0, 0};
