@@ -81,8 +81,9 @@ def test_elc_ionic_sheet_madelung(cls):
     np.testing.assert_allclose(e_ion, k["madelung"], rtol=k["energy_rtol"], atol=0)
 
 
-@pytest.mark.parametrize("neutral,neutralize", [(True, True), (False, True), (False, False)])
-def test_elc_part_vs_oracle(neutral, neutralize):
+@pytest.mark.parametrize("cls,neutral,neutralize", [(P3M, True, True), (P3M, False, True),
+                                                     (P3M, False, False), (P3MGPU, True, True)])
+def test_elc_part_vs_oracle(cls, neutral, neutralize):
     rng = np.random.default_rng(7)
     box = np.array([9.0, 11.0, 14.0])
     gap = 3.5
@@ -92,7 +93,7 @@ def test_elc_part_vs_oracle(neutral, neutralize):
     if not neutral:
         q[:3] = 2.0
     s = _system(box, pos, q)
-    p3m = P3M(prefactor=1.7, accuracy=1e-4, mesh=32, cao=5, r_cut=2.5, alpha=1.3, tune=False,
+    p3m = cls(prefactor=1.7, accuracy=1e-4, mesh=32, cao=5, r_cut=2.5, alpha=1.3, tune=False,
               check_neutrality=False)
     s.electrostatics.solver = p3m
     s.integrator.run(0)
@@ -138,3 +139,50 @@ def test_elc_gap_error():
     # back in the slab: usable again
     p1.pos = [1.0, 1.0, 1.0]
     s.integrator.run(0)
+
+
+def test_elc_through_the_c_abi_long_range():
+    """p3mx_long_range with ELC attached: forces and energy are the bare
+    P3M ones plus the oracle's ELC part, the k-space virial is zero (the
+    reference computes no ELC pressure), and p3mx_set_elc(NULL) detaches."""
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    box = np.array([10.0, 10.0, 15.0])
+    gap = 4.0
+    n = 300
+    pos = rng.uniform([0, 0, 0.1], [box[0], box[1], box[2] - gap - 0.1], (n, 3))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    p3m = P3M(prefactor=1.3, accuracy=1e-4, mesh=32, cao=5, r_cut=2.5, alpha=1.3, tune=False)
+    p3m._set_system(box, 0.3, (True, True, True))
+    p3m._activate(pos, q)
+    h = p3m._handle
+    flags = _lib.P3MX_FORCES | _lib.P3MX_ENERGY | _lib.P3MX_VIRIAL | _lib.P3MX_OVERWRITE
+
+    def long_range():
+        f = np.zeros((n, 3))
+        e = np.zeros(1)
+        v = np.zeros(9)
+        _lib.check(lib.p3mx_long_range(h, n, _lib.dptr(pos), _lib.dptr(q), _lib.dptr(f),
+                                       e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       flags, None), h)
+        return f, e[0], v
+
+    f0, e0, v0 = long_range()
+    assert np.abs(v0).max() > 0.0
+    c = _lib.ElcParams(maxPWerror=1e-6, gap_size=gap, far_cut=-1.0, neutralize=1)
+    _lib.check(lib.p3mx_set_elc(h, ctypes.byref(c)), h)
+    f1, e1, v1 = long_range()
+    fc = ctypes.c_double()
+    bh = ctypes.c_double()
+    _lib.check(lib.p3mx_get_elc(h, ctypes.byref(fc), ctypes.byref(bh), None), h)
+    assert bh.value == box[2] - gap
+    fo, eo = O.elc(box, gap, pos, q, 1.3, fc.value)
+    np.testing.assert_allclose(f1 - f0, fo, atol=1e-9 * np.abs(fo).max(), rtol=0)
+    assert abs((e1 - e0) - eo) <= 1e-9 * max(abs(eo), 1.0)
+    assert np.all(v1 == 0.0)
+    _lib.check(lib.p3mx_set_elc(h, None), h)
+    f2, e2, v2 = long_range()
+    np.testing.assert_array_equal(f2, f0)
+    assert e2 == e0
+    assert lib.p3mx_get_elc(h, None, None, None) != 0
