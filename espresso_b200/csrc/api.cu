@@ -956,6 +956,10 @@ static void stage_out(p3mx_handle *h, size_t n, double *f, bool dev, bool overwr
 // P3M forces; long_range_energy :1189-1229 adds calc_energy).
 static void elc_add(p3mx_handle *h, double *fd, double *energy, cudaStream_t st) {
   Engine &e = *h->eng;
+  // sanity_checks_periodicity (elc.cpp:983-988), also after a later
+  // p3mx_set_system
+  if (!(h->sys.periodic[0] && h->sys.periodic[1] && h->sys.periodic[2]))
+    throw Error(P3MX_ERUNTIME, "ELC: requires periodicity (True, True, True)");
   elc_apply(*h->elc, h->sys.box, h->prm.prefactor, static_cast<long long>(h->n), e.d_pos(),
             e.d_q(), fd, energy, nullptr, st);
 }
