@@ -296,33 +296,58 @@ k_elc_forces(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restr
     elc_part_init(P, g, pos + 3 * i, qv[i]);
     double const q = P.q, z = P.z;
     double fx = 0.0, fy = 0.0, fz = 0.0;
+    // the mode terms factored as q (1/e A +- e B), A and B the phase
+    // products dotted with the mode's sums (the reference's 8-product sums
+    // regrouped; q is multiplied in once at the end)
+    double ax = 0.0, ay = 0.0, az = 0.0;
     for (int m = 0; m < g.nmodes; ++m) {
       ElcMode const md = modes[m];
-      double v[8];
-      elc_products(md, g, P, v);
+      double const e = exp(md.omega * z);
+      double const ie = 1.0 / e;
       const double *Gm = G + static_cast<long long>(m) * 8;
       if (md.kind < 2) {
-        double const ft = v[2] * Gm[1] - v[3] * Gm[0] + v[0] * Gm[3] - v[1] * Gm[2];
+        double sn, cs;
+        if (md.kind == 0) {
+          elc_phase(P.px, md.p, P.s1x, P.c1x, 2.0 * kPi * (1.0 / g.box[0]), P.x);
+          sn = P.px.s;
+          cs = P.px.c;
+        } else {
+          elc_phase(P.py, md.q, P.s1y, P.c1y, 2.0 * kPi * (1.0 / g.box[1]), P.y);
+          sn = P.py.s;
+          cs = P.py.c;
+        }
+        // G: POQESP, POQECP, POQESM, POQECM
+        double const ft = ie * (sn * Gm[1] - cs * Gm[0]) + e * (sn * Gm[3] - cs * Gm[2]);
         if (md.kind == 0)
-          fx += ft;
+          ax += ft;
         else
-          fy += ft;
-        fz += v[3] * Gm[1] + v[2] * Gm[0] - v[1] * Gm[3] - v[0] * Gm[2];
+          ay += ft;
+        double const a1 = cs * Gm[1] + sn * Gm[0], b1 = cs * Gm[3] + sn * Gm[2];
+        az += ie * a1 - e * b1;
         if constexpr (EV)
-          en[0] += (v[3] * Gm[1] + v[2] * Gm[0] + v[1] * Gm[3] + v[0] * Gm[2]) / md.omega;
+          en[0] += q * (ie * a1 + e * b1) / md.omega;
       } else {
-        fx += md.px * (v[5] * Gm[3] + v[4] * Gm[2] - v[7] * Gm[1] - v[6] * Gm[0] +
-                       v[1] * Gm[7] + v[0] * Gm[6] - v[3] * Gm[5] - v[2] * Gm[4]);
-        fy += md.py * (v[6] * Gm[3] + v[4] * Gm[1] - v[7] * Gm[2] - v[5] * Gm[0] +
-                       v[2] * Gm[7] + v[0] * Gm[5] - v[3] * Gm[6] - v[1] * Gm[4]);
-        fz += v[7] * Gm[3] + v[6] * Gm[2] + v[5] * Gm[1] + v[4] * Gm[0] - v[3] * Gm[7] -
-              v[2] * Gm[6] - v[1] * Gm[5] - v[0] * Gm[4];
+        elc_phase(P.px, md.p, P.s1x, P.c1x, 2.0 * kPi * (1.0 / g.box[0]), P.x);
+        elc_phase(P.py, md.q, P.s1y, P.c1y, 2.0 * kPi * (1.0 / g.box[1]), P.y);
+        double const ss = P.px.s * P.py.s, sc = P.px.s * P.py.c;
+        double const cs = P.px.c * P.py.s, cc = P.px.c * P.py.c;
+        // G: PQESSP, PQESCP, PQECSP, PQECCP, PQESSM, PQESCM, PQECSM, PQECCM
+        double const A = cc * Gm[3] + cs * Gm[2] + sc * Gm[1] + ss * Gm[0];
+        double const B = cc * Gm[7] + cs * Gm[6] + sc * Gm[5] + ss * Gm[4];
+        double const Cx = sc * Gm[3] + ss * Gm[2] - cc * Gm[1] - cs * Gm[0];
+        double const Dx = sc * Gm[7] + ss * Gm[6] - cc * Gm[5] - cs * Gm[4];
+        double const Cy = cs * Gm[3] + ss * Gm[1] - cc * Gm[2] - sc * Gm[0];
+        double const Dy = cs * Gm[7] + ss * Gm[5] - cc * Gm[6] - sc * Gm[4];
+        ax += md.px * (ie * Cx + e * Dx);
+        ay += md.py * (ie * Cy + e * Dy);
+        az += ie * A - e * B;
         if constexpr (EV)
-          en[0] += (v[7] * Gm[3] + v[6] * Gm[2] + v[5] * Gm[1] + v[4] * Gm[0] + v[3] * Gm[7] +
-                    v[2] * Gm[6] + v[1] * Gm[5] + v[0] * Gm[4]) /
-                   md.omega;
+          en[0] += q * (ie * A + e * B) / md.omega;
       }
     }
+    fx = q * ax;
+    fy = q * ay;
+    fz = q * az;
     // dipole force (add_dipole_force :201-264 without contrasts / const_pot)
     const double *D = G + static_cast<long long>(g.nmodes) * 8;
     fz -= g.pref_dip * D[0] * q;
