@@ -285,14 +285,15 @@ def bonds(box, pos, bond_types, bond_list):
     return f, energy, vir
 
 
-def elc_far_cut(box, box_h, max_pw_error):
+def elc_far_cut(box, box_h, max_pw_error, lz=None):
     """ELC far-formula cutoff from the maximal pairwise error, restating
-    ElectrostaticLayerCorrection::tune_far_cut (electrostatics/elc.cpp:942-973)
-    without dielectric contrasts (lz = box_l[2]).  Raises RuntimeError when no
-    cutoff below 50 meets the bound, as the reference does."""
+    ElectrostaticLayerCorrection::tune_far_cut (electrostatics/elc.cpp:942-973):
+    lz = L_z, or box_h + space_layer with dielectric contrasts.  Raises
+    RuntimeError when no cutoff below 50 meets the bound, as the reference
+    does."""
     ux, uy = 1.0 / box[0], 1.0 / box[1]
     umin = min(ux, uy)
-    lz = box[2]
+    lz = box[2] if lz is None else lz
     fc = umin
     while True:
         pref = 2.0 * np.pi * fc
@@ -336,16 +337,21 @@ def elc_modes(box, far_cut):
     return modes
 
 
-def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True):
-    """ELC correction forces and energy without dielectric contrasts, in FP64
-    numpy, restating electrostatics/elc.cpp: the dipole force and energy
-    (add_dipole_force :201-264, dipole_energy :267-343), the per-frequency
-    product decomposition (setup_PoQ :501-598, add_PoQ_force :601-618,
-    PoQ_energy :620-634, setup_PQ :641-769, add_PQ_force :771-810,
-    PQ_energy :812-828) and their sums (add_force :830-883, calc_energy
-    :885-940, which halves the total).  Positions are folded into the box
-    first, as the reference's particle positions are.  Returns (forces
-    (N, 3), energy); raises RuntimeError for a charged particle in the gap.
+def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True, delta_top=0.0,
+        delta_bot=0.0, const_pot=False, pot_diff=0.0, space_layer=0.0):
+    """ELC correction forces and energy in FP64 numpy, restating
+    electrostatics/elc.cpp: the dipole force and energy (add_dipole_force
+    :201-264, dipole_energy :267-343), the z terms of dielectric contrasts
+    (z_energy :366-439, add_z_force :441-494), the per-frequency product
+    decomposition with its image-layer terms (setup_PoQ :501-598,
+    add_PoQ_force :601-618, PoQ_energy :620-634, setup_PQ :641-769,
+    add_PQ_force :771-810, PQ_energy :812-828) and their sums (add_force
+    :830-883, calc_energy :885-940, which halves the total).  The flags are
+    the effective ones of elc_data (:1056-1102): contrasts switch
+    neutralization off and const_pot needs a contrast.  Positions are folded
+    into the box first, as the reference's particle positions are.  Returns
+    (forces (N, 3), energy); raises RuntimeError for a charged particle in
+    the gap.
     """
     box = np.asarray(box, dtype=np.float64)
     pos = np.asarray(pos, dtype=np.float64)
@@ -353,42 +359,122 @@ def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True):
     pos = pos - np.floor(pos / box) * box
     x, y, z = pos[:, 0], pos[:, 1], pos[:, 2]
     lz = box[2]
-    box_h = lz - gap_size
-    bad = (q != 0.0) & ((z < 0.0) | (z > box_h))
+    h = lz - gap_size
+    contrast = (delta_top != 0.0) or (delta_bot != 0.0)
+    const_pot = bool(const_pot) and contrast
+    neutralize = bool(neutralize) and not contrast
+    pot_diff = pot_diff if const_pot else 0.0
+    sl = space_layer if contrast else 0.0
+    bad = (q != 0.0) & ((z < 0.0) | (z > h))
     if bad.any():
         i = int(np.flatnonzero(bad)[0])
-        dz = z[i] if z[i] < 0.0 else z[i] - box_h
+        dz = z[i] if z[i] < 0.0 else z[i] - h
         raise RuntimeError("Particle %d entered ELC gap region by %r" % (i, dz))
+    mb = contrast & (z < sl)
+    mt = contrast & (z > h - sl)
+    db, dt = delta_bot, delta_top
     f = np.zeros_like(pos)
     vol = box[0] * box[1] * box[2]
     shift = 0.5 * lz
-    # dipole force (elc.cpp:201-264), no dielectric contrast / const_pot
+    # dipole force (elc.cpp:201-264)
     pref = prefactor * 4.0 * np.pi / vol
-    g0 = pref * np.sum(q * (z - shift))
-    g2 = pref * np.sum(q)
-    f[:, 2] -= g0 * q
+    g0 = np.sum(q * (z - shift)) + np.sum((db * q * (-z - shift))[mb]) + \
+        np.sum((dt * q * (2.0 * h - z - shift))[mt])
+    g1 = np.sum(q * z)
+    g2 = np.sum(q) + np.sum((db * q)[mb]) + np.sum((dt * q)[mt])
+    g0 *= pref
+    g1 *= pref / h * lz
+    g2 *= pref
+    field = g0
+    if const_pot:
+        field -= pot_diff / h + g1
+    f[:, 2] -= field * q
     if not neutralize:
         f[:, 2] += g2 * q * (z - shift)
     # dipole energy (elc.cpp:267-343)
     pref = prefactor * 2.0 * np.pi / vol
     s0 = np.sum(q)
+    s1 = np.sum((db * q)[mb]) + np.sum((dt * q)[mt])
     s2 = np.sum(q * (z - shift))
+    s3 = np.sum((db * q * (-z - shift))[mb]) + np.sum((dt * q * (2.0 * h - z - shift))[mt])
     s4 = np.sum(q * (z - shift) ** 2)
-    energy = 2.0 * pref * s2 * s2
+    s5 = np.sum((db * q * (-z - shift) ** 2)[mb]) + \
+        np.sum((dt * q * (2.0 * h - z - shift) ** 2)[mt])
+    s6 = np.sum(q * z)
+    energy = 2.0 * pref * (s2 * s2 + s2 * s3)
     if not neutralize:
         energy += 2.0 * pref * (-s0 * s4 - (0.25 - 0.5 / 3.0) * (s0 * lz) ** 2)
+    if contrast:
+        if const_pot:
+            energy += pref / h * lz * s6 * s6
+            energy -= 2.0 * pot_diff / h * s6
+        energy += pref * (-(s1 * s4 + s0 * s5) - (1.0 - 2.0 / 3.0) * s0 * s1 * lz * lz)
     area_inv = 1.0 / (box[0] * box[1])
+    if contrast:
+        # z force and z energy (elc.cpp:366-494)
+        pref = prefactor * 2.0 * np.pi * area_inv
+        delta = dt * db
+        if const_pot:
+            gz = np.sum((-db * q)[mb]) + np.sum((dt * q)[mt])
+            z2 = gz
+            z3 = np.sum((-db * q * (-z - shift))[mb]) + \
+                np.sum((dt * q * (2.0 * h - z - shift))[mt])
+        else:
+            # delta = 1 (two metallic walls) needs const_pot (elc.cpp:1095-1101)
+            fdb, fdt, fd = db / (1.0 - delta), dt / (1.0 - delta), delta / (1.0 - delta)
+            gz = np.sum(np.where(mb, fd * (db + 1.0) * q, fdb * (dt + 1.0) * q)) - \
+                np.sum(np.where(mt, fd * (dt + 1.0) * q, fdt * (db + 1.0) * q))
+            dci = 1.0 / (1.0 - delta)
+
+            def img_b(a, zz):
+                return a * dci * (zz - 2.0 * delta * lz * dci) - a * dci * shift
+
+            def img_t(a, zz):
+                return a * dci * (zz + 2.0 * delta * lz * dci) - a * dci * shift
+            z2 = gz
+            z3 = np.sum(q * np.where(mb, img_b(db * delta, -(2.0 * h + z)) +
+                                     img_b(delta, -(2.0 * h - z)),
+                                     img_b(db, -z) + img_b(delta, -(2.0 * h - z))))
+            z3 -= np.sum(q * np.where(mt, img_t(dt * delta, 4.0 * h - z) +
+                                      img_t(delta, 2.0 * h + z),
+                                      img_t(dt, 2.0 * h - z) + img_t(delta, 2.0 * h + z)))
+        f[:, 2] += pref * gz * q
+        z0 = np.sum(q)
+        z1 = np.sum(q * (z - shift))
+        energy += -pref * (z1 * z2 - z0 * z3)
     ux, uy = 1.0 / box[0], 1.0 / box[1]
     for kind, p, qq, omega in elc_modes(box, far_cut):
         e = np.exp(omega * z)
+        if contrast:
+            delta = dt * db
+            fac_elc = 1.0 / (1.0 - delta * np.exp(-omega * 2.0 * h))
+            fdb, fdt = db * fac_elc, dt * fac_elc
+            fd = fdb * dt
+            eb = np.exp(-omega * z)
+            et = np.exp(omega * (2.0 * h - z))
+            e2 = np.where(mb, (np.exp(omega * (-z - 2.0 * h)) * db + np.exp(omega * (z - 2.0 * h))) * fd,
+                          (np.exp(-omega * z) + np.exp(omega * (z - 2.0 * h)) * dt) * fdb)
+            e3 = np.where(mt, (np.exp(omega * (z - 4.0 * h)) * dt + np.exp(omega * (-z - 2.0 * h))) * fd,
+                          (np.exp(omega * (z - 2.0 * h)) + np.exp(omega * (-z - 2.0 * h)) * db) * fdt)
+            wb = np.where(mb, q * db, 0.0)
+            wt = np.where(mt, q * dt, 0.0)
         if kind < 2:
             c = x if kind == 0 else y
             u = ux if kind == 0 else uy
             arg = (2.0 * np.pi * u * (p if kind == 0 else qq)) * c
-            s, co = np.sin(arg), np.cos(arg)
-            pb = np.stack([q * s * e, q * co * e, q * s / e, q * co / e])  # SP CP SM CM
-            pref = -(prefactor * 4.0 * np.pi * area_inv) / np.expm1(omega * lz)
-            G = pref * pb.sum(axis=1)
+            sn, co = np.sin(arg), np.cos(arg)
+            pb = np.stack([q * sn * e, q * co * e, q * sn / e, q * co / e])  # SP CP SM CM
+            pref_di = prefactor * 4.0 * np.pi * area_inv
+            pref = -pref_di / np.expm1(omega * lz)
+            gbl = pb.sum(axis=1)
+            if contrast:
+                gbl = gbl + np.stack([sn * eb, co * eb, sn / eb, co / eb]) @ wb + \
+                    np.stack([sn * et, co * et, sn / et, co / et]) @ wt
+                lcl = np.array([np.sum(q * sn * e2), np.sum(q * co * e2),
+                                np.sum(q * sn * e3), np.sum(q * co * e3)])
+                G = pref * gbl + pref_di * lcl
+            else:
+                G = pref * gbl
             SP, CP, SM, CM = pb
             f[:, kind] += SM * G[1] - CM * G[0] + SP * G[3] - CP * G[2]
             f[:, 2] += CM * G[1] + SM * G[0] - CP * G[3] - SP * G[2]
@@ -397,10 +483,18 @@ def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True):
             ax = (2.0 * np.pi * ux * p) * x
             ay = (2.0 * np.pi * uy * qq) * y
             sx, cx, sy, cy = np.sin(ax), np.cos(ax), np.sin(ay), np.cos(ay)
-            pb = np.stack([sx * sy * q * e, sx * cy * q * e, cx * sy * q * e, cx * cy * q * e,
-                           sx * sy * q / e, sx * cy * q / e, cx * sy * q / e, cx * cy * q / e])
-            pref = -(prefactor * 8.0 * np.pi * area_inv) / np.expm1(omega * lz)
-            G = pref * pb.sum(axis=1)
+            pp = np.stack([sx * sy, sx * cy, cx * sy, cx * cy])  # SS SC CS CC
+            pb = np.concatenate([pp * q * e, pp * q / e])
+            pref_di = prefactor * 8.0 * np.pi * area_inv
+            pref = -pref_di / np.expm1(omega * lz)
+            gbl = pb.sum(axis=1)
+            if contrast:
+                gbl = gbl + np.concatenate([pp * eb, pp / eb]) @ wb + \
+                    np.concatenate([pp * et, pp / et]) @ wt
+                lcl = np.concatenate([pp @ (q * e2), pp @ (q * e3)])
+                G = pref * gbl + pref_di * lcl
+            else:
+                G = pref * gbl
             SSP, SCP, CSP, CCP, SSM, SCM, CSM, CCM = pb
             px = 2.0 * np.pi * ux * p / omega
             py = 2.0 * np.pi * uy * qq / omega
@@ -413,3 +507,110 @@ def elc(box, gap_size, pos, q, prefactor, far_cut, neutralize=True):
             energy += np.sum(CCM * G[3] + CSM * G[2] + SCM * G[1] + SSM * G[0] +
                              CCP * G[7] + CSP * G[6] + SCP * G[5] + SSP * G[4]) / omega
     return f, 0.5 * energy
+
+
+def _p3m_pair(prefactor, alpha, r_cut, q1q2, d):
+    """CoulombP3M::pair_force / pair_energy (electrostatics/p3m.hpp:146-180)
+    with the Abramowitz-Stegun erfc part, vectorised over rows of d."""
+    d = np.atleast_2d(d)
+    q1q2 = np.broadcast_to(np.asarray(q1q2, dtype=np.float64), (len(d),))
+    r = np.sqrt(np.sum(d * d, axis=1))
+    ok = (q1q2 != 0.0) & (r < r_cut) & (r > 0.0)
+    rs = np.where(ok, r, 1.0)
+    ad = alpha * rs
+    t = 1.0 / (1.0 + 0.3275911 * ad)
+    asp = t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 +
+                                                                          t * 1.061405429))))
+    ex = np.exp(-ad * ad)
+    erfc_ri = asp / rs
+    fac = ex * (erfc_ri + 2.0 * alpha / np.sqrt(np.pi)) / (rs * rs)
+    force = np.where(ok[:, None], (fac * prefactor * q1q2)[:, None] * d, 0.0)
+    energy = np.where(ok, prefactor * q1q2 * erfc_ri * ex, 0.0)
+    return force, energy
+
+
+def elc_space_layer(gap_size, box_h, r_cut):
+    """recalc_space_layer (elc.cpp:1032-1054): a third of the gap, at most
+    gap - r_cut and half the slab; RuntimeError when nothing is left."""
+    sl = gap_size / 3.0
+    mx = min(gap_size - r_cut, box_h / 2.0)
+    if sl > mx:
+        if mx <= 0.0:
+            raise RuntimeError("P3M real-space cutoff too large for ELC w/ dielectric contrast")
+        sl = mx
+    return sl
+
+
+def elc_system(box, gap_size, pos, q, prefactor, alpha, r_cut, mesh, cao, max_pw_error,
+               far_cut=-1.0, neutralize=True, delta_top=0.0, delta_bot=0.0,
+               const_pot=False, pot_diff=0.0):
+    """Coulomb forces and energy of P3M + ELC for the whole system (k-space,
+    real space and the correction), restating the reference's combination:
+    without contrasts P3M forces and energy plus `elc`; with contrasts
+    (ElectrostaticLayerCorrection::add_long_range_forces :1231-1254,
+    long_range_energy :1189-1229) the mesh carries the image charges of the
+    particles within space_layer of either wall (charge_assign :1111-1142,
+    modify_p3m_sums :1144-1187: the P3M sums of that charge set), the
+    energy is 0.5 E(real) + 0.5 E(self images) + 0.5 E(real + images)
+    - 0.5 E(images), every particle feels its own image
+    (dielectric_layers_self_forces, elc.hpp) and every pair the image of
+    each partner within space_layer (add_pair_force_corrections /
+    pair_energy_correction, elc.hpp: particle 1 gets pair_force(q_eff,
+    mi(x2 - image(x1))) and the energy is half the sum over both orders).
+    P3M runs metallic (adapt_epsilon_elc).  Returns (forces, energy)."""
+    box = np.asarray(box, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    n = len(q)
+    h = box[2] - gap_size
+    contrast = (delta_top != 0.0) or (delta_bot != 0.0)
+    sl = elc_space_layer(gap_size, h, r_cut) if contrast else 0.0
+    lz_tune = h + sl if contrast else box[2]
+    fc = elc_far_cut(box, h, max_pw_error, lz=lz_tune) if far_cut == -1.0 else far_cut
+    prm = make_params(box, mesh, cao, alpha, r_cut, prefactor)
+    fr, er, _, _ = short_range(prm, pos, q)
+    fe, ee = elc(box, gap_size, pos, q, prefactor, fc, neutralize=neutralize,
+                 delta_top=delta_top, delta_bot=delta_bot, const_pot=const_pot,
+                 pot_diff=pot_diff, space_layer=sl)
+    if not contrast:
+        fk, ek, _ = p3m_kspace(prm, pos, q)
+        return fk + fr + fe, ek + er[0] + ee
+    pf = pos - np.floor(pos / box) * box
+    z = pf[:, 2]
+    mb = (q != 0.0) & (z < sl)
+    mt = (q != 0.0) & (z > h - sl)
+    img_b = pf.copy()
+    img_b[:, 2] = -z
+    img_t = pf.copy()
+    img_t[:, 2] = 2.0 * h - z
+    ipos = np.concatenate([img_b[mb], img_t[mt]])
+    iq = np.concatenate([delta_bot * q[mb], delta_top * q[mt]])
+    both_pos = np.concatenate([pf, ipos])
+    both_q = np.concatenate([q, iq])
+    fk_both, e_both, _ = p3m_kspace(prm, both_pos, both_q)
+    _, e_real, _ = p3m_kspace(prm, pf, q)
+    _, e_img, _ = p3m_kspace(prm, ipos, iq) if len(iq) else (None, 0.0, None)
+    f = fk_both[:n] + fr + fe
+    energy = er[0] + ee + 0.5 * e_real + 0.5 * e_both - 0.5 * e_img
+
+    def mi(d):
+        return d - np.rint(d / box) * box
+    # self images (dielectric_layers_self_forces / _self_energy)
+    e_self = 0.0
+    for m, img, dl in ((mb, img_b, delta_bot), (mt, img_t, delta_top)):
+        idx = np.flatnonzero(m)
+        if len(idx):
+            fs, es = _p3m_pair(prefactor, alpha, r_cut, dl * q[idx] ** 2, mi(pf[idx] - img[idx]))
+            f[idx] += fs
+            e_self += es.sum()
+    energy += 0.5 * e_self
+    # image pairs: particle i in a layer, every partner j != i
+    e_pair = 0.0
+    for m, img, dl in ((mb, img_b, delta_bot), (mt, img_t, delta_top)):
+        for i in np.flatnonzero(m):
+            j = np.flatnonzero(np.arange(n) != i)
+            fs, es = _p3m_pair(prefactor, alpha, r_cut, dl * q[i] * q[j], mi(pf[j] - img[i]))
+            f[i] += fs.sum(axis=0)
+            e_pair += es.sum()
+    energy += 0.5 * e_pair
+    return f, energy
