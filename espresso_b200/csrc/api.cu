@@ -234,6 +234,8 @@ void configure_engine(p3mx_handle *h) {
   h->eng->set_pair_table(h->ntypes, h->table);
   h->eng->configure({c}, static_cast<long long>(h->n));
   h->eng64.reset();
+  if (h->elc)
+    h->elc->img.reset();
 }
 
 Engine &observables_engine(p3mx_handle *h) {
@@ -960,8 +962,87 @@ static void elc_add(p3mx_handle *h, double *fd, double *energy, cudaStream_t st)
   // p3mx_set_system
   if (!(h->sys.periodic[0] && h->sys.periodic[1] && h->sys.periodic[2]))
     throw Error(P3MX_ERUNTIME, "ELC: requires periodicity (True, True, True)");
-  elc_apply(*h->elc, h->sys.box, h->prm.prefactor, static_cast<long long>(h->n), e.d_pos(),
-            e.d_q(), fd, energy, nullptr, st);
+  elc_apply(*h->elc, h->sys.box, h->prm.prefactor, h->r_cut, static_cast<long long>(h->n),
+            e.d_pos(), e.d_q(), fd, energy, nullptr, st);
+}
+
+// ELC with dielectric contrasts, the whole Coulomb + non-bonded force
+// evaluation (add_long_range_forces :1231-1254, long_range_energy
+// :1189-1229, the short-range corrections of elc.hpp): short range and
+// bonds on the engine, the image-layer pair and self terms over its Verlet
+// lists, the mesh part from an FP64 engine over 3N slots holding the
+// particles and their images (forces of the first N slots; the energy
+// 0.5 E(real) + 0.5 E(both) - 0.5 E(images) from three runs whose censuses
+// give the P3M sums of each charge set, as modify_p3m_sums does), then the
+// ELC mode, dipole and z terms.  fd is overwritten.  energy3 / virial27 as
+// p3mx_forces (k-space virial zero).
+static void elc_contrast_forces(p3mx_handle *h, double *fd, double *energy3, double *virial27,
+                                cudaStream_t st) {
+  Engine &e = *h->eng;
+  ElcState &s = *h->elc;
+  elc_prepare(s, h->sys.box, h->prm.prefactor, h->r_cut, st);
+  if (!(h->sys.periodic[0] && h->sys.periodic[1] && h->sys.periodic[2]))
+    throw Error(P3MX_ERUNTIME, "ELC: requires periodicity (True, True, True)");
+  bool const want = energy3 || virial27;
+  e.short_range(fd, true, false, st, nullptr, nullptr);
+  e.bond_forces(fd, st);
+  std::vector<double> ens, virs;
+  if (want)
+    e.short_range(observables_engine(h).d_force(), true, true, st, &ens, &virs, true);
+  double e_img_pairs = 0.0;
+  e.elc_image_pairs(s.space_layer, s.box_h, s.prm.delta_mid_bot, s.prm.delta_mid_top, fd,
+                    energy3 ? &e_img_pairs : nullptr, st);
+  long long const n = static_cast<long long>(h->n);
+  long long const n3 = 3 * n;
+  if (!s.img) {
+    s.img = std::make_unique<Engine>(false);
+    ReplicaConf c = e.conf(0);
+    c.np = n3;
+    s.img->set_pair_table(h->ntypes, h->table);
+    s.img->configure({c}, n3);
+  }
+  Engine &im = *s.img;
+  s.d_aug_pos.ensure(static_cast<size_t>(3 * n3) * sizeof(double));
+  s.d_aug_q.ensure(static_cast<size_t>(n3) * sizeof(double));
+  s.d_faug.ensure(static_cast<size_t>(3 * n3) * sizeof(double));
+  ElcGeom const g = elc_geom(s, h->sys.box, h->prm.prefactor, n);
+  auto run = [&](int which, double *faug, double *energy) {
+    if (n == 0)
+      return;
+    k_elc_augment<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
+        e.d_pos(), e.d_q(), n, g, which, s.d_aug_pos.as<double>(), s.d_aug_q.as<double>());
+    P3MX_CUDA(cudaGetLastError());
+    im.upload(s.d_aug_pos.as<double>(), s.d_aug_q.as<double>(), nullptr, true, st);
+    im.census(st);
+    std::vector<double> en, vir;
+    im.long_range(faug, true, energy != nullptr, false, st, &en, &vir);
+    if (energy)
+      *energy = en.empty() ? 0.0 : en[0];
+  };
+  double e_both = 0.0, e_real = 0.0, e_imgs = 0.0;
+  run(3, s.d_faug.as<double>(), energy3 ? &e_both : nullptr);
+  if (n > 0) {
+    k_elc_add<<<static_cast<unsigned>((3 * n + 255) / 256), 256, 0, st>>>(
+        fd, s.d_faug.as<double>(), 3 * n);
+    P3MX_CUDA(cudaGetLastError());
+  }
+  if (energy3) {
+    run(1, nullptr, &e_real);
+    run(2, nullptr, &e_imgs);
+  }
+  double e_elc = 0.0;
+  elc_add(h, fd, energy3 ? &e_elc : nullptr, st);
+  if (energy3) {
+    energy3[0] = ens[0] + e_img_pairs;
+    energy3[1] = 0.5 * e_real + 0.5 * e_both - 0.5 * e_imgs + e_elc;
+    energy3[2] = ens[1];
+  }
+  if (virial27)
+    for (int k = 0; k < 9; ++k) {
+      virial27[k] = virs[k];
+      virial27[9 + k] = 0.0;
+      virial27[18 + k] = virs[9 + k];
+    }
 }
 
 int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p) {
@@ -980,7 +1061,7 @@ int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p) {
     h->prm.epsilon = 0.0;
     if (h->sys_set) {
       Engine *e = h->eng.get();
-      elc_prepare(*s, h->sys.box, h->prm.prefactor, e ? e->stream() : nullptr);
+      elc_prepare(*s, h->sys.box, h->prm.prefactor, h->r_cut, e ? e->stream() : nullptr);
     }
     h->elc = std::move(s);
   });
@@ -1004,6 +1085,9 @@ int p3mx_long_range(p3mx_handle *h, size_t n, const double *pos, const double *q
                     double *energy, double *virial9, unsigned flags, void *stream) {
   return guarded(h, [&] {
     ensure_ready(h, n);
+    if (h->elc && h->elc->contrast())
+      throw Error(P3MX_ERUNTIME, "ELC with dielectric contrasts: the image terms span the "
+                                 "short and long range; use p3mx_forces");
     Engine &e = *h->eng;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e.stream();
     bool const dev = flags & P3MX_DEVICE_PTRS;
@@ -1085,6 +1169,19 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     bool const want_e = energy3 && (flags & P3MX_ENERGY);
     bool const want_v = virial27 && (flags & P3MX_VIRIAL);
     double *fd = (dev && f) ? f : e.d_force();
+    if (h->elc && h->elc->contrast()) {
+      stage_in(h, n, pos, q, type, dev, st);
+      bool const add_dev = dev && f && !ow;
+      double *fo = add_dev ? e.d_force() : fd;
+      elc_contrast_forces(h, fo, want_e ? energy3 : nullptr, want_v ? virial27 : nullptr, st);
+      if (add_dev && n > 0)
+        k_elc_add<<<static_cast<unsigned>((3 * n + 255) / 256), 256, 0, st>>>(f, fo, 3 * n);
+      if (f)
+        stage_out(h, n, f, dev, ow, st);
+      P3MX_CUDA(cudaStreamSynchronize(st));
+      check_kernels(h, st);
+      return;
+    }
     // Forces only from host arrays, with charges and types staged by an
     // earlier call: the device computes with the staged copies while the
     // host compares them with q and type; on a difference the changed
@@ -1208,7 +1305,8 @@ int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names, int c
     auto prof = h->eng->profile(std::max(1, reps), h->eng->stream());
     if (h->elc) {
       Engine &e = *h->eng;
-      auto pe = elc_profile(*h->elc, h->sys.box, h->prm.prefactor, static_cast<long long>(h->n),
+      auto pe = elc_profile(*h->elc, h->sys.box, h->prm.prefactor, h->r_cut,
+                            static_cast<long long>(h->n),
                             e.d_pos(), e.d_q(), e.d_force(), std::max(1, reps), e.stream());
       prof.insert(prof.end(), pe.begin(), pe.end());
     }

@@ -38,6 +38,10 @@ struct ElcMode {
   double px, py; // 2 pi p / (L_x omega), 2 pi q / (L_y omega) (pq modes)
   int kind;      // 0: p-mode (q = 0), 1: q-mode (p = 0), 2: pq-mode
   int p, q, pad;
+  // dielectric contrasts (setup_PoQ :511-518, setup_PQ :651-658)
+  double pref_di;       // prefactor * {4, 8} pi / (L_x L_y)
+  double fdb, fdt, fd;  // delta_bot fac_elc, delta_top fac_elc, fdb delta_top
+  double em2h;          // exp(-2 omega box_h)
 };
 
 struct ElcGeom {
@@ -47,7 +51,17 @@ struct ElcGeom {
   double pref_dip;     // prefactor 4 pi / V (add_dipole_force)
   long long n;
   int nmodes, nfx, nfy, neutralize;
+  // dielectric contrasts / constant potential (effective flags of elc_data)
+  int contrast, const_pot;
+  double sl;            // space_layer
+  double db, dt;        // delta_mid_bot, delta_mid_top
+  double pot_diff;
+  double pref_z;        // prefactor 2 pi / (L_x L_y) (add_z_force)
+  double zf[3];         // z-force factors fdb, fdt, fd of add_z_force :446-449
 };
+
+// the scalar sums of one evaluation (dipole, z terms), after the mode sums
+constexpr int kElcScalars = 12;
 
 constexpr int kElcThreads = 256;
 constexpr int kElcPPT = 2;            // particles per thread in the sums kernel
@@ -202,12 +216,14 @@ __device__ __forceinline__ double elc_warp_sum8(double const (&v)[8]) {
 // Per particle tile (blockIdx.x) and mode chunk (blockIdx.y): the product sums
 // of each mode; chunk 0 also takes the dipole sums and the gap check
 // (check_gap :184-194: a charged particle below 0 or above L_z - gap).
+template <bool C>
 __global__ void __launch_bounds__(kElcThreads)
 k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ pos,
            const double *__restrict__ qv, double *__restrict__ part, int *__restrict__ gap_err) {
-  __shared__ double red[(kElcThreads / 32) * 8];
-  // per mode of the chunk, per warp, the 8 warp sums (one barrier per chunk)
-  __shared__ double wsum[kElcModesPerBlock][kElcThreads / 32][8];
+  constexpr int R = C ? 16 : 8; // sums per mode: own (+ image layers), then lclimge
+  __shared__ double red[(kElcThreads / 32) * 16];
+  // per mode of the chunk, per warp, the R warp sums (one barrier per chunk)
+  __shared__ double wsum[kElcModesPerBlock][kElcThreads / 32][R];
   long long const tile0 = static_cast<long long>(blockIdx.x) * kElcThreads * kElcPPT;
   int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   ElcPart P[kElcPPT];
@@ -219,9 +235,11 @@ k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restric
   }
   int const m0 = blockIdx.y * kElcModesPerBlock;
   int const m1 = min(g.nmodes, m0 + kElcModesPerBlock);
+  double const h = g.box_h;
   for (int m = m0; m < m1; ++m) {
     ElcMode const md = modes[m];
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double lcl[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < kElcPPT; ++k) {
       // uncharged particles and the tile's tail add zeros (q = 0)
@@ -229,54 +247,163 @@ k_elc_sums(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restric
       int const w = elc_products(md, g, P[k], v);
       for (int c = 0; c < w; ++c)
         acc[c] += v[c];
+      if constexpr (C) {
+        // image-layer terms (setup_PoQ :542-593, setup_PQ :699-763): the
+        // phase products pp (2 or 4) times exp(-+omega z') of the images
+        int const np = w >> 1;
+        double const q = P[k].q, z = P[k].z;
+        double const e = exp(md.omega * z), ie = 1.0 / e;
+        double pp[4];
+        for (int c = 0; c < np; ++c)
+          pp[c] = (q != 0.0) ? v[c] / (q * e) : 0.0;
+        bool const mb = z < g.sl, mt = z > h - g.sl;
+        double const e2 = mb ? (ie * md.em2h * g.db + e * md.em2h) * md.fd
+                             : (ie + e * md.em2h * g.dt) * md.fdb;
+        double const e3 = mt ? (e * md.em2h * md.em2h * g.dt + ie * md.em2h) * md.fd
+                             : (e * md.em2h + ie * md.em2h * g.db) * md.fdt;
+        double const et = mt ? exp(md.omega * (2.0 * h - z)) : 1.0;
+        for (int c = 0; c < np; ++c) {
+          if (mb) {
+            acc[c] += q * g.db * pp[c] * ie;
+            acc[np + c] += q * g.db * pp[c] * e;
+          }
+          if (mt) {
+            acc[c] += q * g.dt * pp[c] * et;
+            acc[np + c] += q * g.dt * pp[c] / et;
+          }
+          lcl[c] += pp[c] * q * e2;
+          lcl[np + c] += pp[c] * q * e3;
+        }
+      }
     }
     double const ws = elc_warp_sum8(acc);
     if ((lane & 3) == 0)
       wsum[m - m0][wid][lane >> 2] = ws;
+    if constexpr (C) {
+      double const wl = elc_warp_sum8(lcl);
+      if ((lane & 3) == 0)
+        wsum[m - m0][wid][8 + (lane >> 2)] = wl;
+    }
   }
   __syncthreads();
-  for (int o = threadIdx.x; o < (m1 - m0) * 8; o += kElcThreads) {
-    int const mm = o >> 3, c = o & 7;
+  for (int o = threadIdx.x; o < (m1 - m0) * R; o += kElcThreads) {
+    int const mm = o / R, c = o % R;
     double t = 0.0;
 #pragma unroll
     for (int w = 0; w < kElcThreads / 32; ++w)
       t += wsum[mm][w][c];
-    part[static_cast<long long>((m0 + mm) * 8 + c) * gridDim.x + blockIdx.x] = t;
+    part[static_cast<long long>((m0 + mm) * R + c) * gridDim.x + blockIdx.x] = t;
   }
   if (blockIdx.y == 0) {
-    double d[3] = {0, 0, 0};
+    // scalar sums (add_dipole_force, dipole_energy, add_z_force, z_energy):
+    // 0 q (z - s) + image terms, 1 q z, 2 q + image q, 3 q, 4 image q,
+    // 5 q (z - s), 6 image q (z' - s), 7 q (z - s)^2, 8 image q (z' - s)^2,
+    // 9 z-force charge sum, 10 z-energy image sum
+    double d[kElcScalars] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < kElcPPT; ++k) {
       long long const i = tile0 + k * kElcThreads + threadIdx.x;
-      if (i < g.n && P[k].q != 0.0) {
-        double const dz = P[k].z - g.shift;
-        d[0] += P[k].q * dz;
-        d[1] += P[k].q;
-        d[2] += P[k].q * dz * dz;
-        if (P[k].z < 0.0 || P[k].z > g.box_h)
+      double const q = P[k].q, z = P[k].z;
+      if (i < g.n && q != 0.0) {
+        double const dz = z - g.shift;
+        d[0] += q * dz;
+        d[1] += q * z;
+        d[2] += q;
+        d[3] += q;
+        d[5] += q * dz;
+        d[7] += q * dz * dz;
+        if (z < 0.0 || z > g.box_h)
           atomicMin(gap_err, static_cast<int>(i));
+        if constexpr (C) {
+          bool const mb = z < g.sl, mt = z > h - g.sl;
+          double const zb = -z - g.shift, zt = 2.0 * h - z - g.shift;
+          if (mb) {
+            d[0] += g.db * q * zb;
+            d[2] += g.db * q;
+            d[4] += g.db * q;
+            d[6] += g.db * q * zb;
+            d[8] += g.db * q * zb * zb;
+          }
+          if (mt) {
+            d[0] += g.dt * q * zt;
+            d[2] += g.dt * q;
+            d[4] += g.dt * q;
+            d[6] += g.dt * q * zt;
+            d[8] += g.dt * q * zt * zt;
+          }
+          double const delta = g.dt * g.db;
+          if (g.const_pot) {
+            double zs = 0.0, z3 = 0.0;
+            if (mb) {
+              zs -= g.db * q;
+              z3 -= g.db * q * zb;
+            }
+            if (mt) {
+              zs += g.dt * q;
+              z3 += g.dt * q * zt;
+            }
+            d[9] += zs;
+            d[10] += z3;
+          } else {
+            double const fdb = g.zf[0], fdt = g.zf[1], fd = g.zf[2];
+            double const dci = 1.0 / (1.0 - delta), lz = g.box[2];
+            auto ib = [&](double a, double zz) {
+              return a * dci * (zz - 2.0 * delta * lz * dci) - a * dci * g.shift;
+            };
+            auto it = [&](double a, double zz) {
+              return a * dci * (zz + 2.0 * delta * lz * dci) - a * dci * g.shift;
+            };
+            d[9] += mb ? fd * (g.db + 1.0) * q : fdb * (g.dt + 1.0) * q;
+            d[9] -= mt ? fd * (g.dt + 1.0) * q : fdt * (g.db + 1.0) * q;
+            d[10] += q * (mb ? ib(g.db * delta, -(2.0 * h + z)) + ib(delta, -(2.0 * h - z))
+                             : ib(g.db, -z) + ib(delta, -(2.0 * h - z)));
+            d[10] -= q * (mt ? it(g.dt * delta, 4.0 * h - z) + it(delta, 2.0 * h + z)
+                             : it(g.dt, 2.0 * h - z) + it(delta, 2.0 * h + z));
+          }
+        }
       }
     }
     long long const nbp = gridDim.x;
-    elc_block_sum<3>(d, red, part + nbp * g.nmodes * 8 + blockIdx.x, nbp);
+    elc_block_sum<kElcScalars>(d, red, part + nbp * g.nmodes * R + blockIdx.x, nbp);
   }
 }
 
-// G[m * 8 + c] = pref_m * (sum over tiles), one block per sum, tiles read
-// contiguously and added in a fixed order; the 3 dipole sums after them.
+// G[m * 8 + c] = pref_m * (sum over tiles) [+ pref_di * (lclimge sum) with
+// contrasts], one block per sum, tiles read contiguously and added in a
+// fixed order; the kElcScalars scalar sums after them.
+template <bool C>
 __global__ void __launch_bounds__(kElcThreads)
 k_elc_reduce(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restrict__ part,
              int nbp, double *__restrict__ G) {
+  constexpr int R = C ? 16 : 8;
   __shared__ double red[kElcThreads / 32];
+  __shared__ double out[1];
   int const t = blockIdx.x;
-  const double *row = part + static_cast<long long>(t) * nbp;
+  int const nm8 = g.nmodes * 8;
+  long long const r0 = (t < nm8) ? static_cast<long long>(t >> 3) * R + (t & 7)
+                                 : static_cast<long long>(g.nmodes) * R + (t - nm8);
   double v[1] = {0.0};
   for (int b = threadIdx.x; b < nbp; b += kElcThreads)
-    v[0] += row[b];
-  __shared__ double out[1];
+    v[0] += part[r0 * nbp + b];
   elc_block_sum<1>(v, red, out);
-  if (threadIdx.x == 0)
-    G[t] = (t < g.nmodes * 8) ? modes[t >> 3].pref * out[0] : out[0];
+  if (t >= nm8) {
+    if (threadIdx.x == 0)
+      G[t] = out[0];
+    return;
+  }
+  double const own = out[0];
+  double other = 0.0;
+  if constexpr (C) {
+    double w[1] = {0.0};
+    for (int b = threadIdx.x; b < nbp; b += kElcThreads)
+      w[0] += part[(r0 + 8) * nbp + b];
+    elc_block_sum<1>(w, red, out);
+    other = out[0];
+  }
+  if (threadIdx.x == 0) {
+    ElcMode const md = modes[t >> 3];
+    G[t] = C ? md.pref * own + md.pref_di * other : md.pref * own;
+  }
 }
 
 // Three blocks per SM (80 registers, a few spilled): 0.401 -> 0.367 ms at
@@ -348,11 +475,17 @@ k_elc_forces(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restr
     fx = q * ax;
     fy = q * ay;
     fz = q * az;
-    // dipole force (add_dipole_force :201-264 without contrasts / const_pot)
+    // dipole force (add_dipole_force :201-264) and the z force of
+    // contrasts (add_z_force :441-494) from the scalar sums
     const double *D = G + static_cast<long long>(g.nmodes) * 8;
-    fz -= g.pref_dip * D[0] * q;
+    double field = g.pref_dip * D[0];
+    if (g.const_pot)
+      field -= g.pot_diff / g.box_h + g.pref_dip / g.box_h * g.box[2] * D[1];
+    fz -= field * q;
     if (!g.neutralize)
-      fz += g.pref_dip * D[1] * q * (z - g.shift);
+      fz += g.pref_dip * D[2] * q * (z - g.shift);
+    if (g.contrast)
+      fz += g.pref_z * D[9] * q;
     f[3 * i + 0] += fx;
     f[3 * i + 1] += fy;
     f[3 * i + 2] += fz;
@@ -363,6 +496,43 @@ k_elc_forces(ElcGeom g, const ElcMode *__restrict__ modes, const double *__restr
     if (threadIdx.x == 0)
       epart[blockIdx.x] = eb[0];
   }
+}
+
+// Image charges for the mesh (charge_assign :1111-1142): slot i the
+// particle (charge kept when bit 0 of which), slot n + i its bottom image
+// (x, y, -z) with q delta_bot, slot 2n + i its top image (x, y, 2h - z) with
+// q delta_top (bit 1; zero charge outside the space layer); positions folded.
+__global__ void k_elc_augment(const double *__restrict__ pos, const double *__restrict__ q,
+                              long long n, ElcGeom g, int which, double *__restrict__ apos,
+                              double *__restrict__ aq) {
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  double x[3];
+  for (int d = 0; d < 3; ++d)
+    x[d] = elc_fold(pos[3 * i + d], g.box[d]);
+  double const qi = q[i];
+  double const h = g.box_h;
+  bool const img = (which & 2) && qi != 0.0;
+  double const zb = elc_fold(-x[2], g.box[2]), zt = elc_fold(2.0 * h - x[2], g.box[2]);
+  for (int d = 0; d < 2; ++d) {
+    apos[3 * i + d] = x[d];
+    apos[3 * (n + i) + d] = x[d];
+    apos[3 * (2 * n + i) + d] = x[d];
+  }
+  apos[3 * i + 2] = x[2];
+  apos[3 * (n + i) + 2] = zb;
+  apos[3 * (2 * n + i) + 2] = zt;
+  aq[i] = (which & 1) ? qi : 0.0;
+  aq[n + i] = (img && x[2] < g.sl) ? g.db * qi : 0.0;
+  aq[2 * n + i] = (img && x[2] > h - g.sl) ? g.dt * qi : 0.0;
+}
+
+// f[k] += a[k], k < m
+__global__ void k_elc_add(double *__restrict__ f, const double *__restrict__ a, long long m) {
+  long long const k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k < m)
+    f[k] += a[k];
 }
 
 } // namespace p3mx

@@ -1311,6 +1311,131 @@ void Engine::set_bonds(std::vector<BondParam> const &types, std::vector<int> con
   m_bond_n = m_n;
 }
 
+// CoulombP3M::pair_force / pair_energy (electrostatics/p3m.hpp:146-180) in
+// FP64 for the ELC image terms.
+__device__ inline void elc_p3m_pair(RepGeom const &G, double q1q2, double const d[3],
+                                    double F[3], double &E) {
+  double const r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  if (q1q2 == 0.0 || r >= G.r_cut || r <= 0.0)
+    return;
+  double const ad = G.alpha * r;
+  double const t = 1.0 / (1.0 + 0.3275911 * ad);
+  double const asp =
+      t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 +
+                                                                       t * 1.061405429))));
+  double const ex = exp(-ad * ad);
+  double const eri = asp / r;
+  double const fac = ex * (eri + 2.0 * G.alpha / sqrt(kPi)) / (r * r) * G.prefactor * q1q2;
+  F[0] += fac * d[0];
+  F[1] += fac * d[1];
+  F[2] += fac * d[2];
+  E += G.prefactor * q1q2 * eri * ex;
+}
+
+// ELC dielectric-layer corrections (elc.hpp dielectric_layers_contribution,
+// dielectric_layers_self_forces / _self_energy, add_pair_force_corrections,
+// pair_energy_correction): particle a within sl of the bottom (top) wall,
+// image x' = (x, y, -z) ((x, y, 2h - z)), q_eff = delta q_a q_b: a gets
+// pair_force(q_eff, mi(x_b - x')) for each Verlet partner b and for itself
+// (b = a); energy: half of each term.  Positions and charges are read in
+// the original order through the sort permutation (always current).
+template <bool EV>
+__global__ void __launch_bounds__(256)
+k_elc_image_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+                  const int *__restrict__ perm, const double *__restrict__ pos,
+                  const double *__restrict__ qv, const int *__restrict__ nb,
+                  const int *__restrict__ nb_cnt, double sl, double h, double db, double dt,
+                  double *__restrict__ f, double *__restrict__ epart) {
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  double en = 0.0;
+  if (a < G.p0 + G.np) {
+    int const i = perm[a];
+    double const qa = qv[i];
+    double xa[3];
+    for (int d = 0; d < 3; ++d)
+      xa[d] = pos[3 * i + d] - floor(pos[3 * i + d] * G.box_i[d]) * G.box[d];
+    bool const mb = qa != 0.0 && xa[2] < sl;
+    bool const mt = qa != 0.0 && xa[2] > h - sl;
+    if (mb || mt) {
+      double F[3] = {0.0, 0.0, 0.0};
+      int const cnt = nb_cnt[a];
+      const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
+      for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? mb : mt))
+          continue;
+        double const dl = side == 0 ? db : dt;
+        double const img[3] = {xa[0], xa[1], side == 0 ? -xa[2] : 2.0 * h - xa[2]};
+        double d[3];
+        for (int c = 0; c < 3; ++c)
+          d[c] = mi_d(xa[c] - img[c], G.box[c], G.box_i[c]);
+        double E = 0.0;
+        elc_p3m_pair(G, dl * qa * qa, d, F, E);
+        for (int k = 0; k < cnt; ++k) {
+          long long const b =
+              G.p0 + static_cast<long long>(static_cast<unsigned>(nbp[nb_entry(0, k)]) & kNbIndexMask);
+          int const j = perm[b];
+          double const qb = qv[j];
+          if (qb == 0.0)
+            continue;
+          for (int c = 0; c < 3; ++c) {
+            double const xb = pos[3 * j + c] - floor(pos[3 * j + c] * G.box_i[c]) * G.box[c];
+            d[c] = mi_d(xb - img[c], G.box[c], G.box_i[c]);
+          }
+          elc_p3m_pair(G, dl * qa * qb, d, F, E);
+        }
+        en += 0.5 * E;
+      }
+      f[3 * i + 0] += F[0];
+      f[3 * i + 1] += F[1];
+      f[3 * i + 2] += F[2];
+    }
+  }
+  if constexpr (EV) {
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1)
+      en += __shfl_down_sync(0xffffffffu, en, o);
+    if ((threadIdx.x & 31) == 0)
+      red[threadIdx.x >> 5] = en;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < 8; ++w)
+        s += red[w];
+      epart[blockIdx.x] = s;
+    }
+  }
+}
+
+void Engine::elc_image_pairs(double sl, double h, double db, double dt, double *f,
+                             double *energy, cudaStream_t st) {
+  if (energy)
+    *energy = 0.0;
+  if (m_n == 0)
+    return;
+  RepGeom const *geom = m_geom_d.as<RepGeom>();
+  if (energy) {
+    m_elc_epart.ensure(static_cast<size_t>(m_n_blk_pair) * sizeof(double));
+    k_elc_image_pairs<true><<<m_n_blk_pair, 256, 0, st>>>(
+        geom, m_blk_pair.as<int2>(), m_cperm.as<int>(), d_pos(), d_q(), m_nb.as<int>(),
+        m_nb_cnt.as<int>(), sl, h, db, dt, f, m_elc_epart.as<double>());
+    ++m_launches;
+    std::vector<double> ep(m_n_blk_pair);
+    P3MX_CUDA(cudaMemcpyAsync(ep.data(), m_elc_epart.p, ep.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    for (double v : ep)
+      *energy += v;
+  } else {
+    k_elc_image_pairs<false><<<m_n_blk_pair, 256, 0, st>>>(
+        geom, m_blk_pair.as<int2>(), m_cperm.as<int>(), d_pos(), d_q(), m_nb.as<int>(),
+        m_nb_cnt.as<int>(), sl, h, db, dt, f, nullptr);
+    ++m_launches;
+  }
+  P3MX_CUDA(cudaGetLastError());
+}
+
 void Engine::bond_forces(double *f, cudaStream_t st) {
   if (m_nbonds == 0)
     return;

@@ -129,6 +129,11 @@ public:
   void set_bonds(std::vector<BondParam> const &types, std::vector<int> const &bonds,
                  cudaStream_t st);
   void bond_forces(double *f, cudaStream_t st);
+  // ELC with dielectric contrasts: every charged particle within sl of a
+  // wall feels its own image and, over its Verlet partners, the partners'
+  // interaction with its image (added to f; energy sum with energy != null)
+  void elc_image_pairs(double sl, double h, double db, double dt, double *f, double *energy,
+                       cudaStream_t st);
   void bond_observables(cudaStream_t st, double *energy, double *virial9);
   // bonded energy of every replica (zeros without bonds); synchronises
   std::vector<double> bond_energies(cudaStream_t st);
@@ -202,6 +207,7 @@ private:
   std::vector<double> m_census_h;
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
+  DevBuf m_elc_epart;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_rflag, m_part_pair, m_sums_pair;
   DevBuf m_type_ref; // types at the last list build (a change triggers a rebuild)
   // kernel error word: [0] a bounded wait ran out; [1] bond status (1 broken,

@@ -18,7 +18,8 @@ def p3m():
     (dict(pot_diff=3.0), ValueError, "Parameter 'const_pot' must be True when 'pot_diff'"),
     (dict(delta_mid_top=1.5), ValueError, "Parameter 'delta_mid_top' must be >= -1 and <= \\+1"),
     (dict(delta_mid_bot=-1.5), ValueError, "Parameter 'delta_mid_bot' must be >= -1 and <= \\+1"),
-    (dict(delta_mid_bot=0.5), RuntimeError, "dielectric contrasts"),
+    (dict(delta_mid_bot=-1.0, delta_mid_top=-1.0), ValueError,
+     "two parallel metallic boundaries requires the const_pot option"),
     (dict(far_cut="x"), TypeError, "far_cut has to be a float"),
     (dict(maxPWerror="x"), TypeError, "maxPWerror has to be a float"),
     (dict(neutralize=1), TypeError, "neutralize has to be a bool"),

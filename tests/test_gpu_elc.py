@@ -186,3 +186,99 @@ def test_elc_through_the_c_abi_long_range():
     np.testing.assert_array_equal(f2, f0)
     assert e2 == e0
     assert lib.p3mx_get_elc(h, None, None, None) != 0
+
+
+# --- dielectric contrasts and constant potential ------------------------------
+
+def test_elc_finite_potential_drop():
+    """testsuite/python/elc.py:43-104 (metallic walls, applied potential)."""
+    gap = 3.0
+    box = np.array([10.0, 10.0, 10.0 + gap])
+    s = _system(box, [[0.0, 0.0, 1.0], [0.0, 0.0, 9.0]], [1.0, -1.0])
+    p3m = P3M(prefactor=1e-100, mesh=32, cao=5, accuracy=1e-3)
+    s.electrostatics.solver = ELC(actor=p3m, gap_size=gap, maxPWerror=1e-3, delta_mid_top=-1,
+                                  delta_mid_bot=-1, const_pot=True, pot_diff=-3.0)
+    u = s.analysis.energy()["coulomb"]
+    e_field = -3.0 / (box[2] - gap)
+    p1, p2 = s.part.by_id(0), s.part.by_id(1)
+    assert u == pytest.approx(-e_field * (1.0 * 1.0 + 9.0 * -1.0), abs=1e-7)
+    s.integrator.run(0)
+    assert p1.f[2] / 1.0 == pytest.approx(e_field, abs=1e-7)
+    assert p2.f[2] / -1.0 == pytest.approx(e_field, abs=1e-7)
+    p1.pos = [box[0] / 2, box[1] / 2, box[2] - gap / 2]
+    with pytest.raises(Exception, match="entered ELC gap region"):
+        s.integrator.run(2)
+
+
+@pytest.mark.parametrize("cls", [P3M, P3MGPU])
+def test_elc_metallic_walls_madelung(cls):
+    """testsuite/python/elc.py:107-145: rock salt between metallic walls."""
+    n = 12
+    idx = np.array(np.meshgrid(np.arange(n), np.arange(n), np.arange(n),
+                               indexing="ij")).reshape(3, -1).T
+    gap = 0.4 * n
+    s = _system([n, n, n + gap], idx + 0.5, (-1.0) ** idx.sum(axis=1))
+    p3m = cls(prefactor=1, mesh=[60, 60, 84], cao=7, r_cut=3.314, alpha=1.18, accuracy=3e-7,
+              tune=False)
+    s.electrostatics.solver = ELC(actor=p3m, gap_size=gap, maxPWerror=3e-7, delta_mid_top=-1,
+                                  delta_mid_bot=-1, const_pot=True, pot_diff=0)
+    u = 2.0 * s.analysis.energy()["coulomb"] / n ** 3
+    np.testing.assert_allclose(u, -1.74756459463318219, rtol=1e-6, atol=0)
+
+
+def test_elc_dielectric_interface_vs_analytic():
+    """testsuite/python/elc_vs_analytic.py:28-98 (delta_mid_bot = 39/41);
+    P3M mesh and cao of the test, r_cut 60 and the alpha of the real-space
+    error 1e-7 (the test tunes them)."""
+    box = np.array([200.0, 200.0, 275.0])
+    gap, dist, dmb = 75.0, 1.0, 39.0 / 41.0
+    zs = np.linspace(0.1, 200.0 - 0.1 - dist, 12)
+    qs = np.arange(-5.0, 5.1, 2.5)
+    s = _system(box, [[100.0, 100.0, 100.0], [100.0, 100.0, 100.0 + dist]], [qs[0], -qs[0]])
+    s.cell_system.skin = 0.4
+    p3m = P3M(prefactor=2.0, accuracy=1e-7, mesh=[58, 58, 70], cao=4, r_cut=60.0,
+              alpha=0.05593284122999153, tune=False)
+    s.electrostatics.solver = ELC(actor=p3m, gap_size=gap, maxPWerror=1e-7, delta_mid_bot=dmb,
+                                  delta_mid_top=0.0)
+    forces = np.empty((len(qs), len(zs)))
+    energies = np.empty_like(forces)
+    p1, p2 = s.part.by_id(0), s.part.by_id(1)
+    for a, qq in enumerate(qs):
+        p1.q, p2.q = qq, -qq
+        for b, z in enumerate(zs):
+            p1.pos = [100.0, 100.0, z]
+            p2.pos = [100.0, 100.0, z + dist]
+            s.integrator.run(0)
+            forces[a, b] = p1.f[2]
+            energies[a, b] = s.analysis.energy()["total"]
+    cq = 2.0 * np.square(qs.reshape(-1, 1))
+    f_ref = cq * (1 / dist ** 2 + dmb * (1 / np.square(2 * zs) - 1 / np.square(2 * zs + dist)))
+    e_ref = cq * (-1 / dist + dmb * (1 / (4 * zs) - 1 / (2 * zs + dist) + 1 / (4 * (zs + dist))))
+    np.testing.assert_allclose(energies, e_ref, atol=1e-4)
+    np.testing.assert_allclose(forces, f_ref, atol=1e-4, rtol=1e-7)
+
+
+def test_elc_contrast_vs_oracle():
+    """A neutral slab between two dielectric walls (delta 0.5 below, -0.3
+    above): forces and energy against the oracle's elc_system."""
+    rng = np.random.default_rng(5)
+    box = np.array([9.0, 10.0, 14.0])
+    gap = 3.5
+    n = 240
+    pos = rng.uniform([0, 0, 0.05], [box[0], box[1], box[2] - gap - 0.05], (n, 3))
+    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    s = _system(box, pos, q)
+    p3m = P3M(prefactor=1.3, accuracy=1e-4, mesh=32, cao=5, r_cut=2.0, alpha=1.6, tune=False)
+    s.electrostatics.solver = ELC(actor=p3m, gap_size=gap, maxPWerror=1e-6, delta_mid_bot=0.5,
+                                  delta_mid_top=-0.3)
+    s.integrator.run(0)
+    f = s.part.all().f
+    e = s.analysis.energy()["coulomb"]
+    fo, eo = O.elc_system(box, gap, pos, q, 1.3, 1.6, 2.0, 32, 5, 1e-6, delta_bot=0.5,
+                          delta_top=-0.3)
+    np.testing.assert_allclose(f, fo, atol=1e-9 * np.abs(fo).max(), rtol=0)
+    assert e == pytest.approx(eo, rel=1e-8, abs=1e-8)
+    # a net charge with a non-metallic contrast is rejected
+    s.part.by_id(0).q = 2.0
+    with pytest.raises(Exception, match="non-neutral"):
+        s.integrator.run(0)
