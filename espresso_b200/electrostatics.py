@@ -185,8 +185,10 @@ class ELC:
     (src/python/espressomd/electrostatics.py:288-365): same keyword
     arguments, defaults and checks.  The base ``actor`` (P3M or P3MGPU)
     computes the 3D-periodic solution and the correction runs in FP64 CUDA
-    kernels of libp3mx.so.  Dielectric contrasts (``delta_mid_top`` /
-    ``delta_mid_bot`` != 0) are not supported and raise RuntimeError.
+    kernels of libp3mx.so; with dielectric contrasts (``delta_mid_top`` /
+    ``delta_mid_bot`` != 0, optionally ``const_pot``) the mesh also carries
+    the image charges (in FP64 for both actors) and the short-range loop the
+    image-layer corrections.
     """
     _so_name = "Coulomb::ElectrostaticLayerCorrection"
     _defaults = {"far_cut": -1., "delta_mid_top": 0., "delta_mid_bot": 0.,

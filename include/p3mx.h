@@ -179,16 +179,15 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q,
 
 /* Parameters of espressomd.electrostatics.ELC (src/python/espressomd/
  * electrostatics.py:288-365) as the elc_data constructor takes them
- * (src/core/electrostatics/elc.cpp:1056-1102).  Dielectric contrasts are not
- * supported: delta_mid_top and delta_mid_bot must be 0 (const_pot then has
- * no effect, as in the reference, where it needs a contrast). */
+ * (src/core/electrostatics/elc.cpp:1056-1102); const_pot has an effect only
+ * with a dielectric contrast, as in the reference. */
 typedef struct {
   double maxPWerror;
   double gap_size;
   double far_cut;       /* -1: tuned from maxPWerror (tune_far_cut) */
-  int neutralize;       /* bool; reference default 1 */
-  double delta_mid_top; /* must be 0 */
-  double delta_mid_bot; /* must be 0 */
+  int neutralize;       /* bool; reference default 1 (off with contrasts) */
+  double delta_mid_top; /* dielectric contrast above the slab, [-1, 1] */
+  double delta_mid_bot; /* dielectric contrast below the slab, [-1, 1] */
   int const_pot;        /* bool */
   double pot_diff;
 } p3mx_elc_params;
@@ -203,7 +202,10 @@ typedef struct {
  * :1189-1229) and report a zero k-space virial (the reference computes no
  * ELC pressure, electrostatics/coulomb.cpp:124-131).  A charged particle in
  * the gap fails the call with "Particle <i> entered ELC gap region by <dz>"
- * (check_gap :184-194). */
+ * (check_gap :184-194).  With dielectric contrasts only p3mx_forces
+ * evaluates (the image terms span short and long range): the mesh carries
+ * the image charges, the short-range loop the image-layer corrections
+ * (elc.hpp), and p3mx_long_range fails with a message. */
 int p3mx_set_elc(p3mx_handle *h, const p3mx_elc_params *p);
 /* The far-formula cutoff in use, the slab height L_z - gap_size and the
  * number of Fourier modes summed (each may be NULL). */
