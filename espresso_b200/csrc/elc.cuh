@@ -1,7 +1,9 @@
 // Electrostatic layer correction (ELC) for slab systems: the far-formula
 // correction that removes the interactions with the periodic images along z
-// from a 3D-periodic P3M solution (electrostatics/elc.cpp), here without
-// dielectric contrasts (delta_mid_top = delta_mid_bot = 0, no const_pot).
+// from a 3D-periodic P3M solution (electrostatics/elc.cpp), with dielectric
+// contrasts at the slab walls and a constant potential difference (their
+// image-charge mesh and short-range terms are driven from elc_host.cuh and
+// the engine's k_elc_image_pairs).
 //
 // The correction is a sum over Fourier modes (p, q) of the x-y plane; per
 // mode it is a product decomposition: each particle contributes 4 (modes with
@@ -19,10 +21,12 @@
 // p-major, so a pq-mode block needs one x sincos per p and rotations in q.
 //
 // Device layout (all FP64):
-//   part : per mode m and component c, the product sums of every particle
-//          tile b, [m * 8 + c][b]; then the 3 dipole sums [nm8 + c][b];
-//   G    : per mode the 8 sums over all tiles times the mode prefactor, then
-//          the 3 dipole sums;
+//   part : per mode m and row c, the sums of every particle tile b,
+//          [m * R + c][b] with R = 8 (own products plus image-layer terms)
+//          or 16 with contrasts (then 8 more lclimge rows); then the
+//          kElcScalars dipole / z sums [nmodes * R + c][b];
+//   G    : per mode the 8 sums over all tiles times the mode prefactors,
+//          then the kElcScalars scalar sums;
 //   epart: per block of the force kernel, its energy sum (EV only).
 // Every sum is taken in a fixed order (no atomics): results are
 // deterministic run to run.

@@ -42,8 +42,8 @@ struct ElcState {
   bool neutralize() const { return prm.neutralize && !contrast(); }
 };
 
-// elc_data::elc_data (elc.cpp:1056-1102); dielectric contrasts and the
-// constant-potential option are not part of this library.
+// elc_data::elc_data (elc.cpp:1056-1102): the parameter domains and the
+// rule that two metallic walls need const_pot.
 inline void elc_validate(p3mx_elc_params const &p) {
   double const delta_range = 1.0 + std::sqrt(1e-14);
   bool const far_calc = (p.far_cut == -1.0);
