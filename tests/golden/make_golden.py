@@ -14,7 +14,8 @@ Sources (paths relative to the ESPResSo tree):
     forces from MMM2D) with the parameters and the MMM2D energy of
     testsuite/python/coulomb_mixed_periodicity.py:30-40, 84-121 (ELC)
   * known answers written in testsuite/python/electrostatic_interactions.py:81-124
-    and testsuite/python/p3m_madelung.py:202-313 (parameters and constants)
+    and testsuite/python/p3m_madelung.py:69-313 (parameters and constants,
+    electric and magnetic)
   * values of the reference's own math headers (bspline.hpp, AS_erfc_part.hpp,
     p3m/math.hpp) evaluated through oracle/_ref/libref_math.so, which
     oracle/Makefile compiles from the reference tree in place.
@@ -90,6 +91,22 @@ def main():
             "energy_rtol": 1e-6, "pressure_rtol": 5e-6,
             "gpu_params": {"mesh": 42, "cao": 7, "r_cut": 5.5,
                            "alpha": 0.709017, "accuracy": 3e-7}},
+    }
+    # dipolar P3M: energy per dipole x spacing^3 / dipm^2 of the magnetic
+    # wire / sheet / cube (testsuite/python/p3m_madelung.py:69-200)
+    known["magnetic"] = {
+        "source": "testsuite/python/p3m_madelung.py:69-200",
+        "dipm": 1.05,
+        "wire": {"n_part": 64, "spacing": 1.2, "mesh": 48, "cao": 6, "r_cut": 28.0,
+                 "alpha": 0.137582516, "accuracy": 1e-9,
+                 "parallel": "-2 zeta(3)", "antiparallel": "3/2 zeta(3)", "rtol": 2e-9},
+        "sheet": {"n_part": 32, "spacing": 2.4, "mesh": 48, "cao": 7, "r_cut": 33.6,
+                  "alpha": 0.1186918, "accuracy": 1e-9,
+                  "parallel": -2.54944, "antiparallel": 3.01716, "rtol": 4e-6},
+        "cube": {"n_part": 8, "spacing": 2.4, "mesh": 64, "cao": 7, "r_cut": 8.2,
+                 "alpha": 0.5091135, "accuracy": 5e-8,
+                 "parallel": -2.67679, "antiparallel": 4.84473,
+                 "rtol": 1e-6, "rtol_antiparallel": 3e-4},
     }
     with open(os.path.join(HERE, "known_answers.json"), "w") as fh:
         json.dump(known, fh, indent=1)

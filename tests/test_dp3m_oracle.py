@@ -1,0 +1,77 @@
+"""The dipolar P3M energy restatement of the oracle (CPU only), pinned on the
+magnetic Madelung cases of the reference's testsuite/python/p3m_madelung.py
+(infinite wire, sheet and cube of point dipoles, parallel and antiparallel
+orderings): energy per dipole x spacing^3 / dipm^2 against the constants and
+tolerances of that test."""
+import itertools
+import json
+import os
+
+import numpy as np
+import pytest
+from scipy.special import zeta
+
+from oracle import oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+MAG = json.load(open(os.path.join(GOLD, "known_answers.json")))["magnetic"]
+
+
+def _run(case, pos, dips):
+    k = MAG[case]
+    n, sp, dipm = k["n_part"], k["spacing"], MAG["dipm"]
+    e = O.dp3m_energy(n * sp, pos * sp, dipm * np.asarray(dips, dtype=float), 1.0, k["alpha"],
+                      k["r_cut"], k["mesh"], k["cao"], k["accuracy"])
+    return e / len(pos) / dipm ** 2 * sp ** 3
+
+
+def test_dp3m_oracle_magnetic_wire():
+    n = MAG["wire"]["n_part"]
+    pos = np.array([[j, 0, 0] for j in range(n)], dtype=float)
+    rtol = MAG["wire"]["rtol"]
+    np.testing.assert_allclose(_run("wire", pos, [[1.0, 0, 0]] * n), -2.0 * zeta(3),
+                               rtol=rtol, atol=0)
+    np.testing.assert_allclose(_run("wire", pos, [[(-1.0) ** j, 0, 0] for j in range(n)]),
+                               1.5 * zeta(3), rtol=rtol, atol=0)
+
+
+def test_dp3m_oracle_magnetic_sheet():
+    n = MAG["sheet"]["n_part"]
+    pos, par, anti = [], [], []
+    for j, k in itertools.product(range(n), repeat=2):
+        th = (-1) ** k * np.pi / 4 + np.pi if j % 2 == 0 else (-1) ** (k + 1) * np.pi / 4
+        anti.append([np.cos(th), np.sin(th), 0.0])
+        par.append([0.0, (-1.0) ** j, 0.0])
+        pos.append([j, k, 0])
+    pos = np.array(pos, dtype=float)
+    rtol = MAG["sheet"]["rtol"]
+    np.testing.assert_allclose(_run("sheet", pos, par), MAG["sheet"]["parallel"], rtol=rtol, atol=0)
+    np.testing.assert_allclose(_run("sheet", pos, anti), MAG["sheet"]["antiparallel"], rtol=rtol,
+                               atol=0)
+
+
+def test_dp3m_oracle_magnetic_cube():
+    n = MAG["cube"]["n_part"]
+    pos, par, anti = [], [], []
+    for i, j, k in itertools.product(range(n), repeat=3):
+        th = np.pi + (-1) ** j * np.pi / 4 if i % 2 == 0 else (-1) ** (j + 1) * np.pi / 4
+        anti.append([np.cos(th), np.sin(th), 0.0])
+        par.append([0.0, 0.0, (-1.0) ** (i + j)])
+        pos.append([i, j, k])
+    pos = np.array(pos, dtype=float)
+    np.testing.assert_allclose(_run("cube", pos, par), MAG["cube"]["parallel"],
+                               rtol=MAG["cube"]["rtol"], atol=0)
+    np.testing.assert_allclose(_run("cube", pos, anti), MAG["cube"]["antiparallel"],
+                               rtol=MAG["cube"]["rtol_antiparallel"], atol=0)
+
+
+def test_dp3m_oracle_influence_function_zeroes_and_symmetry():
+    """The energy is even in the dipoles and invariant under a lattice
+    translation of all particles by one mesh spacing."""
+    rng = np.random.default_rng(2)
+    L, M = 10.0, 16
+    pos = rng.uniform(0, L, (20, 3))
+    dip = rng.normal(size=(20, 3))
+    e = O.dp3m_energy(L, pos, dip, 1.0, 0.9, 3.0, M, 5, 1e-4)
+    assert O.dp3m_energy(L, pos, -dip, 1.0, 0.9, 3.0, M, 5, 1e-4) == pytest.approx(e, rel=1e-12)
+    assert O.dp3m_energy(L, pos + L / M, dip, 1.0, 0.9, 3.0, M, 5, 1e-4) == pytest.approx(e, rel=1e-9)
