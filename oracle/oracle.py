@@ -627,28 +627,54 @@ def _meshift(m, zero_mid):
     return r
 
 
-def dp3m_energy(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy):
-    """Dipolar P3M energy (k space + real space + corrections) in FP64 numpy,
-    restating magnetostatics/dp3m.cpp for a cubic box and mesh: the three
-    dipole-component meshes assigned with the charge-assignment weights
-    (dipole_assign; here through the charge oracle, one component at a
-    time), the dipolar optimal influence function G_opt_dipolar<3> with
-    m = 0 (p3m/influence_function_dipolar.hpp: numerator
-    U^2 exp(-pi^2 |n|^2 / alpha_L^2) / |n|^2 (d_op . n)^3, denominator
-    |d_op|^6 (U^2)^2, zero where all indices are multiples of M/2, times
-    2 M^3 / L^2), the energy sum G |mu(k) . d_op|^2 prefactor pi / (M^3 L)
-    (long_range_kernel :270-310), the self term
+def _dp3m_influence(M, L, cao, alpha, S):
+    """grid_influence_function<S> of the dipolar P3M
+    (p3m/influence_function_dipolar.hpp): G_opt_dipolar<S> with m = 0,
+    numerator U^2 exp(-pi^2 |n|^2 / alpha_L^2) / |n|^2 (d_op . n)^S,
+    denominator |d_op|^(2S) (U^2)^2, zero where all indices are multiples of
+    M/2, times 2 M^3 / L^2.  S = 2 for the energy, 3 for the forces.
+    Returns (g, keep mask, shift grids, d_op grids)."""
+    shift = _meshift(M, False)
+    dop = _meshift(M, True)
+    sx, sy, sz = np.meshgrid(shift, shift, shift, indexing="ij")
+    dx, dy, dz = np.meshgrid(dop, dop, dop, indexing="ij")
+    i0, i1, i2 = np.meshgrid(np.arange(M), np.arange(M), np.arange(M), indexing="ij")
+    h = M // 2
+    keep = (i0 % h != 0) | (i1 % h != 0) | (i2 % h != 0)
+    u2 = (np.sinc(sx / M) * np.sinc(sy / M) * np.sinc(sz / M)) ** (2 * cao)
+    n2 = (sx * sx + sy * sy + sz * sz).astype(np.float64)
+    ex = (np.pi / (alpha * L)) ** 2 * n2
+    dn = (dx * sx + dy * sy + dz * sz).astype(np.float64)
+    dd = (dx * dx + dy * dy + dz * dz).astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        num = np.where(ex < 30.0, u2 * np.exp(-ex) / n2 * dn ** S, 0.0)
+        g = np.where(keep, 2.0 * M ** 3 / L ** 2 * num / (dd ** S * u2 * u2), 0.0)
+    return g, keep, (sx, sy, sz), (dx, dy, dz)
+
+
+def dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy, want_forces=True):
+    """Dipolar P3M (cubic box and mesh, metallic) in FP64 numpy, restating
+    magnetostatics/dp3m.cpp and dp3m.hpp: the three dipole-component meshes
+    assigned with the charge-assignment weights (dipole_assign; here through
+    the charge oracle, one component at a time), the k-space energy
+    G_energy |mu(k) . d_op|^2 prefactor pi / (M^3 L) with the self term
     -prefactor sum mu^2 2 alpha^3 / (3 sqrt pi) and the Madelung-self
-    correction prefactor E_corr / V with E_corr = -sum mu^2 (U_k + E_self +
-    2 pi / 3) (calc_energy_correction, calc_average_self_energy_k_space,
-    grid_influence_function_self_energy with the aliasing sum over
-    m in [-1, 1]^3), and the real-space pair energies
-    prefactor (mi.mj B(r) - (mi.r)(mj.r) C(r)) over minimum-image pairs
-    within r_cut (dp3m.hpp pair_energy; exact erfc below accuracy 5e-6, the
-    Abramowitz-Stegun form above)."""
+    correction (long_range_kernel :270-310, calc_energy_correction,
+    calc_average_self_energy_k_space with the aliasing sum over
+    m in [-1, 1]^3); the k-space torques tau -= mu x (prefactor 2 pi / (M^3 L)
+    E), E_d interpolated from the backward transform of
+    d_op_d G_energy (mu . d_op) (AssignTorques), and forces
+    F_d += mu . (prefactor (2 pi / L)^2 / M^3 E^(d)), E^(d)_c from
+    d_op_c d_op_d G_force (-i) (mu . d_op) (AssignForces, :322-420); the
+    real-space pair energy, force and torque with B, C, D of dp3m.hpp
+    :142-232 over minimum-image pairs within r_cut (exact erfc below accuracy
+    5e-6), the partner getting -F and -(tau + d x F) (calc_opposing_force,
+    forces_inline.hpp:159-171).  Mesh values are interpolated with each
+    particle's own assignment stencil.  Returns (forces, torques, energy)."""
     L = float(box_l)
     pos = np.asarray(pos, dtype=np.float64)
     dip = np.asarray(dip, dtype=np.float64)
+    n = len(pos)
     M = int(mesh)
     prm = make_params([L] * 3, M, cao, alpha, r_cut, 1.0)
     rho = []
@@ -657,44 +683,48 @@ def dp3m_energy(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy):
         rho.append(p3m_kspace(prm, pos, c, want_mesh=True)[3] if np.any(c != 0.0)
                    else np.zeros((M, M, M)))
     F = [np.fft.fftn(r) for r in rho]
-    shift = _meshift(M, False)
-    dop = _meshift(M, True)
-    sx, sy, sz = np.meshgrid(shift, shift, shift, indexing="ij")
-    dx, dy, dz = np.meshgrid(dop, dop, dop, indexing="ij")
-    i0, i1, i2 = np.meshgrid(np.arange(M), np.arange(M), np.arange(M), indexing="ij")
-    h = M // 2
-    keep = (i0 % h != 0) | (i1 % h != 0) | (i2 % h != 0)
-    alpha_L = alpha * L
-    u2 = (np.sinc(sx / M) * np.sinc(sy / M) * np.sinc(sz / M)) ** (2 * cao)
-    n2 = (sx * sx + sy * sy + sz * sz).astype(np.float64)
-    ex = (np.pi / alpha_L) ** 2 * n2
-    dn = (dx * sx + dy * sy + dz * sz).astype(np.float64)
-    dd = (dx * dx + dy * dy + dz * dz).astype(np.float64)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        num = np.where(ex < 30.0, u2 * np.exp(-ex) / n2 * dn ** 3, 0.0)
-        g = np.where(keep, 2.0 * M ** 3 / L ** 2 * num / (dd ** 3 * u2 * u2), 0.0)
-    mk = F[0] * dx + F[1] * dy + F[2] * dz
-    e_k = np.sum(g * (mk.real ** 2 + mk.imag ** 2)) * prefactor / M ** 3 * np.pi / L
+    g_e, keep, (sx, sy, sz), dops = _dp3m_influence(M, L, cao, alpha, 2)
+    mk = F[0] * dops[0] + F[1] * dops[1] + F[2] * dops[2]
+    energy = np.sum(g_e * (mk.real ** 2 + mk.imag ** 2)) * prefactor / M ** 3 * np.pi / L
     sum_mu2 = float(np.sum(dip * dip))
-    e_k -= prefactor * sum_mu2 / np.sqrt(np.pi) * (2.0 / 3.0) * alpha ** 3
-    # Madelung-self correction
-    u2s = np.zeros_like(u2)
+    energy -= prefactor * sum_mu2 / np.sqrt(np.pi) * (2.0 / 3.0) * alpha ** 3
+    u2s = np.zeros((M, M, M))
     for m0 in (-1, 0, 1):
         for m1 in (-1, 0, 1):
             for m2 in (-1, 0, 1):
                 u2s += (np.sinc(sx / M + m0 * M) * np.sinc(sy / M + m1 * M) *
                         np.sinc(sz / M + m2 * M)) ** (2 * cao)
-    phi = np.sum(np.where(keep, g * u2s * dd, 0.0))
+    dd = (dops[0] ** 2 + dops[1] ** 2 + dops[2] ** 2).astype(np.float64)
+    phi = np.sum(np.where(keep, g_e * u2s * dd, 0.0))
     vol = L ** 3
     uk = phi / (3.0 * L * M ** 3) * np.pi * vol
-    e_self = -2.0 * alpha_L ** 3 / np.sqrt(np.pi) / 3.0
-    e_corr = -sum_mu2 * (uk + e_self + 2.0 * np.pi / 3.0)
-    e_k += prefactor * e_corr / vol
+    e_self = -2.0 * (alpha * L) ** 3 / np.sqrt(np.pi) / 3.0
+    energy += prefactor * (-sum_mu2 * (uk + e_self + 2.0 * np.pi / 3.0)) / vol
+    f = np.zeros((n, 3))
+    t = np.zeros((n, 3))
+    if want_forces and n:
+        def back(z):
+            return (np.fft.ifftn(z) * M ** 3).real
+        e_t = [back(dops[d] * g_e * mk) for d in range(3)]
+        g_f = _dp3m_influence(M, L, cao, alpha, 3)[0]
+        kf = -1j * g_f * mk
+        e_f = [[back(dops[c] * dops[d] * kf) for c in range(3)] for d in range(3)]
+        wn = 2.0 * np.pi / L
+        pt = prefactor / M ** 3 * wn
+        pf = prefactor / M ** 3 * wn * wn
+        for i in range(n):
+            w = p3m_kspace(prm, pos[i:i + 1], np.ones(1), want_mesh=True)[3]
+            nz = np.nonzero(w)
+            wv = w[nz]
+            et = np.array([wv @ e_t[d][nz] for d in range(3)])
+            t[i] -= np.cross(dip[i], pt * et)
+            for d in range(3):
+                ef = np.array([wv @ e_f[d][c][nz] for c in range(3)])
+                f[i, d] += dip[i] @ (pf * ef)
     # real space
     from math import erfc
-    e_r = 0.0
-    n = len(pos)
     coeff = 2.0 * alpha / np.sqrt(np.pi)
+    a2 = alpha * alpha
     for i in range(n - 1):
         d = pos[i] - pos[i + 1:]
         d -= np.rint(d / L) * L
@@ -703,20 +733,38 @@ def dp3m_energy(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy):
         ok = (r < r_cut) & (r > 0.0)
         if not ok.any():
             continue
+        js = np.flatnonzero(ok) + i + 1
         d, r, r2 = d[ok], r[ok], r2[ok]
-        mj = dip[i + 1:][ok]
+        mj = dip[js]
+        mi = dip[i]
         ad = alpha * r
         exa = np.exp(-ad * ad)
         if accuracy > 5e-6:
-            t = 1.0 / (1.0 + 0.3275911 * ad)
-            asp = t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 +
-                                                               t * (-1.453152027 + t * 1.061405429))))
+            tt = 1.0 / (1.0 + 0.3275911 * ad)
+            asp = tt * (0.254829592 + tt * (-0.284496736 + tt * (1.421413741 +
+                                                                   tt * (-1.453152027 + tt * 1.061405429))))
             b = (asp / r + coeff) * exa / r2
         else:
             b = (np.array([erfc(x) for x in ad]) / r + coeff * exa) / r2
-        c = (3.0 * b + 2.0 * alpha * alpha * coeff * exa) / r2
-        mimj = mj @ dip[i]
-        mir = d @ dip[i]
+        common = a2 * coeff * exa
+        c = (3.0 * b + 2.0 * common) / r2
+        dcoef = (5.0 * c + 4.0 * common * a2) / r2
+        mimj = mj @ mi
+        mir = d @ mi
         mjr = np.sum(mj * d, axis=1)
-        e_r += prefactor * np.sum(mimj * b - mir * mjr * c)
-    return e_k + e_r
+        energy += prefactor * np.sum(mimj * b - mir * mjr * c)
+        if want_forces:
+            fo = prefactor * ((mimj * c)[:, None] * d + np.outer(mjr * c, mi) + mj * (mir * c)[:, None]
+                              - (mir * mjr * dcoef)[:, None] * d)
+            to = prefactor * (-np.cross(mi, mj) * b[:, None] + np.cross(mi, d) * (mjr * c)[:, None])
+            f[i] += fo.sum(axis=0)
+            t[i] += to.sum(axis=0)
+            f[js] -= fo
+            t[js] -= to + np.cross(d, fo)
+    return f, t, energy
+
+
+def dp3m_energy(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy):
+    """Dipolar P3M energy only (see dp3m)."""
+    return dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy,
+                want_forces=False)[2]

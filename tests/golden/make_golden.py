@@ -13,6 +13,9 @@ Sources (paths relative to the ESPResSo tree):
   * testsuite/python/data/coulomb_mixed_periodicity_system.data (id pos q f,
     forces from MMM2D) with the parameters and the MMM2D energy of
     testsuite/python/coulomb_mixed_periodicity.py:30-40, 84-121 (ELC)
+  * testsuite/python/data/p3m_magnetostatics_{system,expected}.data (id pos
+    dip; id force torque per unit prefactor) with the parameters, energy and
+    tolerances of testsuite/python/dipolar_mdlc_p3m_scafacos_p2nfft.py:115-152
   * known answers written in testsuite/python/electrostatic_interactions.py:81-124
     and testsuite/python/p3m_madelung.py:69-313 (parameters and constants,
     electric and magnetic)
@@ -60,6 +63,14 @@ def main():
         box=np.array([10., 10., 12.]), mesh=np.array([42, 42, 50]), r_cut=3.0,
         accuracy=1e-6, max_pw_error=1e-6, gap_size=3.0, energy=216.640984711,
         force_atol=1e-5, energy_atol=1e-4)
+
+    mg = np.genfromtxt(os.path.join(DATA, "p3m_magnetostatics_system.data"))
+    mx = np.genfromtxt(os.path.join(DATA, "p3m_magnetostatics_expected.data"))
+    np.savez_compressed(
+        os.path.join(HERE, "p3m_magnetostatics.npz"),
+        pos=mg[:, 1:4], dip=mg[:, 4:7], forces=mx[:, 1:4], torques=mx[:, 4:7],
+        box=float(np.cbrt(4 * 1000 * np.pi / (3 * 0.09))), prefactor=1.1, mesh=32,
+        accuracy=1e-6, energy=5.570, force_tol=2e-3, torque_tol=2e-3, energy_tol=1e-3)
 
     known = {
         "two_charges": {

@@ -75,3 +75,50 @@ def test_dp3m_oracle_influence_function_zeroes_and_symmetry():
     e = O.dp3m_energy(L, pos, dip, 1.0, 0.9, 3.0, M, 5, 1e-4)
     assert O.dp3m_energy(L, pos, -dip, 1.0, 0.9, 3.0, M, 5, 1e-4) == pytest.approx(e, rel=1e-12)
     assert O.dp3m_energy(L, pos + L / M, dip, 1.0, 0.9, 3.0, M, 5, 1e-4) == pytest.approx(e, rel=1e-9)
+
+
+def test_dp3m_oracle_vs_magnetostatics_golden():
+    """testsuite/python/dipolar_mdlc_p3m_scafacos_p2nfft.py:115-152: 1000
+    dipoles, prefactor 1.1, mesh 32, accuracy 1e-6: energy 5.570 x prefactor
+    to 1e-3, forces and torques to 2e-3 (sum of |error| / sqrt(N)).  cao 7,
+    alpha 0.35 and r_cut 10 stand in for the tuned values."""
+    g = np.load(os.path.join(GOLD, "p3m_magnetostatics.npz"))
+    pref = float(g["prefactor"])
+    f, t, e = O.dp3m(float(g["box"]), g["pos"], g["dip"], pref, 0.35, 10.0, int(g["mesh"]), 7,
+                     float(g["accuracy"]))
+
+    def verr(a, b):
+        return np.sum(np.linalg.norm(a - b, axis=1)) / np.sqrt(len(a))
+    assert abs(e - float(g["energy"]) * pref) < float(g["energy_tol"])
+    assert verr(f, g["forces"] * pref) < float(g["force_tol"])
+    assert verr(t, g["torques"] * pref) < float(g["torque_tol"])
+
+
+def test_dp3m_oracle_forces_torques_are_energy_derivatives():
+    """Forces are -dE/dx and torques -dE/dphi (rotation of a dipole about
+    each axis), by central differences, to the method's accuracy."""
+    rng = np.random.default_rng(9)
+    L, n = 8.0, 12
+    pos = rng.uniform(0, L, (n, 3))
+    dip = rng.normal(size=(n, 3))
+    args = (1.0, 1.2, 3.5, 32, 7, 1e-9)
+    f, t, _ = O.dp3m(L, pos, dip, *args)
+    h = 1e-5
+    for i in (0, 5):
+        for d in range(3):
+            p1, p2 = pos.copy(), pos.copy()
+            p1[i, d] += h
+            p2[i, d] -= h
+            fd = -(O.dp3m_energy(L, p1, dip, *args) - O.dp3m_energy(L, p2, dip, *args)) / (2 * h)
+            assert fd == pytest.approx(f[i, d], abs=2e-4 * np.abs(f).max())
+            axis = np.eye(3)[d]
+
+            def rot(a):
+                m = dip.copy()
+                v = m[i]
+                m[i] = (v * np.cos(a) + np.cross(axis, v) * np.sin(a) +
+                        axis * (axis @ v) * (1 - np.cos(a)))
+                return m
+            td = -(O.dp3m_energy(L, pos, rot(h), *args) -
+                   O.dp3m_energy(L, pos, rot(-h), *args)) / (2 * h)
+            assert td == pytest.approx(t[i, d], abs=2e-4 * np.abs(t).max())
