@@ -768,3 +768,76 @@ def dp3m_energy(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy):
     """Dipolar P3M energy only (see dp3m)."""
     return dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy,
                 want_forces=False)[2]
+
+
+def dlc_far_cut(box, box_h, n_magnetic, mu_max, max_pw_error):
+    """DipolarLayerCorrection::tune_far_cut (magnetostatics/dlc.cpp:416-460)
+    with g1_DLC_dip / g2_DLC_dip (:80-93): the smallest kc < 200 whose error
+    estimate is below max_pw_error; RuntimeError otherwise."""
+    lx, ly, lz = box
+    if abs(lx - ly) > 0.001:
+        raise RuntimeError("DLC tuning: box size in x direction is different from y direction."
+                           " The tuning formula requires both to be equal.")
+
+    def g1(g, x):
+        c = g / x
+        x3 = x ** 3
+        return g ** 3 / x + 1.5 * c * c + 1.5 * g / x3 + 0.75 / (x3 * x)
+
+    def g2(g, x):
+        return g * g / x + 2.0 * g / (x * x) + 2.0 / (x ** 3)
+    piarea = np.pi / (lx * ly)
+    h = box_h
+    for kc in range(1, 200):
+        gc = kc * 2.0 * np.pi / lx
+        fa0 = np.sqrt(9.0 * np.exp(2.0 * gc * h) * g1(gc, lz - h) +
+                      9.0 * np.exp(-2.0 * gc * h) * g1(gc, lz + h) + 22.0 * g1(gc, lz))
+        fa1 = np.sqrt(0.125 * piarea) * fa0
+        de = n_magnetic * mu_max ** 2 / (4.0 * (np.exp(gc * lz) - 1.0)) * (fa1 + g2(gc, lz))
+        if de < max_pw_error:
+            return float(kc)
+    raise RuntimeError("DLC tuning failed: maxPWerror too small")
+
+
+def dlc_energy_correction(box, gap_size, pos, dip, prefactor, far_cut):
+    """DLC energy correction for a metallic base solver
+    (DipolarLayerCorrection::energy_correction, dlc.cpp:356-396, with
+    dipolar_energy_correction :247-302 after Brodka): the sum over the
+    2D wave vectors |ix|, |iy| <= round(far_cut), (ix, iy) != 0, of
+    -pi / (L_x L_y) fa1 2 (S0 S2 + S1 S3) with fa1 = 1 / (g (exp(g L_z) - 1)),
+    times the prefactor, plus the shape term prefactor 2 pi / V M_z^2.
+    Positions folded; RuntimeError for a magnetic particle in the gap."""
+    box = np.asarray(box, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    dip = np.asarray(dip, dtype=np.float64)
+    pos = pos - np.floor(pos / box) * box
+    mag = np.linalg.norm(dip, axis=1) != 0.0
+    h = box[2] - gap_size
+    z = pos[:, 2]
+    bad = mag & ((z < 0.0) | (z > h))
+    if bad.any():
+        raise RuntimeError("Particle %d entered DLC gap region" % int(np.flatnonzero(bad)[0]))
+    pos, dip = pos[mag], dip[mag]
+    kc = int(np.round(far_cut))
+    fx, fy = 2.0 * np.pi / box[0], 2.0 * np.pi / box[1]
+    e = 0.0
+    for ix in range(-kc, kc + 1):
+        for iy in range(-kc, kc + 1):
+            if ix == 0 and iy == 0:
+                continue
+            gx, gy = ix * fx, iy * fy
+            gr = np.sqrt(gx * gx + gy * gy)
+            fa1 = 1.0 / (gr * (np.exp(gr * box[2]) - 1.0))
+            a = gx * dip[:, 0] + gy * dip[:, 1]
+            b = gr * dip[:, 2]
+            er = gx * pos[:, 0] + gy * pos[:, 1]
+            c, d = np.cos(er), np.sin(er)
+            f = np.exp(gr * pos[:, 2])
+            s0 = np.sum((b * c - a * d) * f)
+            s1 = np.sum((c * a + b * d) * f)
+            s2 = np.sum((-b * c - a * d) / f)
+            s3 = np.sum((c * a - b * d) / f)
+            e += fa1 * 2.0 * (s0 * s2 + s1 * s3)
+    e *= -np.pi / (box[0] * box[1])
+    vol = box[0] * box[1] * box[2]
+    return prefactor * e + prefactor * 2.0 * np.pi / vol * np.sum(dip[:, 2]) ** 2

@@ -16,6 +16,9 @@ Sources (paths relative to the ESPResSo tree):
   * testsuite/python/data/p3m_magnetostatics_{system,expected}.data (id pos
     dip; id force torque per unit prefactor) with the parameters, energy and
     tolerances of testsuite/python/dipolar_mdlc_p3m_scafacos_p2nfft.py:115-152
+  * testsuite/python/data/mdlc_reference_data_{forces_torques,energy}.dat
+    (id pos dip force torque; energy, per unit prefactor) with the DLC
+    parameters of dipolar_mdlc_p3m_scafacos_p2nfft.py:55-95
   * known answers written in testsuite/python/electrostatic_interactions.py:81-124
     and testsuite/python/p3m_madelung.py:69-313 (parameters and constants,
     electric and magnetic)
@@ -71,6 +74,15 @@ def main():
         pos=mg[:, 1:4], dip=mg[:, 4:7], forces=mx[:, 1:4], torques=mx[:, 4:7],
         box=float(np.cbrt(4 * 1000 * np.pi / (3 * 0.09))), prefactor=1.1, mesh=32,
         accuracy=1e-6, energy=5.570, force_tol=2e-3, torque_tol=2e-3, energy_tol=1e-3)
+
+    md = np.genfromtxt(os.path.join(DATA, "mdlc_reference_data_forces_torques.dat"))
+    me = float(np.genfromtxt(os.path.join(DATA, "mdlc_reference_data_energy.dat")))
+    np.savez_compressed(
+        os.path.join(HERE, "mdlc_reference.npz"),
+        pos=md[:, 1:4], dip=md[:, 4:7], forces=md[:, 7:10], torques=md[:, 10:13],
+        energy=me, box=float(np.cbrt(4 * 100 * np.pi / (3 * 0.3)) * 0.5), gap_size=2.0,
+        prefactor=1.1, mesh=32, accuracy=1e-4, max_pw_error=1e-5, energy_tol=1e-3,
+        force_tol=2e-3, torque_tol=2e-3)
 
     known = {
         "two_charges": {
