@@ -841,3 +841,62 @@ def dlc_energy_correction(box, gap_size, pos, dip, prefactor, far_cut):
     e *= -np.pi / (box[0] * box[1])
     vol = box[0] * box[1] * box[2]
     return prefactor * e + prefactor * 2.0 * np.pi / vol * np.sum(dip[:, 2]) ** 2
+
+
+def dlc_force_correction(box, gap_size, pos, dip, prefactor, far_cut):
+    """DLC force and torque corrections for a metallic base solver
+    (DipolarLayerCorrection::add_force_corrections, dlc.cpp:304-354, with
+    dipolar_force_corrections :111-245 after Brodka): per 2D wave vector the
+    particle terms S_j(+-) and their position gradients against the sums S,
+    scaled by pi / (L_x L_y) fa1 (g_x, g_y, g); torques mu x (sum), plus the
+    shape torque mu x (0, 0, -4 pi / V M_z); all times the prefactor.
+    Returns (forces, torques) for all particles (zero for non-magnetic)."""
+    box = np.asarray(box, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    dip = np.asarray(dip, dtype=np.float64)
+    n = len(pos)
+    pos = pos - np.floor(pos / box) * box
+    mag = np.linalg.norm(dip, axis=1) != 0.0
+    kc = int(np.round(far_cut))
+    fx, fy = 2.0 * np.pi / box[0], 2.0 * np.pi / box[1]
+    fs = np.zeros((n, 3))
+    ts = np.zeros((n, 3))
+    for ix in range(-kc, kc + 1):
+        for iy in range(-kc, kc + 1):
+            if ix == 0 and iy == 0:
+                continue
+            gx, gy = ix * fx, iy * fy
+            gr = np.sqrt(gx * gx + gy * gy)
+            fa1 = 1.0 / (gr * (np.exp(gr * box[2]) - 1.0))
+            a = gx * dip[:, 0] + gy * dip[:, 1]
+            b = gr * dip[:, 2]
+            er = gx * pos[:, 0] + gy * pos[:, 1]
+            c, d = np.cos(er), np.sin(er)
+            f = np.exp(gr * pos[:, 2])
+            rp = np.where(mag, (b * c - a * d) * f, 0.0)
+            ip = np.where(mag, (c * a + b * d) * f, 0.0)
+            rm = np.where(mag, (-b * c - a * d) / f, 0.0)
+            im = np.where(mag, (c * a - b * d) / f, 0.0)
+            S = (rp.sum(), ip.sum(), rm.sum(), im.sum())
+            for (xp, yp, xm, ym), acc in (((rp, ip, rm, im), fs),
+                                          ((c * f, d * f, c / f, d / f), ts)):
+                s1 = -(-xp * S[3] + yp * S[2])
+                s2 = xm * S[1] - ym * S[0]
+                s3 = -(-xm * S[1] + ym * S[0])
+                s4 = xp * S[3] - yp * S[2]
+                s1z = xp * S[2] + yp * S[3]
+                s2z = -(xm * S[0] + ym * S[1])
+                ss = np.where(mag, s1 + s2 + s3 + s4, 0.0)
+                sz = np.where(mag, 2.0 * s1z + 2.0 * s2z, 0.0)
+                acc[:, 0] += fa1 * gx * ss
+                acc[:, 1] += fa1 * gy * ss
+                acc[:, 2] += fa1 * gr * sz
+    ts = np.cross(dip, ts)
+    piarea = np.pi / (box[0] * box[1])
+    fs *= piarea
+    ts *= piarea
+    vol = box[0] * box[1] * box[2]
+    mz = np.sum(dip[mag, 2])
+    shape = np.array([0.0, 0.0, -4.0 * np.pi / vol * mz])
+    ts += np.where(mag[:, None], np.cross(dip, shape), 0.0)
+    return prefactor * fs, prefactor * ts
