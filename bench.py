@@ -8,8 +8,17 @@ r_cut 3.5 and cao 7 the error estimate of a 128^3 mesh bottoms out at
 3.9e-3 whatever alpha, so 256^3 is the smallest mesh reaching 1e-4), FP32-mixed
 mesh/FFT path.  One step = one full force evaluation (k-space + real-space
 Coulomb + LJ through the Verlet list) of the whole system; positions stay
-fixed, so the Verlet list is reused (its rebuild cost is reported apart).
-Inputs (>= 1 GB resident with the neighbour list) exceed the 126 MB L2.
+fixed, so the Verlet list is reused (its rebuild cost is measured apart:
+`verlet_rebuild_ms`).  Inputs (>= 1 GB resident with the neighbour list)
+exceed the 126 MB L2.
+
+After the headline timing (outside its timed region) the same run adds:
+`variants` -- the plain FP64 GPU path on the same workload and the batched
+512-replica Langevin step (one CUDA graph per step) -- so that the metric's
+four cells (FP32-mixed vs FP64, single vs batched) sit on one line; and
+`accuracy` -- the rms Coulomb force error of the FP32-mixed and FP64 paths
+and of the oracle's CPU P3M against the FP64 direct Ewald sum on a seeded
+20 000-ion subsample (forces from all 2^20 sources).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -61,6 +70,11 @@ def parse():
                          "skin tuning would choose)")
     ap.add_argument("--profile-only", action="store_true",
                     help="setup + a few evaluations, no JSON (for ncu captures)")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the FP64 and batched variant timings of the default run")
+    ap.add_argument("--no-ewald", action="store_true",
+                    help="skip the full-size accuracy check against the direct Ewald sum")
+    ap.add_argument("--variant-steps", type=int, default=20)
     return ap.parse_args()
 
 
@@ -203,6 +217,70 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0}}))
 
 
+def time_single_variant(lib, h, n, pos_d, q_d, t_d, f_d, stream, sp, args):
+    """ms per force evaluation of handle h on the resident inputs (CUDA
+    events on the launching stream), its stage profile and its dominant
+    stage; same step definition as the headline."""
+    import torch
+    from espresso_b200 import _lib
+    flags = _lib.P3MX_DEVICE_PTRS | _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE
+
+    def step():
+        _lib.check(lib.p3mx_forces(h, n, _lib.dptr(pos_d), _lib.dptr(q_d), _lib.dptr(t_d),
+                                   _lib.dptr(f_d), None, None, flags, sp), h)
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    k = max(args.variant_steps, 10)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1) / k
+    names = (ctypes.c_char_p * 32)()
+    ms = (ctypes.c_double * 32)()
+    nst = ctypes.c_int()
+    _lib.check(lib.p3mx_profile(h, 3, ms, names, 32, ctypes.byref(nst)), h)
+    stages = {names[j].decode(): ms[j] for j in range(nst.value)}
+    dom = max(stages, key=stages.get)
+    return {"value": n / (t_ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": t_ms,
+            "steps": k, "dtype": "f64", "stages_ms": stages,
+            "dominant_stage": {"kernel": dom, "ms": stages[dom]}}
+
+
+EWALD_SUBSAMPLE = 20000
+EWALD_PARAMS = dict(alpha=0.15, r_cut=27.0, kmax=30)
+
+
+def ewald_accuracy(pos, q, box, alpha, args, f32, f64):
+    """rms Coulomb force error on a seeded 20 000-ion subsample against the
+    FP64 direct Ewald sum over all sources (oracle.ewald_targets; real-space
+    and reciprocal truncation terms exp(-16) and exp(-24)), for the
+    FP32-mixed and FP64 GPU forces and for the oracle's CPU P3M."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    sub = np.sort(np.random.default_rng(2024).choice(len(q), min(EWALD_SUBSAMPLE, len(q)),
+                                                     replace=False))
+    if min(box, box, box) < 2 * EWALD_PARAMS["r_cut"]:
+        return {"rms_force_err_vs_ewald_20k": None, "ewald_note": "box too small"}
+    fe = O.ewald_targets([box] * 3, pos, q, sub, 1.0, **EWALD_PARAMS)
+    p = O.make_params(box, args.mesh, args.cao, alpha, args.r_cut, 1.0)
+    fk, _, _ = O.p3m_kspace(p, pos, q)
+    fr, _, _, _ = O.short_range(p, pos, q)
+    fo = (fk + fr)[sub]
+
+    def rms(a):
+        return float(np.sqrt(((a - fe) ** 2).sum(1).mean()))
+    return {"rms_force_err_vs_ewald_20k": rms(f32[sub]),
+            "rms_force_err_vs_ewald_20k_fp64": rms(f64[sub]),
+            "rms_force_err_vs_ewald_20k_oracle_cpu_p3m": rms(fo),
+            "ewald": {"subsample": int(len(sub)), "seed": 2024, **EWALD_PARAMS,
+                      "seconds": time.perf_counter() - t0}}
+
+
 def tuned_alpha(args, n, sum_q2, box):
     """alpha_L from calculate_accuracy (p3m.cpp:636-655) at fixed r_cut."""
     from math import log, sqrt
@@ -243,6 +321,15 @@ def make_replicas(n_rep, seed=0, density=0.3, nmin=1000, nmax=50000):
 def run_batched(args):
     """Batched replicas (config 4): all replicas advance by one graph launch
     per MD step (velocity Verlet + Langevin kT=1, gamma=1, dt=0.01)."""
+    print(json.dumps(batched_measure(args, args.steps, args.warmup,
+                                     cpu=not args.no_cpu_baseline, fp64=args.fp64)))
+
+
+def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
+    """Times `steps` graph-captured Langevin steps of the batched replicas
+    (CUDA events on the batch's stream) and returns the bench line as a
+    dict: value, ms_per_step, stage profile, tuning summary and (cpu=True)
+    the oracle's CPU rate on a sample of the replicas."""
     import torch
     from espresso_b200 import _lib
     P = ctypes.POINTER
@@ -257,7 +344,7 @@ def run_batched(args):
     d.offset = offs.ctypes.data_as(P(ctypes.c_longlong))
     d.accuracy = args.accuracy
     d.skin = args.skin if args.skin is not None else 0.8
-    d.single_precision = 0 if args.fp64 else 1
+    d.single_precision = 0 if fp64 else 1
     d.mesh_min, d.mesh_max, d.cao_min, d.cao_max = 16, 64, 3, 7
     tab = (_lib.PairParams * 1)()
     tab[0].wca_eps = 1.0
@@ -272,7 +359,7 @@ def run_batched(args):
     if rc:
         raise RuntimeError(lib.p3mx_batch_last_error(h).decode())
     stream = torch.cuda.ExternalStream(lib.p3mx_batch_stream(h))
-    _lib.check(lib.p3mx_batch_run(h, max(3, args.warmup), 0.01, 1.0, 1.0, 7), h,
+    _lib.check(lib.p3mx_batch_run(h, max(3, warmup), 0.01, 1.0, 1.0, 7), h,
                lib.p3mx_batch_last_error)
     lc0, lc1 = ctypes.c_longlong(), ctypes.c_longlong()
     lib.p3mx_batch_launch_count(h, ctypes.byref(lc0))
@@ -281,12 +368,12 @@ def run_batched(args):
     torch.cuda.synchronize()
     with ClockSampler(0) as clk:
         e0.record(stream)
-        _lib.check(lib.p3mx_batch_run(h, args.steps, 0.01, 1.0, 1.0, 7), h,
+        _lib.check(lib.p3mx_batch_run(h, steps, 0.01, 1.0, 1.0, 7), h,
                    lib.p3mx_batch_last_error)
         e1.record(stream)
         torch.cuda.synchronize()
     lib.p3mx_batch_launch_count(h, ctypes.byref(lc1))
-    t_ms = e0.elapsed_time(e1) / args.steps
+    t_ms = e0.elapsed_time(e1) / steps
     # stage profile of one force evaluation of the whole batch (outside the
     # timed region)
     names = (ctypes.c_char_p * 32)()
@@ -307,8 +394,8 @@ def run_batched(args):
     # full-list Verlet candidates per step: N (4/3) pi (r_cut + skin)^3 rho
     pair_cand = float((nrep * 4.18879 * (np.maximum(rcs, 2 ** (1 / 6)) + d.skin) ** 3 *
                        nrep / boxes[:, 0] ** 3).sum())
-    cpu = None
-    if not args.no_cpu_baseline:
+    cpu_line = None
+    if cpu:
         # sample: the first 8 replicas, one force evaluation each, FP64 oracle
         from oracle import oracle as O
         otab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
@@ -323,15 +410,16 @@ def run_batched(args):
             O.short_range(p, pos[sl], q[sl], None, 1, otab)
             ts += time.perf_counter() - t1
             ns += offs[r + 1] - offs[r]
-        cpu = {"value": ns / ts, "unit": "particle-steps/s", "cores": os.cpu_count(),
-               "kind": "port", "sample": "one force evaluation of each of the first 8 replicas, "
-                                         "FP64 CPU restatement (OpenMP, all host cores)"}
+        cpu_line = {"value": ns / ts, "unit": "particle-steps/s", "cores": os.cpu_count(),
+                    "kind": "port",
+                    "sample": "one force evaluation of each of the first 8 replicas, "
+                              "FP64 CPU restatement (OpenMP, all host cores)"}
     lib.p3mx_batch_destroy(h)
-    print(json.dumps({
+    return {
         "metric": METRIC.replace("single", "batched"), "value": n / (t_ms * 1e-3),
-        "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "unit": "particle-steps/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
         "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.fp64 else "f32-mixed (f64 positions/accumulators)",
+        "dtype": "f64" if fp64 else "f32-mixed (f64 positions/accumulators)",
         "data": "synthetic",
         "config": {"workload": f"batched: {len(prefs)} cubic replicas, N log-uniform "
                                f"[1e3, 5e4] (total {n}), density 0.3, +/-1 or +/-2 ions, "
@@ -343,8 +431,9 @@ def run_batched(args):
                    "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max()),
                    "r_cut_range": [float(rcs.min()), float(rcs.max())],
                    "verlet_candidates_per_step_est": pair_cand},
-        "stages_ms": stages, "cpu_baseline": cpu, "clocks": clk.summary(),
-        "gpu_launches": int(lc1.value - lc0.value)}))
+        "stages_ms": stages, "cpu_baseline": cpu_line,
+        "clocks": clk.summary() if clocks else None,
+        "gpu_launches": int(lc1.value - lc0.value)}
 
 
 def run_elc(args):
@@ -593,10 +682,23 @@ def main():
         t_e2e = float(tt.item())
     e2e = n * world / t_e2e
 
+    # Verlet rebuild at the headline size: a resort makes the next force
+    # evaluation rebuild the cell and Verlet lists; the stage profile times
+    # the rebuild between CUDA events (outside the timed region)
+    _lib.check(lib.p3mx_resort(h), h)
+    names_r = (ctypes.c_char_p * 32)()
+    ms_r = (ctypes.c_double * 32)()
+    nst_r = ctypes.c_int()
+    _lib.check(lib.p3mx_profile(h, 1, ms_r, names_r, 32, ctypes.byref(nst_r)), h)
+    prof_r = {names_r[k].decode(): ms_r[k] for k in range(nst_r.value)}
+    verlet_rebuild_ms = prof_r.get("sr_rebuild")
+
     # FP32-mixed vs FP64 electrostatic forces (k-space + real-space Coulomb,
     # LJ switched off on both actors) on the same configuration
     fp_diff = None
     f_rms = None
+    ewald_acc = None
+    variants = {}
     if not args.fp64:
         zero_tab = (_lib.PairParams * 1)()
         ref_act = P3M(prefactor=1.0, accuracy=args.accuracy, mesh=args.mesh, cao=args.cao,
@@ -612,6 +714,14 @@ def main():
             res.append(ff)
         fp_diff = float(np.sqrt(((res[0] - res[1]) ** 2).sum(1).mean()))
         f_rms = float(np.sqrt((res[1] ** 2).sum(1).mean()))
+        if rank == 0 and not args.no_ewald:
+            ewald_acc = ewald_accuracy(pos, q, box, prm["alpha"], args, res[0], res[1])
+        if rank == 0 and not args.no_variants:
+            # plain FP64 GPU path on the same workload (LJ back on)
+            s._sync_pairs(ref_act._handle, types)
+            s._sync_pairs(h, types)
+            variants["fp64_single"] = time_single_variant(
+                lib, ref_act._handle, n, pos_d, q_d, t_d, f_d, stream, sp, args)
         del ref_act
 
     if rank != 0:
@@ -658,6 +768,22 @@ def main():
                "sample": "one full force evaluation of the same workload on the FP64 CPU "
                          "restatement of the reference path (OpenMP, all host cores)"}
     n_launch = lc1.value - lc0.value
+    if not args.no_variants and not args.fp64 and world == 1:
+        # the 512-replica batched step (config 4), after the single-system
+        # engines' work is done
+        del act
+        s.electrostatics.clear()
+        torch.cuda.synchronize(dev)
+        try:
+            b = batched_measure(args, max(args.variant_steps, 20), 3, cpu=False, clocks=True)
+            variants["batched_f32_mixed"] = {
+                k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "stages_ms", "config",
+                                  "clocks", "gpu_launches")}
+            sb = b["stages_ms"]
+            dom_b = max(sb, key=sb.get)
+            variants["batched_f32_mixed"]["dominant_stage"] = {"kernel": dom_b, "ms": sb[dom_b]}
+        except Exception as exc:  # reported, not hidden
+            variants["batched_f32_mixed"] = {"error": str(exc)}
     out = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
@@ -683,7 +809,9 @@ def main():
                     "energy/virial sums and the packed field-mesh output"},
         "accuracy": {"rms_force_err_estimate": prm["accuracy"],
                      "fp32_vs_fp64_rms_coulomb_force_diff": fp_diff,
-                     "rms_coulomb_force": f_rms},
+                     "rms_coulomb_force": f_rms, **(ewald_acc or {})},
+        "verlet_rebuild_ms": verlet_rebuild_ms,
+        "variants": variants or None,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(n_launch),

@@ -1325,6 +1325,15 @@ int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names, int c
   });
 }
 
+int p3mx_resort(p3mx_handle *h) {
+  return guarded(h, [&] {
+    if (h->eng)
+      h->eng->invalidate_lists();
+    if (h->eng64)
+      h->eng64->invalidate_lists();
+  });
+}
+
 int p3mx_launch_count(const p3mx_handle *h, long long *count) {
   if (!h || !count)
     return P3MX_EHANDLE;

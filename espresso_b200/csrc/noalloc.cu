@@ -21,7 +21,12 @@
 //    at the same time) race on the array: serialise them;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture on the device.
+//    before any stream capture on the device.  The address is kept for the
+//    life of the process: a cudaDeviceReset (or any teardown of the primary
+//    context) makes it stale, so the entry point must not be called again
+//    after one;
+//  * each call waits for its result (device-to-host copy of one double and a
+//    stream synchronisation).
 #include "../../include/p3mx.h"
 #include "p3m_kernels.cuh"
 

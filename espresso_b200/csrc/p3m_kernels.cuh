@@ -478,6 +478,350 @@ k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Owner-computes charge assignment (AssignCharges, p3m.cpp:225-265;
+// charge_assign, p3m.cpp:283-330): the mesh is cut into owner blocks of
+// kOwnEdge^3 points and one CTA computes every point of its block and
+// stores it once -- no mesh memset, no read-add-write, no colours.  The
+// CTA visits the particles whose stencils reach its block: their corners
+// lie within P-1 points below the block or inside it, i.e. in a few
+// columns of the corner sort's bricks (contiguous ranges of the brick-major
+// order).  For each particle one warp covers the P^2 (x, y) stencil rows
+// (one row per lane, the P z points of a row unrolled) and adds the points
+// that fall into the block, in fixed point, into a shared-memory tile of
+// the block alone.
+//
+// Fixed point: a term v = q wx wy wz becomes t = rint(v S) by one FMA with a
+// magic constant (1.5 * 2^23 in FP32, 1.5 * 2^52 in FP64: the sum's bits
+// minus the constant's are t exactly while |t| < 2^22 / 2^51) and is added
+// with an integer atomic (32-bit words for the FP32-mixed path, 64-bit for
+// FP64).  S is a power of two with qmax wmax^3 S < 2^22 (2^51) and
+// n qmax wmax^3 S < 2^31 (2^62), n the particles the block visits, qmax
+// the replica's largest |q| and wmax the largest B-spline weight of order
+// P, so no term leaves the exact range and no point's final sum overflows
+// (intermediate wrap-around of two's complement sums cancels).  Integer
+// sums do not depend on the order of the atomics: the mesh is bitwise
+// reproducible.  The quantum is 2^-es of a charge with
+// es = min(22 - e(qmax wmax^3), 31 - e(n qmax wmax^3)), about 2^-24 at
+// 2^20 ions on a 256^3 mesh (FP32-mixed) and 2^-54 in FP64.
+constexpr int kOwnEdge = 16;  // owned mesh points per dimension (multiple of 4 and 8)
+constexpr int kOwnWarps = 8;  // warps per owner block
+constexpr int kOwnChunk = 128; // particles whose records are staged at a time
+constexpr int kOwnSkip = -1;   // staged particle whose stencil misses the block
+
+// Largest cardinal B-spline weight of order P over dist in [-1/2, 1/2],
+// rounded up (1, 1, 3/4, 2/3, 115/192, 11/20, 0.51102...).
+template <int P> __host__ __device__ constexpr double bspline_wmax() {
+  return P <= 2 ? 1.0 : P == 3 ? 0.7501 : P == 4 ? 0.6668 : P == 5 ? 0.5991 : P == 6 ? 0.5501 : 0.5112;
+}
+
+template <typename Real> struct OwnWord;
+template <> struct OwnWord<float> {
+  using type = int;
+  static constexpr int term_bits = 22;
+  static constexpr int sum_bits = 31;
+};
+template <> struct OwnWord<double> {
+  using type = unsigned long long;
+  static constexpr int term_bits = 51;
+  static constexpr int sum_bits = 62;
+};
+__device__ inline int own_fixed(float a, float b) {
+  return __float_as_int(fmaf(a, b, 12582912.0f)) - 0x4B400000;
+}
+__device__ inline unsigned long long own_fixed(double a, double b) {
+  return static_cast<unsigned long long>(__double_as_longlong(fma(a, b, 6755399441055744.0))) -
+         0x4338000000000000ull;
+}
+__device__ inline float own_value(int v, float inv_s) { return static_cast<float>(v) * inv_s; }
+__device__ inline double own_value(unsigned long long v, double inv_s) {
+  return static_cast<double>(static_cast<long long>(v)) * inv_s;
+}
+
+// Strides of the owner tile [x][y][z] (z contiguous, words of WB bytes):
+// the smallest y stride >= kOwnEdge and x stride >= kOwnEdge * (y stride)
+// for which the lanes of one shared-memory wavefront (128 bytes: 32 lanes of
+// 4-byte words, 16 of 8-byte words), one (x, y) stencil row each (row
+// r = lane + 32 q, x = r / P, y = r % P), hit distinct banks.
+template <int P, int WB> __host__ __device__ constexpr TileStrides own_strides() {
+  constexpr int E = kOwnEdge;
+  constexpr int L = 128 / WB;
+  for (int sy = E; sy < E + L; ++sy)
+    for (int sx = E * sy; sx < E * sy + 2 * L; ++sx) {
+      bool ok = true;
+      for (int r0 = 0; r0 < P * P && ok; r0 += L) {
+        unsigned long long used = 0;
+        for (int r = r0; r < r0 + L && r < P * P; ++r) {
+          unsigned long long const bit = 1ull << (((r / P) * sx + (r % P) * sy) % L);
+          if (used & bit) {
+            ok = false;
+            break;
+          }
+          used |= bit;
+        }
+      }
+      if (ok)
+        return TileStrides{sy, sx};
+    }
+  return TileStrides{E, E * E};
+}
+template <typename Real, int P> __host__ __device__ constexpr size_t own_tile_bytes() {
+  using W = typename OwnWord<Real>::type;
+  return (sizeof(W) * kOwnEdge * static_cast<size_t>(own_strides<P, sizeof(W)>().sx) + 15) / 16 *
+         16;
+}
+template <typename Real, int P> __host__ __device__ constexpr size_t own_smem() {
+  return own_tile_bytes<Real, P>() + sizeof(Real) * kOwnChunk * wstride<P, 4>() +
+         sizeof(int) * kOwnChunk;
+}
+
+// Sort bricks (per dimension) whose corners can reach the owned points
+// [o, o + ext): corners in [o - (P-1), o + ext), bricks first .. first+cnt-1
+// modulo nb (all nb when the span covers the axis).
+__device__ inline void own_brick_span(int o, int ext, int P, int B, int nb, int &first,
+                                      int &cnt) {
+  int const lo = o - (P - 1);
+  first = (lo >= 0) ? lo / B : -((-lo + B - 1) / B);
+  int const last = (o + ext - 1) / B;
+  cnt = last - first + 1;
+  if (cnt >= nb) {
+    first = 0;
+    cnt = nb;
+  }
+}
+
+template <typename Real, int P>
+__global__ void __launch_bounds__(32 * kOwnWarps)
+k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owners,
+                 const int *__restrict__ start, const Real *__restrict__ W,
+                 const int *__restrict__ s_key, const unsigned *__restrict__ qmax_bits,
+                 Real *__restrict__ rho, int *__restrict__ err) {
+  using Word = typename OwnWord<Real>::type;
+  constexpr int R = 4;
+  constexpr int WS = wstride<P, R>();
+  constexpr int WZ = wz_off<P, R>();
+  constexpr int P2 = P * P;
+  constexpr int NQ = (P2 + 31) / 32;
+  constexpr int NT = 32 * kOwnWarps;
+  constexpr int E = kOwnEdge;
+  constexpr int B = brick_edge<P>(), B3 = B * B * B;
+  constexpr int LB = (B == 4) ? 2 : 3;
+  constexpr TileStrides TS = own_strides<P, sizeof(Word)>();
+  constexpr int SY = TS.sy, SX = TS.sx;
+  constexpr int TW = static_cast<int>(own_tile_bytes<Real, P>() / sizeof(Word));
+  constexpr int CH = kOwnChunk;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long bar;
+  Word *tile = reinterpret_cast<Word *>(smem_raw);
+  Real *rec = reinterpret_cast<Real *>(smem_raw + own_tile_bytes<Real, P>());
+  int *roff = reinterpret_cast<int *>(rec + CH * WS);
+  int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  int2 const ow = owners[blockIdx.x];
+  RepGeom const &G = reps[ow.x];
+  int const M[3] = {G.mesh[0], G.mesh[1], G.mesh[2]};
+  int const no1 = (M[1] + E - 1) / E, no2 = (M[2] + E - 1) / E;
+  int const o[3] = {(ow.y / (no1 * no2)) * E, ((ow.y / no2) % no1) * E, (ow.y % no2) * E};
+  int const ext[3] = {min(E, M[0] - o[0]), min(E, M[1] - o[1]), min(E, M[2] - o[2])};
+  int const nb[3] = {G.nbx, G.nby, G.nbz};
+  // fast geometry: a stencil meets the owned interval at most once per axis
+  bool const fast = (M[0] >= ext[0] + P - 1) && (M[1] >= ext[1] + P - 1) &&
+                    (M[2] >= ext[2] + P - 1);
+  int bf[3], bc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    own_brick_span(o[d], ext[d], P, B, nb[d], bf[d], bc[d]);
+  auto wrapb = [](int v, int n) { return ((v % n) + n) % n; };
+  const int *st = start + G.brk_off;
+  // the particles of the visited bricks: (x, y) brick columns, each with at
+  // most two contiguous z runs
+  auto for_runs = [&](auto &&fn) {
+    int const z0 = wrapb(bf[2], nb[2]);
+    int const z1 = min(z0 + bc[2], nb[2]);
+    int const z2 = z0 + bc[2] - nb[2]; // > 0: second run [0, z2)
+    for (int ix = 0; ix < bc[0]; ++ix) {
+      int const bx = wrapb(bf[0] + ix, nb[0]);
+      for (int iy = 0; iy < bc[1]; ++iy) {
+        int const by = wrapb(bf[1] + iy, nb[1]);
+        int const col = (bx * nb[1] + by) * nb[2];
+        fn(bx, by, z0, st[col + z0], st[col + z1]);
+        if (z2 > 0)
+          fn(bx, by, 0, st[col], st[col + z2]);
+      }
+    }
+  };
+  long long count = 0;
+  for_runs([&](int, int, int, int s0, int s1) { count += s1 - s0; });
+  float const qmax = __uint_as_float(qmax_bits[ow.x]);
+  // zero the tile; initialise the staging barrier
+  for (int t = tid; t < TW; t += NT)
+    tile[t] = Word(0);
+  if (tid == 0)
+    mbar_init(&bar, 1);
+  __syncthreads();
+  int es = 0;
+  bool const any = (count > 0) && (qmax > 0.0f);
+  if (any) {
+    double const unit = static_cast<double>(qmax) * bspline_wmax<P>() * bspline_wmax<P>() *
+                        bspline_wmax<P>();
+    int e1, e2;
+    frexp(unit, &e1);
+    frexp(unit * static_cast<double>(count), &e2);
+    es = min(OwnWord<Real>::term_bits - e1, OwnWord<Real>::sum_bits - e2);
+    es = max(min(es, 1000), -1000);
+  }
+  Real const S = static_cast<Real>(ldexp(1.0, es));
+  // per-lane (x, y) stencil row of each round
+  int qx[NQ], qy[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    int const r = lane + 32 * q;
+    int const rr = (r < P2) ? r : 0;
+    qx[q] = rr / P;
+    qy[q] = rr % P;
+  }
+  unsigned parity = 0;
+  bool ok = true;
+  if (any) {
+    for_runs([&](int bx, int by, int bz0, int s0, int s1) {
+      if (!ok)
+        return;
+      int const b0 = (bx * nb[1] + by) * nb[2] + bz0;
+      for (int c0 = s0; c0 < s1 && ok; c0 += CH) {
+        int const cn = min(CH, s1 - c0);
+        __syncthreads(); // the previous chunk is consumed
+        if (tid == 0) {
+          unsigned const nbytes = static_cast<unsigned>(cn * WS * sizeof(Real));
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive_expect_tx(&bar, nbytes);
+          bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
+        }
+        for (int j = tid; j < cn; j += NT) {
+          int const sk = s_key[c0 + j];
+          int const bz = bz0 + ((sk >> (3 * LB)) - b0);
+          int const l = sk & (B3 - 1);
+          int const g[3] = {bx * B + (l >> (2 * LB)), by * B + ((l >> LB) & (B - 1)),
+                            bz * B + (l & (B - 1))};
+          int pk;
+          if (fast) {
+            bool hit = true;
+            int dd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              int v = g[d] - o[d];
+              if (v < 0)
+                v += M[d];
+              if (v > M[d] - P)
+                v -= M[d];
+              dd[d] = v;
+              hit = hit && (v < ext[d]);
+            }
+            pk = hit ? (((dd[0] + 128) << 16) | ((dd[1] + 128) << 8) | (dd[2] + 128)) : kOwnSkip;
+          } else {
+            pk = (g[0] << 20) | (g[1] << 10) | g[2];
+          }
+          roff[j] = pk;
+        }
+        bool const got = mbar_wait(&bar, parity);
+        parity ^= 1u;
+        if (__syncthreads_or(!got)) {
+          if (tid == 0) {
+            atomicExch(err, 1);
+            mbar_wait(&bar, parity ^ 1u); // bounded wait for the copy in flight
+          }
+          ok = false;
+          return;
+        }
+        for (int j = warp; j < cn; j += kOwnWarps) {
+          int const pk = roff[j];
+          if (pk == kOwnSkip)
+            continue;
+          const Real *w = rec + j * WS;
+          Real wz[P];
+#pragma unroll
+          for (int k = 0; k < P; ++k)
+            wz[k] = w[WZ + k];
+          if (fast) {
+            int const dx = ((pk >> 16) & 255) - 128, dy = ((pk >> 8) & 255) - 128,
+                      dz = (pk & 255) - 128;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+              int const x = dx + qx[q], y = dy + qy[q];
+              if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(ext[0]) &&
+                  static_cast<unsigned>(y) < static_cast<unsigned>(ext[1])) {
+                Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
+                Word *pt = tile + x * SX + y * SY + dz;
+#pragma unroll
+                for (int k = 0; k < P; ++k)
+                  if (static_cast<unsigned>(dz + k) < static_cast<unsigned>(ext[2]))
+                    atomicAdd(pt + k, own_fixed(wxy, wz[k]));
+              }
+            }
+          } else {
+            // small meshes: every stencil point wrapped and tested on its own
+            int const gx = (pk >> 20) & 1023, gy = (pk >> 10) & 1023, gz = pk & 1023;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+              int x = gx + qx[q], y = gy + qy[q];
+              if (x >= M[0])
+                x -= M[0];
+              if (y >= M[1])
+                y -= M[1];
+              x -= o[0];
+              y -= o[1];
+              if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(ext[0]) &&
+                  static_cast<unsigned>(y) < static_cast<unsigned>(ext[1])) {
+                Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
+                Word *pt = tile + x * SX + y * SY;
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                  int z = gz + k;
+                  if (z >= M[2])
+                    z -= M[2];
+                  z -= o[2];
+                  if (static_cast<unsigned>(z) < static_cast<unsigned>(ext[2]))
+                    atomicAdd(pt + z, own_fixed(wxy, wz[k]));
+                }
+              }
+            }
+          }
+        }
+      }
+    });
+  }
+  if (!ok)
+    return;
+  __syncthreads();
+  // store the owned points once (zeros for a block no charge reaches)
+  Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
+  Real *mesh = rho + G.rm_off;
+  if (ext[0] == E && ext[1] == E && ext[2] == E && (M[2] % 4) == 0 && (G.rm_off % 4) == 0) {
+    // four consecutive z points per thread and iteration, one vector store
+    for (int t = tid; t < E * E * (E / 4); t += NT) {
+      int const z4 = (t & 3) * 4, y = (t >> 2) & (E - 1), x = t >> 6;
+      const Word *tp = tile + x * SX + y * SY + z4;
+      Real *mp = mesh + (static_cast<long long>(o[0] + x) * M[1] + (o[1] + y)) * M[2] + o[2] + z4;
+      Real v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        v[k] = own_value(tp[k], inv_S);
+      if constexpr (sizeof(Real) == 4) {
+        *reinterpret_cast<float4 *>(mp) = make_float4(v[0], v[1], v[2], v[3]);
+      } else {
+        reinterpret_cast<double2 *>(mp)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(mp)[1] = make_double2(v[2], v[3]);
+      }
+    }
+  } else {
+    int const nyz = ext[1] * ext[2];
+    for (int t = tid; t < ext[0] * nyz; t += NT) {
+      int const x = t / nyz, yz = t - x * nyz, y = yz / ext[2], z = yz - y * ext[2];
+      mesh[(static_cast<long long>(o[0] + x) * M[1] + (o[1] + y)) * M[2] + o[2] + z] =
+          own_value(tile[x * SX + y * SY + z], inv_S);
+    }
+  }
+}
+
 // Force back-interpolation (AssignForces, electrostatics/p3m.cpp:344-373) as
 // a warp-specialised pipeline over bricks.  Each block takes the bricks
 // blockIdx.x, blockIdx.x + gridDim.x, ... (a persistent grid); its warp 0

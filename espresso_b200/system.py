@@ -21,12 +21,27 @@ from .interactions import BondedInteractions
 
 
 class CellSystem:
-    def __init__(self):
+    def __init__(self, system=None):
         self.skin = 0.4
         self.use_verlet_lists = True
+        self._system = system
 
     def set_regular_decomposition(self, use_verlet_lists=True):
         self.use_verlet_lists = use_verlet_lists
+
+    def resort(self):
+        """Rebuild the cell and Verlet lists at the next force calculation
+        (CellSystem.resort() of the reference, cell_system.py; the next
+        step rebuilds as after CellStructure::set_resort_particles)."""
+        s = self._system
+        if s is None:
+            return
+        handles = [getattr(a, "_handle", None) for a in (s.electrostatics.solver, s._sr_handle)
+                   if a is not None]
+        lib = _lib.load()
+        for h in handles:
+            if h:
+                _lib.check(lib.p3mx_resort(h), h)
 
 
 class _PairIA:
@@ -305,7 +320,7 @@ class System:
         self._box_l = np.array(np.broadcast_to(box_l, (3,)), dtype=float)
         self.periodicity = (True, True, True)
         self.time_step = None
-        self.cell_system = CellSystem()
+        self.cell_system = CellSystem(self)
         self._sr_handle = None
         self._pairs_dirty = True
         self._bond_version = 0

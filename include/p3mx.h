@@ -235,6 +235,11 @@ int p3mx_copy_mesh(p3mx_handle *h, double *out, size_t cap);
  * elc_forces. */
 int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names,
                  int cap, int *nstages);
+/* Forces a rebuild of the cell lists and Verlet lists at the next force
+ * evaluation, as CellSystem.resort() does in the reference
+ * (CellStructure::set_resort_particles(Cells::RESORT_GLOBAL),
+ * CellStructure.hpp:393-401 makes the next step rebuild). */
+int p3mx_resort(p3mx_handle *h);
 /* Total number of kernels launched by the handle's engines so far. */
 int p3mx_launch_count(const p3mx_handle *h, long long *count);
 
@@ -253,9 +258,13 @@ int p3mx_error_estimate(const int *mesh, int cao, int n_c_part,
  * fixed 32 KiB device array inside the library (held on every GPU that loads
  * it until exit): meshes above 4096*16384 points are rejected with
  * P3MX_EDOMAIN and a message in errbuf.  The first call on a device looks up
- * the array's address (make it before any stream capture); all calls share
- * the array, so calls that overlap on the GPU race.  stream: cudaStream_t or
- * NULL; errbuf/errbuf_len may be NULL/0. */
+ * the array's address (make it before any stream capture) and keeps it for
+ * the life of the process: after cudaDeviceReset, or any teardown of the
+ * device's primary context, that address is stale and the entry point must
+ * not be called again in the process.  All calls share the array, so calls
+ * that overlap on the GPU race.  Each call returns only when its result is
+ * on the host (it synchronises the stream).  stream: cudaStream_t or NULL;
+ * errbuf/errbuf_len may be NULL/0. */
 int p3mx_error_estimate_noalloc(const int *mesh, int cao, int n_c_part,
                                 double sum_q2, double alpha_L, double r_cut_iL,
                                 const double *box, double prefactor,

@@ -81,6 +81,13 @@ int oracle_ewald(const double *box, long n, const double *pos, const double *q,
                  double prefactor, double alpha, double r_cut, int kmax,
                  double epsilon, double *f, double *energy);
 
+/* Direct FP64 Ewald forces (metallic) on the nt particles tidx[] from all n
+ * sources: cell-list real space, structure-factor reciprocal space.  Forces
+ * written to f (3 nt).  Returns 0, or nonzero for r_cut > L/2 or a bad index. */
+int oracle_ewald_targets(const double *box, long n, const double *pos, const double *q,
+                         long nt, const long *tidx, double prefactor, double alpha,
+                         double r_cut, int kmax, double *f);
+
 /* Math restatements, exported for comparison with the reference headers. */
 double oracle_bspline(int order, int i, double x);
 double oracle_as_erfc_part(double d);

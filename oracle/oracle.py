@@ -64,6 +64,9 @@ def _load():
     lib.oracle_ewald.argtypes = [dp, ctypes.c_long, dp, dp, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                  ctypes.c_double, dp, dp]
+    lib.oracle_ewald_targets.argtypes = [dp, ctypes.c_long, dp, dp, ctypes.c_long, lp,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, dp]
     for name in ("oracle_bspline", "oracle_as_erfc_part", "oracle_sinc",
                  "oracle_cotangent_sum"):
         getattr(lib, name).restype = ctypes.c_double
@@ -231,6 +234,22 @@ def ewald(box, pos, q, prefactor, alpha, r_cut, kmax, epsilon=0.0):
     lib.oracle_ewald(_d(box), len(q), _d(pos), _d(q), prefactor, alpha, r_cut,
                      int(kmax), epsilon, _d(f), _d(e))
     return f, e[0]
+
+
+def ewald_targets(box, pos, q, targets, prefactor, alpha, r_cut, kmax):
+    """Direct FP64 Ewald forces (metallic) on the particles `targets` from
+    all sources; the real-space cutoff must not exceed half the box."""
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    f = np.zeros((len(t), 3))
+    rc = lib.oracle_ewald_targets(_d(box), len(q), _d(pos), _d(q), len(t),
+                                  t.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                  prefactor, alpha, r_cut, int(kmax), _d(f))
+    if rc:
+        raise ValueError(f"oracle_ewald_targets failed ({rc})")
+    return f
 
 
 BOND_FENE = 1

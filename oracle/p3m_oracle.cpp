@@ -1051,4 +1051,217 @@ int oracle_ewald(const double *box, long n, const double *pos, const double *q,
   return 0;
 }
 
+
+/* Direct FP64 Ewald forces on a subsample of targets from ALL n sources
+ * (metallic boundary), for error measurements on systems too large for the
+ * all-pairs sum.  Real space: exact erfc over a cell list of the sources
+ * (minimum image, r_cut <= min(L)/2).  Reciprocal space: structure factor
+ * S(k) = sum_j q_j exp(i k.r_j) over |n| <= kmax (half space, doubled), the
+ * phases built per source from the three axis phases exp(i 2 pi n x / L) by
+ * repeated multiplication (one complex product per k vector and source),
+ * summed per thread and then added over threads in thread order.  Forces
+ * are written (not added) to f (3 nt). */
+int oracle_ewald_targets(const double *box, long n, const double *pos, const double *q,
+                         long nt, const long *tidx, double prefactor, double alpha,
+                         double r_cut, int kmax, double *f) {
+  double const V = box[0] * box[1] * box[2];
+  for (int d = 0; d < 3; ++d)
+    if (!(r_cut <= 0.5 * box[d]))
+      return 1;
+  for (long t = 0; t < nt; ++t)
+    if (tidx[t] < 0 || tidx[t] >= n)
+      return 2;
+  // cell list of the sources: cells of edge >= r_cut / 4
+  int nc[3];
+  double cs[3];
+  for (int d = 0; d < 3; ++d) {
+    nc[d] = std::max(1, static_cast<int>(std::floor(box[d] / (0.25 * r_cut))));
+    nc[d] = std::min(nc[d], 256);
+    cs[d] = box[d] / nc[d];
+  }
+  long const ncell = static_cast<long>(nc[0]) * nc[1] * nc[2];
+  auto fold = [&](double x, int d) {
+    double y = x - std::floor(x / box[d]) * box[d];
+    return (y >= box[d]) ? 0.0 : y;
+  };
+  std::vector<long> cstart(ncell + 1, 0), order(n);
+  std::vector<int> cell_of(n);
+  for (long j = 0; j < n; ++j) {
+    int c[3];
+    for (int d = 0; d < 3; ++d)
+      c[d] = std::min(nc[d] - 1, static_cast<int>(fold(pos[3 * j + d], d) / cs[d]));
+    cell_of[j] = (c[0] * nc[1] + c[1]) * nc[2] + c[2];
+    ++cstart[cell_of[j] + 1];
+  }
+  for (long c = 0; c < ncell; ++c)
+    cstart[c + 1] += cstart[c];
+  {
+    std::vector<long> fill(cstart.begin(), cstart.end() - 1);
+    for (long j = 0; j < n; ++j)
+      order[fill[cell_of[j]]++] = j;
+  }
+  int reach[3];
+  for (int d = 0; d < 3; ++d)
+    reach[d] = std::min(static_cast<int>(std::ceil(r_cut / cs[d])), (nc[d] - 1) / 2);
+  double const two_a_sqrt_pi_i = 2.0 * alpha / std::sqrt(PI);
+  double const rc2 = r_cut * r_cut;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long t = 0; t < nt; ++t) {
+    long const i = tidx[t];
+    double xi[3];
+    int ci[3];
+    for (int d = 0; d < 3; ++d) {
+      xi[d] = pos[3 * i + d];
+      ci[d] = std::min(nc[d] - 1, static_cast<int>(fold(xi[d], d) / cs[d]));
+    }
+    double fi[3] = {0, 0, 0};
+    // every cell within reach, each visited once even when the reach
+    // covers the whole axis
+    for (int ox = -reach[0]; ox <= reach[0]; ++ox)
+      for (int oy = -reach[1]; oy <= reach[1]; ++oy)
+        for (int oz = -reach[2]; oz <= reach[2]; ++oz) {
+          int const cx = ((ci[0] + ox) % nc[0] + nc[0]) % nc[0];
+          int const cy = ((ci[1] + oy) % nc[1] + nc[1]) % nc[1];
+          int const cz = ((ci[2] + oz) % nc[2] + nc[2]) % nc[2];
+          long const c = (static_cast<long>(cx) * nc[1] + cy) * nc[2] + cz;
+          for (long s = cstart[c]; s < cstart[c + 1]; ++s) {
+            long const j = order[s];
+            if (j == i)
+              continue;
+            double dv[3], d2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+              double dx = xi[d] - pos[3 * j + d];
+              dx -= std::round(dx / box[d]) * box[d];
+              dv[d] = dx;
+              d2 += dx * dx;
+            }
+            if (d2 >= rc2)
+              continue;
+            double const r = std::sqrt(d2);
+            double const fac =
+                q[j] * (std::erfc(alpha * r) / r + two_a_sqrt_pi_i * std::exp(-alpha * alpha * d2)) / d2;
+            for (int d = 0; d < 3; ++d)
+              fi[d] += fac * dv[d];
+          }
+        }
+    for (int d = 0; d < 3; ++d)
+      f[3 * t + d] = prefactor * q[i] * fi[d];
+  }
+  // reciprocal space: k vectors of the half space nx > 0, or nx = 0 and
+  // (ny > 0 or ny = 0 and nz > 0), |n| <= kmax; for each (nx, ny) the nz run
+  // [nz0, nz1] is contiguous
+  struct Run {
+    int nx, ny, nz0, nz1;
+    long k0;
+  };
+  std::vector<Run> runs;
+  long nk = 0;
+  for (int nx = 0; nx <= kmax; ++nx)
+    for (int ny = -kmax; ny <= kmax; ++ny) {
+      int const rem = kmax * kmax - nx * nx - ny * ny;
+      if (rem < 0 || (nx == 0 && ny < 0))
+        continue;
+      int const zm = static_cast<int>(std::floor(std::sqrt(static_cast<double>(rem)) + 1e-12));
+      int const z0 = (nx == 0 && ny == 0) ? 1 : -zm;
+      if (z0 > zm)
+        continue;
+      runs.push_back(Run{nx, ny, z0, zm, nk});
+      nk += zm - z0 + 1;
+    }
+  std::vector<double> A(nk);
+  for (auto const &rn : runs)
+    for (int nz = rn.nz0; nz <= rn.nz1; ++nz) {
+      double const kx = 2.0 * PI * rn.nx / box[0], ky = 2.0 * PI * rn.ny / box[1],
+                   kz = 2.0 * PI * nz / box[2];
+      double const k2 = kx * kx + ky * ky + kz * kz;
+      A[rn.k0 + nz - rn.nz0] = std::exp(-k2 / (4.0 * alpha * alpha)) / k2;
+    }
+  int nthr = 1;
+#ifdef _OPENMP
+  nthr = omp_get_max_threads();
+#endif
+  std::vector<double> Sr_t(static_cast<size_t>(nthr) * nk, 0.0), Si_t(static_cast<size_t>(nthr) * nk, 0.0);
+  int const W = 2 * kmax + 1;
+  // axis phases of one particle: px[n] (n = 0..kmax), py/pz[n + kmax] (n = -kmax..kmax)
+  auto axis_phases = [&](const double *x, std::vector<cd> &px, std::vector<cd> &py,
+                         std::vector<cd> &pz) {
+    cd const ux = std::polar(1.0, 2.0 * PI * x[0] / box[0]);
+    cd const uy = std::polar(1.0, 2.0 * PI * x[1] / box[1]);
+    cd const uz = std::polar(1.0, 2.0 * PI * x[2] / box[2]);
+    px[0] = 1.0;
+    py[kmax] = 1.0;
+    pz[kmax] = 1.0;
+    for (int m = 1; m <= kmax; ++m) {
+      px[m] = px[m - 1] * ux;
+      py[kmax + m] = py[kmax + m - 1] * uy;
+      pz[kmax + m] = pz[kmax + m - 1] * uz;
+      py[kmax - m] = std::conj(py[kmax + m]);
+      pz[kmax - m] = std::conj(pz[kmax + m]);
+    }
+  };
+#pragma omp parallel
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double *sr = Sr_t.data() + static_cast<size_t>(tid) * nk;
+    double *si = Si_t.data() + static_cast<size_t>(tid) * nk;
+    std::vector<cd> px(kmax + 1), py(W), pz(W);
+    std::vector<double> zr(W), zi(W);
+#pragma omp for schedule(static)
+    for (long j = 0; j < n; ++j) {
+      axis_phases(pos + 3 * j, px, py, pz);
+      for (int m = 0; m < W; ++m) {
+        zr[m] = pz[m].real();
+        zi[m] = pz[m].imag();
+      }
+      double const qj = q[j];
+      for (auto const &rn : runs) {
+        cd const exy = qj * px[rn.nx] * py[kmax + rn.ny];
+        double const ar = exy.real(), ai = exy.imag();
+        double *srk = sr + rn.k0 - rn.nz0;
+        double *sik = si + rn.k0 - rn.nz0;
+        for (int nz = rn.nz0; nz <= rn.nz1; ++nz) {
+          double const br = zr[kmax + nz], bi = zi[kmax + nz];
+          srk[nz] += ar * br - ai * bi;
+          sik[nz] += ar * bi + ai * br;
+        }
+      }
+    }
+  }
+  std::vector<double> Sr(nk, 0.0), Si(nk, 0.0);
+  for (int t = 0; t < nthr; ++t)
+    for (long k = 0; k < nk; ++k) {
+      Sr[k] += Sr_t[static_cast<size_t>(t) * nk + k];
+      Si[k] += Si_t[static_cast<size_t>(t) * nk + k];
+    }
+#pragma omp parallel
+  {
+    std::vector<cd> px(kmax + 1), py(W), pz(W);
+#pragma omp for schedule(dynamic, 8)
+    for (long t = 0; t < nt; ++t) {
+      long const i = tidx[t];
+      axis_phases(pos + 3 * i, px, py, pz);
+      double fi[3] = {0, 0, 0};
+      for (auto const &rn : runs) {
+        cd const exy = px[rn.nx] * py[kmax + rn.ny];
+        double const kx = 2.0 * PI * rn.nx / box[0], ky = 2.0 * PI * rn.ny / box[1];
+        for (int nz = rn.nz0; nz <= rn.nz1; ++nz) {
+          cd const e = exy * pz[kmax + nz];
+          long const k = rn.k0 + nz - rn.nz0;
+          // sin(k.r) Sr - cos(k.r) Si
+          double const w = 2.0 * A[k] * (e.imag() * Sr[k] - e.real() * Si[k]);
+          fi[0] += w * kx;
+          fi[1] += w * ky;
+          fi[2] += w * (2.0 * PI * nz / box[2]);
+        }
+      }
+      for (int d = 0; d < 3; ++d)
+        f[3 * t + d] += prefactor * (4.0 * PI * q[i] / V) * fi[d];
+    }
+  }
+  return 0;
+}
+
 } // extern "C"

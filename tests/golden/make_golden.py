@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference tree.
 
-Run once in a container that has the ESPResSo source tree (default
-/root/reference, override with $P3MX_REFERENCE):
+Run once in a container that has the ESPResSo source tree, named by
+$P3MX_REFERENCE:
 
-    python tests/golden/make_golden.py
+    P3MX_REFERENCE=<ESPResSo tree> python tests/golden/make_golden.py
 
 Sources (paths relative to the ESPResSo tree):
   * testsuite/python/data/coulomb_cloud_wall_system.data  (id pos q f)
@@ -33,12 +33,15 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("P3MX_REFERENCE", "/root/reference")
+REF = os.environ.get("P3MX_REFERENCE", "")
 DATA = os.path.join(REF, "testsuite", "python", "data")
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 
 def main():
+    if not REF or not os.path.isdir(DATA):
+        sys.exit("make_golden.py: set P3MX_REFERENCE to the ESPResSo source tree "
+                 f"(got {REF!r})")
     d = np.genfromtxt(os.path.join(DATA, "coulomb_cloud_wall_system.data"))
     np.savez_compressed(
         os.path.join(HERE, "coulomb_cloud_wall.npz"),

@@ -60,7 +60,23 @@ def test_noalloc_matches_existing_entry_point_on_consecutive_calls():
         assert ks > 0.0
 
 
+def test_noalloc_at_its_largest_mesh():
+    # 256 x 256 x 1024 = 4096 * 16384 points: every one of the 4096 partial
+    # sums is written, and the final sum's strided loop covers all of them
+    case = ((256, 256, 1024), 7, 1 << 20, float(1 << 20), 110.0, 0.03, (128.0, 128.0, 512.0), 1.0)
+    for _ in range(2):
+        rc, rs, ks, msg = _noalloc(*case)
+        assert rc == 0, msg
+        rs0, ks0 = _existing(*case)
+        np.testing.assert_allclose(ks, ks0, rtol=1e-10, atol=0)
+        np.testing.assert_allclose(rs, rs0, rtol=1e-14, atol=0)
+
+
 def test_noalloc_rejects_meshes_beyond_its_scratch():
     rc, _, _, msg = _noalloc((512, 512, 512), 7, 1000, 1000.0, 50.0, 0.1, (100.0,) * 3, 1.0)
+    assert rc == 1
+    assert "exceeds the allocation-free maximum" in msg
+    # one point over the limit (4096 * 16384 + 1 = 5 * 13421773)
+    rc, _, _, msg = _noalloc((5, 13421773, 1), 7, 1000, 1000.0, 50.0, 0.1, (100.0,) * 3, 1.0)
     assert rc == 1
     assert "exceeds the allocation-free maximum" in msg
