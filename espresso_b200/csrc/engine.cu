@@ -187,7 +187,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       G.plan[d] = make_plan(c.mesh[d], twoff(c.mesh[d]));
     }
     G.hp = ((c.mesh[2] / 2 + 1) + 3) / 4 * 4;
-    // assignment bricks: edge >= cao-1 so that same-colour tiles never overlap
+    // sort bricks (stencil corners binned by brick; interpolation tiles)
     G.brick = (c.cao <= 5) ? 4 : 8; // brick_edge<cao>() of the kernels
     G.nbx = (c.mesh[0] + G.brick - 1) / G.brick;
     G.nby = (c.mesh[1] + G.brick - 1) / G.brick;
@@ -272,62 +272,20 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         bp.push_back(int2{r, b});
       m_blk_pair_start.push_back(static_cast<int>(bp.size()));
     }
-    // bricks of the assignment grouped by colour: per dimension, the tile
-    // intervals [bB, bB + min(B, M - bB) + cao - 1) on the periodic axis are
-    // coloured greedily so that intervals of one colour never intersect
-    // (modulo M); bricks sharing the colour triple then have disjoint tiles
-    {
-      auto colours = [](int M, int B, int P) {
-        int const nb = (M + B - 1) / B;
-        std::vector<int> s(nb), e(nb), col(nb, -1);
-        for (int b = 0; b < nb; ++b) {
-          s[b] = b * B;
-          e[b] = s[b] + std::min(B, M - s[b]) + P - 1;
-        }
-        auto hit = [&](int a, int b) {
-          if (e[a] - s[a] >= M || e[b] - s[b] >= M)
-            return true;
-          for (int k = -1; k <= 1; ++k)
-            if (s[a] < e[b] + k * M && s[b] + k * M < e[a])
-              return true;
-          return false;
-        };
-        for (int b = 0; b < nb; ++b) {
-          std::vector<char> used(nb + 1, 0);
-          for (int a = 0; a < nb; ++a)
-            if (a != b && col[a] >= 0 && hit(a, b))
-              used[col[a]] = 1;
-          int c = 0;
-          while (used[c])
-            ++c;
-          col[b] = c;
-        }
-        return col;
-      };
-      std::vector<std::vector<int2>> phase;
-      nat.clear();
-      for (int r = 0; r < R; ++r) {
-        auto const &G = m_geom[r];
-        auto const cxv = colours(G.mesh[0], G.brick, G.cao);
-        auto const cyv = colours(G.mesh[1], G.brick, G.cao);
-        auto const czv = colours(G.mesh[2], G.brick, G.cao);
-        for (int bx = 0; bx < G.nbx; ++bx)
-          for (int by = 0; by < G.nby; ++by)
-            for (int bz = 0; bz < G.nbz; ++bz) {
-              int const p = cxv[bx] + 8 * (cyv[by] + 8 * czv[bz]);
-              if (static_cast<int>(phase.size()) <= p)
-                phase.resize(p + 1);
-              phase[p].push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
-              nat.push_back(int2{r, (bx * G.nby + by) * G.nbz + bz});
-            }
-      }
-      m_phase_off.assign(1, 0);
-      for (auto const &ph : phase) {
-        bm.insert(bm.end(), ph.begin(), ph.end());
-        m_phase_off.push_back(static_cast<int>(bm.size()));
-      }
+    // owner blocks of the charge assignment (kOwnEdge^3 mesh points each,
+    // x-major) and all sort bricks in spatial order (interpolation)
+    nat.clear();
+    for (int r = 0; r < R; ++r) {
+      auto const &G = m_geom[r];
+      int const no = ceil_div(G.mesh[0], kOwnEdge) * ceil_div(G.mesh[1], kOwnEdge) *
+                     ceil_div(G.mesh[2], kOwnEdge);
+      for (int k = 0; k < no; ++k)
+        bm.push_back(int2{r, k});
+      for (int b = 0; b < G.nbx * G.nby * G.nbz; ++b)
+        nat.push_back(int2{r, b});
     }
     m_n_blk_mesh = static_cast<int>(bm.size());
+    m_n_bricks = static_cast<int>(nat.size());
     m_n_blk_cplx = static_cast<int>(bc.size());
     m_n_blk_census = static_cast<int>(bcen.size());
     m_n_blk_pair = static_cast<int>(bp.size());
@@ -413,22 +371,24 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
                                      static_cast<int>(limit)));
     };
     {
-      // assignment tiles: (brick + cao - 1)^3 fixed-point points per block
+      // assignment: owner tile plus staged records (FP64: above 48 KB)
       auto aset = [&](auto kern) {
         P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(limit)));
       };
       if (m_fp32) {
-        aset(k_p3m_assign<float, 1>); aset(k_p3m_assign<float, 2>); aset(k_p3m_assign<float, 3>);
-        aset(k_p3m_assign<float, 4>); aset(k_p3m_assign<float, 5>); aset(k_p3m_assign<float, 6>);
-        aset(k_p3m_assign<float, 7>);
+        aset(k_p3m_assign_own<float, 1>); aset(k_p3m_assign_own<float, 2>);
+        aset(k_p3m_assign_own<float, 3>); aset(k_p3m_assign_own<float, 4>);
+        aset(k_p3m_assign_own<float, 5>); aset(k_p3m_assign_own<float, 6>);
+        aset(k_p3m_assign_own<float, 7>);
         aset(k_p3m_interp<float, 1>); aset(k_p3m_interp<float, 2>); aset(k_p3m_interp<float, 3>);
         aset(k_p3m_interp<float, 4>); aset(k_p3m_interp<float, 5>); aset(k_p3m_interp<float, 6>);
         aset(k_p3m_interp<float, 7>);
       } else {
-        aset(k_p3m_assign<double, 1>); aset(k_p3m_assign<double, 2>); aset(k_p3m_assign<double, 3>);
-        aset(k_p3m_assign<double, 4>); aset(k_p3m_assign<double, 5>); aset(k_p3m_assign<double, 6>);
-        aset(k_p3m_assign<double, 7>);
+        aset(k_p3m_assign_own<double, 1>); aset(k_p3m_assign_own<double, 2>);
+        aset(k_p3m_assign_own<double, 3>); aset(k_p3m_assign_own<double, 4>);
+        aset(k_p3m_assign_own<double, 5>); aset(k_p3m_assign_own<double, 6>);
+        aset(k_p3m_assign_own<double, 7>);
         aset(k_p3m_interp<double, 1>); aset(k_p3m_interp<double, 2>); aset(k_p3m_interp<double, 3>);
         aset(k_p3m_interp<double, 4>); aset(k_p3m_interp<double, 5>); aset(k_p3m_interp<double, 6>);
         aset(k_p3m_interp<double, 7>);
@@ -461,7 +421,9 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_slot.ensure(n * sizeof(int));
   // + 8: the back-interpolation copies 16-byte aligned windows of these
   m_perm.ensure((n + 8) * sizeof(int));
-  m_cnt.ensure((m_nkeys + 1) * sizeof(int));
+  // sort-brick counts, then one word per replica: the bits of its largest
+  // |q| (FP32, rounded up), which the assignment's fixed-point scale needs
+  m_cnt.ensure((m_nkeys + 1 + R) * sizeof(int));
   m_start.ensure((m_nkeys + 1) * sizeof(int));
   m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
@@ -607,25 +569,6 @@ void Engine::encode_field_maps(cudaStream_t st) {
 }
 
 namespace {
-// One colour launch of the charge assignment; `chained` launches it as a
-// programmatic dependent of the previous colour (see k_p3m_assign).
-template <typename Real, int P>
-void launch_assign(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
-                   int const *start, Real const *W, int const *s_key, Real *rho, int *err) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(static_cast<unsigned>(cnt));
-  cfg.blockDim = dim3(32 * kAssignWarps);
-  cfg.dynamicSmemBytes = assign_smem<Real, P>();
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = chained ? 1 : 0;
-  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign<Real, P>, geom, tab, cnt, start, W, s_key, rho,
-                               err));
-}
-
 // Persistent grid of the back-interpolation pipeline: resident blocks per
 // SM times the SM count (computed once per kernel instance and process),
 // at most one block per brick.
@@ -684,7 +627,8 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   }
   mark("start", st);
   // 1. corner binning + deterministic counting sort
-  P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_nkeys + 1) * sizeof(int), st));
+  P3MX_CUDA(cudaMemsetAsync(m_cnt.p, 0, (m_nkeys + 1 + R) * sizeof(int), st));
+  unsigned *qmax_bits = reinterpret_cast<unsigned *>(m_cnt.as<int>() + m_nkeys + 1);
   int const nb = ceil_div(m_n, 256);
   if (m_n > 0) {
     k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
@@ -695,29 +639,22 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
     mark("p3m_sort", st);
     P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P, R><<<nb, 256, 0, st>>>(
                                geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
-                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_skey.as<int>())));
+                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_skey.as<int>(),
+                               qmax_bits)));
     ++m_launches;
     mark("p3m_weights", st);
   } else {
     P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_nkeys + 1) * sizeof(int), st));
   }
-  // 2. charge assignment: one warp per brick, colour by colour
-  P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
-  {
-    bool chained = false; // the first colour waits for the mesh memset normally
-    for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
-      int const cnt = m_phase_off[p + 1] - m_phase_off[p];
-      if (cnt == 0)
-        continue;
-      int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(cao, (launch_assign<Real, P>(chained, cnt, st, geom, tab,
-                                                       m_start.as<int>(), m_W.as<Real>(),
-                                                       m_skey.as<int>(), m_rho.as<Real>(),
-                                                       m_kerr.as<int>())));
-      chained = true;
-      ++m_launches;
-    }
-  }
+  // 2. charge assignment: one block per owned kOwnEdge^3 block of the mesh,
+  // every mesh point stored once (no memset, no read-add-write)
+  if (m_n_blk_mesh > 0)
+    P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign_own<Real, P><<<m_n_blk_mesh, 32 * kOwnWarps,
+                                                           own_smem<Real, P>(), st>>>(
+                                 geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
+                                 m_skey.as<int>(), qmax_bits, m_rho.as<Real>(),
+                                 m_kerr.as<int>())));
+  ++m_launches;
   mark("p3m_assign", st);
   // 3. forward FFT z (r2c) and y
   C const *tw = m_tw.as<C>();
@@ -765,7 +702,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   if (m_interp_wait)
     P3MX_CUDA(cudaStreamWaitEvent(st, m_interp_wait, 0));
   if (m_n > 0) {
-    int const nbr = m_phase_off.back();
+    int const nbr = m_n_bricks;
     P3MX_CAO_DISPATCH_R(cao, (k_p3m_interp<Real, P><<<interp_grid<Real, P>(nbr),
                                  32 * (1 + kInterpWarps), interp_smem<Real, P>(), st>>>(
                                  geom, m_blk_brick.as<int2>(), nbr, m_start.as<int>(),

@@ -178,13 +178,14 @@ private:
   long long m_bins = 0, m_cplx = 0, m_cells = 0, m_nkeys = 0; // m_nkeys: bricks (sort keys)
   long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
-  std::vector<int> m_phase_off; // assignment brick table offsets per colour
+  int m_n_bricks = 0; // sort bricks of all replicas (interpolation blocks)
   int m_ntypes = 1;
   std::vector<PairIA> m_ia;
 
   // tables
   DevBuf m_geom_d, m_rep_of, m_tw, m_ia_d;
-  DevBuf m_blk_mesh, m_blk_cplx, m_blk_census, m_blk_pair;
+  DevBuf m_blk_mesh; // owner blocks of the charge assignment
+  DevBuf m_blk_cplx, m_blk_census, m_blk_pair;
   DevBuf m_blk_brick; // all bricks in spatial order (interpolation)
   DevBuf m_blk_zf, m_blk_y, m_blk_x, m_blk_zi;
   std::vector<int> m_blk_x_start, m_blk_census_start, m_blk_pair_start;

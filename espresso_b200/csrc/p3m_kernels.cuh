@@ -94,17 +94,30 @@ template <int P, int R> __host__ __device__ constexpr int wstride() {
 template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
 
 // Weights in brick-sorted order; also the corner key (relative to the
-// replica's corner range) of every sorted particle.
+// replica's corner range) of every sorted particle, and each replica's
+// largest |q| (FP32 bits rounded up, atomic maximum: order-independent) for
+// the fixed-point scale of the charge assignment.
 template <typename Real, int P, int R>
 __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
                               const int *__restrict__ key, const Real *__restrict__ dist,
                               const double *__restrict__ q, const int *__restrict__ rep_of,
-                              long long n, Real *__restrict__ W, int *__restrict__ s_key) {
+                              long long n, Real *__restrict__ W, int *__restrict__ s_key,
+                              unsigned *__restrict__ qmax_bits) {
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
   int const i = perm[s];
-  RepGeom const &G = reps[rep_of[i]];
+  int const rep = rep_of[i];
+  RepGeom const &G = reps[rep];
+  {
+    // one atomic per group of lanes of the same replica
+    unsigned const qb = __float_as_uint(__double2float_ru(fabs(q[i])));
+    unsigned const act = __activemask();
+    unsigned const grp = __match_any_sync(act, rep);
+    unsigned const mx = __reduce_max_sync(grp, qb);
+    if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1))
+      atomicMax(&qmax_bits[rep], mx);
+  }
   Real w[3][P];
   bspline_weights<P>(dist[3 * i + 0], w[0]);
   bspline_weights<P>(dist[3 * i + 1], w[1]);
@@ -137,346 +150,15 @@ __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__res
   s_key[s] = key[i] - static_cast<int>(G.bin_off);
 }
 
-// Two-sum (Knuth): exact error term of a + b, for compensated summation.
-template <typename Real> __device__ inline void two_sum(Real &s, Real &c, Real v) {
-  Real const t = s + v;
-  Real const bp = t - s;
-  Real const err = (s - (t - bp)) + (v - bp);
-  s = t;
-  c += err;
-}
-
-// Brick edge (mesh points) of the charge assignment for order P: at least
-// P - 1 so that the tiles of one colour never overlap (the engine sets
-// RepGeom::brick by the same rule).
+// Edge (mesh points) of the sort bricks that bin the particles by stencil
+// corner for order P (the interpolation stages one brick's field tile of
+// (B + P - 1)^3 points; owner blocks of the assignment are whole numbers
+// of bricks).
 template <int P> __host__ __device__ constexpr int brick_edge() { return (P <= 5) ? 4 : 8; }
 
-// Strides of the charge-assignment tile [x][y][z] (z contiguous): the
-// smallest y stride >= E and x stride >= E * (y stride) for which the lanes of
-// a warp, one (x, y) stencil row each (row s = lane + 32 q, x = s / P,
-// y = s % P), hit distinct shared-memory banks.
 struct TileStrides {
   int sy, sx;
 };
-template <int P> __host__ __device__ constexpr TileStrides assign_strides() {
-  constexpr int E = brick_edge<P>() + P - 1;
-  for (int sy = E; sy < E + 16; ++sy)
-    for (int sx = E * sy; sx < E * sy + 64; ++sx) {
-      bool ok = true;
-      for (int q = 0; q * 32 < P * P && ok; ++q) {
-        unsigned used = 0;
-        for (int lane = 0; lane < 32 && lane + 32 * q < P * P; ++lane) {
-          int const r = lane + 32 * q;
-          unsigned const bit = 1u << (((r / P) * sx + (r % P) * sy) % 32);
-          if (used & bit) {
-            ok = false;
-            break;
-          }
-          used |= bit;
-        }
-      }
-      if (ok)
-        return TileStrides{sy, sx};
-    }
-  return TileStrides{E, E * E};
-}
-// Points (per word array) of the assignment tile for interpolation order P.
-template <int P> __host__ __device__ constexpr int assign_tile_points() {
-  return (brick_edge<P>() + P - 1) * assign_strides<P>().sx;
-}
-
-// Warps per brick (block) of the charge assignment, and particles whose
-// weight records are staged in shared memory at a time.
-constexpr int kAssignWarps = 4;
-constexpr int kAssignChunk = 64;
-
-// Bytes of dynamic shared memory of one assignment block: the split
-// fixed-point tile (two 32-bit words per point) and one staged chunk of
-// weight records and tile offsets.
-template <int P> __host__ __device__ constexpr size_t assign_tile_bytes() {
-  return (2 * sizeof(int) * static_cast<size_t>(assign_tile_points<P>()) + 15) / 16 * 16;
-}
-template <typename Real, int P> __host__ __device__ constexpr size_t assign_smem() {
-  return assign_tile_bytes<P>() + sizeof(Real) * kAssignChunk * wstride<P, 4>() +
-         sizeof(int) * kAssignChunk;
-}
-
-// Round-to-nearest split of a fixed-point contribution t (|t| <= 2^(22+kb))
-// into hi = rint(t / 2^kb) and lo = rint(t - hi 2^kb), both |.| <= 2^22.
-// FP32: the 1.5 * 2^23 magic-add rounding keeps the work on the FMA and ALU
-// pipes (no conversion instructions); t - hi 2^kb is exact (Sterbenz).
-__device__ inline void split_fixed(float t, float two_kb, float inv_two_kb, int &hi, int &lo) {
-  float const magic = 12582912.0f; // 1.5 * 2^23
-  float const hs = t * inv_two_kb + magic;
-  float const hf = hs - magic;
-  float const lf = fmaf(-hf, two_kb, t);
-  float const ls = lf + magic;
-  hi = __float_as_int(hs) - 0x4B400000;
-  lo = __float_as_int(ls) - 0x4B400000;
-}
-__device__ inline void split_fixed(double t, double two_kb, double inv_two_kb, int &hi, int &lo) {
-  double const hf = rint(t * inv_two_kb);
-  hi = static_cast<int>(hf);
-  lo = __double2int_rn(fma(-hf, two_kb, t));
-}
-template <typename Real> __device__ inline Real from_ll(long long v);
-template <> __device__ inline float from_ll<float>(long long v) { return __ll2float_rn(v); }
-template <> __device__ inline double from_ll<double>(long long v) { return __ll2double_rn(v); }
-
-// Deterministic charge assignment (AssignCharges, p3m.cpp:225-265), one
-// block of kAssignWarps warps per brick.  The particles of a brick (corners
-// in a B^3 block: one contiguous range of the brick-major sorted order) are
-// spread over the warps; for each particle the 32 lanes cover its P^3 stencil
-// points and add q*wx*wy*wz into the brick's shared-memory tile of
-// (B+P-1)^3 points.
-//
-// The tile holds fixed point: a contribution t = v*S (S a power of two) is
-// split into hi = rint(t / 2^kb) and lo = rint(t - hi*2^kb), |lo| <= 2^(kb-1),
-// added with 32-bit integer atomics to two words per point.  With n
-// particles in the brick, kb = min(23, 32 - bits(n)) keeps every lo sum
-// inside int32, and S = 2^(22+kb-ex) with sum|q| < 2^ex keeps |t| < 2^(22+kb)
-// (so |hi| < 2^22) and every hi sum inside int32; the point value is
-// (hi*2^kb + lo)/S.  Integer sums do not depend on the order of the adds, so
-// the tile is bitwise reproducible although the warps run concurrently; the
-// quantum is 2^-(22+kb) (at most 2^-45) of the brick's sum|q|.
-//
-// Tiles are then added to the mesh; bricks of one launch share a colour
-// (greedy interval colouring per dimension), so the tiles of one launch never
-// overlap and plain read-add-write is race-free; colours run in a fixed
-// order, making the mesh reproducible.  The colour launches are chained by
-// programmatic dependent launch: each block lets the next colour's grid start
-// (griddepcontrol.launch_dependents) as soon as it runs, so that grid fills
-// its tiles while this one drains, and waits (griddepcontrol.wait, the
-// completion and memory flush of the previous colour) only before its own
-// read-add-write of the mesh.
-template <typename Real, int P>
-__global__ void __launch_bounds__(32 * kAssignWarps)
-k_p3m_assign(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, int nbricks,
-             const int *__restrict__ start, const Real *__restrict__ W,
-             const int *__restrict__ s_key, Real *__restrict__ rho, int *__restrict__ err) {
-  constexpr int R = 4;
-  constexpr int WS = wstride<P, R>();
-  constexpr int WZ = wz_off<P, R>();
-  constexpr int P2 = P * P;
-  constexpr int NQ = (P2 + 31) / 32; // rounds of (x, y) stencil rows
-  constexpr int NT = 32 * kAssignWarps;
-  constexpr int TP = assign_tile_points<P>();
-  constexpr int SY = assign_strides<P>().sy, SX = assign_strides<P>().sx;
-  constexpr int CH = kAssignChunk;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double s_red[kAssignWarps];
-  __shared__ __align__(8) unsigned long long bar;
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  if (static_cast<int>(blockIdx.x) >= nbricks)
-    return; // whole block
-  int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int2 const bk = bricks[blockIdx.x];
-  RepGeom const &G = reps[bk.x];
-  constexpr int B = brick_edge<P>(), B3 = B * B * B;
-  const int *st = start + G.brk_off;
-  int const s0 = st[bk.y], s1 = st[bk.y + 1];
-  if (s0 == s1)
-    return; // empty brick: nothing to add
-  int *t_hi = reinterpret_cast<int *>(smem_raw);
-  int *t_lo = t_hi + TP;
-  Real *rec = reinterpret_cast<Real *>(smem_raw + assign_tile_bytes<P>());
-  int *rbase = reinterpret_cast<int *>(rec + CH * WS);
-  if (tid == 0)
-    mbar_init(&bar, 1);
-  {
-    int4 *z4 = reinterpret_cast<int4 *>(smem_raw);
-    for (int t = tid; t < static_cast<int>(assign_tile_bytes<P>() / 16); t += NT)
-      z4[t] = make_int4(0, 0, 0, 0);
-  }
-  __syncthreads(); // barrier initialised
-  // stage a chunk of records (contiguous, 16-byte aligned: one bulk copy by
-  // the TMA engine, completing on the mbarrier) and each particle's tile base
-  // offset; false when the copy did not land within the wait limit
-  unsigned parity = 0;
-  auto stage = [&](int c0, int cn) -> bool {
-    if (tid == 0) {
-      unsigned const nbytes = static_cast<unsigned>(cn * WS * sizeof(Real));
-      // the records of the previous chunk were read through the generic
-      // proxy: order those reads before the asynchronous-proxy writes
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive_expect_tx(&bar, nbytes);
-      bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
-    }
-    for (int j = tid; j < cn; j += NT) {
-      int const l = s_key[c0 + j] - bk.y * B3;
-      int const lb = __ffs(B) - 1; // B is a power of two
-      rbase[j] = (l >> (2 * lb)) * SX + ((l >> lb) & (B - 1)) * SY + (l & (B - 1));
-    }
-    bool const ok = mbar_wait(&bar, parity);
-    parity ^= 1u;
-    // the whole block leaves together if any thread gave up
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicExch(err, 1);
-        mbar_wait(&bar, parity ^ 1u); // second bounded wait for the copy in flight
-      }
-      return false;
-    }
-    return true;
-  };
-  int const cnt = s1 - s0;
-  if (!stage(s0, min(CH, cnt)))
-    return;
-  // (the vote inside stage() also orders the tile zeroing and the first chunk)
-  // total |q| of the brick: the x weights of a record are q*wx with wx >= 0
-  // summing to 1, so sum_k |q wx_k| = |q|
-  double aq = 0.0;
-  for (int s = s0 + tid; s < s1; s += NT) {
-    const Real *w = (s - s0 < CH) ? rec + (s - s0) * WS : W + static_cast<long long>(s) * WS;
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-      aq += fabs(static_cast<double>(w[k]));
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-    aq += __shfl_xor_sync(0xffffffffu, aq, o);
-  if (lane == 0)
-    s_red[warp] = aq;
-  __syncthreads();
-  double qabs = 0.0;
-#pragma unroll
-  for (int k = 0; k < kAssignWarps; ++k)
-    qabs += s_red[k];
-  if (qabs == 0.0)
-    return; // all charges zero: the tile would stay zero
-  int const kb = min(23, 32 - (32 - __clz(cnt))); // cnt < 2^(32-kb)
-  int ex;
-  frexp(qabs * (1.0 + 1e-12), &ex);
-  int const es = min(max(22 + kb - ex, -100), 100);
-  Real const S = static_cast<Real>(ldexp(1.0, es));
-  Real const two_kb = static_cast<Real>(1u << kb);
-  Real const inv_two_kb = static_cast<Real>(1.0 / (1u << kb));
-  // per-lane (x, y) stencil row of each round and its tile offset
-  int qx[NQ], qy[NQ], qoff[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    int const r = lane + 32 * q;
-    int const rr = (r < P2) ? r : 0;
-    qx[q] = rr / P;
-    qy[q] = rr % P;
-    qoff[q] = qx[q] * SX + qy[q] * SY;
-  }
-  for (int c0 = s0; c0 < s1; c0 += CH) {
-    int const cn = min(CH, s1 - c0);
-    if (c0 != s0) {
-      __syncthreads(); // previous chunk consumed
-      if (!stage(c0, cn))
-        return;
-    }
-    for (int j = warp; j < cn; j += kAssignWarps) {
-      int const base = rbase[j];
-      const Real *w = rec + j * WS;
-      Real wz[P];
-#pragma unroll
-      for (int k = 0; k < P; ++k)
-        wz[k] = w[WZ + k];
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        if (lane + 32 * q < P2) {
-          // the lane's row: P consecutive z points of one (x, y)
-          Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
-          int *const ph = t_hi + base + qoff[q];
-          int *const pl = t_lo + base + qoff[q];
-#pragma unroll
-          for (int k = 0; k < P; ++k) {
-            int hi, lo;
-            split_fixed(wxy * wz[k], two_kb, inv_two_kb, hi, lo);
-            atomicAdd(ph + k, hi);
-            atomicAdd(pl + k, lo);
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
-  // the previous colour's flush has completed and is visible
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  // add the tile to the mesh: real extent of the brick plus the stencil
-  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
-  int const bz = bk.y % G.nbz, by = (bk.y / G.nbz) % G.nby, bx = bk.y / (G.nbz * G.nby);
-  int const x0 = bx * B, y0 = by * B, z0 = bz * B;
-  int const ex0 = min(B, M0 - x0) + P - 1, ey = min(B, M1 - y0) + P - 1, ez = min(B, M2 - z0) + P - 1;
-  Real *mesh = rho + G.rm_off;
-  // a tile wider than the mesh maps two tile points onto one mesh point:
-  // add such points in separate passes (one per wrap class)
-  bool const self_wrap = (ex0 > M0) || (ey > M1) || (ez > M2);
-  int const passes = self_wrap ? 8 : 1;
-  // each thread owns fixed (y, z) slots of the tile's yz plane; loop over x
-  constexpr int EMAX = 8 + P - 1;
-  constexpr int NS = (EMAX * EMAX + NT - 1) / NT;
-  int yzt[NS], yzg[NS], ycls[NS];
-  int const nyz = ey * ez;
-#pragma unroll
-  for (int k2 = 0; k2 < NS; ++k2) {
-    int const t = tid + NT * k2;
-    int const y = (t < nyz) ? t / ez : 0, z = (t < nyz) ? t - (t / ez) * ez : 0;
-    int gy = y0 + y, gz = z0 + z, cls = 0;
-    if (gy >= M1) { gy -= M1; cls |= 2; }
-    if (gy >= M1) gy -= M1;
-    if (gz >= M2) { gz -= M2; cls |= 4; }
-    if (gz >= M2) gz -= M2;
-    yzt[k2] = (t < nyz) ? y * SY + z : -1;
-    yzg[k2] = gy * M2 + gz;
-    ycls[k2] = cls;
-  }
-  auto tile_val = [&](int ti) {
-    long long const v = static_cast<long long>(t_hi[ti]) * (1ll << kb) + t_lo[ti];
-    return from_ll<Real>(v) * inv_S;
-  };
-  if (!self_wrap) {
-    // every tile point maps to its own mesh point: issue all of the
-    // thread's mesh loads first, then the adds and stores
-    Real old[EMAX][NS];
-#pragma unroll
-    for (int x = 0; x < EMAX; ++x) {
-      if (x < ex0) {
-        int gx = x0 + x;
-        if (gx >= M0)
-          gx -= M0;
-        long long const gbase = static_cast<long long>(gx) * M1 * M2;
-#pragma unroll
-        for (int k2 = 0; k2 < NS; ++k2)
-          if (yzt[k2] >= 0)
-            old[x][k2] = mesh[gbase + yzg[k2]];
-      }
-    }
-#pragma unroll
-    for (int x = 0; x < EMAX; ++x) {
-      if (x < ex0) {
-        int gx = x0 + x;
-        if (gx >= M0)
-          gx -= M0;
-        long long const gbase = static_cast<long long>(gx) * M1 * M2;
-#pragma unroll
-        for (int k2 = 0; k2 < NS; ++k2)
-          if (yzt[k2] >= 0)
-            mesh[gbase + yzg[k2]] = old[x][k2] + tile_val(x * SX + yzt[k2]);
-      }
-    }
-    return;
-  }
-  for (int pass = 0; pass < passes; ++pass) {
-    for (int x = 0; x < ex0; ++x) {
-      int gx = x0 + x, xcls = 0;
-      if (gx >= M0) { gx -= M0; xcls = 1; }
-      if (gx >= M0) gx -= M0;
-      long long const gbase = static_cast<long long>(gx) * M1 * M2;
-#pragma unroll
-      for (int k2 = 0; k2 < NS; ++k2) {
-        if (yzt[k2] < 0 || (xcls | ycls[k2]) != pass)
-          continue;
-        mesh[gbase + yzg[k2]] += tile_val(x * SX + yzt[k2]);
-      }
-    }
-    __syncthreads();
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Owner-computes charge assignment (AssignCharges, p3m.cpp:225-265;
@@ -576,19 +258,27 @@ template <typename Real, int P> __host__ __device__ constexpr size_t own_smem() 
 }
 
 // Sort bricks (per dimension) whose corners can reach the owned points
-// [o, o + ext): corners in [o - (P-1), o + ext), bricks first .. first+cnt-1
-// modulo nb (all nb when the span covers the axis).
-__device__ inline void own_brick_span(int o, int ext, int P, int B, int nb, int &first,
-                                      int &cnt) {
-  int const lo = o - (P - 1);
-  first = (lo >= 0) ? lo / B : -((-lo + B - 1) / B);
-  int const last = (o + ext - 1) / B;
-  cnt = last - first + 1;
-  if (cnt >= nb) {
-    first = 0;
-    cnt = nb;
-  }
+// [o, o + ext): corners in [o - (P-1), o + ext) modulo M.  Corners are
+// folded into [0, M), so a span reaching below 0 is the two corner ranges
+// [lo + M, M) and [0, o + ext) (M need not be a multiple of B); the bricks
+// are [a0, a0 + n0) and [a1, a1 + n1) (n1 = 0 when one range suffices, all
+// nb bricks when the ranges meet).
+struct BrickSpan {
+  int a0, n0, a1, n1;
+};
+__device__ inline BrickSpan own_brick_span(int o, int ext, int P, int B, int M, int nb) {
+  int const lo = o - (P - 1), hi = o + ext; // hi <= M, lo + M >= 1 (P <= M)
+  if (lo >= 0)
+    return BrickSpan{lo / B, (hi - 1) / B - lo / B + 1, 0, 0};
+  int const w0 = (lo + M) / B, h1 = (hi - 1) / B;
+  if (w0 <= h1)
+    return BrickSpan{0, nb, 0, 0};
+  return BrickSpan{w0, nb - w0, 0, h1 + 1};
 }
+
+// Runs of the owner-block table: at most (bricks per column span)^2 (x, y)
+// brick columns, each with at most two contiguous z runs.
+constexpr int kOwnMaxRuns = 128;
 
 template <typename Real, int P>
 __global__ void __launch_bounds__(32 * kOwnWarps)
@@ -610,8 +300,12 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
   constexpr int SY = TS.sy, SX = TS.sx;
   constexpr int TW = static_cast<int>(own_tile_bytes<Real, P>() / sizeof(Word));
   constexpr int CH = kOwnChunk;
+  static_assert(2 * ((E + P - 1 + B - 1) / B + 1) * ((E + P - 1 + B - 1) / B + 1) <= kOwnMaxRuns,
+                "run table too small");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bar;
+  __shared__ int s_r0[kOwnMaxRuns], s_r1[kOwnMaxRuns], s_rb[kOwnMaxRuns];
+  __shared__ long long s_count;
   Word *tile = reinterpret_cast<Word *>(smem_raw);
   Real *rec = reinterpret_cast<Real *>(smem_raw + own_tile_bytes<Real, P>());
   int *roff = reinterpret_cast<int *>(rec + CH * WS);
@@ -619,55 +313,64 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
 
   int2 const ow = owners[blockIdx.x];
   RepGeom const &G = reps[ow.x];
-  int const M[3] = {G.mesh[0], G.mesh[1], G.mesh[2]};
-  int const no1 = (M[1] + E - 1) / E, no2 = (M[2] + E - 1) / E;
-  int const o[3] = {(ow.y / (no1 * no2)) * E, ((ow.y / no2) % no1) * E, (ow.y % no2) * E};
-  int const ext[3] = {min(E, M[0] - o[0]), min(E, M[1] - o[1]), min(E, M[2] - o[2])};
-  int const nb[3] = {G.nbx, G.nby, G.nbz};
+  int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
+  int const no1 = (M1 + E - 1) / E, no2 = (M2 + E - 1) / E;
+  int const o0 = (ow.y / (no1 * no2)) * E, o1 = ((ow.y / no2) % no1) * E, o2 = (ow.y % no2) * E;
+  int const e0 = min(E, M0 - o0), e1 = min(E, M1 - o1), e2 = min(E, M2 - o2);
+  int const nb0 = G.nbx, nb1 = G.nby, nb2 = G.nbz;
   // fast geometry: a stencil meets the owned interval at most once per axis
-  bool const fast = (M[0] >= ext[0] + P - 1) && (M[1] >= ext[1] + P - 1) &&
-                    (M[2] >= ext[2] + P - 1);
-  int bf[3], bc[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d)
-    own_brick_span(o[d], ext[d], P, B, nb[d], bf[d], bc[d]);
-  auto wrapb = [](int v, int n) { return ((v % n) + n) % n; };
-  const int *st = start + G.brk_off;
-  // the particles of the visited bricks: (x, y) brick columns, each with at
-  // most two contiguous z runs
-  auto for_runs = [&](auto &&fn) {
-    int const z0 = wrapb(bf[2], nb[2]);
-    int const z1 = min(z0 + bc[2], nb[2]);
-    int const z2 = z0 + bc[2] - nb[2]; // > 0: second run [0, z2)
-    for (int ix = 0; ix < bc[0]; ++ix) {
-      int const bx = wrapb(bf[0] + ix, nb[0]);
-      for (int iy = 0; iy < bc[1]; ++iy) {
-        int const by = wrapb(bf[1] + iy, nb[1]);
-        int const col = (bx * nb[1] + by) * nb[2];
-        fn(bx, by, z0, st[col + z0], st[col + z1]);
-        if (z2 > 0)
-          fn(bx, by, 0, st[col], st[col + z2]);
-      }
+  bool const fast = (M0 >= e0 + P - 1) && (M1 >= e1 + P - 1) && (M2 >= e2 + P - 1);
+  BrickSpan const sx = own_brick_span(o0, e0, P, B, M0, nb0);
+  BrickSpan const sy = own_brick_span(o1, e1, P, B, M1, nb1);
+  BrickSpan const sz = own_brick_span(o2, e2, P, B, M2, nb2);
+  // run table: column t = (ix, iy) of the x and y brick lists gives runs 2t
+  // and 2t + 1, its two z brick ranges (the second possibly empty); s_rb
+  // packs the column's brick coordinates and the run's first z brick
+  int const cy = sy.n0 + sy.n1;
+  int const ncol = (sx.n0 + sx.n1) * cy;
+  {
+    const int *st = start + G.brk_off;
+    for (int t = tid; t < ncol; t += NT) {
+      int const ix = t / cy, iy = t - ix * cy;
+      int const bx = (ix < sx.n0) ? sx.a0 + ix : sx.a1 + (ix - sx.n0);
+      int const by = (iy < sy.n0) ? sy.a0 + iy : sy.a1 + (iy - sy.n0);
+      int const col = (bx * nb1 + by) * nb2;
+      s_r0[2 * t] = st[col + sz.a0];
+      s_r1[2 * t] = st[col + sz.a0 + sz.n0];
+      s_rb[2 * t] = (bx << 20) | (by << 10) | sz.a0;
+      s_r0[2 * t + 1] = (sz.n1 > 0) ? st[col + sz.a1] : 0;
+      s_r1[2 * t + 1] = (sz.n1 > 0) ? st[col + sz.a1 + sz.n1] : 0;
+      s_rb[2 * t + 1] = (bx << 20) | (by << 10) | sz.a1;
     }
-  };
-  long long count = 0;
-  for_runs([&](int, int, int, int s0, int s1) { count += s1 - s0; });
-  float const qmax = __uint_as_float(qmax_bits[ow.x]);
+  }
   // zero the tile; initialise the staging barrier
   for (int t = tid; t < TW; t += NT)
     tile[t] = Word(0);
   if (tid == 0)
     mbar_init(&bar, 1);
   __syncthreads();
+  if (warp == 0) {
+    long long c = 0;
+    for (int t = lane; t < 2 * ncol; t += 32)
+      c += s_r1[t] - s_r0[t];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      c += __shfl_xor_sync(0xffffffffu, c, off);
+    if (lane == 0)
+      s_count = c;
+  }
+  __syncthreads();
+  long long const count = s_count;
+  float const qmax = __uint_as_float(qmax_bits[ow.x]);
   int es = 0;
   bool const any = (count > 0) && (qmax > 0.0f);
   if (any) {
     double const unit = static_cast<double>(qmax) * bspline_wmax<P>() * bspline_wmax<P>() *
                         bspline_wmax<P>();
-    int e1, e2;
-    frexp(unit, &e1);
-    frexp(unit * static_cast<double>(count), &e2);
-    es = min(OwnWord<Real>::term_bits - e1, OwnWord<Real>::sum_bits - e2);
+    int ea, eb;
+    frexp(unit, &ea);
+    frexp(unit * static_cast<double>(count), &eb);
+    es = min(OwnWord<Real>::term_bits - ea, OwnWord<Real>::sum_bits - eb);
     es = max(min(es, 1000), -1000);
   }
   Real const S = static_cast<Real>(ldexp(1.0, es));
@@ -681,126 +384,111 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
     qy[q] = rr % P;
   }
   unsigned parity = 0;
-  bool ok = true;
-  if (any) {
-    for_runs([&](int bx, int by, int bz0, int s0, int s1) {
-      if (!ok)
-        return;
-      int const b0 = (bx * nb[1] + by) * nb[2] + bz0;
-      for (int c0 = s0; c0 < s1 && ok; c0 += CH) {
-        int const cn = min(CH, s1 - c0);
-        __syncthreads(); // the previous chunk is consumed
+  for (int run = 0; any && run < 2 * ncol; ++run) {
+    int const s0 = s_r0[run], s1 = s_r1[run];
+    if (s0 >= s1)
+      continue;
+    int const rb = s_rb[run];
+    int const bx = rb >> 20, by = (rb >> 10) & 1023, bz0 = rb & 1023;
+    int const b0 = (bx * nb1 + by) * nb2 + bz0;
+    for (int c0 = s0; c0 < s1; c0 += CH) {
+      int const cn = min(CH, s1 - c0);
+      __syncthreads(); // the previous chunk is consumed
+      if (tid == 0) {
+        unsigned const nbytes = static_cast<unsigned>(cn * WS * sizeof(Real));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&bar, nbytes);
+        bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
+      }
+      for (int j = tid; j < cn; j += NT) {
+        int const sk = s_key[c0 + j];
+        int const bz = bz0 + ((sk >> (3 * LB)) - b0);
+        int const l = sk & (B3 - 1);
+        int const gx = bx * B + (l >> (2 * LB)), gy = by * B + ((l >> LB) & (B - 1)),
+                  gz = bz * B + (l & (B - 1));
+        int pk;
+        if (fast) {
+          // offset from the block origin, wrapped into [-(P-1), M-(P-1))
+          int dx = gx - o0, dy = gy - o1, dz = gz - o2;
+          dx += (dx < 0) ? M0 : 0;
+          dy += (dy < 0) ? M1 : 0;
+          dz += (dz < 0) ? M2 : 0;
+          dx -= (dx > M0 - P) ? M0 : 0;
+          dy -= (dy > M1 - P) ? M1 : 0;
+          dz -= (dz > M2 - P) ? M2 : 0;
+          bool const hit = (dx < e0) && (dy < e1) && (dz < e2);
+          pk = hit ? (((dx + 128) << 16) | ((dy + 128) << 8) | (dz + 128)) : kOwnSkip;
+        } else {
+          pk = (gx << 20) | (gy << 10) | gz;
+        }
+        roff[j] = pk;
+      }
+      bool const got = mbar_wait(&bar, parity);
+      parity ^= 1u;
+      if (__syncthreads_or(!got)) {
         if (tid == 0) {
-          unsigned const nbytes = static_cast<unsigned>(cn * WS * sizeof(Real));
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_arrive_expect_tx(&bar, nbytes);
-          bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
+          atomicExch(err, 1);
+          mbar_wait(&bar, parity ^ 1u); // bounded wait for the copy in flight
         }
-        for (int j = tid; j < cn; j += NT) {
-          int const sk = s_key[c0 + j];
-          int const bz = bz0 + ((sk >> (3 * LB)) - b0);
-          int const l = sk & (B3 - 1);
-          int const g[3] = {bx * B + (l >> (2 * LB)), by * B + ((l >> LB) & (B - 1)),
-                            bz * B + (l & (B - 1))};
-          int pk;
-          if (fast) {
-            bool hit = true;
-            int dd[3];
+        return;
+      }
+      for (int j = warp; j < cn; j += kOwnWarps) {
+        int const pk = roff[j];
+        if (pk == kOwnSkip)
+          continue;
+        const Real *w = rec + j * WS;
+        Real wz[P];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              int v = g[d] - o[d];
-              if (v < 0)
-                v += M[d];
-              if (v > M[d] - P)
-                v -= M[d];
-              dd[d] = v;
-              hit = hit && (v < ext[d]);
+        for (int k = 0; k < P; ++k)
+          wz[k] = w[WZ + k];
+        if (fast) {
+          int const dx = ((pk >> 16) & 255) - 128, dy = ((pk >> 8) & 255) - 128,
+                    dz = (pk & 255) - 128;
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) {
+            int const x = dx + qx[q], y = dy + qy[q];
+            if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(e0) &&
+                static_cast<unsigned>(y) < static_cast<unsigned>(e1)) {
+              Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
+              Word *pt = tile + x * SX + y * SY + dz;
+#pragma unroll
+              for (int k = 0; k < P; ++k)
+                if (static_cast<unsigned>(dz + k) < static_cast<unsigned>(e2))
+                  atomicAdd(pt + k, own_fixed(wxy, wz[k]));
             }
-            pk = hit ? (((dd[0] + 128) << 16) | ((dd[1] + 128) << 8) | (dd[2] + 128)) : kOwnSkip;
-          } else {
-            pk = (g[0] << 20) | (g[1] << 10) | g[2];
           }
-          roff[j] = pk;
-        }
-        bool const got = mbar_wait(&bar, parity);
-        parity ^= 1u;
-        if (__syncthreads_or(!got)) {
-          if (tid == 0) {
-            atomicExch(err, 1);
-            mbar_wait(&bar, parity ^ 1u); // bounded wait for the copy in flight
-          }
-          ok = false;
-          return;
-        }
-        for (int j = warp; j < cn; j += kOwnWarps) {
-          int const pk = roff[j];
-          if (pk == kOwnSkip)
-            continue;
-          const Real *w = rec + j * WS;
-          Real wz[P];
+        } else {
+          // small meshes: every stencil point wrapped and tested on its own
+          int const gx = (pk >> 20) & 1023, gy = (pk >> 10) & 1023, gz = pk & 1023;
 #pragma unroll
-          for (int k = 0; k < P; ++k)
-            wz[k] = w[WZ + k];
-          if (fast) {
-            int const dx = ((pk >> 16) & 255) - 128, dy = ((pk >> 8) & 255) - 128,
-                      dz = (pk & 255) - 128;
+          for (int q = 0; q < NQ; ++q) {
+            int const x = (gx + qx[q]) % M0 - o0, y = (gy + qy[q]) % M1 - o1;
+            if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(e0) &&
+                static_cast<unsigned>(y) < static_cast<unsigned>(e1)) {
+              Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
+              Word *pt = tile + x * SX + y * SY;
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-              int const x = dx + qx[q], y = dy + qy[q];
-              if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(ext[0]) &&
-                  static_cast<unsigned>(y) < static_cast<unsigned>(ext[1])) {
-                Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
-                Word *pt = tile + x * SX + y * SY + dz;
-#pragma unroll
-                for (int k = 0; k < P; ++k)
-                  if (static_cast<unsigned>(dz + k) < static_cast<unsigned>(ext[2]))
-                    atomicAdd(pt + k, own_fixed(wxy, wz[k]));
-              }
-            }
-          } else {
-            // small meshes: every stencil point wrapped and tested on its own
-            int const gx = (pk >> 20) & 1023, gy = (pk >> 10) & 1023, gz = pk & 1023;
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-              int x = gx + qx[q], y = gy + qy[q];
-              if (x >= M[0])
-                x -= M[0];
-              if (y >= M[1])
-                y -= M[1];
-              x -= o[0];
-              y -= o[1];
-              if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(ext[0]) &&
-                  static_cast<unsigned>(y) < static_cast<unsigned>(ext[1])) {
-                Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
-                Word *pt = tile + x * SX + y * SY;
-#pragma unroll
-                for (int k = 0; k < P; ++k) {
-                  int z = gz + k;
-                  if (z >= M[2])
-                    z -= M[2];
-                  z -= o[2];
-                  if (static_cast<unsigned>(z) < static_cast<unsigned>(ext[2]))
-                    atomicAdd(pt + z, own_fixed(wxy, wz[k]));
-                }
+              for (int k = 0; k < P; ++k) {
+                int const z = (gz + k) % M2 - o2;
+                if (static_cast<unsigned>(z) < static_cast<unsigned>(e2))
+                  atomicAdd(pt + z, own_fixed(wxy, wz[k]));
               }
             }
           }
         }
       }
-    });
+    }
   }
-  if (!ok)
-    return;
   __syncthreads();
   // store the owned points once (zeros for a block no charge reaches)
   Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
   Real *mesh = rho + G.rm_off;
-  if (ext[0] == E && ext[1] == E && ext[2] == E && (M[2] % 4) == 0 && (G.rm_off % 4) == 0) {
+  if (e0 == E && e1 == E && e2 == E && (M2 % 4) == 0 && (G.rm_off % 4) == 0) {
     // four consecutive z points per thread and iteration, one vector store
     for (int t = tid; t < E * E * (E / 4); t += NT) {
       int const z4 = (t & 3) * 4, y = (t >> 2) & (E - 1), x = t >> 6;
       const Word *tp = tile + x * SX + y * SY + z4;
-      Real *mp = mesh + (static_cast<long long>(o[0] + x) * M[1] + (o[1] + y)) * M[2] + o[2] + z4;
+      Real *mp = mesh + (static_cast<long long>(o0 + x) * M1 + (o1 + y)) * M2 + o2 + z4;
       Real v[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k)
@@ -813,10 +501,10 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
       }
     }
   } else {
-    int const nyz = ext[1] * ext[2];
-    for (int t = tid; t < ext[0] * nyz; t += NT) {
-      int const x = t / nyz, yz = t - x * nyz, y = yz / ext[2], z = yz - y * ext[2];
-      mesh[(static_cast<long long>(o[0] + x) * M[1] + (o[1] + y)) * M[2] + o[2] + z] =
+    int const nyz = e1 * e2;
+    for (int t = tid; t < e0 * nyz; t += NT) {
+      int const x = t / nyz, yz = t - x * nyz, y = yz / e2, z = yz - y * e2;
+      mesh[(static_cast<long long>(o0 + x) * M1 + (o1 + y)) * M2 + o2 + z] =
           own_value(tile[x * SX + y * SY + z], inv_S);
     }
   }
