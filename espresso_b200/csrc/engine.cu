@@ -272,17 +272,65 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         bp.push_back(int2{r, b});
       m_blk_pair_start.push_back(static_cast<int>(bp.size()));
     }
-    // owner blocks of the charge assignment (kOwnEdge^3 mesh points each,
-    // x-major) and all sort bricks in spatial order (interpolation)
-    nat.clear();
-    for (int r = 0; r < R; ++r) {
-      auto const &G = m_geom[r];
-      int const no = ceil_div(G.mesh[0], kOwnEdge) * ceil_div(G.mesh[1], kOwnEdge) *
-                     ceil_div(G.mesh[2], kOwnEdge);
-      for (int k = 0; k < no; ++k)
-        bm.push_back(int2{r, k});
-      for (int b = 0; b < G.nbx * G.nby * G.nbz; ++b)
-        nat.push_back(int2{r, b});
+    // super-bricks of the charge assignment grouped by colour: per
+    // dimension, the tile intervals [bE, bE + min(E, M - bE) + cao - 1) of
+    // the super-bricks (E = kSbEdge) on the periodic axis are coloured
+    // greedily so that intervals of one colour never intersect (modulo M);
+    // super-bricks sharing the colour triple then have disjoint tiles.  All
+    // sort bricks in spatial order feed the interpolation.
+    {
+      auto colours = [](int M, int B, int P) {
+        int const nb = (M + B - 1) / B;
+        std::vector<int> s(nb), e(nb), col(nb, -1);
+        for (int b = 0; b < nb; ++b) {
+          s[b] = b * B;
+          e[b] = s[b] + std::min(B, M - s[b]) + P - 1;
+        }
+        auto hit = [&](int a, int b) {
+          if (e[a] - s[a] >= M || e[b] - s[b] >= M)
+            return true;
+          for (int k = -1; k <= 1; ++k)
+            if (s[a] < e[b] + k * M && s[b] + k * M < e[a])
+              return true;
+          return false;
+        };
+        for (int b = 0; b < nb; ++b) {
+          std::vector<char> used(nb + 1, 0);
+          for (int a = 0; a < nb; ++a)
+            if (a != b && col[a] >= 0 && hit(a, b))
+              used[col[a]] = 1;
+          int c = 0;
+          while (used[c])
+            ++c;
+          col[b] = c;
+        }
+        return col;
+      };
+      std::vector<std::vector<int2>> phase;
+      nat.clear();
+      for (int r = 0; r < R; ++r) {
+        auto const &G = m_geom[r];
+        auto const cxv = colours(G.mesh[0], kSbEdge, G.cao);
+        auto const cyv = colours(G.mesh[1], kSbEdge, G.cao);
+        auto const czv = colours(G.mesh[2], kSbEdge, G.cao);
+        int const n0 = static_cast<int>(cxv.size()), n1 = static_cast<int>(cyv.size()),
+                  n2 = static_cast<int>(czv.size());
+        for (int bx = 0; bx < n0; ++bx)
+          for (int by = 0; by < n1; ++by)
+            for (int bz = 0; bz < n2; ++bz) {
+              int const p = cxv[bx] + 8 * (cyv[by] + 8 * czv[bz]);
+              if (static_cast<int>(phase.size()) <= p)
+                phase.resize(p + 1);
+              phase[p].push_back(int2{r, (bx * n1 + by) * n2 + bz});
+            }
+        for (int b = 0; b < G.nbx * G.nby * G.nbz; ++b)
+          nat.push_back(int2{r, b});
+      }
+      m_phase_off.assign(1, 0);
+      for (auto const &ph : phase) {
+        bm.insert(bm.end(), ph.begin(), ph.end());
+        m_phase_off.push_back(static_cast<int>(bm.size()));
+      }
     }
     m_n_blk_mesh = static_cast<int>(bm.size());
     m_n_bricks = static_cast<int>(nat.size());
@@ -371,24 +419,24 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
                                      static_cast<int>(limit)));
     };
     {
-      // assignment: owner tile plus staged records (FP64: above 48 KB)
+      // assignment: super-brick tile plus staged records (above 48 KB)
       auto aset = [&](auto kern) {
         P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(limit)));
       };
       if (m_fp32) {
-        aset(k_p3m_assign_own<float, 1>); aset(k_p3m_assign_own<float, 2>);
-        aset(k_p3m_assign_own<float, 3>); aset(k_p3m_assign_own<float, 4>);
-        aset(k_p3m_assign_own<float, 5>); aset(k_p3m_assign_own<float, 6>);
-        aset(k_p3m_assign_own<float, 7>);
+        aset(k_p3m_assign_sb<float, 1>); aset(k_p3m_assign_sb<float, 2>);
+        aset(k_p3m_assign_sb<float, 3>); aset(k_p3m_assign_sb<float, 4>);
+        aset(k_p3m_assign_sb<float, 5>); aset(k_p3m_assign_sb<float, 6>);
+        aset(k_p3m_assign_sb<float, 7>);
         aset(k_p3m_interp<float, 1>); aset(k_p3m_interp<float, 2>); aset(k_p3m_interp<float, 3>);
         aset(k_p3m_interp<float, 4>); aset(k_p3m_interp<float, 5>); aset(k_p3m_interp<float, 6>);
         aset(k_p3m_interp<float, 7>);
       } else {
-        aset(k_p3m_assign_own<double, 1>); aset(k_p3m_assign_own<double, 2>);
-        aset(k_p3m_assign_own<double, 3>); aset(k_p3m_assign_own<double, 4>);
-        aset(k_p3m_assign_own<double, 5>); aset(k_p3m_assign_own<double, 6>);
-        aset(k_p3m_assign_own<double, 7>);
+        aset(k_p3m_assign_sb<double, 1>); aset(k_p3m_assign_sb<double, 2>);
+        aset(k_p3m_assign_sb<double, 3>); aset(k_p3m_assign_sb<double, 4>);
+        aset(k_p3m_assign_sb<double, 5>); aset(k_p3m_assign_sb<double, 6>);
+        aset(k_p3m_assign_sb<double, 7>);
         aset(k_p3m_interp<double, 1>); aset(k_p3m_interp<double, 2>); aset(k_p3m_interp<double, 3>);
         aset(k_p3m_interp<double, 4>); aset(k_p3m_interp<double, 5>); aset(k_p3m_interp<double, 6>);
         aset(k_p3m_interp<double, 7>);
@@ -569,6 +617,26 @@ void Engine::encode_field_maps(cudaStream_t st) {
 }
 
 namespace {
+// One colour launch of the charge assignment; `chained` launches it as a
+// programmatic dependent of the previous colour (see k_p3m_assign_sb).
+template <typename Real, int P>
+void launch_assign(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
+                   int const *start, Real const *W, int const *s_key, unsigned const *qmax_bits,
+                   Real *rho, int *err) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(cnt));
+  cfg.blockDim = dim3(32 * kSbWarps);
+  cfg.dynamicSmemBytes = sb_smem<Real, P>();
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = chained ? 1 : 0;
+  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign_sb<Real, P>, geom, tab, cnt, start, W, s_key,
+                               qmax_bits, rho, err));
+}
+
 // Persistent grid of the back-interpolation pipeline: resident blocks per
 // SM times the SM count (computed once per kernel instance and process),
 // at most one block per brick.
@@ -646,15 +714,23 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   } else {
     P3MX_CUDA(cudaMemsetAsync(m_start.p, 0, (m_nkeys + 1) * sizeof(int), st));
   }
-  // 2. charge assignment: one block per owned kOwnEdge^3 block of the mesh,
-  // every mesh point stored once (no memset, no read-add-write)
-  if (m_n_blk_mesh > 0)
-    P3MX_CAO_DISPATCH_R(cao, (k_p3m_assign_own<Real, P><<<m_n_blk_mesh, 32 * kOwnWarps,
-                                                           own_smem<Real, P>(), st>>>(
-                                 geom, m_blk_mesh.as<int2>(), m_start.as<int>(), m_W.as<Real>(),
-                                 m_skey.as<int>(), qmax_bits, m_rho.as<Real>(),
-                                 m_kerr.as<int>())));
-  ++m_launches;
+  // 2. charge assignment: one block per super-brick, colour by colour
+  P3MX_CUDA(cudaMemsetAsync(m_rho.p, 0, m_bins * sizeof(Real), st));
+  {
+    bool chained = false; // the first colour waits for the mesh memset normally
+    for (size_t p = 0; p + 1 < m_phase_off.size(); ++p) {
+      int const cnt = m_phase_off[p + 1] - m_phase_off[p];
+      if (cnt == 0)
+        continue;
+      int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
+      P3MX_CAO_DISPATCH_R(cao, (launch_assign<Real, P>(chained, cnt, st, geom, tab,
+                                                       m_start.as<int>(), m_W.as<Real>(),
+                                                       m_skey.as<int>(), qmax_bits,
+                                                       m_rho.as<Real>(), m_kerr.as<int>())));
+      chained = true;
+      ++m_launches;
+    }
+  }
   mark("p3m_assign", st);
   // 3. forward FFT z (r2c) and y
   C const *tw = m_tw.as<C>();

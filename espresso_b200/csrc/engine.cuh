@@ -179,12 +179,13 @@ private:
   long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
   int m_n_bricks = 0; // sort bricks of all replicas (interpolation blocks)
+  std::vector<int> m_phase_off; // assignment super-brick table offsets per colour
   int m_ntypes = 1;
   std::vector<PairIA> m_ia;
 
   // tables
   DevBuf m_geom_d, m_rep_of, m_tw, m_ia_d;
-  DevBuf m_blk_mesh; // owner blocks of the charge assignment
+  DevBuf m_blk_mesh; // super-bricks of the charge assignment, grouped by colour
   DevBuf m_blk_cplx, m_blk_census, m_blk_pair;
   DevBuf m_blk_brick; // all bricks in spatial order (interpolation)
   DevBuf m_blk_zf, m_blk_y, m_blk_x, m_blk_zi;

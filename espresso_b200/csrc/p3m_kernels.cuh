@@ -161,35 +161,40 @@ struct TileStrides {
 };
 
 // ---------------------------------------------------------------------------
-// Owner-computes charge assignment (AssignCharges, p3m.cpp:225-265;
-// charge_assign, p3m.cpp:283-330): the mesh is cut into owner blocks of
-// kOwnEdge^3 points and one CTA computes every point of its block and
-// stores it once -- no mesh memset, no read-add-write, no colours.  The
-// CTA visits the particles whose stencils reach its block: their corners
-// lie within P-1 points below the block or inside it, i.e. in a few
-// columns of the corner sort's bricks (contiguous ranges of the brick-major
-// order).  For each particle one warp covers the P^2 (x, y) stencil rows
-// (one row per lane, the P z points of a row unrolled) and adds the points
-// that fall into the block, in fixed point, into a shared-memory tile of
-// the block alone.
+// Charge assignment by super-bricks (AssignCharges, p3m.cpp:225-265;
+// charge_assign, p3m.cpp:283-330).  One CTA takes the particles whose
+// stencil corners lie in a super-brick of kSbEdge^3 corner positions (whole
+// sort bricks: a few contiguous ranges of the brick-major order), so every
+// particle is visited once.  For each particle one warp covers its P^2
+// (x, y) stencil rows (one row per lane, the P z points of a row unrolled)
+// and adds q wx wy wz into a shared-memory tile of (kSbEdge + P - 1)^3
+// points, in fixed point; the tile is then added to the mesh.  Tiles of
+// neighbouring super-bricks overlap by P - 1 points, so super-bricks are
+// coloured (greedy interval colouring per dimension: tiles of one colour
+// never overlap, modulo the mesh) and launched colour by colour: the plain
+// read-add-write of a tile is race-free and the colour order fixes the
+// order of the FP adds, so the mesh is bitwise reproducible.  The colour
+// launches are chained by programmatic dependent launch: a colour fills its
+// tiles while the previous one drains, and waits (griddepcontrol.wait) only
+// before its read-add-write of the mesh.
 //
-// Fixed point: a term v = q wx wy wz becomes t = rint(v S) by one FMA with a
-// magic constant (1.5 * 2^23 in FP32, 1.5 * 2^52 in FP64: the sum's bits
-// minus the constant's are t exactly while |t| < 2^22 / 2^51) and is added
-// with an integer atomic (32-bit words for the FP32-mixed path, 64-bit for
-// FP64).  S is a power of two with qmax wmax^3 S < 2^22 (2^51) and
-// n qmax wmax^3 S < 2^31 (2^62), n the particles the block visits, qmax
-// the replica's largest |q| and wmax the largest B-spline weight of order
-// P, so no term leaves the exact range and no point's final sum overflows
-// (intermediate wrap-around of two's complement sums cancels).  Integer
-// sums do not depend on the order of the atomics: the mesh is bitwise
-// reproducible.  The quantum is 2^-es of a charge with
-// es = min(22 - e(qmax wmax^3), 31 - e(n qmax wmax^3)), about 2^-24 at
-// 2^20 ions on a 256^3 mesh (FP32-mixed) and 2^-54 in FP64.
-constexpr int kOwnEdge = 16;  // owned mesh points per dimension (multiple of 4 and 8)
-constexpr int kOwnWarps = 8;  // warps per owner block
-constexpr int kOwnChunk = 128; // particles whose records are staged at a time
-constexpr int kOwnSkip = -1;   // staged particle whose stencil misses the block
+// Fixed point: a term v = q wx wy wz becomes t = rint(v S) by one FP64 FMA
+// with the magic constant 1.5 * 2^52 (the bits of the sum are those of the
+// constant plus t while |t| < 2^51) and is added with one integer atomic:
+// FP32-mixed path, the low 32 bits (the constant's low word is zero, so the
+// word is t modulo 2^32, and a tile point's sum is exact modulo 2^32); FP64
+// path, the 64-bit t.  S is a power of two with n qmax wmax^3 S < 2^31
+// (FP32-mixed) or < 2^62 and qmax wmax^3 S < 2^51 (FP64), n the particles of
+// the super-brick, qmax the replica's largest |q|, wmax the largest B-spline
+// weight of order P: no term leaves the exact range and no tile point's
+// final sum overflows (wrap-around of intermediate two's complement sums
+// cancels).  Integer sums do not depend on the order of the atomics; the
+// quantum 1/S is about 2^-25 of a charge at 2^20 ions on a 256^3 mesh
+// (FP32-mixed) and 2^-56 in FP64, and each tile point is rounded once to
+// the working precision before it is added to the mesh.
+constexpr int kSbEdge = 16;   // corner positions per dimension of a super-brick (multiple of 4 and 8)
+constexpr int kSbWarps = 8;   // warps per super-brick block
+constexpr int kSbChunk = 64;  // particles whose records are staged at a time
 
 // Largest cardinal B-spline weight of order P over dist in [-1/2, 1/2],
 // rounded up (1, 1, 3/4, 2/3, 115/192, 11/20, 0.51102...).
@@ -197,39 +202,45 @@ template <int P> __host__ __device__ constexpr double bspline_wmax() {
   return P <= 2 ? 1.0 : P == 3 ? 0.7501 : P == 4 ? 0.6668 : P == 5 ? 0.5991 : P == 6 ? 0.5501 : 0.5112;
 }
 
-template <typename Real> struct OwnWord;
-template <> struct OwnWord<float> {
-  using type = int;
-  static constexpr int term_bits = 22;
+template <typename Real> struct SbWord;
+template <> struct SbWord<float> {
+  using type = unsigned;
   static constexpr int sum_bits = 31;
 };
-template <> struct OwnWord<double> {
+template <> struct SbWord<double> {
   using type = unsigned long long;
-  static constexpr int term_bits = 51;
   static constexpr int sum_bits = 62;
 };
-__device__ inline int own_fixed(float a, float b) {
-  return __float_as_int(fmaf(a, b, 12582912.0f)) - 0x4B400000;
+constexpr int kSbTermBits = 51;
+// t = rint(a b) for |a b| < 2^51, added modulo 2^32 (low word of the FMA
+// with the magic constant) or as a 64-bit integer
+__device__ inline void sb_add(unsigned *p, double a, double b) {
+  double const r = fma(a, b, 6755399441055744.0); // 1.5 * 2^52
+  atomicAdd(p, static_cast<unsigned>(__double2loint(r)));
 }
-__device__ inline unsigned long long own_fixed(double a, double b) {
-  return static_cast<unsigned long long>(__double_as_longlong(fma(a, b, 6755399441055744.0))) -
-         0x4338000000000000ull;
+__device__ inline void sb_add(unsigned long long *p, double a, double b) {
+  double const r = fma(a, b, 6755399441055744.0);
+  atomicAdd(p, static_cast<unsigned long long>(__double_as_longlong(r)) - 0x4338000000000000ull);
 }
-__device__ inline float own_value(int v, float inv_s) { return static_cast<float>(v) * inv_s; }
-__device__ inline double own_value(unsigned long long v, double inv_s) {
+__device__ inline float sb_value(unsigned v, float inv_s) {
+  return static_cast<float>(static_cast<int>(v)) * inv_s;
+}
+__device__ inline double sb_value(unsigned long long v, double inv_s) {
   return static_cast<double>(static_cast<long long>(v)) * inv_s;
 }
 
-// Strides of the owner tile [x][y][z] (z contiguous, words of WB bytes):
-// the smallest y stride >= kOwnEdge and x stride >= kOwnEdge * (y stride)
-// for which the lanes of one shared-memory wavefront (128 bytes: 32 lanes of
+// Tile edge of a super-brick for order P.
+template <int P> __host__ __device__ constexpr int sb_tile_edge() { return kSbEdge + P - 1; }
+// Strides of the tile [x][y][z] (z contiguous, words of WB bytes): the
+// smallest y stride >= the tile edge and x stride >= edge * (y stride) for
+// which the lanes of one shared-memory wavefront (128 bytes: 32 lanes of
 // 4-byte words, 16 of 8-byte words), one (x, y) stencil row each (row
 // r = lane + 32 q, x = r / P, y = r % P), hit distinct banks.
-template <int P, int WB> __host__ __device__ constexpr TileStrides own_strides() {
-  constexpr int E = kOwnEdge;
+template <int P, int WB> __host__ __device__ constexpr TileStrides sb_strides() {
+  constexpr int TE = sb_tile_edge<P>();
   constexpr int L = 128 / WB;
-  for (int sy = E; sy < E + L; ++sy)
-    for (int sx = E * sy; sx < E * sy + 2 * L; ++sx) {
+  for (int sy = TE; sy < TE + L; ++sy)
+    for (int sx = TE * sy; sx < TE * sy + 2 * L; ++sx) {
       bool ok = true;
       for (int r0 = 0; r0 < P * P && ok; r0 += L) {
         unsigned long long used = 0;
@@ -245,103 +256,73 @@ template <int P, int WB> __host__ __device__ constexpr TileStrides own_strides()
       if (ok)
         return TileStrides{sy, sx};
     }
-  return TileStrides{E, E * E};
+  return TileStrides{TE, TE * TE};
 }
-template <typename Real, int P> __host__ __device__ constexpr size_t own_tile_bytes() {
-  using W = typename OwnWord<Real>::type;
-  return (sizeof(W) * kOwnEdge * static_cast<size_t>(own_strides<P, sizeof(W)>().sx) + 15) / 16 *
-         16;
+template <typename Real, int P> __host__ __device__ constexpr size_t sb_tile_bytes() {
+  using W = typename SbWord<Real>::type;
+  return (sizeof(W) * sb_tile_edge<P>() * static_cast<size_t>(sb_strides<P, sizeof(W)>().sx) +
+          15) / 16 * 16;
 }
-template <typename Real, int P> __host__ __device__ constexpr size_t own_smem() {
-  return own_tile_bytes<Real, P>() + sizeof(Real) * kOwnChunk * wstride<P, 4>() +
-         sizeof(int) * kOwnChunk;
+// shared memory: tile, staged weight records, per staged particle its z
+// weights times S in FP64 (8 slots) and its tile offset
+template <typename Real, int P> __host__ __device__ constexpr size_t sb_smem() {
+  return sb_tile_bytes<Real, P>() + sizeof(Real) * kSbChunk * wstride<P, 4>() +
+         sizeof(double) * 8 * kSbChunk + sizeof(int) * kSbChunk;
 }
-
-// Sort bricks (per dimension) whose corners can reach the owned points
-// [o, o + ext): corners in [o - (P-1), o + ext) modulo M.  Corners are
-// folded into [0, M), so a span reaching below 0 is the two corner ranges
-// [lo + M, M) and [0, o + ext) (M need not be a multiple of B); the bricks
-// are [a0, a0 + n0) and [a1, a1 + n1) (n1 = 0 when one range suffices, all
-// nb bricks when the ranges meet).
-struct BrickSpan {
-  int a0, n0, a1, n1;
-};
-__device__ inline BrickSpan own_brick_span(int o, int ext, int P, int B, int M, int nb) {
-  int const lo = o - (P - 1), hi = o + ext; // hi <= M, lo + M >= 1 (P <= M)
-  if (lo >= 0)
-    return BrickSpan{lo / B, (hi - 1) / B - lo / B + 1, 0, 0};
-  int const w0 = (lo + M) / B, h1 = (hi - 1) / B;
-  if (w0 <= h1)
-    return BrickSpan{0, nb, 0, 0};
-  return BrickSpan{w0, nb - w0, 0, h1 + 1};
-}
-
-// Runs of the owner-block table: at most (bricks per column span)^2 (x, y)
-// brick columns, each with at most two contiguous z runs.
-constexpr int kOwnMaxRuns = 128;
+// sort-brick runs of a super-brick: (kSbEdge / B)^2 brick columns, one
+// contiguous z run each
+constexpr int kSbMaxRuns = (kSbEdge / 4) * (kSbEdge / 4);
 
 template <typename Real, int P>
-__global__ void __launch_bounds__(32 * kOwnWarps)
-k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owners,
-                 const int *__restrict__ start, const Real *__restrict__ W,
-                 const int *__restrict__ s_key, const unsigned *__restrict__ qmax_bits,
-                 Real *__restrict__ rho, int *__restrict__ err) {
-  using Word = typename OwnWord<Real>::type;
+__global__ void __launch_bounds__(32 * kSbWarps, sizeof(Real) == 4 ? 4 : 1)
+k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, int nsb,
+                const int *__restrict__ start, const Real *__restrict__ W,
+                const int *__restrict__ s_key, const unsigned *__restrict__ qmax_bits,
+                Real *__restrict__ rho, int *__restrict__ err) {
+  using Word = typename SbWord<Real>::type;
   constexpr int R = 4;
   constexpr int WS = wstride<P, R>();
   constexpr int WZ = wz_off<P, R>();
   constexpr int P2 = P * P;
   constexpr int NQ = (P2 + 31) / 32;
-  constexpr int NT = 32 * kOwnWarps;
-  constexpr int E = kOwnEdge;
-  constexpr int B = brick_edge<P>(), B3 = B * B * B;
+  constexpr int NT = 32 * kSbWarps;
+  constexpr int E = kSbEdge;
+  constexpr int TE = sb_tile_edge<P>();
+  constexpr int B = brick_edge<P>(), B3 = B * B * B, NBS = E / B;
   constexpr int LB = (B == 4) ? 2 : 3;
-  constexpr TileStrides TS = own_strides<P, sizeof(Word)>();
+  constexpr TileStrides TS = sb_strides<P, sizeof(Word)>();
   constexpr int SY = TS.sy, SX = TS.sx;
-  constexpr int TW = static_cast<int>(own_tile_bytes<Real, P>() / sizeof(Word));
-  constexpr int CH = kOwnChunk;
-  static_assert(2 * ((E + P - 1 + B - 1) / B + 1) * ((E + P - 1 + B - 1) / B + 1) <= kOwnMaxRuns,
-                "run table too small");
+  constexpr int TW = static_cast<int>(sb_tile_bytes<Real, P>() / sizeof(Word));
+  constexpr int CH = kSbChunk;
+  static_assert(NBS * NBS <= kSbMaxRuns, "run table too small");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bar;
-  __shared__ int s_r0[kOwnMaxRuns], s_r1[kOwnMaxRuns], s_rb[kOwnMaxRuns];
-  __shared__ long long s_count;
+  __shared__ int s_r0[kSbMaxRuns], s_r1[kSbMaxRuns];
+  __shared__ int s_count;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  if (static_cast<int>(blockIdx.x) >= nsb)
+    return; // whole block
   Word *tile = reinterpret_cast<Word *>(smem_raw);
-  Real *rec = reinterpret_cast<Real *>(smem_raw + own_tile_bytes<Real, P>());
-  int *roff = reinterpret_cast<int *>(rec + CH * WS);
+  Real *rec = reinterpret_cast<Real *>(smem_raw + sb_tile_bytes<Real, P>());
+  double *wzd = reinterpret_cast<double *>(rec + CH * WS);
+  int *toff = reinterpret_cast<int *>(wzd + 8 * CH);
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  int2 const ow = owners[blockIdx.x];
-  RepGeom const &G = reps[ow.x];
+  int2 const sb = sbs[blockIdx.x];
+  RepGeom const &G = reps[sb.x];
   int const M0 = G.mesh[0], M1 = G.mesh[1], M2 = G.mesh[2];
   int const no1 = (M1 + E - 1) / E, no2 = (M2 + E - 1) / E;
-  int const o0 = (ow.y / (no1 * no2)) * E, o1 = ((ow.y / no2) % no1) * E, o2 = (ow.y % no2) * E;
-  int const e0 = min(E, M0 - o0), e1 = min(E, M1 - o1), e2 = min(E, M2 - o2);
-  int const nb0 = G.nbx, nb1 = G.nby, nb2 = G.nbz;
-  // fast geometry: a stencil meets the owned interval at most once per axis
-  bool const fast = (M0 >= e0 + P - 1) && (M1 >= e1 + P - 1) && (M2 >= e2 + P - 1);
-  BrickSpan const sx = own_brick_span(o0, e0, P, B, M0, nb0);
-  BrickSpan const sy = own_brick_span(o1, e1, P, B, M1, nb1);
-  BrickSpan const sz = own_brick_span(o2, e2, P, B, M2, nb2);
-  // run table: column t = (ix, iy) of the x and y brick lists gives runs 2t
-  // and 2t + 1, its two z brick ranges (the second possibly empty); s_rb
-  // packs the column's brick coordinates and the run's first z brick
-  int const cy = sy.n0 + sy.n1;
-  int const ncol = (sx.n0 + sx.n1) * cy;
-  {
+  int const o0 = (sb.y / (no1 * no2)) * E, o1 = ((sb.y / no2) % no1) * E, o2 = (sb.y % no2) * E;
+  // the super-brick's sort bricks (fewer at the high end of a mesh that is
+  // not a multiple of kSbEdge)
+  int const bx0 = o0 / B, by0 = o1 / B, bz0 = o2 / B;
+  int const nbx = min(NBS, G.nbx - bx0), nby = min(NBS, G.nby - by0), nbz = min(NBS, G.nbz - bz0);
+  int const ncol = nbx * nby;
+  if (tid < ncol) {
     const int *st = start + G.brk_off;
-    for (int t = tid; t < ncol; t += NT) {
-      int const ix = t / cy, iy = t - ix * cy;
-      int const bx = (ix < sx.n0) ? sx.a0 + ix : sx.a1 + (ix - sx.n0);
-      int const by = (iy < sy.n0) ? sy.a0 + iy : sy.a1 + (iy - sy.n0);
-      int const col = (bx * nb1 + by) * nb2;
-      s_r0[2 * t] = st[col + sz.a0];
-      s_r1[2 * t] = st[col + sz.a0 + sz.n0];
-      s_rb[2 * t] = (bx << 20) | (by << 10) | sz.a0;
-      s_r0[2 * t + 1] = (sz.n1 > 0) ? st[col + sz.a1] : 0;
-      s_r1[2 * t + 1] = (sz.n1 > 0) ? st[col + sz.a1 + sz.n1] : 0;
-      s_rb[2 * t + 1] = (bx << 20) | (by << 10) | sz.a1;
-    }
+    int const col = ((bx0 + tid / nby) * G.nby + (by0 + tid % nby)) * G.nbz + bz0;
+    s_r0[tid] = st[col];
+    s_r1[tid] = st[col + nbz];
   }
   // zero the tile; initialise the staging barrier
   for (int t = tid; t < TW; t += NT)
@@ -350,9 +331,7 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
     mbar_init(&bar, 1);
   __syncthreads();
   if (warp == 0) {
-    long long c = 0;
-    for (int t = lane; t < 2 * ncol; t += 32)
-      c += s_r1[t] - s_r0[t];
+    int c = (lane < ncol) ? s_r1[lane] - s_r0[lane] : 0;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
       c += __shfl_xor_sync(0xffffffffu, c, off);
@@ -360,37 +339,36 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
       s_count = c;
   }
   __syncthreads();
-  long long const count = s_count;
-  float const qmax = __uint_as_float(qmax_bits[ow.x]);
-  int es = 0;
-  bool const any = (count > 0) && (qmax > 0.0f);
-  if (any) {
+  int const count = s_count;
+  float const qmax = __uint_as_float(qmax_bits[sb.x]);
+  if (count == 0 || !(qmax > 0.0f))
+    return; // nothing to add to the mesh
+  int es;
+  {
     double const unit = static_cast<double>(qmax) * bspline_wmax<P>() * bspline_wmax<P>() *
                         bspline_wmax<P>();
     int ea, eb;
     frexp(unit, &ea);
     frexp(unit * static_cast<double>(count), &eb);
-    es = min(OwnWord<Real>::term_bits - ea, OwnWord<Real>::sum_bits - eb);
+    es = min(kSbTermBits - ea, SbWord<Real>::sum_bits - eb);
     es = max(min(es, 1000), -1000);
   }
-  Real const S = static_cast<Real>(ldexp(1.0, es));
-  // per-lane (x, y) stencil row of each round
-  int qx[NQ], qy[NQ];
+  double const S = ldexp(1.0, es);
+  // per-lane (x, y) stencil row of each round and its tile offset
+  int qx[NQ], qy[NQ], qoff[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     int const r = lane + 32 * q;
     int const rr = (r < P2) ? r : 0;
     qx[q] = rr / P;
     qy[q] = rr % P;
+    qoff[q] = qx[q] * SX + qy[q] * SY;
   }
   unsigned parity = 0;
-  for (int run = 0; any && run < 2 * ncol; ++run) {
+  for (int run = 0; run < ncol; ++run) {
     int const s0 = s_r0[run], s1 = s_r1[run];
-    if (s0 >= s1)
-      continue;
-    int const rb = s_rb[run];
-    int const bx = rb >> 20, by = (rb >> 10) & 1023, bz0 = rb & 1023;
-    int const b0 = (bx * nb1 + by) * nb2 + bz0;
+    int const bx = bx0 + run / nby, by = by0 + run % nby;
+    int const b0 = (bx * G.nby + by) * G.nbz + bz0;
     for (int c0 = s0; c0 < s1; c0 += CH) {
       int const cn = min(CH, s1 - c0);
       __syncthreads(); // the previous chunk is consumed
@@ -401,27 +379,13 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
         bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
       }
       for (int j = tid; j < cn; j += NT) {
+        // corner offset inside the super-brick, [0, kSbEdge)^3
         int const sk = s_key[c0 + j];
         int const bz = bz0 + ((sk >> (3 * LB)) - b0);
         int const l = sk & (B3 - 1);
-        int const gx = bx * B + (l >> (2 * LB)), gy = by * B + ((l >> LB) & (B - 1)),
-                  gz = bz * B + (l & (B - 1));
-        int pk;
-        if (fast) {
-          // offset from the block origin, wrapped into [-(P-1), M-(P-1))
-          int dx = gx - o0, dy = gy - o1, dz = gz - o2;
-          dx += (dx < 0) ? M0 : 0;
-          dy += (dy < 0) ? M1 : 0;
-          dz += (dz < 0) ? M2 : 0;
-          dx -= (dx > M0 - P) ? M0 : 0;
-          dy -= (dy > M1 - P) ? M1 : 0;
-          dz -= (dz > M2 - P) ? M2 : 0;
-          bool const hit = (dx < e0) && (dy < e1) && (dz < e2);
-          pk = hit ? (((dx + 128) << 16) | ((dy + 128) << 8) | (dz + 128)) : kOwnSkip;
-        } else {
-          pk = (gx << 20) | (gy << 10) | gz;
-        }
-        roff[j] = pk;
+        int const dx = bx * B + (l >> (2 * LB)) - o0, dy = by * B + ((l >> LB) & (B - 1)) - o1,
+                  dz = bz * B + (l & (B - 1)) - o2;
+        toff[j] = dx * SX + dy * SY + dz;
       }
       bool const got = mbar_wait(&bar, parity);
       parity ^= 1u;
@@ -432,81 +396,107 @@ k_p3m_assign_own(const RepGeom *__restrict__ reps, const int2 *__restrict__ owne
         }
         return;
       }
-      for (int j = warp; j < cn; j += kOwnWarps) {
-        int const pk = roff[j];
-        if (pk == kOwnSkip)
-          continue;
+      // z weights of the staged records in FP64, times S
+      for (int t = tid; t < cn * P; t += NT) {
+        int const j = t / P, k = t - j * P;
+        wzd[8 * j + k] = static_cast<double>(rec[j * WS + WZ + k]) * S;
+      }
+      __syncthreads();
+      for (int j = warp; j < cn; j += kSbWarps) {
+        int const base = toff[j];
         const Real *w = rec + j * WS;
-        Real wz[P];
+        double wz[P];
 #pragma unroll
         for (int k = 0; k < P; ++k)
-          wz[k] = w[WZ + k];
-        if (fast) {
-          int const dx = ((pk >> 16) & 255) - 128, dy = ((pk >> 8) & 255) - 128,
-                    dz = (pk & 255) - 128;
+          wz[k] = wzd[8 * j + k];
 #pragma unroll
-          for (int q = 0; q < NQ; ++q) {
-            int const x = dx + qx[q], y = dy + qy[q];
-            if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(e0) &&
-                static_cast<unsigned>(y) < static_cast<unsigned>(e1)) {
-              Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
-              Word *pt = tile + x * SX + y * SY + dz;
+        for (int q = 0; q < NQ; ++q) {
+          if (lane + 32 * q < P2) {
+            double const wxy = static_cast<double>(w[qx[q]] * w[P + qy[q]]);
+            Word *pt = tile + base + qoff[q];
 #pragma unroll
-              for (int k = 0; k < P; ++k)
-                if (static_cast<unsigned>(dz + k) < static_cast<unsigned>(e2))
-                  atomicAdd(pt + k, own_fixed(wxy, wz[k]));
-            }
-          }
-        } else {
-          // small meshes: every stencil point wrapped and tested on its own
-          int const gx = (pk >> 20) & 1023, gy = (pk >> 10) & 1023, gz = pk & 1023;
-#pragma unroll
-          for (int q = 0; q < NQ; ++q) {
-            int const x = (gx + qx[q]) % M0 - o0, y = (gy + qy[q]) % M1 - o1;
-            if (lane + 32 * q < P2 && static_cast<unsigned>(x) < static_cast<unsigned>(e0) &&
-                static_cast<unsigned>(y) < static_cast<unsigned>(e1)) {
-              Real const wxy = (w[qx[q]] * w[P + qy[q]]) * S;
-              Word *pt = tile + x * SX + y * SY;
-#pragma unroll
-              for (int k = 0; k < P; ++k) {
-                int const z = (gz + k) % M2 - o2;
-                if (static_cast<unsigned>(z) < static_cast<unsigned>(e2))
-                  atomicAdd(pt + z, own_fixed(wxy, wz[k]));
-              }
-            }
+            for (int k = 0; k < P; ++k)
+              sb_add(pt + k, wxy, wz[k]);
           }
         }
       }
     }
   }
   __syncthreads();
-  // store the owned points once (zeros for a block no charge reaches)
   Real const inv_S = static_cast<Real>(ldexp(1.0, -es));
+  // the previous colour's read-add-write has completed and is visible
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // add the tile to the mesh: real extent of the super-brick plus the stencil
+  int const ex0 = min(E, M0 - o0) + P - 1, ey = min(E, M1 - o1) + P - 1,
+            ez = min(E, M2 - o2) + P - 1;
   Real *mesh = rho + G.rm_off;
-  if (e0 == E && e1 == E && e2 == E && (M2 % 4) == 0 && (G.rm_off % 4) == 0) {
-    // four consecutive z points per thread and iteration, one vector store
-    for (int t = tid; t < E * E * (E / 4); t += NT) {
-      int const z4 = (t & 3) * 4, y = (t >> 2) & (E - 1), x = t >> 6;
-      const Word *tp = tile + x * SX + y * SY + z4;
-      Real *mp = mesh + (static_cast<long long>(o0 + x) * M1 + (o1 + y)) * M2 + o2 + z4;
-      Real v[4];
+  // a tile wider than the mesh maps two tile points onto one mesh point:
+  // add such points in separate passes (one per wrap class)
+  bool const self_wrap = (ex0 > M0) || (ey > M1) || (ez > M2);
+  int const passes = self_wrap ? 8 : 1;
+  // each thread owns fixed (y, z) slots of the tile's yz plane; loop over x
+  constexpr int NS = (TE * TE + NT - 1) / NT;
+  int yzt[NS], yzg[NS], ycls[NS];
+  int const nyz = ey * ez;
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        v[k] = own_value(tp[k], inv_S);
-      if constexpr (sizeof(Real) == 4) {
-        *reinterpret_cast<float4 *>(mp) = make_float4(v[0], v[1], v[2], v[3]);
-      } else {
-        reinterpret_cast<double2 *>(mp)[0] = make_double2(v[0], v[1]);
-        reinterpret_cast<double2 *>(mp)[1] = make_double2(v[2], v[3]);
+  for (int k2 = 0; k2 < NS; ++k2) {
+    int const t = tid + NT * k2;
+    int const y = (t < nyz) ? t / ez : 0, z = (t < nyz) ? t - (t / ez) * ez : 0;
+    int gy = o1 + y, gz = o2 + z, cls = 0;
+    if (gy >= M1) { gy -= M1; cls |= 2; }
+    if (gy >= M1) gy -= M1;
+    if (gz >= M2) { gz -= M2; cls |= 4; }
+    if (gz >= M2) gz -= M2;
+    yzt[k2] = (t < nyz) ? y * SY + z : -1;
+    yzg[k2] = gy * M2 + gz;
+    ycls[k2] = cls;
+  }
+  if (!self_wrap) {
+    // every tile point maps to its own mesh point: issue the thread's mesh
+    // loads of XG x planes first, then the adds and stores
+    constexpr int XG = 8;
+#pragma unroll 1
+    for (int xg = 0; xg < ex0; xg += XG) {
+      Real old[XG][NS];
+#pragma unroll
+      for (int xx = 0; xx < XG; ++xx) {
+        int const x = xg + xx;
+        int gx = o0 + x;
+        gx -= (gx >= M0) ? M0 : 0;
+        long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+          if (x < ex0 && yzt[k2] >= 0)
+            old[xx][k2] = mesh[gbase + yzg[k2]];
+      }
+#pragma unroll
+      for (int xx = 0; xx < XG; ++xx) {
+        int const x = xg + xx;
+        int gx = o0 + x;
+        gx -= (gx >= M0) ? M0 : 0;
+        long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+          if (x < ex0 && yzt[k2] >= 0)
+            mesh[gbase + yzg[k2]] = old[xx][k2] + sb_value(tile[x * SX + yzt[k2]], inv_S);
       }
     }
-  } else {
-    int const nyz = e1 * e2;
-    for (int t = tid; t < e0 * nyz; t += NT) {
-      int const x = t / nyz, yz = t - x * nyz, y = yz / e2, z = yz - y * e2;
-      mesh[(static_cast<long long>(o0 + x) * M1 + (o1 + y)) * M2 + o2 + z] =
-          own_value(tile[x * SX + y * SY + z], inv_S);
+    return;
+  }
+  for (int pass = 0; pass < passes; ++pass) {
+    for (int x = 0; x < ex0; ++x) {
+      int gx = o0 + x, xcls = 0;
+      if (gx >= M0) { gx -= M0; xcls = 1; }
+      if (gx >= M0) gx -= M0;
+      long long const gbase = static_cast<long long>(gx) * M1 * M2;
+#pragma unroll
+      for (int k2 = 0; k2 < NS; ++k2) {
+        if (yzt[k2] < 0 || (xcls | ycls[k2]) != pass)
+          continue;
+        mesh[gbase + yzg[k2]] += sb_value(tile[x * SX + yzt[k2]], inv_S);
+      }
     }
+    __syncthreads();
   }
 }
 
