@@ -858,7 +858,7 @@ void Engine::build_lists(cudaStream_t st) {
   int const R = n_rep();
   for (int attempt = 0; attempt < 4; ++attempt) {
     P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, R * sizeof(int), st));
-    k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+    k_verlet_build<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                        m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
@@ -980,6 +980,11 @@ void Engine::launch_pair(double *f, bool overwrite, bool want_ev, cudaStream_t s
     // FP32-mixed: cell-relative FP32 geometry
     if (want_ev)
       k_pair_forces_rel<true><<<m_n_blk_pair, 256, smem, st>>>(
+          geom, m_blk_pair.as<int2>(), m_spf.as<float4>(), m_stype.as<int>(), m_cperm.as<int>(),
+          m_ia_d.as<PairIA>(), m_ntypes, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
+          overwrite ? 1 : 0, m_part_pair.as<double>());
+    else if (m_ntypes == 1 && m_ia[0].ia_cut != -1.0 && m_ia[0].lj_offset == 0.0)
+      k_pair_forces_rel<false, true><<<m_n_blk_pair, 256, smem, st>>>(
           geom, m_blk_pair.as<int2>(), m_spf.as<float4>(), m_stype.as<int>(), m_cperm.as<int>(),
           m_ia_d.as<PairIA>(), m_ntypes, m_nb.as<int>(), m_nb_cnt.as<int>(), f,
           overwrite ? 1 : 0, m_part_pair.as<double>());
@@ -1116,7 +1121,7 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
             m_cperm.as<int>(), m_cells, st, flag);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
                                     m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
-  k_verlet_build<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+  k_verlet_build<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
@@ -1213,9 +1218,9 @@ std::vector<int> Engine::verlet_pairs(cudaStream_t st) {
   std::vector<int> pairs;
   for (auto const &G : m_geom)
     for (long long a = G.p0; a < G.p0 + G.np; ++a)
-      for (int k = 0; k < cnt[a]; ++k) {
-        unsigned const ent =
-            static_cast<unsigned>(nbh[nb_entry(nb_base(G.nb_off, G.max_nb, a - G.p0), k)]);
+      for (int k = 0; k < nb_count(cnt[a]); ++k) {
+        unsigned const ent = static_cast<unsigned>(
+            nbh[nb_logical(nb_base(G.nb_off, G.max_nb, a - G.p0), G.max_nb, nb_count_a(cnt[a]), k)]);
         int const b = static_cast<int>(G.p0 + (ent & kNbIndexMask));
         int const i = perm[a], j = perm[b];
         if (i < j) {
@@ -1373,7 +1378,7 @@ k_elc_image_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
     bool const mt = qa != 0.0 && xa[2] > h - sl;
     if (mb || mt) {
       double F[3] = {0.0, 0.0, 0.0};
-      int const cnt = nb_cnt[a];
+      int const cnt = nb_count(nb_cnt[a]), cna = nb_count_a(nb_cnt[a]);
       const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
       for (int side = 0; side < 2; ++side) {
         if (!(side == 0 ? mb : mt))
@@ -1387,7 +1392,8 @@ k_elc_image_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
         elc_p3m_pair(G, dl * qa * qa, d, F, E);
         for (int k = 0; k < cnt; ++k) {
           long long const b =
-              G.p0 + static_cast<long long>(static_cast<unsigned>(nbp[nb_entry(0, k)]) & kNbIndexMask);
+              G.p0 + static_cast<long long>(static_cast<unsigned>(nbp[nb_logical(0, G.max_nb, cna, k)]) &
+                                            kNbIndexMask);
           int const j = perm[b];
           double const qb = qv[j];
           if (qb == 0.0)

@@ -5,6 +5,8 @@
 #include "common.cuh"
 #include "p3m_kernels.cuh"
 
+#include <type_traits>
+
 namespace p3mx {
 
 // LJ/WCA parameters of a type pair, device copy (lj.hpp, wca.hpp).
@@ -133,6 +135,26 @@ __host__ __device__ inline long long nb_base(long long nb_off, int cap, long lon
 __host__ __device__ inline long long nb_entry(long long base, int k) {
   return base + (static_cast<long long>(k >> 3) << 8) + (k & 7);
 }
+// Two classes of entries share a particle's capacity: class A (the pair's
+// LJ / WCA range plus the skin at build time: all terms) fills groups from
+// the first one up, class B (beyond it: the pair stays outside the LJ / WCA
+// cutoff until the next rebuild, as no particle moves more than skin/2, so
+// only Coulomb can act) fills groups from the last one down.  nb_cnt packs
+// nA (low 16 bits) and nB (high 16 bits).
+__host__ __device__ inline int nb_count_a(int c) { return c & 0xFFFF; }
+__host__ __device__ inline int nb_count_b(int c) { return static_cast<int>(static_cast<unsigned>(c) >> 16); }
+__host__ __device__ inline int nb_count(int c) { return nb_count_a(c) + nb_count_b(c); }
+// Group g of class B (g = 0 the first).
+__host__ __device__ inline long long nb_group_b(long long base, int cap, int g) {
+  return base + (static_cast<long long>((cap >> 3) - 1 - g) << 8);
+}
+// Entry k of the logical list [class A entries, class B entries].
+__host__ __device__ inline long long nb_logical(long long base, int cap, int na, int k) {
+  if (k < na)
+    return nb_entry(base, k);
+  int const kk = k - na;
+  return nb_group_b(base, cap, kk >> 3) + (kk & 7);
+}
 
 // Copy one group of 8 entries (32 bytes, 16-byte aligned on both sides).
 __device__ inline void store_group(int *p, const int *g) {
@@ -145,36 +167,42 @@ __device__ inline void store_group(int *p, const int *g) {
 // VerletCriterion (VerletCriterion.hpp:68-97): d^2 <= (max_cut+skin)^2 and
 // (both charged and d^2 <= (r_cut+skin)^2, or the type pair is active and
 // d^2 <= (ia_cut+skin)^2).  Stored in the warp-tiled layout above
-// (per-replica capacity G.max_nb); a replica whose capacity is exceeded
-// reports its largest count in overflow[replica].
-__global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
-                               const double4 *__restrict__ spq, const float4 *__restrict__ spf,
-                               const int *__restrict__ stype,
-                               const int *__restrict__ scell, const int *__restrict__ cstart,
-                               const PairIA *__restrict__ ia, int ntypes, long long n,
-                               int *__restrict__ nb, int *__restrict__ nb_cnt,
-                               int *__restrict__ overflow, const int *__restrict__ cond,
-                               const int *__restrict__ rflag) {
-  if (cond && !*cond)
-    return;
-  __shared__ __align__(16) int s_group[256 * 8];
-  long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (a >= n)
-    return;
+// (per-replica capacity G.max_nb), class A entries (type pair active and
+// d^2 <= (ia_cut+skin)^2) from the first group up, class B from the last
+// group down; a replica whose capacity is exceeded reports the capacity it
+// needs in overflow[replica] (nothing more is stored for that particle and
+// its counts are those of the entries stored).
+// Verlet list of one cell-sorted particle a (k_verlet_build); gbuf / gbuf_b
+// are the lane's shared-memory buffers of the class A / B group being
+// filled, s_icut the ia_cut table of the type pairs in shared memory.
+__device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__ reps,
+                                        const int *__restrict__ rep_of_sorted,
+                                        const double4 *__restrict__ spq,
+                                        const float4 *__restrict__ spf,
+                                        const int *__restrict__ stype,
+                                        const int *__restrict__ scell,
+                                        const int *__restrict__ cstart,
+                                        const PairIA *__restrict__ ia, int ntypes,
+                                        int *__restrict__ nb, int *__restrict__ nb_cnt,
+                                        int *__restrict__ overflow,
+                                        const int *__restrict__ rflag, const float *s_icut,
+                                        int *gbuf, int *gbuf_b) {
   int const rep = rep_of_sorted[a];
   if (rflag && !rflag[rep])
     return; // this replica keeps its list
   RepGeom const &G = reps[rep];
   int const max_nb = G.max_nb;
   int *nbp = nb + nb_base(G.nb_off, max_nb, a - G.p0);
-  int *gbuf = s_group + threadIdx.x * 8; // the group being filled (shared memory)
+  int const ngroups = max_nb >> 3;
   double4 const pa = spq[a];
   double const cs[3] = {G.box[0] / G.cg[0], G.box[1] / G.cg[1], G.box[2] / G.cg[2]};
   double const ics[3] = {G.cg[0] * G.box_i[0], G.cg[1] * G.box_i[1], G.cg[2] * G.box_i[2]};
   bool const small_grid = (G.cg[0] < 3) || (G.cg[1] < 3) || (G.cg[2] < 3);
-  // FP32 pre-check on the cell-relative offsets (exact geometry up to FP32
-  // rounding): candidates clearly beyond the list range are dropped before
-  // the FP64 minimum-image test, which alone decides membership
+  // FP32 geometry on the cell-relative offsets (error ~1e-6 of the cell
+  // size): a candidate whose FP32 distance lies within a relative band of
+  // 1e-4 around one of its thresholds is decided by the FP64 minimum-image
+  // test (the reference's criterion); all others are decided in FP32, which
+  // cannot differ from FP64 outside the band, so the pair set is the FP64 one
   float4 const pfa = spf[a];
   float const csf[3] = {static_cast<float>(cs[0]), static_cast<float>(cs[1]),
                         static_cast<float>(cs[2])};
@@ -186,8 +214,43 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
   double const emax2 = (G.max_cut + G.skin) * (G.max_cut + G.skin);
   float const emax2_pre = static_cast<float>(emax2 * (1.0 + 1e-4));
   double const ecoul2 = (G.coulomb_cut > 0.0) ? (G.coulomb_cut + G.skin) * (G.coulomb_cut + G.skin) : -1.0;
+  // Coulomb threshold band in FP32 (no Coulomb pairs when a is uncharged)
+  bool const coul_a = ecoul2 >= 0.0 && pa.w != 0.0;
+  float const ec_lo = static_cast<float>(ecoul2 * (1.0 - 1e-4));
+  float const ec_hi = static_cast<float>(ecoul2 * (1.0 + 1e-4));
+  float const skin_f = static_cast<float>(G.skin);
   double const Li[3] = {G.box_i[0], G.box_i[1], G.box_i[2]};
-  int count = 0;
+  int na = 0, nb_b = 0; // entries stored per class
+  int need_a = 0, need_b = 0; // entries found per class
+  // store one taken entry of class A (LJ / WCA range) or B
+  auto put = [&](int b, bool cls_a, int code) {
+    // room for the entry: class A groups [0, ceil(na'/8)) and class B
+    // groups [ngroups - ceil(nb'/8), ngroups) disjoint
+    bool const room = (need_a == na) && (need_b == nb_b) &&
+                      ((cls_a ? (na & 7) : (nb_b & 7)) != 0 ||
+                       ((na + 7) >> 3) + ((nb_b + 7) >> 3) + 1 <= ngroups);
+    if (room) {
+      int const ent = static_cast<int>(static_cast<unsigned>(b - G.p0) |
+                                       (static_cast<unsigned>(code) << kNbIndexBits));
+      if (cls_a) {
+        int const slot = na & 7;
+        gbuf[slot] = ent;
+        if (slot == 7)
+          store_group(nbp + (static_cast<long long>(na >> 3) << 8), gbuf);
+        ++na;
+      } else {
+        int const slot = nb_b & 7;
+        gbuf_b[slot] = ent;
+        if (slot == 7)
+          store_group(nbp + (static_cast<long long>(ngroups - 1 - (nb_b >> 3)) << 8), gbuf_b);
+        ++nb_b;
+      }
+    }
+    if (cls_a)
+      ++need_a;
+    else
+      ++need_b;
+  };
   // offsets per axis without duplicates for grids of size 1 or 2
   int lo[3], hi[3];
 #pragma unroll
@@ -225,43 +288,33 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
             double const d2 = d0 * d0 + d1 * d1 + d2v * d2v;
             if (d2 > emax2)
               return;
-            bool take = (ecoul2 >= 0.0 && d2 <= ecoul2 && pa.w != 0.0 && pb.w != 0.0);
-            if (!take) {
-              double const ic = ia[ta * ntypes + stype[b]].ia_cut;
-              take = (ic != -1.0) && d2 <= (ic + G.skin) * (ic + G.skin);
-            }
+            double const ic = ia[ta * ntypes + stype[b]].ia_cut;
+            bool const cls_a = (ic != -1.0) && d2 <= (ic + G.skin) * (ic + G.skin);
+            bool const take =
+                cls_a || (ecoul2 >= 0.0 && d2 <= ecoul2 && pa.w != 0.0 && pb.w != 0.0);
             if (take) {
-              if (count < max_nb) {
-                // cell offset dc of the partner's image: x_b' - x_a = dc cs +
-                // (off_b - off_a), an exact multiple of the cell size; with
-                // cells >= the list range, dc is -1, 0 or +1 per axis.  With
-                // 3 or more cells along an axis the minimum image is the image
-                // in the visited neighbour cell, so dc is the loop offset;
-                // with 1 or 2 cells it follows from the minimum-image vector.
-                int dcv[3] = {dx, dy, dz};
-                if (small_grid) {
-                  int const lb = scell[b] - static_cast<int>(G.cell_off);
-                  int const cb[3] = {lb % G.cg[0], (lb / G.cg[0]) % G.cg[1],
-                                     lb / (G.cg[0] * G.cg[1])};
-                  int const ca[3] = {c0, c1, c2};
-                  double const xa[3] = {pa.x, pa.y, pa.z}, xb[3] = {pb.x, pb.y, pb.z};
-                  double const dmi[3] = {-d0, -d1, -d2v};
+              // cell offset dc of the partner's image: x_b' - x_a = dc cs +
+              // (off_b - off_a), an exact multiple of the cell size; with
+              // cells >= the list range, dc is -1, 0 or +1 per axis.  With
+              // 3 or more cells along an axis the minimum image is the image
+              // in the visited neighbour cell, so dc is the loop offset;
+              // with 1 or 2 cells it follows from the minimum-image vector.
+              int dcv[3] = {dx, dy, dz};
+              if (small_grid) {
+                int const lb = scell[b] - static_cast<int>(G.cell_off);
+                int const cb[3] = {lb % G.cg[0], (lb / G.cg[0]) % G.cg[1],
+                                   lb / (G.cg[0] * G.cg[1])};
+                int const ca[3] = {c0, c1, c2};
+                double const xa[3] = {pa.x, pa.y, pa.z}, xb[3] = {pb.x, pb.y, pb.z};
+                double const dmi[3] = {-d0, -d1, -d2v};
 #pragma unroll
-                  for (int d = 0; d < 3; ++d)
-                    if (G.cg[d] < 3) {
-                      double const oa = xa[d] - ca[d] * cs[d], ob = xb[d] - cb[d] * cs[d];
-                      dcv[d] = static_cast<int>(rint((dmi[d] - (ob - oa)) * ics[d]));
-                    }
-                }
-                int const code = (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1);
-                int const ent = static_cast<int>(static_cast<unsigned>(b - G.p0) |
-                                                 (static_cast<unsigned>(code) << kNbIndexBits));
-                int const slot = count & 7;
-                gbuf[slot] = ent;
-                if (slot == 7)
-                  store_group(nbp + (static_cast<long long>(count >> 3) << 8), gbuf);
+                for (int d = 0; d < 3; ++d)
+                  if (G.cg[d] < 3) {
+                    double const oa = xa[d] - ca[d] * cs[d], ob = xb[d] - cb[d] * cs[d];
+                    dcv[d] = static_cast<int>(rint((dmi[d] - (ob - oa)) * ics[d]));
+                  }
               }
-              ++count;
+              put(b, cls_a, (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1));
             }
         };
         int const b_lo = cstart[cell], b_hi = cstart[cell + 1];
@@ -270,7 +323,10 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
             if (b != a)
               consider(b);
         } else {
-          // FP32 pre-check, kPre candidates per round (loads issued together)
+          int const code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+          // kPre candidates per round (loads issued together): an FP32
+          // pre-check, then for the candidates near or inside the list
+          // range the FP32 decision, or the FP64 test inside the bands
           constexpr int kPre = 8;
           for (int b0 = b_lo; b0 < b_hi; b0 += kPre) {
             float4 pf[kPre];
@@ -278,30 +334,81 @@ __global__ void __launch_bounds__(256, 3) k_verlet_build(const RepGeom *__restri
             for (int u = 0; u < kPre; ++u)
               pf[u] = (b0 + u < b_hi) ? spf[b0 + u] : pfa;
             unsigned keep = 0;
+            float r2v[kPre];
 #pragma unroll
             for (int u = 0; u < kPre; ++u) {
               float const e0 = (pfa.x - pf[u].x) + shx, e1 = (pfa.y - pf[u].y) + shy,
                           e2 = (pfa.z - pf[u].z) + shz;
-              bool const in = (b0 + u < b_hi) && (b0 + u != a) &&
-                              (e0 * e0 + e1 * e1 + e2 * e2 <= emax2_pre);
+              r2v[u] = e0 * e0 + e1 * e1 + e2 * e2;
+              bool const in = (b0 + u < b_hi) && (b0 + u != a) && (r2v[u] <= emax2_pre);
               keep |= (in ? 1u : 0u) << u;
             }
             while (keep) {
               int const u = __ffs(keep) - 1;
               keep &= keep - 1;
-              consider(b0 + u);
+              int const b = b0 + u;
+              float r2 = r2v[0];
+              float qb = pf[0].w;
+#pragma unroll
+              for (int w = 1; w < kPre; ++w) {
+                r2 = (u == w) ? r2v[w] : r2;
+                qb = (u == w) ? pf[w].w : qb;
+              }
+              float const icf = (ntypes == 1) ? s_icut[0] : s_icut[ta * ntypes + stype[b]];
+              float const it = icf + skin_f;
+              float const it2 = it * it;
+              bool const ia_on = icf != -1.f;
+              bool const a_lo = ia_on && r2 < it2 * (1.f - 1e-4f);
+              bool const a_band = ia_on && !a_lo && r2 <= it2 * (1.f + 1e-4f);
+              // Coulomb: both charged (an FP32 zero charge is checked in FP64)
+              bool const c_lo = coul_a && qb != 0.f && r2 < ec_lo;
+              bool const c_band = coul_a && r2 <= ec_hi && !c_lo;
+              if (a_band || c_band)
+                consider(b);
+              else if (a_lo || c_lo)
+                put(b, a_lo, code);
             }
           }
         }
       }
     }
   }
-  int const stored = min(count, max_nb);
-  if (stored & 7) // last partial group (entries beyond the count are never read)
-    store_group(nbp + (static_cast<long long>(stored >> 3) << 8), gbuf);
-  nb_cnt[a] = stored;
-  if (count > max_nb)
-    atomicMax(&overflow[rep], count);
+  // last partial groups (entries beyond the counts are never read)
+  if (na & 7)
+    store_group(nbp + (static_cast<long long>(na >> 3) << 8), gbuf);
+  if (nb_b & 7)
+    store_group(nbp + (static_cast<long long>(ngroups - 1 - (nb_b >> 3)) << 8), gbuf_b);
+  nb_cnt[a] = na | (nb_b << 16);
+  int const need = 8 * (((need_a + 7) >> 3) + ((need_b + 7) >> 3));
+  if (need > max_nb)
+    atomicMax(&overflow[rep], need);
+}
+
+// Verlet lists, one thread per cell-sorted particle (the 32 lanes of a warp
+// are consecutive particles: the same or adjacent cells).
+__global__ void __launch_bounds__(256, 2)
+k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
+               const double4 *__restrict__ spq, const float4 *__restrict__ spf,
+               const int *__restrict__ stype, const int *__restrict__ scell,
+               const int *__restrict__ cstart, const PairIA *__restrict__ ia, int ntypes,
+               long long n, int *__restrict__ nb, int *__restrict__ nb_cnt,
+               int *__restrict__ overflow, const int *__restrict__ cond,
+               const int *__restrict__ rflag) {
+  if (cond && !*cond)
+    return;
+  __shared__ __align__(16) int s_group[256 * 8], s_group_b[256 * 8];
+  // ia_cut of every type pair (-1: inactive) in shared memory (the skin,
+  // per replica, is added per candidate)
+  extern __shared__ float s_icut[];
+  for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
+    s_icut[k] = static_cast<float>(ia[k].ia_cut);
+  __syncthreads();
+  long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (a >= n)
+    return;
+  verlet_build_one(a, reps, rep_of_sorted, spq, spf, stype, scell, cstart, ia, ntypes, nb,
+                   nb_cnt, overflow, rflag, s_icut, s_group + threadIdx.x * 8,
+                   s_group_b + threadIdx.x * 8);
 }
 
 // A&S 7.1.26 approximation of exp(d^2) erfc(d), as the reference's real-
@@ -408,6 +515,32 @@ __device__ inline void lj_wca_sel(PairR<float> const &p, float dist, float inv_d
   }
 }
 
+// Branch-free LJ + WCA for pairs without an LJ offset (r_off = r, so the
+// LJ powers come from the same 1/r^2 as WCA's): one reciprocal square root
+// serves every term.  in_lj / in_wca select the terms by range.
+__device__ inline void lj_wca_sel_nooff(PairR<float> const &p, float dist, float inv_d2,
+                                        float &fn) {
+  {
+    float const s2 = (p.lsig * p.lsig) * inv_d2;
+    float const f6 = s2 * s2 * s2;
+    bool const in = dist < p.lcut && dist > p.lmin;
+    fn += in ? 48.f * p.leps * f6 * (f6 - 0.5f) * inv_d2 : 0.f;
+  }
+  if (p.wcut > 0.f) {
+    float const s2 = (p.wsig * p.wsig) * inv_d2;
+    float const f6 = s2 * s2 * s2;
+    bool const in = dist < p.wcut;
+    fn += in ? 48.f * p.weps * f6 * (f6 - 0.5f) * inv_d2 : 0.f;
+  }
+}
+
+// 2^x, hardware approximation (ex2.approx, relative error ~2^-22).
+__device__ inline float ex2_approx(float x) {
+  float e;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(x));
+  return e;
+}
+
 __device__ inline float rsqrt_approx(float x) {
   float r;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -431,7 +564,9 @@ __device__ inline float rsqrt_approx(float x) {
 // gathers); the geometry error is about one ulp of the cell size.  Pair
 // physics as k_pair_forces; per-particle force sums are FP32 over runs of 8
 // partners and FP64 across runs.
-template <bool EV>
+// NOOFF: one particle type whose LJ has no offset (the host checks), so the
+// LJ and WCA powers use the Coulomb term's 1/r^2 (lj_wca_sel_nooff).
+template <bool EV, bool NOOFF = false>
 __global__ void __launch_bounds__(256, EV ? 1 : 4)
 k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
                   const float4 *__restrict__ spf, const int *__restrict__ stype,
@@ -441,7 +576,7 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
                   double *__restrict__ partials) {
   using Real = float;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ float4 shift[27];
+  __shared__ float shift_x[32], shift_y[32], shift_z[32];
   PairIA *ia = reinterpret_cast<PairIA *>(smem_raw);
   for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
     ia[k] = ia_g[k];
@@ -450,9 +585,9 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
   if (threadIdx.x < 27) {
     int const c = threadIdx.x;
     int const dc[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
-    shift[c] = make_float4(static_cast<float>(-dc[0] * (G.box[0] / G.cg[0])),
-                           static_cast<float>(-dc[1] * (G.box[1] / G.cg[1])),
-                           static_cast<float>(-dc[2] * (G.box[2] / G.cg[2])), 0.f);
+    shift_x[c] = static_cast<float>(-dc[0] * (G.box[0] / G.cg[0]));
+    shift_y[c] = static_cast<float>(-dc[1] * (G.box[1] / G.cg[1]));
+    shift_z[c] = static_cast<float>(-dc[2] * (G.box[2] / G.cg[2]));
   }
   __syncthreads();
   long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
@@ -460,108 +595,132 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
 #pragma unroll
   for (int k = 0; k < (EV ? 20 : 1); ++k)
     ev[k] = 0.0;
-  if (a < G.p0 + G.np) {
-    float4 const pa = spf[a];
-    int const ta = stype[a];
-    Real const alpha = static_cast<Real>(G.alpha);
-    Real const r_cut = static_cast<Real>(G.r_cut);
-    Real const two_a_sqrt_pi_i = static_cast<Real>(2.0 * G.alpha / sqrt(kPi));
-    Real const pref_qa = static_cast<Real>(G.prefactor) * pa.w;
-    bool const one_type = (ntypes == 1);
-    PairR<Real> const p0(ia[0]);
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    int const cnt = nb_cnt[a];
-    const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
-    long long const base0 = G.p0;
-    // the particle itself with the zero cell offset (code 13: dc = 0)
-    unsigned const self_ent =
-        static_cast<unsigned>(a - G.p0) | (13u << kNbIndexBits);
-    for (int k0 = 0; k0 < cnt; k0 += 8) {
-      // one group of 8 entries: two 16-byte loads
-      const int4 *gp = reinterpret_cast<const int4 *>(nbp + (static_cast<long long>(k0 >> 3) << 8));
-      int4 const g0 = gp[0], g1 = gp[1];
-      unsigned const ent[8] = {static_cast<unsigned>(g0.x), static_cast<unsigned>(g0.y),
-                               static_cast<unsigned>(g0.z), static_cast<unsigned>(g0.w),
-                               static_cast<unsigned>(g1.x), static_cast<unsigned>(g1.y),
-                               static_cast<unsigned>(g1.z), static_cast<unsigned>(g1.w)};
-      int const kn = min(8, cnt - k0);
-#pragma unroll
-      for (int h = 0; h < 8; h += 4) {
-        // entries past the count stand for the particle itself (zero
-        // distance: no term passes its range test), so no lane branches on
-        // the count; the partners' positions, four gathers in flight
-        unsigned eu[4];
-        float4 pbv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          eu[u] = (h + u < kn) ? ent[h + u] : self_ent;
-          pbv[u] = spf[base0 + (eu[u] & kNbIndexMask)];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          unsigned const e = eu[u];
-          int const code = static_cast<int>(e >> kNbIndexBits);
-          float4 const pb = pbv[u];
-          float4 const sh = shift[code];
-          Real const d0 = (pa.x - pb.x) + sh.x;
-          Real const d1 = (pa.y - pb.y) + sh.y;
-          Real const d2v = (pa.z - pb.z) + sh.z;
-          Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
-          Real const inv_d = rsqrt_approx(dist2);
-          Real const dist = dist2 * inv_d;
-          bool const pos = dist2 > Real(0);
-          // Coulomb, evaluated for every entry and selected
-          Real const adist = alpha * dist;
-          Real const ex = exp_r(-adist * adist);
-          Real const t = rcp_r(Real(1) + Real(0.3275911) * adist);
-          Real const asp =
-              t * (Real(0.254829592) +
-                   t * (Real(-0.284496736) +
-                        t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
-          Real const erfc_part_ri = asp * inv_d;
-          Real const pq = pref_qa * pb.w;
-          bool const in_c = pos && dist < r_cut;
-          Real const fc = in_c ? pq * (ex * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d)) : Real(0);
-          Real ec = Real(0);
-          if constexpr (EV)
-            ec = in_c ? pq * erfc_part_ri * ex : Real(0);
-          Real fn = Real(0), en = Real(0);
-          if (one_type) {
-            if (p0.active)
-              lj_wca_sel(p0, dist, inv_d, fn, en);
-          } else {
-            int const b = static_cast<int>(base0 + (e & kNbIndexMask));
-            PairR<Real> const p(ia[ta * ntypes + stype[b]]);
-            if (p.active)
-              lj_wca_sel(p, dist, inv_d, fn, en);
-          }
-          fn = pos ? fn : Real(0);
-          en = pos ? en : Real(0);
-          Real const ft = fc + fn;
-          sx += ft * d0;
-          sy += ft * d1;
-          sz += ft * d2v;
-          if constexpr (EV) {
-            double const dd[3] = {d0, d1, d2v};
-            ev[0] += 0.5 * double(ec);
-            ev[1] += 0.5 * double(en);
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-              for (int c = 0; c < 3; ++c) {
-                ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
-                ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
-              }
-          }
-        }
+  bool const active = a < G.p0 + G.np;
+  // groups of 8 entries: class A first (all terms), then class B
+  // (Coulomb only); the loop runs to the warp's largest group count so that
+  // the vote on LJ stays warp-wide
+  int na = 0, nbb = 0;
+  if (active) {
+    int const c = nb_cnt[a];
+    na = nb_count_a(c);
+    nbb = nb_count_b(c);
+  }
+  int const ga = (na + 7) >> 3, gt = ga + ((nbb + 7) >> 3);
+  int const gmax = __reduce_max_sync(0xffffffffu, gt);
+  float4 const pa = active ? spf[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int const ta = active ? stype[a] : 0;
+  Real const rc2 = static_cast<Real>(G.r_cut * G.r_cut);
+  Real const two_a_sqrt_pi_i = static_cast<Real>(2.0 * G.alpha / sqrt(kPi));
+  Real const pref_qa = static_cast<Real>(G.prefactor) * pa.w;
+  // exp(-(alpha r)^2) = 2^(c_exp r^2); A&S t = 1 / (1 + p alpha r)
+  Real const c_exp = static_cast<Real>(-G.alpha * G.alpha * 1.4426950408889634);
+  Real const p_alpha = static_cast<Real>(0.3275911 * G.alpha);
+  bool const one_type = (ntypes == 1);
+  PairR<Real> const p0(ia[0]);
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  const int *nbp = nb + nb_base(G.nb_off, G.max_nb, active ? a - G.p0 : 0);
+  int const ngroups = G.max_nb >> 3;
+  long long const base0 = G.p0;
+  // the particle itself with the zero cell offset (code 13: dc = 0)
+  unsigned const self_ent = static_cast<unsigned>(active ? a - G.p0 : 0) | (13u << kNbIndexBits);
+  // one entry: Coulomb always, LJ / WCA when the group may hold class A
+  auto entry = [&](auto lj, unsigned e, float4 pb, float &sx, float &sy, float &sz) {
+    int const code = static_cast<int>(e >> kNbIndexBits);
+    Real const d0 = (pa.x - pb.x) + shift_x[code];
+    Real const d1 = (pa.y - pb.y) + shift_y[code];
+    Real const d2v = (pa.z - pb.z) + shift_z[code];
+    Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
+    Real const inv_d = rsqrt_approx(dist2);
+    Real const dist = dist2 * inv_d;
+    bool const pos = dist2 > Real(0);
+    Real const ex = ex2_approx(c_exp * dist2);
+    Real const t = rcp_r(fmaf(p_alpha, dist, Real(1)));
+    Real const asp =
+        t * (Real(0.254829592) +
+             t * (Real(-0.284496736) +
+                  t * (Real(1.421413741) + t * (Real(-1.453152027) + t * Real(1.061405429)))));
+    Real const erfc_part_ri = asp * inv_d;
+    Real const pq = pref_qa * pb.w;
+    bool const in_c = pos && dist2 < rc2;
+    Real const fc =
+        in_c ? (pq * ex) * (erfc_part_ri + two_a_sqrt_pi_i) * (inv_d * inv_d) : Real(0);
+    Real fn = Real(0), en = Real(0);
+    if constexpr (decltype(lj)::value) {
+      if constexpr (NOOFF) {
+        lj_wca_sel_nooff(p0, dist, inv_d * inv_d, fn);
+      } else if (one_type) {
+        if (p0.active)
+          lj_wca_sel(p0, dist, inv_d, fn, en);
+      } else {
+        int const b = static_cast<int>(base0 + (e & kNbIndexMask));
+        PairR<Real> const p(ia[ta * ntypes + stype[b]]);
+        if (p.active)
+          lj_wca_sel(p, dist, inv_d, fn, en);
       }
-      // FP32 sums of this group into the FP64 accumulators
-      fx += static_cast<double>(sx);
-      fy += static_cast<double>(sy);
-      fz += static_cast<double>(sz);
-      sx = sy = sz = 0.f;
+      fn = pos ? fn : Real(0);
+      en = pos ? en : Real(0);
     }
+    Real const ft = fc + fn;
+    sx += ft * d0;
+    sy += ft * d1;
+    sz += ft * d2v;
+    if constexpr (EV) {
+      Real const ec = in_c ? pq * erfc_part_ri * ex : Real(0);
+      double const dd[3] = {d0, d1, d2v};
+      ev[0] += 0.5 * double(ec);
+      ev[1] += 0.5 * double(en);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ev[2 + 3 * r + c] += 0.5 * double(fc) * dd[r] * dd[c];
+          ev[11 + 3 * r + c] += 0.5 * double(fn) * dd[r] * dd[c];
+        }
+    }
+  };
+  auto group = [&](auto lj, int v) {
+    // the lane's group v: class A group v, or class B group v - ga
+    bool const in_a = v < ga;
+    int const grp = in_a ? v : ngroups - 1 - (v - ga);
+    int const kn = in_a ? min(8, na - 8 * v) : min(8, nbb - 8 * (v - ga));
+    const int4 *gp = reinterpret_cast<const int4 *>(nbp + (static_cast<long long>(grp) << 8));
+    int4 const g0 = gp[0], g1 = gp[1];
+    unsigned const ent[8] = {static_cast<unsigned>(g0.x), static_cast<unsigned>(g0.y),
+                             static_cast<unsigned>(g0.z), static_cast<unsigned>(g0.w),
+                             static_cast<unsigned>(g1.x), static_cast<unsigned>(g1.y),
+                             static_cast<unsigned>(g1.z), static_cast<unsigned>(g1.w)};
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+    for (int h = 0; h < 8; h += 4) {
+      // entries past the count stand for the particle itself (zero
+      // distance: no term passes its range test), so no lane branches on
+      // the count; the partners' positions, four gathers in flight
+      unsigned eu[4];
+      float4 pbv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        eu[u] = (h + u < kn) ? ent[h + u] : self_ent;
+        pbv[u] = spf[base0 + (eu[u] & kNbIndexMask)];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        entry(lj, eu[u], pbv[u], sx, sy, sz);
+    }
+    // FP32 sums of this group into the FP64 accumulators
+    fx += static_cast<double>(sx);
+    fy += static_cast<double>(sy);
+    fz += static_cast<double>(sz);
+  };
+  for (int v = 0; v < gmax; ++v) {
+    bool const any_a = __any_sync(0xffffffffu, active && v < ga);
+    if (active && v < gt) {
+      if (any_a)
+        group(std::true_type{}, v);
+      else
+        group(std::false_type{}, v);
+    }
+  }
+  if (active) {
     int const i = perm[a];
     if (overwrite) {
       f[3 * i + 0] = fx;
@@ -625,17 +784,20 @@ k_pair_forces(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     bool const one_type = (ntypes == 1);
     PairR<Real> const p0(ia[0]);
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    int const cnt = nb_cnt[a];
+    int const cw = nb_cnt[a];
+    int const cnt = nb_count(cw), cna = nb_count_a(cw);
     const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
     int const base0 = static_cast<int>(G.p0);
     int b_next =
-        (cnt > 0) ? base0 + static_cast<int>(static_cast<unsigned>(nbp[0]) & kNbIndexMask) : 0;
+        (cnt > 0) ? base0 + static_cast<int>(static_cast<unsigned>(nbp[nb_logical(0, G.max_nb, cna, 0)]) &
+                                             kNbIndexMask)
+                  : 0;
     double4 p_next = (cnt > 0) ? spq[b_next] : pa;
     for (int k = 0; k < cnt; ++k) {
       int const b = b_next;
       double4 const pb = p_next;
       if (k + 1 < cnt) {
-        b_next = base0 + static_cast<int>(static_cast<unsigned>(nbp[nb_entry(0, k + 1)]) &
+        b_next = base0 + static_cast<int>(static_cast<unsigned>(nbp[nb_logical(0, G.max_nb, cna, k + 1)]) &
                                           kNbIndexMask);
         p_next = spq[b_next];
       }

@@ -135,6 +135,98 @@ def _handle_compute(cls, box, pos, q, mesh, cao, alpha, r_cut, pref=1.0):
     return act, f, e[0], v.reshape(3, 3), mesh_out
 
 
+@pytest.mark.parametrize("mesh_off", [0.25, 0.5, 0.75, (0.1, 0.6, 0.9)])
+@pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
+def test_mesh_off_vs_oracle(mesh_off, cls, rtol):
+    """Non-default mesh offsets (P3MParameters::mesh_off, p3m/common.hpp:
+    156-171: grid position pos * ai - mesh_off, CA-mesh origin ld_pos):
+    charge mesh and k-space forces, energy and virial equal the oracle's."""
+    box = np.array([11.0, 10.0, 12.0])
+    rng = np.random.default_rng(17)
+    n = 300
+    pos = rng.uniform(0.0, 1.0, (n, 3)) * box
+    q = rng.choice([-1.0, 1.0], n)
+    q -= q.mean()
+    mesh = [22, 20, 24]
+    off = np.broadcast_to(np.asarray(mesh_off, dtype=float), (3,))
+    act = cls(prefactor=1.3, accuracy=1e-4, mesh=mesh, cao=5, alpha=1.2, r_cut=2.5,
+              mesh_off=list(off), tune=False, check_neutrality=False)
+    act._set_system(box, 0.4, (True, True, True))
+    act._activate(pos, q)
+    lib = _lib.load()
+    f = np.zeros((n, 3))
+    e = np.zeros(1)
+    v = np.zeros(9)
+    rc = lib.p3mx_long_range(act._handle, n, _lib.dptr(_lib.as_f64(pos)), _lib.dptr(_lib.as_f64(q)),
+                             _lib.dptr(f), e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             _lib.P3MX_FORCES | _lib.P3MX_ENERGY | _lib.P3MX_VIRIAL |
+                             _lib.P3MX_OVERWRITE, None)
+    _lib.check(rc, act._handle)
+    mesh_gpu = np.zeros(int(np.prod(mesh)))
+    _lib.check(lib.p3mx_copy_mesh(act._handle, mesh_gpu.ctypes.data_as(
+        ctypes.POINTER(ctypes.c_double)), mesh_gpu.size), act._handle)
+    p = O.make_params(box, mesh, 5, 1.2, 2.5, 1.3, mesh_off=off)
+    fo, eo, vo, rho = O.p3m_kspace(p, pos, q, want_mesh=True)
+    np.testing.assert_allclose(mesh_gpu, rho.ravel(), atol=rtol * np.abs(rho).max() * 10, rtol=0)
+    np.testing.assert_allclose(f, fo, atol=rtol * np.abs(fo).max(), rtol=0)
+    assert abs(e[0] - eo) <= rtol * abs(eo) * 10 + 1e-12
+    np.testing.assert_allclose(v.reshape(3, 3), vo, atol=rtol * np.abs(vo).max() * 10, rtol=0)
+
+
+@pytest.mark.parametrize("eps", [0.5, 1.0, 80.0])
+def test_fp32_mixed_dipole_correction_vs_oracle(eps):
+    """The FP32-mixed actor with a finite dielectric (epsilon != metallic:
+    the dipole force and energy terms of p3m.cpp:481-488, 540-547, 575-577)
+    against the FP64 oracle, element-wise at the FP32-mixed tolerance."""
+    box = 14.0
+    pos, q = jittered_lattice(8, box, 0.3, seed=31)  # 512 ions
+    pos[:40, 2] += 2.0  # a net dipole moment
+    s = make_system([box] * 3, pos, q)
+    s.electrostatics.solver = P3MGPU(prefactor=1.0, accuracy=1e-4, mesh=32, cao=6, r_cut=3.0,
+                                     alpha=1.1, epsilon=eps, tune=False)
+    s.integrator.run(0)
+    f = s.part.all().f
+    e = s.analysis.energy()["coulomb"]
+    fo, eo, _ = oracle_total([box] * 3, pos, q, 32, 6, 1.1, 3.0, 1.0, epsilon=eps)
+    np.testing.assert_allclose(f, fo, atol=FP32_RTOL * np.abs(fo).max(), rtol=0)
+    assert abs(e - eo) <= FP32_RTOL * abs(eo) + 1e-9
+
+
+def test_mixed_observables_vs_oracle():
+    """P3MX_MIXED_OBSERVABLES: energies and virials of the FP32-mixed actor
+    from its own FP32 kernels (not the default FP64 observables engine)
+    against the FP64 oracle, at the FP32-mixed tolerance (x 10 for sums)."""
+    box = 13.0
+    pos, q = jittered_lattice(8, box, 0.25, seed=41)
+    act = P3MGPU(prefactor=1.7, accuracy=1e-4, mesh=32, cao=5, r_cut=3.0, alpha=1.2,
+                 tune=False)
+    s = make_system([box] * 3, pos, q)
+    s.electrostatics.solver = act
+    lib = _lib.load()
+    n = len(q)
+    f = np.zeros((n, 3))
+    e3 = np.zeros(3)
+    v27 = np.zeros(27)
+    flags = (_lib.P3MX_FORCES | _lib.P3MX_ENERGY | _lib.P3MX_VIRIAL | _lib.P3MX_OVERWRITE |
+             _lib.P3MX_MIXED_OBSERVABLES)
+    rc = lib.p3mx_forces(act._handle, n, _lib.dptr(pos), _lib.dptr(q), None, _lib.dptr(f),
+                         e3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                         v27.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), flags, None)
+    _lib.check(rc, act._handle)
+    p = O.make_params([box] * 3, 32, 5, 1.2, 3.0, 1.7)
+    fk, ek, vk = O.p3m_kspace(p, pos, q)
+    fr, er, vc, _ = O.short_range(p, pos, q)
+    # energy3: real-space Coulomb, k-space, non-bonded; virial27: the same
+    assert abs(e3[1] - ek) <= FP32_RTOL * 10 * abs(ek)
+    assert abs(e3[0] - er[0]) <= FP32_RTOL * 10 * abs(er[0])
+    np.testing.assert_allclose(v27[9:18].reshape(3, 3), vk, atol=FP32_RTOL * 10 * np.abs(vk).max(),
+                               rtol=0)
+    np.testing.assert_allclose(v27[0:9].reshape(3, 3), vc, atol=FP32_RTOL * 10 * np.abs(vc).max(),
+                               rtol=0)
+    np.testing.assert_allclose(f, fk + fr, atol=FP32_RTOL * np.abs(fk + fr).max(), rtol=0)
+
+
 @pytest.mark.parametrize("cao", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("cls,rtol", [(P3M, FP64_RTOL), (P3MGPU, FP32_RTOL)])
 def test_kspace_elementwise_vs_oracle(cao, cls, rtol):
@@ -190,6 +282,55 @@ def test_resort_rebuilds_to_the_same_forces(cls):
     s.cell_system.resort()
     s.integrator.run(0)
     assert np.array_equal(s.part.all().f, f1)
+
+
+def test_fp32_real_space_pair_force_vs_fp64_formula():
+    """The FP32 real-space Coulomb force of CoulombP3M::pair_force
+    (p3m.hpp:146-163: exp(-(alpha r)^2) (AS(alpha r)/r + 2 alpha/sqrt(pi)) / r^2
+    times q1 q2 d, with the A&S 7.1.26 exp(x^2) erfc(x) of AS_erfc_part.hpp)
+    against the same formula in FP64, over r in (0.2, r_cut): isolated pairs,
+    one per lattice site of a large box, through p3mx_short_range.  The FP32
+    kernel forms exp(-(alpha r)^2) as 2^(-alpha^2 log2(e) r^2) with the
+    hardware ex2 approximation and uses approximate reciprocals; its force
+    stays within 4e-6 of the FP64 value relative to the force at that r, and
+    the forces on the two particles of a pair cancel to round-off."""
+    alpha, r_cut = 0.87, 3.5
+    n_side, spacing = 10, 8.0  # pairs farther apart than r_cut + skin
+    box = n_side * spacing
+    rng = np.random.default_rng(5)
+    n_pairs = n_side ** 3
+    r = np.linspace(0.2, r_cut - 0.01, n_pairs)
+    u = rng.normal(size=(n_pairs, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    site = (np.stack(np.meshgrid(*[np.arange(n_side)] * 3, indexing="ij"), -1).reshape(-1, 3)
+            + 0.5) * spacing
+    pos = np.empty((2 * n_pairs, 3))
+    pos[0::2] = site - 0.5 * r[:, None] * u
+    pos[1::2] = site + 0.5 * r[:, None] * u
+    qa = rng.choice([-2.0, -1.0, 1.0, 2.0], n_pairs)
+    q = np.empty(2 * n_pairs)
+    q[0::2] = qa
+    q[1::2] = -qa
+    act = P3MGPU(prefactor=1.0, accuracy=1e-4, mesh=32, cao=5, alpha=alpha, r_cut=r_cut,
+                 tune=False)
+    act._set_system(np.array([box] * 3), 0.4, (True, True, True))
+    act._activate(pos, q)
+    lib = _lib.load()
+    f = np.zeros((2 * n_pairs, 3))
+    rc = lib.p3mx_short_range(act._handle, len(q), _lib.dptr(pos), _lib.dptr(q), None,
+                              _lib.dptr(f), None, None,
+                              _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE, None)
+    _lib.check(rc, act._handle)
+    d = pos[0::2] - pos[1::2]
+    ar = alpha * r
+    t = 1.0 / (1.0 + 0.3275911 * ar)
+    asp = t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 +
+                                                                        t * 1.061405429))))
+    fac = qa * (-qa) * np.exp(-ar ** 2) * (asp / r + 2 * alpha / np.sqrt(np.pi)) / r ** 2
+    f_ref = fac[:, None] * d
+    rel = np.linalg.norm(f[0::2] - f_ref, axis=1) / np.linalg.norm(f_ref, axis=1)
+    assert rel.max() < 4e-6, rel.max()
+    np.testing.assert_allclose(f[1::2], -f[0::2], rtol=0, atol=1e-12 * np.abs(f).max())
 
 
 def test_lj_system():
