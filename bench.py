@@ -428,7 +428,9 @@ def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
                                f"CUDA graph per step, Verlet skin {d.skin:g}",
                    "total_particles": int(n), "tuning_s": t_tune,
                    "mesh_hist": {int(m): int((meshes == m).sum()) for m in np.unique(meshes)},
-                   "cao": int(tuned[0][1]), "max_accuracy_estimate": float(acc.max()),
+                   "cao_hist": {int(c): int(sum(1 for t in tuned if t[1] == c))
+                                for c in sorted({t[1] for t in tuned})},
+                   "max_accuracy_estimate": float(acc.max()),
                    "r_cut_range": [float(rcs.min()), float(rcs.max())],
                    "verlet_candidates_per_step_est": pair_cand},
         "stages_ms": stages, "cpu_baseline": cpu_line,

@@ -128,6 +128,7 @@ SIGNATURES = {
     "p3mx_batch_last_error": (ctypes.c_char_p, [_vp]),
     "p3mx_batch_get_tuned": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(Tuned)]),
     "p3mx_batch_forces": (ctypes.c_int, [_vp, _dp]),
+    "p3mx_batch_set_cao": (ctypes.c_int, [_vp, _ip]),
     "p3mx_batch_run": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_ulonglong]),
     "p3mx_batch_stream": (ctypes.c_void_p, [_vp]),

@@ -121,6 +121,12 @@ __global__ void k_ks_error_batch(const int2 *__restrict__ mc, const double *__re
   }
 }
 
+// Tuned parameters of one replica for one cao (batch autotuner).
+struct BatchChoice {
+  int mesh = 0;
+  double r_cut_iL = 0, alpha_L = 0, acc = 0, rs = 0, ks = 0, cost = 0;
+};
+
 } // namespace p3mx
 
 struct p3mx_batch {
@@ -131,6 +137,10 @@ struct p3mx_batch {
   std::vector<int> n_charged;
   std::vector<double> sum_q2, accuracy, rs_err, ks_err;
   std::unique_ptr<Engine> eng;
+  // per cao (index 1..7) the tuned choice of every replica (mesh 0: the
+  // accuracy is out of reach at that cao)
+  std::vector<std::vector<BatchChoice>> by_cao;
+  std::vector<int> caos; // the cao of every replica
   DevBuf vel, step;
   bool forces_valid = false;
   cudaGraphExec_t graph = nullptr;
@@ -205,10 +215,7 @@ std::vector<double> ks_heq_batch(std::vector<int2> const &mc, std::vector<double
   return out;
 }
 
-struct Choice {
-  int mesh = 0;
-  double r_cut_iL = 0, alpha_L = 0, acc = 0, rs = 0, ks = 0, cost = 0;
-};
+using Choice = BatchChoice;
 
 // Per-replica choice of (mesh, r_cut, alpha) for one cao: lock-step
 // bisection of r_cut (P3M_RCUT_PREC) over every feasible (replica, mesh)
@@ -321,7 +328,7 @@ std::vector<Choice> choose_for_cao(p3mx_batch *b, int cao, std::vector<int> cons
   return best;
 }
 
-void configure_batch(p3mx_batch *b, int cao, std::vector<Choice> const &ch) {
+void configure_batch(p3mx_batch *b, std::vector<int> const &caos, std::vector<Choice> const &ch) {
   std::vector<ReplicaConf> conf(b->d.n_rep);
   for (int r = 0; r < b->d.n_rep; ++r) {
     auto &c = conf[r];
@@ -331,7 +338,7 @@ void configure_batch(p3mx_batch *b, int cao, std::vector<Choice> const &ch) {
       c.mesh[d] = ch[r].mesh;
     }
     c.prefactor = b->pref[r];
-    c.cao = cao;
+    c.cao = caos[r];
     c.r_cut = ch[r].r_cut_iL * L;
     c.alpha = ch[r].alpha_L / L;
     c.skin = b->d.skin;
@@ -450,38 +457,78 @@ int p3mx_batch_create(const p3mx_batch_desc *d, const double *pos, const double 
         meshes.push_back(m);
     if (meshes.empty())
       throw Error(P3MX_EDOMAIN, "no FFT-friendly even mesh in [mesh_min, mesh_max]");
-    double best_t = std::numeric_limits<double>::max();
-    int best_cao = -1;
-    std::vector<Choice> best_ch;
+    // per cao: every replica's best (mesh, r_cut, alpha) by the error
+    // estimate and the cost model; uncharged replicas get the smallest mesh
+    std::vector<std::vector<Choice>> by_cao(8);
+    std::vector<char> cao_ok(8, 0);
     for (int cao = d->cao_min; cao <= d->cao_max; ++cao) {
       auto ch = choose_for_cao(b.get(), cao, meshes, e.stream());
       bool feasible = true;
       for (int r = 0; r < R; ++r)
         if (b->n_charged[r] > 0 && ch[r].mesh == 0)
           feasible = false;
-      if (!feasible)
-        continue;
       for (int r = 0; r < R; ++r)
-        if (ch[r].mesh == 0) { // uncharged replica: smallest mesh, tiny cutoff
+        if (ch[r].mesh == 0 && b->n_charged[r] == 0) {
           ch[r].mesh = std::max(meshes[0], cao + 2);
           ch[r].r_cut_iL = 1e-6;
           ch[r].alpha_L = 1.0;
+          ch[r].cost = 0.0;
         }
-      configure_batch(b.get(), cao, ch);
+      by_cao[cao] = ch;
+      cao_ok[cao] = feasible;
+    }
+    // candidate assignments: one cao for every replica (each feasible cao),
+    // and per replica the cao of lowest model cost among those that reach the
+    // accuracy for it; the timed trials pick the fastest
+    std::vector<std::vector<int>> cands;
+    for (int cao = d->cao_min; cao <= d->cao_max; ++cao)
+      if (cao_ok[cao])
+        cands.push_back(std::vector<int>(R, cao));
+    {
+      std::vector<int> mix(R, -1);
+      bool ok = true;
+      for (int r = 0; r < R; ++r) {
+        double best = std::numeric_limits<double>::max();
+        for (int cao = d->cao_min; cao <= d->cao_max; ++cao) {
+          auto const &ch = by_cao[cao];
+          if (ch.empty() || ch[r].mesh == 0)
+            continue;
+          if (ch[r].cost < best) {
+            best = ch[r].cost;
+            mix[r] = cao;
+          }
+        }
+        ok = ok && mix[r] > 0;
+      }
+      if (ok && std::find(cands.begin(), cands.end(), mix) == cands.end())
+        cands.push_back(mix);
+    }
+    if (cands.empty())
+      throw Error(P3MX_ERUNTIME, "CoulombP3MGPU: failed to reach requested accuracy");
+    auto choices_of = [&](std::vector<int> const &caos) {
+      std::vector<Choice> ch(R);
+      for (int r = 0; r < R; ++r)
+        ch[r] = by_cao[caos[r]][r];
+      return ch;
+    };
+    double best_t = std::numeric_limits<double>::max();
+    std::vector<int> best_caos;
+    for (auto const &caos : cands) {
+      configure_batch(b.get(), caos, choices_of(caos));
       e.upload(pos, q, type, false, e.stream());
       e.census(e.stream());
       double const t = time_batch(b.get(), 3);
       if (t < best_t) {
         best_t = t;
-        best_cao = cao;
-        best_ch = ch;
+        best_caos = caos;
       }
     }
-    if (best_cao < 0)
-      throw Error(P3MX_ERUNTIME, "CoulombP3MGPU: failed to reach requested accuracy");
-    configure_batch(b.get(), best_cao, best_ch);
+    std::vector<Choice> const best_ch = choices_of(best_caos);
+    configure_batch(b.get(), best_caos, best_ch);
     e.upload(pos, q, type, false, e.stream());
     e.census(e.stream());
+    b->by_cao = by_cao;
+    b->caos = best_caos;
     b->accuracy.resize(R);
     b->rs_err.resize(R);
     b->ks_err.resize(R);
@@ -604,6 +651,55 @@ int p3mx_batch_run(p3mx_batch *b, int steps, double dt, double kT, double gamma,
     e.check_kernel_error(st);
     if (e.list_overflow(st))
       throw Error(P3MX_ERUNTIME, "Verlet list capacity exceeded during the graph run");
+  });
+}
+
+int p3mx_batch_set_cao(p3mx_batch *b, const int *cao) {
+  return bguard(b, [&] {
+    if (!cao)
+      throw Error(P3MX_EHANDLE, "cao array must not be NULL");
+    int const R = b->d.n_rep;
+    std::vector<int> caos(cao, cao + R);
+    std::vector<BatchChoice> ch(R);
+    for (int r = 0; r < R; ++r) {
+      if (caos[r] < b->d.cao_min || caos[r] > b->d.cao_max)
+        throw Error(P3MX_EDOMAIN, "cao of replica " + std::to_string(r) +
+                                      " outside the batch's [cao_min, cao_max]");
+      auto const &bc = b->by_cao[caos[r]];
+      if (bc.empty() || bc[r].mesh == 0)
+        throw Error(P3MX_EDOMAIN, "replica " + std::to_string(r) +
+                                      " cannot reach the accuracy with cao " +
+                                      std::to_string(caos[r]));
+      ch[r] = bc[r];
+    }
+    Engine &e = *b->eng;
+    cudaStream_t st = e.stream();
+    long long const N = e.n_part();
+    // keep the current particles across the reconfiguration
+    DevBuf xp, qp, tp;
+    xp.ensure(3 * std::max<long long>(1, N) * sizeof(double));
+    qp.ensure(std::max<long long>(1, N) * sizeof(double));
+    tp.ensure(std::max<long long>(1, N) * sizeof(int));
+    if (N > 0) {
+      P3MX_CUDA(cudaMemcpyAsync(xp.p, e.d_pos(), 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      P3MX_CUDA(cudaMemcpyAsync(qp.p, e.d_q(), N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      P3MX_CUDA(cudaMemcpyAsync(tp.p, e.d_type(), N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    }
+    configure_batch(b, caos, ch);
+    e.upload(xp.as<double>(), qp.as<double>(), tp.as<int>(), true, st);
+    e.census(st);
+    P3MX_CUDA(cudaStreamSynchronize(st));
+    b->caos = caos;
+    for (int r = 0; r < R; ++r) {
+      b->accuracy[r] = ch[r].acc;
+      b->rs_err[r] = ch[r].rs;
+      b->ks_err[r] = ch[r].ks;
+    }
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->forces_valid = false;
   });
 }
 

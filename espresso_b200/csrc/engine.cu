@@ -256,7 +256,6 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   size_t const cap = m_fp32 ? 4096 : 2048; // complex elements per smem buffer
   {
     std::vector<int2> bm, bc, bcen, bp, nat;
-    m_run = 4; // weight-record padding (R) used by every assignment/interp kernel
     m_blk_census_start.assign(1, 0);
     m_blk_pair_start.assign(1, 0);
     for (int r = 0; r < R; ++r) {
@@ -306,7 +305,10 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         }
         return col;
       };
+      // replicas may differ in cao: one phase per (cao, colour), and the
+      // sort bricks grouped by cao (one interpolation launch per order)
       std::vector<std::vector<int2>> phase;
+      std::vector<std::vector<int2>> bricks_of(8);
       nat.clear();
       for (int r = 0; r < R; ++r) {
         auto const &G = m_geom[r];
@@ -318,19 +320,29 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
         for (int bx = 0; bx < n0; ++bx)
           for (int by = 0; by < n1; ++by)
             for (int bz = 0; bz < n2; ++bz) {
-              int const p = cxv[bx] + 8 * (cyv[by] + 8 * czv[bz]);
+              int const p = (G.cao - 1) * 512 + cxv[bx] + 8 * (cyv[by] + 8 * czv[bz]);
               if (static_cast<int>(phase.size()) <= p)
                 phase.resize(p + 1);
               phase[p].push_back(int2{r, (bx * n1 + by) * n2 + bz});
             }
         for (int b = 0; b < G.nbx * G.nby * G.nbz; ++b)
-          nat.push_back(int2{r, b});
+          bricks_of[G.cao].push_back(int2{r, b});
       }
       m_phase_off.assign(1, 0);
-      for (auto const &ph : phase) {
-        bm.insert(bm.end(), ph.begin(), ph.end());
+      m_phase_cao.clear();
+      for (size_t p = 0; p < phase.size(); ++p) {
+        if (phase[p].empty())
+          continue;
+        bm.insert(bm.end(), phase[p].begin(), phase[p].end());
         m_phase_off.push_back(static_cast<int>(bm.size()));
+        m_phase_cao.push_back(static_cast<int>(p / 512) + 1);
       }
+      m_brick_off.assign(9, 0);
+      for (int c = 1; c <= 7; ++c) {
+        nat.insert(nat.end(), bricks_of[c].begin(), bricks_of[c].end());
+        m_brick_off[c + 1] = static_cast<int>(nat.size());
+      }
+      m_brick_off[1] = 0;
     }
     m_n_blk_mesh = static_cast<int>(bm.size());
     m_n_bricks = static_cast<int>(nat.size());
@@ -666,28 +678,13 @@ template <typename Real, int P> int interp_grid(int nbricks) {
   case 6: { constexpr int P = 6; KERNEL_CALL; } break;                         \
   default: { constexpr int P = 7; KERNEL_CALL; } break;                        \
   }
-// cao (template P) x z-run length of the assignment (template R: 4 when
-// every mesh has M2 % 4 == 0, else 2)
-#define P3MX_CAO_DISPATCH(cao, KERNEL_CALL)                                    \
-  if (m_run == 4) {                                                            \
-    constexpr int R = 4;                                                       \
-    P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                      \
-  } else {                                                                     \
-    constexpr int R = 2;                                                       \
-    P3MX_CAO_DISPATCH_R(cao, KERNEL_CALL)                                      \
-  }
-
 template <typename Real>
 void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
                           cudaStream_t st) {
   using C = typename CplxOf<Real>::type;
   int const R = n_rep();
-  // all replicas of one engine share cao (the batch tuner fixes cao per
-  // batch); meshes may differ
-  int const cao = m_geom[0].cao;
-  for (auto const &G : m_geom)
-    if (G.cao != cao)
-      throw Error(1, "replicas of one batch must share the charge-assignment order");
+  // replicas may differ in mesh and cao: the order-templated kernels run
+  // once per order present
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   if (!m_ginf_valid) {
     k_influence<Real><<<m_n_blk_cplx, 256, 0, st>>>(geom, m_blk_cplx.as<int2>(), m_ginf.as<Real>()); ++m_launches;
@@ -705,10 +702,9 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
     sort_keys(m_bkey.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
               m_perm.as<int>(), m_nkeys, st);
     mark("p3m_sort", st);
-    P3MX_CAO_DISPATCH(cao, (k_p3m_weights<Real, P, R><<<nb, 256, 0, st>>>(
-                               geom, m_perm.as<int>(), m_key.as<int>(), m_dist.as<Real>(), d_q(),
-                               m_rep_of.as<int>(), m_n, m_W.as<Real>(), m_skey.as<int>(),
-                               qmax_bits)));
+    k_p3m_weights<Real><<<nb, 256, 0, st>>>(geom, m_perm.as<int>(), m_key.as<int>(),
+                                            m_dist.as<Real>(), d_q(), m_rep_of.as<int>(), m_n,
+                                            m_W.as<Real>(), m_skey.as<int>(), qmax_bits);
     ++m_launches;
     mark("p3m_weights", st);
   } else {
@@ -723,7 +719,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
       if (cnt == 0)
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(cao, (launch_assign<Real, P>(chained, cnt, st, geom, tab,
+      P3MX_CAO_DISPATCH_R(m_phase_cao[p], (launch_assign<Real, P>(chained, cnt, st, geom, tab,
                                                        m_start.as<int>(), m_W.as<Real>(),
                                                        m_skey.as<int>(), qmax_bits,
                                                        m_rho.as<Real>(), m_kerr.as<int>())));
@@ -777,15 +773,17 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
   // 6. force back-interpolation (after the concurrent pair kernel, if any)
   if (m_interp_wait)
     P3MX_CUDA(cudaStreamWaitEvent(st, m_interp_wait, 0));
-  if (m_n > 0) {
-    int const nbr = m_n_bricks;
-    P3MX_CAO_DISPATCH_R(cao, (k_p3m_interp<Real, P><<<interp_grid<Real, P>(nbr),
-                                 32 * (1 + kInterpWarps), interp_smem<Real, P>(), st>>>(
-                                 geom, m_blk_brick.as<int2>(), nbr, m_start.as<int>(),
-                                 m_perm.as<int>(), m_skey.as<int>(), m_W.as<Real>(),
-                                 m_E.as<Real>(), m_tmap.as<CUtensorMap>(), d_q(),
-                                 m_dipole.as<double>(), f,
-                                 overwrite ? 1 : 0, m_kerr.as<int>())));
+  for (int c = 1; m_n > 0 && c <= 7; ++c) {
+    int const nbr = m_brick_off[c + 1] - m_brick_off[c];
+    if (nbr == 0)
+      continue;
+    int2 const *tab = m_blk_brick.as<int2>() + m_brick_off[c];
+    P3MX_CAO_DISPATCH_R(c, (k_p3m_interp<Real, P><<<interp_grid<Real, P>(nbr),
+                               32 * (1 + kInterpWarps), interp_smem<Real, P>(), st>>>(
+                               geom, tab, nbr, m_start.as<int>(), m_perm.as<int>(),
+                               m_skey.as<int>(), m_W.as<Real>(), m_E.as<Real>(),
+                               m_tmap.as<CUtensorMap>(), d_q(), m_dipole.as<double>(), f,
+                               overwrite ? 1 : 0, m_kerr.as<int>())));
     ++m_launches;
   }
   mark("p3m_interp", st);

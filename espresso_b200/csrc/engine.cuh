@@ -179,7 +179,9 @@ private:
   long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
   int m_n_bricks = 0; // sort bricks of all replicas (interpolation blocks)
-  std::vector<int> m_phase_off; // assignment super-brick table offsets per colour
+  std::vector<int> m_phase_off; // assignment super-brick table offsets per (cao, colour) phase
+  std::vector<int> m_phase_cao; // the cao of each phase
+  std::vector<int> m_brick_off; // interpolation brick table offsets per cao (index cao .. cao+1)
   int m_ntypes = 1;
   std::vector<PairIA> m_ia;
 
@@ -194,7 +196,6 @@ private:
   int m_n_blk_mesh = 0, m_n_blk_cplx = 0, m_n_blk_census = 0, m_n_blk_pair = 0;
   int m_n_blk_zf = 0, m_n_blk_y = 0, m_n_blk_x = 0, m_n_blk_zi = 0;
   int m_tile_y = 16, m_tile_x = 16;
-  int m_run = 4; // z points per thread of the charge assignment
   size_t m_smem_zf = 0, m_smem_y = 0, m_smem_x = 0, m_smem_zi = 0;
 
   // particles

@@ -92,12 +92,51 @@ template <int P, int R> __host__ __device__ constexpr int wstride() {
   return (3 * P + 2 * (R - 1) + 3) / 4 * 4;
 }
 template <int P, int R> __host__ __device__ constexpr int wz_off() { return 2 * P + (R - 1); }
+// Record stride of every order (that of order 7), so that replicas of one
+// batch may use different orders: a sorted particle's record starts at
+// s * kRecStride whatever its replica's order.
+constexpr int kRecStride = wstride<7, 4>();
 
-// Weights in brick-sorted order; also the corner key (relative to the
-// replica's corner range) of every sorted particle, and each replica's
-// largest |q| (FP32 bits rounded up, atomic maximum: order-independent) for
-// the fixed-point scale of the charge assignment.
-template <typename Real, int P, int R>
+// Weight record of one sorted particle for order P (R = 4):
+// {q*wx[0..P), wy[0..P), 0[R-1], wz[0..P), 0[R-1]}, zero-padded to the
+// common stride kRecStride, stored as 16- or 32-byte vectors.
+template <typename Real, int P>
+__device__ inline void weights_record(const Real *dist3, double q, Real *__restrict__ out) {
+  constexpr int R = 4;
+  Real w[3][P];
+  bspline_weights<P>(dist3[0], w[0]);
+  bspline_weights<P>(dist3[1], w[1]);
+  bspline_weights<P>(dist3[2], w[2]);
+  Real const qi = static_cast<Real>(q);
+  constexpr int WS = kRecStride;
+  Real rec[WS];
+#pragma unroll
+  for (int k = 0; k < WS; ++k)
+    rec[k] = Real(0);
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    rec[k] = qi * w[0][k];
+    rec[P + k] = w[1][k];
+    rec[wz_off<P, R>() + k] = w[2][k];
+  }
+  using R4 = typename Real4Of<Real>::type;
+  R4 *o = reinterpret_cast<R4 *>(out);
+#pragma unroll
+  for (int k = 0; k < WS / 4; ++k) {
+    R4 v;
+    v.x = rec[4 * k];
+    v.y = rec[4 * k + 1];
+    v.z = rec[4 * k + 2];
+    v.w = rec[4 * k + 3];
+    o[k] = v;
+  }
+}
+
+// Weights in brick-sorted order (each replica's order), the corner key
+// (relative to the replica's corner range) of every sorted particle, and
+// each replica's largest |q| (FP32 bits rounded up, atomic maximum:
+// order-independent) for the fixed-point scale of the charge assignment.
+template <typename Real>
 __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
                               const int *__restrict__ key, const Real *__restrict__ dist,
                               const double *__restrict__ q, const int *__restrict__ rep_of,
@@ -118,34 +157,16 @@ __global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__res
     if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1))
       atomicMax(&qmax_bits[rep], mx);
   }
-  Real w[3][P];
-  bspline_weights<P>(dist[3 * i + 0], w[0]);
-  bspline_weights<P>(dist[3 * i + 1], w[1]);
-  bspline_weights<P>(dist[3 * i + 2], w[2]);
-  Real const qi = static_cast<Real>(q[i]);
-  // assemble the record in registers, then store it as 16- or 32-byte
-  // vectors (the stride is a multiple of 4 elements)
-  constexpr int WS = wstride<P, R>();
-  Real rec[WS];
-#pragma unroll
-  for (int k = 0; k < WS; ++k)
-    rec[k] = Real(0);
-#pragma unroll
-  for (int k = 0; k < P; ++k) {
-    rec[k] = qi * w[0][k];
-    rec[P + k] = w[1][k];
-    rec[wz_off<P, R>() + k] = w[2][k];
-  }
-  using R4 = typename Real4Of<Real>::type;
-  R4 *o = reinterpret_cast<R4 *>(W + s * WS);
-#pragma unroll
-  for (int k = 0; k < WS / 4; ++k) {
-    R4 v;
-    v.x = rec[4 * k];
-    v.y = rec[4 * k + 1];
-    v.z = rec[4 * k + 2];
-    v.w = rec[4 * k + 3];
-    o[k] = v;
+  Real *out = W + s * kRecStride;
+  const Real *d3 = dist + 3 * i;
+  switch (G.cao) {
+  case 1: weights_record<Real, 1>(d3, q[i], out); break;
+  case 2: weights_record<Real, 2>(d3, q[i], out); break;
+  case 3: weights_record<Real, 3>(d3, q[i], out); break;
+  case 4: weights_record<Real, 4>(d3, q[i], out); break;
+  case 5: weights_record<Real, 5>(d3, q[i], out); break;
+  case 6: weights_record<Real, 6>(d3, q[i], out); break;
+  default: weights_record<Real, 7>(d3, q[i], out); break;
   }
   s_key[s] = key[i] - static_cast<int>(G.bin_off);
 }
@@ -266,7 +287,7 @@ template <typename Real, int P> __host__ __device__ constexpr size_t sb_tile_byt
 // shared memory: tile, staged weight records, per staged particle its z
 // weights times S in FP64 (8 slots) and its tile offset
 template <typename Real, int P> __host__ __device__ constexpr size_t sb_smem() {
-  return sb_tile_bytes<Real, P>() + sizeof(Real) * kSbChunk * wstride<P, 4>() +
+  return sb_tile_bytes<Real, P>() + sizeof(Real) * kSbChunk * kRecStride +
          sizeof(double) * 8 * kSbChunk + sizeof(int) * kSbChunk;
 }
 // sort-brick runs of a super-brick: (kSbEdge / B)^2 brick columns, one
@@ -281,7 +302,7 @@ k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, 
                 Real *__restrict__ rho, int *__restrict__ err) {
   using Word = typename SbWord<Real>::type;
   constexpr int R = 4;
-  constexpr int WS = wstride<P, R>();
+  constexpr int WS = kRecStride;
   constexpr int WZ = wz_off<P, R>();
   constexpr int P2 = P * P;
   constexpr int NQ = (P2 + 31) / 32;
@@ -531,7 +552,7 @@ template <typename Real, int P> struct InterpStage {
   using R4 = typename Real4Of<Real>::type;
   static constexpr int Ed = brick_edge<P>() + P - 1;
   static constexpr size_t tile = sizeof(R4) * Ed * Ed * Ed;
-  static constexpr size_t rec = sizeof(Real) * kInterpCap * wstride<P, 4>();
+  static constexpr size_t rec = sizeof(Real) * kInterpCap * kRecStride;
   // key / index window: the 16-byte aligned superset of the staged range
   static constexpr size_t ids = sizeof(int) * (kInterpCap + 8);
   // stages start on 128-byte boundaries (tensor copy destinations)
@@ -562,7 +583,7 @@ k_p3m_interp(const RepGeom *__restrict__ reps, const int2 *__restrict__ bricks, 
              double *__restrict__ f, int overwrite, int *__restrict__ err) {
   static_assert(P <= 8, "one lane per stencil z offset");
   constexpr int R = 4;
-  constexpr int WS = wstride<P, R>();
+  constexpr int WS = kRecStride;
   constexpr int WZ = wz_off<P, R>();
   constexpr int S = kInterpStages, CW = kInterpWarps, CAP = kInterpCap;
   using L = InterpStage<Real, P>;

@@ -300,6 +300,13 @@ void p3mx_batch_destroy(p3mx_batch *b);
 const char *p3mx_batch_last_error(const p3mx_batch *b);
 /* Tuned parameters of replica r. */
 int p3mx_batch_get_tuned(const p3mx_batch *b, int r, p3mx_tuned *out);
+/* Fix the charge-assignment order of every replica (n_rep values in the
+ * batch's [cao_min, cao_max]), as P3M(cao=...) fixes it for one system
+ * (p3m/common.hpp:59-172; no batched counterpart in the reference): each
+ * replica takes the mesh, r_cut and alpha the autotuner found for that
+ * order.  P3MX_EDOMAIN when an order cannot reach the accuracy for a
+ * replica.  Positions, charges and velocities are kept. */
+int p3mx_batch_set_cao(p3mx_batch *b, const int *cao);
 /* One force evaluation for all replicas (forces overwritten, device
  * resident); optional per-replica energies (n_rep doubles, host). */
 int p3mx_batch_forces(p3mx_batch *b, double *energy_out);

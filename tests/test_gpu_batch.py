@@ -95,10 +95,8 @@ def test_batch_forces_match_oracle_per_replica():
         f = np.zeros_like(pos)
         assert lib.p3mx_batch_get(h, None, f.ctypes.data_as(_P(ctypes.c_double)), None) == 0
         tab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
-        caos = set()
         for r in range(R):
             t = tuned(h, r)
-            caos.add(t.cao)
             assert t.accuracy <= 1e-3
             sl = slice(offs[r], offs[r + 1])
             p = O.make_params(boxes[r], list(t.mesh), t.cao, t.alpha, t.r_cut, prefs[r])
@@ -109,7 +107,47 @@ def test_batch_forces_match_oracle_per_replica():
             np.testing.assert_allclose(f[sl], ref, atol=3e-5 * scale, rtol=0)
             e_ref = ek + er[0] + er[1]
             assert abs(en[r] - e_ref) <= 1e-4 * (abs(e_ref) + np.abs(ek) + 1.0)
-        assert len(caos) == 1  # one cao per batch
+    finally:
+        lib.p3mx_batch_destroy(h)
+
+
+def test_batch_per_replica_cao_matches_oracle():
+    """Replicas of one batch with different charge-assignment orders
+    (p3mx_batch_set_cao: each replica takes the tuner's mesh, r_cut and
+    alpha for its order): forces and energies of every replica against the
+    FP64 oracle, then a graph-captured Langevin run and the forces again."""
+    lib = _lib.load()
+    boxes, prefs, pos, q, offs = make_replicas(seed=13, n_rep=5)
+    h = create(boxes, prefs, pos, q, offs, cao=(3, 7))
+    try:
+        R = len(prefs)
+        want = np.array([5, 7, 6, 7, 5], dtype=np.int32)
+        rc = lib.p3mx_batch_set_cao(h, want.ctypes.data_as(_P(ctypes.c_int)))
+        assert rc == 0, lib.p3mx_batch_last_error(h).decode()
+        bad = np.array([2, 7, 6, 7, 5], dtype=np.int32)
+        assert lib.p3mx_batch_set_cao(h, bad.ctypes.data_as(_P(ctypes.c_int))) != 0
+        tab = O.pair_table(1, {(0, 0): dict(wca_eps=1.0, wca_sig=1.0)})
+        for stage in range(2):
+            if stage == 1:
+                assert lib.p3mx_batch_run(h, 20, 0.005, 1.0, 1.0, 3) == 0
+            en = np.zeros(R)
+            assert lib.p3mx_batch_forces(h, en.ctypes.data_as(_P(ctypes.c_double))) == 0
+            x = np.zeros_like(pos)
+            f = np.zeros_like(pos)
+            assert lib.p3mx_batch_get(h, x.ctypes.data_as(_P(ctypes.c_double)),
+                                      f.ctypes.data_as(_P(ctypes.c_double)), None) == 0
+            for r in range(R):
+                t = tuned(h, r)
+                assert t.cao == want[r]
+                assert t.accuracy <= 1e-3
+                sl = slice(offs[r], offs[r + 1])
+                p = O.make_params(boxes[r], list(t.mesh), t.cao, t.alpha, t.r_cut, prefs[r])
+                fk, ek, _ = O.p3m_kspace(p, x[sl], q[sl])
+                fr, er, _, _ = O.short_range(p, x[sl], q[sl], None, 1, tab)
+                ref = fk + fr
+                np.testing.assert_allclose(f[sl], ref, atol=3e-5 * np.abs(ref).max(), rtol=0)
+                e_ref = ek + er[0] + er[1]
+                assert abs(en[r] - e_ref) <= 1e-4 * (abs(e_ref) + np.abs(ek) + 1.0)
     finally:
         lib.p3mx_batch_destroy(h)
 
