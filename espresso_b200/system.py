@@ -266,21 +266,57 @@ class Electrostatics:
         self._system._pairs_dirty = True
 
 
+class Thermostat:
+    """Langevin thermostat of the velocity-Verlet integrator, mirroring
+    ``espressomd.thermostat.Thermostat.set_langevin`` (thermostats/
+    langevin_inline.hpp:40-59): at every force calculation each particle
+    gets the friction -gamma v and a noise force of uniform components
+    sqrt(24 kT gamma / dt) (U(0, 1) - 1/2), drawn from a counter-based
+    Philox stream keyed by the seed (deterministic for a given seed)."""
+
+    def __init__(self):
+        self.kT = None
+        self.gamma = None
+        self.seed = None
+        self._rng = None
+
+    def set_langevin(self, kT, gamma, seed):
+        if kT < 0 or gamma < 0:
+            raise ValueError("kT and gamma must be >= 0")
+        self.kT, self.gamma, self.seed = float(kT), float(gamma), int(seed)
+        self._rng = np.random.Generator(np.random.Philox(key=self.seed))
+
+    def turn_off(self):
+        self.kT = self.gamma = self.seed = None
+        self._rng = None
+
+    def _forces(self, v, dt):
+        if self._rng is None or not self.gamma:
+            return 0.0
+        noise = np.sqrt(24.0 * self.kT * self.gamma / dt)
+        return -self.gamma * v + noise * (self._rng.random(v.shape) - 0.5)
+
+
 class Integrator:
     def __init__(self, system):
         self._system = system
 
     def run(self, steps=1, recalc_forces=False):
+        """Velocity Verlet (integrators/velocity_verlet_inline.hpp:34-58)
+        with the Langevin forces of ``system.thermostat`` added to the
+        conservative forces from libp3mx.so at every step."""
         s = self._system
         if s.time_step is None:
             raise RuntimeError("time_step not set")
-        s._calc_forces()
         dt = s.time_step
+        s._calc_forces()
+        s.part._f = s.part._f + s.thermostat._forces(s.part._v, dt)
         for _ in range(int(steps)):
             m = s.part._mass[:, None]
             s.part._v += 0.5 * dt * s.part._f / m
             s.part._pos += dt * s.part._v
             s._calc_forces()
+            s.part._f = s.part._f + s.thermostat._forces(s.part._v, dt)
             s.part._v += 0.5 * dt * s.part._f / m
 
 
@@ -321,6 +357,7 @@ class System:
         self.periodicity = (True, True, True)
         self.time_step = None
         self.cell_system = CellSystem(self)
+        self.thermostat = Thermostat()
         self._sr_handle = None
         self._pairs_dirty = True
         self._bond_version = 0

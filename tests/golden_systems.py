@@ -48,3 +48,20 @@ def jittered_lattice(n_side, box, jitter, seed, valence=1.0):
     pos = (idx + 0.5) * a + rng.uniform(-jitter, jitter, idx.shape)
     q = np.where(idx.sum(1) % 2 == 0, valence, -valence)
     return pos, q
+
+
+def c1_system(seed=0, n=2000, box=20.0, jitter=0.2):
+    """The 2000-charge system of the CPU-runnable configuration: a jittered
+    simple-cubic lattice of side 13 in a box of side 20 with alternating
+    charges, thinned symmetrically to n/2 ions of each sign."""
+    side = int(np.ceil(n ** (1.0 / 3.0)))
+    rng = np.random.default_rng(seed)
+    a = box / side
+    idx = np.array(list(itertools.product(range(side), repeat=3)), float)
+    q = np.where(idx.sum(1) % 2 == 0, 1.0, -1.0)
+    pos = (idx + 0.5) * a + rng.uniform(-jitter, jitter, idx.shape)
+    plus, minus = np.flatnonzero(q > 0), np.flatnonzero(q < 0)
+    keep = np.zeros(len(q), bool)
+    keep[rng.choice(plus, n // 2, replace=False)] = True
+    keep[rng.choice(minus, n // 2, replace=False)] = True
+    return pos[keep].copy(), q[keep].copy(), box
