@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--no-ewald", action="store_true",
                     help="skip the full-size accuracy check against the direct Ewald sum")
     ap.add_argument("--variant-steps", type=int, default=20)
+    ap.add_argument("--sample-every", type=int, default=0,
+                    help="batched: record temperature and potential energy every K steps "
+                         "(outside the timed chunks), e.g. --steps 10000 --sample-every 1000")
     return ap.parse_args()
 
 
@@ -418,14 +421,36 @@ def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    series = []
+    chunk = getattr(args, "sample_every", 0) or steps
+    t_total = 0.0
     with ClockSampler(0) as clk:
-        e0.record(stream)
-        _lib.check(lib.p3mx_batch_run(h, steps, 0.01, 1.0, 1.0, 7), h,
-                   lib.p3mx_batch_last_error)
-        e1.record(stream)
-        torch.cuda.synchronize()
+        done = 0
+        while done < steps:
+            k = min(chunk, steps - done)
+            e0.record(stream)
+            _lib.check(lib.p3mx_batch_run(h, k, 0.01, 1.0, 1.0, 7), h,
+                       lib.p3mx_batch_last_error)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_total += e0.elapsed_time(e1)
+            done += k
+            if chunk < steps:
+                # stability record outside the timed chunks: per-replica
+                # kinetic temperature and the total potential energy
+                ep = np.zeros(len(prefs))
+                _lib.check(lib.p3mx_batch_forces(h, ep.ctypes.data_as(P(ctypes.c_double))), h,
+                           lib.p3mx_batch_last_error)
+                v = np.zeros((n, 3))
+                _lib.check(lib.p3mx_batch_get(h, None, None, v.ctypes.data_as(P(ctypes.c_double))),
+                           h, lib.p3mx_batch_last_error)
+                tr = np.array([(v[offs[r]:offs[r + 1]] ** 2).mean() for r in range(len(prefs))])
+                series.append({"step": done, "kT_mean": float(tr.mean()),
+                               "kT_min": float(tr.min()), "kT_max": float(tr.max()),
+                               "e_pot_per_particle": float(ep.sum() / n),
+                               "finite": bool(np.isfinite(v).all())})
     lib.p3mx_batch_launch_count(h, ctypes.byref(lc1))
-    t_ms = e0.elapsed_time(e1) / steps
+    t_ms = t_total / steps
     # stage profile of one force evaluation of the whole batch (outside the
     # timed region)
     names = (ctypes.c_char_p * 32)()
@@ -486,6 +511,7 @@ def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
                    "r_cut_range": [float(rcs.min()), float(rcs.max())],
                    "verlet_candidates_per_step_est": pair_cand},
         "stages_ms": stages, "cpu_baseline": cpu_line,
+        "stability": series or None,
         "clocks": clk.summary() if clocks else None,
         "gpu_launches": int(lc1.value - lc0.value)}
 
