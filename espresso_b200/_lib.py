@@ -80,6 +80,15 @@ class BatchDesc(ctypes.Structure):
                 ("cao_max", ctypes.c_int)]
 
 
+class Dp3mParams(ctypes.Structure):
+    _fields_ = [("prefactor", ctypes.c_double), ("accuracy", ctypes.c_double),
+                ("mesh", ctypes.c_int * 3), ("cao", ctypes.c_int),
+                ("r_cut", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("epsilon", ctypes.c_double), ("mesh_off", ctypes.c_double * 3),
+                ("tune", ctypes.c_int), ("timings", ctypes.c_int),
+                ("verbose", ctypes.c_int), ("single_precision", ctypes.c_int)]
+
+
 # every symbol of include/p3mx.h, with its ctypes signature
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -134,6 +143,14 @@ SIGNATURES = {
     "p3mx_batch_stream": (ctypes.c_void_p, [_vp]),
     "p3mx_batch_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "p3mx_batch_get": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "p3mx_dp3m_create": (ctypes.c_int, [ctypes.POINTER(Dp3mParams), ctypes.POINTER(_vp)]),
+    "p3mx_dp3m_destroy": (None, [_vp]),
+    "p3mx_dp3m_last_error": (ctypes.c_char_p, [_vp]),
+    "p3mx_dp3m_set_system": (ctypes.c_int, [_vp, ctypes.POINTER(SystemDesc)]),
+    "p3mx_dp3m_activate": (ctypes.c_int, [_vp, _sz, _vp, _vp, ctypes.c_uint]),
+    "p3mx_dp3m_get_tuned": (ctypes.c_int, [_vp, ctypes.POINTER(Tuned)]),
+    "p3mx_dp3m_compute": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, ctypes.c_uint, _vp]),
+    "p3mx_dp3m_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 _lib = None

@@ -61,7 +61,10 @@ struct Timing {
   float ms_long = 0.f, ms_short = 0.f;
 };
 
+class Dp3mEngine;
+
 class Engine {
+  friend class Dp3mEngine; // the dipolar P3M pipeline drives the mesh stages
 public:
   explicit Engine(bool fp32);
   ~Engine();

@@ -4,3 +4,4 @@
 #include "api.cu"
 #include "batch.cu"
 #include "noalloc.cu"
+#include "dp3m.cu"

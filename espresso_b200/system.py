@@ -1,7 +1,8 @@
 """Minimal host-side system mirroring the slice of ``espressomd.System`` that
 the P3M + short-range force path needs: particles (pos, q, type, v, f), box,
 periodicity, Verlet skin, LJ/WCA parameters, FENE / harmonic bonds, the
-electrostatics container,
+electrostatics and magnetostatics containers (point dipoles in ``dip``,
+torques in ``torque_lab``),
 ``integrator.run`` and ``analysis.energy/pressure/pressure_tensor``.
 
 Every force, energy and virial comes from libp3mx.so through the C ABI
@@ -18,6 +19,7 @@ import numpy as np
 from . import _lib
 from .electrostatics import ELC, P3M, _P3MBase
 from .interactions import BondedInteractions
+from .magnetostatics import Magnetostatics
 
 
 class CellSystem:
@@ -137,13 +139,17 @@ class ParticleHandle:
         self._pl, self._idx = plist, idx
 
     def __getattr__(self, name):
-        if name in ("pos", "f", "v", "q", "type", "mass"):
+        if name in ("pos", "f", "v", "q", "type", "mass", "dip"):
             arr = getattr(self._pl, "_" + name)
             return np.copy(arr[self._idx])
+        if name == "torque_lab":
+            return np.copy(self._pl._torque[self._idx])
+        if name == "dipm":
+            return np.linalg.norm(self._pl._dip[self._idx], axis=-1)
         raise AttributeError(name)
 
     def __setattr__(self, name, value):
-        if name in ("pos", "f", "v", "q", "type", "mass"):
+        if name in ("pos", "f", "v", "q", "type", "mass", "dip"):
             getattr(self._pl, "_" + name)[self._idx] = value
             self._pl._system._touch(name)
         else:
@@ -195,12 +201,14 @@ class ParticleList:
         self._q = np.zeros(0)
         self._type = np.zeros(0, dtype=np.int32)
         self._mass = np.zeros(0)
+        self._dip = np.zeros((0, 3))
+        self._torque = np.zeros((0, 3))
         self._bonds = []  # (bond object, owner index, partner index)
         self._system._touch("all")
         if hasattr(self._system, "_bond_version"):
             self._system._bonds_changed()
 
-    def add(self, pos, q=None, type=None, v=None, mass=None):
+    def add(self, pos, q=None, type=None, v=None, mass=None, dip=None):
         pos = np.asarray(pos, dtype=float)
         single = pos.ndim == 1
         pos = np.atleast_2d(pos)
@@ -218,6 +226,8 @@ class ParticleList:
         self._q = np.concatenate([self._q, col(q, 0.0, (n,))])
         self._type = np.concatenate([self._type, col(type, 0, (n,), np.int32)])
         self._mass = np.concatenate([self._mass, col(mass, 1.0, (n,))])
+        self._dip = np.vstack([self._dip, col(dip, 0.0, (n, 3))])
+        self._torque = np.vstack([self._torque, np.zeros((n, 3))])
         self._system._touch("all")
         return ParticleHandle(self, i0 if single else slice(i0, i0 + n))
 
@@ -330,8 +340,9 @@ class Analysis:
         kin = 0.5 * float((s.part._mass[:, None] * s.part._v ** 2).sum())
         eb, _ = s._bond_observables()
         out = {"kinetic": kin, "coulomb": e3[0] + e3[1], "non_bonded": e3[2],
-               "bonded": eb}
-        out["total"] = kin + out["coulomb"] + out["non_bonded"] + out["bonded"]
+               "bonded": eb, "dipolar": s._e_dipolar}
+        out["total"] = (kin + out["coulomb"] + out["non_bonded"] + out["bonded"] +
+                        out["dipolar"])
         return out
 
     def pressure_tensor(self):
@@ -365,6 +376,8 @@ class System:
         self.bonded_inter = BondedInteractions(self)
         self.non_bonded_inter = NonBondedInteractions(self)
         self.electrostatics = Electrostatics(self)
+        self.magnetostatics = Magnetostatics(self)
+        self._e_dipolar = 0.0
         self.integrator = Integrator(self)
         self.analysis = Analysis(self)
 
@@ -378,6 +391,9 @@ class System:
         if self.electrostatics.solver is not None:
             self.electrostatics.solver._set_system(self._box_l, self.cell_system.skin,
                                                    self.periodicity)
+        if self.magnetostatics.solver is not None:
+            self.magnetostatics.solver._set_system(self._box_l, self.cell_system.skin,
+                                                   self.periodicity)
         self._sr_handle = None
 
     def volume(self):
@@ -389,14 +405,19 @@ class System:
         st = dict(self.__dict__)
         st["_sr_handle"] = None
         st["_restore_solver"] = self.electrostatics._solver
+        st["_restore_dipolar"] = self.magnetostatics._solver
         return st
 
     def __setstate__(self, st):
         solver = st.pop("_restore_solver")
+        dipolar = st.pop("_restore_dipolar", None)
         self.__dict__.update(st)
         self.electrostatics._solver = None
+        self.magnetostatics._solver = None
         if solver is not None:
             self.electrostatics.solver = solver
+        if dipolar is not None:
+            self.magnetostatics.solver = dipolar
 
     def _touch(self, what):
         pass
@@ -500,6 +521,17 @@ class System:
             _lib.check(rc, h)
             e3[2] = e2[1]
             v27[18:] = v18[9:]
+        # dipolar P3M: forces added, torques stored, energy returned apart
+        self._e_dipolar = 0.0
+        mag = self.magnetostatics.solver
+        if mag is not None and n > 0 and (forces or energy):
+            fd, td, ed = mag._compute(self.part._pos, self.part._dip, forces=forces,
+                                      energy=energy)
+            if forces:
+                f += fd
+                self.part._torque = td
+            if energy:
+                self._e_dipolar = ed
         return f, e3, v27.reshape(3, 3, 3)
 
     def _calc_forces(self):

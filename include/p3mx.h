@@ -333,6 +333,55 @@ int p3mx_batch_launch_count(const p3mx_batch *b, long long *count);
 /* Copy positions / forces (3*N doubles, host) of all replicas. */
 int p3mx_batch_get(p3mx_batch *b, double *pos, double *f, double *vel);
 
+/* --- dipolar P3M --------------------------------------------------------- */
+
+/* Actor parameters: the kwargs of espressomd.magnetostatics.DipolarP3M
+ * (src/python/espressomd/magnetostatics.py:82-160) and the P3MParameters of
+ * DipolarP3M (script_interface/magnetostatics/DipolarP3M.hpp:95-112).
+ * -1 marks a value left to the tuner; the mesh must be cubic. */
+typedef struct {
+  double prefactor;
+  double accuracy;
+  int mesh[3];
+  int cao;
+  double r_cut;
+  double alpha;
+  double epsilon;       /* 0 = metallic */
+  double mesh_off[3];   /* -1 = P3M_MESHOFF (0.5) */
+  int tune;             /* bool */
+  int timings;          /* force evaluations timed per tuning trial */
+  int verbose;          /* print the tuning log */
+  int single_precision; /* 1 = FP32 mesh/FFT path, 0 = FP64 */
+} p3mx_dp3m_params;
+
+typedef struct p3mx_dp3m p3mx_dp3m;
+
+/* Validates and stores the parameters, as DipolarP3M::do_construct +
+ * new_dp3m_handle (script_interface/magnetostatics/DipolarP3M.hpp:95-130,
+ * core/magnetostatics/dp3m.impl.hpp:80-92).  On a validation failure *out
+ * still receives a handle that carries the message. */
+int p3mx_dp3m_create(const p3mx_dp3m_params *params, p3mx_dp3m **out);
+void p3mx_dp3m_destroy(p3mx_dp3m *h);
+const char *p3mx_dp3m_last_error(const p3mx_dp3m *h);
+/* Box and skin (on_boxl_change -> scaleby_box_l once activated). */
+int p3mx_dp3m_set_system(p3mx_dp3m *h, const p3mx_system *sys);
+/* on_activation: sanity checks and tune() (dp3m.cpp:647-680, 880-893).
+ * dip: 3*n moments (AoS, Particle::calc_dip()). */
+int p3mx_dp3m_activate(p3mx_dp3m *h, size_t n, const double *pos,
+                       const double *dip, unsigned flags);
+int p3mx_dp3m_get_tuned(const p3mx_dp3m *h, p3mx_tuned *out);
+/* k-space (DipolarP3MImpl::long_range_kernel, dp3m.cpp:247-445) plus the
+ * real-space pair part (dp3m.hpp:142-232) for all n particles.  With
+ * P3MX_FORCES, forces and torques (3*n each) are added to f / torque (or
+ * overwrite them with P3MX_OVERWRITE); with P3MX_ENERGY, energy[0] gets
+ * the k-space energy with its self and Madelung corrections (and the
+ * surface term for epsilon != 0) and energy[1] the real-space energy. */
+int p3mx_dp3m_compute(p3mx_dp3m *h, size_t n, const double *pos,
+                      const double *dip, double *f, double *torque,
+                      double *energy, unsigned flags, void *stream);
+/* Kernels launched by the handle so far. */
+int p3mx_dp3m_launch_count(const p3mx_dp3m *h, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -671,7 +671,8 @@ def _dp3m_influence(M, L, cao, alpha, S):
     return g, keep, (sx, sy, sz), (dx, dy, dz)
 
 
-def dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy, want_forces=True):
+def dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy, want_forces=True,
+         epsilon=0.0, mesh_off=(0.5, 0.5, 0.5)):
     """Dipolar P3M (cubic box and mesh, metallic) in FP64 numpy, restating
     magnetostatics/dp3m.cpp and dp3m.hpp: the three dipole-component meshes
     assigned with the charge-assignment weights (dipole_assign; here through
@@ -689,13 +690,16 @@ def dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy, want_for
     :142-232 over minimum-image pairs within r_cut (exact erfc below accuracy
     5e-6), the partner getting -F and -(tau + d x F) (calc_opposing_force,
     forces_inline.hpp:159-171).  Mesh values are interpolated with each
-    particle's own assignment stencil.  Returns (forces, torques, energy)."""
+    particle's own assignment stencil.  For epsilon != 0 the surface term of
+    calc_surface_term (dp3m.cpp:452-510): energy + pref/2 |M|^2 and torques
+    -pref mu x M, M the total moment, pref = prefactor 4 pi / (V (2 eps + 1)).
+    Returns (forces, torques, energy)."""
     L = float(box_l)
     pos = np.asarray(pos, dtype=np.float64)
     dip = np.asarray(dip, dtype=np.float64)
     n = len(pos)
     M = int(mesh)
-    prm = make_params([L] * 3, M, cao, alpha, r_cut, 1.0)
+    prm = make_params([L] * 3, M, cao, alpha, r_cut, 1.0, mesh_off=mesh_off)
     rho = []
     for d in range(3):
         c = np.ascontiguousarray(dip[:, d])
@@ -780,6 +784,11 @@ def dp3m(box_l, pos, dip, prefactor, alpha, r_cut, mesh, cao, accuracy, want_for
             t[i] += to.sum(axis=0)
             f[js] -= fo
             t[js] -= to + np.cross(d, fo)
+    if epsilon != 0.0:
+        ps = prefactor * 4.0 * np.pi / L ** 3 / (2.0 * epsilon + 1.0)
+        mtot = dip.sum(axis=0)
+        energy += 0.5 * ps * float(mtot @ mtot)
+        t -= ps * np.cross(dip, mtot)
     return f, t, energy
 
 
