@@ -60,9 +60,13 @@ def parse():
                     help="box side; N = 0.5 box^3 (128 -> 2^20); smaller boxes for ncu captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="single",
-                    choices=["single", "batched", "elc", "melt", "pe_sweep"],
-                    help="single large system (default), batched replicas, or the single "
-                         "system as a slab with an empty gap along z (P3M + ELC)")
+                    choices=["single", "batched", "elc", "melt", "pe_sweep", "dipolar"],
+                    help="single large system (default), batched replicas, the single "
+                         "system as a slab with an empty gap along z (P3M + ELC), a bead-spring "
+                         "melt, a salt sweep of polyelectrolyte replicas, or point dipoles "
+                         "(dipolar P3M)")
+    ap.add_argument("--dipoles", type=int, default=1 << 20,
+                    help="dipole count of --workload dipolar (density 0.5)")
     ap.add_argument("--gap", type=float, default=16.0, help="ELC gap size (--workload elc)")
     ap.add_argument("--replicas", type=int, default=512)
     ap.add_argument("--skin", type=float, default=None,
@@ -917,6 +921,101 @@ def run_elc(args):
     print(json.dumps(out))
 
 
+def run_dipolar(args):
+    """Point-dipole workload: N dipoles of unit moment, random orientations,
+    on a jittered lattice at number density 0.5 (cubic box), dipolar P3M
+    tuned for accuracy 1e-4 (DipolarTuningAlgorithm: mesh, cao, r_cut,
+    alpha; outside the timed region), FP64 and FP32 mesh paths.  One step =
+    one evaluation of forces and torques (k-space + real space) through
+    p3mx_dp3m_compute with device pointers; e2e = the same through pinned
+    host arrays (positions and moments in, forces and torques out).  Prints
+    one JSON line."""
+    import torch
+    from espresso_b200 import _lib
+    from espresso_b200.magnetostatics import DipolarP3M
+
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n = int(args.dipoles)
+    L = (n / 0.5) ** (1.0 / 3.0)
+    rng = np.random.default_rng(0)
+    side = int(np.ceil(n ** (1.0 / 3.0)))
+    g = np.stack(np.meshgrid(*(np.arange(side),) * 3, indexing="ij"), -1).reshape(-1, 3)[:n]
+    pos = (g + 0.5 + rng.uniform(-0.2, 0.2, (n, 3))) * (L / side)
+    dip = rng.normal(size=(n, 3))
+    dip /= np.linalg.norm(dip, axis=1, keepdims=True)
+    pos_d = torch.from_numpy(pos).to(dev)
+    dip_d = torch.from_numpy(dip).to(dev)
+    f_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    t_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    pos_h = torch.from_numpy(pos).pin_memory()
+    dip_h = torch.from_numpy(dip).pin_memory()
+    f_h = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    t_h = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    out = {}
+    for label, sprec in (("fp64", False), ("fp32_mesh", True)):
+        act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, timings=2,
+                         verbose=False)
+        act._set_system([L] * 3, args.skin if args.skin is not None else 0.4, (True,) * 3)
+        act._activate(pos, dip)
+        h = act._handle
+        flags = _lib.P3MX_FORCES | _lib.P3MX_OVERWRITE
+
+        def step(device=True):
+            if device:
+                rc = lib.p3mx_dp3m_compute(h, n, _lib.dptr(pos_d), _lib.dptr(dip_d),
+                                           _lib.dptr(f_d), _lib.dptr(t_d), None,
+                                           flags | _lib.P3MX_DEVICE_PTRS, sp)
+            else:
+                rc = lib.p3mx_dp3m_compute(h, n, _lib.dptr(pos_h), _lib.dptr(dip_h),
+                                           _lib.dptr(f_h), _lib.dptr(t_h), None, flags, sp)
+            _lib.check(rc, h, lib.p3mx_dp3m_last_error)
+
+        def timed(device):
+            for _ in range(max(3, args.warmup)):
+                step(device)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(device)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            return e0.elapsed_time(e1) / args.steps
+
+        l0 = ctypes.c_longlong()
+        lib.p3mx_dp3m_launch_count(h, ctypes.byref(l0))
+        with ClockSampler(0) as clk:
+            ms = timed(True)
+        l1 = ctypes.c_longlong()
+        lib.p3mx_dp3m_launch_count(h, ctypes.byref(l1))
+        ms_e2e = timed(False)
+        p = act.get_params()
+        out[label] = {"ms_per_step": ms, "value": n / (ms * 1e-3),
+                      "e2e": {"value": n / (ms_e2e * 1e-3), "unit": "dipole-steps/s",
+                              "ms_per_step": ms_e2e, "h2d_bytes_per_step": 48 * n,
+                              "d2h_bytes_per_step": 48 * n},
+                      "gpu_launches_per_step": (l1.value - l0.value) / max(1, args.steps),
+                      "tuned": {"mesh": p["mesh"][0], "cao": p["cao"], "r_cut": p["r_cut"],
+                                "alpha": p["alpha"], "accuracy_estimate": p["accuracy"]},
+                      "clocks": clk.summary()}
+    line = {
+        "metric": "dipole-steps/s (dipolar P3M forces + torques at accuracy 1e-4)",
+        "impl": "ours", "workload": "dipolar", "value": out["fp64"]["value"],
+        "unit": "dipole-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic", "e2e": out["fp64"]["e2e"], "variants": out,
+        "config": {"workload": f"{n} unit point dipoles, random orientations, density 0.5, "
+                               f"box {L:.4g}^3, dipolar P3M tuned for accuracy 1e-4",
+                   "inputs": "resident in HBM, larger than L2 with the Verlet lists"},
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.workload == "batched":
@@ -930,6 +1029,9 @@ def main():
         return
     if args.workload == "pe_sweep":
         run_pe_sweep(args)
+        return
+    if args.workload == "dipolar":
+        run_dipolar(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
