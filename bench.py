@@ -957,8 +957,14 @@ def run_dipolar(args):
     sp = ctypes.c_void_p(stream.cuda_stream)
     out = {}
     for label, sprec in (("fp64", False), ("fp32_mesh", True)):
-        act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, timings=2,
-                         verbose=False)
+        if args.profile_only:
+            # the parameters the tuner chose for 2^17 dipoles in a plain run
+            # (timings under a profiler would mislead the tuner)
+            act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, tune=False,
+                             mesh=96, cao=7, r_cut=5.23, alpha=0.635)
+        else:
+            act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, timings=2,
+                             verbose=False)
         act._set_system([L] * 3, args.skin if args.skin is not None else 0.4, (True,) * 3)
         act._activate(pos, dip)
         h = act._handle
