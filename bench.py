@@ -1013,12 +1013,19 @@ def run_dipolar(args):
         l1 = ctypes.c_longlong()
         lib.p3mx_dp3m_launch_count(h, ctypes.byref(l1))
         ms_e2e = timed(False)
+        names = (ctypes.c_char_p * 40)()
+        sms = (ctypes.c_double * 40)()
+        nst = ctypes.c_int()
+        _lib.check(lib.p3mx_dp3m_profile(h, n, _lib.dptr(pos), _lib.dptr(dip), 5, sms, names, 40,
+                                         ctypes.byref(nst)), h, lib.p3mx_dp3m_last_error)
+        stages = {names[k].decode(): round(sms[k], 4) for k in range(min(40, nst.value))}
         p = act.get_params()
         out[label] = {"ms_per_step": ms, "value": n / (ms * 1e-3),
                       "e2e": {"value": n / (ms_e2e * 1e-3), "unit": "dipole-steps/s",
                               "ms_per_step": ms_e2e, "h2d_bytes_per_step": 48 * n,
                               "d2h_bytes_per_step": 48 * n},
                       "gpu_launches_per_step": (l1.value - l0.value) / max(1, args.steps),
+                      "stages_ms": stages,
                       "tuned": {"mesh": p["mesh"][0], "cao": p["cao"], "r_cut": p["r_cut"],
                                 "alpha": p["alpha"], "accuracy_estimate": p["accuracy"]},
                       "clocks": clk.summary()}

@@ -150,6 +150,8 @@ SIGNATURES = {
     "p3mx_dp3m_activate": (ctypes.c_int, [_vp, _sz, _vp, _vp, ctypes.c_uint]),
     "p3mx_dp3m_get_tuned": (ctypes.c_int, [_vp, ctypes.POINTER(Tuned)]),
     "p3mx_dp3m_compute": (ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, _vp, _dp, ctypes.c_uint, _vp]),
+    "p3mx_dp3m_profile": (ctypes.c_int, [_vp, _sz, _vp, _vp, ctypes.c_int, _dp,
+                                         ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, _ip]),
     "p3mx_dp3m_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
 }
 

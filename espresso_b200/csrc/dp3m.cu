@@ -163,6 +163,7 @@ public:
     ++E.m_launches;
     E.sort_keys(E.m_bkey.as<int>(), E.m_slot.as<int>(), E.m_cnt.as<int>(), E.m_start.as<int>(),
                 E.m_perm.as<int>(), E.m_nkeys, st);
+    E.mark("dp_sort", st);
     // 2. the three component meshes: assignment and z pass each
     C const *tw = E.m_tw.as<C>();
     C *ck3 = m_ck3.as<C>();
@@ -181,7 +182,8 @@ public:
           continue;
         int2 const *tab = E.m_blk_mesh.as<int2>() + E.m_phase_off[p];
         P3MX_CAO_DISPATCH_R(E.m_phase_cao[p],
-                            (launch_assign<Real, P>(chained, cnt, st, geom, tab, E.m_start.as<int>(),
+                            (launch_assign<Real, P>(E.m_sb_edge, chained, cnt, st, geom, tab,
+                                                    E.m_start.as<int>(),
                                                     E.m_W.as<Real>(), E.m_skey.as<int>(),
                                                     qmax_bits, E.m_rho.as<Real>(),
                                                     E.m_kerr.as<int>())));
@@ -192,6 +194,7 @@ public:
           geom, E.m_blk_zf.as<Blk>(), E.m_rho.as<Real>(), ck3 + d * E.m_cplx, tw, E.m_kerr.as<int>());
       ++E.m_launches;
     }
+    E.mark("dp_assign_fft_z", st);
     k_fft_y<Real><<<dim3(E.m_n_blk_y, 3), 256, E.m_smem_y, st>>>(geom, E.m_blk_y.as<Blk>(), ck3,
                                                                  E.m_cplx, E.m_tile_y, false, tw);
     ++E.m_launches;
@@ -203,6 +206,7 @@ public:
                                               E.m_W.as<Real>(), E.m_skey.as<int>(), qmax_bits);
       ++E.m_launches;
     }
+    E.mark("dp_fft_y_weights", st);
     // 3. x pass per mode, backward y and z, interpolation
     for (int mode = 0; mode < 3; ++mode) {
       bool const ev = want_e && mode == 0;
@@ -222,6 +226,7 @@ public:
             E.m_field.as<C>(), E.m_tile_x, nullptr, tw);
         ++E.m_launches;
       }
+      E.mark("dp_x_pass", st);
       if (!want_ft)
         break;
       k_fft_y<Real><<<dim3(E.m_n_blk_y, 3), 256, E.m_smem_y, st>>>(
@@ -231,6 +236,7 @@ public:
           geom, E.m_blk_zi.as<Blk>(), E.m_field.as<C>(), E.m_cplx, E.m_E.as<Real>(), tw,
           E.m_kerr.as<int>());
       ++E.m_launches;
+      E.mark("dp_inv_yz", st);
       double *out = m_out.as<double>() + 3 * n * mode;
       RepGeom const *gi = m_geom_interp.as<RepGeom>();
       for (int c = 1; n > 0 && c <= 7; ++c) {
@@ -246,6 +252,7 @@ public:
                                    out, 1, E.m_kerr.as<int>())));
         ++E.m_launches;
       }
+      E.mark("dp_interp", st);
     }
   }
 
@@ -278,6 +285,7 @@ public:
             n, m_mu.as<double>(), o, o + 3 * n, o + 6 * n, pt, pf, ps, m_sums.as<double>(), f, t,
             overwrite ? 1 : 0);
         ++E.m_launches;
+        E.mark("dp_combine", st);
       } else if (overwrite) {
         P3MX_CUDA(cudaMemsetAsync(f, 0, 3 * n * sizeof(double), st));
         P3MX_CUDA(cudaMemsetAsync(t, 0, 3 * n * sizeof(double), st));
@@ -290,6 +298,7 @@ public:
       k_dp3m_sort_mu<<<static_cast<int>(ceil_div(n, 256)), 256, 0, st>>>(
           n, E.m_cperm.as<int>(), m_mu.as<double>(), m_smu.as<double4>());
       ++E.m_launches;
+      E.mark("dp_sort_mu", st);
       int const exact = accuracy > 5e-6 ? 0 : 1;
       RepGeom const *geom = E.m_geom_d.as<RepGeom>();
       if (want_e) {
@@ -308,6 +317,7 @@ public:
             nullptr);
         ++E.m_launches;
       }
+      E.mark("dp_pairs", st);
     }
     P3MX_CUDA(cudaGetLastError());
     if (want_e) {
@@ -337,6 +347,39 @@ public:
       energies[0] = e_k;
       energies[1] = e_r;
     }
+  }
+
+  // Per-stage device times (ms, mean of reps) of one force and torque
+  // evaluation of the staged particles, from CUDA events between stages.
+  std::vector<std::pair<std::string, double>> profile(double prefactor, double accuracy,
+                                                      double epsilon,
+                                                      std::vector<double> const &census,
+                                                      double *f, double *t, int reps,
+                                                      cudaStream_t st) {
+    Engine &E = m_eng;
+    std::vector<std::pair<std::string, double>> acc;
+    for (int r = 0; r < reps; ++r) {
+      E.m_marks.clear();
+      E.m_profiling = true;
+      E.mark("start", st);
+      compute(prefactor, accuracy, epsilon, f, t, true, false, census, st, nullptr);
+      E.m_profiling = false;
+      P3MX_CUDA(cudaStreamSynchronize(st));
+      for (size_t k = 1; k < E.m_marks.size(); ++k) {
+        float ms = 0.f;
+        P3MX_CUDA(cudaEventElapsedTime(&ms, E.m_marks[k - 1].second, E.m_marks[k].second));
+        std::string const &name = E.m_marks[k].first;
+        auto it = std::find_if(acc.begin(), acc.end(), [&](auto const &p) { return p.first == name; });
+        if (it == acc.end())
+          acc.emplace_back(name, ms / reps);
+        else
+          it->second += ms / reps;
+      }
+      for (auto &m : E.m_marks)
+        cudaEventDestroy(m.second);
+      E.m_marks.clear();
+    }
+    return acc;
   }
 
   // sum over the full mesh of G_energy U2s |d_op|^2 (cached per geometry).
@@ -976,6 +1019,41 @@ int p3mx_dp3m_compute(p3mx_dp3m *h, size_t n, const double *pos, const double *d
     if (want_e) {
       energy[0] = e2[0];
       energy[1] = e2[1];
+    }
+  });
+}
+
+int p3mx_dp3m_profile(p3mx_dp3m *h, size_t n, const double *pos, const double *dip, int reps,
+                      double *ms, const char **names, int cap, int *nstages) {
+  return dp_guarded(h, [&] {
+    if (!h->activated)
+      throw Error(P3MX_ERUNTIME, "DipolarP3M: actor not activated");
+    if (n != h->n || !h->de) {
+      h->n = n;
+      dp_configure(h);
+    }
+    Dp3mEngine &de = *h->de;
+    cudaStream_t const st = de.engine().stream();
+    auto const census = de.upload(pos, dip, false, st);
+    h->scratch.ensure(6 * std::max<size_t>(1, n) * sizeof(double));
+    double *f = h->scratch.as<double>(), *t = f + 3 * n;
+    // one unprofiled evaluation first (list build, influence functions)
+    de.compute(h->prm.prefactor, h->accuracy, h->prm.epsilon, f, t, true, false, census, st,
+               nullptr);
+    static std::vector<std::string> keep;
+    auto prof = de.profile(h->prm.prefactor, h->accuracy, h->prm.epsilon, census, f, t,
+                           std::max(1, reps), st);
+    keep.clear();
+    for (auto const &p : prof)
+      keep.push_back(p.first);
+    int const ns = static_cast<int>(prof.size());
+    if (nstages)
+      *nstages = ns;
+    for (int k = 0; k < std::min(ns, cap); ++k) {
+      if (ms)
+        ms[k] = prof[k].second;
+      if (names)
+        names[k] = keep[k].c_str();
     }
   });
 }

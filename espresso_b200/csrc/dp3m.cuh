@@ -229,9 +229,11 @@ __global__ void k_dp3m_sum_rows(const double *__restrict__ partials, int nblk, i
 
 // ---- x pass of the dipolar k-space operator ------------------------------
 // Per block: one ky, a tile of kz (the block table of the charge x pass).
-// The three forward-transformed components F_d are staged and transformed
-// along x one after another, accumulating mk = sum_d d_op_d F_d; then three
-// output spectra are formed from mk and transformed backward along x:
+// In mode 0 the three forward-transformed components F_d are staged and
+// transformed along x one after another, accumulating mk = sum_d d_op_d F_d,
+// which then replaces component x in place (each block rewrites only the
+// lines it read); modes 1 and 2 load that mk.  Three output spectra are
+// formed from mk and transformed backward along x:
 //   mode 0 (torques, AssignTorques, dp3m.cpp:372-395):
 //     d_op_j G_energy mk,                                   j = x, y, z
 //   mode 1 / 2 (forces, AssignForces, dp3m.cpp:396-430):
@@ -243,7 +245,7 @@ __global__ void k_dp3m_sum_rows(const double *__restrict__ partials, int nblk, i
 template <typename Real, bool EV>
 __global__ void __launch_bounds__(256, 1)
 k_fft_x_dp3m(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
-             const typename CplxOf<Real>::type *__restrict__ comp_hat, long long fstride,
+             typename CplxOf<Real>::type *__restrict__ comp_hat, long long fstride,
              const Real *__restrict__ g_e, const Real *__restrict__ g_f, int mode,
              typename CplxOf<Real>::type *__restrict__ field0, int tile,
              double *__restrict__ partials, const typename CplxOf<Real>::type *__restrict__ twtab) {
@@ -268,8 +270,8 @@ k_fft_x_dp3m(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   bool const col = tq < T;
   int const kz = kz0 + tq;
   int const dop_y = dp_dop(y, M1), dop_z = dp_dop(kz, M2);
-  for (int d = 0; d < 3; ++d) {
-    const C *src = comp_hat + fstride * d;
+  // stage T lines of src (column tq, rows x) into dst
+  auto stage = [&](const C *src, C *dst) {
     for (int x0 = xq; x0 < M0; x0 += 64) {
       C v[4];
 #pragma unroll
@@ -282,17 +284,30 @@ k_fft_x_dp3m(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
       for (int u = 0; u < 4; ++u) {
         int const x = x0 + 16 * u;
         if (col && x < M0)
-          a[tq * ld + pix(x)] = v[u];
+          dst[tq * ld + pix(x)] = v[u];
       }
     }
-    __syncthreads();
-    C const *res = fft_lines<C>(a, b, T, ld, G.plan[0], tw, false);
-    for (int x = xq; col && x < M0; x += 16) {
-      Real const op = static_cast<Real>(d == 0 ? dp_dop(x, M0) : (d == 1 ? dop_y : dop_z));
-      C const v = res[tq * ld + pix(x)];
-      C const m = (d == 0) ? C{Real(0), Real(0)} : mk[tq * ld + pix(x)];
-      mk[tq * ld + pix(x)] = C{m.x + op * v.x, m.y + op * v.y};
+  };
+  if (mode == 0) {
+    for (int d = 0; d < 3; ++d) {
+      stage(comp_hat + fstride * d, a);
+      __syncthreads();
+      C const *res = fft_lines<C>(a, b, T, ld, G.plan[0], tw, false);
+      for (int x = xq; col && x < M0; x += 16) {
+        Real const op = static_cast<Real>(d == 0 ? dp_dop(x, M0) : (d == 1 ? dop_y : dop_z));
+        C const v = res[tq * ld + pix(x)];
+        C const m = (d == 0) ? C{Real(0), Real(0)} : mk[tq * ld + pix(x)];
+        mk[tq * ld + pix(x)] = C{m.x + op * v.x, m.y + op * v.y};
+      }
+      __syncthreads();
     }
+    // mk for the force modes, in place of component x (same thread, same
+    // point as the staging: the block's own lines only)
+    if (col)
+      for (int x = xq; x < M0; x += 16)
+        comp_hat[base + x * stride_x + tq] = mk[tq * ld + pix(x)];
+  } else {
+    stage(comp_hat, mk);
     __syncthreads();
   }
   if constexpr (EV) {
@@ -435,10 +450,23 @@ k_dp3m_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
     int const cnt = nb_count(cw), cna = nb_count_a(cw);
     const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
     int const base0 = static_cast<int>(G.p0);
+    // the next partner's records are loaded while the current pair is
+    // evaluated (two dependent gathers per entry otherwise serialise)
+    auto partner = [&](int k) {
+      return base0 + static_cast<int>(static_cast<unsigned>(nbp[nb_logical(0, G.max_nb, cna, k)]) &
+                                      kNbIndexMask);
+    };
+    int b_next = (cnt > 0) ? partner(0) : 0;
+    double4 p_next = (cnt > 0) ? spq[b_next] : pa;
+    double4 m_next = (cnt > 0) ? smu[b_next] : ma;
     for (int k = 0; k < cnt; ++k) {
-      int const b = base0 + static_cast<int>(static_cast<unsigned>(
-                                nbp[nb_logical(0, G.max_nb, cna, k)]) & kNbIndexMask);
-      double4 const pb = spq[b];
+      double4 const pb = p_next;
+      double4 const mb = m_next;
+      if (k + 1 < cnt) {
+        b_next = partner(k + 1);
+        p_next = spq[b_next];
+        m_next = smu[b_next];
+      }
       double const d0 = mi_d(pa.x - pb.x, G.box[0], G.box_i[0]);
       double const d1 = mi_d(pa.y - pb.y, G.box[1], G.box_i[1]);
       double const d2 = mi_d(pa.z - pb.z, G.box[2], G.box_i[2]);
@@ -446,22 +474,24 @@ k_dp3m_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
       double const r = sqrt(r2);
       if (!(r < rc) || !(r > 0.0))
         continue;
-      double4 const mb = smu[b];
+      // one division for 1/r^2 (1/r = r / r^2) and one for the A&S t
+      double const inv_r2 = 1.0 / r2;
+      double const inv_r = r * inv_r2;
       double const ad = alpha * r;
       double const exa = exp(-ad * ad);
       double B;
       if (exact_erfc) {
-        B = (erfc(ad) / r + coeff * exa) / r2;
+        B = (erfc(ad) * inv_r + coeff * exa) * inv_r2;
       } else {
         double const t = 1.0 / (1.0 + 0.3275911 * ad);
         double const asp =
             t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 +
                                                                          t * 1.061405429))));
-        B = (asp / r + coeff) * exa / r2;
+        B = (asp * inv_r + coeff) * exa * inv_r2;
       }
       double const common = a2 * coeff * exa;
-      double const Cc = (3.0 * B + 2.0 * common) / r2;
-      double const Dd = (5.0 * Cc + 4.0 * common * a2) / r2;
+      double const Cc = (3.0 * B + 2.0 * common) * inv_r2;
+      double const Dd = (5.0 * Cc + 4.0 * common * a2) * inv_r2;
       double const mimj = ma.x * mb.x + ma.y * mb.y + ma.z * mb.z;
       double const mir = ma.x * d0 + ma.y * d1 + ma.z * d2;
       double const mjr = mb.x * d0 + mb.y * d1 + mb.z * d2;

@@ -278,6 +278,18 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     // super-bricks sharing the colour triple then have disjoint tiles.  All
     // sort bricks in spatial order feed the interpolation.
     {
+      // super-brick edge: 16, unless one colour's 16^3 super-bricks (about
+      // an eighth of them) would leave SMs without a block
+      {
+        long long n16 = 0;
+        for (auto const &G : m_geom)
+          n16 += static_cast<long long>(ceil_div(G.mesh[0], kSbEdge)) * ceil_div(G.mesh[1], kSbEdge) *
+                 ceil_div(G.mesh[2], kSbEdge);
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        m_sb_edge = (n16 / 8 < sms) ? kSbEdgeSmall : kSbEdge;
+      }
       auto colours = [](int M, int B, int P) {
         int const nb = (M + B - 1) / B;
         std::vector<int> s(nb), e(nb), col(nb, -1);
@@ -312,9 +324,9 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
       nat.clear();
       for (int r = 0; r < R; ++r) {
         auto const &G = m_geom[r];
-        auto const cxv = colours(G.mesh[0], kSbEdge, G.cao);
-        auto const cyv = colours(G.mesh[1], kSbEdge, G.cao);
-        auto const czv = colours(G.mesh[2], kSbEdge, G.cao);
+        auto const cxv = colours(G.mesh[0], m_sb_edge, G.cao);
+        auto const cyv = colours(G.mesh[1], m_sb_edge, G.cao);
+        auto const czv = colours(G.mesh[2], m_sb_edge, G.cao);
         int const n0 = static_cast<int>(cxv.size()), n1 = static_cast<int>(cyv.size()),
                   n2 = static_cast<int>(czv.size());
         for (int bx = 0; bx < n0; ++bx)
@@ -437,18 +449,26 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
                                        static_cast<int>(limit)));
       };
       if (m_fp32) {
-        aset(k_p3m_assign_sb<float, 1>); aset(k_p3m_assign_sb<float, 2>);
-        aset(k_p3m_assign_sb<float, 3>); aset(k_p3m_assign_sb<float, 4>);
-        aset(k_p3m_assign_sb<float, 5>); aset(k_p3m_assign_sb<float, 6>);
-        aset(k_p3m_assign_sb<float, 7>);
+        aset(k_p3m_assign_sb<float, 1, 16>); aset(k_p3m_assign_sb<float, 2, 16>);
+        aset(k_p3m_assign_sb<float, 3, 16>); aset(k_p3m_assign_sb<float, 4, 16>);
+        aset(k_p3m_assign_sb<float, 5, 16>); aset(k_p3m_assign_sb<float, 6, 16>);
+        aset(k_p3m_assign_sb<float, 7, 16>);
+        aset(k_p3m_assign_sb<float, 1, 8>); aset(k_p3m_assign_sb<float, 2, 8>);
+        aset(k_p3m_assign_sb<float, 3, 8>); aset(k_p3m_assign_sb<float, 4, 8>);
+        aset(k_p3m_assign_sb<float, 5, 8>); aset(k_p3m_assign_sb<float, 6, 8>);
+        aset(k_p3m_assign_sb<float, 7, 8>);
         aset(k_p3m_interp<float, 1>); aset(k_p3m_interp<float, 2>); aset(k_p3m_interp<float, 3>);
         aset(k_p3m_interp<float, 4>); aset(k_p3m_interp<float, 5>); aset(k_p3m_interp<float, 6>);
         aset(k_p3m_interp<float, 7>);
       } else {
-        aset(k_p3m_assign_sb<double, 1>); aset(k_p3m_assign_sb<double, 2>);
-        aset(k_p3m_assign_sb<double, 3>); aset(k_p3m_assign_sb<double, 4>);
-        aset(k_p3m_assign_sb<double, 5>); aset(k_p3m_assign_sb<double, 6>);
-        aset(k_p3m_assign_sb<double, 7>);
+        aset(k_p3m_assign_sb<double, 1, 16>); aset(k_p3m_assign_sb<double, 2, 16>);
+        aset(k_p3m_assign_sb<double, 3, 16>); aset(k_p3m_assign_sb<double, 4, 16>);
+        aset(k_p3m_assign_sb<double, 5, 16>); aset(k_p3m_assign_sb<double, 6, 16>);
+        aset(k_p3m_assign_sb<double, 7, 16>);
+        aset(k_p3m_assign_sb<double, 1, 8>); aset(k_p3m_assign_sb<double, 2, 8>);
+        aset(k_p3m_assign_sb<double, 3, 8>); aset(k_p3m_assign_sb<double, 4, 8>);
+        aset(k_p3m_assign_sb<double, 5, 8>); aset(k_p3m_assign_sb<double, 6, 8>);
+        aset(k_p3m_assign_sb<double, 7, 8>);
         aset(k_p3m_interp<double, 1>); aset(k_p3m_interp<double, 2>); aset(k_p3m_interp<double, 3>);
         aset(k_p3m_interp<double, 4>); aset(k_p3m_interp<double, 5>); aset(k_p3m_interp<double, 6>);
         aset(k_p3m_interp<double, 7>);
@@ -631,22 +651,34 @@ void Engine::encode_field_maps(cudaStream_t st) {
 namespace {
 // One colour launch of the charge assignment; `chained` launches it as a
 // programmatic dependent of the previous colour (see k_p3m_assign_sb).
-template <typename Real, int P>
-void launch_assign(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
-                   int const *start, Real const *W, int const *s_key, unsigned const *qmax_bits,
-                   Real *rho, int *err) {
+template <typename Real, int P, int E>
+void launch_assign_e(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
+                     int const *start, Real const *W, int const *s_key, unsigned const *qmax_bits,
+                     Real *rho, int *err) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(static_cast<unsigned>(cnt));
   cfg.blockDim = dim3(32 * kSbWarps);
-  cfg.dynamicSmemBytes = sb_smem<Real, P>();
+  cfg.dynamicSmemBytes = sb_smem<Real, P, E>();
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = chained ? 1 : 0;
-  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign_sb<Real, P>, geom, tab, cnt, start, W, s_key,
+  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign_sb<Real, P, E>, geom, tab, cnt, start, W, s_key,
                                qmax_bits, rho, err));
+}
+// ... with the engine's super-brick edge (16 or 8)
+template <typename Real, int P>
+void launch_assign(int edge, bool chained, int cnt, cudaStream_t st, RepGeom const *geom,
+                   int2 const *tab, int const *start, Real const *W, int const *s_key,
+                   unsigned const *qmax_bits, Real *rho, int *err) {
+  if (edge == kSbEdgeSmall)
+    launch_assign_e<Real, P, kSbEdgeSmall>(chained, cnt, st, geom, tab, start, W, s_key, qmax_bits,
+                                           rho, err);
+  else
+    launch_assign_e<Real, P, kSbEdge>(chained, cnt, st, geom, tab, start, W, s_key, qmax_bits, rho,
+                                      err);
 }
 
 // Persistent grid of the back-interpolation pipeline: resident blocks per
@@ -719,7 +751,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
       if (cnt == 0)
         continue;
       int2 const *tab = m_blk_mesh.as<int2>() + m_phase_off[p];
-      P3MX_CAO_DISPATCH_R(m_phase_cao[p], (launch_assign<Real, P>(chained, cnt, st, geom, tab,
+      P3MX_CAO_DISPATCH_R(m_phase_cao[p], (launch_assign<Real, P>(m_sb_edge, chained, cnt, st, geom, tab,
                                                        m_start.as<int>(), m_W.as<Real>(),
                                                        m_skey.as<int>(), qmax_bits,
                                                        m_rho.as<Real>(), m_kerr.as<int>())));

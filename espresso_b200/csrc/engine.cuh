@@ -182,6 +182,7 @@ private:
   long long m_ebins = 0; // field mesh records (ghost layers included)
   long long m_ncorner = 0; // corner keys (bricks x brick^3)
   int m_n_bricks = 0; // sort bricks of all replicas (interpolation blocks)
+  int m_sb_edge = 16; // super-brick edge of the charge assignment (16, or 8 for small meshes)
   std::vector<int> m_phase_off; // assignment super-brick table offsets per (cao, colour) phase
   std::vector<int> m_phase_cao; // the cao of each phase
   std::vector<int> m_brick_off; // interpolation brick table offsets per cao (index cao .. cao+1)

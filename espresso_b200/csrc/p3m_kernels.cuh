@@ -184,12 +184,14 @@ struct TileStrides {
 // ---------------------------------------------------------------------------
 // Charge assignment by super-bricks (AssignCharges, p3m.cpp:225-265;
 // charge_assign, p3m.cpp:283-330).  One CTA takes the particles whose
-// stencil corners lie in a super-brick of kSbEdge^3 corner positions (whole
+// stencil corners lie in a super-brick of E^3 corner positions (whole
 // sort bricks: a few contiguous ranges of the brick-major order), so every
 // particle is visited once.  For each particle one warp covers its P^2
 // (x, y) stencil rows (one row per lane, the P z points of a row unrolled)
-// and adds q wx wy wz into a shared-memory tile of (kSbEdge + P - 1)^3
-// points, in fixed point; the tile is then added to the mesh.  Tiles of
+// and adds q wx wy wz into a shared-memory tile of (E + P - 1)^3
+// points, in fixed point; the tile is then added to the mesh.  E = 16, or 8
+// when the 16^3 super-bricks of one colour would not give every SM a block
+// (small meshes: more, smaller tiles with a larger halo share).  Tiles of
 // neighbouring super-bricks overlap by P - 1 points, so super-bricks are
 // coloured (greedy interval colouring per dimension: tiles of one colour
 // never overlap, modulo the mesh) and launched colour by colour: the plain
@@ -214,6 +216,7 @@ struct TileStrides {
 // (FP32-mixed) and 2^-56 in FP64, and each tile point is rounded once to
 // the working precision before it is added to the mesh.
 constexpr int kSbEdge = 16;   // corner positions per dimension of a super-brick (multiple of 4 and 8)
+constexpr int kSbEdgeSmall = 8; // the edge for meshes with too few 16^3 super-bricks to fill the GPU
 constexpr int kSbWarps = 8;   // warps per super-brick block
 constexpr int kSbChunk = 64;  // particles whose records are staged at a time
 
@@ -239,9 +242,20 @@ __device__ inline void sb_add(unsigned *p, double a, double b) {
   double const r = fma(a, b, 6755399441055744.0); // 1.5 * 2^52
   atomicAdd(p, static_cast<unsigned>(__double2loint(r)));
 }
+// FP64 path: the 64-bit t added as two 32-bit words (the low word's atomic
+// returns its old value, whose wrap-around gives the carry into the high
+// word), so the sum is exact modulo 2^64 with native 32-bit shared-memory
+// atomics only
 __device__ inline void sb_add(unsigned long long *p, double a, double b) {
   double const r = fma(a, b, 6755399441055744.0);
-  atomicAdd(p, static_cast<unsigned long long>(__double_as_longlong(r)) - 0x4338000000000000ull);
+  unsigned long long const t =
+      static_cast<unsigned long long>(__double_as_longlong(r)) - 0x4338000000000000ull;
+  unsigned *w = reinterpret_cast<unsigned *>(p); // little endian: w[0] low, w[1] high
+  unsigned const lo = static_cast<unsigned>(t);
+  unsigned const old = atomicAdd(w, lo);
+  unsigned const hi = static_cast<unsigned>(t >> 32) + ((old + lo < old) ? 1u : 0u);
+  if (hi != 0u)
+    atomicAdd(w + 1, hi);
 }
 __device__ inline float sb_value(unsigned v, float inv_s) {
   return static_cast<float>(static_cast<int>(v)) * inv_s;
@@ -250,15 +264,15 @@ __device__ inline double sb_value(unsigned long long v, double inv_s) {
   return static_cast<double>(static_cast<long long>(v)) * inv_s;
 }
 
-// Tile edge of a super-brick for order P.
-template <int P> __host__ __device__ constexpr int sb_tile_edge() { return kSbEdge + P - 1; }
+// Tile edge of a super-brick of edge E for order P.
+template <int P, int E> __host__ __device__ constexpr int sb_tile_edge() { return E + P - 1; }
 // Strides of the tile [x][y][z] (z contiguous, words of WB bytes): the
 // smallest y stride >= the tile edge and x stride >= edge * (y stride) for
 // which the lanes of one shared-memory wavefront (128 bytes: 32 lanes of
 // 4-byte words, 16 of 8-byte words), one (x, y) stencil row each (row
 // r = lane + 32 q, x = r / P, y = r % P), hit distinct banks.
-template <int P, int WB> __host__ __device__ constexpr TileStrides sb_strides() {
-  constexpr int TE = sb_tile_edge<P>();
+template <int P, int WB, int E> __host__ __device__ constexpr TileStrides sb_strides() {
+  constexpr int TE = sb_tile_edge<P, E>();
   constexpr int L = 128 / WB;
   for (int sy = TE; sy < TE + L; ++sy)
     for (int sx = TE * sy; sx < TE * sy + 2 * L; ++sx) {
@@ -279,22 +293,22 @@ template <int P, int WB> __host__ __device__ constexpr TileStrides sb_strides() 
     }
   return TileStrides{TE, TE * TE};
 }
-template <typename Real, int P> __host__ __device__ constexpr size_t sb_tile_bytes() {
+template <typename Real, int P, int E> __host__ __device__ constexpr size_t sb_tile_bytes() {
   using W = typename SbWord<Real>::type;
-  return (sizeof(W) * sb_tile_edge<P>() * static_cast<size_t>(sb_strides<P, sizeof(W)>().sx) +
+  return (sizeof(W) * sb_tile_edge<P, E>() * static_cast<size_t>(sb_strides<P, sizeof(W), E>().sx) +
           15) / 16 * 16;
 }
 // shared memory: tile, staged weight records, per staged particle its z
 // weights times S in FP64 (8 slots) and its tile offset
-template <typename Real, int P> __host__ __device__ constexpr size_t sb_smem() {
-  return sb_tile_bytes<Real, P>() + sizeof(Real) * kSbChunk * kRecStride +
+template <typename Real, int P, int E> __host__ __device__ constexpr size_t sb_smem() {
+  return sb_tile_bytes<Real, P, E>() + sizeof(Real) * kSbChunk * kRecStride +
          sizeof(double) * 8 * kSbChunk + sizeof(int) * kSbChunk;
 }
 // sort-brick runs of a super-brick: (kSbEdge / B)^2 brick columns, one
 // contiguous z run each
 constexpr int kSbMaxRuns = (kSbEdge / 4) * (kSbEdge / 4);
 
-template <typename Real, int P>
+template <typename Real, int P, int E>
 __global__ void __launch_bounds__(32 * kSbWarps, sizeof(Real) == 4 ? 4 : 1)
 k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, int nsb,
                 const int *__restrict__ start, const Real *__restrict__ W,
@@ -307,13 +321,13 @@ k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, 
   constexpr int P2 = P * P;
   constexpr int NQ = (P2 + 31) / 32;
   constexpr int NT = 32 * kSbWarps;
-  constexpr int E = kSbEdge;
-  constexpr int TE = sb_tile_edge<P>();
+  constexpr int TE = sb_tile_edge<P, E>();
   constexpr int B = brick_edge<P>(), B3 = B * B * B, NBS = E / B;
   constexpr int LB = (B == 4) ? 2 : 3;
-  constexpr TileStrides TS = sb_strides<P, sizeof(Word)>();
+  constexpr TileStrides TS = sb_strides<P, sizeof(Word), E>();
   constexpr int SY = TS.sy, SX = TS.sx;
-  constexpr int TW = static_cast<int>(sb_tile_bytes<Real, P>() / sizeof(Word));
+  constexpr int TW = static_cast<int>(sb_tile_bytes<Real, P, E>() / sizeof(Word));
+  static_assert(E % B == 0 && E <= kSbEdge, "super-brick edge: a multiple of the sort brick");
   constexpr int CH = kSbChunk;
   static_assert(NBS * NBS <= kSbMaxRuns, "run table too small");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -324,7 +338,7 @@ k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, 
   if (static_cast<int>(blockIdx.x) >= nsb)
     return; // whole block
   Word *tile = reinterpret_cast<Word *>(smem_raw);
-  Real *rec = reinterpret_cast<Real *>(smem_raw + sb_tile_bytes<Real, P>());
+  Real *rec = reinterpret_cast<Real *>(smem_raw + sb_tile_bytes<Real, P, E>());
   double *wzd = reinterpret_cast<double *>(rec + CH * WS);
   int *toff = reinterpret_cast<int *>(wzd + 8 * CH);
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -335,7 +349,7 @@ k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, 
   int const no1 = (M1 + E - 1) / E, no2 = (M2 + E - 1) / E;
   int const o0 = (sb.y / (no1 * no2)) * E, o1 = ((sb.y / no2) % no1) * E, o2 = (sb.y % no2) * E;
   // the super-brick's sort bricks (fewer at the high end of a mesh that is
-  // not a multiple of kSbEdge)
+  // not a multiple of E)
   int const bx0 = o0 / B, by0 = o1 / B, bz0 = o2 / B;
   int const nbx = min(NBS, G.nbx - bx0), nby = min(NBS, G.nby - by0), nbz = min(NBS, G.nbz - bz0);
   int const ncol = nbx * nby;
@@ -400,7 +414,7 @@ k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, 
         bulk_g2s(rec, W + static_cast<long long>(c0) * WS, nbytes, &bar);
       }
       for (int j = tid; j < cn; j += NT) {
-        // corner offset inside the super-brick, [0, kSbEdge)^3
+        // corner offset inside the super-brick, [0, E)^3
         int const sk = s_key[c0 + j];
         int const bz = bz0 + ((sk >> (3 * LB)) - b0);
         int const l = sk & (B3 - 1);

@@ -379,6 +379,13 @@ int p3mx_dp3m_get_tuned(const p3mx_dp3m *h, p3mx_tuned *out);
 int p3mx_dp3m_compute(p3mx_dp3m *h, size_t n, const double *pos,
                       const double *dip, double *f, double *torque,
                       double *energy, unsigned flags, void *stream);
+/* Stage profile (no counterpart in the reference): the host arrays pos and
+ * dip (3*n each) are staged, one evaluation of forces and torques runs
+ * unprofiled, then reps profiled ones; ms[k] is the mean device time of
+ * stage names[k] (static strings), *nstages the stage count. */
+int p3mx_dp3m_profile(p3mx_dp3m *h, size_t n, const double *pos,
+                      const double *dip, int reps, double *ms, const char **names,
+                      int cap, int *nstages);
 /* Kernels launched by the handle so far. */
 int p3mx_dp3m_launch_count(const p3mx_dp3m *h, long long *count);
 
