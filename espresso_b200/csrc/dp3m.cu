@@ -162,7 +162,7 @@ public:
                                         E.m_dist.as<Real>());
     ++E.m_launches;
     E.sort_keys(E.m_bkey.as<int>(), E.m_slot.as<int>(), E.m_cnt.as<int>(), E.m_start.as<int>(),
-                E.m_perm.as<int>(), E.m_nkeys, st);
+                E.m_perm.as<int>(), E.m_nkeys, st, nullptr, false);
     E.mark("dp_sort", st);
     // 2. the three component meshes: assignment and z pass each
     C const *tw = E.m_tw.as<C>();

@@ -525,6 +525,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_ccnt.ensure((m_cells + 1) * sizeof(int));
   m_cstart.ensure((m_cells + 1) * sizeof(int));
   m_cperm.ensure(n * sizeof(int));
+  m_cinv.ensure(n * sizeof(int));
   m_pq.ensure(n * sizeof(double4));
   m_spq.ensure(n * sizeof(double4));
   m_spf.ensure(n * sizeof(float4));
@@ -592,10 +593,12 @@ void Engine::census(cudaStream_t st) {
 }
 
 void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
-                       cudaStream_t st, const int *cond) {
+                       cudaStream_t st, const int *cond, bool index_order) {
   exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
   m_launches += 3;
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
+  if (!index_order)
+    return;
   k_fix_buckets<<<ceil_div(nkeys * 32, 256), 256, 0, st>>>(start, perm, nkeys, cond); ++m_launches;
   k_fix_big_buckets<<<static_cast<int>(std::min<long long>(ceil_div(nkeys, 256), 296)), 256, 0,
                       st>>>(
@@ -731,8 +734,11 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
     k_p3m_bin<Real><<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_n, m_key.as<int>(),
                                         m_bkey.as<int>(),
                                         m_slot.as<int>(), m_cnt.as<int>(), m_dist.as<Real>()); ++m_launches;
+    // the order inside a brick is left as the atomic slots made it: the
+    // fixed-point assignment sums integers and the interpolation treats
+    // every particle on its own, so the results do not depend on it
     sort_keys(m_bkey.as<int>(), m_slot.as<int>(), m_cnt.as<int>(), m_start.as<int>(),
-              m_perm.as<int>(), m_nkeys, st);
+              m_perm.as<int>(), m_nkeys, st, nullptr, false);
     mark("p3m_sort", st);
     k_p3m_weights<Real><<<nb, 256, 0, st>>>(geom, m_perm.as<int>(), m_key.as<int>(),
                                             m_dist.as<Real>(), d_q(), m_rep_of.as<int>(), m_n,
@@ -882,7 +888,7 @@ void Engine::build_lists(cudaStream_t st) {
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), nullptr); ++m_launches;
+                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), m_cinv.as<int>(), nullptr); ++m_launches;
   if (m_cap.size() != m_geom.size())
     set_list_capacity(1.5);
   int const R = n_rep();
@@ -931,23 +937,24 @@ __global__ void k_refresh_spq(const RepGeom *__restrict__ reps, const int *__res
                        qi);
 }
 
-// Displacement check fused with the sorted-position refresh, over the
-// cell-sorted order: sets *flag when a particle moved more than skin/2 or
-// changed type since the last build (k_displacement_check's test) and
-// writes the pair kernel's sorted records as k_refresh_spq does (a rebuild
-// that follows rewrites them).  One pass over the gathered positions
-// instead of two.
+// Displacement check fused with the sorted-position refresh: sets *flag
+// when a particle moved more than skin/2 or changed type since the last
+// build (k_displacement_check's test) and writes the pair kernel's sorted
+// records as k_refresh_spq does (a rebuild that follows rewrites them).
+// One thread per particle in index order (coalesced reads of positions,
+// reference positions, types and build-time cells), each writing its
+// records to its sorted slot inv[i].
 __global__ void k_check_refresh(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
-                                const int *__restrict__ perm, const double *__restrict__ pos,
-                                const double *__restrict__ q, const int *__restrict__ scell,
+                                const int *__restrict__ inv, const double *__restrict__ pos,
+                                const double *__restrict__ q, const int *__restrict__ ckey,
                                 const double *__restrict__ pos_ref, const int *__restrict__ type,
                                 const int *__restrict__ type_ref, long long n,
                                 double4 *__restrict__ spq, float4 *__restrict__ spf,
                                 int *__restrict__ flag) {
-  long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= n)
+  long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n)
     return;
-  int const i = perm[s];
+  int const s = inv[i];
   RepGeom const &G = reps[rep_of[i]];
   double d2 = 0.0;
 #pragma unroll
@@ -962,7 +969,7 @@ __global__ void k_check_refresh(const RepGeom *__restrict__ reps, const int *__r
   if (spq)
     spq[s] = make_double4(fold_coord(pos[3 * i], G.box[0]), fold_coord(pos[3 * i + 1], G.box[1]),
                           fold_coord(pos[3 * i + 2], G.box[2]), qi);
-  spf[s] = cell_offset(G, scell[s] - static_cast<int>(G.cell_off), pos_ref + 3 * i, pos + 3 * i,
+  spf[s] = cell_offset(G, ckey[i] - static_cast<int>(G.cell_off), pos_ref + 3 * i, pos + 3 * i,
                        qi);
 }
 
@@ -984,8 +991,8 @@ void Engine::prepare_short_range(cudaStream_t st, bool need_spq) {
     // check and refresh in one pass; the records it writes stand unless a
     // rebuild follows
     P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
-    k_check_refresh<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), d_pos(), d_q(),
-                                        m_scell.as<int>(), m_pos_ref.as<double>(), d_type(),
+    k_check_refresh<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cinv.as<int>(), d_pos(), d_q(),
+                                        m_ckey.as<int>(), m_pos_ref.as<double>(), d_type(),
                                         m_type_ref.as<int>(), m_n,
                                         need_spq ? m_spq.as<double4>() : nullptr,
                                         m_spf.as<float4>(), m_flag.as<int>());
@@ -1150,7 +1157,7 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
             m_cperm.as<int>(), m_cells, st, flag);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
-                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), flag); ++m_launches;
+                                    m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), m_cinv.as<int>(), flag); ++m_launches;
   k_verlet_build<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),

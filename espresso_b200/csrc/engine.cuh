@@ -162,8 +162,11 @@ private:
   void encode_field_maps(cudaStream_t st);
   // want_spq: also the FP64 double4 positions (FP64 pair kernel)
   void refresh_sorted_positions(cudaStream_t st, bool want_spq = true);
+  // Counting sort by key (perm: sorted position -> particle); index_order
+  // orders each bucket by particle index (deterministic), else the order
+  // inside a bucket is that of the atomic slots.
   void sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
-                 cudaStream_t st, const int *cond = nullptr);
+                 cudaStream_t st, const int *cond = nullptr, bool index_order = true);
 
   void mark(const char *name, cudaStream_t st);
 
@@ -214,6 +217,7 @@ private:
   std::vector<double> m_census_h;
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
+  DevBuf m_cinv; // sorted slot of each particle (inverse of m_cperm)
   DevBuf m_elc_epart;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_rflag, m_part_pair, m_sums_pair;
   DevBuf m_type_ref; // types at the last list build (a change triggers a rebuild)

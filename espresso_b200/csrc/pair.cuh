@@ -89,19 +89,20 @@ __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restri
   }
 }
 
-// Gather particle data into cell-sorted order.
+// Gather particle data into cell-sorted order (and the inverse permutation).
 __global__ void k_cell_gather(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                               const int *__restrict__ perm, const double4 *__restrict__ pq,
                               const int *__restrict__ type, const int *__restrict__ key,
                               long long n, double4 *__restrict__ spq, float4 *__restrict__ spf,
                               int *__restrict__ stype, int *__restrict__ scell,
-                              const int *__restrict__ cond) {
+                              int *__restrict__ inv, const int *__restrict__ cond) {
   if (cond && !*cond)
     return;
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
   int const i = perm[s];
+  inv[i] = static_cast<int>(s); // sorted slot of particle i
   double4 const v = pq[i];
   spq[s] = v;
   stype[s] = type ? type[i] : 0;
