@@ -1195,7 +1195,7 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
       auto forces = [&] {
         if (h->prm.epsilon != 0.)
           e.census(st);
-        e.forces_overlapped(fd, true, st);
+        e.forces_all(fd, true, st);
         if (h->elc)
           elc_add(h, fd, nullptr, st);
       };
@@ -1216,7 +1216,7 @@ int p3mx_forces(p3mx_handle *h, size_t n, const double *pos, const double *q, co
     bool const obs64 = h->prm.single_precision && !(flags & P3MX_MIXED_OBSERVABLES);
     if (!want_e && !want_v) {
       // forces only: real-space pairs concurrent with the k-space chain
-      e.forces_overlapped(fd, dev ? ow : true, st);
+      e.forces_all(fd, dev ? ow : true, st);
     } else {
       e.long_range(fd, dev ? ow : true, want_e && !obs64, want_v && !obs64, st, &enk, &virk);
       e.short_range(fd, false, (want_e || want_v) && !obs64, st, &ens, &virs);

@@ -111,16 +111,6 @@ Engine::Engine(bool fp32) : m_fp32(fp32) {
 }
 
 Engine::~Engine() {
-  if (m_side)
-    cudaStreamSynchronize(m_side);
-  if (m_ev_fork)
-    cudaEventDestroy(m_ev_fork);
-  if (m_ev_join)
-    cudaEventDestroy(m_ev_join);
-  if (m_ev_kdone)
-    cudaEventDestroy(m_ev_kdone);
-  if (m_side)
-    cudaStreamDestroy(m_side);
   if (m_stream)
     cudaStreamDestroy(m_stream);
 }
@@ -808,9 +798,7 @@ void Engine::long_range_t(double *f, bool overwrite, bool want_e, bool want_v,
                                                          m_cplx, m_E.as<Real>(), tw, m_kerr.as<int>());
   ++m_launches;
   mark("fft_inv_yz", st);
-  // 6. force back-interpolation (after the concurrent pair kernel, if any)
-  if (m_interp_wait)
-    P3MX_CUDA(cudaStreamWaitEvent(st, m_interp_wait, 0));
+  // 6. force back-interpolation
   for (int c = 1; m_n > 0 && c <= 7; ++c) {
     int const nbr = m_brick_off[c + 1] - m_brick_off[c];
     if (nbr == 0)
@@ -1059,43 +1047,25 @@ void Engine::short_range_t(double *f, bool overwrite, bool want_ev, cudaStream_t
 // Forces only (no energies or virials): the pair kernel runs on a side
 // stream, concurrently with the k-space chain (sort, assignment, FFTs); the
 // interpolation waits for it and adds the k-space forces on top.
-void Engine::forces_overlapped(double *f, bool overwrite, cudaStream_t st) {
+void Engine::forces_all(double *f, bool overwrite, cudaStream_t st) {
   if (m_n == 0 || m_profiling) {
     long_range(f, overwrite, false, false, st, nullptr, nullptr);
     short_range(f, false, false, st, nullptr, nullptr);
     bond_forces(f, st);
     return;
   }
-  if (m_side == nullptr) {
-    // the k-space chain (many dependent launches, each with a tail) runs at
-    // the highest stream priority; the pair kernel's blocks fill the SMs
-    // its tails and launch gaps leave free
-    int lo = 0, hi = 0;
-    P3MX_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-    P3MX_CUDA(cudaStreamCreateWithPriority(&m_side, cudaStreamNonBlocking, hi));
-    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_fork, cudaEventDisableTiming));
-    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_join, cudaEventDisableTiming));
-    P3MX_CUDA(cudaEventCreateWithFlags(&m_ev_kdone, cudaEventDisableTiming));
-  }
+  // one stream: the k-space chain first, so that the host waits for the
+  // list check's flag while the GPU is busy with it, then the pair kernel.
+  // The stage kernels each fill the GPU; this measured faster than the pair
+  // kernel on a second stream beside the k-space chain (1.58 vs 1.62 ms at
+  // 2^20 ions) and than the check and pair kernel first (1.60 ms)
+  long_range(f, overwrite, false, false, st, nullptr, nullptr);
   prepare_short_range(st, !m_fp32);
-  P3MX_CUDA(cudaEventRecord(m_ev_fork, st));
-  P3MX_CUDA(cudaStreamWaitEvent(m_side, m_ev_fork, 0));
-  // pair (+ bond) forces on the caller's stream; the interpolation, which
-  // adds onto them, waits for m_ev_join
   if (m_fp32)
-    launch_pair<float>(f, overwrite, false, st);
+    launch_pair<float>(f, false, false, st);
   else
-    launch_pair<double>(f, overwrite, false, st);
+    launch_pair<double>(f, false, false, st);
   bond_forces(f, st);
-  P3MX_CUDA(cudaEventRecord(m_ev_join, st));
-  struct Reset {
-    cudaEvent_t &ev;
-    ~Reset() { ev = nullptr; }
-  } reset{m_interp_wait};
-  m_interp_wait = m_ev_join;
-  long_range(f, false, false, false, m_side, nullptr, nullptr);
-  P3MX_CUDA(cudaEventRecord(m_ev_kdone, m_side));
-  P3MX_CUDA(cudaStreamWaitEvent(st, m_ev_kdone, 0));
 }
 
 void Engine::short_range(double *f, bool overwrite, bool want_ev, cudaStream_t st,

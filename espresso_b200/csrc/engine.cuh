@@ -105,8 +105,8 @@ public:
                    std::vector<double> *energies, std::vector<double> *virials,
                    bool fp64_math = false);
   // Forces of the whole path (k-space + real-space + LJ/WCA), no energies:
-  // the pair kernel overlaps the k-space chain on a side stream.
-  void forces_overlapped(double *f, bool overwrite, cudaStream_t st);
+  // the k-space chain, the list check, then the pair kernel, on one stream.
+  void forces_all(double *f, bool overwrite, cudaStream_t st);
   // Graph-capturable short-range evaluation (device-side rebuild decision).
   void short_range_graph(double *f, bool overwrite, cudaStream_t st);
   // Build lists now if invalid (capacity margin factor for graph use).
@@ -174,9 +174,6 @@ private:
   cudaStream_t m_stream = nullptr;
   long long m_launches = 0;
   bool m_profiling = false;
-  cudaStream_t m_side = nullptr;          // k-space chain of forces_overlapped (high priority)
-  cudaEvent_t m_ev_fork = nullptr, m_ev_join = nullptr, m_ev_kdone = nullptr;
-  cudaEvent_t m_interp_wait = nullptr;    // event the interpolation waits for
   std::vector<std::pair<std::string, cudaEvent_t>> m_marks;
   std::vector<ReplicaConf> m_conf;
   std::vector<RepGeom> m_geom;

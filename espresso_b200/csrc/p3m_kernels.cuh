@@ -137,38 +137,56 @@ __device__ inline void weights_record(const Real *dist3, double q, Real *__restr
 // each replica's largest |q| (FP32 bits rounded up, atomic maximum:
 // order-independent) for the fixed-point scale of the charge assignment.
 template <typename Real>
-__global__ void k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
-                              const int *__restrict__ key, const Real *__restrict__ dist,
-                              const double *__restrict__ q, const int *__restrict__ rep_of,
-                              long long n, Real *__restrict__ W, int *__restrict__ s_key,
-                              unsigned *__restrict__ qmax_bits) {
+__global__ void __launch_bounds__(256)
+k_p3m_weights(const RepGeom *__restrict__ reps, const int *__restrict__ perm,
+              const int *__restrict__ key, const Real *__restrict__ dist,
+              const double *__restrict__ q, const int *__restrict__ rep_of,
+              long long n, Real *__restrict__ W, int *__restrict__ s_key,
+              unsigned *__restrict__ qmax_bits) {
+  // FP32 records are built in shared memory and each warp's 32 records
+  // (contiguous in W) leave with 16-byte lane stores of consecutive
+  // addresses; a thread's own record would be 7 stores 112 bytes apart
+  constexpr bool kStage = sizeof(Real) == 4;
+  __shared__ __align__(16) Real s_rec[kStage ? 256 * kRecStride : 1];
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= n)
-    return;
-  int const i = perm[s];
-  int const rep = rep_of[i];
-  RepGeom const &G = reps[rep];
-  {
-    // one atomic per group of lanes of the same replica
-    unsigned const qb = __float_as_uint(__double2float_ru(fabs(q[i])));
-    unsigned const act = __activemask();
-    unsigned const grp = __match_any_sync(act, rep);
-    unsigned const mx = __reduce_max_sync(grp, qb);
-    if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1))
-      atomicMax(&qmax_bits[rep], mx);
+  int const lane = threadIdx.x & 31;
+  if (s < n) {
+    int const i = perm[s];
+    int const rep = rep_of[i];
+    RepGeom const &G = reps[rep];
+    {
+      // one atomic per group of lanes of the same replica
+      unsigned const qb = __float_as_uint(__double2float_ru(fabs(q[i])));
+      unsigned const act = __activemask();
+      unsigned const grp = __match_any_sync(act, rep);
+      unsigned const mx = __reduce_max_sync(grp, qb);
+      if (lane == __ffs(grp) - 1)
+        atomicMax(&qmax_bits[rep], mx);
+    }
+    Real *out = kStage ? s_rec + threadIdx.x * kRecStride : W + s * kRecStride;
+    const Real *d3 = dist + 3 * i;
+    switch (G.cao) {
+    case 1: weights_record<Real, 1>(d3, q[i], out); break;
+    case 2: weights_record<Real, 2>(d3, q[i], out); break;
+    case 3: weights_record<Real, 3>(d3, q[i], out); break;
+    case 4: weights_record<Real, 4>(d3, q[i], out); break;
+    case 5: weights_record<Real, 5>(d3, q[i], out); break;
+    case 6: weights_record<Real, 6>(d3, q[i], out); break;
+    default: weights_record<Real, 7>(d3, q[i], out); break;
+    }
+    s_key[s] = key[i] - static_cast<int>(G.bin_off);
   }
-  Real *out = W + s * kRecStride;
-  const Real *d3 = dist + 3 * i;
-  switch (G.cao) {
-  case 1: weights_record<Real, 1>(d3, q[i], out); break;
-  case 2: weights_record<Real, 2>(d3, q[i], out); break;
-  case 3: weights_record<Real, 3>(d3, q[i], out); break;
-  case 4: weights_record<Real, 4>(d3, q[i], out); break;
-  case 5: weights_record<Real, 5>(d3, q[i], out); break;
-  case 6: weights_record<Real, 6>(d3, q[i], out); break;
-  default: weights_record<Real, 7>(d3, q[i], out); break;
+  if constexpr (kStage) {
+    __syncwarp();
+    long long const s0 = s - lane;
+    if (s0 >= n)
+      return;
+    int const nv = static_cast<int>(min(32LL, n - s0));
+    const float4 *src = reinterpret_cast<const float4 *>(s_rec + (threadIdx.x - lane) * kRecStride);
+    float4 *dst = reinterpret_cast<float4 *>(W + s0 * kRecStride);
+    for (int k = lane; k < nv * (kRecStride / 4); k += 32)
+      dst[k] = src[k];
   }
-  s_key[s] = key[i] - static_cast<int>(G.bin_off);
 }
 
 // Edge (mesh points) of the sort bricks that bin the particles by stencil
