@@ -961,7 +961,7 @@ def run_dipolar(args):
             # the parameters the tuner chose for 2^17 dipoles in a plain run
             # (timings under a profiler would mislead the tuner)
             act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, tune=False,
-                             mesh=96, cao=7, r_cut=5.23, alpha=0.635)
+                             mesh=112, cao=7, r_cut=4.70, alpha=0.718)
         else:
             act = DipolarP3M(prefactor=1.0, accuracy=1e-4, single_precision=sprec, timings=2,
                              verbose=False)
