@@ -4,9 +4,10 @@
 //
 // Pipeline of one force/torque/energy evaluation (one cubic system):
 //  1. k_dp3m_prepare: moment components, list selector, census partials;
-//  2. brick binning and sort of the particles (once), then per component
-//     d = x, y, z: weights with q = mu_d, the coloured super-brick
-//     assignment, the r2c z pass; one y pass over the three spectra;
+//  2. brick binning and sort of the particles (once), weight records with
+//     q = mu_d for each component d = x, y, z, the coloured super-brick
+//     assignment of all three per colour launch, the r2c z pass of each;
+//     one y pass over the three spectra;
 //  3. k_fft_x_dp3m in three modes (torque fields with the energy sum, the
 //     two halves of the force-field tensor), each followed by the backward
 //     y and z passes and the back-interpolation with unit-charge weights;
@@ -71,6 +72,11 @@ public:
     m_smu.ensure(nn * sizeof(double4));
     m_ck3.ensure(3 * E.m_cplx * csz);
     m_ge.ensure(E.m_cplx * rsz);
+    // three weight-record sets and meshes for the one-launch assignment
+    // (+ slack: the z pass stages 16-byte aligned supersets of mesh rows)
+    m_W3.ensure(3 * static_cast<size_t>(kRecStride) * nn * rsz);
+    m_rho3.ensure(3 * E.m_bins * rsz + 64);
+    m_qmax3.ensure(4 * sizeof(unsigned));
     m_gf.ensure(E.m_cplx * rsz);
     long long const nprep = ceil_div(nn, 256);
     size_t const np = std::max<size_t>({static_cast<size_t>(E.m_n_blk_x), 5 * static_cast<size_t>(nprep),
@@ -164,17 +170,23 @@ public:
     E.sort_keys(E.m_bkey.as<int>(), E.m_slot.as<int>(), E.m_cnt.as<int>(), E.m_start.as<int>(),
                 E.m_perm.as<int>(), E.m_nkeys, st, nullptr, false);
     E.mark("dp_sort", st);
-    // 2. the three component meshes: assignment and z pass each
+    // 2. the three component meshes: weight records per component, then
+    // every colour launch assigns all three (blockIdx.y = component), then
+    // the z pass of each
     C const *tw = E.m_tw.as<C>();
     C *ck3 = m_ck3.as<C>();
+    long long const wst = static_cast<long long>(kRecStride) * n;
+    unsigned *qmax3 = m_qmax3.as<unsigned>();
+    P3MX_CUDA(cudaMemsetAsync(qmax3, 0, 3 * sizeof(unsigned), st));
     for (int d = 0; d < 3; ++d) {
-      P3MX_CUDA(cudaMemsetAsync(qmax_bits, 0, sizeof(unsigned), st));
       k_p3m_weights<Real><<<nb, 256, 0, st>>>(geom, E.m_perm.as<int>(), E.m_key.as<int>(),
                                               E.m_dist.as<Real>(), m_comp.as<double>() + d * n,
-                                              E.m_rep_of.as<int>(), n, E.m_W.as<Real>(),
-                                              E.m_skey.as<int>(), qmax_bits);
+                                              E.m_rep_of.as<int>(), n, m_W3.as<Real>() + d * wst,
+                                              E.m_skey.as<int>(), qmax3 + d);
       ++E.m_launches;
-      P3MX_CUDA(cudaMemsetAsync(E.m_rho.p, 0, E.m_bins * sizeof(Real), st));
+    }
+    P3MX_CUDA(cudaMemsetAsync(m_rho3.p, 0, 3 * E.m_bins * sizeof(Real), st));
+    {
       bool chained = false;
       for (size_t p = 0; p + 1 < E.m_phase_off.size(); ++p) {
         int const cnt = E.m_phase_off[p + 1] - E.m_phase_off[p];
@@ -183,15 +195,17 @@ public:
         int2 const *tab = E.m_blk_mesh.as<int2>() + E.m_phase_off[p];
         P3MX_CAO_DISPATCH_R(E.m_phase_cao[p],
                             (launch_assign<Real, P>(E.m_sb_edge, chained, cnt, st, geom, tab,
-                                                    E.m_start.as<int>(),
-                                                    E.m_W.as<Real>(), E.m_skey.as<int>(),
-                                                    qmax_bits, E.m_rho.as<Real>(),
-                                                    E.m_kerr.as<int>())));
+                                                    E.m_start.as<int>(), m_W3.as<Real>(),
+                                                    E.m_skey.as<int>(), qmax3, m_rho3.as<Real>(),
+                                                    E.m_kerr.as<int>(), 3, wst, E.m_bins, 1)));
         chained = true;
         ++E.m_launches;
       }
+    }
+    for (int d = 0; d < 3; ++d) {
       k_fft_z_fwd<Real><<<E.m_n_blk_zf, 256, E.m_smem_zf, st>>>(
-          geom, E.m_blk_zf.as<Blk>(), E.m_rho.as<Real>(), ck3 + d * E.m_cplx, tw, E.m_kerr.as<int>());
+          geom, E.m_blk_zf.as<Blk>(), m_rho3.as<Real>() + d * E.m_bins, ck3 + d * E.m_cplx, tw,
+          E.m_kerr.as<int>());
       ++E.m_launches;
     }
     E.mark("dp_assign_fft_z", st);
@@ -402,6 +416,7 @@ public:
 private:
   Engine m_eng;
   DevBuf m_mu, m_comp, m_out, m_smu, m_ck3, m_ge, m_gf, m_part, m_sums, m_flag, m_geom_interp;
+  DevBuf m_W3, m_rho3, m_qmax3;
   bool m_g_valid = false, m_phi_valid = false, m_table_set = false;
   double m_phi = 0.0;
   int m_M = 0, m_cao = 0;

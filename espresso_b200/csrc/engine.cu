@@ -647,9 +647,10 @@ namespace {
 template <typename Real, int P, int E>
 void launch_assign_e(bool chained, int cnt, cudaStream_t st, RepGeom const *geom, int2 const *tab,
                      int const *start, Real const *W, int const *s_key, unsigned const *qmax_bits,
-                     Real *rho, int *err) {
+                     Real *rho, int *err, int ncomp, long long comp_w, long long comp_rho,
+                     int comp_q) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(static_cast<unsigned>(cnt));
+  cfg.gridDim = dim3(static_cast<unsigned>(cnt), static_cast<unsigned>(ncomp));
   cfg.blockDim = dim3(32 * kSbWarps);
   cfg.dynamicSmemBytes = sb_smem<Real, P, E>();
   cfg.stream = st;
@@ -659,19 +660,21 @@ void launch_assign_e(bool chained, int cnt, cudaStream_t st, RepGeom const *geom
   cfg.attrs = at;
   cfg.numAttrs = chained ? 1 : 0;
   P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign_sb<Real, P, E>, geom, tab, cnt, start, W, s_key,
-                               qmax_bits, rho, err));
+                               qmax_bits, rho, err, comp_w, comp_rho, comp_q));
 }
-// ... with the engine's super-brick edge (16 or 8)
+// ... with the engine's super-brick edge (16 or 8); ncomp charge sets
+// (records, meshes and |q| maxima comp_w / comp_rho / comp_q apart)
 template <typename Real, int P>
 void launch_assign(int edge, bool chained, int cnt, cudaStream_t st, RepGeom const *geom,
                    int2 const *tab, int const *start, Real const *W, int const *s_key,
-                   unsigned const *qmax_bits, Real *rho, int *err) {
+                   unsigned const *qmax_bits, Real *rho, int *err, int ncomp = 1,
+                   long long comp_w = 0, long long comp_rho = 0, int comp_q = 0) {
   if (edge == kSbEdgeSmall)
     launch_assign_e<Real, P, kSbEdgeSmall>(chained, cnt, st, geom, tab, start, W, s_key, qmax_bits,
-                                           rho, err);
+                                           rho, err, ncomp, comp_w, comp_rho, comp_q);
   else
     launch_assign_e<Real, P, kSbEdge>(chained, cnt, st, geom, tab, start, W, s_key, qmax_bits, rho,
-                                      err);
+                                      err, ncomp, comp_w, comp_rho, comp_q);
 }
 
 // Persistent grid of the back-interpolation pipeline: resident blocks per

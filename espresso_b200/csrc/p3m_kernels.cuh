@@ -331,7 +331,14 @@ __global__ void __launch_bounds__(32 * kSbWarps, sizeof(Real) == 4 ? 4 : 1)
 k_p3m_assign_sb(const RepGeom *__restrict__ reps, const int2 *__restrict__ sbs, int nsb,
                 const int *__restrict__ start, const Real *__restrict__ W,
                 const int *__restrict__ s_key, const unsigned *__restrict__ qmax_bits,
-                Real *__restrict__ rho, int *__restrict__ err) {
+                Real *__restrict__ rho, int *__restrict__ err, long long comp_w,
+                long long comp_rho, int comp_q) {
+  // blockIdx.y picks one of several charge sets assigned by one launch (the
+  // dipole components): its weight records, mesh and |q| maxima lie
+  // comp_w / comp_rho / comp_q elements after the previous set's
+  W += blockIdx.y * comp_w;
+  rho += blockIdx.y * comp_rho;
+  qmax_bits += blockIdx.y * comp_q;
   using Word = typename SbWord<Real>::type;
   constexpr int R = 4;
   constexpr int WS = kRecStride;

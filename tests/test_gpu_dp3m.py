@@ -266,3 +266,65 @@ def test_md_run_with_dipolar_forces():
     f, t, e = _forces_torques_energy(s)
     fo, to, eo = O.dp3m(L, s.part.all().pos, s.part.all().dip, 1.0, 0.9, 3.0, 16, 5, 1e-4)
     assert _rel(f, fo) < 1e-9 and _rel(t, to) < 1e-9
+
+
+def test_c_abi_device_pointers_and_energy_only():
+    """p3mx_dp3m_compute through the C ABI with device pointers (torch CUDA
+    tensors), accumulating into given forces and torques (no
+    P3MX_OVERWRITE), and an energy-only call, against the host-pointer
+    results of the same handle."""
+    import ctypes
+    import torch
+    from espresso_b200 import _lib
+    L, n = 10.0, 70
+    pos, dip = _random(n, L, 31)
+    act = DipolarP3M(prefactor=1.2, tune=False, alpha=0.9, r_cut=3.0, mesh=16, cao=5,
+                     accuracy=1e-4)
+    act._set_system([L] * 3, 0.4, (True,) * 3)
+    act._activate(pos, dip)
+    f_h, t_h, e_h = act._compute(pos, dip, forces=True, energy=True)
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    pos_d = torch.from_numpy(pos).to(dev)
+    dip_d = torch.from_numpy(dip).to(dev)
+    f0 = torch.full((n, 3), 0.5, dtype=torch.float64, device=dev)
+    t0 = torch.full((n, 3), -0.25, dtype=torch.float64, device=dev)
+    e = np.zeros(2)
+    flags = _lib.P3MX_DEVICE_PTRS | _lib.P3MX_FORCES | _lib.P3MX_ENERGY
+    rc = lib.p3mx_dp3m_compute(act._handle, n, _lib.dptr(pos_d), _lib.dptr(dip_d), _lib.dptr(f0),
+                               _lib.dptr(t0), e.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               flags, None)
+    act._check(rc)
+    torch.cuda.synchronize(dev)
+    # the same kernels on the same inputs: equal up to the rounding of the
+    # offsets the results were added to
+    assert _rel(f0.cpu().numpy() - 0.5, f_h) < 1e-12
+    assert _rel(t0.cpu().numpy() + 0.25, t_h) < 1e-12
+    assert e.sum() == pytest.approx(e_h, rel=1e-13)
+    _, _, e_only = act._compute(pos, dip, forces=False, energy=True)
+    assert e_only == pytest.approx(e_h, rel=1e-13)
+    count = ctypes.c_longlong()
+    act._check(lib.p3mx_dp3m_launch_count(act._handle, ctypes.byref(count)))
+    assert count.value > 0
+
+
+def test_stage_profile_entry_point():
+    import ctypes
+    from espresso_b200 import _lib
+    L, n = 10.0, 50
+    pos, dip = _random(n, L, 32)
+    act = DipolarP3M(prefactor=1.0, tune=False, alpha=0.9, r_cut=3.0, mesh=16, cao=5,
+                     accuracy=1e-4)
+    act._set_system([L] * 3, 0.4, (True,) * 3)
+    act._activate(pos, dip)
+    lib = _lib.load()
+    names = (ctypes.c_char_p * 32)()
+    ms = (ctypes.c_double * 32)()
+    nst = ctypes.c_int()
+    p = _lib.as_f64(pos)
+    d = _lib.as_f64(dip)
+    act._check(lib.p3mx_dp3m_profile(act._handle, n, _lib.dptr(p), _lib.dptr(d), 2, ms, names, 32,
+                                     ctypes.byref(nst)))
+    got = {names[k].decode() for k in range(nst.value)}
+    assert {"dp_assign_fft_z", "dp_x_pass", "dp_interp", "dp_pairs"} <= got
+    assert all(ms[k] >= 0.0 for k in range(nst.value))
