@@ -124,6 +124,7 @@ SIGNATURES = {
                                     ctypes.c_int, _ip]),
     "p3mx_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "p3mx_resort": (ctypes.c_int, [_vp]),
+    "p3mx_exp_check": (ctypes.c_int, [_sz, _vp, _vp, _vp]),
     "p3mx_error_estimate": (ctypes.c_int, [_ip, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, _dp, ctypes.c_double,
                                            _dp, _dp]),

@@ -1341,6 +1341,17 @@ int p3mx_launch_count(const p3mx_handle *h, long long *count) {
   return P3MX_OK;
 }
 
+int p3mx_exp_check(size_t n, const float *x, float *out, void *stream) {
+  if (n && (!x || !out))
+    return P3MX_EDOMAIN;
+  if (n == 0)
+    return P3MX_OK;
+  cudaStream_t const st = static_cast<cudaStream_t>(stream);
+  long long const nn = static_cast<long long>(n);
+  k_exp_check<<<static_cast<unsigned>((nn + 255) / 256), 256, 0, st>>>(nn, x, out);
+  return cudaGetLastError() == cudaSuccess ? P3MX_OK : P3MX_ECUDA;
+}
+
 int p3mx_error_estimate(const int *mesh, int cao, int n_c_part, double sum_q2, double alpha_L,
                         double r_cut_iL, const double *box, double prefactor, double *rs_err,
                         double *ks_err) {

@@ -542,6 +542,20 @@ __device__ inline float ex2_approx(float x) {
   return e;
 }
 
+// The FP32 exponentials of the real-space kernels on n values, for their
+// accuracy test: out[k] = exp_fast(x), out[n + k] = one ex2.approx of
+// x log2(e) rounded to FP32 (the form of the force-only kernel, which folds
+// log2(e) into its coefficient), out[2n + k] = CUDA's expf(x).
+__global__ void k_exp_check(long long n, const float *__restrict__ x, float *__restrict__ out) {
+  long long const k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  float const v = x[k];
+  out[k] = exp_fast(v);
+  out[n + k] = ex2_approx(v * 1.44269504088896341f);
+  out[2 * n + k] = expf(v);
+}
+
 __device__ inline float rsqrt_approx(float x) {
   float r;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));

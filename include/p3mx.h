@@ -242,6 +242,11 @@ int p3mx_profile(p3mx_handle *h, int reps, double *ms, const char **names,
 int p3mx_resort(p3mx_handle *h);
 /* Total number of kernels launched by the handle's engines so far. */
 int p3mx_launch_count(const p3mx_handle *h, long long *count);
+/* Accuracy check of the FP32 exponentials of the FP32-mixed real-space
+ * kernels (no counterpart in the reference): for n device values x, writes
+ * to the device array out (3n floats) exp_fast(x), the single hardware
+ * ex2 of x log2(e) the force-only kernel uses, and CUDA's expf(x). */
+int p3mx_exp_check(size_t n, const float *x, float *out, void *stream);
 
 /* Tuning error estimates (p3m.cpp:187-243; GPU k-space sum of
  * p3m_gpu_error_cuda.cu:87-143). */
