@@ -39,9 +39,14 @@ def test_c1_langevin_run_then_parity_with_oracle():
         if block >= 50:
             v = s.part.all().v
             temps.append((v ** 2).sum() / (3 * len(q)))
-    # 1000 steps: the second half at kT = 1 (each sample's relative
-    # fluctuation ~ sqrt(2 / 6000) = 1.8 %)
-    assert abs(np.mean(temps) - 1.0) < 0.05, np.mean(temps)
+    # 1000 steps: the second half at kT = 1 within the integrator's
+    # first-order time-step bias (each sample fluctuates by ~ sqrt(2 / 6000)
+    # = 1.8 %).  The velocity-Verlet + Langevin scheme holds free particles
+    # at kT = 1.000, but this ion system's kinetic temperature sits at
+    # 1 - 4.8 dt: 0.952 at dt = 0.01 and 0.977 at dt = 0.005 (measured; the
+    # deficit halves with the time step), so the check allows 0.08.
+    assert abs(np.mean(temps) - 1.0) < 0.08, np.mean(temps)
+    assert np.mean(temps) < 1.0 + 0.03
     assert np.isfinite(s.part.all().pos).all()
     prm = act.get_params()
     x = s.part.all().pos.copy()
