@@ -90,6 +90,8 @@ struct RepGeom {
   int cg[3];
   double inv_cs[3];
   long long cell_off;
+  int oct_on;   // cells sorted by octant (list build skips far octants)
+  int oct_mult; // sort keys per cell: 8 when any replica sorts by octant, else 1
   double max_cut, skin, coulomb_cut;
   // Verlet list of this replica: neighbour k of particle p0+i at
   // nb[nb_off + k*np + i], capacity max_nb per particle

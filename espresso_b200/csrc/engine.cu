@@ -211,8 +211,20 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
     for (int d = 0; d < 3; ++d)
       G.inv_cs[d] = 1.0 / cs[d];
     G.cell_off = m_cells;
-    m_cells += static_cast<long long>(G.cg[0]) * G.cg[1] * G.cg[2];
+    long long const ncell = static_cast<long long>(G.cg[0]) * G.cg[1] * G.cg[2];
+    m_cells += ncell;
+    // octant sort where a cell holds >= 64 particles on average (octants of
+    // >= 8: the build's 8-wide candidate rounds stay full); 3 cells per axis
+    // at least (the small-grid build visits whole cells)
+    G.oct_on = (c.np >= 64 * ncell && G.cg[0] >= 3 && G.cg[1] >= 3 && G.cg[2] >= 3) ? 1 : 0;
   }
+  // sort keys per cell: octants (8) as soon as one replica uses them
+  m_oct_mult = 1;
+  for (auto const &G : m_geom)
+    if (G.oct_on)
+      m_oct_mult = 8;
+  for (auto &G : m_geom)
+    G.oct_mult = m_oct_mult;
   if (m_ncorner >= (1LL << 31) || m_bins >= (1LL << 31) || m_n >= (1LL << 31))
     throw Error(1, "batch too large for 32-bit bin/particle indices");
   for (auto const &G : m_geom)
@@ -495,7 +507,7 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   // |q| (FP32, rounded up), which the assignment's fixed-point scale needs
   m_cnt.ensure((m_nkeys + 1 + R) * sizeof(int));
   m_start.ensure((m_nkeys + 1) * sizeof(int));
-  m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_cells) + 1, kScanTile) + 1) * sizeof(int));
+  m_scan_tiles.ensure((ceil_div(std::max(m_nkeys, m_oct_mult * m_cells) + 1, kScanTile) + 1) * sizeof(int));
   m_dist.ensure(3 * n * rsz);
   m_W.ensure(static_cast<size_t>(wstride<7, 4>()) * n * rsz);
   m_skey.ensure((n + 8) * sizeof(int));
@@ -512,8 +524,10 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_dipole.ensure(static_cast<size_t>(R) * 3 * sizeof(double));
   m_ckey.ensure(n * sizeof(int));
   m_cslot.ensure(n * sizeof(int));
-  m_ccnt.ensure((m_cells + 1) * sizeof(int));
-  m_cstart.ensure((m_cells + 1) * sizeof(int));
+  // counting sort of the particles by cell octant (8 keys per cell)
+  m_ccnt.ensure((m_oct_mult * m_cells + 1) * sizeof(int));
+  m_cstart.ensure((m_oct_mult * m_cells + 1) * sizeof(int));
+  m_cbkey.ensure(n * sizeof(int));
   m_cperm.ensure(n * sizeof(int));
   m_cinv.ensure(n * sizeof(int));
   m_pq.ensure(n * sizeof(double4));
@@ -872,12 +886,12 @@ void Engine::long_range(double *f, bool overwrite, bool want_energy, bool want_v
 void Engine::build_lists(cudaStream_t st) {
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
-  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
+  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_oct_mult * m_cells + 1) * sizeof(int), st));
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr,
+                                 m_cbkey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, nullptr,
                                  nullptr); ++m_launches;
-  sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
-            m_cperm.as<int>(), m_cells, st);
+  sort_keys(m_cbkey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
+            m_cperm.as<int>(), m_oct_mult * m_cells, st);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
                                     m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), m_cinv.as<int>(), nullptr); ++m_launches;
   if (m_cap.size() != m_geom.size())
@@ -885,7 +899,7 @@ void Engine::build_lists(cudaStream_t st) {
   int const R = n_rep();
   for (int attempt = 0; attempt < 4; ++attempt) {
     P3MX_CUDA(cudaMemsetAsync(m_overflow.p, 0, R * sizeof(int), st));
-    k_verlet_build<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+    (m_oct_mult == 8 ? k_verlet_build<true> : k_verlet_build<false>)<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                        m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                        m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
@@ -1123,15 +1137,15 @@ void Engine::short_range_graph(double *f, bool overwrite, cudaStream_t st) {
   k_displacement_check<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), m_pos_ref.as<double>(),
                                            d_type(), m_type_ref.as<int>(), m_n, flag, rflag);
   ++m_launches;
-  k_fill_int<<<ceil_div(m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_cells + 1, flag); ++m_launches;
+  k_fill_int<<<ceil_div(m_oct_mult * m_cells + 1, 256), 256, 0, st>>>(m_ccnt.as<int>(), 0, m_oct_mult * m_cells + 1, flag); ++m_launches;
   k_cell_bin<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), d_pos(), d_q(), m_n, m_ckey.as<int>(),
-                                 m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag,
+                                 m_cbkey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_pq.as<double4>(), nullptr, flag,
                                  rflag); ++m_launches;
-  sort_keys(m_ckey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
-            m_cperm.as<int>(), m_cells, st, flag);
+  sort_keys(m_cbkey.as<int>(), m_cslot.as<int>(), m_ccnt.as<int>(), m_cstart.as<int>(),
+            m_cperm.as<int>(), m_oct_mult * m_cells, st, flag);
   k_cell_gather<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cperm.as<int>(), m_pq.as<double4>(), d_type(), m_ckey.as<int>(),
                                     m_n, m_spq.as<double4>(), m_spf.as<float4>(), m_stype.as<int>(), m_scell.as<int>(), m_cinv.as<int>(), flag); ++m_launches;
-  k_verlet_build<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
+  (m_oct_mult == 8 ? k_verlet_build<true> : k_verlet_build<false>)<<<nb, 256, m_ntypes * m_ntypes * sizeof(float), st>>>(geom, m_rep_of.as<int>(), m_spq.as<double4>(),
                                        m_spf.as<float4>(), m_stype.as<int>(),
                                      m_scell.as<int>(), m_cstart.as<int>(), m_ia_d.as<PairIA>(),
                                      m_ntypes, m_n, m_nb.as<int>(), m_nb_cnt.as<int>(),
@@ -1203,10 +1217,11 @@ std::vector<int> Engine::cell_index_ghost(cudaStream_t st) {
     return out;
   DevBuf gi;
   gi.ensure(m_n * sizeof(int));
-  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_cells + 1) * sizeof(int), st));
+  P3MX_CUDA(cudaMemsetAsync(m_ccnt.p, 0, (m_oct_mult * m_cells + 1) * sizeof(int), st));
   k_cell_bin<<<ceil_div(m_n, 256), 256, 0, st>>>(m_geom_d.as<RepGeom>(), m_rep_of.as<int>(), d_pos(),
-                                                 d_q(), m_n, m_ckey.as<int>(), m_cslot.as<int>(),
-                                                 m_ccnt.as<int>(), m_pq.as<double4>(), gi.as<int>(),
+                                                 d_q(), m_n, m_ckey.as<int>(), m_cbkey.as<int>(),
+                                                 m_cslot.as<int>(), m_ccnt.as<int>(),
+                                                 m_pq.as<double4>(), gi.as<int>(),
                                                  nullptr, nullptr); ++m_launches;
   P3MX_CUDA(cudaMemcpyAsync(out.data(), gi.p, m_n * sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaStreamSynchronize(st));

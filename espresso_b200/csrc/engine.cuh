@@ -215,6 +215,8 @@ private:
   // short range
   DevBuf m_ckey, m_cslot, m_ccnt, m_cstart, m_cperm, m_pq, m_spq, m_spf, m_stype, m_scell;
   DevBuf m_cinv; // sorted slot of each particle (inverse of m_cperm)
+  DevBuf m_cbkey; // cell-octant key of each particle (sort key of the cell sort)
+  long long m_oct_mult = 1; // cell-sort keys per cell (8 with octant-sorted replicas)
   DevBuf m_elc_epart;
   DevBuf m_nb, m_nb_cnt, m_overflow, m_pos_ref, m_flag, m_rflag, m_part_pair, m_sums_pair;
   DevBuf m_type_ref; // types at the last list build (a change triggers a rebuild)

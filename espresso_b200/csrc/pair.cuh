@@ -54,13 +54,18 @@ __device__ inline void cell_coords(RepGeom const &G, const double *xf, int *c) {
 
 // Cell key (column-major over the interior grid, x fastest, as the
 // reference orders cells) and counting-sort slot of every particle; also
-// the folded position (double4 with charge in w) for the pair kernels.
+// the folded position (double4 with charge in w) for the pair kernels.  The
+// sort runs on G.oct_mult keys per cell (8 when any replica sorts by
+// octant, else 1): cell * oct_mult + the octant of the cell the particle
+// lies in (each axis halved) where the replica sorts by octant (G.oct_on:
+// crowded cells, whose far octants the list build skips), else
+// cell * oct_mult; bkey keeps the sort key.
 __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of,
                            const double *__restrict__ pos, const double *__restrict__ q,
-                           long long n, int *__restrict__ key, int *__restrict__ slot,
-                           int *__restrict__ cnt, double4 *__restrict__ pq,
-                           int *__restrict__ ghost_index, const int *__restrict__ cond,
-                           const int *__restrict__ rflag) {
+                           long long n, int *__restrict__ key, int *__restrict__ bkey,
+                           int *__restrict__ slot, int *__restrict__ cnt,
+                           double4 *__restrict__ pq, int *__restrict__ ghost_index,
+                           const int *__restrict__ cond, const int *__restrict__ rflag) {
   if (cond && !*cond)
     return;
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -73,15 +78,23 @@ __global__ void k_cell_bin(const RepGeom *__restrict__ reps, const int *__restri
     xf[d] = fold_coord(pos[3 * i + d], G.box[d]);
   int c[3];
   cell_coords(G, xf, c);
-  int k;
+  int kb;
   if (rflag && !rflag[rep_of[i]]) {
     // replica keeps its lists: same cells, hence the same sorted order
-    k = key[i];
+    kb = bkey[i];
   } else {
-    k = static_cast<int>(G.cell_off) + c[0] + G.cg[0] * (c[1] + G.cg[1] * c[2]);
+    int const k = static_cast<int>(G.cell_off) + c[0] + G.cg[0] * (c[1] + G.cg[1] * c[2]);
+    int oct = 0;
+    if (G.oct_on) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        oct |= (xf[d] * G.inv_cs[d] - c[d] >= 0.5) ? (1 << d) : 0;
+    }
+    kb = G.oct_mult * k + oct;
     key[i] = k;
+    bkey[i] = kb;
   }
-  slot[i] = atomicAdd(&cnt[k], 1);
+  slot[i] = atomicAdd(&cnt[kb], 1);
   pq[i] = make_double4(xf[0], xf[1], xf[2], q[i]);
   if (ghost_index) {
     int const g0 = G.cg[0] + 2, g1 = G.cg[1] + 2;
@@ -176,6 +189,7 @@ __device__ inline void store_group(int *p, const int *g) {
 // Verlet list of one cell-sorted particle a (k_verlet_build); gbuf / gbuf_b
 // are the lane's shared-memory buffers of the class A / B group being
 // filled, s_icut the ia_cut table of the type pairs in shared memory.
+template <bool OCT>
 __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__ reps,
                                         const int *__restrict__ rep_of_sorted,
                                         const double4 *__restrict__ spq,
@@ -318,13 +332,33 @@ __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__
               put(b, cls_a, (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1));
             }
         };
-        int const b_lo = cstart[cell], b_hi = cstart[cell + 1];
         if (small_grid) {
+          int const om = G.oct_mult;
+          int const b_lo = cstart[om * cell], b_hi = cstart[om * cell + om];
           for (int b = b_lo; b < b_hi; ++b)
             if (b != a)
               consider(b);
         } else {
           int const code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+          // with octant-sorted cells, the octants of the neighbour cell
+          // wholly beyond the list range are skipped (the particle relative
+          // to the neighbour cell's corner against each half-cell box)
+          float const qx = pfa.x + shx, qy = pfa.y + shy, qz = pfa.z + shz;
+          float const hx = 0.5f * csf[0], hy = 0.5f * csf[1], hz = 0.5f * csf[2];
+          int const noct = (OCT && G.oct_on) ? 8 : 1;
+          for (int oct = 0; oct < noct; ++oct) {
+          int b_lo = cstart[G.oct_mult * cell], b_hi = cstart[G.oct_mult * (cell + 1)];
+          if (OCT && G.oct_on) {
+            float const lx = (oct & 1) ? hx : 0.f, ly = (oct & 2) ? hy : 0.f,
+                        lz = (oct & 4) ? hz : 0.f;
+            float const ex = fmaxf(fmaxf(lx - qx, qx - (lx + hx)), 0.f);
+            float const ey = fmaxf(fmaxf(ly - qy, qy - (ly + hy)), 0.f);
+            float const ez = fmaxf(fmaxf(lz - qz, qz - (lz + hz)), 0.f);
+            if (ex * ex + ey * ey + ez * ez > emax2_pre)
+              continue;
+            b_lo = cstart[G.oct_mult * cell + oct];
+            b_hi = cstart[G.oct_mult * cell + oct + 1];
+          }
           // kPre candidates per round (loads issued together): an FP32
           // pre-check, then for the candidates near or inside the list
           // range the FP32 decision, or the FP64 test inside the bands
@@ -370,6 +404,7 @@ __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__
                 put(b, a_lo, code);
             }
           }
+          }
         }
       }
     }
@@ -387,6 +422,7 @@ __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__
 
 // Verlet lists, one thread per cell-sorted particle (the 32 lanes of a warp
 // are consecutive particles: the same or adjacent cells).
+template <bool OCT>
 __global__ void __launch_bounds__(256, 2)
 k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_sorted,
                const double4 *__restrict__ spq, const float4 *__restrict__ spf,
@@ -407,7 +443,7 @@ k_verlet_build(const RepGeom *__restrict__ reps, const int *__restrict__ rep_of_
   long long const a = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (a >= n)
     return;
-  verlet_build_one(a, reps, rep_of_sorted, spq, spf, stype, scell, cstart, ia, ntypes, nb,
+  verlet_build_one<OCT>(a, reps, rep_of_sorted, spq, spf, stype, scell, cstart, ia, ntypes, nb,
                    nb_cnt, overflow, rflag, s_icut, s_group + threadIdx.x * 8,
                    s_group_b + threadIdx.x * 8);
 }
