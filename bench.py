@@ -380,8 +380,10 @@ def make_replicas(n_rep, seed=0, density=0.3, nmin=1000, nmax=50000):
 def run_batched(args):
     """Batched replicas (config 4): all replicas advance by one graph launch
     per MD step (velocity Verlet + Langevin kT=1, gamma=1, dt=0.01)."""
-    print(json.dumps(batched_measure(args, args.steps, args.warmup,
-                                     cpu=not args.no_cpu_baseline, fp64=args.fp64)))
+    res = batched_measure(args, args.steps, args.warmup, cpu=not args.no_cpu_baseline,
+                          fp64=args.fp64)
+    if res is not None:
+        print(json.dumps(res))
 
 
 def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
@@ -420,6 +422,16 @@ def batched_measure(args, steps, warmup, cpu=True, fp64=False, clocks=True):
     stream = torch.cuda.ExternalStream(lib.p3mx_batch_stream(h))
     _lib.check(lib.p3mx_batch_run(h, max(3, warmup), 0.01, 1.0, 1.0, 7), h,
                lib.p3mx_batch_last_error)
+    if getattr(args, "profile_only", False):
+        # `steps` graph steps inside a profiler range (ncu --profile-from-start
+        # off captures them without the tuner's trial launches)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        _lib.check(lib.p3mx_batch_run(h, steps, 0.01, 1.0, 1.0, 7), h, lib.p3mx_batch_last_error)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        lib.p3mx_batch_destroy(h)
+        return None
     lc0, lc1 = ctypes.c_longlong(), ctypes.c_longlong()
     lib.p3mx_batch_launch_count(h, ctypes.byref(lc0))
     e0 = torch.cuda.Event(enable_timing=True)
