@@ -942,6 +942,14 @@ def run_dipolar(args):
     p3mx_dp3m_compute with device pointers; e2e = the same through pinned
     host arrays (positions and moments in, forces and torques out).  Prints
     one JSON line."""
+    line = dipolar_measure(args, int(args.dipoles), args.steps, args.warmup)
+    if line is not None:
+        print(json.dumps(line))
+
+
+def dipolar_measure(args, n, steps, warmup):
+    """The dipolar workload's measurement (see run_dipolar): the JSON line,
+    or None under --profile-only."""
     import torch
     from espresso_b200 import _lib
     from espresso_b200.magnetostatics import DipolarP3M
@@ -949,7 +957,6 @@ def run_dipolar(args):
     lib = _lib.load()
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    n = int(args.dipoles)
     L = (n / 0.5) ** (1.0 / 3.0)
     rng = np.random.default_rng(0)
     side = int(np.ceil(n ** (1.0 / 3.0)))
@@ -993,7 +1000,7 @@ def run_dipolar(args):
                            h, lib.p3mx_dp3m_last_error)
             torch.cuda.synchronize(dev)
             torch.cuda.profiler.stop()
-            return
+            return None
 
         def step(device=True):
             if device:
@@ -1006,17 +1013,17 @@ def run_dipolar(args):
             _lib.check(rc, h, lib.p3mx_dp3m_last_error)
 
         def timed(device):
-            for _ in range(max(3, args.warmup)):
+            for _ in range(max(3, warmup)):
                 step(device)
             torch.cuda.synchronize(dev)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 step(device)
             e1.record(stream)
             torch.cuda.synchronize(dev)
-            return e0.elapsed_time(e1) / args.steps
+            return e0.elapsed_time(e1) / steps
 
         l0 = ctypes.c_longlong()
         lib.p3mx_dp3m_launch_count(h, ctypes.byref(l0))
@@ -1036,7 +1043,7 @@ def run_dipolar(args):
                       "e2e": {"value": n / (ms_e2e * 1e-3), "unit": "dipole-steps/s",
                               "ms_per_step": ms_e2e, "h2d_bytes_per_step": 48 * n,
                               "d2h_bytes_per_step": 48 * n},
-                      "gpu_launches_per_step": (l1.value - l0.value) / max(1, args.steps),
+                      "gpu_launches_per_step": (l1.value - l0.value) / max(1, steps),
                       "stages_ms": stages,
                       "tuned": {"mesh": p["mesh"][0], "cao": p["cao"], "r_cut": p["r_cut"],
                                 "alpha": p["alpha"], "accuracy_estimate": p["accuracy"]},
@@ -1044,14 +1051,14 @@ def run_dipolar(args):
     line = {
         "metric": "dipole-steps/s (dipolar P3M forces + torques at accuracy 1e-4)",
         "impl": "ours", "workload": "dipolar", "value": out["fp64"]["value"],
-        "unit": "dipole-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "unit": "dipole-steps/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
         "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True, "dtype": "f64",
         "data": "synthetic", "e2e": out["fp64"]["e2e"], "variants": out,
         "config": {"workload": f"{n} unit point dipoles, random orientations, density 0.5, "
                                f"box {L:.4g}^3, dipolar P3M tuned for accuracy 1e-4",
                    "inputs": "resident in HBM, larger than L2 with the Verlet lists"},
     }
-    print(json.dumps(line))
+    return line
 
 
 def main():
@@ -1324,6 +1331,17 @@ def main():
             variants["batched_f32_mixed"]["dominant_stage"] = {"kernel": dom_b, "ms": sb[dom_b]}
         except Exception as exc:  # reported, not hidden
             variants["batched_f32_mixed"] = {"error": str(exc)}
+        # dipolar P3M (the magnetostatics actor on the same kernels): 2^17
+        # unit dipoles, tuned for accuracy 1e-4, FP64 and FP32 mesh
+        try:
+            dl = dipolar_measure(args, 1 << 17, max(args.variant_steps, 10), 3)
+            variants["dipolar_p3m"] = {
+                "config": dl["config"]["workload"], "unit": "dipole-steps/s",
+                **{k: {kk: v[kk] for kk in ("value", "ms_per_step", "tuned", "stages_ms",
+                                            "gpu_launches_per_step")}
+                   for k, v in dl["variants"].items()}}
+        except Exception as exc:  # reported, not hidden
+            variants["dipolar_p3m"] = {"error": str(exc)}
     out = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
