@@ -11,10 +11,27 @@
 #include <cmath>
 #include <complex>
 #include <map>
+#include <utility>
 
 namespace p3mx {
 
 namespace {
+
+// Dynamic shared-memory opt-in of every charge-assignment instance of one
+// precision: orders 1..7, both super-brick edges, single- and multi-set.
+template <typename K> void set_smem_limit(K kern, size_t limit) {
+  P3MX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(limit)));
+}
+template <typename Real, bool MC, int... P>
+void assign_smem_attrs_mc(size_t limit, std::integer_sequence<int, P...>) {
+  (set_smem_limit(k_p3m_assign_sb<Real, P + 1, kSbEdge, MC>, limit), ...);
+  (set_smem_limit(k_p3m_assign_sb<Real, P + 1, kSbEdgeSmall, MC>, limit), ...);
+}
+template <typename Real> void assign_smem_attrs(size_t limit) {
+  assign_smem_attrs_mc<Real, false>(limit, std::make_integer_sequence<int, 7>{});
+  assign_smem_attrs_mc<Real, true>(limit, std::make_integer_sequence<int, 7>{});
+}
 
 // Radix factorisation of an FFT length: the power of two as radix-16 stages
 // (then one 8, 4 or 2), then 3, 5, 7 and any remaining prime (handled by the
@@ -451,26 +468,12 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
                                        static_cast<int>(limit)));
       };
       if (m_fp32) {
-        aset(k_p3m_assign_sb<float, 1, 16>); aset(k_p3m_assign_sb<float, 2, 16>);
-        aset(k_p3m_assign_sb<float, 3, 16>); aset(k_p3m_assign_sb<float, 4, 16>);
-        aset(k_p3m_assign_sb<float, 5, 16>); aset(k_p3m_assign_sb<float, 6, 16>);
-        aset(k_p3m_assign_sb<float, 7, 16>);
-        aset(k_p3m_assign_sb<float, 1, 8>); aset(k_p3m_assign_sb<float, 2, 8>);
-        aset(k_p3m_assign_sb<float, 3, 8>); aset(k_p3m_assign_sb<float, 4, 8>);
-        aset(k_p3m_assign_sb<float, 5, 8>); aset(k_p3m_assign_sb<float, 6, 8>);
-        aset(k_p3m_assign_sb<float, 7, 8>);
+        assign_smem_attrs<float>(limit);
         aset(k_p3m_interp<float, 1>); aset(k_p3m_interp<float, 2>); aset(k_p3m_interp<float, 3>);
         aset(k_p3m_interp<float, 4>); aset(k_p3m_interp<float, 5>); aset(k_p3m_interp<float, 6>);
         aset(k_p3m_interp<float, 7>);
       } else {
-        aset(k_p3m_assign_sb<double, 1, 16>); aset(k_p3m_assign_sb<double, 2, 16>);
-        aset(k_p3m_assign_sb<double, 3, 16>); aset(k_p3m_assign_sb<double, 4, 16>);
-        aset(k_p3m_assign_sb<double, 5, 16>); aset(k_p3m_assign_sb<double, 6, 16>);
-        aset(k_p3m_assign_sb<double, 7, 16>);
-        aset(k_p3m_assign_sb<double, 1, 8>); aset(k_p3m_assign_sb<double, 2, 8>);
-        aset(k_p3m_assign_sb<double, 3, 8>); aset(k_p3m_assign_sb<double, 4, 8>);
-        aset(k_p3m_assign_sb<double, 5, 8>); aset(k_p3m_assign_sb<double, 6, 8>);
-        aset(k_p3m_assign_sb<double, 7, 8>);
+        assign_smem_attrs<double>(limit);
         aset(k_p3m_interp<double, 1>); aset(k_p3m_interp<double, 2>); aset(k_p3m_interp<double, 3>);
         aset(k_p3m_interp<double, 4>); aset(k_p3m_interp<double, 5>); aset(k_p3m_interp<double, 6>);
         aset(k_p3m_interp<double, 7>);
@@ -673,8 +676,9 @@ void launch_assign_e(bool chained, int cnt, cudaStream_t st, RepGeom const *geom
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = chained ? 1 : 0;
-  P3MX_CUDA(cudaLaunchKernelEx(&cfg, k_p3m_assign_sb<Real, P, E>, geom, tab, cnt, start, W, s_key,
-                               qmax_bits, rho, err, comp_w, comp_rho, comp_q));
+  auto const kern = ncomp > 1 ? k_p3m_assign_sb<Real, P, E, true> : k_p3m_assign_sb<Real, P, E, false>;
+  P3MX_CUDA(cudaLaunchKernelEx(&cfg, kern, geom, tab, cnt, start, W, s_key, qmax_bits, rho, err,
+                               comp_w, comp_rho, comp_q));
 }
 // ... with the engine's super-brick edge (16 or 8); ncomp charge sets
 // (records, meshes and |q| maxima comp_w / comp_rho / comp_q apart)
