@@ -209,9 +209,7 @@ public:
       ++E.m_launches;
     }
     E.mark("dp_assign_fft_z", st);
-    k_fft_y<Real><<<dim3(E.m_n_blk_y, 3), 256, E.m_smem_y, st>>>(geom, E.m_blk_y.as<Blk>(), ck3,
-                                                                 E.m_cplx, E.m_tile_y, false, tw);
-    ++E.m_launches;
+    E.launch_fft_y<Real>(ck3, E.m_cplx, 3, false, st);
     // unit-charge weights of the magnetic particles (selector) for the
     // back-interpolation
     if (want_ft) {
@@ -243,9 +241,7 @@ public:
       E.mark("dp_x_pass", st);
       if (!want_ft)
         break;
-      k_fft_y<Real><<<dim3(E.m_n_blk_y, 3), 256, E.m_smem_y, st>>>(
-          geom, E.m_blk_y.as<Blk>(), E.m_field.as<C>(), E.m_cplx, E.m_tile_y, true, tw);
-      ++E.m_launches;
+      E.launch_fft_y<Real>(E.m_field.p, E.m_cplx, 3, true, st);
       k_fft_z_inv3<Real><<<E.m_n_blk_zi, 256, E.m_smem_zi, st>>>(
           geom, E.m_blk_zi.as<Blk>(), E.m_field.as<C>(), E.m_cplx, E.m_E.as<Real>(), tw,
           E.m_kerr.as<int>());

@@ -153,6 +153,8 @@ private:
                                              cudaStream_t st);
   template <typename Real> void short_range_t(double *f, bool overwrite, bool want_ev,
                                               cudaStream_t st);
+  template <typename Real>
+  void launch_fft_y(void *c0, long long field_stride, int nf, bool inv, cudaStream_t st);
   template <typename Real> void launch_pair(double *f, bool overwrite, bool want_ev,
                                             cudaStream_t st);
   void prepare_short_range(cudaStream_t st, bool need_spq);
@@ -200,6 +202,7 @@ private:
   int m_n_blk_mesh = 0, m_n_blk_cplx = 0, m_n_blk_census = 0, m_n_blk_pair = 0;
   int m_n_blk_zf = 0, m_n_blk_y = 0, m_n_blk_x = 0, m_n_blk_zi = 0;
   int m_tile_y = 16, m_tile_x = 16;
+  bool m_yin = true;  // every replica's y lines transform in place
   size_t m_smem_zf = 0, m_smem_y = 0, m_smem_x = 0, m_smem_zi = 0;
 
   // particles

@@ -501,7 +501,9 @@ k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
 // ---- pass y (either direction, nf field arrays via blockIdx.y) ---------
 // Shared memory: tile staged lines of line_ld(M1) (two sets unless the
 // lines transform in place), twiddles (M1).
-template <typename Real>
+// INPL: every replica's lines transform in place (the host checks), so the
+// instance carries none of the out-of-place transform's code or registers.
+template <typename Real, bool INPL>
 __global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2)
 k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
         typename CplxOf<Real>::type *__restrict__ c0, long long field_stride, int tile,
@@ -516,7 +518,7 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   int const x = bk.a, kz0 = bk.b;
   int const T = min(tile, H - kz0);
   int const ld = line_ld(M1);
-  bool const inplace = fft_inplace_ok(M1, tile, blockDim.x);
+  bool const inplace = INPL || fft_inplace_ok(M1, tile, blockDim.x);
   C *a = reinterpret_cast<C *>(smem_raw);
   C *b = inplace ? nullptr : a + tile * ld;
   C *tw = a + (inplace ? 1 : 2) * tile * ld;
@@ -542,8 +544,12 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
     }
   }
   __syncthreads();
-  C *res = inplace ? fft_lines_inplace<C>(a, T, ld, G.plan[1], tw, inv)
-                   : fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
+  C *res;
+  if constexpr (INPL)
+    res = fft_lines_inplace<C>(a, T, ld, G.plan[1], tw, inv);
+  else
+    res = inplace ? fft_lines_inplace<C>(a, T, ld, G.plan[1], tw, inv)
+                  : fft_lines<C>(a, b, T, ld, G.plan[1], tw, inv);
   if (col)
     for (int y = yq; y < M1; y += 16)
       cm[rowbase + y * hp + tq] = res[tq * ld + pix(y)];
@@ -700,9 +706,11 @@ __host__ __device__ inline int z_inv_b_size(int nl, int n) {
 // extended by Hermitian symmetry with the imaginary parts of the k = 0 and
 // k = n/2 entries dropped (c2r semantics), so both packed outputs are real.
 // Shared memory: 2 x (nl + ceil(nl/2)) staged lines of line_ld(n),
-// twiddles (n).
+// twiddles (n).  FP32: four blocks per SM -- the block's load, transform and
+// store phases do not overlap, so the fourth resident block pays for the
+// spills of the 64-register bound.
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2)
 k_fft_z_inv3(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
              const typename CplxOf<Real>::type *__restrict__ field0, long long field_stride,
              Real *__restrict__ efield, const typename CplxOf<Real>::type *__restrict__ twtab,
