@@ -279,11 +279,20 @@ public:
     double const M3 = static_cast<double>(m_M) * m_M * m_M;
     double e_k = 0.0, e_r = 0.0;
     bool const kspace_on = sum_mu2 > 0.0;
-    if (kspace_on && (want_ft || want_e)) {
-      if (E.fp32())
-        kspace<float>(want_ft, want_e, st);
-      else
-        kspace<double>(want_ft, want_e, st);
+    // the Verlet-list check goes ahead of the k-space chain (outside stage
+    // profiles), so the host waits for its flag while the GPU is busy
+    if (n > 0 && (want_ft || want_e) && !E.m_profiling)
+      E.check_lists(st, true);
+    try {
+      if (kspace_on && (want_ft || want_e)) {
+        if (E.fp32())
+          kspace<float>(want_ft, want_e, st);
+        else
+          kspace<double>(want_ft, want_e, st);
+      }
+    } catch (...) {
+      E.m_check_pending = false;
+      throw;
     }
     double const ps = (epsilon != 0.0) ? prefactor * 4.0 * kPi / V / (2.0 * epsilon + 1.0) : 0.0;
     if (want_ft && n > 0) {

@@ -158,6 +158,10 @@ private:
   template <typename Real> void launch_pair(double *f, bool overwrite, bool want_ev,
                                             cudaStream_t st);
   void prepare_short_range(cudaStream_t st, bool need_spq);
+  // the list check of prepare_short_range issued early: its flag lands in
+  // pinned host memory behind m_check_ev, so the host can wait for it while
+  // later work keeps the GPU busy; prepare_short_range consumes it
+  void check_lists(cudaStream_t st, bool need_spq);
   void build_lists(cudaStream_t st);
   void set_list_capacity(double margin);
   void layout_lists(cudaStream_t st);
@@ -230,6 +234,11 @@ private:
   DevBuf m_bstart, m_bent, m_bparam, m_bpart;
   std::vector<int> m_cap; // neighbour capacity per replica
   bool m_lists_valid = false;
+  // pending early list check (check_lists): rebuild regardless, or read the
+  // flag copied to m_flag_host once m_check_ev has completed
+  bool m_check_pending = false, m_check_rebuild = false;
+  int *m_flag_host = nullptr;
+  cudaEvent_t m_check_ev = nullptr;
   // misc host staging
   DevBuf m_ks_part;
 };

@@ -445,7 +445,7 @@ __device__ inline const T *bulk_stage(const T *src, long long count, unsigned ch
 // bk.b real lines per block (an odd last line is paired with zeros).
 // Shared memory: 2 x ceil(bk.b/2) staged lines of line_ld(n), twiddles (n).
 template <typename Real>
-__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(Real) == 4 ? 4 : 2)
 k_fft_z_fwd(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
             const Real *__restrict__ rmesh, typename CplxOf<Real>::type *__restrict__ cmesh,
             const typename CplxOf<Real>::type *__restrict__ twtab, int *__restrict__ err) {
