@@ -570,6 +570,10 @@ void Engine::configure(std::vector<ReplicaConf> const &conf, long long n_total) 
   m_overflow.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_rflag.ensure(static_cast<size_t>(std::max(R, 1)) * sizeof(int));
   m_flag.ensure(sizeof(int));
+  // the list check's two alternating flag words, both zero
+  m_chk.ensure(2 * sizeof(int));
+  P3MX_CUDA(cudaMemsetAsync(m_chk.p, 0, 2 * sizeof(int), st));
+  m_chk_slot = 0;
   if (m_kerr.p == nullptr) {
     m_kerr.ensure(4 * sizeof(int));
     P3MX_CUDA(cudaMemsetAsync(m_kerr.p, 0, 4 * sizeof(int), st));
@@ -629,8 +633,7 @@ void Engine::census(cudaStream_t st) {
 
 void Engine::sort_keys(int *key, int *slot, int *cnt, int *start, int *perm, long long nkeys,
                        cudaStream_t st, const int *cond, bool index_order) {
-  exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
-  m_launches += 3;
+  m_launches += exclusive_scan(cnt, start, m_scan_tiles.as<int>(), nkeys, st, cond);
   k_place<<<ceil_div(m_n, 256), 256, 0, st>>>(key, slot, start, perm, m_n, cond); ++m_launches;
   if (!index_order)
     return;
@@ -985,7 +988,10 @@ __global__ void k_check_refresh(const RepGeom *__restrict__ reps, const int *__r
                                 const double *__restrict__ pos_ref, const int *__restrict__ type,
                                 const int *__restrict__ type_ref, long long n,
                                 double4 *__restrict__ spq, float4 *__restrict__ spf,
-                                int *__restrict__ flag) {
+                                int *__restrict__ flag, int *__restrict__ flag_next) {
+  // the flag word of the next check starts at zero (no memset between checks)
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    *flag_next = 0;
   long long const i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n)
     return;
@@ -1031,14 +1037,15 @@ void Engine::check_lists(cudaStream_t st, bool need_spq) {
   // rebuild follows
   RepGeom const *geom = m_geom_d.as<RepGeom>();
   int const nb = ceil_div(m_n, 256);
-  P3MX_CUDA(cudaMemsetAsync(m_flag.p, 0, sizeof(int), st));
+  int *const flag = m_chk.as<int>() + m_chk_slot;
+  m_chk_slot ^= 1;
   k_check_refresh<<<nb, 256, 0, st>>>(geom, m_rep_of.as<int>(), m_cinv.as<int>(), d_pos(), d_q(),
                                       m_ckey.as<int>(), m_pos_ref.as<double>(), d_type(),
                                       m_type_ref.as<int>(), m_n,
                                       need_spq ? m_spq.as<double4>() : nullptr,
-                                      m_spf.as<float4>(), m_flag.as<int>());
+                                      m_spf.as<float4>(), flag, m_chk.as<int>() + m_chk_slot);
   ++m_launches;
-  P3MX_CUDA(cudaMemcpyAsync(m_flag_host, m_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  P3MX_CUDA(cudaMemcpyAsync(m_flag_host, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   P3MX_CUDA(cudaEventRecord(m_check_ev, st));
 }
 

@@ -239,6 +239,8 @@ private:
   bool m_check_pending = false, m_check_rebuild = false;
   int *m_flag_host = nullptr;
   cudaEvent_t m_check_ev = nullptr;
+  DevBuf m_chk;       // the check's two flag words (slot m_chk_slot is next)
+  int m_chk_slot = 0;
   // misc host staging
   DevBuf m_ks_part;
 };

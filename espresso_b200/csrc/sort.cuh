@@ -235,15 +235,63 @@ __global__ void k_fill_int(int *__restrict__ p, int v, long long n, const int *_
     p[i] = v;
 }
 
-// Host driver of the three-pass exclusive scan (out has n+1 entries).
+// Exclusive scan of up to kScanOneMax items by one block of 32 warps: warp
+// w scans the segment [w L, (w+1) L) (L = 32 R) in R rounds of 32
+// consecutive items (coalesced), the warp totals are scanned across the
+// block; writes the total to out[n].
+constexpr int kScanOneRounds = 32;
+constexpr long long kScanOneMax = 32LL * 32 * kScanOneRounds;
+__global__ void __launch_bounds__(1024) k_scan_one(const int *__restrict__ in,
+                                                   int *__restrict__ out, long long n,
+                                                   const int *__restrict__ cond) {
+  if (cond && !*cond)
+    return;
+  int const lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int const R = static_cast<int>((n + 1023) / 1024);
+  long long const seg = static_cast<long long>(w) * 32 * R;
+  int v[kScanOneRounds];
+  int s = 0;
+#pragma unroll
+  for (int r = 0; r < kScanOneRounds; ++r) {
+    long long const i = seg + 32 * r + lane;
+    v[r] = (r < R && i < n) ? in[i] : 0;
+    s += v[r];
+  }
+  // warp total, then the exclusive scan of the 32 warp totals
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  int total;
+  int carry = block_excl_scan(lane == 0 ? s : 0, total);
+  carry = __shfl_sync(0xffffffffu, carry, 0);
+#pragma unroll
+  for (int r = 0; r < kScanOneRounds; ++r) {
+    if (r < R) {
+      int const incl = warp_incl_scan(v[r]);
+      long long const i = seg + 32 * r + lane;
+      if (i < n)
+        out[i] = carry + incl - v[r];
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+  if (threadIdx.x == 0)
+    out[n] = total;
+}
+
+// Host driver of the exclusive scan (out has n+1 entries): one block for up
+// to kScanOneMax items, else three passes; returns the kernels launched.
 // `cond` (device int, may be NULL) skips the whole scan when zero, so the
 // scan can sit inside a captured CUDA graph behind a device-side decision.
-inline void exclusive_scan(const int *in, int *out, int *tile_buf, long long n,
-                           cudaStream_t st, const int *cond = nullptr) {
+inline int exclusive_scan(const int *in, int *out, int *tile_buf, long long n,
+                          cudaStream_t st, const int *cond = nullptr) {
+  if (n <= kScanOneMax) {
+    k_scan_one<<<1, 1024, 0, st>>>(in, out, n, cond);
+    return 1;
+  }
   int const ntiles = ceil_div(n, kScanTile);
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(in, out, tile_buf, n, cond);
   k_scan_tile_sums<<<1, 1024, 0, st>>>(tile_buf, ntiles, out, n, cond);
   k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, tile_buf, n, cond);
+  return 3;
 }
 
 } // namespace p3mx
