@@ -139,9 +139,20 @@ __device__ inline double mi_d(double dx, double L, double Li) {
 // (cap, the per-replica capacity, a multiple of 8).  The build writes whole
 // groups with vector stores and the pair kernels read whole groups with
 // vector loads.  An entry packs the partner's index inside the replica
-// (26 bits) and its cell offset code (cell_offset).
+// (26 bits) and its cell offset code (cell_offset_code, 6 bits).
 constexpr int kNbIndexBits = 26;
 constexpr unsigned kNbIndexMask = (1u << kNbIndexBits) - 1u;
+// Cell offset code of an entry: the partner image's cell offset dc (each
+// axis -1, 0 or +1) as three 2-bit fields dc + 1 (x lowest), in the 6 bits
+// above the index.
+__host__ __device__ constexpr int cell_offset_code(int dx, int dy, int dz) {
+  return (dx + 1) | ((dy + 1) << 2) | ((dz + 1) << 4);
+}
+// dc of axis d from a code, as an FP32 value (exact: 2^23 + field, minus
+// 2^23 + 1)
+__device__ inline float code_axis(unsigned code, int d) {
+  return __uint_as_float(0x4B000000u | ((code >> (2 * d)) & 3u)) - 8388609.0f;
+}
 // First entry (group 0) of local particle la; group g at + g * 256.
 __host__ __device__ inline long long nb_base(long long nb_off, int cap, long long la) {
   return nb_off + (((la >> 5) * (cap >> 3)) << 8) + ((la & 31) << 3);
@@ -329,7 +340,7 @@ __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__
                     dcv[d] = static_cast<int>(rint((dmi[d] - (ob - oa)) * ics[d]));
                   }
               }
-              put(b, cls_a, (dcv[0] + 1) + 3 * (dcv[1] + 1) + 9 * (dcv[2] + 1));
+              put(b, cls_a, cell_offset_code(dcv[0], dcv[1], dcv[2]));
             }
         };
         if (small_grid) {
@@ -339,7 +350,7 @@ __device__ inline void verlet_build_one(long long a, const RepGeom *__restrict__
             if (b != a)
               consider(b);
         } else {
-          int const code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+          int const code = cell_offset_code(dx, dy, dz);
           // with octant-sorted cells, the octants of the neighbour cell
           // wholly beyond the list range are skipped (the particle relative
           // to the neighbour cell's corner against each half-cell box)
@@ -627,19 +638,16 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
                   double *__restrict__ partials) {
   using Real = float;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ float shift_x[32], shift_y[32], shift_z[32];
   PairIA *ia = reinterpret_cast<PairIA *>(smem_raw);
   for (int k = threadIdx.x; k < ntypes * ntypes; k += blockDim.x)
     ia[k] = ia_g[k];
   int2 const bk = blk[blockIdx.x];
   RepGeom const &G = reps[bk.x];
-  if (threadIdx.x < 27) {
-    int const c = threadIdx.x;
-    int const dc[3] = {c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1};
-    shift_x[c] = static_cast<float>(-dc[0] * (G.box[0] / G.cg[0]));
-    shift_y[c] = static_cast<float>(-dc[1] * (G.box[1] / G.cg[1]));
-    shift_z[c] = static_cast<float>(-dc[2] * (G.box[2] / G.cg[2]));
-  }
+  // cell sizes: the image shift of an entry is -dc cs per axis, dc from
+  // its offset code (registers, no table lookup per entry)
+  float const cs_x = static_cast<float>(G.box[0] / G.cg[0]);
+  float const cs_y = static_cast<float>(G.box[1] / G.cg[1]);
+  float const cs_z = static_cast<float>(G.box[2] / G.cg[2]);
   __syncthreads();
   long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
   double ev[EV ? 20 : 1];
@@ -673,13 +681,16 @@ k_pair_forces_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk
   int const ngroups = G.max_nb >> 3;
   long long const base0 = G.p0;
   // the particle itself with the zero cell offset (code 13: dc = 0)
-  unsigned const self_ent = static_cast<unsigned>(active ? a - G.p0 : 0) | (13u << kNbIndexBits);
+  unsigned const self_ent = static_cast<unsigned>(active ? a - G.p0 : 0) |
+                            (static_cast<unsigned>(cell_offset_code(0, 0, 0)) << kNbIndexBits);
   // one entry: Coulomb always, LJ / WCA when the group may hold class A
   auto entry = [&](auto lj, unsigned e, float4 pb, float &sx, float &sy, float &sz) {
-    int const code = static_cast<int>(e >> kNbIndexBits);
-    Real const d0 = (pa.x - pb.x) + shift_x[code];
-    Real const d1 = (pa.y - pb.y) + shift_y[code];
-    Real const d2v = (pa.z - pb.z) + shift_z[code];
+    // d = (x_a - x_b) - dc cs (dc in {-1, 0, 1}: the FMA's product is
+    // exact, so this rounds as the sum with a stored shift would)
+    unsigned const code = e >> kNbIndexBits;
+    Real const d0 = fmaf(code_axis(code, 0), -cs_x, pa.x - pb.x);
+    Real const d1 = fmaf(code_axis(code, 1), -cs_y, pa.y - pb.y);
+    Real const d2v = fmaf(code_axis(code, 2), -cs_z, pa.z - pb.z);
     Real const dist2 = d0 * d0 + d1 * d1 + d2v * d2v;
     Real const inv_d = rsqrt_approx(dist2);
     Real const dist = dist2 * inv_d;
