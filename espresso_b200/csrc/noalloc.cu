@@ -19,12 +19,11 @@
 //    call overwrites every slot it reads, so nothing has to start at zero;
 //  * calls whose kernels overlap on the GPU (different streams or threads
 //    at the same time) race on the array: serialise them;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture on the device.  The address is kept for the
-//    life of the process: a cudaDeviceReset (or any teardown of the primary
-//    context) makes it stale, so the entry point must not be called again
-//    after one;
+//  * every call looks up the array's device address on the current device
+//    (cudaGetSymbolAddress: no allocation), so the address cannot go stale
+//    after a cudaDeviceReset; the first call on a device may load the
+//    library's device code, so make that first call before any stream
+//    capture on the device;
 //  * each call waits for its result (device-to-host copy of one double and a
 //    stream synchronisation).
 #include "../../include/p3mx.h"
@@ -32,7 +31,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 namespace p3mx {
 namespace {
@@ -40,7 +38,6 @@ namespace {
 constexpr int kNoAllocPartials = 4096;                    // one partial sum per CTA
 constexpr long long kNoAllocPointsPerBlock = 256LL * 64;  // k-points per CTA
 constexpr long long kNoAllocMaxPoints = kNoAllocPartials * kNoAllocPointsPerBlock;
-constexpr int kNoAllocMaxDevices = 64;
 
 // slots [0, nblk): partial sums of the current call; slot kNoAllocPartials:
 // the total
@@ -64,27 +61,14 @@ __global__ void k_noalloc_sum_partials(int nblk) {
     g_noalloc_scratch[kNoAllocPartials] = red[0];
 }
 
-std::mutex g_noalloc_mutex;
-double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the array on the current device, looked up once per
-// device with that device current.
+// Device address of the array on the current device, looked up on every
+// call.
 cudaError_t noalloc_scratch(double **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  double *ptr = nullptr;
+  cudaError_t const e = cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), g_noalloc_scratch);
   if (e != cudaSuccess)
     return e;
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    double *ptr = nullptr;
-    e = cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return e;
-    g_noalloc_ptr[dev] = ptr;
-  }
-  *out = g_noalloc_ptr[dev];
+  *out = ptr;
   return cudaSuccess;
 }
 

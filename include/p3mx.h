@@ -262,11 +262,10 @@ int p3mx_error_estimate(const int *mesh, int cao, int n_c_part,
  * may imply.  Same results as p3mx_error_estimate, but the scratch is a
  * fixed 32 KiB device array inside the library (held on every GPU that loads
  * it until exit): meshes above 4096*16384 points are rejected with
- * P3MX_EDOMAIN and a message in errbuf.  The first call on a device looks up
- * the array's address (make it before any stream capture) and keeps it for
- * the life of the process: after cudaDeviceReset, or any teardown of the
- * device's primary context, that address is stale and the entry point must
- * not be called again in the process.  All calls share the array, so calls
+ * P3MX_EDOMAIN and a message in errbuf.  Every call looks up the array's
+ * address on the current device (no allocation), so a cudaDeviceReset leaves
+ * no stale address behind; the first call on a device may load the
+ * library's device code: make it before any stream capture.  All calls share the array, so calls
  * that overlap on the GPU race.  Each call returns only when its result is
  * on the host (it synchronises the stream).  stream: cudaStream_t or NULL;
  * errbuf/errbuf_len may be NULL/0. */
