@@ -528,16 +528,18 @@ k_fft_y(const RepGeom *__restrict__ reps, const Blk *__restrict__ blks,
   // 16 x 16 thread mapping (tile <= 16 columns): column tq, rows yq + 16 i
   int const tq = threadIdx.x & 15, yq = threadIdx.x >> 4;
   bool const col = tq < T;
-  for (int y0 = yq; y0 < M1; y0 += 64) {
-    C v[4];
+  // all of a thread's rows in flight at once (up to 16: M1 <= 256 in one
+  // round)
+  for (int y0 = yq; y0 < M1; y0 += 256) {
+    C v[16];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 16; ++u) {
       int const y = y0 + 16 * u;
       if (col && y < M1)
         v[u] = cm[rowbase + y * hp + tq];
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 16; ++u) {
       int const y = y0 + 16 * u;
       if (col && y < M1)
         a[tq * ld + pix(y)] = v[u];
