@@ -20,6 +20,7 @@
 #include "engine.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <limits>
@@ -314,27 +315,35 @@ public:
     // particles out of them)
     if (n > 0 && (want_ft || want_e)) {
       E.prepare_short_range(st, true);
+      bool const rel = E.fp32();
       k_dp3m_sort_mu<<<static_cast<int>(ceil_div(n, 256)), 256, 0, st>>>(
-          n, E.m_cperm.as<int>(), m_mu.as<double>(), m_smu.as<double4>());
+          n, E.m_cperm.as<int>(), m_mu.as<double>(), m_smu.as<double4>(), rel ? 1 : 0);
       ++E.m_launches;
       E.mark("dp_sort_mu", st);
       int const exact = accuracy > 5e-6 ? 0 : 1;
       RepGeom const *geom = E.m_geom_d.as<RepGeom>();
-      if (want_e) {
-        k_dp3m_pairs<true><<<E.m_n_blk_pair, 256, 0, st>>>(
-            geom, E.m_blk_pair.as<int2>(), E.m_spq.as<double4>(), m_smu.as<double4>(),
-            E.m_cperm.as<int>(), E.m_nb.as<int>(), E.m_nb_cnt.as<int>(), prefactor, exact,
-            want_ft ? f : nullptr, t, 0, m_part.as<double>());
+      // FP32-mesh mode: the pair terms in FP32 on the cell-relative offsets
+      auto pairs = [&](auto ev, double *fo, double *part) {
+        constexpr bool EV = decltype(ev)::value;
+        if (rel)
+          k_dp3m_pairs_rel<EV><<<E.m_n_blk_pair, 256, 0, st>>>(
+              geom, E.m_blk_pair.as<int2>(), E.m_spf.as<float4>(), m_smu.as<float4>(),
+              E.m_cperm.as<int>(), E.m_nb.as<int>(), E.m_nb_cnt.as<int>(), prefactor, exact, fo,
+              t, 0, part);
+        else
+          k_dp3m_pairs<EV><<<E.m_n_blk_pair, 256, 0, st>>>(
+              geom, E.m_blk_pair.as<int2>(), E.m_spq.as<double4>(), m_smu.as<double4>(),
+              E.m_cperm.as<int>(), E.m_nb.as<int>(), E.m_nb_cnt.as<int>(), prefactor, exact, fo,
+              t, 0, part);
         ++E.m_launches;
+      };
+      if (want_e) {
+        pairs(std::true_type{}, want_ft ? f : nullptr, m_part.as<double>());
         k_dp3m_sum_rows<<<1, 32, 0, st>>>(m_part.as<double>(), E.m_n_blk_pair, 1,
                                           m_sums.as<double>() + 6);
         ++E.m_launches;
       } else {
-        k_dp3m_pairs<false><<<E.m_n_blk_pair, 256, 0, st>>>(
-            geom, E.m_blk_pair.as<int2>(), E.m_spq.as<double4>(), m_smu.as<double4>(),
-            E.m_cperm.as<int>(), E.m_nb.as<int>(), E.m_nb_cnt.as<int>(), prefactor, exact, f, t, 0,
-            nullptr);
-        ++E.m_launches;
+        pairs(std::false_type{}, f, nullptr);
       }
       E.mark("dp_pairs", st);
     }

@@ -404,14 +404,21 @@ __global__ void k_dp3m_combine(long long n, const double *__restrict__ mu,
   }
 }
 
-// Dipole moments in cell-sorted order (the pair kernel's partner reads).
+// Dipole moments in cell-sorted order (the pair kernel's partner reads):
+// FP64 records, or FP32 records in the same buffer for k_dp3m_pairs_rel.
 __global__ void k_dp3m_sort_mu(long long n, const int *__restrict__ perm,
-                               const double *__restrict__ mu, double4 *__restrict__ smu) {
+                               const double *__restrict__ mu, double4 *__restrict__ smu,
+                               int fp32) {
   long long const s = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= n)
     return;
   int const i = perm[s];
-  smu[s] = make_double4(mu[3 * i], mu[3 * i + 1], mu[3 * i + 2], 0.0);
+  if (fp32)
+    reinterpret_cast<float4 *>(smu)[s] =
+        make_float4(static_cast<float>(mu[3 * i]), static_cast<float>(mu[3 * i + 1]),
+                    static_cast<float>(mu[3 * i + 2]), 0.f);
+  else
+    smu[s] = make_double4(mu[3 * i], mu[3 * i + 1], mu[3 * i + 2], 0.0);
 }
 
 // Real-space dipole-dipole energy, force and torque over the Verlet lists
@@ -505,6 +512,132 @@ k_dp3m_pairs(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
       tx += -(ma.y * mb.z - ma.z * mb.y) * B + (ma.y * d2 - ma.z * d1) * s;
       ty += -(ma.z * mb.x - ma.x * mb.z) * B + (ma.z * d0 - ma.x * d2) * s;
       tz += -(ma.x * mb.y - ma.y * mb.x) * B + (ma.x * d1 - ma.y * d0) * s;
+    }
+    if (f) {
+      int const i = perm[a];
+      if (overwrite) {
+        f[3 * i] = pref * fx;
+        f[3 * i + 1] = pref * fy;
+        f[3 * i + 2] = pref * fz;
+        tq[3 * i] = pref * tx;
+        tq[3 * i + 1] = pref * ty;
+        tq[3 * i + 2] = pref * tz;
+      } else {
+        f[3 * i] += pref * fx;
+        f[3 * i + 1] += pref * fy;
+        f[3 * i + 2] += pref * fz;
+        tq[3 * i] += pref * tx;
+        tq[3 * i + 1] += pref * ty;
+        tq[3 * i + 2] += pref * tz;
+      }
+    }
+  }
+  if constexpr (EV) {
+    __shared__ double red[8];
+    int const lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double v = 0.5 * pref * energy;
+    for (int o = 16; o > 0; o >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0)
+      red[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (blockDim.x >> 5); ++w)
+        s += red[w];
+      partials[blockIdx.x] = s;
+    }
+  }
+}
+
+// The same pair terms for the FP32-mesh mode, in FP32 from the cell-relative
+// offsets (as k_pair_forces_rel: d = (off_a - off_b) - dc cs with dc from
+// the entry's offset code, no minimum-image arithmetic): hardware reciprocal
+// square root, reciprocal and 2^x, A&S 7.1.26 or erfcf; each pair's force, torque and
+// energy terms summed in FP64.
+template <bool EV>
+__global__ void __launch_bounds__(256)
+k_dp3m_pairs_rel(const RepGeom *__restrict__ reps, const int2 *__restrict__ blk,
+                 const float4 *__restrict__ spf, const float4 *__restrict__ smu,
+                 const int *__restrict__ perm, const int *__restrict__ nb,
+                 const int *__restrict__ nb_cnt, double pref, int exact_erfc,
+                 double *__restrict__ f, double *__restrict__ tq, int overwrite,
+                 double *__restrict__ partials) {
+  int2 const bk = blk[blockIdx.x];
+  RepGeom const &G = reps[bk.x];
+  long long const a = G.p0 + static_cast<long long>(bk.y) * blockDim.x + threadIdx.x;
+  double energy = 0.0;
+  if (a < G.p0 + G.np) {
+    float4 const pa = spf[a];
+    float4 const ma = smu[a];
+    float const alpha = static_cast<float>(G.alpha);
+    float const rc2 = static_cast<float>(G.r_cut * G.r_cut);
+    float const coeff = static_cast<float>(2.0 * G.alpha / sqrt(kPi));
+    float const a2 = static_cast<float>(G.alpha * G.alpha);
+    // exp(-(alpha r)^2) = 2^(c_exp r^2)
+    float const c_exp = static_cast<float>(-G.alpha * G.alpha * 1.4426950408889634);
+    float const cs_x = static_cast<float>(G.box[0] / G.cg[0]);
+    float const cs_y = static_cast<float>(G.box[1] / G.cg[1]);
+    float const cs_z = static_cast<float>(G.box[2] / G.cg[2]);
+    double fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0;
+    int const cw = nb_cnt[a];
+    int const cnt = nb_count(cw), cna = nb_count_a(cw);
+    const int *nbp = nb + nb_base(G.nb_off, G.max_nb, a - G.p0);
+    long long const base0 = G.p0;
+    auto entry = [&](int k) {
+      return static_cast<unsigned>(nbp[nb_logical(0, G.max_nb, cna, k)]);
+    };
+    // the next partner's records are loaded while the current pair is
+    // evaluated
+    unsigned e_next = (cnt > 0) ? entry(0) : 0u;
+    float4 p_next = (cnt > 0) ? spf[base0 + (e_next & kNbIndexMask)] : pa;
+    float4 m_next = (cnt > 0) ? smu[base0 + (e_next & kNbIndexMask)] : ma;
+    for (int k = 0; k < cnt; ++k) {
+      unsigned const e = e_next;
+      float4 const pb = p_next;
+      float4 const mb = m_next;
+      if (k + 1 < cnt) {
+        e_next = entry(k + 1);
+        p_next = spf[base0 + (e_next & kNbIndexMask)];
+        m_next = smu[base0 + (e_next & kNbIndexMask)];
+      }
+      unsigned const code = e >> kNbIndexBits;
+      float const d0 = fmaf(code_axis(code, 0), -cs_x, pa.x - pb.x);
+      float const d1 = fmaf(code_axis(code, 1), -cs_y, pa.y - pb.y);
+      float const d2 = fmaf(code_axis(code, 2), -cs_z, pa.z - pb.z);
+      float const r2 = d0 * d0 + d1 * d1 + d2 * d2;
+      if (!(r2 < rc2) || !(r2 > 0.f))
+        continue;
+      float const inv_r = rsqrt_approx(r2);
+      float const inv_r2 = inv_r * inv_r;
+      float const ad = alpha * (r2 * inv_r);
+      float const exa = ex2_approx(c_exp * r2);
+      float B;
+      if (exact_erfc) {
+        B = (erfcf(ad) * inv_r + coeff * exa) * inv_r2;
+      } else {
+        float const t = rcp_r(1.f + 0.3275911f * ad);
+        float const asp =
+            t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f +
+                                                                           t * 1.061405429f))));
+        B = (asp * inv_r + coeff) * exa * inv_r2;
+      }
+      float const common = a2 * coeff * exa;
+      float const Cc = (3.f * B + 2.f * common) * inv_r2;
+      float const Dd = (5.f * Cc + 4.f * common * a2) * inv_r2;
+      float const mimj = ma.x * mb.x + ma.y * mb.y + ma.z * mb.z;
+      float const mir = ma.x * d0 + ma.y * d1 + ma.z * d2;
+      float const mjr = mb.x * d0 + mb.y * d1 + mb.z * d2;
+      if constexpr (EV)
+        energy += static_cast<double>(mimj * B - mir * mjr * Cc);
+      float const cd = mimj * Cc - mir * mjr * Dd;
+      fx += static_cast<double>(cd * d0 + mjr * Cc * ma.x + mir * Cc * mb.x);
+      fy += static_cast<double>(cd * d1 + mjr * Cc * ma.y + mir * Cc * mb.y);
+      fz += static_cast<double>(cd * d2 + mjr * Cc * ma.z + mir * Cc * mb.z);
+      float const s = mjr * Cc;
+      tx += static_cast<double>(-(ma.y * mb.z - ma.z * mb.y) * B + (ma.y * d2 - ma.z * d1) * s);
+      ty += static_cast<double>(-(ma.z * mb.x - ma.x * mb.z) * B + (ma.z * d0 - ma.x * d2) * s);
+      tz += static_cast<double>(-(ma.x * mb.y - ma.y * mb.x) * B + (ma.x * d1 - ma.y * d0) * s);
     }
     if (f) {
       int const i = perm[a];

@@ -3,8 +3,8 @@
 ``DipolarP3M`` takes the keyword arguments of the reference actor
 (src/python/espressomd/magnetostatics.py:82-160) with the same defaults,
 validation and error messages; the computation runs in libp3mx.so on the GPU
-(``single_precision=True`` selects the FP32 mesh/FFT path, ``False`` the
-FP64 path; the real-space pair part is FP64 in both).  It is activated with
+(``single_precision=True`` selects the FP32 mesh/FFT path with FP32
+real-space pair terms summed in FP64, ``False`` the FP64 path).  It is activated with
 ``system.magnetostatics.solver = DipolarP3M(...)``; particles carry their
 moments in ``dip`` and receive ``torque_lab``.
 """

@@ -3,9 +3,9 @@ restatement of magnetostatics/dp3m.cpp and the reference's own data.
 
 Tolerances: the FP64 path against the FP64 oracle differs only by rounding
 (fixed-point mesh assignment with 2^-51 resolution, a different FFT and
-summation order): 1e-9 relative to the largest component.  The FP32 mesh
-path (single_precision=True) keeps the FP64 real-space part; its k-space
-carries FP32 rounding: 1e-4 relative rms.  Reference data are checked with
+summation order): 1e-9 relative to the largest component.  The FP32 path
+(single_precision=True: FP32 mesh, FFT and real-space pair terms, FP64
+sums) carries FP32 rounding: 1e-4 relative rms.  Reference data are checked with
 the tolerances of the reference's tests (p3m_madelung.py,
 dipolar_mdlc_p3m_scafacos_p2nfft.py).
 """
