@@ -136,7 +136,7 @@ public:
     k_dp3m_prepare<<<nb, 256, 0, st>>>(n, m_mu.as<double>(), m_comp.as<double>(), E.d_q(),
                                        m_flag.as<int>(), m_part.as<double>());
     ++E.m_launches;
-    k_dp3m_sum_rows<<<1, 32, 0, st>>>(m_part.as<double>(), nb, 5, m_sums.as<double>());
+    k_dp3m_sum_rows<<<1, 32 * 5, 0, st>>>(m_part.as<double>(), nb, 5, m_sums.as<double>());
     ++E.m_launches;
     int flag = 0;
     P3MX_CUDA(cudaMemcpyAsync(census.data(), m_sums.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -230,7 +230,7 @@ public:
             geom, E.m_blk_x.as<Blk>(), ck3, E.m_cplx, m_ge.as<Real>(), m_gf.as<Real>(), mode,
             E.m_field.as<C>(), E.m_tile_x, m_part.as<double>(), tw);
         ++E.m_launches;
-        k_dp3m_sum_rows<<<1, 32, 0, st>>>(m_part.as<double>(), E.m_n_blk_x, 1,
+        k_dp3m_sum_rows<<<1, 32 * 1, 0, st>>>(m_part.as<double>(), E.m_n_blk_x, 1,
                                           m_sums.as<double>() + 5);
         ++E.m_launches;
       } else {
@@ -339,7 +339,7 @@ public:
       };
       if (want_e) {
         pairs(std::true_type{}, want_ft ? f : nullptr, m_part.as<double>());
-        k_dp3m_sum_rows<<<1, 32, 0, st>>>(m_part.as<double>(), E.m_n_blk_pair, 1,
+        k_dp3m_sum_rows<<<1, 32 * 1, 0, st>>>(m_part.as<double>(), E.m_n_blk_pair, 1,
                                           m_sums.as<double>() + 6);
         ++E.m_launches;
       } else {
@@ -415,7 +415,7 @@ public:
     if (!m_phi_valid) {
       k_dp3m_self_sum<<<kSumBlocks, 256, 0, st>>>(m_M, m_L, m_alpha, m_cao, m_part.as<double>());
       ++m_eng.m_launches;
-      k_dp3m_sum_rows<<<1, 32, 0, st>>>(m_part.as<double>(), kSumBlocks, 1, m_sums.as<double>() + 7);
+      k_dp3m_sum_rows<<<1, 32 * 1, 0, st>>>(m_part.as<double>(), kSumBlocks, 1, m_sums.as<double>() + 7);
       ++m_eng.m_launches;
       P3MX_CUDA(cudaMemcpyAsync(&m_phi, m_sums.as<double>() + 7, sizeof(double),
                                 cudaMemcpyDeviceToHost, st));
@@ -600,7 +600,7 @@ double dp_ks_error(p3mx_dp3m *h, int M, int cao, double alpha_L) {
   int const nblk = Dp3mEngine::kSumBlocks;
   h->ks_part.ensure((nblk + 1) * sizeof(double));
   k_dp3m_ks_error<<<nblk, 256, 0, st>>>(M, cao, alpha_L, h->ks_part.as<double>());
-  k_dp3m_sum_rows<<<1, 32, 0, st>>>(h->ks_part.as<double>(), nblk, 1, h->ks_part.as<double>() + nblk);
+  k_dp3m_sum_rows<<<1, 32 * 1, 0, st>>>(h->ks_part.as<double>(), nblk, 1, h->ks_part.as<double>() + nblk);
   double he_q = 0.0;
   P3MX_CUDA(cudaGetLastError());
   P3MX_CUDA(cudaMemcpyAsync(&he_q, h->ks_part.as<double>() + nblk, sizeof(double),

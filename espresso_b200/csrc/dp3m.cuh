@@ -215,16 +215,22 @@ __global__ void k_dp3m_prepare(long long n, const double *__restrict__ mu,
   }
 }
 
-// Fixed-order sum of nblk rows of `width` partials (one thread per column).
+// Fixed-order sum of nblk rows of `width` partials: one warp per column
+// (launched with 32 * width threads), lane l summing rows l, l + 32, ...,
+// then a fixed shuffle tree (deterministic; the loads of a lane are
+// independent, not one serial chain per column).
 __global__ void k_dp3m_sum_rows(const double *__restrict__ partials, int nblk, int width,
                                 double *__restrict__ out) {
-  int const k = threadIdx.x;
+  int const k = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (k >= width)
     return;
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b)
+  for (int b = lane; b < nblk; b += 32)
     s += partials[static_cast<long long>(b) * width + k];
-  out[k] = s;
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0)
+    out[k] = s;
 }
 
 // ---- x pass of the dipolar k-space operator ------------------------------
