@@ -937,7 +937,8 @@ def run_dipolar(args):
     """Point-dipole workload: N dipoles of unit moment, random orientations,
     on a jittered lattice at number density 0.5 (cubic box), dipolar P3M
     tuned for accuracy 1e-4 (DipolarTuningAlgorithm: mesh, cao, r_cut,
-    alpha; outside the timed region), FP64 and FP32 mesh paths.  One step =
+    alpha; outside the timed region), FP64 and FP32 paths (``fp32_mesh``:
+    FP32 mesh, FFT and real-space pair terms, FP64 sums).  One step =
     one evaluation of forces and torques (k-space + real space) through
     p3mx_dp3m_compute with device pointers; e2e = the same through pinned
     host arrays (positions and moments in, forces and torques out).  Prints
