@@ -114,6 +114,25 @@ def test_fp32_mesh_path():
     assert e == pytest.approx(eo, rel=1e-5)
 
 
+def test_fp32_path_cell_grid():
+    """The FP32 path on a box of 4 cells per axis (the real-space pairs from
+    the cell-relative offsets and the entries' cell-offset fields, no
+    minimum-image arithmetic), against the oracle."""
+    L, n = 16.0, 300
+    pos, dip = _random(n, L, 11)
+    args = dict(prefactor=1.0, alpha=0.9, r_cut=3.0, mesh=32, cao=5, accuracy=1e-4)
+    s = _system(L, pos, dip)
+    s.magnetostatics.solver = DipolarP3M(tune=False, single_precision=True, **args)
+    f, t, e = _forces_torques_energy(s)
+    fo, to, eo = O.dp3m(L, pos, dip, 1.0, 0.9, 3.0, 32, 5, 1e-4)
+
+    def rms_rel(a, b):
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+    assert rms_rel(f, fo) < 1e-4
+    assert rms_rel(t, to) < 1e-4
+    assert e == pytest.approx(eo, rel=1e-5)
+
+
 def test_deterministic_and_repeatable():
     L, n = 10.0, 80
     pos, dip = _random(n, L, 5)
